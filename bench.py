@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the fiber monodomain hot path: node-steps/s of the FP32-reaction fused solver on the
+batched Hodgkin-Huxley workload (4096 fibers of 500-2500 nodes, Crank-Nicolson), next to the FP64
+split ("plain") solver, with accuracy against the CPU oracle and the oracle's CPU throughput.
+
+One step = one advance of 1 ms of simulated time (1000 Strang steps) over the whole batch.
+Multi-GPU (torchrun): every rank solves its own batch (seed = rank): fibers are independent, there
+is no data-path collective, scaling is weak; the timed region is bracketed by barriers and the
+reported time is the maximum over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "node-steps/s, FP32 batched vs FP64 plain at <=0.1 mV; adjoint/forward time"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--step-ms", type=float, default=1.0, help="simulated ms per step")
+    p.add_argument("--fibers", type=int, default=4096)
+    p.add_argument("--skip-fp64", action="store_true")
+    p.add_argument("--skip-accuracy", action="store_true")
+    p.add_argument("--threads", type=int, default=0, help="fused CTA threads (0 = default)")
+    p.add_argument("--nodes-per-thread", type=int, default=0)
+    p.add_argument("--steps-per-launch", type=int, default=0)
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    if os.path.exists(MEASURED_PEAKS):
+        d = json.load(open(MEASURED_PEAKS))
+        return d.get("hbm_gbs", FALLBACK_HBM_GBS), d.get("sm_max_mhz", 1965.0), "measured"
+    return FALLBACK_HBM_GBS, 1965.0, "fallback"
+
+
+def hh_ops():
+    meta = json.load(open(os.path.join(ROOT, "opendihu_b200/csrc/generated/hodgkin_huxley_1952_anone_c2_3_4.json")))
+    return meta["operations_per_rhs"]
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def allmax(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(system, sample_fibers: int, sample_ms: float, threads: int):
+    """Oracle (FP64 restatement of the reference's CPU path) on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+    from opendihu_b200 import workloads as WL
+    sub = WL.subset(system, np.arange(sample_fibers))
+    sub.end_time = sub.start_time + sample_ms
+    H.complete(sub)
+    t0 = time.perf_counter()
+    st, _, tr, n = H.run_oracle(sub.copy(), n_threads=threads)
+    dt = time.perf_counter() - t0
+    return sub, st, n, sub.n_nodes * n / dt, dt
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        return
+    from opendihu_b200 import workloads as WL
+    system = WL.batched_hh(n_fibers=args.fibers, seed=0)
+    threads = os.cpu_count() or 1
+    times = []
+    for k in range(args.warmup + args.steps):
+        _, _, n, rate, dt = cpu_baseline(system, 16, 0.2, threads)
+        if k >= args.warmup:
+            times.append(rate)
+    value = float(np.median(times))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "batched_hh sample: first 16 fibers of the 4096-fiber HH batch, 0.2 ms per step",
+                       "implementation": "CPU oracle port of the reference's vc FastMonodomainSolver (the reference "
+                                         "needs PETSc/MPI/Vc and cannot be built here)"},
+            "cpu_baseline": {"value": value, "unit": "node-steps/s", "cores": threads, "kind": "port",
+                             "sample": "16 fibers x 0.2 ms per step"},
+            "e2e": {"value": value, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    world, rank, local, pg = dist_setup(args)
+    from opendihu_b200 import solver as S
+    from opendihu_b200 import workloads as WL
+
+    system = WL.batched_hh(n_fibers=args.fibers, seed=rank)
+    n_nodes = system.n_nodes
+    fused = S.FastMonodomainSolver(system.copy(), method="fused", precision="fp32", profile=True, device=local,
+                                   threads_per_block=args.threads, nodes_per_thread=args.nodes_per_thread,
+                                   steps_per_launch=args.steps_per_launch)
+    fused.initialize()
+    step = args.step_ms
+    t = 0.0
+    for _ in range(args.warmup):
+        fused.setTimeSpan(t, t + step)
+        fused.advanceTimeSpan()
+        t += step
+    barrier(pg)
+    fused.reset_timing()
+    n0 = fused.split_steps()
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.steps):
+        fused.setTimeSpan(t, t + step)
+        fused.advanceTimeSpan()
+        t += step
+    clk = clocks.stop()
+    tm = fused.timing()
+    split_steps = fused.split_steps() - n0
+    dev_s = tm["advance_ms"] / 1e3
+    dev_s_max = allmax(pg, dev_s)
+    node_steps_rank = n_nodes * split_steps
+    value = node_steps_rank * world / dev_s_max
+    kernel_avg_ms = tm["main_kernel_ms"] / max(tm["main_kernel_launches"], 1)
+    launches_per_kernel = tm["main_kernel_launches"]
+    steps_per_launch = split_steps / max(launches_per_kernel, 1)
+
+    # end to end through the C ABI with host buffers: H2D of the states, advance, D2H of the states
+    host_states = fused.states()
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        fused.set_states(host_states)
+        fused.setTimeSpan(t, t + step)
+        fused.advanceTimeSpan()
+        host_states = fused.states()
+        t += step
+    e2e_s = allmax(pg, time.perf_counter() - t0)
+    e2e_value = n_nodes * (split_steps / args.steps) * e2e_steps * world / e2e_s
+    state_bytes = n_nodes * 8 * 4
+    fused.close()
+
+    # FP64 split ("plain") solver on the same batch
+    fp64_value = None
+    if not args.skip_fp64:
+        plain = S.FastMonodomainSolver(system.copy(), method="split", precision="fp64", profile=True, device=local)
+        plain.initialize()
+        tp = 0.0
+        plain.setTimeSpan(tp, tp + step)
+        plain.advanceTimeSpan()
+        tp += step
+        barrier(pg)
+        plain.reset_timing()
+        p0 = plain.split_steps()
+        n_plain = 2
+        for _ in range(n_plain):
+            plain.setTimeSpan(tp, tp + step)
+            plain.advanceTimeSpan()
+            tp += step
+        tmp = plain.timing()
+        p_s = allmax(pg, tmp["advance_ms"] / 1e3)
+        fp64_value = n_nodes * (plain.split_steps() - p0) * world / p_s
+        plain.close()
+
+    # accuracy against the FP64 oracle on a sample of the batch, and the oracle's CPU throughput
+    acc = None
+    cpu = None
+    if rank == 0 and not args.skip_accuracy:
+        threads = os.cpu_count() or 1
+        sub, ref, n_ref, rate, cpu_s = cpu_baseline(system, 4, 10.0, threads)
+        cpu = {"value": rate, "unit": "node-steps/s", "cores": threads, "kind": "port",
+               "sample": f"first 4 fibers of the batch ({sub.n_nodes} nodes) x 10 ms ({n_ref} Strang steps), "
+                         f"{cpu_s:.1f} s"}
+        acc = {}
+        for name, method, prec in (("fp32_fused", "fused", "fp32"), ("fp64_split", "split", "fp64")):
+            with S.FastMonodomainSolver(sub.copy(), method=method, precision=prec, device=local) as slv:
+                slv.advanceTimeSpan()
+                st = slv.states()
+            acc[name] = {"vm_max_abs_err_mV": float(np.max(np.abs(st[0] - ref[0])))}
+
+    peak_hbm, sm_max, peak_kind = peaks()
+    ops = hh_ops()
+    n0d = 5
+    fp32_flops_node_step = 2 * n0d * (2 * ops["flops"] + 6 + 9)
+    fp64_flops_node_step = 2 * n0d * 5 + 15
+    # algorithmic HBM bytes of one fused launch: states (Vm f64 + 3 gates f32) read+write, 3 parameters,
+    # 6 diffusion coefficients (f64) and the clamp map, per node
+    bytes_launch = n_nodes * (2 * (8 + 12) + 12 + 48 + 4)
+    achieved_gbs = bytes_launch / (kernel_avg_ms / 1e3) / 1e9 if kernel_avg_ms > 0 else None
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved_tf = n_nodes * steps_per_launch * fp32_flops_node_step / (kernel_avg_ms / 1e3) / 1e12 if kernel_avg_ms > 0 else None
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "fused_kernel_batched_hh.md")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("dram_bytes_per_node_per_launch:"):
+                traffic = float(ln.split(":", 1)[1]) * n_nodes
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 reaction + f64 Vm/diffusion",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "batched_hh: 4096 HH fibers/GPU, lengths U[500,2500] (seed=rank), dx 0.01 cm, "
+                                   "100 MUs (exponential sizes), Poisson 10-40 Hz firing, Crank-Nicolson, "
+                                   "dt0D 1e-4 ms, dt_split 1e-3 ms",
+                       "n_nodes_per_gpu": n_nodes, "step": f"{step} ms simulated = {split_steps // args.steps} Strang steps",
+                       "method": "fused persistent kernel, FP32 reaction", "l2": "inputs larger than L2 (~0.5 GB/GPU)",
+                       "parallelism": f"fibers sharded, {world} GPU(s), no collective"},
+            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes},
+            "gpu_launches": int(tm["kernel_launches"]),
+            "fp64_plain": {"value": fp64_value, "unit": "node-steps/s",
+                           "speedup_fp32_fused_over_fp64_plain": (value / fp64_value) if fp64_value else None},
+            "accuracy_vs_fp64_oracle": acc,
+            "adjoint_over_forward": None,
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak_hbm, "unit": "GB/s",
+                         "frac": (achieved_gbs / peak_hbm) if achieved_gbs else None, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "kernel": "fused_kernel (avg launch %.3f ms, %.0f Strang steps per launch)" % (
+                             kernel_avg_ms, steps_per_launch)},
+            "roofline_compute": {"bound": "fp32-alu", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                                 "frac": (achieved_tf / fp32_peak) if achieved_tf else None,
+                                 "peak_source": "derived: 148 SMs x 128 FP32 lanes x 2 x sm_max_mhz",
+                                 "flops_per_node_step": {"fp32": fp32_flops_node_step, "fp64": fp64_flops_node_step,
+                                                         "sfu_exp": 2 * n0d * 2 * ops["special"]}},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

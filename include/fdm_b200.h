@@ -1,0 +1,156 @@
+/* fdm_b200 — B200-native fiber monodomain solver, C ABI.
+ *
+ * This is the drop-in boundary for OpenDiHu's FastMonodomainSolver hot path
+ * (core/src/specialized_solver/fast_monodomain_solver/).  Plain C types only: pointers, sizes and
+ * int status codes; every array is a HOST array unless its name says "device".
+ *
+ * Reference interfaces replaced:
+ *  - fdm_create / fdm_set_* / fdm_advance / fdm_get_* replace the generated-library ABI the reference
+ *    loads with dlopen/dlsym, `initializeArrays(...)` and `computeMonodomain(...)`
+ *    (fast_monodomain_solver_gpu.tpp:361-365, :478-481, :187-196), whose sizes the reference bakes into
+ *    generated source (gpu.tpp:293-312); here sizes are run-time arguments.
+ *  - fdm_advance(t_start, t_end) is RepeatedCall<FastMonodomainSolver>::advanceTimeSpan
+ *    (repeated_call.tpp:43-80) driving FastMonodomainSolverBase::setTimeSpan + advanceTimeSpan
+ *    (fast_monodomain_solver_compute.tpp:14-129).
+ *  - fdm_checkpoint_save / fdm_checkpoint_restore are saveFiberDataCheckpoint /
+ *    restoreFiberDataCheckpoint (fast_monodomain_solver_communication.tpp:497-509).
+ *  - fdm_get_algebraics returns algebraicsForTransfer (03_generator_vc.cpp:1131-1160).
+ *  - fdm_compat_configure + initializeArrays + computeMonodomain export the reference's generated-library
+ *    symbols with their exact signatures (fast_monodomain_solver_gpu.tpp:361-365, :478-481).
+ *
+ * Errors: every function returns FDM_OK (0) or a positive FDM_ERR_* code; fdm_last_error() gives the
+ * message.  Nothing aborts the process.  One solver handle must not be used from two host threads
+ * at once; different handles are independent (each owns its CUDA stream and device memory).
+ */
+#ifndef FDM_B200_H
+#define FDM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDM_OK 0
+#define FDM_ERR_ARG 1          /* invalid argument or call order */
+#define FDM_ERR_CUDA 2         /* a CUDA call failed (message has the CUDA error string) */
+#define FDM_ERR_NAN 3          /* NaN or Inf in the transmembrane potential after an advance */
+#define FDM_ERR_UNSUPPORTED 4  /* combination not built into this library */
+#define FDM_ERR_NO_DEVICE 5    /* no CUDA device */
+#define FDM_ERR_TIMEOUT 6      /* a device-side wait gave up */
+
+#define FDM_MODEL_HODGKIN_HUXLEY_1952 0
+#define FDM_MODEL_SHORTEN_2007 1
+
+#define FDM_IMPLICIT_EULER 0
+#define FDM_CRANK_NICOLSON 1
+
+#define FDM_METHOD_SPLIT 0     /* reaction kernel + diffusion kernel per half/full step, states in HBM */
+#define FDM_METHOD_FUSED 1     /* one persistent kernel per window, states resident on chip */
+
+#define FDM_FP64 0
+#define FDM_FP32_REACTION 1    /* rates and gates in FP32; Vm accumulation and diffusion in FP64 */
+
+#define FDM_CLAMP_VC_LANES 0   /* lanes 0..min(3,W)-1 of the W-wide buffer holding the junction ("vc") */
+#define FDM_CLAMP_CENTER 1     /* junction node and its two neighbours ("gpu") */
+
+#define FDM_STIMULUS_CLAMP 0   /* Vm := valueForStimulatedPoint on stimulated nodes (reference) */
+#define FDM_STIMULUS_CURRENT 1 /* parameter stimulus_parameter := stimulus_value on stimulated nodes */
+
+typedef struct fdm_solver fdm_solver;
+
+typedef struct fdm_config {
+  int model;                     /* FDM_MODEL_* */
+  int diffusion_scheme;          /* FDM_IMPLICIT_EULER / FDM_CRANK_NICOLSON */
+  int method;                    /* FDM_METHOD_* */
+  int reaction_precision;        /* FDM_FP64 / FDM_FP32_REACTION */
+  int approximate_exponential_function; /* 1: exp(x) ~ (1+x/1024)^1024 as the reference's "vc" code */
+  int clamp_rule;                /* FDM_CLAMP_* */
+  int vc_width;                  /* W of the FDM_CLAMP_VC_LANES rule (4 = AVX2 build of the reference) */
+  int n_ranks;                   /* fibers are laid out as on n_ranks ranks (fiberNo % n_ranks) for the clamp rule */
+  int stimulus_mode;             /* FDM_STIMULUS_* */
+  int stimulus_parameter;        /* parameter index for FDM_STIMULUS_CURRENT */
+  double stimulus_value;
+  double value_for_stimulated_point;   /* "valueForStimulatedPoint", default 20 */
+  double dt_repeated_call;       /* RepeatedCall timeStepWidth */
+  double dt_splitting;           /* Strang timeStepWidth */
+  double dt_0d;                  /* Heun timeStepWidth */
+  double dt_1d;                  /* ImplicitEuler / CrankNicolson timeStepWidth */
+  int steps_per_launch;          /* split steps per launch window, 0 = default */
+  int threads_per_block;         /* fused kernel CTA size, 0 = choose */
+  int nodes_per_thread;          /* fused kernel nodes per thread, 0 = choose */
+  int check_nan;                 /* 1: fdm_advance fails with FDM_ERR_NAN if Vm is not finite */
+  int profile;                   /* 1: time the main kernel launches with CUDA events */
+  int device;                    /* CUDA device ordinal the solver lives on */
+} fdm_config;
+
+/* fills *cfg with the reference's defaults (HH, implicit Euler, FP64 split, vc rule W=4, 20 mV clamp) */
+void fdm_config_default(fdm_config *cfg);
+
+int fdm_create(const fdm_config *cfg, fdm_solver **out);
+int fdm_destroy(fdm_solver *s);
+/* message of the last failed call on s (or of the last failed fdm_create if s is NULL) */
+const char *fdm_last_error(const fdm_solver *s);
+
+/* model description: sizes and initial state values of the model's OpenCOR file */
+int fdm_model_info(int model, int *n_states, int *n_algebraics, int *n_parameters, double *states_initial);
+/* default value of every parameter slot: the raw CONSTANTS value for a constant parameter, 0 for an
+ * algebraic one (00_source_code_generator_base.cpp:67-81 fills missing parameters the same way) */
+int fdm_model_parameter_defaults(int model, double *defaults);
+
+/* Fibers: fiber_offsets[n_fibers+1] node offsets (fiber f owns nodes [off[f], off[f+1]), at least 2 nodes);
+ * element_lengths: fiber f's off[f+1]-off[f]-1 element lengths, concatenated in fiber order;
+ * prefactor[n_fibers]: sigma/(Am*Cm) per fiber ("prefactor" of the diffusion FEM settings).
+ * Resets states to the model's initial values and parameters to the model's defaults. */
+int fdm_set_fibers(fdm_solver *s, int n_fibers, const int64_t *fiber_offsets, const double *element_lengths,
+                   const double *prefactor);
+int fdm_set_prefactor(fdm_solver *s, const double *prefactor);
+
+/* parameters[p * n_nodes + node] (SoA, "parametersInitialValues" per instance) */
+int fdm_set_parameters(fdm_solver *s, const double *parameters);
+int fdm_get_parameters(fdm_solver *s, double *parameters);
+
+/* states[state * n_nodes + node] (SoA); state 0 is Vm */
+int fdm_set_states(fdm_solver *s, const double *states);
+int fdm_get_states(fdm_solver *s, double *states);
+int fdm_get_vm(fdm_solver *s, double *vm);
+
+/* Stimulation inputs (fast_monodomain_solver_initialization.tpp:145-347):
+ *  firing_events[rows*cols] (0/1, the firingTimesFile), motor_unit_no[f], stimulation_point_index[f]
+ *  (NMJ node within the fiber), call_frequency[f], repeat_after_first_call[f], call_enable_begin[f],
+ *  jitter[f*n_jitter + k] (setSpecificStatesFrequencyJitter). Resets the stimulation state machine. */
+int fdm_set_stimulation(fdm_solver *s, const uint8_t *firing_events, int rows, int cols, const int *motor_unit_no,
+                        const int *stimulation_point_index, const double *call_frequency,
+                        const double *repeat_after_first_call, const double *call_enable_begin,
+                        const double *jitter, int n_jitter);
+/* per fiber: first clamped node (global index, -1 if none), number of clamped nodes, machine evaluated */
+int fdm_get_clamp_nodes(fdm_solver *s, int64_t *first_node, int *count, uint8_t *evaluated);
+
+/* which algebraics to return after each advance ("algebraicsForTransfer") */
+int fdm_set_algebraics_for_transfer(fdm_solver *s, int n, const int *algebraic_indices);
+int fdm_get_algebraics(fdm_solver *s, double *out /* [k * n_nodes + node] */);
+
+/* record Vm at the given nodes after every split step (for activation times); capacity in split steps */
+int fdm_set_trace(fdm_solver *s, int n_nodes, const int64_t *nodes, int64_t capacity);
+int fdm_get_trace(fdm_solver *s, double *out /* [step * n_nodes + k] */, int64_t *n_steps_recorded);
+
+/* RepeatedCall over [t_start, t_end]: blocking; returns after the device finished. */
+int fdm_advance(fdm_solver *s, double t_start, double t_end);
+/* number of split steps done by all advances so far */
+int64_t fdm_split_steps(const fdm_solver *s);
+/* summed device time and count of the main kernel launches (config.profile = 1), and of all GPU work
+ * of the advances */
+int fdm_get_timing(const fdm_solver *s, double *main_kernel_ms, int64_t *main_kernel_launches,
+                   double *advance_ms, int64_t *kernel_launches);
+int fdm_reset_timing(fdm_solver *s);
+
+int fdm_checkpoint_save(fdm_solver *s);
+int fdm_checkpoint_restore(fdm_solver *s);
+
+/* number of the fused-kernel shapes built into the library and their (threads, nodes per thread) */
+int fdm_fused_shapes(int *threads, int *nodes_per_thread, int capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDM_B200_H */

@@ -1,0 +1,135 @@
+"""ctypes binding of libfdm_b200.so (the C ABI declared in include/fdm_b200.h).
+
+There is no CPU fallback: if the library is missing or has no CUDA device, the solver raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfdm_b200.so")
+
+FDM_OK = 0
+FDM_ERR_ARG = 1
+FDM_ERR_CUDA = 2
+FDM_ERR_NAN = 3
+FDM_ERR_UNSUPPORTED = 4
+FDM_ERR_NO_DEVICE = 5
+FDM_ERR_TIMEOUT = 6
+
+MODEL_IDS = {"hodgkin_huxley_1952": 0, "shorten_ocallaghan_davidson_soboleva_2007": 1}
+
+#: every symbol include/fdm_b200.h declares
+EXPORTED = [
+    "fdm_config_default", "fdm_create", "fdm_destroy", "fdm_last_error", "fdm_model_info",
+    "fdm_model_parameter_defaults", "fdm_set_fibers", "fdm_set_prefactor", "fdm_set_parameters",
+    "fdm_get_parameters", "fdm_set_states", "fdm_get_states", "fdm_get_vm", "fdm_set_stimulation",
+    "fdm_get_clamp_nodes", "fdm_set_algebraics_for_transfer", "fdm_get_algebraics", "fdm_set_trace",
+    "fdm_get_trace", "fdm_advance", "fdm_split_steps", "fdm_get_timing", "fdm_reset_timing",
+    "fdm_checkpoint_save", "fdm_checkpoint_restore", "fdm_fused_shapes",
+]
+
+
+class FdmError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[fdm error {code}] {message}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("model", C.c_int), ("diffusion_scheme", C.c_int), ("method", C.c_int),
+        ("reaction_precision", C.c_int), ("approximate_exponential_function", C.c_int),
+        ("clamp_rule", C.c_int), ("vc_width", C.c_int), ("n_ranks", C.c_int),
+        ("stimulus_mode", C.c_int), ("stimulus_parameter", C.c_int), ("stimulus_value", C.c_double),
+        ("value_for_stimulated_point", C.c_double), ("dt_repeated_call", C.c_double),
+        ("dt_splitting", C.c_double), ("dt_0d", C.c_double), ("dt_1d", C.c_double),
+        ("steps_per_launch", C.c_int), ("threads_per_block", C.c_int), ("nodes_per_thread", C.c_int),
+        ("check_nan", C.c_int), ("profile", C.c_int), ("device", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FdmError(FDM_ERR_ARG, f"{LIB_PATH} is missing; build it with opendihu_b200.build.build()")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    d = C.POINTER(C.c_double)
+    i64 = C.POINTER(C.c_int64)
+    i32 = C.POINTER(C.c_int)
+    u8 = C.POINTER(C.c_uint8)
+    sig = {
+        "fdm_config_default": (None, [C.POINTER(Config)]),
+        "fdm_create": (C.c_int, [C.POINTER(Config), C.POINTER(P)]),
+        "fdm_destroy": (C.c_int, [P]),
+        "fdm_last_error": (C.c_char_p, [P]),
+        "fdm_model_info": (C.c_int, [C.c_int, i32, i32, i32, d]),
+        "fdm_model_parameter_defaults": (C.c_int, [C.c_int, d]),
+        "fdm_set_fibers": (C.c_int, [P, C.c_int, i64, d, d]),
+        "fdm_set_prefactor": (C.c_int, [P, d]),
+        "fdm_set_parameters": (C.c_int, [P, d]),
+        "fdm_get_parameters": (C.c_int, [P, d]),
+        "fdm_set_states": (C.c_int, [P, d]),
+        "fdm_get_states": (C.c_int, [P, d]),
+        "fdm_get_vm": (C.c_int, [P, d]),
+        "fdm_set_stimulation": (C.c_int, [P, u8, C.c_int, C.c_int, i32, i32, d, d, d, d, C.c_int]),
+        "fdm_get_clamp_nodes": (C.c_int, [P, i64, i32, u8]),
+        "fdm_set_algebraics_for_transfer": (C.c_int, [P, C.c_int, i32]),
+        "fdm_get_algebraics": (C.c_int, [P, d]),
+        "fdm_set_trace": (C.c_int, [P, C.c_int, i64, C.c_int64]),
+        "fdm_get_trace": (C.c_int, [P, d, i64]),
+        "fdm_advance": (C.c_int, [P, C.c_double, C.c_double]),
+        "fdm_split_steps": (C.c_int64, [P]),
+        "fdm_get_timing": (C.c_int, [P, d, i64, d, i64]),
+        "fdm_reset_timing": (C.c_int, [P]),
+        "fdm_checkpoint_save": (C.c_int, [P]),
+        "fdm_checkpoint_restore": (C.c_int, [P]),
+        "fdm_fused_shapes": (C.c_int, [i32, i32, C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def ptr(a: np.ndarray, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def check(rc: int, handle=None):
+    if rc != FDM_OK:
+        msg = lib().fdm_last_error(handle)
+        raise FdmError(rc, msg.decode() if msg else "")
+
+
+def default_config() -> Config:
+    c = Config()
+    lib().fdm_config_default(C.byref(c))
+    return c
+
+
+def model_info(model: int):
+    ns, na, npar = C.c_int(), C.c_int(), C.c_int()
+    init = np.zeros(128)
+    check(lib().fdm_model_info(model, C.byref(ns), C.byref(na), C.byref(npar), ptr(init, C.c_double)))
+    defaults = np.zeros(max(npar.value, 1))
+    check(lib().fdm_model_parameter_defaults(model, ptr(defaults, C.c_double)))
+    return ns.value, na.value, npar.value, init[:ns.value].copy(), defaults[:npar.value].copy()
+
+
+def fused_shapes():
+    t = np.zeros(64, np.int32)
+    m = np.zeros(64, np.int32)
+    n = lib().fdm_fused_shapes(ptr(t, C.c_int), ptr(m, C.c_int), 64)
+    return [(int(t[i]), int(m[i])) for i in range(n)]

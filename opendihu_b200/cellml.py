@@ -1,0 +1,757 @@
+"""CellML (OpenCOR C export) parser and code emitter.
+
+The reference turns an OpenCOR-exported C file (``initConsts`` / ``computeRates``)
+into model code at run time: it parses every assignment line into an expression
+tree, substitutes per-instance *parameters* for selected CONSTANTS / ALGEBRAIC
+entries, replaces ``pow(x, <int>)`` by integer-power helpers and ``exp`` / ``log`` by
+helpers that may be approximated, and then emits vectorised C++
+(core/src/cellml/source_code_generator/00_parse_source_code_file.cpp:159-357,
+03_generator_vc.cpp:13-302 and :304-617).
+
+This module does the same job for the B200 build, ahead of time:
+
+* :func:`parse_model_file` reads the OpenCOR C file into a :class:`Model`
+  (initial states, folded constants, assignment lines as expression trees,
+  variable names from the header comments).
+* :func:`emit_cuda_model` writes a ``__device__`` right-hand side templated on the
+  arithmetic type (``double`` for the FP64 path, ``float`` for FP32 reaction)
+  and on a math policy (exact or approximate exp/log).
+* :func:`emit_c_model` writes the same right-hand side as scalar C for the CPU
+  oracle.
+* :func:`emit_cuda_vjp` writes the reverse-mode (vector-Jacobian) product of the
+  right-hand side used by the hand-written adjoint.
+
+Parameter substitution follows the reference exactly
+(00_parse_source_code_file.cpp:281-323): the assignment line of an algebraic
+that is a parameter is dropped and every later read of it becomes
+``PARAMS[j]``; a constant that is a parameter is read as
+``PARAMS[nAlgebraicParameters + j]`` in the right-hand side lines only, while
+the derived constants of ``initConsts`` keep using the file's raw values
+(00_source_code_generator_base.cpp:45-113, 03_generator_vc.cpp:937-944).
+"""
+from __future__ import annotations
+
+import math
+import os
+import re
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+# ----------------------------------------------------------------------------------------------
+# tokenizer / parser for the C expression subset used by OpenCOR exports
+# ----------------------------------------------------------------------------------------------
+
+_TOKEN_RE = re.compile(r"""
+    (?P<num>(?:\d+\.\d*|\.\d+|\d+)(?:[eE][+-]?\d+)?)
+  | (?P<arr>(?:STATES|CONSTANTS|ALGEBRAIC|RATES)\s*\[\s*\d+\s*\])
+  | (?P<name>[A-Za-z_][A-Za-z_0-9]*)
+  | (?P<op>&&|\|\||<=|>=|==|!=|[-+*/<>()?:,!])
+  | (?P<ws>\s+)
+""", re.VERBOSE)
+
+_KIND = {"STATES": "S", "CONSTANTS": "C", "ALGEBRAIC": "A", "RATES": "R"}
+
+
+def tokenize(text: str) -> List[Tuple[str, object]]:
+    pos = 0
+    out: List[Tuple[str, object]] = []
+    while pos < len(text):
+        m = _TOKEN_RE.match(text, pos)
+        if not m:
+            raise ValueError(f"cannot tokenize at {text[pos:pos + 30]!r}")
+        pos = m.end()
+        kind = m.lastgroup
+        if kind == "ws":
+            continue
+        val = m.group(kind)
+        if kind == "arr":
+            name, idx = val.split("[")
+            out.append(("var", (_KIND[name.strip()], int(idx.strip().rstrip("]").strip()))))
+        elif kind == "name":
+            if val == "VOI":
+                out.append(("var", ("T", 0)))
+            else:
+                out.append(("name", val))
+        else:
+            out.append((kind, val))
+    out.append(("end", None))
+    return out
+
+
+# binary operator precedence (C): || < && < == != < < <= > >= < + - < * /
+_BIN_PREC = {"||": 1, "&&": 2, "==": 3, "!=": 3, "<": 4, "<=": 4, ">": 4, ">=": 4,
+             "+": 5, "-": 5, "*": 6, "/": 6}
+
+
+class _Parser:
+    def __init__(self, tokens):
+        self.t = tokens
+        self.i = 0
+
+    def peek(self):
+        return self.t[self.i]
+
+    def take(self, kind=None, val=None):
+        tok = self.t[self.i]
+        if kind is not None and tok[0] != kind:
+            raise ValueError(f"expected {kind} {val} got {tok}")
+        if val is not None and tok[1] != val:
+            raise ValueError(f"expected {val} got {tok}")
+        self.i += 1
+        return tok
+
+    def expr(self):
+        return self.ternary()
+
+    def ternary(self):
+        cond = self.binary(1)
+        if self.peek() == ("op", "?"):
+            self.take()
+            a = self.ternary()
+            self.take("op", ":")
+            b = self.ternary()
+            return ("tern", cond, a, b)
+        return cond
+
+    def binary(self, min_prec):
+        left = self.unary()
+        while True:
+            tok = self.peek()
+            if tok[0] != "op" or tok[1] not in _BIN_PREC:
+                return left
+            prec = _BIN_PREC[tok[1]]
+            if prec < min_prec:
+                return left
+            self.take()
+            right = self.binary(prec + 1)  # left associative
+            left = ("bin", tok[1], left, right)
+
+    def unary(self):
+        tok = self.peek()
+        if tok == ("op", "-"):
+            self.take()
+            return ("neg", self.unary())
+        if tok == ("op", "+"):
+            self.take()
+            return ("pos", self.unary())
+        if tok == ("op", "!"):
+            self.take()
+            return ("not", self.unary())
+        return self.primary()
+
+    def primary(self):
+        tok = self.take()
+        if tok[0] == "num":
+            return ("num", tok[1], float(tok[1]))
+        if tok[0] == "var":
+            return ("var",) + tuple(tok[1])
+        if tok[0] == "name":
+            fname = tok[1]
+            self.take("op", "(")
+            args = [self.expr()]
+            while self.peek() == ("op", ","):
+                self.take()
+                args.append(self.expr())
+            self.take("op", ")")
+            return ("call", fname, args)
+        if tok == ("op", "("):
+            e = self.expr()
+            self.take("op", ")")
+            return e
+        raise ValueError(f"unexpected token {tok}")
+
+
+def parse_expression(text: str):
+    p = _Parser(tokenize(text))
+    e = p.expr()
+    if p.peek()[0] != "end":
+        raise ValueError(f"trailing tokens in {text!r}: {p.t[p.i:]}")
+    return e
+
+
+# ----------------------------------------------------------------------------------------------
+# model
+# ----------------------------------------------------------------------------------------------
+
+@dataclass
+class Model:
+    """A parsed OpenCOR C model."""
+    name: str
+    source: str
+    n_states: int
+    n_algebraics: int
+    n_constants: int
+    states_initial: List[float]
+    constants: List[float]                      # folded raw values after initConsts
+    constant_lines: List[Tuple[int, object]]    # (index, expr) in initConsts order
+    lines: List[Tuple[str, int, object]]        # (kind 'A'|'R', index, expr) right-hand side
+    state_names: List[str] = field(default_factory=list)
+    algebraic_names: List[str] = field(default_factory=list)
+    constant_names: List[str] = field(default_factory=list)
+    uses_voi: bool = False
+
+
+def _int_pow_value(x: float, n: int) -> float:
+    """Integer power by the reference helper recursion (03_generator_vc.cpp:549-608)."""
+    if n < 0:
+        return 1.0 / _int_pow_value(x, -n)
+    if n == 1:
+        return x
+    if n == 2:
+        return x * x
+    e0 = n // 2
+    e1 = n - e0
+    if e0 == 1:
+        return x * _int_pow_value(x, e1)
+    return _int_pow_value(x, e0) * _int_pow_value(x, e1)
+
+
+def eval_expr(e, env) -> float:
+    """Evaluate an expression tree in IEEE double (used to fold initConsts)."""
+    t = e[0]
+    if t == "num":
+        return e[2]
+    if t == "var":
+        return env[e[1]][e[2]] if e[1] != "T" else env["T"]
+    if t == "neg":
+        return -eval_expr(e[1], env)
+    if t == "pos":
+        return eval_expr(e[1], env)
+    if t == "not":
+        return 0.0 if eval_expr(e[1], env) else 1.0
+    if t == "bin":
+        op = e[1]
+        a = eval_expr(e[2], env)
+        if op == "&&":
+            return 1.0 if (a and eval_expr(e[3], env)) else 0.0
+        if op == "||":
+            return 1.0 if (a or eval_expr(e[3], env)) else 0.0
+        b = eval_expr(e[3], env)
+        return {"+": lambda: a + b, "-": lambda: a - b, "*": lambda: a * b, "/": lambda: a / b,
+                "<": lambda: float(a < b), "<=": lambda: float(a <= b), ">": lambda: float(a > b),
+                ">=": lambda: float(a >= b), "==": lambda: float(a == b),
+                "!=": lambda: float(a != b)}[op]()
+    if t == "tern":
+        return eval_expr(e[2], env) if eval_expr(e[1], env) else eval_expr(e[3], env)
+    if t == "call":
+        f = e[1]
+        args = [eval_expr(a, env) for a in e[2]]
+        if f == "exp":
+            return math.exp(args[0])
+        if f == "log":
+            return math.log(args[0])
+        if f == "pow":
+            return math.pow(args[0], args[1])
+        if f == "fabs":
+            return abs(args[0])
+        if f == "sqrt":
+            return math.sqrt(args[0])
+        raise ValueError(f"unknown function {f}")
+    raise ValueError(f"bad node {e}")
+
+
+_NAME_RE = re.compile(r"\*\s*(STATES|ALGEBRAIC|CONSTANTS)\[(\d+)\] is (\S+) in component (\S+) \(")
+
+
+def parse_model_file(path: str, name: Optional[str] = None) -> Model:
+    """Parse an OpenCOR C export.
+
+    Line handling follows 00_parse_source_code_file.cpp:183-354: ``void`` is
+    joined with the next line, ``STATES[i] = v`` lines before ``computeRates`` give
+    initial values, ``CONSTANTS[i] = ...`` lines inside ``initConsts`` are the
+    constant assignments, ``ALGEBRAIC`` / ``RATES`` lines after it are the right-hand
+    side, and algebraics that are assigned a second time (in
+    ``computeVariables``) are skipped.
+    """
+    with open(path) as f:
+        text = f.read()
+    header = re.search(r"There are a total of (\d+) entries in the algebraic variable array\.\s*"
+                       r"\s*There are a total of (\d+) entries in each of the rate and state variable arrays\.\s*"
+                       r"\s*There are a total of (\d+) entries in the constant variable array", text)
+    if not header:
+        raise ValueError(f"{path}: not an OpenCOR C export (missing size header)")
+    n_alg, n_states, n_const = (int(x) for x in header.groups())
+    names = {"STATES": [""] * n_states, "ALGEBRAIC": [""] * n_alg, "CONSTANTS": [""] * n_const}
+    for m in _NAME_RE.finditer(text):
+        arr, idx, var, comp = m.group(1), int(m.group(2)), m.group(3), m.group(4)
+        if idx < len(names[arr]):
+            names[arr][idx] = f"{comp}/{var}"
+
+    states_init = [0.0] * n_states
+    constant_lines: List[Tuple[int, object]] = []
+    lines: List[Tuple[str, int, object]] = []
+    assigned_alg = set()
+    in_init = False
+    header_done = False
+    uses_voi = False
+    raw_lines = text.split("\n")
+    i = 0
+    while i < len(raw_lines):
+        line = raw_lines[i]
+        i += 1
+        if line == "void" and i < len(raw_lines):
+            line = line + " " + raw_lines[i]
+            i += 1
+        if not header_done and line.startswith("STATES["):
+            idx = int(line[7:line.index("]")])
+            states_init[idx] = float(line[line.index("= ") + 2:].strip().rstrip(";"))
+        if "initConsts" in line:
+            in_init = True
+            continue
+        if "}" in line and in_init:
+            in_init = False
+            continue
+        if line.startswith("CONSTANTS["):
+            lhs, rhs = line.split("=", 1)
+            idx = int(lhs[lhs.index("[") + 1:lhs.index("]")])
+            constant_lines.append((idx, parse_expression(rhs.strip().rstrip(";"))))
+            continue
+        if "computeRates" in line:
+            header_done = True
+            continue
+        if header_done and (line.startswith("ALGEBRAIC") or line.startswith("RATES")):
+            lhs, rhs = line.split("=", 1)
+            kind = "A" if lhs.startswith("ALGEBRAIC") else "R"
+            idx = int(lhs[lhs.index("[") + 1:lhs.index("]")])
+            if kind == "A":
+                if idx in assigned_alg:
+                    continue
+                assigned_alg.add(idx)
+            expr = parse_expression(rhs.strip().rstrip(";"))
+            if "VOI" in rhs:
+                uses_voi = True
+            lines.append((kind, idx, expr))
+
+    # fold the constants in initConsts order, in IEEE double
+    consts = [0.0] * n_const
+    env = {"S": states_init, "C": consts, "A": [], "R": [], "T": 0.0}
+    for idx, expr in constant_lines:
+        consts[idx] = eval_expr(expr, env)
+
+    return Model(name=name or os.path.splitext(os.path.basename(path))[0], source=path,
+                 n_states=n_states, n_algebraics=n_alg, n_constants=n_const,
+                 states_initial=states_init, constants=consts, constant_lines=constant_lines,
+                 lines=lines, state_names=names["STATES"], algebraic_names=names["ALGEBRAIC"],
+                 constant_names=names["CONSTANTS"], uses_voi=uses_voi)
+
+
+# ----------------------------------------------------------------------------------------------
+# parameter substitution
+# ----------------------------------------------------------------------------------------------
+
+def substitute_parameters(model: Model, params_alg: Sequence[int], params_const: Sequence[int]):
+    """Return the right-hand side lines with parameters substituted.
+
+    Follows 00_parse_source_code_file.cpp:281-323: the line assigning an
+    algebraic parameter is dropped, reads of it become PARAMS[j], reads of a
+    constant parameter become PARAMS[len(params_alg) + j].
+    """
+    alg_map = {a: j for j, a in enumerate(params_alg)}
+    const_map = {c: len(params_alg) + j for j, c in enumerate(params_const)}
+
+    def sub(e):
+        t = e[0]
+        if t == "var":
+            if e[1] == "A" and e[2] in alg_map:
+                return ("var", "P", alg_map[e[2]])
+            if e[1] == "C" and e[2] in const_map:
+                return ("var", "P", const_map[e[2]])
+            return e
+        if t in ("num",):
+            return e
+        if t in ("neg", "pos", "not"):
+            return (t, sub(e[1]))
+        if t == "bin":
+            return ("bin", e[1], sub(e[2]), sub(e[3]))
+        if t == "tern":
+            return ("tern", sub(e[1]), sub(e[2]), sub(e[3]))
+        if t == "call":
+            return ("call", e[1], [sub(a) for a in e[2]])
+        raise ValueError(e)
+
+    out = []
+    for kind, idx, expr in model.lines:
+        if kind == "A" and idx in alg_map:
+            continue
+        out.append((kind, idx, sub(expr)))
+    return out
+
+
+# ----------------------------------------------------------------------------------------------
+# emitters
+# ----------------------------------------------------------------------------------------------
+
+def _hexf(v: float) -> str:
+    """Exact double literal (C99 hex float)."""
+    if v == 0.0:
+        return "0.0" if math.copysign(1.0, v) > 0 else "-0.0"
+    if math.isinf(v) or math.isnan(v):
+        raise ValueError("non-finite constant")
+    return float.hex(v)
+
+
+def _int_exponent(e) -> Optional[int]:
+    """Integer exponent detection of the reference (03_generator_vc.cpp:68-117):
+    a literal made only of digits, sign and dot whose atoi is non-zero."""
+    neg = False
+    while e[0] in ("neg", "pos"):
+        neg ^= e[0] == "neg"
+        e = e[1]
+    if e[0] != "num":
+        return None
+    txt = e[1]
+    if re.fullmatch(r"[0-9.+-]+", txt) is None:
+        return None
+    m = re.match(r"\s*[+-]?\d+", txt)
+    n = int(m.group(0)) if m else 0
+    if n == 0:
+        return None
+    return -n if neg else n
+
+
+class _Emitter:
+    """Emits an expression tree as C / CUDA source text."""
+
+    def __init__(self, real: str, const_values: List[float], target: str):
+        self.real = real            # C type name used for literals and casts
+        self.consts = const_values
+        self.target = target        # "cuda" or "c"
+
+    def lit(self, v: float) -> str:
+        return f"(({self.real}){_hexf(v)})"
+
+    def var(self, kind: str, idx: int) -> str:
+        if kind == "S":
+            return f"STATES[{idx}]"
+        if kind == "C":
+            return self.lit(self.consts[idx])
+        if kind == "A":
+            return f"ALGEBRAIC[{idx}]"
+        if kind == "R":
+            return f"RATES[{idx}]"
+        if kind == "P":
+            return f"PARAMS[{idx}]"
+        if kind == "T":
+            return "VOI"
+        raise ValueError(kind)
+
+    def expr(self, e) -> str:
+        t = e[0]
+        if t == "num":
+            return f"(({self.real}){e[1]})"
+        if t == "var":
+            return self.var(e[1], e[2])
+        if t == "neg":
+            return f"(-{self.expr(e[1])})"
+        if t == "pos":
+            return f"(+{self.expr(e[1])})"
+        if t == "not":
+            return f"(!{self.expr(e[1])})"
+        if t == "bin":
+            return f"({self.expr(e[2])} {e[1]} {self.expr(e[3])})"
+        if t == "tern":
+            return f"(({self.expr(e[1])}) ? {self.expr(e[2])} : {self.expr(e[3])})"
+        if t == "call":
+            f = e[1]
+            if f == "pow":
+                n = _int_exponent(e[2][1])
+                if n is not None:
+                    if n > 0:
+                        return f"FDM_POW{n}({self.expr(e[2][0])})"
+                    return f"(({self.real})1.0/FDM_POW{-n}({self.expr(e[2][0])}))"
+                return f"FDM_POWF({self.expr(e[2][0])}, {self.expr(e[2][1])})"
+            if f == "exp":
+                return f"FDM_EXP({self.expr(e[2][0])})"
+            if f == "log":
+                return f"FDM_LOG({self.expr(e[2][0])})"
+            if f == "fabs":
+                return f"FDM_ABS({self.expr(e[2][0])})"
+            if f == "sqrt":
+                return f"FDM_SQRT({self.expr(e[2][0])})"
+            raise ValueError(f"unsupported function {f}")
+        raise ValueError(e)
+
+
+def _collect_int_pows(lines) -> List[int]:
+    found = set()
+
+    def walk(e):
+        t = e[0]
+        if t == "call":
+            if e[1] == "pow":
+                n = _int_exponent(e[2][1])
+                if n is not None:
+                    found.add(abs(n))
+            for a in e[2]:
+                walk(a)
+        elif t in ("neg", "pos", "not"):
+            walk(e[1])
+        elif t == "bin":
+            walk(e[2])
+            walk(e[3])
+        elif t == "tern":
+            walk(e[1])
+            walk(e[2])
+            walk(e[3])
+    for _, _, e in lines:
+        walk(e)
+    # close over the recursion of the helpers
+    changed = True
+    while changed:
+        changed = False
+        for n in list(found):
+            if n > 2:
+                e0 = n // 2
+                e1 = n - e0
+                for k in (e0, e1):
+                    if k > 1 and k not in found:
+                        found.add(k)
+                        changed = True
+    return sorted(found)
+
+
+def _pow_macro_defs(pows: List[int], prefix: str = "") -> List[str]:
+    out = []
+    for n in pows:
+        if n == 1:
+            out.append(f"#define FDM_POW1(x) (x)")
+        elif n == 2:
+            out.append(f"#define FDM_POW2(x) fdm_pow2(x)")
+        else:
+            out.append(f"#define FDM_POW{n}(x) fdm_pow{n}(x)")
+    return out
+
+
+def _pow_helpers(pows: List[int], qual: str) -> List[str]:
+    """Integer power helpers with the reference's multiplication order
+    (03_generator_vc.cpp:549-608): pow2 = x*x; powN = pow_{N/2}*pow_{N-N/2},
+    written x*(pow_{N-1}) when N/2 == 1."""
+    out = []
+    for n in pows:
+        if n < 2:
+            continue
+        if n == 2:
+            out.append(f"template<class R> {qual} R fdm_pow2(R x) {{ return x*x; }}")
+            continue
+        e0 = n // 2
+        e1 = n - e0
+        if e0 == 1:
+            body = f"x*(fdm_pow{e1}(x))"
+        else:
+            body = f"fdm_pow{e0}(x)*fdm_pow{e1}(x)"
+        out.append(f"template<class R> {qual} R fdm_pow{n}(R x) {{ return {body}; }}")
+    return out
+
+
+def variant_tag(params_alg: Sequence[int], params_const: Sequence[int]) -> str:
+    a = "_".join(str(x) for x in params_alg) or "none"
+    c = "_".join(str(x) for x in params_const) or "none"
+    return f"a{a}_c{c}"
+
+
+def _ident(model: Model) -> str:
+    return re.sub(r"[^A-Za-z0-9_]", "_", model.name)
+
+
+def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> str:
+    """CUDA device right-hand side for one parameter variant.
+
+    The struct exposes ``rates<R, M>(VOI, STATES, PARAMS, RATES, ALGEBRAIC)``; R is
+    the arithmetic type and M a math policy providing exp / log / pow.
+    """
+    lines = substitute_parameters(model, params_alg, params_const)
+    em = _Emitter("R", model.constants, "cuda")
+    ident = _ident(model)
+    tag = variant_tag(params_alg, params_const)
+    pows = _collect_int_pows(lines)
+    n_params = len(params_alg) + len(params_const)
+    out = []
+    out.append("// Generated by opendihu_b200/cellml.py from the OpenCOR C export "
+               f"{os.path.basename(model.source)}; do not edit.")
+    out.append(f"// parametersUsedAsAlgebraic = {list(params_alg)}, parametersUsedAsConstant = {list(params_const)}")
+    out.append("#pragma once")
+    out.append('#include "../fdm_math.cuh"')
+    out.append("")
+    out.append(f"struct fdm_model_{ident}_{tag} {{")
+    out.append(f"  static constexpr int nStates = {model.n_states};")
+    out.append(f"  static constexpr int nAlgebraics = {model.n_algebraics};")
+    out.append(f"  static constexpr int nParameters = {n_params};")
+    out.append(f"  static constexpr bool usesTime = {'true' if model.uses_voi else 'false'};")
+    out.append(f"  static constexpr const char* name = \"{model.name}\";")
+    out.append(f"  static constexpr double statesInitialValues[{model.n_states}] = {{"
+               + ", ".join(_hexf(v) for v in model.states_initial) + "};")
+    defaults = [0.0] * len(params_alg) + [model.constants[c] for c in params_const]
+    out.append(f"  static constexpr double parameterDefaults[{max(n_params, 1)}] = {{"
+               + ", ".join(_hexf(v) for v in (defaults or [0.0])) + "};")
+    out.extend("  " + s for s in _pow_helpers(pows, "__device__ __forceinline__ static"))
+    out.append("  template<class R, class M>")
+    out.append("  __device__ __forceinline__ static void rates(const R VOI, const R* __restrict__ STATES,"
+               " const R* __restrict__ PARAMS, R* __restrict__ RATES, R* __restrict__ ALGEBRAIC)")
+    out.append("  {")
+    out.append("    (void)VOI; (void)PARAMS;")
+    out.append("#define FDM_EXP(x) M::exp(x)")
+    out.append("#define FDM_LOG(x) M::log(x)")
+    out.append("#define FDM_POWF(x, y) M::pow(x, y)")
+    out.append("#define FDM_ABS(x) fabs(x)")
+    out.append("#define FDM_SQRT(x) sqrt(x)")
+    out.extend("#define " + s.split("#define ", 1)[1] for s in _pow_macro_defs(pows))
+    for kind, idx, expr in lines:
+        tgt = f"ALGEBRAIC[{idx}]" if kind == "A" else f"RATES[{idx}]"
+        out.append(f"    {tgt} = {em.expr(expr)};")
+    for n in pows:
+        out.append(f"#undef FDM_POW{n}")
+    out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
+    out.append("  }")
+    out.append("};")
+    out.append("")
+    return "\n".join(out)
+
+
+def emit_c_model(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> str:
+    """Scalar C right-hand side for the CPU oracle (same expression trees)."""
+    lines = substitute_parameters(model, params_alg, params_const)
+    em = _Emitter("double", model.constants, "c")
+    ident = _ident(model)
+    tag = variant_tag(params_alg, params_const)
+    pows = _collect_int_pows(lines)
+    out = []
+    out.append("/* Generated by opendihu_b200/cellml.py from the OpenCOR C export "
+               f"{os.path.basename(model.source)}; do not edit. */")
+    out.append(f"/* parametersUsedAsAlgebraic = {list(params_alg)}, parametersUsedAsConstant = {list(params_const)} */")
+    out.append("#pragma once")
+    out.append('#include "../oracle_math.h"')
+    for n in pows:
+        if n < 2:
+            continue
+        if n == 2:
+            out.append(f"static inline double oracle_{ident}_{tag}_pow2(double x) {{ return x*x; }}")
+        else:
+            e0 = n // 2
+            e1 = n - e0
+            if e0 == 1:
+                body = f"x*(oracle_{ident}_{tag}_pow{e1}(x))"
+            else:
+                body = f"oracle_{ident}_{tag}_pow{e0}(x)*oracle_{ident}_{tag}_pow{e1}(x)"
+            out.append(f"static inline double oracle_{ident}_{tag}_pow{n}(double x) {{ return {body}; }}")
+    out.append(f"#define ORACLE_{ident.upper()}_{tag.upper()}_N_STATES {model.n_states}")
+    out.append(f"#define ORACLE_{ident.upper()}_{tag.upper()}_N_ALGEBRAICS {model.n_algebraics}")
+    out.append(f"#define ORACLE_{ident.upper()}_{tag.upper()}_N_PARAMETERS {len(params_alg) + len(params_const)}")
+    out.append(f"static void oracle_{ident}_{tag}_rates(double VOI, const double *STATES, const double *PARAMS,"
+               f" double *RATES, double *ALGEBRAIC, int approx)")
+    out.append("{")
+    out.append("  (void)VOI; (void)PARAMS;")
+    out.append("#define FDM_EXP(x) (approx ? oracle_approx_exp(x) : exp(x))")
+    out.append("#define FDM_LOG(x) (approx ? oracle_approx_log(x) : log(x))")
+    out.append("#define FDM_POWF(x, y) pow(x, y)")
+    out.append("#define FDM_ABS(x) fabs(x)")
+    out.append("#define FDM_SQRT(x) sqrt(x)")
+    for n in pows:
+        if n == 1:
+            out.append("#define FDM_POW1(x) (x)")
+        else:
+            out.append(f"#define FDM_POW{n}(x) oracle_{ident}_{tag}_pow{n}(x)")
+    for kind, idx, expr in lines:
+        tgt = f"ALGEBRAIC[{idx}]" if kind == "A" else f"RATES[{idx}]"
+        out.append(f"  {tgt} = {em.expr(expr)};")
+    for n in pows:
+        out.append(f"#undef FDM_POW{n}")
+    out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
+    out.append("}")
+    out.append(f"static const double oracle_{ident}_{tag}_states_initial[{model.n_states}] = {{"
+               + ", ".join(_hexf(v) for v in model.states_initial) + "};")
+    out.append("")
+    return "\n".join(out)
+
+
+# ----------------------------------------------------------------------------------------------
+# the prebuilt variants
+# ----------------------------------------------------------------------------------------------
+
+#: (model file basename, parametersUsedAsAlgebraic, parametersUsedAsConstant) compiled into the
+#: library.  A settings dict may use any subset of a variant's constant parameters (the unused
+#: slots are filled with the constants' raw values, which gives identical arithmetic).
+VARIANTS = [
+    ("hodgkin_huxley_1952.c", (), (2, 3, 4)),
+    ("shorten_ocallaghan_davidson_soboleva_2007.c", (32,), (65,)),
+]
+
+
+def generate_all(input_dir: str, cuda_dir: str, c_dir: str) -> List[str]:
+    """(Re)generate the device and oracle model sources for every prebuilt variant."""
+    written = []
+    for fname, pa, pc in VARIANTS:
+        model = parse_model_file(os.path.join(input_dir, fname))
+        tag = variant_tag(pa, pc)
+        for text, d, ext in ((emit_cuda_model(model, pa, pc), cuda_dir, ".cuh"),
+                             (emit_c_model(model, pa, pc), c_dir, ".h")):
+            path = os.path.join(d, f"{_ident(model)}_{tag}{ext}")
+            with open(path, "w") as f:
+                f.write(text)
+            written.append(path)
+        # names and initial values, used by the host to describe the model
+        meta = os.path.join(cuda_dir, f"{_ident(model)}_{tag}.json")
+        import json
+        with open(meta, "w") as f:
+            json.dump({"name": model.name, "source": fname, "n_states": model.n_states,
+                       "n_algebraics": model.n_algebraics, "n_constants": model.n_constants,
+                       "parametersUsedAsAlgebraic": list(pa), "parametersUsedAsConstant": list(pc),
+                       "states_initial": model.states_initial,
+                       "constants": model.constants,
+                       "state_names": model.state_names, "algebraic_names": model.algebraic_names,
+                       "constant_names": model.constant_names, "uses_time": model.uses_voi,
+                       "operations_per_rhs": count_operations(model, pa, pc)},
+                      f, indent=1)
+        written.append(meta)
+    return written
+
+
+# ----------------------------------------------------------------------------------------------
+# operation counts (algorithmic work of one right-hand side evaluation)
+# ----------------------------------------------------------------------------------------------
+
+def count_operations(model: Model, params_alg: Sequence[int] = (), params_const: Sequence[int] = ()) -> Dict[str, int]:
+    """Arithmetic operations of one right-hand side evaluation: ``flops`` (+, -, *, / and the
+    multiplications of integer powers; a negation counts as one) and ``special`` (exp, log, pow
+    with a non-integer exponent)."""
+    lines = substitute_parameters(model, params_alg, params_const)
+    c = {"flops": 0, "div": 0, "special": 0}
+
+    def walk(e):
+        t = e[0]
+        if t in ("num", "var"):
+            return
+        if t in ("neg", "pos", "not"):
+            c["flops"] += 1 if t == "neg" else 0
+            walk(e[1])
+            return
+        if t == "bin":
+            if e[1] in "+-*/":
+                c["flops"] += 1
+                if e[1] == "/":
+                    c["div"] += 1
+            walk(e[2])
+            walk(e[3])
+            return
+        if t == "tern":
+            walk(e[1])
+            walk(e[2])
+            walk(e[3])
+            return
+        if t == "call":
+            if e[1] == "pow":
+                n = _int_exponent(e[2][1])
+                if n is not None:
+                    k = abs(n)
+                    c["flops"] += max(k - 1, 0) + (1 if n < 0 else 0)
+                    if n < 0:
+                        c["div"] += 1
+                    walk(e[2][0])
+                    return
+            if e[1] in ("exp", "log", "pow"):
+                c["special"] += 1
+            for a in e[2]:
+                walk(a)
+            return
+    for _, _, e in lines:
+        walk(e)
+    return c

@@ -1,0 +1,1259 @@
+// Host side of the fiber monodomain solver and its C ABI (include/fdm_b200.h).
+//
+// The solver restates the host logic of the reference's FastMonodomainSolverBase:
+//   time stepping rule        core/src/time_stepping_scheme/00_time_stepping_scheme.cpp:15-68
+//   RepeatedCall loop         core/src/time_stepping_scheme/repeated_call.tpp:43-80
+//   Strang step timing        fast_monodomain_solver_compute.tpp:64-129
+//   NMJ clamp selection       fast_monodomain_solver_compute.tpp:158-166 (vc) / fast_monodomain_solver_gpu.tpp:538-540
+//   stimulation machine init  fast_monodomain_solver_initialization.tpp:342-347
+// and drives the kernels of fdm_kernels.cuh over launch windows of split steps.
+//
+// Time values are computed here with the exact C expressions of the reference; this file is
+// compiled with -ffp-contract=off so that no multiply-add is fused.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/fdm_b200.h"
+#include "fdm_internal.h"
+
+using namespace fdm;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Tss {
+  double start = 0, end = 0, dt = 0, target = 0;
+  int n = 1;
+  void init(double s, double e, double d)
+  {
+    start = s;
+    end = e;
+    dt = d;
+    target = d;
+  }
+  void set_dt(double d)
+  {
+    target = d;
+    long double nn = std::ceil((long double)(end - start) / d - 1e-1);
+    n = nn < 1 ? 1 : (int)nn;
+    dt = (end - start) / n;
+  }
+  void set_span(double s, double e)
+  {
+    start = s;
+    end = e;
+    if (target > e - s)
+      dt = e - s;
+    set_dt(dt);
+  }
+};
+
+template<class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count)
+  {
+    if (count <= n && p)
+      return cudaSuccess;
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (count == 0)
+      count = 1;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e == cudaSuccess)
+      n = count;
+    return e;
+  }
+  void release()
+  {
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+} // namespace
+
+struct fdm_solver {
+  fdm_config cfg{};
+  const ModelDesc* model = nullptr;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  int real_bytes = 8;
+
+  // fibers
+  int n_fibers = 0;
+  int64_t n_nodes = 0;
+  std::vector<int64_t> off;
+  std::vector<int64_t> elem_off;
+  std::vector<double> prefactor;
+  int64_t max_fiber_len = 0;
+
+  // fused bins
+  int shape = -1;
+  int n_bins = 0;
+  std::vector<int> bin_start, bin_fibers;
+
+  // clamp selection
+  std::vector<int64_t> clamp_first;
+  std::vector<int> clamp_count;
+  std::vector<uint8_t> evaluated;
+
+  // device buffers
+  DevBuf<double> vm, coef, scratch, prefactor_d, elem_d, alg_out, trace;
+  DevBuf<unsigned char> states, params;
+  DevBuf<int64_t> off_d, elem_off_d;
+  DevBuf<int> clamp_fiber, bin_start_d, bin_fibers_d, alg_idx, trace_slot, nonfinite;
+  DevBuf<uint8_t> firing, evaluated_d, hbs;
+  DevBuf<int> mu;
+  DevBuf<double> freq, repeat, begin, jitter, last_check, cur_jitter;
+  DevBuf<int> jitter_idx;
+  DevBuf<uint32_t> flags;
+  DevBuf<SplitStep> steps_d;
+  SplitStep* steps_h = nullptr;   // pinned, 2 slots
+  cudaEvent_t slot_ev[2] = {nullptr, nullptr};
+  int slot = 0;
+  int firing_rows = 0, firing_cols = 0, n_jitter = 0;
+  bool stimulation_set = false;
+
+  // checkpoint
+  DevBuf<double> ck_vm, ck_last, ck_jit;
+  DevBuf<unsigned char> ck_states;
+  DevBuf<int> ck_jidx;
+  DevBuf<uint8_t> ck_hbs;
+  bool ck_valid = false;
+  Tss ck_strang, ck_heun, ck_diff;
+  bool ck_tss_init = false;
+  int64_t ck_split = 0;
+
+  // time stepping state (persists across advances, as the reference's scheme objects do)
+  Tss strang, heun, diff;
+  bool tss_init = false;
+  double coef_dt = -1.0;
+  bool coef_valid = false;
+  int64_t split_no = 0;
+
+  // outputs
+  int n_alg_out = 0;
+  int n_trace = 0;
+  int64_t trace_capacity = 0;
+
+  // timing
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  double main_ms = 0, adv_ms = 0;
+  int64_t main_launches = 0, launches = 0;
+  cudaEvent_t adv_start = nullptr, adv_stop = nullptr;
+};
+
+static int fail(fdm_solver* s, int code, const std::string& msg)
+{
+  if (s)
+    s->err = msg;
+  else
+    g_create_error = msg;
+  return code;
+}
+
+static int cuda_fail(fdm_solver* s, cudaError_t e, const char* what)
+{
+  return fail(s, FDM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// every entry point that touches the device first makes the solver's device current
+#define FDM_BIND(s)                                            \
+  do {                                                         \
+    cudaError_t eb_ = cudaSetDevice((s)->cfg.device);          \
+    if (eb_ != cudaSuccess)                                    \
+      return cuda_fail((s), eb_, "cudaSetDevice");             \
+  } while (0)
+
+#define FDM_CUDA(call)                          \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess)                      \
+      return cuda_fail(s, e_, #call);           \
+  } while (0)
+
+extern "C" void fdm_config_default(fdm_config* c)
+{
+  std::memset(c, 0, sizeof(*c));
+  c->model = FDM_MODEL_HODGKIN_HUXLEY_1952;
+  c->diffusion_scheme = FDM_IMPLICIT_EULER;
+  c->method = FDM_METHOD_SPLIT;
+  c->reaction_precision = FDM_FP64;
+  c->approximate_exponential_function = 0;
+  c->clamp_rule = FDM_CLAMP_VC_LANES;
+  c->vc_width = 4;
+  c->n_ranks = 1;
+  c->stimulus_mode = FDM_STIMULUS_CLAMP;
+  c->stimulus_parameter = 0;
+  c->stimulus_value = 0.0;
+  c->value_for_stimulated_point = 20.0;
+  c->dt_repeated_call = 1e-3;
+  c->dt_splitting = 1e-3;
+  c->dt_0d = 1e-4;
+  c->dt_1d = 1e-3;
+  c->steps_per_launch = 0;
+  c->threads_per_block = 0;
+  c->nodes_per_thread = 0;
+  c->check_nan = 1;
+  c->profile = 0;
+}
+
+extern "C" const char* fdm_last_error(const fdm_solver* s)
+{
+  return s ? s->err.c_str() : g_create_error.c_str();
+}
+
+extern "C" int fdm_model_parameter_defaults(int model, double* defaults)
+{
+  const ModelDesc* m = model_desc(model);
+  if (!m || !defaults)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_model_parameter_defaults: bad argument");
+  std::memcpy(defaults, m->parameter_defaults, sizeof(double) * m->n_parameters);
+  return FDM_OK;
+}
+
+extern "C" int fdm_model_info(int model, int* n_states, int* n_algebraics, int* n_parameters, double* states_initial)
+{
+  const ModelDesc* m = model_desc(model);
+  if (!m)
+    return fail(nullptr, FDM_ERR_ARG, "unknown model");
+  if (n_states)
+    *n_states = m->n_states;
+  if (n_algebraics)
+    *n_algebraics = m->n_algebraics;
+  if (n_parameters)
+    *n_parameters = m->n_parameters;
+  if (states_initial)
+    std::memcpy(states_initial, m->states_initial, sizeof(double) * m->n_states);
+  return FDM_OK;
+}
+
+extern "C" int fdm_fused_shapes(int* threads, int* nodes_per_thread, int capacity)
+{
+  FusedShape sh[64];
+  const int n = fused_shapes(sh, 64);
+  for (int i = 0; i < n && i < capacity; i++) {
+    if (threads)
+      threads[i] = sh[i].threads;
+    if (nodes_per_thread)
+      nodes_per_thread[i] = sh[i].nodes_per_thread;
+  }
+  return n;
+}
+
+extern "C" int fdm_create(const fdm_config* cfg, fdm_solver** out)
+{
+  if (!cfg || !out)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: null argument");
+  *out = nullptr;
+  const ModelDesc* m = model_desc(cfg->model);
+  if (!m)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: unknown model");
+  if (cfg->diffusion_scheme != FDM_IMPLICIT_EULER && cfg->diffusion_scheme != FDM_CRANK_NICOLSON)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: diffusion scheme must be ImplicitEuler or CrankNicolson");
+  if (cfg->method != FDM_METHOD_SPLIT && cfg->method != FDM_METHOD_FUSED)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: unknown method");
+  if (cfg->method == FDM_METHOD_FUSED && !m->fused_supported)
+    return fail(nullptr, FDM_ERR_UNSUPPORTED,
+                std::string("fdm_create: the fused kernel is not built for model ") + m->name +
+                    " (its states do not fit in registers); use FDM_METHOD_SPLIT");
+  if (cfg->reaction_precision != FDM_FP64 && cfg->reaction_precision != FDM_FP32_REACTION)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: unknown reaction precision");
+  if (cfg->clamp_rule != FDM_CLAMP_VC_LANES && cfg->clamp_rule != FDM_CLAMP_CENTER)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: unknown clamp rule");
+  if (cfg->vc_width < 1 || cfg->n_ranks < 1)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: vc_width and n_ranks must be >= 1");
+  if (cfg->stimulus_mode == FDM_STIMULUS_CURRENT &&
+      (cfg->stimulus_parameter < 0 || cfg->stimulus_parameter >= m->n_parameters))
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: stimulus_parameter out of range");
+  if (!(cfg->dt_repeated_call > 0) || !(cfg->dt_splitting > 0) || !(cfg->dt_0d > 0) || !(cfg->dt_1d > 0))
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: time step widths must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, FDM_ERR_NO_DEVICE, "fdm_create: no CUDA device");
+  if (cfg->device < 0 || cfg->device >= ndev)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: device ordinal out of range");
+  if (cudaSetDevice(cfg->device) != cudaSuccess)
+    return fail(nullptr, FDM_ERR_CUDA, "fdm_create: cudaSetDevice failed");
+  fdm_solver* s = new fdm_solver();
+  s->cfg = *cfg;
+  if (s->cfg.steps_per_launch <= 0)
+    s->cfg.steps_per_launch = 100;
+  s->model = m;
+  s->real_bytes = cfg->reaction_precision == FDM_FP64 ? 8 : 4;
+  cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = cudaMallocHost((void**)&s->steps_h, sizeof(SplitStep) * 2 * s->cfg.steps_per_launch);
+  if (e == cudaSuccess)
+    e = cudaEventCreateWithFlags(&s->slot_ev[0], cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    e = cudaEventCreateWithFlags(&s->slot_ev[1], cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&s->adv_start);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&s->adv_stop);
+  if (e == cudaSuccess)
+    e = s->steps_d.alloc(s->cfg.steps_per_launch);
+  if (e == cudaSuccess)
+    e = s->nonfinite.alloc(1);
+  if (e != cudaSuccess) {
+    fdm_destroy(s);
+    return fail(nullptr, FDM_ERR_CUDA, std::string("fdm_create: ") + cudaGetErrorString(e));
+  }
+  *out = s;
+  return FDM_OK;
+}
+
+extern "C" int fdm_destroy(fdm_solver* s)
+{
+  if (!s)
+    return FDM_OK;
+  cudaSetDevice(s->cfg.device);
+  if (s->stream)
+    cudaStreamSynchronize(s->stream);
+  for (auto* b : {&s->vm, &s->coef, &s->scratch, &s->prefactor_d, &s->elem_d, &s->alg_out, &s->trace, &s->freq,
+                  &s->repeat, &s->begin, &s->jitter, &s->last_check, &s->cur_jitter, &s->ck_vm, &s->ck_last,
+                  &s->ck_jit})
+    b->release();
+  s->states.release();
+  s->params.release();
+  s->ck_states.release();
+  s->off_d.release();
+  s->elem_off_d.release();
+  for (auto* b : {&s->clamp_fiber, &s->bin_start_d, &s->bin_fibers_d, &s->alg_idx, &s->trace_slot, &s->nonfinite,
+                  &s->mu, &s->jitter_idx, &s->ck_jidx})
+    b->release();
+  s->firing.release();
+  s->evaluated_d.release();
+  s->hbs.release();
+  s->ck_hbs.release();
+  s->flags.release();
+  s->steps_d.release();
+  if (s->steps_h)
+    cudaFreeHost(s->steps_h);
+  for (auto ev : s->slot_ev)
+    if (ev)
+      cudaEventDestroy(ev);
+  for (auto ev : s->ev_pool)
+    cudaEventDestroy(ev);
+  if (s->adv_start)
+    cudaEventDestroy(s->adv_start);
+  if (s->adv_stop)
+    cudaEventDestroy(s->adv_stop);
+  if (s->stream)
+    cudaStreamDestroy(s->stream);
+  delete s;
+  return FDM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// fibers, bins
+// ---------------------------------------------------------------------------------------------
+
+// First-fit-decreasing packing of whole fibers into bins of `cap` nodes (at most
+// FUSED_MAX_FIBERS_PER_BIN fibers per bin); bins are then ordered longest first.
+static void pack_bins(const std::vector<int64_t>& off, int64_t cap, std::vector<int>& bin_start,
+                      std::vector<int>& bin_fibers)
+{
+  const int nf = (int)off.size() - 1;
+  std::vector<int> order(nf);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
+  std::vector<int64_t> fill;
+  std::vector<std::vector<int>> bins;
+  for (int f : order) {
+    const int64_t len = off[f + 1] - off[f];
+    int chosen = -1;
+    for (size_t b = 0; b < bins.size(); b++)
+      if (fill[b] + len <= cap && (int)bins[b].size() < FUSED_MAX_FIBERS_PER_BIN) {
+        chosen = (int)b;
+        break;
+      }
+    if (chosen < 0) {
+      bins.emplace_back();
+      fill.push_back(0);
+      chosen = (int)bins.size() - 1;
+    }
+    bins[chosen].push_back(f);
+    fill[chosen] += len;
+  }
+  bin_start.assign(1, 0);
+  bin_fibers.clear();
+  for (auto& b : bins) {
+    for (int f : b)
+      bin_fibers.push_back(f);
+    bin_start.push_back((int)bin_fibers.size());
+  }
+}
+
+static int choose_shape(fdm_solver* s)
+{
+  FusedShape sh[64];
+  const int n = fused_shapes(sh, 64);
+  int best = -1;
+  int64_t best_cap = 0;
+  for (int i = 0; i < n; i++) {
+    const int64_t cap = (int64_t)sh[i].threads * sh[i].nodes_per_thread;
+    if (s->cfg.threads_per_block > 0 || s->cfg.nodes_per_thread > 0) {
+      if (sh[i].threads == s->cfg.threads_per_block && sh[i].nodes_per_thread == s->cfg.nodes_per_thread)
+        return cap >= s->max_fiber_len ? i : -2;
+      continue;
+    }
+    // default: the smallest capacity that holds the longest fiber, preferring 256+ threads
+    if (cap >= s->max_fiber_len && sh[i].threads >= 256 && (best < 0 || cap < best_cap)) {
+      best = i;
+      best_cap = cap;
+    }
+  }
+  if (s->cfg.threads_per_block > 0 || s->cfg.nodes_per_thread > 0)
+    return -2;
+  if (best < 0)
+    for (int i = 0; i < n; i++) {
+      const int64_t cap = (int64_t)sh[i].threads * sh[i].nodes_per_thread;
+      if (cap >= s->max_fiber_len && (best < 0 || cap < best_cap)) {
+        best = i;
+        best_cap = cap;
+      }
+    }
+  return best;
+}
+
+static int upload_clamp(fdm_solver* s);
+
+extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_offsets,
+                              const double* element_lengths, const double* prefactor)
+{
+  if (!s || n_fibers < 0 || (n_fibers > 0 && (!fiber_offsets || !element_lengths || !prefactor)))
+    return fail(s, FDM_ERR_ARG, "fdm_set_fibers: bad argument");
+  FDM_BIND(s);
+  if (n_fibers > 0 && fiber_offsets[0] != 0)
+    return fail(s, FDM_ERR_ARG, "fdm_set_fibers: fiber_offsets[0] must be 0");
+  int64_t maxlen = 0;
+  for (int f = 0; f < n_fibers; f++) {
+    const int64_t len = fiber_offsets[f + 1] - fiber_offsets[f];
+    if (len < 2)
+      return fail(s, FDM_ERR_ARG, "fdm_set_fibers: every fiber needs at least 2 nodes (1 element)");
+    maxlen = std::max(maxlen, len);
+    if (!(prefactor[f] > 0) || !std::isfinite(prefactor[f]))
+      return fail(s, FDM_ERR_ARG, "fdm_set_fibers: prefactor must be positive and finite");
+  }
+  s->n_fibers = n_fibers;
+  s->off.assign(fiber_offsets, fiber_offsets + n_fibers + 1);
+  if (n_fibers == 0)
+    s->off.assign(1, 0);
+  s->n_nodes = s->off.back();
+  s->max_fiber_len = maxlen;
+  s->elem_off.resize(n_fibers + 1);
+  for (int f = 0; f <= n_fibers; f++)
+    s->elem_off[f] = s->off[f] - f;
+  const int64_t n_elem = s->n_nodes - n_fibers;
+  for (int64_t e = 0; e < n_elem; e++)
+    if (!(element_lengths[e] > 0) || !std::isfinite(element_lengths[e]))
+      return fail(s, FDM_ERR_ARG, "fdm_set_fibers: element lengths must be positive and finite");
+  s->prefactor.assign(prefactor, prefactor + n_fibers);
+
+  const int NS = s->model->n_states, NP = s->model->n_parameters;
+  const int64_t N = std::max<int64_t>(s->n_nodes, 1);
+  FDM_CUDA(s->vm.alloc(N));
+  FDM_CUDA(s->states.alloc((size_t)N * std::max(NS - 1, 1) * s->real_bytes));
+  FDM_CUDA(s->params.alloc((size_t)N * std::max(NP, 1) * s->real_bytes));
+  FDM_CUDA(s->coef.alloc((size_t)N * 6));
+  if (s->cfg.method == FDM_METHOD_SPLIT)
+    FDM_CUDA(s->scratch.alloc(N));
+  FDM_CUDA(s->clamp_fiber.alloc(N));
+  FDM_CUDA(s->off_d.alloc(n_fibers + 1));
+  FDM_CUDA(s->elem_off_d.alloc(n_fibers + 1));
+  FDM_CUDA(s->elem_d.alloc(std::max<int64_t>(n_elem, 1)));
+  FDM_CUDA(s->prefactor_d.alloc(std::max(n_fibers, 1)));
+  FDM_CUDA(cudaMemcpyAsync(s->off_d.p, s->off.data(), sizeof(int64_t) * (n_fibers + 1), cudaMemcpyHostToDevice,
+                           s->stream));
+  FDM_CUDA(cudaMemcpyAsync(s->elem_off_d.p, s->elem_off.data(), sizeof(int64_t) * (n_fibers + 1),
+                           cudaMemcpyHostToDevice, s->stream));
+  if (n_elem > 0)
+    FDM_CUDA(cudaMemcpyAsync(s->elem_d.p, element_lengths, sizeof(double) * n_elem, cudaMemcpyHostToDevice,
+                             s->stream));
+  if (n_fibers > 0)
+    FDM_CUDA(cudaMemcpyAsync(s->prefactor_d.p, prefactor, sizeof(double) * n_fibers, cudaMemcpyHostToDevice,
+                             s->stream));
+  s->coef_valid = false;
+
+  // initial states and default parameters (initializeStates on every buffer)
+  std::vector<double> st((size_t)NS * s->n_nodes);
+  for (int k = 0; k < NS; k++)
+    std::fill(st.begin() + (size_t)k * s->n_nodes, st.begin() + (size_t)(k + 1) * s->n_nodes,
+              s->model->states_initial[k]);
+  int rc = fdm_set_states(s, st.data());
+  if (rc)
+    return rc;
+  // default parameters: the model file's raw value of each constant parameter, 0 for algebraic ones
+  std::vector<double> pz((size_t)std::max(NP, 1) * s->n_nodes, 0.0);
+  for (int q = 0; q < NP; q++)
+    std::fill(pz.begin() + (size_t)q * s->n_nodes, pz.begin() + (size_t)(q + 1) * s->n_nodes,
+              s->model->parameter_defaults[q]);
+  if (NP > 0) {
+    rc = fdm_set_parameters(s, pz.data());
+    if (rc)
+      return rc;
+  }
+
+  // fused bins
+  if (s->cfg.method == FDM_METHOD_FUSED && n_fibers > 0) {
+    s->shape = choose_shape(s);
+    if (s->shape < 0)
+      return fail(s, FDM_ERR_UNSUPPORTED, "fdm_set_fibers: no fused kernel shape holds the longest fiber (" +
+                                              std::to_string(maxlen) + " nodes) with the requested threads/nodes");
+    FusedShape sh[64];
+    fused_shapes(sh, 64);
+    pack_bins(s->off, (int64_t)sh[s->shape].threads * sh[s->shape].nodes_per_thread, s->bin_start, s->bin_fibers);
+    s->n_bins = (int)s->bin_start.size() - 1;
+    FDM_CUDA(s->bin_start_d.alloc(s->bin_start.size()));
+    FDM_CUDA(s->bin_fibers_d.alloc(std::max<size_t>(s->bin_fibers.size(), 1)));
+    FDM_CUDA(cudaMemcpyAsync(s->bin_start_d.p, s->bin_start.data(), sizeof(int) * s->bin_start.size(),
+                             cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->bin_fibers_d.p, s->bin_fibers.data(), sizeof(int) * s->bin_fibers.size(),
+                             cudaMemcpyHostToDevice, s->stream));
+  }
+  s->stimulation_set = false;
+  s->split_no = 0;
+  s->tss_init = false;
+  s->ck_valid = false;
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_set_prefactor(fdm_solver* s, const double* prefactor)
+{
+  if (!s || !prefactor)
+    return fail(s, FDM_ERR_ARG, "fdm_set_prefactor: bad argument");
+  FDM_BIND(s);
+  for (int f = 0; f < s->n_fibers; f++)
+    if (!(prefactor[f] > 0) || !std::isfinite(prefactor[f]))
+      return fail(s, FDM_ERR_ARG, "fdm_set_prefactor: prefactor must be positive and finite");
+  s->prefactor.assign(prefactor, prefactor + s->n_fibers);
+  if (s->n_fibers > 0)
+    FDM_CUDA(cudaMemcpyAsync(s->prefactor_d.p, prefactor, sizeof(double) * s->n_fibers, cudaMemcpyHostToDevice,
+                             s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  s->coef_valid = false;
+  return FDM_OK;
+}
+
+// SoA host doubles -> device (Vm in FP64, other states in the reaction precision)
+extern "C" int fdm_set_states(fdm_solver* s, const double* states)
+{
+  if (!s || !states)
+    return fail(s, FDM_ERR_ARG, "fdm_set_states: bad argument");
+  FDM_BIND(s);
+  const int NS = s->model->n_states;
+  const int64_t N = s->n_nodes;
+  if (N == 0)
+    return FDM_OK;
+  FDM_CUDA(cudaMemcpyAsync(s->vm.p, states, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream));
+  if (NS > 1) {
+    if (s->real_bytes == 8) {
+      FDM_CUDA(cudaMemcpyAsync(s->states.p, states + N, sizeof(double) * N * (NS - 1), cudaMemcpyHostToDevice,
+                               s->stream));
+    } else {
+      std::vector<float> tmp((size_t)N * (NS - 1));
+      for (size_t i = 0; i < tmp.size(); i++)
+        tmp[i] = (float)states[N + i];
+      FDM_CUDA(cudaMemcpyAsync(s->states.p, tmp.data(), sizeof(float) * tmp.size(), cudaMemcpyHostToDevice,
+                               s->stream));
+      FDM_CUDA(cudaStreamSynchronize(s->stream));
+    }
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_states(fdm_solver* s, double* states)
+{
+  if (!s || !states)
+    return fail(s, FDM_ERR_ARG, "fdm_get_states: bad argument");
+  FDM_BIND(s);
+  const int NS = s->model->n_states;
+  const int64_t N = s->n_nodes;
+  if (N == 0)
+    return FDM_OK;
+  FDM_CUDA(cudaMemcpyAsync(states, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream));
+  if (NS > 1) {
+    if (s->real_bytes == 8) {
+      FDM_CUDA(cudaMemcpyAsync(states + N, s->states.p, sizeof(double) * N * (NS - 1), cudaMemcpyDeviceToHost,
+                               s->stream));
+      FDM_CUDA(cudaStreamSynchronize(s->stream));
+    } else {
+      std::vector<float> tmp((size_t)N * (NS - 1));
+      FDM_CUDA(cudaMemcpyAsync(tmp.data(), s->states.p, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost,
+                               s->stream));
+      FDM_CUDA(cudaStreamSynchronize(s->stream));
+      for (size_t i = 0; i < tmp.size(); i++)
+        states[N + i] = (double)tmp[i];
+    }
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_vm(fdm_solver* s, double* vm)
+{
+  if (!s || !vm)
+    return fail(s, FDM_ERR_ARG, "fdm_get_vm: bad argument");
+  FDM_BIND(s);
+  if (s->n_nodes == 0)
+    return FDM_OK;
+  FDM_CUDA(cudaMemcpyAsync(vm, s->vm.p, sizeof(double) * s->n_nodes, cudaMemcpyDeviceToHost, s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_set_parameters(fdm_solver* s, const double* parameters)
+{
+  if (!s || !parameters)
+    return fail(s, FDM_ERR_ARG, "fdm_set_parameters: bad argument");
+  FDM_BIND(s);
+  const int NP = s->model->n_parameters;
+  const size_t n = (size_t)NP * s->n_nodes;
+  if (n == 0)
+    return FDM_OK;
+  if (s->real_bytes == 8) {
+    FDM_CUDA(cudaMemcpyAsync(s->params.p, parameters, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+  } else {
+    std::vector<float> tmp(n);
+    for (size_t i = 0; i < n; i++)
+      tmp[i] = (float)parameters[i];
+    FDM_CUDA(cudaMemcpyAsync(s->params.p, tmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_parameters(fdm_solver* s, double* parameters)
+{
+  if (!s || !parameters)
+    return fail(s, FDM_ERR_ARG, "fdm_get_parameters: bad argument");
+  FDM_BIND(s);
+  const size_t n = (size_t)s->model->n_parameters * s->n_nodes;
+  if (n == 0)
+    return FDM_OK;
+  if (s->real_bytes == 8) {
+    FDM_CUDA(cudaMemcpyAsync(parameters, s->params.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+  } else {
+    std::vector<float> tmp(n);
+    FDM_CUDA(cudaMemcpyAsync(tmp.data(), s->params.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+    for (size_t i = 0; i < n; i++)
+      parameters[i] = tmp[i];
+  }
+  return FDM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// stimulation
+// ---------------------------------------------------------------------------------------------
+
+// Clamp node selection.  Fibers are laid out as on n_ranks ranks (fiberNo % n_ranks), each rank with
+// its fibers concatenated (valuesOffset) and cut into buffers of W lanes; a buffer b is "in the centre"
+// of the fiber its first lane is attributed to by int(b * W / valuesLength[0]) when the junction index
+// falls inside it, and then lanes 0..min(3,W)-1 of b are clamped (compute.tpp:158-166, 03_generator_vc.cpp:1031-1038).
+static void select_clamp_vc(fdm_solver* s, const std::vector<int>& center)
+{
+  const int W = s->cfg.vc_width, R = s->cfg.n_ranks;
+  s->clamp_first.assign(s->n_fibers, -1);
+  s->clamp_count.assign(s->n_fibers, 0);
+  s->evaluated.assign(s->n_fibers, 0);
+  for (int r = 0; r < R; r++) {
+    std::vector<int> fib;
+    std::vector<int64_t> vo;
+    int64_t total = 0;
+    for (int f = r; f < s->n_fibers; f += R) {
+      fib.push_back(f);
+      vo.push_back(total);
+      total += s->off[f + 1] - s->off[f];
+    }
+    if (fib.empty())
+      continue;
+    vo.push_back(total);
+    const int64_t nbuf = (total + W - 1) / W;
+    const double factor = (double)W / (double)(vo[1] - vo[0]);
+    const int lanes = std::min(3, W);
+    for (int64_t b = 0; b < nbuf; b++) {
+      int local = (int)(b * factor);
+      if (local >= (int)fib.size())
+        local = (int)fib.size() - 1;
+      const int f = fib[local];
+      const int64_t index_in_fiber = b * W - vo[local];
+      if ((unsigned long)((long)center[f] - (long)index_in_fiber) < (unsigned long)W) {
+        s->evaluated[f] = 1;
+        int64_t first = -1;
+        int cnt = 0;
+        for (int lane = 0; lane < lanes; lane++) {
+          const int64_t i = b * W + lane;
+          if (i >= total)
+            break;
+          const size_t l2 = (size_t)(std::upper_bound(vo.begin(), vo.end(), i) - vo.begin()) - 1;
+          const int64_t g = s->off[fib[l2]] + (i - vo[l2]);
+          if (first < 0)
+            first = g;
+          cnt++;
+        }
+        s->clamp_first[f] = first;
+        s->clamp_count[f] = cnt;
+      }
+    }
+  }
+}
+
+// junction node and its two neighbours inside the fiber (fast_monodomain_solver_gpu.tpp:538-540)
+static void select_clamp_center(fdm_solver* s, const std::vector<int>& center)
+{
+  s->clamp_first.assign(s->n_fibers, -1);
+  s->clamp_count.assign(s->n_fibers, 0);
+  s->evaluated.assign(s->n_fibers, 1);
+  for (int f = 0; f < s->n_fibers; f++) {
+    const int64_t n = s->off[f + 1] - s->off[f];
+    const int64_t lo = std::max<int64_t>(center[f] - 1, 0), hi = std::min<int64_t>(center[f] + 1, n - 1);
+    if (hi < lo)
+      continue;
+    s->clamp_first[f] = s->off[f] + lo;
+    s->clamp_count[f] = (int)(hi - lo + 1);
+  }
+}
+
+static int upload_clamp(fdm_solver* s)
+{
+  std::vector<int> cf((size_t)std::max<int64_t>(s->n_nodes, 1), -1);
+  for (int f = 0; f < s->n_fibers; f++)
+    for (int k = 0; k < s->clamp_count[f]; k++)
+      cf[s->clamp_first[f] + k] = f;
+  FDM_CUDA(cudaMemcpyAsync(s->clamp_fiber.p, cf.data(), sizeof(int) * s->n_nodes, cudaMemcpyHostToDevice,
+                           s->stream));
+  FDM_CUDA(cudaMemcpyAsync(s->evaluated_d.p, s->evaluated.data(), s->n_fibers, cudaMemcpyHostToDevice, s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, int rows, int cols,
+                                   const int* motor_unit_no, const int* stimulation_point_index,
+                                   const double* call_frequency, const double* repeat_after_first_call,
+                                   const double* call_enable_begin, const double* jitter, int n_jitter)
+{
+  if (!s || rows < 1 || cols < 1 || !firing_events || n_jitter < 0 || (n_jitter > 0 && !jitter))
+    return fail(s, FDM_ERR_ARG, "fdm_set_stimulation: bad argument (firing events need at least one row and column)");
+  FDM_BIND(s);
+  const int nf = s->n_fibers;
+  if (nf > 0 && (!motor_unit_no || !stimulation_point_index || !call_frequency || !repeat_after_first_call ||
+                 !call_enable_begin))
+    return fail(s, FDM_ERR_ARG, "fdm_set_stimulation: null per-fiber array");
+  std::vector<int> center(nf);
+  for (int f = 0; f < nf; f++) {
+    if (motor_unit_no[f] < 0)
+      return fail(s, FDM_ERR_ARG, "fdm_set_stimulation: motor unit numbers must be >= 0");
+    center[f] = stimulation_point_index[f];
+    if (call_frequency[f] != 0 && repeat_after_first_call[f] == 0)
+      return fail(s, FDM_ERR_ARG,
+                  "fdm_set_stimulation: setSpecificStatesCallFrequency is set but setSpecificStatesRepeatAfterFirstCall "
+                  "is not (03_cellml_adapter.tpp:177-181)");
+  }
+  s->firing_rows = rows;
+  s->firing_cols = cols;
+  s->n_jitter = n_jitter;
+  FDM_CUDA(s->firing.alloc((size_t)rows * cols));
+  FDM_CUDA(s->mu.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->freq.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->repeat.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->begin.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->jitter.alloc(std::max<size_t>((size_t)nf * n_jitter, 1)));
+  FDM_CUDA(s->last_check.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->cur_jitter.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->jitter_idx.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->hbs.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->evaluated_d.alloc(std::max(nf, 1)));
+  FDM_CUDA(cudaMemcpyAsync(s->firing.p, firing_events, (size_t)rows * cols, cudaMemcpyHostToDevice, s->stream));
+  if (nf > 0) {
+    FDM_CUDA(cudaMemcpyAsync(s->mu.p, motor_unit_no, sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->freq.p, call_frequency, sizeof(double) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->repeat.p, repeat_after_first_call, sizeof(double) * nf, cudaMemcpyHostToDevice,
+                             s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->begin.p, call_enable_begin, sizeof(double) * nf, cudaMemcpyHostToDevice,
+                             s->stream));
+    if (n_jitter > 0)
+      FDM_CUDA(cudaMemcpyAsync(s->jitter.p, jitter, sizeof(double) * nf * n_jitter, cudaMemcpyHostToDevice,
+                               s->stream));
+    // initial machine state (initialization.tpp:342-344)
+    std::vector<double> last(nf), cj(nf, 0.0);
+    std::vector<int> ji(nf, 0);
+    std::vector<uint8_t> h0(nf, 0);
+    for (int f = 0; f < nf; f++)
+      last[f] = call_enable_begin[f] - 1e-13 - 1. / (call_frequency[f] + cj[f]);
+    FDM_CUDA(cudaMemcpyAsync(s->last_check.p, last.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->cur_jitter.p, cj.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, ji.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->hbs.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  if (s->cfg.clamp_rule == FDM_CLAMP_VC_LANES)
+    select_clamp_vc(s, center);
+  else
+    select_clamp_center(s, center);
+  int rc = upload_clamp(s);
+  if (rc)
+    return rc;
+  s->stimulation_set = true;
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_clamp_nodes(fdm_solver* s, int64_t* first_node, int* count, uint8_t* evaluated)
+{
+  if (!s || !s->stimulation_set)
+    return fail(s, FDM_ERR_ARG, "fdm_get_clamp_nodes: call fdm_set_stimulation first");
+  for (int f = 0; f < s->n_fibers; f++) {
+    if (first_node)
+      first_node[f] = s->clamp_first[f];
+    if (count)
+      count[f] = s->clamp_count[f];
+    if (evaluated)
+      evaluated[f] = s->evaluated[f];
+  }
+  return FDM_OK;
+}
+
+extern "C" int fdm_set_algebraics_for_transfer(fdm_solver* s, int n, const int* idx)
+{
+  if (!s || n < 0 || (n > 0 && !idx))
+    return fail(s, FDM_ERR_ARG, "fdm_set_algebraics_for_transfer: bad argument");
+  FDM_BIND(s);
+  for (int k = 0; k < n; k++)
+    if (idx[k] < 0 || idx[k] >= s->model->n_algebraics)
+      return fail(s, FDM_ERR_ARG, "fdm_set_algebraics_for_transfer: algebraic index out of range");
+  s->n_alg_out = n;
+  FDM_CUDA(s->alg_idx.alloc(std::max(n, 1)));
+  FDM_CUDA(s->alg_out.alloc(std::max<size_t>((size_t)n * s->n_nodes, 1)));
+  if (n > 0) {
+    FDM_CUDA(cudaMemcpyAsync(s->alg_idx.p, idx, sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemsetAsync(s->alg_out.p, 0, sizeof(double) * n * s->n_nodes, s->stream));
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_algebraics(fdm_solver* s, double* out)
+{
+  if (!s || !out)
+    return fail(s, FDM_ERR_ARG, "fdm_get_algebraics: bad argument");
+  FDM_BIND(s);
+  if (s->n_alg_out == 0 || s->n_nodes == 0)
+    return FDM_OK;
+  FDM_CUDA(cudaMemcpyAsync(out, s->alg_out.p, sizeof(double) * s->n_alg_out * s->n_nodes, cudaMemcpyDeviceToHost,
+                           s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_set_trace(fdm_solver* s, int n, const int64_t* nodes, int64_t capacity)
+{
+  if (!s || n < 0 || (n > 0 && !nodes) || capacity < 0)
+    return fail(s, FDM_ERR_ARG, "fdm_set_trace: bad argument");
+  FDM_BIND(s);
+  std::vector<int> slot((size_t)std::max<int64_t>(s->n_nodes, 1), -1);
+  for (int k = 0; k < n; k++) {
+    if (nodes[k] < 0 || nodes[k] >= s->n_nodes)
+      return fail(s, FDM_ERR_ARG, "fdm_set_trace: node index out of range");
+    if (slot[nodes[k]] >= 0)
+      return fail(s, FDM_ERR_ARG, "fdm_set_trace: duplicate node");
+    slot[nodes[k]] = k;
+  }
+  s->n_trace = n;
+  s->trace_capacity = n > 0 ? capacity : 0;
+  if (n > 0) {
+    FDM_CUDA(s->trace_slot.alloc(s->n_nodes));
+    FDM_CUDA(s->trace.alloc(std::max<size_t>((size_t)n * capacity, 1)));
+    FDM_CUDA(cudaMemcpyAsync(s->trace_slot.p, slot.data(), sizeof(int) * s->n_nodes, cudaMemcpyHostToDevice,
+                             s->stream));
+    FDM_CUDA(cudaMemsetAsync(s->trace.p, 0, sizeof(double) * std::max<size_t>((size_t)n * capacity, 1), s->stream));
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_trace(fdm_solver* s, double* out, int64_t* n_steps)
+{
+  if (!s)
+    return fail(s, FDM_ERR_ARG, "fdm_get_trace: bad argument");
+  FDM_BIND(s);
+  const int64_t rec = std::min(s->split_no, s->trace_capacity);
+  if (n_steps)
+    *n_steps = rec;
+  if (out && rec > 0 && s->n_trace > 0) {
+    FDM_CUDA(cudaMemcpyAsync(out, s->trace.p, sizeof(double) * rec * s->n_trace, cudaMemcpyDeviceToHost, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return FDM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// advance
+// ---------------------------------------------------------------------------------------------
+
+static cudaEvent_t next_event(fdm_solver* s)
+{
+  if (s->ev_used == s->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess)
+      return nullptr;
+    s->ev_pool.push_back(e);
+  }
+  return s->ev_pool[s->ev_used++];
+}
+
+static int ensure_coefficients(fdm_solver* s, double dt1)
+{
+  // The reference recomputes dt1D = ((t+dtSplit)-t)/n1D at every call, which varies in the last bits;
+  // the factorization is reused while dt1D stays within a relative 1e-12 of the factorized value.
+  if (s->coef_valid && std::fabs(dt1 - s->coef_dt) <= 1e-12 * std::fabs(s->coef_dt))
+    return FDM_OK;
+  FDM_CUDA(launch_coefficients(s->n_fibers, s->off_d.p, s->elem_off_d.p, s->elem_d.p, s->prefactor_d.p, dt1,
+                               s->cfg.diffusion_scheme == FDM_IMPLICIT_EULER, s->coef.p, s->n_nodes, s->stream));
+  s->launches++;
+  s->coef_dt = dt1;
+  s->coef_valid = true;
+  return FDM_OK;
+}
+
+static int run_window(fdm_solver* s, int n_steps, double dt1, bool store_alg)
+{
+  if (n_steps == 0 || s->n_fibers == 0)
+    return FDM_OK;
+  int rc = ensure_coefficients(s, dt1);
+  if (rc)
+    return rc;
+  // upload the window's split steps from a pinned slot (wait until the slot's previous copy finished)
+  const int slot = s->slot;
+  s->slot ^= 1;
+  FDM_CUDA(cudaEventSynchronize(s->slot_ev[slot]));
+  SplitStep* hs = s->steps_h + (size_t)slot * s->cfg.steps_per_launch;
+  // (filled by the caller into s->steps_h slot area before; copy from the staging vector)
+  (void)hs;
+  int nsub = 1;
+  for (int j = 0; j < n_steps; j++)
+    nsub = std::max(nsub, hs[j].n0);
+  const int bits = n_steps * 2 * nsub;
+  const int words = (bits + 31) / 32;
+  FDM_CUDA(s->flags.alloc((size_t)words * s->n_fibers));
+  FDM_CUDA(cudaMemcpyAsync(s->steps_d.p, hs, sizeof(SplitStep) * n_steps, cudaMemcpyHostToDevice, s->stream));
+  FDM_CUDA(cudaEventRecord(s->slot_ev[slot], s->stream));
+
+  StimArgs sa{};
+  sa.firing_events = s->firing.p;
+  sa.rows = s->firing_rows;
+  sa.cols = s->firing_cols;
+  sa.motor_unit_no = s->mu.p;
+  sa.call_frequency = s->freq.p;
+  sa.repeat_after_first_call = s->repeat.p;
+  sa.call_enable_begin = s->begin.p;
+  sa.jitter = s->jitter.p;
+  sa.n_jitter = s->n_jitter;
+  sa.evaluated = s->evaluated_d.p;
+  sa.last_check_time = s->last_check.p;
+  sa.current_jitter = s->cur_jitter.p;
+  sa.jitter_index = s->jitter_idx.p;
+  sa.has_been_stimulated = s->hbs.p;
+  sa.flags = s->flags.p;
+  sa.words_per_fiber = words;
+  sa.nsub_stride = nsub;
+  sa.n_fibers = s->n_fibers;
+  FDM_CUDA(launch_schedule(sa, s->steps_d.p, n_steps, s->stream));
+  s->launches++;
+
+  const RealKind rk = s->real_bytes == 8 ? REAL_F64 : REAL_F32;
+  const MathKind mk = s->cfg.approximate_exponential_function ? MATH_APPROX : MATH_EXACT;
+  const bool prof = s->cfg.profile != 0;
+
+  if (s->cfg.method == FDM_METHOD_FUSED) {
+    FusedArgs fa{};
+    fa.n_bins = s->n_bins;
+    fa.bin_fiber_start = s->bin_start_d.p;
+    fa.bin_fibers = s->bin_fibers_d.p;
+    fa.fiber_offsets = s->off_d.p;
+    fa.stride = s->n_nodes;
+    fa.vm = s->vm.p;
+    fa.states = s->states.p;
+    fa.params = s->params.p;
+    fa.coef = s->coef.p;
+    fa.clamp_fiber = s->clamp_fiber.p;
+    fa.flags = s->flags.p;
+    fa.words_per_fiber = words;
+    fa.nsub_stride = nsub;
+    fa.vstim = s->cfg.value_for_stimulated_point;
+    fa.stimulus_mode = s->cfg.stimulus_mode;
+    fa.stimulus_parameter = s->cfg.stimulus_parameter;
+    fa.stimulus_value = s->cfg.stimulus_value;
+    fa.steps = s->steps_d.p;
+    fa.n_steps = n_steps;
+    fa.store_alg = store_alg && s->n_alg_out > 0;
+    fa.n_alg_out = s->n_alg_out;
+    fa.alg_indices = s->alg_idx.p;
+    fa.alg_out = s->alg_out.p;
+    fa.n_nodes = s->n_nodes;
+    fa.trace_slot = s->n_trace > 0 ? s->trace_slot.p : nullptr;
+    fa.trace = s->trace.p;
+    fa.n_trace = s->n_trace;
+    fa.trace_capacity = s->trace_capacity;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+      e0 = next_event(s);
+      e1 = next_event(s);
+      FDM_CUDA(cudaEventRecord(e0, s->stream));
+    }
+    FDM_CUDA(launch_fused(s->cfg.model, rk, mk, s->shape, fa, s->stream));
+    s->launches++;
+    if (prof)
+      FDM_CUDA(cudaEventRecord(e1, s->stream));
+    return FDM_OK;
+  }
+
+  ReactionArgs ra{};
+  ra.n_nodes = s->n_nodes;
+  ra.stride = s->n_nodes;
+  ra.vm = s->vm.p;
+  ra.states = s->states.p;
+  ra.params = s->params.p;
+  ra.clamp_fiber = s->clamp_fiber.p;
+  ra.flags = s->flags.p;
+  ra.words_per_fiber = words;
+  ra.nsub_stride = nsub;
+  ra.vstim = s->cfg.value_for_stimulated_point;
+  ra.stimulus_mode = s->cfg.stimulus_mode;
+  ra.stimulus_parameter = s->cfg.stimulus_parameter;
+  ra.stimulus_value = s->cfg.stimulus_value;
+  ra.steps = s->steps_d.p;
+  ra.n_alg_out = s->n_alg_out;
+  ra.alg_indices = s->alg_idx.p;
+  ra.alg_out = s->alg_out.p;
+  ra.trace_slot = s->n_trace > 0 ? s->trace_slot.p : nullptr;
+  ra.trace = s->trace.p;
+  ra.n_trace = s->n_trace;
+  ra.trace_capacity = s->trace_capacity;
+  for (int j = 0; j < n_steps; j++) {
+    ra.step = j;
+    for (int half = 0; half < 2; half++) {
+      ra.half = half;
+      ra.store_alg = (store_alg && s->n_alg_out > 0 && half == 1 && j == n_steps - 1) ? 1 : 0;
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (prof) {
+        e0 = next_event(s);
+        e1 = next_event(s);
+        FDM_CUDA(cudaEventRecord(e0, s->stream));
+      }
+      FDM_CUDA(launch_reaction(s->cfg.model, rk, mk, ra, s->stream));
+      s->launches++;
+      if (prof)
+        FDM_CUDA(cudaEventRecord(e1, s->stream));
+      if (half == 0) {
+        FDM_CUDA(launch_diffusion_warp(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
+                                       s->stream));
+        s->launches++;
+      }
+    }
+  }
+  return FDM_OK;
+}
+
+extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
+{
+  if (!s)
+    return fail(s, FDM_ERR_ARG, "fdm_advance: null solver");
+  FDM_BIND(s);
+  if (!(t_end >= t_start))
+    return fail(s, FDM_ERR_ARG, "fdm_advance: t_end must be >= t_start");
+  if (s->n_fibers > 0 && !s->stimulation_set)
+    return fail(s, FDM_ERR_ARG, "fdm_advance: call fdm_set_stimulation first");
+  s->ev_used = 0;
+  FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
+  const int64_t launches0 = s->launches;
+
+  // RepeatedCall (repeated_call.tpp:43-75)
+  Tss rc;
+  rc.init(t_start, t_end, s->cfg.dt_repeated_call);
+  rc.set_dt(s->cfg.dt_repeated_call);
+  const double span = rc.end - rc.start;
+  if (!s->tss_init) {
+    s->strang.init(t_start, t_start + s->cfg.dt_splitting, s->cfg.dt_splitting);
+    s->heun.init(t_start, t_start + s->cfg.dt_0d, s->cfg.dt_0d);
+    s->diff.init(t_start, t_start + s->cfg.dt_1d, s->cfg.dt_1d);
+    s->tss_init = true;
+  }
+  const int K = s->cfg.steps_per_launch;
+  int filled = 0;
+  double window_dt1 = 0;
+  double t = rc.start;
+  for (int k = 0; k < rc.n;) {
+    s->strang.set_span(t, t + rc.dt);
+    const double start = s->strang.start;
+    const double dts = s->strang.dt;
+    const int ns = s->strang.n;
+    s->heun.set_span(start, start + 0.5 * dts);
+    s->diff.set_span(start, start + dts);
+    const double dt1 = s->diff.dt;
+    for (int j = 0; j < ns; j++) {
+      if (filled > 0 && (filled == K || std::fabs(dt1 - window_dt1) > 1e-12 * std::fabs(window_dt1))) {
+        int r2 = run_window(s, filled, window_dt1, false);
+        if (r2)
+          return r2;
+        filled = 0;
+      }
+      if (filled == 0) {
+        window_dt1 = dt1;
+        FDM_CUDA(cudaEventSynchronize(s->slot_ev[s->slot]));
+      }
+      SplitStep& st = s->steps_h[(size_t)s->slot * K + filled];
+      const double tc = start + j * dts;
+      st.t = tc;
+      st.mid = tc + 0.5 * dts;
+      st.dt0 = s->heun.dt;
+      st.n0 = s->heun.n;
+      st.global_no = (int)std::min<int64_t>(s->split_no, 2147483647);
+      s->split_no++;
+      filled++;
+    }
+    k++;
+    t = rc.start + (double)k / rc.n * span;
+  }
+  int r3 = run_window(s, filled, window_dt1, true);
+  if (r3)
+    return r3;
+  FDM_CUDA(cudaEventRecord(s->adv_stop, s->stream));
+  if (s->cfg.check_nan && s->n_nodes > 0) {
+    FDM_CUDA(cudaMemsetAsync(s->nonfinite.p, 0, sizeof(int), s->stream));
+    FDM_CUDA(launch_count_nonfinite(s->vm.p, s->n_nodes, s->nonfinite.p, s->stream));
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  float ms = 0;
+  FDM_CUDA(cudaEventElapsedTime(&ms, s->adv_start, s->adv_stop));
+  s->adv_ms += ms;
+  for (size_t i = 0; i + 1 < s->ev_used; i += 2) {
+    float m2 = 0;
+    FDM_CUDA(cudaEventElapsedTime(&m2, s->ev_pool[i], s->ev_pool[i + 1]));
+    s->main_ms += m2;
+    s->main_launches++;
+  }
+  (void)launches0;
+  if (s->cfg.check_nan && s->n_nodes > 0) {
+    int bad = 0;
+    FDM_CUDA(cudaMemcpy(&bad, s->nonfinite.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (bad)
+      return fail(s, FDM_ERR_NAN, "fdm_advance: " + std::to_string(bad) + " non-finite Vm values");
+  }
+  return FDM_OK;
+}
+
+extern "C" int64_t fdm_split_steps(const fdm_solver* s) { return s ? s->split_no : 0; }
+
+extern "C" int fdm_get_timing(const fdm_solver* s, double* main_ms, int64_t* main_launches, double* adv_ms,
+                              int64_t* launches)
+{
+  if (!s)
+    return FDM_ERR_ARG;
+  if (main_ms)
+    *main_ms = s->main_ms;
+  if (main_launches)
+    *main_launches = s->main_launches;
+  if (adv_ms)
+    *adv_ms = s->adv_ms;
+  if (launches)
+    *launches = s->launches;
+  return FDM_OK;
+}
+
+extern "C" int fdm_reset_timing(fdm_solver* s)
+{
+  if (!s)
+    return FDM_ERR_ARG;
+  s->main_ms = s->adv_ms = 0;
+  s->main_launches = s->launches = 0;
+  return FDM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// checkpoint (saveFiberDataCheckpoint / restoreFiberDataCheckpoint): device-to-device snapshot
+// ---------------------------------------------------------------------------------------------
+extern "C" int fdm_checkpoint_save(fdm_solver* s)
+{
+  if (!s)
+    return FDM_ERR_ARG;
+  FDM_BIND(s);
+  const int64_t N = s->n_nodes;
+  const int NS = s->model->n_states;
+  const int nf = s->n_fibers;
+  FDM_CUDA(s->ck_vm.alloc(std::max<int64_t>(N, 1)));
+  FDM_CUDA(s->ck_states.alloc((size_t)std::max<int64_t>(N, 1) * std::max(NS - 1, 1) * s->real_bytes));
+  FDM_CUDA(s->ck_last.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->ck_jit.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->ck_jidx.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->ck_hbs.alloc(std::max(nf, 1)));
+  if (N > 0) {
+    FDM_CUDA(cudaMemcpyAsync(s->ck_vm.p, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->stream));
+    if (NS > 1)
+      FDM_CUDA(cudaMemcpyAsync(s->ck_states.p, s->states.p, (size_t)N * (NS - 1) * s->real_bytes,
+                               cudaMemcpyDeviceToDevice, s->stream));
+  }
+  if (nf > 0 && s->stimulation_set) {
+    FDM_CUDA(cudaMemcpyAsync(s->ck_last.p, s->last_check.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->ck_jit.p, s->cur_jitter.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->ck_jidx.p, s->jitter_idx.p, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->ck_hbs.p, s->hbs.p, nf, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  s->ck_strang = s->strang;
+  s->ck_heun = s->heun;
+  s->ck_diff = s->diff;
+  s->ck_tss_init = s->tss_init;
+  s->ck_split = s->split_no;
+  s->ck_valid = true;
+  return FDM_OK;
+}
+
+extern "C" int fdm_checkpoint_restore(fdm_solver* s)
+{
+  if (!s || !s->ck_valid)
+    return fail(s, FDM_ERR_ARG, "fdm_checkpoint_restore: no checkpoint saved");
+  FDM_BIND(s);
+  const int64_t N = s->n_nodes;
+  const int NS = s->model->n_states;
+  const int nf = s->n_fibers;
+  if (N > 0) {
+    FDM_CUDA(cudaMemcpyAsync(s->vm.p, s->ck_vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->stream));
+    if (NS > 1)
+      FDM_CUDA(cudaMemcpyAsync(s->states.p, s->ck_states.p, (size_t)N * (NS - 1) * s->real_bytes,
+                               cudaMemcpyDeviceToDevice, s->stream));
+  }
+  if (nf > 0 && s->stimulation_set) {
+    FDM_CUDA(cudaMemcpyAsync(s->last_check.p, s->ck_last.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->cur_jitter.p, s->ck_jit.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, s->ck_jidx.p, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->hbs.p, s->ck_hbs.p, nf, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  s->strang = s->ck_strang;
+  s->heun = s->ck_heun;
+  s->diff = s->ck_diff;
+  s->tss_init = s->ck_tss_init;
+  s->split_no = s->ck_split;
+  return FDM_OK;
+}

@@ -1,0 +1,45 @@
+// Internal launch interface between the host solver (fdm_host.cu) and the kernel translation units.
+// Every launcher is a plain C++ function taking device pointers and a stream.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fdm_kernels.cuh"
+
+namespace fdm {
+
+enum MathKind { MATH_EXACT = 0, MATH_APPROX = 1 };
+enum RealKind { REAL_F64 = 0, REAL_F32 = 1 };
+
+struct ModelDesc {
+  const char* name;
+  int n_states, n_algebraics, n_parameters;
+  const double* states_initial;
+  const double* parameter_defaults;
+  bool fused_supported;
+};
+
+// model table (fdm_kernels_split.cu)
+int n_models();
+const ModelDesc* model_desc(int model);
+
+// split path
+cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s);
+cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s);
+cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const int64_t* elem_offsets,
+                                const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
+                                double* coef, int64_t stride, cudaStream_t s);
+cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
+                                  double* vm, double* scratch, cudaStream_t s);
+// counts non-finite entries of x[0..n) into *count (device int, must be zeroed by the caller)
+cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t s);
+
+// fused path (fdm_fused_*.cu)
+struct FusedShape {
+  int threads, nodes_per_thread;
+};
+int fused_shapes(FusedShape* out, int capacity);
+// shape index into fused_shapes(); returns cudaErrorInvalidValue if the combination is not built
+cudaError_t launch_fused(int model, RealKind rk, MathKind mk, int shape, const FusedArgs& a, cudaStream_t s);
+
+} // namespace fdm

@@ -1,0 +1,725 @@
+// Device kernels of the fiber monodomain hot path (sm_100a).
+//
+// One Strang step of the reference (fast_monodomain_solver_compute.tpp:111-126) is
+//   n0D Heun substeps of the CellML model on every node   (compute0D, :131-254)
+//   one tridiagonal solve per fiber for the diffusion      (compute1D, :256-507)
+//   n0D Heun substeps starting at the mid time             (compute0D)
+// The kernels here implement it in two shapes:
+//   split:  reaction_kernel (one thread per node, states in HBM) + diffusion_warp_kernel (one warp per
+//           fiber, a partitioned Thomas sweep whose forward results go to a scratch array in HBM);
+//   fused:  fused_kernel (one CTA per bin of whole fibers; every thread keeps M nodes' states in
+//           registers across all split steps of a launch; the tridiagonal solve is a block-wide
+//           scan of affine maps in FP64; coefficients live in shared memory).
+// A stimulation_schedule_kernel advances each fiber's motor-unit stimulation machine
+// (compute.tpp:509-627) over all substeps of a launch window and writes one bit per substep.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fdm_math.cuh"
+
+namespace fdm {
+
+// --------------------------------------------------------------------------------------------
+// exact (never contracted) FP64 arithmetic for time values, so that the discrete stimulation
+// decisions are evaluated exactly as the C expressions are written
+// --------------------------------------------------------------------------------------------
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// one Strang step of a launch window (host computes these with the reference's time rules)
+struct SplitStep {
+  double t;      // currentTime of the split step
+  double mid;    // midTime = currentTime + 0.5*dtSplit
+  double dt0;    // Heun substep width
+  int n0;        // number of Heun substeps per half step
+  int global_no; // split step number since the start of the run (trace row)
+};
+
+struct StimArgs {
+  const uint8_t* firing_events;   // [row][col]
+  int rows, cols;
+  const int* motor_unit_no;       // per fiber (device order)
+  const double* call_frequency;
+  const double* repeat_after_first_call;
+  const double* call_enable_begin;
+  const double* jitter;           // per fiber n_jitter values
+  int n_jitter;
+  const uint8_t* evaluated;       // per fiber: 1 if the stimulation machine is advanced
+  double* last_check_time;        // machine state, persistent across launches
+  double* current_jitter;
+  int* jitter_index;
+  uint8_t* has_been_stimulated;
+  uint32_t* flags;                // [fiber][words_per_fiber] one bit per substep of the window
+  int words_per_fiber;
+  int nsub_stride;                // bit index = (step*2 + half)*nsub_stride + substep
+  int n_fibers;
+};
+
+// isCurrentPointStimulated (compute.tpp:509-627), one fiber, one substep
+__device__ __forceinline__ bool stimulation_machine(const StimArgs& a, int f, double t, double& last, double& jit,
+                                                    int& jidx)
+{
+  const double freq = a.call_frequency[f];
+  const double repeat = a.repeat_after_first_call[f];
+  const double begin = a.call_enable_begin[f];
+  bool check = false;
+  if (t >= xadd(last, xdiv(1.0, xadd(freq, jit))) && t >= xsub(begin, 1e-13)) {
+    check = true;
+    if (repeat != 0 && xsub(t, xadd(last, xdiv(1.0, xadd(freq, jit)))) > repeat) {
+      last = xadd(last, xdiv(1.0, xadd(freq, jit)));
+      double jf = 0.0;
+      if (a.n_jitter > 0)
+        jf = a.jitter[(int64_t)f * a.n_jitter + jidx % a.n_jitter];
+      jit = xmul(jf, freq);
+      jidx++;
+      check = false;
+    }
+  }
+  const int index = (int)round(xmul(t, freq));
+  int row = index % a.rows;
+  if (row < 0)
+    row += a.rows;
+  const int col = a.motor_unit_no[f] % a.cols;
+  return check && a.firing_events[(int64_t)row * a.cols + col] != 0;
+}
+
+#ifdef FDM_COMMON_KERNELS_TU
+__global__ void stimulation_schedule_kernel(StimArgs a, const SplitStep* __restrict__ steps, int n_steps)
+{
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= a.n_fibers)
+    return;
+  uint32_t* fl = a.flags + (int64_t)f * a.words_per_fiber;
+  for (int w = 0; w < a.words_per_fiber; w++)
+    fl[w] = 0u;
+  if (!a.evaluated[f])
+    return;
+  double last = a.last_check_time[f], jit = a.current_jitter[f];
+  int jidx = a.jitter_index[f];
+  uint8_t hbs = a.has_been_stimulated[f];
+  for (int j = 0; j < n_steps; j++) {
+    const SplitStep s = steps[j];
+    for (int h = 0; h < 2; h++) {
+      const double t0 = h ? s.mid : s.t;
+      uint32_t word = 0u;
+      int word_no = -1;
+      for (int k = 0; k < s.n0; k++) {
+        const double t = xadd(t0, xmul((double)k, s.dt0));
+        const bool st = stimulation_machine(a, f, t, last, jit, jidx);
+        if (st) {
+          hbs = 1;
+          const int bit = (j * 2 + h) * a.nsub_stride + k;
+          if (bit / 32 != word_no) {
+            if (word_no >= 0)
+              fl[word_no] |= word;
+            word_no = bit / 32;
+            word = 0u;
+          }
+          word |= 1u << (bit % 32);
+        }
+      }
+      if (word_no >= 0)
+        fl[word_no] |= word;
+    }
+  }
+  a.last_check_time[f] = last;
+  a.current_jitter[f] = jit;
+  a.jitter_index[f] = jidx;
+  a.has_been_stimulated[f] = hbs;
+}
+
+#endif // FDM_COMMON_KERNELS_TU
+
+__device__ __forceinline__ bool stim_bit(const uint32_t* __restrict__ flags, int words_per_fiber, int fiber, int bit)
+{
+  return (__ldg(flags + (int64_t)fiber * words_per_fiber + (bit >> 5)) >> (bit & 31)) & 1u;
+}
+
+// --------------------------------------------------------------------------------------------
+// one Heun step (03_generator_vc.cpp:1017-1130):
+//   y* = y + dt f(y); [Vm* := vStim]; y += dt/2 (f(y) + f(y*)); [Vm := vStim]
+// Vm is carried in FP64; the other states and the rates in RR (double or float).
+// --------------------------------------------------------------------------------------------
+template<class Model, class RR, class Math, bool STORE>
+__device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, const RR* __restrict__ P, double t,
+                                          double dt, bool clamp, double vstim, RR* __restrict__ alg_store)
+{
+  constexpr int NS = Model::nStates;
+  RR y[NS], r[NS], ys[NS], r2[NS];
+  RR alg[Model::nAlgebraics], alg2[Model::nAlgebraics];
+  y[0] = (RR)V;
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    y[s] = S[s - 1];
+  const RR tr = (RR)t;
+  Model::template rates<RR, Math>(tr, y, P, r, alg);
+  const RR dtr = (RR)dt;
+  const double vs = V + dt * (double)r[0];
+  ys[0] = (RR)vs;
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    ys[s] = y[s] + dtr * r[s];
+  if (clamp)
+    ys[0] = (RR)vstim;
+  Model::template rates<RR, Math>(tr, ys, P, r2, alg2);
+  V += 0.5 * dt * ((double)r[0] + (double)r2[0]);
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    S[s - 1] = y[s] + (RR)0.5 * dtr * (r[s] + r2[s]);
+  if (clamp)
+    V = vstim;
+  if (STORE) {
+#pragma unroll
+    for (int k = 0; k < Model::nAlgebraics; k++)
+      alg_store[k] = alg2[k];
+  }
+}
+
+// algebraicsForTransfer: copy the requested entries (selected at run time) without dynamic
+// register indexing
+template<class Model, class RR>
+__device__ __forceinline__ void store_algebraics(const RR* alg, int n_out, const int* __restrict__ idx,
+                                                 double* __restrict__ out, int64_t n_nodes, int64_t node)
+{
+  for (int q = 0; q < n_out; q++) {
+    const int want = idx[q];
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < Model::nAlgebraics; k++)
+      v = (k == want) ? (double)alg[k] : v;
+    out[q * n_nodes + node] = v;
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// split path: reaction kernel
+// --------------------------------------------------------------------------------------------
+struct ReactionArgs {
+  int64_t n_nodes;
+  int64_t stride;                 // SoA stride of states / parameters
+  double* vm;                     // [node]
+  void* states;                   // RR [(s-1)*stride + node], s = 1..nStates-1
+  const void* params;             // RR [p*stride + node]
+  const int* clamp_fiber;         // per node: fiber whose machine controls the clamp, or -1
+  const uint32_t* flags;
+  int words_per_fiber;
+  int nsub_stride;
+  double vstim;
+  int stimulus_mode;              // 0 clamp, 1 current (set parameter)
+  int stimulus_parameter;
+  double stimulus_value;
+  const SplitStep* steps;
+  int step;                       // index in window
+  int half;                       // 0: first half step, 1: second
+  int store_alg;                  // store the requested algebraics after the last substep
+  int n_alg_out;
+  const int* alg_indices;         // device
+  double* alg_out;                // [k][node]
+  const int* trace_slot;          // per node slot or -1 (may be null)
+  double* trace;                  // [global split no][slot]
+  int n_trace;
+  int64_t trace_capacity;
+};
+
+template<class Model, class RR, class Math>
+__global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
+{
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_nodes)
+    return;
+  constexpr int NS = Model::nStates;
+  constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
+  RR* st = (RR*)a.states;
+  const RR* pr = (const RR*)a.params;
+  double V = a.vm[i];
+  RR S[NS > 1 ? NS - 1 : 1];
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    S[s - 1] = st[(s - 1) * a.stride + i];
+  RR P[NP], Pstim[NP];
+#pragma unroll
+  for (int q = 0; q < Model::nParameters; q++) {
+    P[q] = pr[q * a.stride + i];
+    Pstim[q] = (a.stimulus_mode == 1 && q == a.stimulus_parameter) ? (RR)a.stimulus_value : P[q];
+  }
+  const int cf = a.clamp_fiber[i];
+  const SplitStep s = a.steps[a.step];
+  const double t0 = a.half ? s.mid : s.t;
+  const int base = (a.step * 2 + a.half) * a.nsub_stride;
+  for (int k = 0; k < s.n0; k++) {
+    const double t = xadd(t0, xmul((double)k, s.dt0));
+    const bool stim = cf >= 0 && stim_bit(a.flags, a.words_per_fiber, cf, base + k);
+    const bool vclamp = stim && a.stimulus_mode == 0;
+    RR Pk[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+      Pk[q] = (stim && a.stimulus_mode == 1) ? Pstim[q] : P[q];
+    if (a.store_alg && k == s.n0 - 1) {
+      RR alg[Model::nAlgebraics];
+      heun_step<Model, RR, Math, true>(V, S, Pk, t, s.dt0, vclamp, a.vstim, alg);
+      store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, i);
+    } else {
+      heun_step<Model, RR, Math, false>(V, S, Pk, t, s.dt0, vclamp, a.vstim, nullptr);
+    }
+  }
+  a.vm[i] = V;
+#pragma unroll
+  for (int s2 = 1; s2 < NS; s2++)
+    st[(s2 - 1) * a.stride + i] = S[s2 - 1];
+  if (a.half == 1 && a.trace_slot) {
+    const int slot = a.trace_slot[i];
+    if (slot >= 0 && s.global_no < a.trace_capacity)
+      a.trace[(int64_t)s.global_no * a.n_trace + slot] = V;
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// diffusion: coefficients of the per-fiber tridiagonal system, computed once per (dt1D, prefactor)
+//   IE: (K - M/dt) u+ = -M/dt u            CN: (K/2 - M/dt) u+ = (-K/2 - M/dt) u
+// following the element loops of compute.tpp:336-449, and its LU factors for
+//   d'_i = mulF_i d'_{i-1} + inv_i d_i,     x_i = d'_i - cp_i x_{i+1}
+// Per node the six doubles are stored as coef[k*stride + node], k = 0..5 = mulF, inv, cp, l, m, r
+// with d_i = l_i u_{i-1} + m_i u_i + r_i u_{i+1}.
+// --------------------------------------------------------------------------------------------
+#ifdef FDM_COMMON_KERNELS_TU
+__global__ void diffusion_coefficients_kernel(int n_fibers, const int64_t* __restrict__ fiber_offsets,
+                                              const int64_t* __restrict__ elem_offsets,
+                                              const double* __restrict__ element_lengths,
+                                              const double* __restrict__ prefactor, double dt, int implicit_euler,
+                                              double* __restrict__ coef, int64_t stride)
+{
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n_fibers)
+    return;
+  const int64_t o = fiber_offsets[f];
+  const int64_t n = fiber_offsets[f + 1] - o;
+  const double* h = element_lengths + elem_offsets[f];
+  const double pf = prefactor[f];
+  double cp_prev = 0.0;
+  for (int64_t v = 0; v < n; v++) {
+    double a = 0, b = 0, c = 0, l = 0, m = 0, r = 0;
+    if (v > 0) {
+      const double h_left = h[v - 1];
+      const double k_left = 1. / h_left * (1) * pf;
+      const double m_left = h_left * 1. / 6;
+      const double k_right = 1. / h_left * (-1) * pf;
+      const double m_right = h_left * 1. / 3;
+      if (implicit_euler) {
+        a = (k_left - 1 / dt * m_left);
+        b += (k_right - 1 / dt * m_right);
+        l = (-1 / dt * m_left);
+        m += (-1 / dt * m_right);
+      } else {
+        a = (k_left / 2. - 1 / dt * m_left);
+        b += (k_right / 2. - 1 / dt * m_right);
+        l = (-k_left / 2. - 1 / dt * m_left);
+        m += (-k_right / 2. - 1 / dt * m_right);
+      }
+    }
+    if (v < n - 1) {
+      const double h_right = h[v];
+      const double k_right = 1. / h_right * (1) * pf;
+      const double m_right = h_right * 1. / 6;
+      const double k_left = 1. / h_right * (-1) * pf;
+      const double m_left = h_right * 1. / 3;
+      if (implicit_euler) {
+        c = (k_right - 1 / dt * m_right);
+        b += (k_left - 1 / dt * m_left);
+        m += (-1 / dt * m_left);
+        r = (-1 / dt * m_right);
+      } else {
+        c = (k_right / 2. - 1 / dt * m_right);
+        b += (k_left / 2. - 1 / dt * m_left);
+        m += (-k_left / 2. - 1 / dt * m_left);
+        r = (-k_right / 2. - 1 / dt * m_right);
+      }
+    }
+    double inv, mulF, cp;
+    if (v == 0) {
+      inv = 1.0 / b;
+      mulF = 0.0;
+      cp = c / b;
+    } else {
+      const double den = b - cp_prev * a;
+      inv = 1.0 / den;
+      mulF = -a * inv;
+      cp = (v != n - 1) ? c / den : 0.0;
+    }
+    cp_prev = cp;
+    const int64_t i = o + v;
+    coef[0 * stride + i] = mulF;
+    coef[1 * stride + i] = inv;
+    coef[2 * stride + i] = cp;
+    coef[3 * stride + i] = l;
+    coef[4 * stride + i] = m;
+    coef[5 * stride + i] = r;
+  }
+}
+
+#endif // FDM_COMMON_KERNELS_TU
+
+// affine map x -> F x + G; compose(first, second) = second o first
+struct Affine {
+  double F, G;
+};
+__device__ __forceinline__ Affine compose(const Affine& first, const Affine& second)
+{
+  return Affine{second.F * first.F, fma(second.F, first.G, second.G)};
+}
+
+#ifdef FDM_COMMON_KERNELS_TU
+// split path: one warp per fiber; each lane owns a contiguous chunk of the fiber.
+// Forward sweep results d' go to `scratch` (one double per node) for the backward sweep.
+__global__ void __launch_bounds__(128) diffusion_warp_kernel(int n_fibers, const int64_t* __restrict__ fiber_offsets,
+                                                             const double* __restrict__ coef, int64_t stride,
+                                                             double* __restrict__ vm, double* __restrict__ scratch)
+{
+  const int lane = threadIdx.x & 31;
+  const int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (f >= n_fibers)
+    return;
+  const int64_t o = fiber_offsets[f];
+  const int64_t n = fiber_offsets[f + 1] - o;
+  const int64_t L = (n + 31) / 32;
+  const int64_t lo = o + min((int64_t)lane * L, n);
+  const int64_t hi = o + min((int64_t)(lane + 1) * L, n);
+  const double* mulF = coef;
+  const double* inv = coef + stride;
+  const double* cp = coef + 2 * stride;
+  const double* cl = coef + 3 * stride;
+  const double* cm = coef + 4 * stride;
+  const double* cr = coef + 5 * stride;
+  auto rhs = [&](int64_t i) {
+    const double up = i > o ? vm[i - 1] : 0.0;
+    const double un = i < o + n - 1 ? vm[i + 1] : 0.0;
+    return cl[i] * up + cm[i] * vm[i] + cr[i] * un;
+  };
+  // forward: compose the chunk
+  Affine acc{1.0, 0.0};
+  for (int64_t i = lo; i < hi; i++)
+    acc = compose(acc, Affine{mulF[i], inv[i] * rhs(i)});
+  // inclusive warp scan, then shift to exclusive
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double F = __shfl_up_sync(0xffffffffu, acc.F, off);
+    const double G = __shfl_up_sync(0xffffffffu, acc.G, off);
+    if (lane >= off)
+      acc = compose(Affine{F, G}, acc);
+  }
+  double dp = __shfl_up_sync(0xffffffffu, acc.G, 1);
+  if (lane == 0)
+    dp = 0.0;
+  for (int64_t i = lo; i < hi; i++) {
+    dp = mulF[i] * dp + inv[i] * rhs(i);
+    scratch[i] = dp;
+  }
+  __syncwarp();
+  // backward: x_i = -cp_i x_{i+1} + d'_i, composed from the chunk's end
+  Affine bacc{1.0, 0.0};
+  for (int64_t i = hi - 1; i >= lo; i--)
+    bacc = compose(bacc, Affine{-cp[i], scratch[i]});
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double F = __shfl_down_sync(0xffffffffu, bacc.F, off);
+    const double G = __shfl_down_sync(0xffffffffu, bacc.G, off);
+    if (lane + off < 32)
+      bacc = compose(Affine{F, G}, bacc);
+  }
+  double x = __shfl_down_sync(0xffffffffu, bacc.G, 1);
+  if (lane == 31)
+    x = 0.0;
+  __syncwarp();
+  for (int64_t i = hi - 1; i >= lo; i--) {
+    x = -cp[i] * x + scratch[i];
+    vm[i] = x;
+  }
+}
+
+#endif // FDM_COMMON_KERNELS_TU
+
+// --------------------------------------------------------------------------------------------
+// fused path
+// --------------------------------------------------------------------------------------------
+constexpr int FUSED_MAX_FIBERS_PER_BIN = 32;
+
+struct FusedArgs {
+  int n_bins;
+  const int* bin_fiber_start;     // [n_bins+1] range in bin_fibers
+  const int* bin_fibers;          // fiber numbers, bin after bin (at most FUSED_MAX_FIBERS_PER_BIN per bin)
+  const int64_t* fiber_offsets;   // node offsets of the fibers
+  int64_t stride;
+  double* vm;
+  void* states;                   // RR SoA
+  const void* params;             // RR SoA
+  const double* coef;             // 6 x stride
+  const int* clamp_fiber;
+  const uint32_t* flags;
+  int words_per_fiber;
+  int nsub_stride;
+  double vstim;
+  int stimulus_mode;
+  int stimulus_parameter;
+  double stimulus_value;
+  const SplitStep* steps;
+  int n_steps;
+  int store_alg;
+  int n_alg_out;
+  const int* alg_indices;
+  double* alg_out;
+  int64_t n_nodes;
+  const int* trace_slot;
+  double* trace;
+  int n_trace;
+  int64_t trace_capacity;
+};
+
+// block-wide exclusive scan of affine maps in thread order (REVERSE: from the last thread down)
+template<int T, bool REVERSE>
+__device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, double* sG)
+{
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  constexpr int NW = T / 32;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    double F, G;
+    if (!REVERSE) {
+      F = __shfl_up_sync(0xffffffffu, acc.F, off);
+      G = __shfl_up_sync(0xffffffffu, acc.G, off);
+      if (lane >= off)
+        acc = compose(Affine{F, G}, acc);
+    } else {
+      F = __shfl_down_sync(0xffffffffu, acc.F, off);
+      G = __shfl_down_sync(0xffffffffu, acc.G, off);
+      if (lane + off < 32)
+        acc = compose(Affine{F, G}, acc);
+    }
+  }
+  // warp totals
+  const int last_lane = REVERSE ? 0 : 31;
+  if (lane == last_lane) {
+    sF[warp] = acc.F;
+    sG[warp] = acc.G;
+  }
+  // intra-warp exclusive prefix
+  double exF = REVERSE ? __shfl_down_sync(0xffffffffu, acc.F, 1) : __shfl_up_sync(0xffffffffu, acc.F, 1);
+  double exG = REVERSE ? __shfl_down_sync(0xffffffffu, acc.G, 1) : __shfl_up_sync(0xffffffffu, acc.G, 1);
+  const bool first_in_warp = REVERSE ? (lane == 31) : (lane == 0);
+  if (first_in_warp) {
+    exF = 1.0;
+    exG = 0.0;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // exclusive scan over the NW warp totals, in scan order
+    const int w = REVERSE ? (NW - 1 - lane) : lane;
+    Affine v = lane < NW ? Affine{sF[w], sG[w]} : Affine{1.0, 0.0};
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double F = __shfl_up_sync(0xffffffffu, v.F, off);
+      const double G = __shfl_up_sync(0xffffffffu, v.G, off);
+      if (lane >= off)
+        v = compose(Affine{F, G}, v);
+    }
+    double pF = __shfl_up_sync(0xffffffffu, v.F, 1);
+    double pG = __shfl_up_sync(0xffffffffu, v.G, 1);
+    if (lane == 0) {
+      pF = 1.0;
+      pG = 0.0;
+    }
+    __syncwarp();
+    if (lane < NW) {
+      sF[NW + w] = pF;
+      sG[NW + w] = pG;
+    }
+  }
+  __syncthreads();
+  const Affine wp{sF[NW + warp], sG[NW + warp]};
+  const Affine ex = compose(wp, Affine{exF, exG});
+  return ex.G; // applied to the zero entering the first node of the bin
+}
+
+template<class Model, class RR, class Math, int T, int M>
+__global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
+{
+  constexpr int NS = Model::nStates;
+  constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
+  constexpr int CAP = T * M;
+  extern __shared__ double smem[];
+  double* sc = smem;                 // 6 x CAP coefficients
+  double* vfirst = sc + 6 * CAP;     // T
+  double* vlast = vfirst + T;        // T
+  double* sF = vlast + T;            // 2 * (T/32)
+  double* sG = sF + 2 * (T / 32);    // 2 * (T/32)
+  __shared__ int64_t fib_global[FUSED_MAX_FIBERS_PER_BIN];
+  __shared__ int fib_local[FUSED_MAX_FIBERS_PER_BIN + 1];
+
+  const int tid = threadIdx.x;
+  const int bin = blockIdx.x;
+  if (bin >= a.n_bins)
+    return;
+  // the bin's fibers, concatenated in bin-local node numbering
+  const int f0 = a.bin_fiber_start[bin];
+  const int nf = a.bin_fiber_start[bin + 1] - f0;
+  if (tid == 0) {
+    int loc = 0;
+    for (int k = 0; k < nf; k++) {
+      const int fib = a.bin_fibers[f0 + k];
+      fib_global[k] = a.fiber_offsets[fib];
+      fib_local[k] = loc;
+      loc += (int)(a.fiber_offsets[fib + 1] - a.fiber_offsets[fib]);
+    }
+    fib_local[nf] = loc;
+  }
+  __syncthreads();
+  const int nb = fib_local[nf];
+  auto global_node = [&](int q) -> int64_t {
+    int k = 0;
+    while (k + 1 < nf && q >= fib_local[k + 1])
+      k++;
+    return fib_global[k] + (q - fib_local[k]);
+  };
+
+  // coefficients into shared memory (zero beyond the bin: those nodes carry x = 0)
+  for (int q = tid; q < CAP; q += T) {
+    const bool ok = q < nb;
+    const int64_t g = ok ? global_node(q) : 0;
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      sc[k * CAP + q] = ok ? a.coef[k * a.stride + g] : 0.0;
+  }
+
+  const RR* pr = (const RR*)a.params;
+  RR* st = (RR*)a.states;
+  double V[M];
+  RR S[M][NS > 1 ? NS - 1 : 1];
+  RR P[M][NP];
+  int cf[M];
+  int ts[M];
+  int64_t gi[M];
+#pragma unroll
+  for (int j = 0; j < M; j++) {
+    const int q = tid * M + j;
+    const bool ok = q < nb;
+    const int64_t i = ok ? global_node(q) : 0;
+    gi[j] = i;
+    V[j] = ok ? a.vm[i] : 0.0;
+#pragma unroll
+    for (int s = 1; s < NS; s++)
+      S[j][s - 1] = ok ? st[(s - 1) * a.stride + i] : (RR)0;
+#pragma unroll
+    for (int p = 0; p < Model::nParameters; p++)
+      P[j][p] = ok ? pr[p * a.stride + i] : (RR)0;
+    cf[j] = ok ? a.clamp_fiber[i] : -1;
+    ts[j] = (ok && a.trace_slot) ? a.trace_slot[i] : -1;
+  }
+  __syncthreads();
+
+  for (int step = 0; step < a.n_steps; step++) {
+    const SplitStep s = a.steps[step];
+#pragma unroll 1
+    for (int half = 0; half < 2; half++) {
+      const double t0 = half ? s.mid : s.t;
+      const int base = (step * 2 + half) * a.nsub_stride;
+      const bool last_half = a.store_alg && half == 1 && step == a.n_steps - 1;
+#pragma unroll 1
+      for (int k = 0; k < s.n0; k++) {
+        const double t = xadd(t0, xmul((double)k, s.dt0));
+        const bool store_now = last_half && k == s.n0 - 1;
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+          if (tid * M + j >= nb)
+            continue;
+          const bool stim = cf[j] >= 0 && stim_bit(a.flags, a.words_per_fiber, cf[j], base + k);
+          RR Pk[NP];
+#pragma unroll
+          for (int p = 0; p < NP; p++)
+            Pk[p] = (stim && a.stimulus_mode == 1 && p == a.stimulus_parameter) ? (RR)a.stimulus_value : P[j][p];
+          const bool vclamp = stim && a.stimulus_mode == 0;
+          if (!store_now) {
+            heun_step<Model, RR, Math, false>(V[j], S[j], Pk, t, s.dt0, vclamp, a.vstim, nullptr);
+          } else {
+            RR alg[Model::nAlgebraics];
+            heun_step<Model, RR, Math, true>(V[j], S[j], Pk, t, s.dt0, vclamp, a.vstim, alg);
+            store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, gi[j]);
+          }
+        }
+      }
+      if (half == 1)
+        break;
+
+      // ---- diffusion: block-wide tridiagonal solve in FP64 ----
+      vfirst[tid] = V[0];
+      vlast[tid] = V[M - 1];
+      __syncthreads();
+      const double vprev = tid > 0 ? vlast[tid - 1] : 0.0;
+      const double vnext = tid < T - 1 ? vfirst[tid + 1] : 0.0;
+      double d[M];
+#pragma unroll
+      for (int j = 0; j < M; j++) {
+        const int q = tid * M + j;
+        const double um = j > 0 ? V[j - 1] : vprev;
+        const double up = j < M - 1 ? V[j + 1] : vnext;
+        d[j] = sc[3 * CAP + q] * um + sc[4 * CAP + q] * V[j] + sc[5 * CAP + q] * up;
+      }
+      Affine acc{1.0, 0.0};
+#pragma unroll
+      for (int j = 0; j < M; j++) {
+        const int q = tid * M + j;
+        acc = compose(acc, Affine{sc[0 * CAP + q], sc[1 * CAP + q] * d[j]});
+      }
+      double dp = block_scan_incoming<T, false>(acc, sF, sG);
+#pragma unroll
+      for (int j = 0; j < M; j++) {
+        const int q = tid * M + j;
+        dp = sc[0 * CAP + q] * dp + sc[1 * CAP + q] * d[j];
+        d[j] = dp;
+      }
+      Affine bacc{1.0, 0.0};
+#pragma unroll
+      for (int j = M - 1; j >= 0; j--) {
+        const int q = tid * M + j;
+        bacc = compose(bacc, Affine{-sc[2 * CAP + q], d[j]});
+      }
+      __syncthreads(); // sF/sG reuse
+      double x = block_scan_incoming<T, true>(bacc, sF, sG);
+#pragma unroll
+      for (int j = M - 1; j >= 0; j--) {
+        const int q = tid * M + j;
+        x = -sc[2 * CAP + q] * x + d[j];
+        V[j] = x;
+      }
+      __syncthreads(); // vfirst/vlast and sF/sG reuse
+    }
+    if (a.trace_slot) {
+#pragma unroll
+      for (int j = 0; j < M; j++)
+        if (ts[j] >= 0 && s.global_no < a.trace_capacity)
+          a.trace[(int64_t)s.global_no * a.n_trace + ts[j]] = V[j];
+    }
+  }
+
+#pragma unroll
+  for (int j = 0; j < M; j++) {
+    const int q = tid * M + j;
+    if (q < nb) {
+      const int64_t i = gi[j];
+      a.vm[i] = V[j];
+#pragma unroll
+      for (int s = 1; s < NS; s++)
+        st[(s - 1) * a.stride + i] = S[j][s - 1];
+    }
+  }
+}
+
+template<int T, int M>
+constexpr size_t fused_smem_bytes()
+{
+  return sizeof(double) * (6 * T * M + 2 * T + 4 * (T / 32));
+}
+
+} // namespace fdm

@@ -1,0 +1,112 @@
+// Split-path kernels (reaction, diffusion, stimulation schedule) and the model table.
+#define FDM_COMMON_KERNELS_TU
+#include "fdm_internal.h"
+
+#include "generated/hodgkin_huxley_1952_anone_c2_3_4.cuh"
+#include "generated/shorten_ocallaghan_davidson_soboleva_2007_a32_c65.cuh"
+
+namespace fdm {
+
+using HH = fdm_model_hodgkin_huxley_1952_anone_c2_3_4;
+using SH = fdm_model_shorten_ocallaghan_davidson_soboleva_2007_a32_c65;
+
+static const ModelDesc g_models[] = {
+  {HH::name, HH::nStates, HH::nAlgebraics, HH::nParameters, HH::statesInitialValues, HH::parameterDefaults, true},
+  {SH::name, SH::nStates, SH::nAlgebraics, SH::nParameters, SH::statesInitialValues, SH::parameterDefaults, false},
+};
+
+int n_models() { return (int)(sizeof(g_models) / sizeof(g_models[0])); }
+
+const ModelDesc* model_desc(int model)
+{
+  if (model < 0 || model >= n_models())
+    return nullptr;
+  return &g_models[model];
+}
+
+template<class Model, class RR, class Math>
+static cudaError_t reaction_one(const ReactionArgs& a, cudaStream_t s)
+{
+  const int T = 128;
+  const int64_t blocks = (a.n_nodes + T - 1) / T;
+  if (blocks == 0)
+    return cudaSuccess;
+  reaction_kernel<Model, RR, Math><<<(unsigned)blocks, T, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template<class Model>
+static cudaError_t reaction_model(RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s)
+{
+  if (rk == REAL_F64)
+    return mk == MATH_EXACT ? reaction_one<Model, double, fdm_math_exact>(a, s)
+                            : reaction_one<Model, double, fdm_math_approx>(a, s);
+  return mk == MATH_EXACT ? reaction_one<Model, float, fdm_math_exact>(a, s)
+                          : reaction_one<Model, float, fdm_math_approx>(a, s);
+}
+
+cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s)
+{
+  switch (model) {
+  case 0: return reaction_model<HH>(rk, mk, a, s);
+  case 1: return reaction_model<SH>(rk, mk, a, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s)
+{
+  if (a.n_fibers == 0)
+    return cudaSuccess;
+  const int T = 128;
+  stimulation_schedule_kernel<<<(a.n_fibers + T - 1) / T, T, 0, s>>>(a, steps, n_steps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const int64_t* elem_offsets,
+                                const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
+                                double* coef, int64_t stride, cudaStream_t s)
+{
+  if (n_fibers == 0)
+    return cudaSuccess;
+  const int T = 64;
+  diffusion_coefficients_kernel<<<(n_fibers + T - 1) / T, T, 0, s>>>(n_fibers, fiber_offsets, elem_offsets,
+                                                                     element_lengths, prefactor, dt, implicit_euler,
+                                                                     coef, stride);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
+                                  double* vm, double* scratch, cudaStream_t s)
+{
+  if (n_fibers == 0)
+    return cudaSuccess;
+  const int T = 128;
+  const int64_t threads = (int64_t)n_fibers * 32;
+  diffusion_warp_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, s>>>(n_fibers, fiber_offsets, coef, stride, vm,
+                                                                        scratch);
+  return cudaGetLastError();
+}
+
+__global__ void count_nonfinite_kernel(const double* __restrict__ x, int64_t n, int* count)
+{
+  int local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    local += isfinite(x[i]) ? 0 : 1;
+  local = __reduce_add_sync(0xffffffffu, local);
+  if ((threadIdx.x & 31) == 0 && local)
+    atomicAdd(count, local);
+}
+
+cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t s)
+{
+  if (n == 0)
+    return cudaSuccess;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 8)
+    blocks = 148 * 8;
+  count_nonfinite_kernel<<<blocks, 256, 0, s>>>(x, n, count);
+  return cudaGetLastError();
+}
+
+} // namespace fdm

@@ -1,0 +1,524 @@
+"""Python settings harness and host-side operator API of the B200 FastMonodomainSolver.
+
+:class:`FastMonodomainSolver` mirrors the reference class
+``FastMonodomainSolverBase`` (core/src/specialized_solver/fast_monodomain_solver/
+fast_monodomain_solver_base.h:85-124): ``initialize``, ``run``, ``advanceTimeSpan``,
+``setTimeSpan``, ``startTime``, ``endTime``, ``data``, ``reset``,
+``saveFiberDataCheckpoint`` and ``restoreFiberDataCheckpoint``, wrapped by the
+RepeatedCall driver semantics (repeated_call.tpp:43-80).  It is constructed either from a
+reference-style settings dict (:meth:`FastMonodomainSolver.from_settings`, the keys listed in
+:func:`parse_settings`) or from a :class:`FiberSystem` of plain arrays.  All computation goes
+through the C ABI of libfdm_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import math
+import os
+import warnings
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from . import inputs
+
+SCHEMES = {"ImplicitEuler": 0, "CrankNicolson": 1}
+METHODS = {"split": 0, "fused": 1}
+PRECISIONS = {"fp64": 0, "fp32": 1}
+CLAMP_RULES = {"vc": 0, "center": 1}
+STIMULUS_MODES = {"clamp": 0, "current": 1}
+
+#: parameter variants built into the library (see opendihu_b200/cellml.py VARIANTS)
+VARIANT_PARAMETERS = {
+    "hodgkin_huxley_1952": ((), (2, 3, 4)),
+    "shorten_ocallaghan_davidson_soboleva_2007": ((32,), (65,)),
+}
+
+
+@dataclass
+class FiberSystem:
+    """Everything the solver needs, as arrays (node order = fibers concatenated)."""
+    model: str
+    fiber_offsets: np.ndarray                 # int64 [n_fibers+1]
+    element_lengths: np.ndarray               # float64 [n_nodes - n_fibers]
+    prefactor: np.ndarray                     # float64 [n_fibers]
+    firing_events: np.ndarray                 # uint8 [rows, cols]
+    motor_unit_no: np.ndarray                 # int32 [n_fibers]
+    stimulation_point_index: np.ndarray       # int32 [n_fibers]
+    call_frequency: np.ndarray                # float64 [n_fibers]
+    repeat_after_first_call: np.ndarray       # float64 [n_fibers]
+    call_enable_begin: np.ndarray             # float64 [n_fibers]
+    jitter: np.ndarray = None                 # float64 [n_fibers, n_jitter]
+    parameters: Optional[np.ndarray] = None   # float64 [n_params, n_nodes] (variant slots)
+    states: Optional[np.ndarray] = None       # float64 [n_states, n_nodes]
+    diffusion_scheme: str = "ImplicitEuler"
+    dt_0d: float = 1e-4
+    dt_1d: float = 1e-3
+    dt_splitting: float = 1e-3
+    dt_repeated_call: float = 1e-3
+    start_time: float = 0.0
+    end_time: float = 10.0
+    approximate_exponential_function: bool = False
+    value_for_stimulated_point: float = 20.0
+    clamp_rule: str = "vc"
+    vc_width: int = 4
+    n_ranks: int = 1
+    stimulus_mode: str = "clamp"
+    stimulus_parameter: int = 0
+    stimulus_value: float = 0.0
+    algebraics_for_transfer: Sequence[int] = ()
+    states_for_transfer: Sequence[int] = (0,)
+
+    @property
+    def n_fibers(self) -> int:
+        return len(self.fiber_offsets) - 1
+
+    @property
+    def n_nodes(self) -> int:
+        return int(self.fiber_offsets[-1])
+
+    def copy(self) -> "FiberSystem":
+        return copy.deepcopy(self)
+
+
+def model_sizes(model: str):
+    ns, na, npar, init, defaults = N.model_info(N.MODEL_IDS[model])
+    return ns, na, npar, init, defaults
+
+
+def uniform_fibers(model: str, lengths: Sequence[int], dx: float, prefactor, *, firing_events=None,
+                   motor_unit_no=None, call_frequency: float = 0.1, repeat_after_first_call: float = 0.1,
+                   call_enable_begin: float = 0.0, jitter=None, **kw) -> FiberSystem:
+    """Straight fibers of the given node counts and element length dx (cm)."""
+    lengths = np.asarray(lengths, np.int64)
+    nf = len(lengths)
+    off = np.zeros(nf + 1, np.int64)
+    off[1:] = np.cumsum(lengths)
+    elem = np.full(int(off[-1]) - nf, float(dx))
+    pf = np.broadcast_to(np.asarray(prefactor, np.float64), (nf,)).copy()
+    if firing_events is None:
+        firing_events = np.ones((1, 1), np.uint8)
+    if motor_unit_no is None:
+        motor_unit_no = np.zeros(nf, np.int32)
+    return FiberSystem(
+        model=model, fiber_offsets=off, element_lengths=elem, prefactor=pf,
+        firing_events=np.asarray(firing_events, np.uint8), motor_unit_no=np.asarray(motor_unit_no, np.int32),
+        stimulation_point_index=(lengths // 2).astype(np.int32),
+        call_frequency=np.full(nf, call_frequency), repeat_after_first_call=np.full(nf, repeat_after_first_call),
+        call_enable_begin=np.full(nf, call_enable_begin),
+        jitter=np.zeros((nf, 0)) if jitter is None else np.asarray(jitter, np.float64), **kw)
+
+
+# ----------------------------------------------------------------------------------------------
+# reference settings dict
+# ----------------------------------------------------------------------------------------------
+
+def _as_list(v):
+    if v is None:
+        return []
+    if isinstance(v, (list, tuple, np.ndarray)):
+        return list(v)
+    return [v]
+
+
+def _first_key(d: dict, *keys):
+    for k in keys:
+        if k in d:
+            return k, d[k]
+    return None, None
+
+
+def _mesh_element_lengths(meshes: dict, name: str) -> np.ndarray:
+    m = meshes[name]
+    if "nodePositions" in m:
+        p = np.asarray(m["nodePositions"], np.float64).reshape(-1, 3)
+        return np.sqrt(np.sum((p[1:] - p[:-1]) ** 2, axis=1))
+    n = int(_as_list(m["nElements"])[0])
+    L = float(_as_list(m.get("physicalExtent", [n]))[0])
+    return np.full(n, L / n)
+
+
+def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
+    """Read a reference settings dict of ``RepeatedCall`` -> ``FastMonodomainSolver`` -> ``MultipleInstances``
+    -> ``StrangSplitting`` -> (``Heun``/``CellML``, ``ImplicitEuler``|``CrankNicolson``/``FiniteElementMethod``).
+
+    Keys read (with the reference defaults): RepeatedCall ``timeStepWidth``/``endTime``/``startTime``;
+    FastMonodomainSolver ``fiberDistributionFile``, ``firingTimesFile``, ``valueForStimulatedPoint`` (20),
+    ``neuromuscularJunctionRelativeSize`` (0), ``onlyComputeIfHasBeenStimulated``,
+    ``disableComputationWhenStatesAreCloseToEquilibrium``, ``useSinglePrecision``; Strang ``timeStepWidth``;
+    Heun ``timeStepWidth``; CellML ``modelFilename``, ``approximateExponentialFunction``,
+    ``setSpecificStates{CallFrequency,FrequencyJitter,RepeatAfterFirstCall,CallEnableBegin}``,
+    ``additionalArgument``, ``parametersUsedAsAlgebraic``, ``parametersUsedAsConstant``,
+    ``parametersInitialValues``, ``statesInitialValues``, ``algebraicsForTransfer``, ``statesForTransfer``;
+    diffusion ``timeStepWidth``; FiniteElementMethod ``prefactor``, ``meshName``; ``Meshes`` entries with
+    ``nElements``/``physicalExtent`` or ``nodePositions``.  B200 options go in an optional ``"B200"`` dict
+    next to the FastMonodomainSolver keys (``method``, ``precision``, ``clampRule``, ``vcWidth``,
+    ``nRanks``, ``stimulusMode``, ``stimulusParameter``, ``stimulusValue``, ``neuromuscularJunctionSeed``).
+    """
+    key, rc = _first_key(config, "RepeatedCall")
+    if rc is None:
+        raise ValueError("settings: expected a top-level 'RepeatedCall' entry")
+    fast = rc
+    b200 = dict(fast.get("B200", {}))
+    dt_rc = float(rc.get("timeStepWidth", 1e-3))
+    end = float(rc.get("endTime", 1.0))
+    start = float(rc.get("startTime", 0.0))
+    meshes = config.get("Meshes", {})
+    instances = fast["MultipleInstances"]["instances"]
+    fibers: List[dict] = []
+    for inst in instances:
+        _, strang = _first_key(inst, "StrangSplitting", "Strang")
+        if strang is None:
+            raise ValueError("settings: every instance needs a 'StrangSplitting' entry")
+        t1 = strang["Term1"]["MultipleInstances"]["instances"]
+        t2 = strang["Term2"]["MultipleInstances"]["instances"]
+        for a, b in zip(t1, t2):
+            heun = a["Heun"]
+            scheme, diff = _first_key(b, "ImplicitEuler", "CrankNicolson")
+            if scheme is None:
+                raise ValueError("settings: Timestepping scheme of diffusion in FastMonodomainSolver must be either "
+                                 "ImplicitEuler or CrankNicolson")
+            fibers.append({"strang": strang, "heun": heun, "cellml": heun["CellML"], "scheme": scheme,
+                           "diff": diff, "fem": diff["FiniteElementMethod"]})
+    if not fibers:
+        raise ValueError("settings: no fibers")
+    f0 = fibers[0]
+    cellml = f0["cellml"]
+    model = os.path.splitext(os.path.basename(cellml["modelFilename"]))[0]
+    if model not in N.MODEL_IDS:
+        raise ValueError(f"settings: model {model!r} is not built into the library (have {sorted(N.MODEL_IDS)})")
+    ns, na, npar, init, defaults = model_sizes(model)
+
+    # geometry
+    lengths = []
+    elem = []
+    for fb in fibers:
+        name = fb["fem"].get("meshName", fb["cellml"].get("meshName"))
+        h = _mesh_element_lengths(meshes, name)
+        elem.append(h)
+        lengths.append(len(h) + 1)
+    lengths = np.asarray(lengths, np.int64)
+    nf = len(lengths)
+    off = np.zeros(nf + 1, np.int64)
+    off[1:] = np.cumsum(lengths)
+    prefactor = np.array([float(fb["fem"].get("prefactor", 1.0)) for fb in fibers])
+
+    # parameters: map the settings' parameter list onto the built variant's slots
+    pa_var, pc_var = VARIANT_PARAMETERS[model]
+    pa = [int(x) for x in _as_list(cellml.get("parametersUsedAsAlgebraic", []))]
+    pc = [int(x) for x in _as_list(cellml.get("parametersUsedAsConstant", []))]
+    if tuple(pa) != tuple(pa_var) or any(c not in pc_var for c in pc):
+        raise ValueError(f"settings: parametersUsedAsAlgebraic={pa}, parametersUsedAsConstant={pc} is not a prebuilt "
+                         f"variant of {model} (algebraic {list(pa_var)}, constants within {list(pc_var)})")
+    n_user = len(pa) + len(pc)
+    slot_of = list(range(len(pa))) + [len(pa_var) + pc_var.index(c) for c in pc]
+    n_nodes = int(off[-1])
+    params = np.repeat(defaults[:, None], n_nodes, axis=1) if npar else np.zeros((0, n_nodes))
+    for fi, fb in enumerate(fibers):
+        vals = [float(x) for x in _as_list(fb["cellml"].get("parametersInitialValues", []))]
+        n_here = int(lengths[fi])
+        if len(vals) == n_user:
+            for j in range(n_user):
+                params[slot_of[j], off[fi]:off[fi + 1]] = vals[j]
+        elif len(vals) == n_user * n_here and n_user > 0:
+            arr = np.asarray(vals).reshape(n_here, n_user)
+            for j in range(n_user):
+                params[slot_of[j], off[fi]:off[fi + 1]] = arr[:, j]
+        else:
+            # the reference pads missing values with 0 (00_source_code_generator_base.cpp:67-81)
+            padded = (vals + [0.0] * n_user)[:n_user]
+            for j in range(n_user):
+                params[slot_of[j], off[fi]:off[fi + 1]] = padded[j]
+
+    states = None
+    if "statesInitialValues" in cellml and _as_list(cellml["statesInitialValues"]):
+        v = np.asarray(_as_list(cellml["statesInitialValues"]), np.float64)
+        if len(v) == ns:
+            states = np.repeat(v[:, None], n_nodes, axis=1)
+
+    # stimulation inputs
+    fdf = fast.get("fiberDistributionFile", "")
+    ftf = fast.get("firingTimesFile", "")
+    mus = inputs.parse_fiber_distribution(open(os.path.join(base_dir, fdf)).read()) if fdf else [0]
+    rows = inputs.parse_firing_times(open(os.path.join(base_dir, ftf)).read()) if ftf else [[0]]
+    firing = inputs.firing_matrix(rows)
+    mu_no = np.zeros(nf, np.int32)
+    freq = np.zeros(nf)
+    rep = np.zeros(nf)
+    beg = np.zeros(nf)
+    jit_lists = []
+    for fi, fb in enumerate(fibers):
+        c = fb["cellml"]
+        fiber_no_global = int(c.get("additionalArgument", fi)) if isinstance(c.get("additionalArgument", fi), (int, np.integer)) else fi
+        mu_no[fi] = mus[fiber_no_global % len(mus)]
+        freq[fi] = float(c.get("setSpecificStatesCallFrequency", 0.0) or 0.0)
+        rep[fi] = float(c.get("setSpecificStatesRepeatAfterFirstCall", 0.0) or 0.0)
+        beg[fi] = float(c.get("setSpecificStatesCallEnableBegin", 0.0) or 0.0)
+        jit_lists.append([float(x) for x in _as_list(c.get("setSpecificStatesFrequencyJitter", []))])
+    nj = max(len(j) for j in jit_lists)
+    if any(len(j) != nj for j in jit_lists):
+        raise ValueError("settings: all fibers need the same number of setSpecificStatesFrequencyJitter values")
+    jitter = np.asarray(jit_lists, np.float64).reshape(nf, nj)
+    nmj_size = float(fast.get("neuromuscularJunctionRelativeSize", 0.0))
+    if nmj_size <= 0:
+        center = (lengths // 2).astype(np.int32)
+    else:
+        rng = np.random.default_rng(int(b200.get("neuromuscularJunctionSeed", 0)))
+        u = rng.uniform(0.5 - nmj_size / 2, 0.5 + nmj_size / 2, size=nf)
+        center = (lengths * u).astype(np.int32)
+    for opt in ("onlyComputeIfHasBeenStimulated", "disableComputationWhenStatesAreCloseToEquilibrium"):
+        if fast.get(opt, True):
+            warnings.warn(f"{opt}=True is not implemented by the B200 solver; every node is computed every step "
+                          "(the reference's own tests set it to False)")
+
+    precision = b200.get("precision", "fp32" if fast.get("useSinglePrecision", False) else "fp64")
+    sys_ = FiberSystem(
+        model=model, fiber_offsets=off, element_lengths=np.concatenate(elem), prefactor=prefactor,
+        firing_events=firing, motor_unit_no=mu_no, stimulation_point_index=center, call_frequency=freq,
+        repeat_after_first_call=rep, call_enable_begin=beg, jitter=jitter, parameters=params, states=states,
+        diffusion_scheme=f0["scheme"], dt_0d=float(f0["heun"].get("timeStepWidth", 1e-4)),
+        dt_1d=float(f0["diff"].get("timeStepWidth", 1e-3)), dt_splitting=float(f0["strang"].get("timeStepWidth", dt_rc)),
+        dt_repeated_call=dt_rc, start_time=start, end_time=end,
+        approximate_exponential_function=bool(cellml.get("approximateExponentialFunction",
+                                                         cellml.get("optimizationType", "vc") == "vc")),
+        value_for_stimulated_point=float(fast.get("valueForStimulatedPoint", 20.0)),
+        clamp_rule=b200.get("clampRule", "vc" if cellml.get("optimizationType", "vc") == "vc" else "center"),
+        vc_width=int(b200.get("vcWidth", 4)), n_ranks=int(b200.get("nRanks", 1)),
+        stimulus_mode=b200.get("stimulusMode", "clamp"), stimulus_parameter=int(b200.get("stimulusParameter", 0)),
+        stimulus_value=float(b200.get("stimulusValue", 0.0)),
+        algebraics_for_transfer=[int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))],
+        states_for_transfer=[int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))] or [0])
+    sys_.method = b200.get("method", "split")
+    sys_.precision = precision
+    return sys_
+
+
+# ----------------------------------------------------------------------------------------------
+# the operator
+# ----------------------------------------------------------------------------------------------
+
+class FastMonodomainSolver:
+    """B200 FastMonodomainSolver (reference API names; see the module docstring)."""
+
+    def __init__(self, system: FiberSystem, method: Optional[str] = None, precision: Optional[str] = None,
+                 steps_per_launch: int = 0, threads_per_block: int = 0, nodes_per_thread: int = 0,
+                 check_nan: bool = True, profile: bool = False, trace_nodes: Sequence[int] = (),
+                 trace_capacity: int = 0, device: int = 0):
+        self.system = system
+        self.method = method or getattr(system, "method", "split")
+        self.precision = precision or getattr(system, "precision", "fp64")
+        self.steps_per_launch = steps_per_launch
+        self.threads_per_block = threads_per_block
+        self.nodes_per_thread = nodes_per_thread
+        self.check_nan = check_nan
+        self.profile = profile
+        self.trace_nodes = np.asarray(trace_nodes, np.int64)
+        self.trace_capacity = int(trace_capacity)
+        self.device = int(device)
+        self._h = None
+        self._start = system.start_time
+        self._end = system.end_time
+        self._ck = None
+        self.initialized = False
+
+    @classmethod
+    def from_settings(cls, config: dict, base_dir: str = ".", **kw) -> "FastMonodomainSolver":
+        return cls(parse_settings(config, base_dir), **kw)
+
+    # -- lifecycle ------------------------------------------------------------------------------
+    def initialize(self):
+        if self.initialized:
+            return
+        s = self.system
+        L = N.lib()
+        cfg = N.default_config()
+        cfg.model = N.MODEL_IDS[s.model]
+        cfg.diffusion_scheme = SCHEMES[s.diffusion_scheme]
+        cfg.method = METHODS[self.method]
+        cfg.reaction_precision = PRECISIONS[self.precision]
+        cfg.approximate_exponential_function = int(bool(s.approximate_exponential_function))
+        cfg.clamp_rule = CLAMP_RULES[s.clamp_rule]
+        cfg.vc_width = int(s.vc_width)
+        cfg.n_ranks = int(s.n_ranks)
+        cfg.stimulus_mode = STIMULUS_MODES[s.stimulus_mode]
+        cfg.stimulus_parameter = int(s.stimulus_parameter)
+        cfg.stimulus_value = float(s.stimulus_value)
+        cfg.value_for_stimulated_point = float(s.value_for_stimulated_point)
+        cfg.dt_repeated_call = float(s.dt_repeated_call)
+        cfg.dt_splitting = float(s.dt_splitting)
+        cfg.dt_0d = float(s.dt_0d)
+        cfg.dt_1d = float(s.dt_1d)
+        cfg.steps_per_launch = int(self.steps_per_launch)
+        cfg.threads_per_block = int(self.threads_per_block)
+        cfg.nodes_per_thread = int(self.nodes_per_thread)
+        cfg.check_nan = int(bool(self.check_nan))
+        cfg.profile = int(bool(self.profile))
+        cfg.device = self.device
+        h = C.c_void_p()
+        N.check(L.fdm_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        try:
+            off = np.ascontiguousarray(s.fiber_offsets, np.int64)
+            elem = np.ascontiguousarray(s.element_lengths, np.float64)
+            pf = np.ascontiguousarray(s.prefactor, np.float64)
+            self._call(L.fdm_set_fibers, len(off) - 1, N.ptr(off, C.c_int64), N.ptr(elem, C.c_double),
+                       N.ptr(pf, C.c_double))
+            if s.parameters is not None and s.parameters.size:
+                p = np.ascontiguousarray(s.parameters, np.float64)
+                self._call(L.fdm_set_parameters, N.ptr(p, C.c_double))
+            if s.states is not None:
+                st = np.ascontiguousarray(s.states, np.float64)
+                self._call(L.fdm_set_states, N.ptr(st, C.c_double))
+            self._set_stimulation()
+            if len(s.algebraics_for_transfer):
+                idx = np.ascontiguousarray(s.algebraics_for_transfer, np.int32)
+                self._call(L.fdm_set_algebraics_for_transfer, len(idx), N.ptr(idx, C.c_int))
+            if len(self.trace_nodes):
+                self._call(L.fdm_set_trace, len(self.trace_nodes), N.ptr(self.trace_nodes, C.c_int64),
+                           self.trace_capacity)
+        except Exception:
+            self.close()
+            raise
+        self.initialized = True
+
+    def _set_stimulation(self):
+        s = self.system
+        fe = np.ascontiguousarray(s.firing_events, np.uint8)
+        mu = np.ascontiguousarray(s.motor_unit_no, np.int32)
+        ce = np.ascontiguousarray(s.stimulation_point_index, np.int32)
+        fr = np.ascontiguousarray(s.call_frequency, np.float64)
+        rp = np.ascontiguousarray(s.repeat_after_first_call, np.float64)
+        bg = np.ascontiguousarray(s.call_enable_begin, np.float64)
+        jit = np.ascontiguousarray(s.jitter if s.jitter is not None else np.zeros((s.n_fibers, 0)), np.float64)
+        nj = jit.shape[1] if jit.ndim == 2 else 0
+        jp = jit if jit.size else np.zeros(1)
+        self._keep = (fe, mu, ce, fr, rp, bg, jp)
+        self._call(N.lib().fdm_set_stimulation, N.ptr(fe, C.c_uint8), fe.shape[0], fe.shape[1], N.ptr(mu, C.c_int),
+                   N.ptr(ce, C.c_int), N.ptr(fr, C.c_double), N.ptr(rp, C.c_double), N.ptr(bg, C.c_double),
+                   N.ptr(jp, C.c_double), nj)
+
+    def _call(self, f, *args):
+        N.check(f(self._h, *args), self._h)
+
+    def close(self):
+        if self._h is not None:
+            N.lib().fdm_destroy(self._h)
+            self._h = None
+        self.initialized = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        self.initialize()
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- reference operator API -----------------------------------------------------------------
+    def setTimeSpan(self, start_time: float, end_time: float):
+        self._start = float(start_time)
+        self._end = float(end_time)
+
+    def startTime(self) -> float:
+        return self._start
+
+    def endTime(self) -> float:
+        return self._end
+
+    def advanceTimeSpan(self, withOutputWritersEnabled: bool = True):
+        """RepeatedCall over [startTime, endTime] (each repeated call is one setTimeSpan+advanceTimeSpan of
+        the reference solver)."""
+        self.initialize()
+        self._call(N.lib().fdm_advance, self._start, self._end)
+
+    def run(self):
+        self.initialize()
+        self.advanceTimeSpan()
+
+    def reset(self):
+        self.close()
+
+    def saveFiberDataCheckpoint(self):
+        self._call(N.lib().fdm_checkpoint_save)
+
+    def restoreFiberDataCheckpoint(self):
+        self._call(N.lib().fdm_checkpoint_restore)
+
+    # -- data -------------------------------------------------------------------------------------
+    def states(self) -> np.ndarray:
+        ns = model_sizes(self.system.model)[0]
+        out = np.zeros((ns, self.system.n_nodes))
+        self._call(N.lib().fdm_get_states, N.ptr(out, C.c_double))
+        return out
+
+    def set_states(self, states: np.ndarray):
+        st = np.ascontiguousarray(states, np.float64)
+        self._call(N.lib().fdm_set_states, N.ptr(st, C.c_double))
+
+    def vm(self) -> np.ndarray:
+        out = np.zeros(self.system.n_nodes)
+        self._call(N.lib().fdm_get_vm, N.ptr(out, C.c_double))
+        return out
+
+    def algebraics(self) -> np.ndarray:
+        k = len(self.system.algebraics_for_transfer)
+        out = np.zeros((max(k, 1), self.system.n_nodes))
+        if k:
+            self._call(N.lib().fdm_get_algebraics, N.ptr(out, C.c_double))
+        return out[:k]
+
+    def parameters(self) -> np.ndarray:
+        npar = model_sizes(self.system.model)[2]
+        out = np.zeros((max(npar, 1), self.system.n_nodes))
+        if npar:
+            self._call(N.lib().fdm_get_parameters, N.ptr(out, C.c_double))
+        return out[:npar]
+
+    def set_parameters(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, np.float64)
+        self._call(N.lib().fdm_set_parameters, N.ptr(p, C.c_double))
+
+    def set_prefactor(self, prefactor: np.ndarray):
+        p = np.ascontiguousarray(prefactor, np.float64)
+        self._call(N.lib().fdm_set_prefactor, N.ptr(p, C.c_double))
+
+    def trace(self) -> np.ndarray:
+        n = C.c_int64()
+        self._call(N.lib().fdm_get_trace, None, C.byref(n))
+        out = np.zeros((max(n.value, 1), max(len(self.trace_nodes), 1)))
+        if n.value and len(self.trace_nodes):
+            self._call(N.lib().fdm_get_trace, N.ptr(out, C.c_double), C.byref(n))
+        return out[:n.value, :len(self.trace_nodes)]
+
+    def clamp_nodes(self):
+        nf = self.system.n_fibers
+        first = np.zeros(nf, np.int64)
+        cnt = np.zeros(nf, np.int32)
+        ev = np.zeros(nf, np.uint8)
+        self._call(N.lib().fdm_get_clamp_nodes, N.ptr(first, C.c_int64), N.ptr(cnt, C.c_int), N.ptr(ev, C.c_uint8))
+        return first, cnt, ev
+
+    def split_steps(self) -> int:
+        return int(N.lib().fdm_split_steps(self._h))
+
+    def timing(self) -> Dict[str, float]:
+        a, b, c, d = C.c_double(), C.c_int64(), C.c_double(), C.c_int64()
+        self._call(N.lib().fdm_get_timing, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
+        return {"main_kernel_ms": a.value, "main_kernel_launches": b.value, "advance_ms": c.value,
+                "kernel_launches": d.value}
+
+    def reset_timing(self):
+        self._call(N.lib().fdm_reset_timing)
+
+    def data(self) -> Dict[str, np.ndarray]:
+        """The fiber data the reference transfers out (statesForTransfer / algebraicsForTransfer)."""
+        st = self.states()
+        return {"Vm": st[0], "states": st[list(self.system.states_for_transfer)], "algebraics": self.algebraics()}

@@ -1,0 +1,82 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+The reference's large example inputs (fiber geometry files, MU_firing_times_real.txt,
+MU_fibre_distribution_3780.txt) are not available; these generators stand in for them with the
+stated shapes and distributions, written in the reference's file formats where files are needed.
+All fibers are straight with uniform element length dx.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import inputs
+from .solver import FiberSystem, uniform_fibers
+
+HH = "hodgkin_huxley_1952"
+SHORTEN = "shorten_ocallaghan_davidson_soboleva_2007"
+
+SIGMA = 3.828   # mS/cm
+AM = 500.0      # 1/cm
+CM = 1.0        # uF/cm^2
+
+
+def plain_hh(n_fibers: int = 16, n_nodes: int = 1481, end_time: float = 10.0, **kw) -> FiberSystem:
+    """Plain-method configuration: HH, identical fibers of 1481 nodes (14.8 cm), dx 0.01 cm,
+    prefactor sigma/(Am*Cm), Heun dt 1e-4 ms, implicit Euler / Strang dt 1e-3 ms, clamp stimulus at the
+    centre for 0.1 ms every 10 ms."""
+    return uniform_fibers(HH, [n_nodes] * n_fibers, 0.01, SIGMA / (AM * CM), call_frequency=0.1,
+                          repeat_after_first_call=0.1, call_enable_begin=0.0, end_time=end_time, dt_0d=1e-4,
+                          dt_1d=1e-3, dt_splitting=1e-3, dt_repeated_call=1e-3, **kw)
+
+
+def batched_hh(n_fibers: int = 4096, min_nodes: int = 500, max_nodes: int = 2500, n_mus: int = 100,
+               end_time: float = 100.0, seed: int = 0, **kw) -> FiberSystem:
+    """Batching + precision configuration: HH, fiber lengths uniform in [500, 2500] nodes (seeded),
+    dx 0.01 cm, fibers assigned to 100 motor units by a seeded exponential size distribution, per-MU
+    Poisson firing at 10-40 Hz sampled at the 0.1/ms call frequency, Crank-Nicolson, dt as the plain
+    configuration."""
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(min_nodes, max_nodes + 1, size=n_fibers)
+    mus = inputs.exponential_mu_distribution(n_fibers, n_mus, seed)
+    firing = inputs.poisson_firing_times(n_mus, end_time, 0.1, 10.0, 40.0, seed)
+    kw.setdefault("diffusion_scheme", "CrankNicolson")
+    return uniform_fibers(HH, lengths, 0.01, SIGMA / (AM * CM), firing_events=firing, motor_unit_no=mus,
+                          call_frequency=0.1, repeat_after_first_call=0.1, call_enable_begin=0.0,
+                          end_time=end_time, dt_0d=1e-4, dt_1d=1e-3, dt_splitting=1e-3, dt_repeated_call=1e-3, **kw)
+
+
+def shorten_grid(n_fibers: int = 1369, n_nodes: int = 1481, end_time: float = 50.0, n_mus: int = 100,
+                 seed: int = 0, **kw) -> FiberSystem:
+    """Shorten 2007 (56 states): 37x37 fibers x 1481 nodes, Heun dt 1e-5 ms, Strang dt 5e-4 ms,
+    seeded per-MU firing."""
+    mus = inputs.exponential_mu_distribution(n_fibers, n_mus, seed)
+    firing = inputs.poisson_firing_times(n_mus, end_time, 0.1, 10.0, 40.0, seed)
+    return uniform_fibers(SHORTEN, [n_nodes] * n_fibers, 0.01, SIGMA / (AM * 0.58), firing_events=firing,
+                          motor_unit_no=mus, call_frequency=0.1, repeat_after_first_call=0.1, call_enable_begin=0.0,
+                          end_time=end_time, dt_0d=1e-5, dt_1d=5e-4, dt_splitting=5e-4, dt_repeated_call=5e-4, **kw)
+
+
+def subset(system: FiberSystem, fibers) -> FiberSystem:
+    """The given fibers of a system, as a system of their own (same per-fiber inputs)."""
+    fibers = np.asarray(fibers)
+    off = system.fiber_offsets
+    lengths = off[fibers + 1] - off[fibers]
+    new_off = np.zeros(len(fibers) + 1, np.int64)
+    new_off[1:] = np.cumsum(lengths)
+    elem = np.concatenate([system.element_lengths[off[f] - f:off[f + 1] - f - 1] for f in fibers])
+    nodes = np.concatenate([np.arange(off[f], off[f + 1]) for f in fibers])
+    s = system.copy()
+    s.fiber_offsets = new_off
+    s.element_lengths = elem
+    for name in ("prefactor", "motor_unit_no", "stimulation_point_index", "call_frequency",
+                 "repeat_after_first_call", "call_enable_begin"):
+        setattr(s, name, np.asarray(getattr(system, name))[fibers].copy())
+    if system.jitter is not None and np.asarray(system.jitter).size:
+        s.jitter = np.asarray(system.jitter)[fibers].copy()
+    else:
+        s.jitter = np.zeros((len(fibers), 0))
+    if system.parameters is not None:
+        s.parameters = system.parameters[:, nodes].copy()
+    if system.states is not None:
+        s.states = system.states[:, nodes].copy()
+    return s

@@ -1,0 +1,117 @@
+"""CellML parser / code generator."""
+import glob
+import os
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import helpers as H
+from opendihu_b200 import cellml
+from oracle import oracle as O
+
+ROOT = H.ROOT
+REF_INPUT = os.path.join(os.environ.get("OPENDIHU_REFERENCE", "/root/reference"), "testing/unit_testing/input")
+
+
+def test_expression_precedence():
+    e = cellml.parse_expression("a0 - 1 > 0 && 2 < 3 ? 1 : 0".replace("a0", "STATES[0]"))
+    assert e[0] == "tern" and e[1][0] == "bin" and e[1][1] == "&&"
+    assert cellml.eval_expr(cellml.parse_expression("2 - 3 - 4"), {}) == -5
+    assert cellml.eval_expr(cellml.parse_expression("2 / 4 * 8"), {}) == 4
+    assert cellml.eval_expr(cellml.parse_expression("- 2 * 3 + 1"), {}) == -5
+    assert cellml.eval_expr(cellml.parse_expression("1 + - 2"), {}) == -1
+    env = {"T": 0.25, "S": [], "C": [], "A": [], "R": []}
+    e = cellml.parse_expression("VOI>=0.00000&&VOI<0.500000 ? 150.000 : 0.00000")
+    assert cellml.eval_expr(e, env) == 150.0
+
+
+def test_integer_exponent_detection():
+    # reference rule (03_generator_vc.cpp:68-117): digits/sign/dot only and atoi != 0
+    f = lambda t: cellml._int_exponent(cellml.parse_expression(t))
+    assert f("3.00000") == 3
+    assert f("- 1.00000") == -1
+    assert f("0.500000") is None
+    assert f("CONSTANTS[1]") is None
+
+
+def test_integer_power_helpers_multiplication_order():
+    x = 1.1
+    assert cellml._int_pow_value(x, 2) == x * x
+    assert cellml._int_pow_value(x, 3) == x * (x * x)
+    assert cellml._int_pow_value(x, 4) == (x * x) * (x * x)
+    assert cellml._int_pow_value(x, -1) == 1.0 / x
+
+
+def test_parameter_substitution():
+    model = cellml.Model(name="t", source="t.c", n_states=1, n_algebraics=2, n_constants=2, states_initial=[0.0],
+                         constants=[1.0, 2.0], constant_lines=[],
+                         lines=[("A", 0, cellml.parse_expression("CONSTANTS[1]*STATES[0]")),
+                                ("A", 1, cellml.parse_expression("ALGEBRAIC[0]+CONSTANTS[0]")),
+                                ("R", 0, cellml.parse_expression("ALGEBRAIC[1]"))])
+    lines = cellml.substitute_parameters(model, [0], [1])
+    assert len(lines) == 2  # the line assigning ALGEBRAIC[0] is dropped
+    assert lines[0][2][2] == ("var", "P", 0)  # ALGEBRAIC[0] -> PARAMS[0]
+    lines = cellml.substitute_parameters(model, [], [1])
+    assert lines[0][2][2] == ("var", "P", 0)  # CONSTANTS[1] -> PARAMS[0]
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_INPUT), reason="reference checkout not present")
+def test_generated_sources_are_current(tmp_path):
+    cuda_dir = tmp_path / "cuda"
+    c_dir = tmp_path / "c"
+    cuda_dir.mkdir()
+    c_dir.mkdir()
+    cellml.generate_all(REF_INPUT, str(cuda_dir), str(c_dir))
+    for d, committed in ((cuda_dir, os.path.join(ROOT, "opendihu_b200/csrc/generated")),
+                         (c_dir, os.path.join(ROOT, "oracle/generated"))):
+        for f in os.listdir(d):
+            assert open(os.path.join(d, f)).read() == open(os.path.join(committed, f)).read(), f
+
+
+def _ref_lib(name):
+    p = os.path.join(ROOT, "oracle", "_ref", f"libref_{name}.so")
+    if not os.path.exists(p):
+        pytest.skip("oracle/_ref not built (make -C oracle ref needs the reference checkout)")
+    L = C.CDLL(p)
+    L.computeRates.argtypes = [C.c_double] + [C.POINTER(C.c_double)] * 4
+    L.initConsts.argtypes = [C.POINTER(C.c_double)] * 3
+    return L
+
+
+@pytest.mark.parametrize("model,params_alg,params_const,n_const", [
+    (H.HH, [], [2, 3, 4], 9), (H.SHORTEN, [32], [65], 105)])
+def test_generated_rhs_matches_reference_model_file(model, params_alg, params_const, n_const):
+    """generated C right-hand side == the reference's own computeRates (compiled in oracle/_ref)."""
+    L = _ref_lib(model)
+    ns, na, npar, init = O.model_info(model)
+    consts = np.zeros(n_const)
+    rates0 = np.zeros(ns)
+    states0 = np.zeros(ns)
+    L.initConsts(consts.ctypes.data_as(C.POINTER(C.c_double)), rates0.ctypes.data_as(C.POINTER(C.c_double)),
+                 states0.ctypes.data_as(C.POINTER(C.c_double)))
+    np.testing.assert_array_equal(states0, init)
+    rng = np.random.default_rng(0)
+    for trial in range(20):
+        st = init * (1 + 0.05 * rng.standard_normal(ns))
+        st[0] = init[0] + 30 * rng.standard_normal()
+        t = 0.3 if trial % 2 else 60.2
+        # parameters: constant parameters at random values, algebraic parameters at a fixed value
+        p_const = [consts[c] * (1 + 0.1 * rng.standard_normal()) for c in params_const]
+        p_alg = [12.5 for _ in params_alg]
+        c2 = consts.copy()
+        for c, v in zip(params_const, p_const):
+            c2[c] = v
+        r_ref = np.zeros(ns)
+        a_ref = np.zeros(max(na, 1))
+        L.computeRates(t, c2.ctypes.data_as(C.POINTER(C.c_double)), r_ref.ctypes.data_as(C.POINTER(C.c_double)),
+                       st.ctypes.data_as(C.POINTER(C.c_double)), a_ref.ctypes.data_as(C.POINTER(C.c_double)))
+        r, a = O.rates(model, st, np.array(p_alg + p_const), t=t)
+        if params_alg:
+            # the reference computes the algebraic parameter from VOI; the generated code reads the
+            # parameter instead, so compare against the reference evaluated with that value forced in:
+            # only the lines not depending on it are expected to agree exactly
+            dep = np.abs(r - r_ref) > 1e-12 * (1 + np.abs(r_ref))
+            assert dep.sum() <= 2, np.nonzero(dep)
+        else:
+            np.testing.assert_allclose(r, r_ref, rtol=1e-14, atol=1e-300)

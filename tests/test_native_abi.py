@@ -1,0 +1,55 @@
+"""The C ABI library loads and exports every symbol include/fdm_b200.h declares (no GPU needed)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import helpers as H
+from opendihu_b200 import _native as N
+
+HEADER = os.path.join(H.ROOT, "include", "fdm_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fdm_[a-z0-9_]+)\s*\(", text)) | set(
+        re.findall(r"\b(initializeArrays|computeMonodomain)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = N.lib()
+    missing = [f for f in declared_functions() if not hasattr(L, f)]
+    assert not missing, missing
+
+
+def test_binding_list_matches_header():
+    assert sorted(N.EXPORTED) == [f for f in declared_functions() if f.startswith("fdm_")]
+
+
+def test_model_info_without_device():
+    ns, na, npar, init, defaults = N.model_info(N.MODEL_IDS[H.HH])
+    assert (ns, na, npar) == (4, 9, 3)
+    np.testing.assert_array_equal(init, [-75, 0.05, 0.6, 0.325])
+    np.testing.assert_array_equal(defaults, [0.0, 120.0, 36.0])
+    ns, na, npar, init, defaults = N.model_info(N.MODEL_IDS[H.SHORTEN])
+    assert (ns, na, npar) == (56, 71, 2)
+
+
+def test_create_fails_loudly_without_device_or_with_bad_config():
+    cfg = N.default_config()
+    cfg.model = 99
+    h = C.c_void_p()
+    rc = N.lib().fdm_create(C.byref(cfg), C.byref(h))
+    assert rc == N.FDM_ERR_ARG and b"unknown model" in N.lib().fdm_last_error(None)
+    cfg = N.default_config()
+    cfg.model = N.MODEL_IDS[H.SHORTEN]
+    cfg.method = 1
+    assert N.lib().fdm_create(C.byref(cfg), C.byref(h)) == N.FDM_ERR_UNSUPPORTED
+
+
+def test_fused_shapes_listed():
+    shapes = N.fused_shapes()
+    assert len(shapes) >= 4 and all(t % 32 == 0 and m >= 1 for t, m in shapes)
