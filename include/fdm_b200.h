@@ -147,6 +147,15 @@ int fdm_reset_timing(fdm_solver *s);
 int fdm_checkpoint_save(fdm_solver *s);
 int fdm_checkpoint_restore(fdm_solver *s);
 
+/* One diffusion solve of compute1D (fast_monodomain_solver_compute.tpp:256-507) for every fiber, as a
+ * standalone operator on DEVICE arrays of the current CUDA device: d_fiber_offsets[n_fibers+1] (node offsets),
+ * d_element_lengths (each fiber's n_f-1 lengths, concatenated), d_prefactor[n_fibers], d_vm[n_nodes] (in: u,
+ * out: u+).  diffusion_scheme is FDM_IMPLICIT_EULER or FDM_CRANK_NICOLSON, dt the diffusion step width.
+ * Scratch memory (7 doubles per node) is allocated by the library with cudaMalloc and kept for later calls.
+ * stream is a cudaStream_t (NULL: the legacy default stream); the call returns after the solve. */
+int fdm_diffusion_solve(int n_fibers, int64_t n_nodes, const int64_t *d_fiber_offsets, const double *d_element_lengths,
+                        const double *d_prefactor, double dt, int diffusion_scheme, double *d_vm, void *stream);
+
 /* number of the fused-kernel shapes built into the library and their (threads, nodes per thread) */
 int fdm_fused_shapes(int *threads, int *nodes_per_thread, int capacity);
 

@@ -113,7 +113,7 @@ struct fdm_solver {
 
   // device buffers
   DevBuf<double> vm, coef, scratch, prefactor_d, elem_d, alg_out, trace;
-  DevBuf<unsigned char> states, params;
+  DevBuf<unsigned char> states, states_lo, params;
   DevBuf<int64_t> off_d, elem_off_d;
   DevBuf<int> clamp_fiber, bin_start_d, bin_fibers_d, alg_idx, trace_slot, nonfinite;
   DevBuf<uint8_t> firing, evaluated_d, hbs;
@@ -130,7 +130,7 @@ struct fdm_solver {
 
   // checkpoint
   DevBuf<double> ck_vm, ck_last, ck_jit;
-  DevBuf<unsigned char> ck_states;
+  DevBuf<unsigned char> ck_states, ck_states_lo;
   DevBuf<int> ck_jidx;
   DevBuf<uint8_t> ck_hbs;
   bool ck_valid = false;
@@ -331,8 +331,10 @@ extern "C" int fdm_destroy(fdm_solver* s)
                   &s->ck_jit})
     b->release();
   s->states.release();
+  s->states_lo.release();
   s->params.release();
   s->ck_states.release();
+  s->ck_states_lo.release();
   s->off_d.release();
   s->elem_off_d.release();
   for (auto* b : {&s->clamp_fiber, &s->bin_start_d, &s->bin_fibers_d, &s->alg_idx, &s->trace_slot, &s->nonfinite,
@@ -472,6 +474,8 @@ extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_
   const int64_t N = std::max<int64_t>(s->n_nodes, 1);
   FDM_CUDA(s->vm.alloc(N));
   FDM_CUDA(s->states.alloc((size_t)N * std::max(NS - 1, 1) * s->real_bytes));
+  if (s->real_bytes == 4)
+    FDM_CUDA(s->states_lo.alloc((size_t)N * std::max(NS - 1, 1) * 4));
   FDM_CUDA(s->params.alloc((size_t)N * std::max(NP, 1) * s->real_bytes));
   FDM_CUDA(s->coef.alloc((size_t)N * 6));
   if (s->cfg.method == FDM_METHOD_SPLIT)
@@ -570,10 +574,15 @@ extern "C" int fdm_set_states(fdm_solver* s, const double* states)
       FDM_CUDA(cudaMemcpyAsync(s->states.p, states + N, sizeof(double) * N * (NS - 1), cudaMemcpyHostToDevice,
                                s->stream));
     } else {
-      std::vector<float> tmp((size_t)N * (NS - 1));
-      for (size_t i = 0; i < tmp.size(); i++)
-        tmp[i] = (float)states[N + i];
-      FDM_CUDA(cudaMemcpyAsync(s->states.p, tmp.data(), sizeof(float) * tmp.size(), cudaMemcpyHostToDevice,
+      // each state as an FP32 pair (value, residual) whose sum reproduces the double
+      std::vector<float> hi((size_t)N * (NS - 1)), lo((size_t)N * (NS - 1));
+      for (size_t i = 0; i < hi.size(); i++) {
+        hi[i] = (float)states[N + i];
+        lo[i] = (float)(states[N + i] - (double)hi[i]);
+      }
+      FDM_CUDA(cudaMemcpyAsync(s->states.p, hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice,
+                               s->stream));
+      FDM_CUDA(cudaMemcpyAsync(s->states_lo.p, lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice,
                                s->stream));
       FDM_CUDA(cudaStreamSynchronize(s->stream));
     }
@@ -598,12 +607,14 @@ extern "C" int fdm_get_states(fdm_solver* s, double* states)
                                s->stream));
       FDM_CUDA(cudaStreamSynchronize(s->stream));
     } else {
-      std::vector<float> tmp((size_t)N * (NS - 1));
-      FDM_CUDA(cudaMemcpyAsync(tmp.data(), s->states.p, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost,
+      std::vector<float> hi((size_t)N * (NS - 1)), lo((size_t)N * (NS - 1));
+      FDM_CUDA(cudaMemcpyAsync(hi.data(), s->states.p, sizeof(float) * hi.size(), cudaMemcpyDeviceToHost,
+                               s->stream));
+      FDM_CUDA(cudaMemcpyAsync(lo.data(), s->states_lo.p, sizeof(float) * lo.size(), cudaMemcpyDeviceToHost,
                                s->stream));
       FDM_CUDA(cudaStreamSynchronize(s->stream));
-      for (size_t i = 0; i < tmp.size(); i++)
-        states[N + i] = (double)tmp[i];
+      for (size_t i = 0; i < hi.size(); i++)
+        states[N + i] = (double)hi[i] + (double)lo[i];
     }
   }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
@@ -928,7 +939,7 @@ static int ensure_coefficients(fdm_solver* s, double dt1)
   // the factorization is reused while dt1D stays within a relative 1e-12 of the factorized value.
   if (s->coef_valid && std::fabs(dt1 - s->coef_dt) <= 1e-12 * std::fabs(s->coef_dt))
     return FDM_OK;
-  FDM_CUDA(launch_coefficients(s->n_fibers, s->off_d.p, s->elem_off_d.p, s->elem_d.p, s->prefactor_d.p, dt1,
+  FDM_CUDA(launch_coefficients(s->n_fibers, s->off_d.p, s->elem_d.p, s->prefactor_d.p, dt1,
                                s->cfg.diffusion_scheme == FDM_IMPLICIT_EULER, s->coef.p, s->n_nodes, s->stream));
   s->launches++;
   s->coef_dt = dt1;
@@ -994,6 +1005,7 @@ static int run_window(fdm_solver* s, int n_steps, double dt1, bool store_alg)
     fa.stride = s->n_nodes;
     fa.vm = s->vm.p;
     fa.states = s->states.p;
+    fa.states_lo = s->states_lo.p;
     fa.params = s->params.p;
     fa.coef = s->coef.p;
     fa.clamp_fiber = s->clamp_fiber.p;
@@ -1033,6 +1045,7 @@ static int run_window(fdm_solver* s, int n_steps, double dt1, bool store_alg)
   ra.stride = s->n_nodes;
   ra.vm = s->vm.p;
   ra.states = s->states.p;
+  ra.states_lo = s->states_lo.p;
   ra.params = s->params.p;
   ra.clamp_fiber = s->clamp_fiber.p;
   ra.flags = s->flags.p;
@@ -1212,6 +1225,11 @@ extern "C" int fdm_checkpoint_save(fdm_solver* s)
     if (NS > 1)
       FDM_CUDA(cudaMemcpyAsync(s->ck_states.p, s->states.p, (size_t)N * (NS - 1) * s->real_bytes,
                                cudaMemcpyDeviceToDevice, s->stream));
+    if (NS > 1 && s->real_bytes == 4) {
+      FDM_CUDA(s->ck_states_lo.alloc((size_t)N * (NS - 1) * 4));
+      FDM_CUDA(cudaMemcpyAsync(s->ck_states_lo.p, s->states_lo.p, (size_t)N * (NS - 1) * 4,
+                               cudaMemcpyDeviceToDevice, s->stream));
+    }
   }
   if (nf > 0 && s->stimulation_set) {
     FDM_CUDA(cudaMemcpyAsync(s->ck_last.p, s->last_check.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
@@ -1242,6 +1260,9 @@ extern "C" int fdm_checkpoint_restore(fdm_solver* s)
     if (NS > 1)
       FDM_CUDA(cudaMemcpyAsync(s->states.p, s->ck_states.p, (size_t)N * (NS - 1) * s->real_bytes,
                                cudaMemcpyDeviceToDevice, s->stream));
+    if (NS > 1 && s->real_bytes == 4)
+      FDM_CUDA(cudaMemcpyAsync(s->states_lo.p, s->ck_states_lo.p, (size_t)N * (NS - 1) * 4,
+                               cudaMemcpyDeviceToDevice, s->stream));
   }
   if (nf > 0 && s->stimulation_set) {
     FDM_CUDA(cudaMemcpyAsync(s->last_check.p, s->ck_last.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
@@ -1255,5 +1276,55 @@ extern "C" int fdm_checkpoint_restore(fdm_solver* s)
   s->diff = s->ck_diff;
   s->tss_init = s->ck_tss_init;
   s->split_no = s->ck_split;
+  return FDM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// compute1D as a standalone operator on device arrays
+// ---------------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+struct ScratchPool {
+  std::mutex mu;
+  double* p[64] = {};
+  size_t n[64] = {};
+};
+ScratchPool g_scratch;
+} // namespace
+
+extern "C" int fdm_diffusion_solve(int n_fibers, int64_t n_nodes, const int64_t* d_fiber_offsets,
+                                   const double* d_element_lengths, const double* d_prefactor, double dt,
+                                   int diffusion_scheme, double* d_vm, void* stream)
+{
+  fdm_solver* s = nullptr;
+  if (n_fibers < 0 || n_nodes < 0 || (n_fibers > 0 && (!d_fiber_offsets || !d_element_lengths || !d_prefactor || !d_vm)))
+    return fail(s, FDM_ERR_ARG, "fdm_diffusion_solve: bad argument");
+  if (!(dt > 0) || (diffusion_scheme != FDM_IMPLICIT_EULER && diffusion_scheme != FDM_CRANK_NICOLSON))
+    return fail(s, FDM_ERR_ARG, "fdm_diffusion_solve: dt must be positive and the scheme IE or CN");
+  if (n_fibers == 0)
+    return FDM_OK;
+  int dev = 0;
+  FDM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64)
+    return fail(s, FDM_ERR_ARG, "fdm_diffusion_solve: device ordinal beyond 63");
+  cudaStream_t st = (cudaStream_t)stream;
+  std::lock_guard<std::mutex> lock(g_scratch.mu);
+  // scratch: 6 factorization doubles + 1 forward-sweep double per node, allocated by the library
+  const size_t need = (size_t)7 * (size_t)n_nodes;
+  if (g_scratch.n[dev] < need) {
+    if (g_scratch.p[dev])
+      FDM_CUDA(cudaFree(g_scratch.p[dev]));
+    g_scratch.p[dev] = nullptr;
+    g_scratch.n[dev] = 0;
+    FDM_CUDA(cudaMalloc((void**)&g_scratch.p[dev], need * sizeof(double)));
+    g_scratch.n[dev] = need;
+  }
+  double* coef = g_scratch.p[dev];
+  double* fwd = coef + 6 * (size_t)n_nodes;
+  FDM_CUDA(launch_coefficients(n_fibers, d_fiber_offsets, d_element_lengths, d_prefactor, dt,
+                               diffusion_scheme == FDM_IMPLICIT_EULER, coef, n_nodes, st));
+  FDM_CUDA(launch_diffusion_warp(n_fibers, d_fiber_offsets, coef, n_nodes, d_vm, fwd, st));
+  FDM_CUDA(cudaStreamSynchronize(st));
   return FDM_OK;
 }

@@ -26,8 +26,7 @@ const ModelDesc* model_desc(int model);
 // split path
 cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s);
 cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s);
-cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const int64_t* elem_offsets,
-                                const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
+cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
                                 double* coef, int64_t stride, cudaStream_t s);
 cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
                                   double* vm, double* scratch, cudaStream_t s);

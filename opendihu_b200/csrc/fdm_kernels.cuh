@@ -142,10 +142,38 @@ __device__ __forceinline__ bool stim_bit(const uint32_t* __restrict__ flags, int
 // one Heun step (03_generator_vc.cpp:1017-1130):
 //   y* = y + dt f(y); [Vm* := vStim]; y += dt/2 (f(y) + f(y*)); [Vm := vStim]
 // Vm is carried in FP64; the other states and the rates in RR (double or float).
+// In FP32 every state other than Vm is a pair (S, L) whose sum is the value: the update
+// S + dt/2 (f + f*) is accumulated with Fast2Sum (error of the addition kept in L).  Without it,
+// increments below half an FP32 ulp of the gate are lost at every step and the slowly relaxing
+// gates stagnate (a single HH cell at rest drifts 6e-3 mV from FP64 within 10 ms; with the
+// compensation 1e-6 mV).
 // --------------------------------------------------------------------------------------------
+template<class RR>
+struct Compensated {
+  static constexpr bool value = false;
+};
+template<>
+struct Compensated<float> {
+  static constexpr bool value = true;
+};
+
+template<class RR>
+__device__ __forceinline__ void accumulate(RR& s, RR& l, RR inc)
+{
+  if (Compensated<RR>::value) {
+    inc += l;
+    const RR t = s + inc;
+    l = inc - (t - s);
+    s = t;
+  } else {
+    s += inc;
+  }
+}
+
 template<class Model, class RR, class Math, bool STORE>
-__device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, const RR* __restrict__ P, double t,
-                                          double dt, bool clamp, double vstim, RR* __restrict__ alg_store)
+__device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __restrict__ L,
+                                          const RR* __restrict__ P, double t, double dt, bool clamp, double vstim,
+                                          RR* __restrict__ alg_store)
 {
   constexpr int NS = Model::nStates;
   RR y[NS], r[NS], ys[NS], r2[NS];
@@ -168,7 +196,7 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, const R
   V += 0.5 * dt * ((double)r[0] + (double)r2[0]);
 #pragma unroll
   for (int s = 1; s < NS; s++)
-    S[s - 1] = y[s] + (RR)0.5 * dtr * (r[s] + r2[s]);
+    accumulate<RR>(S[s - 1], L[s - 1], (RR)0.5 * dtr * (r[s] + r2[s]));
   if (clamp)
     V = vstim;
   if (STORE) {
@@ -202,6 +230,7 @@ struct ReactionArgs {
   int64_t stride;                 // SoA stride of states / parameters
   double* vm;                     // [node]
   void* states;                   // RR [(s-1)*stride + node], s = 1..nStates-1
+  void* states_lo;                // FP32 only: compensation terms, same layout
   const void* params;             // RR [p*stride + node]
   const int* clamp_fiber;         // per node: fiber whose machine controls the clamp, or -1
   const uint32_t* flags;
@@ -235,10 +264,13 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
   RR* st = (RR*)a.states;
   const RR* pr = (const RR*)a.params;
   double V = a.vm[i];
-  RR S[NS > 1 ? NS - 1 : 1];
+  RR* stl = (RR*)a.states_lo;
+  RR S[NS > 1 ? NS - 1 : 1], L[NS > 1 ? NS - 1 : 1];
 #pragma unroll
-  for (int s = 1; s < NS; s++)
+  for (int s = 1; s < NS; s++) {
     S[s - 1] = st[(s - 1) * a.stride + i];
+    L[s - 1] = Compensated<RR>::value ? stl[(s - 1) * a.stride + i] : (RR)0;
+  }
   RR P[NP], Pstim[NP];
 #pragma unroll
   for (int q = 0; q < Model::nParameters; q++) {
@@ -259,16 +291,19 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
       Pk[q] = (stim && a.stimulus_mode == 1) ? Pstim[q] : P[q];
     if (a.store_alg && k == s.n0 - 1) {
       RR alg[Model::nAlgebraics];
-      heun_step<Model, RR, Math, true>(V, S, Pk, t, s.dt0, vclamp, a.vstim, alg);
+      heun_step<Model, RR, Math, true>(V, S, L, Pk, t, s.dt0, vclamp, a.vstim, alg);
       store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, i);
     } else {
-      heun_step<Model, RR, Math, false>(V, S, Pk, t, s.dt0, vclamp, a.vstim, nullptr);
+      heun_step<Model, RR, Math, false>(V, S, L, Pk, t, s.dt0, vclamp, a.vstim, nullptr);
     }
   }
   a.vm[i] = V;
 #pragma unroll
-  for (int s2 = 1; s2 < NS; s2++)
+  for (int s2 = 1; s2 < NS; s2++) {
     st[(s2 - 1) * a.stride + i] = S[s2 - 1];
+    if (Compensated<RR>::value)
+      stl[(s2 - 1) * a.stride + i] = L[s2 - 1];
+  }
   if (a.half == 1 && a.trace_slot) {
     const int slot = a.trace_slot[i];
     if (slot >= 0 && s.global_no < a.trace_capacity)
@@ -286,7 +321,6 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
 // --------------------------------------------------------------------------------------------
 #ifdef FDM_COMMON_KERNELS_TU
 __global__ void diffusion_coefficients_kernel(int n_fibers, const int64_t* __restrict__ fiber_offsets,
-                                              const int64_t* __restrict__ elem_offsets,
                                               const double* __restrict__ element_lengths,
                                               const double* __restrict__ prefactor, double dt, int implicit_euler,
                                               double* __restrict__ coef, int64_t stride)
@@ -296,7 +330,7 @@ __global__ void diffusion_coefficients_kernel(int n_fibers, const int64_t* __res
     return;
   const int64_t o = fiber_offsets[f];
   const int64_t n = fiber_offsets[f + 1] - o;
-  const double* h = element_lengths + elem_offsets[f];
+  const double* h = element_lengths + (o - f); // fiber f's elements follow the previous fibers' n-1 each
   const double pf = prefactor[f];
   double cp_prev = 0.0;
   for (int64_t v = 0; v < n; v++) {
@@ -453,6 +487,7 @@ struct FusedArgs {
   int64_t stride;
   double* vm;
   void* states;                   // RR SoA
+  void* states_lo;                // FP32 only: compensation terms
   const void* params;             // RR SoA
   const double* coef;             // 6 x stride
   const int* clamp_fiber;
@@ -595,8 +630,10 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 
   const RR* pr = (const RR*)a.params;
   RR* st = (RR*)a.states;
+  RR* stl = (RR*)a.states_lo;
   double V[M];
   RR S[M][NS > 1 ? NS - 1 : 1];
+  RR L[M][NS > 1 ? NS - 1 : 1];
   RR P[M][NP];
   int cf[M];
   int ts[M];
@@ -609,8 +646,10 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     gi[j] = i;
     V[j] = ok ? a.vm[i] : 0.0;
 #pragma unroll
-    for (int s = 1; s < NS; s++)
+    for (int s = 1; s < NS; s++) {
       S[j][s - 1] = ok ? st[(s - 1) * a.stride + i] : (RR)0;
+      L[j][s - 1] = (ok && Compensated<RR>::value) ? stl[(s - 1) * a.stride + i] : (RR)0;
+    }
 #pragma unroll
     for (int p = 0; p < Model::nParameters; p++)
       P[j][p] = ok ? pr[p * a.stride + i] : (RR)0;
@@ -641,10 +680,10 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
             Pk[p] = (stim && a.stimulus_mode == 1 && p == a.stimulus_parameter) ? (RR)a.stimulus_value : P[j][p];
           const bool vclamp = stim && a.stimulus_mode == 0;
           if (!store_now) {
-            heun_step<Model, RR, Math, false>(V[j], S[j], Pk, t, s.dt0, vclamp, a.vstim, nullptr);
+            heun_step<Model, RR, Math, false>(V[j], S[j], L[j], Pk, t, s.dt0, vclamp, a.vstim, nullptr);
           } else {
             RR alg[Model::nAlgebraics];
-            heun_step<Model, RR, Math, true>(V[j], S[j], Pk, t, s.dt0, vclamp, a.vstim, alg);
+            heun_step<Model, RR, Math, true>(V[j], S[j], L[j], Pk, t, s.dt0, vclamp, a.vstim, alg);
             store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, gi[j]);
           }
         }
@@ -710,8 +749,11 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       const int64_t i = gi[j];
       a.vm[i] = V[j];
 #pragma unroll
-      for (int s = 1; s < NS; s++)
+      for (int s = 1; s < NS; s++) {
         st[(s - 1) * a.stride + i] = S[j][s - 1];
+        if (Compensated<RR>::value)
+          stl[(s - 1) * a.stride + i] = L[j][s - 1];
+      }
     }
   }
 }

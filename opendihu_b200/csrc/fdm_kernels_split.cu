@@ -63,16 +63,15 @@ cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_ste
   return cudaGetLastError();
 }
 
-cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const int64_t* elem_offsets,
-                                const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
-                                double* coef, int64_t stride, cudaStream_t s)
+cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths,
+                                const double* prefactor, double dt, int implicit_euler, double* coef, int64_t stride,
+                                cudaStream_t s)
 {
   if (n_fibers == 0)
     return cudaSuccess;
   const int T = 64;
-  diffusion_coefficients_kernel<<<(n_fibers + T - 1) / T, T, 0, s>>>(n_fibers, fiber_offsets, elem_offsets,
-                                                                     element_lengths, prefactor, dt, implicit_euler,
-                                                                     coef, stride);
+  diffusion_coefficients_kernel<<<(n_fibers + T - 1) / T, T, 0, s>>>(n_fibers, fiber_offsets, element_lengths,
+                                                                     prefactor, dt, implicit_euler, coef, stride);
   return cudaGetLastError();
 }
 
