@@ -156,6 +156,19 @@ int fdm_checkpoint_restore(fdm_solver *s);
 int fdm_diffusion_solve(int n_fibers, int64_t n_nodes, const int64_t *d_fiber_offsets, const double *d_element_lengths,
                         const double *d_prefactor, double dt, int diffusion_scheme, double *d_vm, void *stream);
 
+/* fdm_diffusion_solve without any device allocation; no counterpart in the reference.  For callers that
+ * cannot allocate device memory while they run (an application whose memory pool owns the whole GPU, a
+ * coupled code that has reserved HBM for its own mesh, a stepping loop that must not synchronize on
+ * cudaMalloc/cudaFree).  The scratch is one array compiled into the library, sized for at most
+ * FDM_NOALLOC_MAX_NODES nodes (14.7 MB held on every GPU that loads the library until the process exits);
+ * larger n_nodes fail with FDM_ERR_ARG.  The first call on a device looks the array's address up; make it
+ * before any stream capture.  All calls share the array: calls that overlap on the GPU race, so order them
+ * on one stream.  Arguments and result as fdm_diffusion_solve. */
+#define FDM_NOALLOC_MAX_NODES 262144
+int fdm_diffusion_solve_noalloc(int n_fibers, int64_t n_nodes, const int64_t *d_fiber_offsets,
+                                const double *d_element_lengths, const double *d_prefactor, double dt,
+                                int diffusion_scheme, double *d_vm, void *stream);
+
 /* number of the fused-kernel shapes built into the library and their (threads, nodes per thread) */
 int fdm_fused_shapes(int *threads, int *nodes_per_thread, int capacity);
 

@@ -29,7 +29,11 @@ EXPORTED = [
     "fdm_get_clamp_nodes", "fdm_set_algebraics_for_transfer", "fdm_get_algebraics", "fdm_set_trace",
     "fdm_get_trace", "fdm_advance", "fdm_split_steps", "fdm_get_timing", "fdm_reset_timing",
     "fdm_checkpoint_save", "fdm_checkpoint_restore", "fdm_fused_shapes", "fdm_diffusion_solve",
+    "fdm_diffusion_solve_noalloc",
 ]
+
+#: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
+NOALLOC_MAX_NODES = 262144
 
 
 class FdmError(RuntimeError):
@@ -95,6 +99,7 @@ def lib() -> C.CDLL:
         "fdm_checkpoint_restore": (C.c_int, [P]),
         "fdm_fused_shapes": (C.c_int, [i32, i32, C.c_int]),
         "fdm_diffusion_solve": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
+        "fdm_diffusion_solve_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -22,7 +22,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libfdm_b200.so")
 
-SOURCES = ["fdm_host.cu", "fdm_kernels_split.cu", "fdm_fused.cu"]
+SOURCES = ["fdm_host.cu", "fdm_kernels_split.cu", "fdm_fused.cu", "fdm_noalloc.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",

@@ -167,6 +167,12 @@ static int fail(fdm_solver* s, int code, const std::string& msg)
   return code;
 }
 
+int fdm::fdm_report_error(int code, const std::string& msg)
+{
+  g_create_error = msg;
+  return code;
+}
+
 static int cuda_fail(fdm_solver* s, cudaError_t e, const char* what)
 {
   return fail(s, FDM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));

@@ -4,9 +4,14 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "fdm_kernels.cuh"
 
 namespace fdm {
+
+// records msg as the message fdm_last_error(NULL) returns on this thread; returns code
+int fdm_report_error(int code, const std::string& msg);
 
 enum MathKind { MATH_EXACT = 0, MATH_APPROX = 1 };
 enum RealKind { REAL_F64 = 0, REAL_F32 = 1 };
