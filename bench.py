@@ -43,6 +43,7 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0, help="fused CTA threads (0 = default)")
     p.add_argument("--nodes-per-thread", type=int, default=0)
     p.add_argument("--steps-per-launch", type=int, default=0)
+    p.add_argument("--no-autotune", action="store_true")
     return p.parse_args()
 
 
@@ -198,8 +199,9 @@ def main():
     n_nodes = system.n_nodes
     fused = S.FastMonodomainSolver(system.copy(), method="fused", precision="fp32", profile=True, device=local,
                                    threads_per_block=args.threads, nodes_per_thread=args.nodes_per_thread,
-                                   steps_per_launch=args.steps_per_launch)
+                                   steps_per_launch=args.steps_per_launch, autotune=not args.no_autotune)
     fused.initialize()
+    tuning = fused.tuning
     step = args.step_ms
     t = 0.0
     for _ in range(args.warmup):
@@ -309,6 +311,8 @@ def main():
                                    "dt0D 1e-4 ms, dt_split 1e-3 ms",
                        "n_nodes_per_gpu": n_nodes, "step": f"{step} ms simulated = {split_steps // args.steps} Strang steps",
                        "method": "fused persistent kernel, FP32 reaction", "l2": "inputs larger than L2 (~0.5 GB/GPU)",
+                       "fused_shape": {"threads": fused.threads_per_block, "nodes_per_thread": fused.nodes_per_thread,
+                                       "steps_per_launch": steps_per_launch, "autotuned": tuning is not None},
                        "parallelism": f"fibers sharded, {world} GPU(s), no collective"},
             "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes},

@@ -1,0 +1,108 @@
+"""Autotuner of the fused kernel's launch shape.
+
+The fused kernel packs whole fibers into bins of T*M nodes (T threads per CTA, M nodes per thread, so the
+number of fibers per CTA follows from the fiber lengths) and runs K Strang steps per launch.  The best
+(T, M) depends on the model's register footprint and on the length distribution (bin fill, waves on
+148 SMs); K trades launch overhead against stimulation-schedule memory.  The tuner times every built shape
+that holds the longest fiber on the actual workload for a few Strang steps (device time of the kernel
+launches, CUDA events) and then a few K values for the winner.  Results are cached per workload signature
+in memory and, if FDM_AUTOTUNE_CACHE names a file, in that JSON file.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+
+_MEMO: Dict[str, dict] = {}
+
+
+def signature(system, precision: str) -> str:
+    lengths = np.diff(np.asarray(system.fiber_offsets))
+    hist = np.histogram(lengths, bins=16, range=(0, int(lengths.max()) + 1))[0]
+    desc = [system.model, precision, system.diffusion_scheme, bool(system.approximate_exponential_function),
+            int(lengths.max()), int(lengths.sum()), hist.tolist()]
+    return hashlib.sha1(json.dumps(desc).encode()).hexdigest()[:16]
+
+
+def _load_cache() -> Dict[str, dict]:
+    path = os.environ.get("FDM_AUTOTUNE_CACHE")
+    if path and os.path.exists(path):
+        try:
+            return json.load(open(path))
+        except (OSError, ValueError):
+            return {}
+    return {}
+
+
+def _store_cache(key: str, value: dict):
+    path = os.environ.get("FDM_AUTOTUNE_CACHE")
+    if not path:
+        return
+    data = _load_cache()
+    data[key] = value
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1)
+    os.replace(tmp, path)
+
+
+def _time_shape(system, precision, threads, m, k, n_steps, device) -> float:
+    """Seconds of device time per Strang step (all GPU work of the advance: schedule + fused kernels)."""
+    from .solver import FastMonodomainSolver
+    s = system.copy()
+    dt = s.dt_splitting
+    with FastMonodomainSolver(s, method="fused", precision=precision, threads_per_block=threads,
+                              nodes_per_thread=m, steps_per_launch=k, profile=True, device=device,
+                              check_nan=False) as slv:
+        slv.setTimeSpan(s.start_time, s.start_time + dt * min(k, n_steps))
+        slv.advanceTimeSpan()  # warm-up (module load, factorization)
+        slv.reset_timing()
+        t0 = s.start_time + dt * min(k, n_steps)
+        slv.setTimeSpan(t0, t0 + dt * n_steps)
+        slv.advanceTimeSpan()
+        tm = slv.timing()
+    return tm["advance_ms"] / 1e3 / n_steps
+
+
+def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0,
+             steps_per_launch: Sequence[int] = (50, 100, 200), use_cache: bool = True) -> dict:
+    """Return {"threads", "nodes_per_thread", "steps_per_launch", "s_per_step", "trials"} for the workload."""
+    key = signature(system, precision)
+    if use_cache:
+        if key in _MEMO:
+            return _MEMO[key]
+        cached = _load_cache().get(key)
+        if cached:
+            _MEMO[key] = cached
+            return cached
+    max_len = int(np.diff(np.asarray(system.fiber_offsets)).max())
+    shapes = [(t, m) for t, m in N.fused_shapes() if t * m >= max_len]
+    if not shapes:
+        raise N.FdmError(N.FDM_ERR_UNSUPPORTED, f"no fused shape holds a fiber of {max_len} nodes")
+    trials = []
+    k0 = 100
+    for t, m in shapes:
+        trials.append({"threads": t, "nodes_per_thread": m, "steps_per_launch": min(k0, n_steps),
+                       "s_per_step": _time_shape(system, precision, t, m, min(k0, n_steps), n_steps, device)})
+    best = min(trials, key=lambda r: r["s_per_step"])
+    # window length for the winner, over a span of a few windows
+    k_trials = []
+    for k in steps_per_launch:
+        span = max(n_steps, 2 * k)
+        k_trials.append({"threads": best["threads"], "nodes_per_thread": best["nodes_per_thread"],
+                         "steps_per_launch": k,
+                         "s_per_step": _time_shape(system, precision, best["threads"], best["nodes_per_thread"], k,
+                                                   span, device)})
+    best_k = min(k_trials, key=lambda r: r["s_per_step"])
+    result = dict(best_k)
+    result["trials"] = trials + k_trials
+    _MEMO[key] = result
+    if use_cache:
+        _store_cache(key, result)
+    return result

@@ -553,6 +553,103 @@ def _ident(model: Model) -> str:
     return re.sub(r"[^A-Za-z0-9_]", "_", model.name)
 
 
+def _affine(e, consts):
+    """e as (coefficients {(kind, idx): a}, constant b) if it is affine in STATES/PARAMS/VOI with numeric
+    coefficients, else None (CONSTANTS count as numbers: they are folded)."""
+    t = e[0]
+    if t == "num":
+        return {}, e[2]
+    if t == "var":
+        if e[1] == "C":
+            return {}, consts[e[2]]
+        if e[1] in ("S", "P", "T"):
+            return {(e[1], e[2]): 1.0}, 0.0
+        return None
+    if t == "neg":
+        a = _affine(e[1], consts)
+        return None if a is None else ({k: -v for k, v in a[0].items()}, -a[1])
+    if t == "pos":
+        return _affine(e[1], consts)
+    if t == "bin" and e[1] in "+-":
+        a = _affine(e[2], consts)
+        b = _affine(e[3], consts)
+        if a is None or b is None:
+            return None
+        sg = 1.0 if e[1] == "+" else -1.0
+        c = dict(a[0])
+        for k, v in b[0].items():
+            c[k] = c.get(k, 0.0) + sg * v
+        return c, a[1] + sg * b[1]
+    if t == "bin" and e[1] in "*/":
+        a = _affine(e[2], consts)
+        b = _affine(e[3], consts)
+        if a is None or b is None:
+            return None
+        if e[1] == "*":
+            if not a[0]:
+                return {k: a[1] * v for k, v in b[0].items()}, a[1] * b[1]
+            if not b[0]:
+                return {k: b[1] * v for k, v in a[0].items()}, b[1] * a[1]
+            return None
+        if not b[0] and b[1] != 0.0:
+            return {k: v / b[1] for k, v in a[0].items()}, a[1] / b[1]
+        return None
+    return None
+
+
+def _exp_groups(lines, consts):
+    """Exponentials whose arguments are affine in the same variables with the same coefficients, differing
+    only by a constant: exp(a.x + b_k) = exp(a.x) * e^{b_k}.  Returns {repr(exp node): (group, b_k)} and the
+    list of group (coefficients) of the groups with at least two distinct members."""
+    found = {}
+
+    def walk(e):
+        t = e[0]
+        if t == "call":
+            if e[1] == "exp":
+                af = _affine(e[2][0], consts)
+                if af is not None and af[0]:
+                    key = tuple(sorted((k, round(v, 15)) for k, v in af[0].items()))
+                    found.setdefault(key, {})[repr(e)] = af[1]
+            for a in e[2]:
+                walk(a)
+        elif t in ("neg", "pos", "not"):
+            walk(e[1])
+        elif t == "bin":
+            walk(e[2])
+            walk(e[3])
+        elif t == "tern":
+            walk(e[1])
+            walk(e[2])
+            walk(e[3])
+    for _, _, e in lines:
+        walk(e)
+    repl = {}
+    groups = []
+    for key, members in found.items():
+        if len(members) < 2:
+            continue
+        g = len(groups)
+        groups.append(key)
+        for r, b in members.items():
+            repl[r] = (g, b)
+    return repl, groups
+
+
+class _FastEmitter(_Emitter):
+    """FP32 variant: shared exponentials (see _exp_groups)."""
+
+    def __init__(self, real, consts, repl):
+        super().__init__(real, consts, "cuda")
+        self.repl = repl
+
+    def expr(self, e):
+        if e[0] == "call" and e[1] == "exp" and repr(e) in self.repl:
+            g, b = self.repl[repr(e)]
+            return f"(fdm_e{g} * (({self.real}){_hexf(math.exp(b))}))"
+        return super().expr(e)
+
+
 def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> str:
     """CUDA device right-hand side for one parameter variant.
 
@@ -598,6 +695,32 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     for kind, idx, expr in lines:
         tgt = f"ALGEBRAIC[{idx}]" if kind == "A" else f"RATES[{idx}]"
         out.append(f"    {tgt} = {em.expr(expr)};")
+    for n in pows:
+        out.append(f"#undef FDM_POW{n}")
+    out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
+    out.append("  }")
+    # FP32 variant with shared exponentials
+    repl, groups = _exp_groups(lines, model.constants)
+    fem = _FastEmitter("R", model.constants, repl)
+    out.append("  // FP32 form: exponentials exp(a.x + b_k) that share a.x are evaluated once as exp(a.x) * e^{b_k}")
+    out.append(f"  static constexpr int nSharedExponentials = {len(groups)};")
+    out.append("  template<class R, class M>")
+    out.append("  __device__ __forceinline__ static void rates_fast(const R VOI, const R* __restrict__ STATES,"
+               " const R* __restrict__ PARAMS, R* __restrict__ RATES, R* __restrict__ ALGEBRAIC)")
+    out.append("  {")
+    out.append("    (void)VOI; (void)PARAMS;")
+    out.append("#define FDM_EXP(x) M::exp(x)")
+    out.append("#define FDM_LOG(x) M::log(x)")
+    out.append("#define FDM_POWF(x, y) M::pow(x, y)")
+    out.append("#define FDM_ABS(x) fabs(x)")
+    out.append("#define FDM_SQRT(x) sqrt(x)")
+    out.extend("#define " + s2.split("#define ", 1)[1] for s2 in _pow_macro_defs(pows))
+    for g, key in enumerate(groups):
+        terms = " + ".join(f"(({'R'}){_hexf(v)}) * {fem.var(k[0], k[1])}" for k, v in key)
+        out.append(f"    const R fdm_e{g} = FDM_EXP({terms});")
+    for kind, idx, expr in lines:
+        tgt = f"ALGEBRAIC[{idx}]" if kind == "A" else f"RATES[{idx}]"
+        out.append(f"    {tgt} = {fem.expr(expr)};")
     for n in pows:
         out.append(f"#undef FDM_POW{n}")
     out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")

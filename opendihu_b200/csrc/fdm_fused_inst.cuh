@@ -1,0 +1,61 @@
+// Fused-kernel instantiations for one (precision, math policy); included by fdm_fused_*.cu.
+#pragma once
+#include "fdm_internal.h"
+
+#include "generated/hodgkin_huxley_1952_anone_c2_3_4.cuh"
+
+// (threads per CTA, nodes per thread); capacity T*M nodes per bin
+#define FDM_FUSED_SHAPES(X) \
+  X(128, 8)                 \
+  X(256, 4)                 \
+  X(256, 6)                 \
+  X(256, 8)                 \
+  X(256, 10)                \
+  X(384, 7)                 \
+  X(512, 3)                 \
+  X(512, 5)                 \
+  X(640, 4)                 \
+  X(768, 4)                 \
+  X(1024, 3)
+
+namespace fdm {
+
+using FusedHH = fdm_model_hodgkin_huxley_1952_anone_c2_3_4;
+
+cudaError_t launch_fused_hh_f64_exact(int shape, const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_hh_f64_approx(int shape, const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_hh_f32_exact(int shape, const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_hh_f32_approx(int shape, const FusedArgs& a, cudaStream_t s);
+
+template<class Model, class RR, class Math, int T, int M>
+static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s)
+{
+  constexpr size_t smem = fused_smem_bytes<T, M>();
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(fused_kernel<Model, RR, Math, T, M>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return e;
+    attr_set = true;
+  }
+  if (a.n_bins == 0)
+    return cudaSuccess;
+  fused_kernel<Model, RR, Math, T, M><<<a.n_bins, T, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template<class Model, class RR, class Math>
+static cudaError_t fused_shape(int shape, const FusedArgs& a, cudaStream_t s)
+{
+  int k = 0;
+#define FDM_SHAPE_CASE(T, M)                       \
+  if (shape == k)                                  \
+    return fused_one<Model, RR, Math, T, M>(a, s); \
+  k++;
+  FDM_FUSED_SHAPES(FDM_SHAPE_CASE)
+#undef FDM_SHAPE_CASE
+  return cudaErrorInvalidValue;
+}
+
+} // namespace fdm

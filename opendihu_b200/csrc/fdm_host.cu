@@ -423,8 +423,9 @@ static int choose_shape(fdm_solver* s)
         return cap >= s->max_fiber_len ? i : -2;
       continue;
     }
-    // default: the smallest capacity that holds the longest fiber, preferring 256+ threads
-    if (cap >= s->max_fiber_len && sh[i].threads >= 256 && (best < 0 || cap < best_cap)) {
+    // default (without the autotuner): the smallest capacity that holds the longest fiber among the
+    // shapes with at least 512 threads (16 warps per SM for the HH register footprint)
+    if (cap >= s->max_fiber_len && sh[i].threads >= 512 && (best < 0 || cap < best_cap)) {
       best = i;
       best_cap = cap;
     }

@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "fdm_math.cuh"
 
 namespace fdm {
@@ -170,6 +172,17 @@ __device__ __forceinline__ void accumulate(RR& s, RR& l, RR inc)
   }
 }
 
+// right-hand side: the FP32 exact-exp mode uses the model's shared-exponential form (fewer SFU
+// operations); FP64 and the approximate-exp policy (whose exp is not multiplicative) use the plain form
+template<class Model, class RR, class Math>
+__device__ __forceinline__ void model_rates(const RR t, const RR* y, const RR* P, RR* r, RR* alg)
+{
+  if constexpr (std::is_same<RR, float>::value && std::is_same<Math, fdm_math_exact>::value)
+    Model::template rates_fast<RR, Math>(t, y, P, r, alg);
+  else
+    Model::template rates<RR, Math>(t, y, P, r, alg);
+}
+
 template<class Model, class RR, class Math, bool STORE>
 __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __restrict__ L,
                                           const RR* __restrict__ P, double t, double dt, bool clamp, double vstim,
@@ -183,7 +196,7 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __r
   for (int s = 1; s < NS; s++)
     y[s] = S[s - 1];
   const RR tr = (RR)t;
-  Model::template rates<RR, Math>(tr, y, P, r, alg);
+  model_rates<Model, RR, Math>(tr, y, P, r, alg);
   const RR dtr = (RR)dt;
   const double vs = V + dt * (double)r[0];
   ys[0] = (RR)vs;
@@ -192,7 +205,7 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __r
     ys[s] = y[s] + dtr * r[s];
   if (clamp)
     ys[0] = (RR)vstim;
-  Model::template rates<RR, Math>(tr, ys, P, r2, alg2);
+  model_rates<Model, RR, Math>(tr, ys, P, r2, alg2);
   V += 0.5 * dt * ((double)r[0] + (double)r2[0]);
 #pragma unroll
   for (int s = 1; s < NS; s++)
@@ -664,11 +677,12 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     for (int half = 0; half < 2; half++) {
       const double t0 = half ? s.mid : s.t;
       const int base = (step * 2 + half) * a.nsub_stride;
-      const bool last_half = a.store_alg && half == 1 && step == a.n_steps - 1;
+      // the substep after which algebraicsForTransfer are stored runs outside the hot loop
+      const bool store_here = a.store_alg && half == 1 && step == a.n_steps - 1;
+      const int k_end = store_here ? s.n0 - 1 : s.n0;
 #pragma unroll 1
-      for (int k = 0; k < s.n0; k++) {
+      for (int k = 0; k < k_end; k++) {
         const double t = xadd(t0, xmul((double)k, s.dt0));
-        const bool store_now = last_half && k == s.n0 - 1;
 #pragma unroll
         for (int j = 0; j < M; j++) {
           if (tid * M + j >= nb)
@@ -679,13 +693,25 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
           for (int p = 0; p < NP; p++)
             Pk[p] = (stim && a.stimulus_mode == 1 && p == a.stimulus_parameter) ? (RR)a.stimulus_value : P[j][p];
           const bool vclamp = stim && a.stimulus_mode == 0;
-          if (!store_now) {
-            heun_step<Model, RR, Math, false>(V[j], S[j], L[j], Pk, t, s.dt0, vclamp, a.vstim, nullptr);
-          } else {
-            RR alg[Model::nAlgebraics];
-            heun_step<Model, RR, Math, true>(V[j], S[j], L[j], Pk, t, s.dt0, vclamp, a.vstim, alg);
-            store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, gi[j]);
-          }
+          heun_step<Model, RR, Math, false>(V[j], S[j], L[j], Pk, t, s.dt0, vclamp, a.vstim, nullptr);
+        }
+      }
+      if (store_here) {
+        const int k = s.n0 - 1;
+        const double t = xadd(t0, xmul((double)k, s.dt0));
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+          if (tid * M + j >= nb)
+            continue;
+          const bool stim = cf[j] >= 0 && stim_bit(a.flags, a.words_per_fiber, cf[j], base + k);
+          RR Pk[NP];
+#pragma unroll
+          for (int p = 0; p < NP; p++)
+            Pk[p] = (stim && a.stimulus_mode == 1 && p == a.stimulus_parameter) ? (RR)a.stimulus_value : P[j][p];
+          RR alg[Model::nAlgebraics];
+          heun_step<Model, RR, Math, true>(V[j], S[j], L[j], Pk, t, s.dt0, stim && a.stimulus_mode == 0, a.vstim,
+                                           alg);
+          store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, gi[j]);
         }
       }
       if (half == 1)

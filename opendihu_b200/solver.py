@@ -306,7 +306,7 @@ class FastMonodomainSolver:
     def __init__(self, system: FiberSystem, method: Optional[str] = None, precision: Optional[str] = None,
                  steps_per_launch: int = 0, threads_per_block: int = 0, nodes_per_thread: int = 0,
                  check_nan: bool = True, profile: bool = False, trace_nodes: Sequence[int] = (),
-                 trace_capacity: int = 0, device: int = 0):
+                 trace_capacity: int = 0, device: int = 0, autotune: bool = False):
         self.system = system
         self.method = method or getattr(system, "method", "split")
         self.precision = precision or getattr(system, "precision", "fp64")
@@ -318,6 +318,8 @@ class FastMonodomainSolver:
         self.trace_nodes = np.asarray(trace_nodes, np.int64)
         self.trace_capacity = int(trace_capacity)
         self.device = int(device)
+        self.autotune = bool(autotune)
+        self.tuning = None
         self._h = None
         self._start = system.start_time
         self._end = system.end_time
@@ -334,6 +336,13 @@ class FastMonodomainSolver:
             return
         s = self.system
         L = N.lib()
+        if self.autotune and self.method == "fused" and not self.threads_per_block:
+            from .autotune import autotune
+            self.tuning = autotune(s, self.precision, device=self.device)
+            self.threads_per_block = self.tuning["threads"]
+            self.nodes_per_thread = self.tuning["nodes_per_thread"]
+            if not self.steps_per_launch:
+                self.steps_per_launch = self.tuning["steps_per_launch"]
         cfg = N.default_config()
         cfg.model = N.MODEL_IDS[s.model]
         cfg.diffusion_scheme = SCHEMES[s.diffusion_scheme]
