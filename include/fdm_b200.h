@@ -15,8 +15,8 @@
  *  - fdm_checkpoint_save / fdm_checkpoint_restore are saveFiberDataCheckpoint /
  *    restoreFiberDataCheckpoint (fast_monodomain_solver_communication.tpp:497-509).
  *  - fdm_get_algebraics returns algebraicsForTransfer (03_generator_vc.cpp:1131-1160).
- *  - fdm_compat_configure + initializeArrays + computeMonodomain export the reference's generated-library
- *    symbols with their exact signatures (fast_monodomain_solver_gpu.tpp:361-365, :478-481).
+ *  - fdm_compat_configure + initializeArrays + computeMonodomain (end of this header) export the reference's
+ *    generated-library symbols with their exact signatures (fast_monodomain_solver_gpu.tpp:361-365, :478-481).
  *
  * Errors: every function returns FDM_OK (0) or a positive FDM_ERR_* code; fdm_last_error() gives the
  * message.  Nothing aborts the process.  One solver handle must not be used from two host threads
@@ -171,6 +171,31 @@ int fdm_diffusion_solve_noalloc(int n_fibers, int64_t n_nodes, const int64_t *d_
 
 /* number of the fused-kernel shapes built into the library and their (threads, nodes per thread) */
 int fdm_fused_shapes(int *threads, int *nodes_per_thread, int capacity);
+
+/* ---- compatibility export of the reference's generated-library ABI ---------------------------------
+ * The reference's FastMonodomainSolver with optimizationType "gpu" dlopens a library and binds
+ * initializeArrays and computeMonodomain (fast_monodomain_solver_gpu.tpp:185-196); pointing its
+ * "libraryFilename" at libfdm_b200.so makes it use this solver.  The reference bakes the sizes into the
+ * generated source (gpu.tpp:293-312); here fdm_compat_configure gives them first.  The nodes use the clamp set
+ * of the reference's GPU code (junction node and its neighbours); parameters fill the model's first
+ * parameter slots.  One process-wide instance; fdm_compat_release frees it. */
+int fdm_compat_configure(int model, int n_fibers, int n_instances_per_fiber, int n_parameters_per_instance,
+                         int firing_rows, int firing_cols, int n_jitter_per_fiber, int n_algebraics_for_transfer,
+                         int n_states_for_transfer, int diffusion_scheme, int approximate_exponential_function,
+                         int reaction_precision, int method);
+/* fast_monodomain_solver_gpu.tpp:361-365 */
+void initializeArrays(const double *statesOneInstance, const int *algebraicsForTransferIndices,
+                      const int *statesForTransferIndices, const char *firingEvents,
+                      const double *setSpecificStatesFrequencyJitter, const int *motorUnitNo,
+                      const int *fiberStimulationPointIndex, const double *lastStimulationCheckTime,
+                      const double *setSpecificStatesCallFrequency, const double *setSpecificStatesRepeatAfterFirstCall,
+                      const double *setSpecificStatesCallEnableBegin);
+/* fast_monodomain_solver_gpu.tpp:478-481 */
+void computeMonodomain(const float *parameters, double *algebraicsForTransfer, double *statesForTransfer,
+                       const float *elementLengths, double startTime, double timeStepWidthSplitting,
+                       int nTimeStepsSplitting, double dt0D, int nTimeSteps0D, double dt1D, int nTimeSteps1D,
+                       double prefactor, double valueForStimulatedPoint);
+int fdm_compat_release(void);
 
 #ifdef __cplusplus
 }

@@ -1183,6 +1183,45 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
   return FDM_OK;
 }
 
+// Strang steps given explicitly, as the reference's generated computeMonodomain receives them
+// (fast_monodomain_solver_gpu.tpp:478-481, 505-515): currentTime = startTime + j*dtSplit, substeps at
+// currentTime + k*dt0D and midTime + k*dt0D, one diffusion solve with dt1D per step.
+static int advance_explicit(fdm_solver* s, double start, double dts, int ns, double dt0, int n0, double dt1)
+{
+  s->ev_used = 0;
+  FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
+  const int K = s->cfg.steps_per_launch;
+  int filled = 0;
+  for (int j = 0; j < ns; j++) {
+    if (filled == K) {
+      int r = run_window(s, filled, dt1, false);
+      if (r)
+        return r;
+      filled = 0;
+    }
+    if (filled == 0)
+      FDM_CUDA(cudaEventSynchronize(s->slot_ev[s->slot]));
+    SplitStep& st = s->steps_h[(size_t)s->slot * K + filled];
+    const double tc = start + j * dts;
+    st.t = tc;
+    st.mid = tc + 0.5 * dts;
+    st.dt0 = dt0;
+    st.n0 = n0;
+    st.global_no = (int)std::min<int64_t>(s->split_no, 2147483647);
+    s->split_no++;
+    filled++;
+  }
+  int r = run_window(s, filled, dt1, true);
+  if (r)
+    return r;
+  FDM_CUDA(cudaEventRecord(s->adv_stop, s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  float ms = 0;
+  FDM_CUDA(cudaEventElapsedTime(&ms, s->adv_start, s->adv_stop));
+  s->adv_ms += ms;
+  return FDM_OK;
+}
+
 extern "C" int64_t fdm_split_steps(const fdm_solver* s) { return s ? s->split_no : 0; }
 
 extern "C" int fdm_get_timing(const fdm_solver* s, double* main_ms, int64_t* main_launches, double* adv_ms,
@@ -1333,5 +1372,177 @@ extern "C" int fdm_diffusion_solve(int n_fibers, int64_t n_nodes, const int64_t*
                                diffusion_scheme == FDM_IMPLICIT_EULER, coef, n_nodes, st));
   FDM_CUDA(launch_diffusion_warp(n_fibers, d_fiber_offsets, coef, n_nodes, d_vm, fwd, st));
   FDM_CUDA(cudaStreamSynchronize(st));
+  return FDM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// compatibility export of the reference's generated-library ABI
+// (fast_monodomain_solver_gpu.tpp:361-365 initializeArrays, :478-481 computeMonodomain)
+// ---------------------------------------------------------------------------------------------
+namespace {
+struct Compat {
+  fdm_solver* s = nullptr;
+  int n_fibers = 0, n_per_fiber = 0, n_params = 0, rows = 0, cols = 0, n_jitter = 0;
+  int n_alg = 0, n_states_tr = 0;
+  std::vector<int> alg_idx, state_idx;
+  std::vector<float> last_params, last_lengths;
+  double last_prefactor = -1;
+  bool initialized = false;
+};
+Compat g_compat;
+std::mutex g_compat_mu;
+} // namespace
+
+extern "C" int fdm_compat_configure(int model, int n_fibers, int n_instances_per_fiber, int n_parameters_per_instance,
+                                    int firing_rows, int firing_cols, int n_jitter_per_fiber,
+                                    int n_algebraics_for_transfer, int n_states_for_transfer, int diffusion_scheme,
+                                    int approximate_exponential_function, int reaction_precision, int method)
+{
+  std::lock_guard<std::mutex> lock(g_compat_mu);
+  const ModelDesc* m = model_desc(model);
+  if (!m || n_fibers < 1 || n_instances_per_fiber < 2 || n_parameters_per_instance < 0 ||
+      n_parameters_per_instance > m->n_parameters || firing_rows < 1 || firing_cols < 1 || n_jitter_per_fiber < 0 ||
+      n_algebraics_for_transfer < 0 || n_states_for_transfer < 1)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_compat_configure: bad sizes");
+  if (g_compat.s) {
+    fdm_destroy(g_compat.s);
+    g_compat.s = nullptr;
+  }
+  fdm_config c;
+  fdm_config_default(&c);
+  c.model = model;
+  c.diffusion_scheme = diffusion_scheme;
+  c.approximate_exponential_function = approximate_exponential_function;
+  c.reaction_precision = reaction_precision;
+  c.method = method;
+  c.clamp_rule = FDM_CLAMP_CENTER; // the clamp set of the reference's GPU code
+  fdm_solver* s = nullptr;
+  int rc = fdm_create(&c, &s);
+  if (rc)
+    return rc;
+  g_compat = Compat();
+  g_compat.s = s;
+  g_compat.n_fibers = n_fibers;
+  g_compat.n_per_fiber = n_instances_per_fiber;
+  g_compat.n_params = n_parameters_per_instance;
+  g_compat.rows = firing_rows;
+  g_compat.cols = firing_cols;
+  g_compat.n_jitter = n_jitter_per_fiber;
+  g_compat.n_alg = n_algebraics_for_transfer;
+  g_compat.n_states_tr = n_states_for_transfer;
+  // fibers of equal length and unit element length until computeMonodomain passes the real lengths
+  std::vector<int64_t> off(n_fibers + 1);
+  for (int f = 0; f <= n_fibers; f++)
+    off[f] = (int64_t)f * n_instances_per_fiber;
+  std::vector<double> h((size_t)n_fibers * (n_instances_per_fiber - 1), 1.0), pf(n_fibers, 1.0);
+  return fdm_set_fibers(s, n_fibers, off.data(), h.data(), pf.data());
+}
+
+extern "C" void initializeArrays(const double* statesOneInstance, const int* algebraicsForTransferIndices,
+                                 const int* statesForTransferIndices, const char* firingEvents,
+                                 const double* setSpecificStatesFrequencyJitter, const int* motorUnitNo,
+                                 const int* fiberStimulationPointIndex, const double* lastStimulationCheckTime,
+                                 const double* setSpecificStatesCallFrequency,
+                                 const double* setSpecificStatesRepeatAfterFirstCall,
+                                 const double* setSpecificStatesCallEnableBegin)
+{
+  std::lock_guard<std::mutex> lock(g_compat_mu);
+  Compat& g = g_compat;
+  fdm_solver* s = g.s;
+  if (!s) {
+    fail(nullptr, FDM_ERR_ARG, "initializeArrays: call fdm_compat_configure first");
+    return;
+  }
+  const int NS = s->model->n_states;
+  const int64_t N = s->n_nodes;
+  std::vector<double> st((size_t)NS * N);
+  for (int k = 0; k < NS; k++)
+    std::fill(st.begin() + (size_t)k * N, st.begin() + (size_t)(k + 1) * N, statesOneInstance[k]);
+  if (fdm_set_states(s, st.data()))
+    return;
+  g.alg_idx.assign(algebraicsForTransferIndices, algebraicsForTransferIndices + g.n_alg);
+  g.state_idx.assign(statesForTransferIndices, statesForTransferIndices + g.n_states_tr);
+  if (fdm_set_algebraics_for_transfer(s, g.n_alg, g.alg_idx.data()))
+    return;
+  std::vector<uint8_t> fe((size_t)g.rows * g.cols);
+  for (size_t i = 0; i < fe.size(); i++)
+    fe[i] = firingEvents[i] ? 1 : 0;
+  if (fdm_set_stimulation(s, fe.data(), g.rows, g.cols, motorUnitNo, fiberStimulationPointIndex,
+                          setSpecificStatesCallFrequency, setSpecificStatesRepeatAfterFirstCall,
+                          setSpecificStatesCallEnableBegin, setSpecificStatesFrequencyJitter, g.n_jitter))
+    return;
+  // the caller's initial check times replace the default ones (initialization.tpp:344 computes the same)
+  if (cudaSetDevice(s->cfg.device) != cudaSuccess)
+    return;
+  cudaMemcpy(s->last_check.p, lastStimulationCheckTime, sizeof(double) * g.n_fibers, cudaMemcpyHostToDevice);
+  g.last_params.clear();
+  g.last_lengths.clear();
+  g.last_prefactor = -1;
+  g.initialized = true;
+}
+
+extern "C" void computeMonodomain(const float* parameters, double* algebraicsForTransfer, double* statesForTransfer,
+                                  const float* elementLengths, double startTime, double timeStepWidthSplitting,
+                                  int nTimeStepsSplitting, double dt0D, int nTimeSteps0D, double dt1D,
+                                  int nTimeSteps1D, double prefactor, double valueForStimulatedPoint)
+{
+  (void)nTimeSteps1D; // the reference solves once per split step with dt1D (gpu.tpp:622, compute.tpp:284)
+  std::lock_guard<std::mutex> lock(g_compat_mu);
+  Compat& g = g_compat;
+  fdm_solver* s = g.s;
+  if (!s || !g.initialized) {
+    fail(nullptr, FDM_ERR_ARG, "computeMonodomain: call fdm_compat_configure and initializeArrays first");
+    return;
+  }
+  if (cudaSetDevice(s->cfg.device) != cudaSuccess)
+    return;
+  const int64_t N = s->n_nodes;
+  const int NP = s->model->n_parameters;
+  // element lengths and prefactor (re-sent by the reference at every call)
+  const size_t ne = (size_t)g.n_fibers * (g.n_per_fiber - 1);
+  if (g.last_lengths.size() != ne || std::memcmp(g.last_lengths.data(), elementLengths, ne * sizeof(float)) ||
+      g.last_prefactor != prefactor) {
+    g.last_lengths.assign(elementLengths, elementLengths + ne);
+    g.last_prefactor = prefactor;
+    std::vector<double> h(ne), pf(g.n_fibers, prefactor);
+    for (size_t i = 0; i < ne; i++)
+      h[i] = elementLengths[i];
+    if (cudaMemcpy(s->elem_d.p, h.data(), sizeof(double) * ne, cudaMemcpyHostToDevice) != cudaSuccess)
+      return;
+    if (fdm_set_prefactor(s, pf.data()))
+      return;
+  }
+  // parameters: the caller's per-instance values fill the model's first parameter slots
+  const size_t npv = (size_t)g.n_params * N;
+  if (g.last_params.size() != npv || std::memcmp(g.last_params.data(), parameters, npv * sizeof(float))) {
+    g.last_params.assign(parameters, parameters + npv);
+    std::vector<double> p((size_t)NP * N);
+    for (int q = 0; q < NP; q++)
+      for (int64_t i = 0; i < N; i++)
+        p[(size_t)q * N + i] = q < g.n_params ? (double)parameters[(size_t)q * N + i] : s->model->parameter_defaults[q];
+    if (fdm_set_parameters(s, p.data()))
+      return;
+  }
+  s->cfg.value_for_stimulated_point = valueForStimulatedPoint;
+  if (advance_explicit(s, startTime, timeStepWidthSplitting, nTimeStepsSplitting, dt0D, nTimeSteps0D, dt1D))
+    return;
+  // transfer outputs (gpu.tpp:1086-1115 reads them as [k * nInstances + instance])
+  std::vector<double> st((size_t)s->model->n_states * N);
+  if (fdm_get_states(s, st.data()))
+    return;
+  for (int k = 0; k < g.n_states_tr; k++) {
+    const int idx = g.state_idx[k];
+    std::memcpy(statesForTransfer + (size_t)k * N, st.data() + (size_t)idx * N, sizeof(double) * N);
+  }
+  if (g.n_alg > 0 && algebraicsForTransfer)
+    fdm_get_algebraics(s, algebraicsForTransfer);
+}
+
+extern "C" int fdm_compat_release(void)
+{
+  std::lock_guard<std::mutex> lock(g_compat_mu);
+  if (g_compat.s)
+    fdm_destroy(g_compat.s);
+  g_compat = Compat();
   return FDM_OK;
 }

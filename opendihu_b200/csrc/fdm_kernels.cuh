@@ -198,15 +198,23 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __r
   const RR tr = (RR)t;
   model_rates<Model, RR, Math>(tr, y, P, r, alg);
   const RR dtr = (RR)dt;
-  const double vs = V + dt * (double)r[0];
-  ys[0] = (RR)vs;
+  if (Compensated<RR>::value) {
+    // FP32 reaction: y* only feeds the FP32 right-hand side, so Vm* is formed in FP32; the increment of Vm
+    // is formed in FP32 and accumulated into the FP64 Vm (one conversion each way per substep)
+    ys[0] = y[0] + dtr * r[0];
+  } else {
+    ys[0] = (RR)(V + dt * (double)r[0]);
+  }
 #pragma unroll
   for (int s = 1; s < NS; s++)
     ys[s] = y[s] + dtr * r[s];
   if (clamp)
     ys[0] = (RR)vstim;
   model_rates<Model, RR, Math>(tr, ys, P, r2, alg2);
-  V += 0.5 * dt * ((double)r[0] + (double)r2[0]);
+  if (Compensated<RR>::value)
+    V += (double)((RR)0.5 * dtr * (r[0] + r2[0]));
+  else
+    V += 0.5 * dt * ((double)r[0] + (double)r2[0]);
 #pragma unroll
   for (int s = 1; s < NS; s++)
     accumulate<RR>(S[s - 1], L[s - 1], (RR)0.5 * dtr * (r[s] + r2[s]));
@@ -688,12 +696,16 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
           if (tid * M + j >= nb)
             continue;
           const bool stim = cf[j] >= 0 && stim_bit(a.flags, a.words_per_fiber, cf[j], base + k);
-          RR Pk[NP];
+          if (stim && a.stimulus_mode == 1) {
+            // stimulus current: the junction nodes see the stimulus parameter while stimulated
+            RR Pk[NP];
 #pragma unroll
-          for (int p = 0; p < NP; p++)
-            Pk[p] = (stim && a.stimulus_mode == 1 && p == a.stimulus_parameter) ? (RR)a.stimulus_value : P[j][p];
-          const bool vclamp = stim && a.stimulus_mode == 0;
-          heun_step<Model, RR, Math, false>(V[j], S[j], L[j], Pk, t, s.dt0, vclamp, a.vstim, nullptr);
+            for (int p = 0; p < NP; p++)
+              Pk[p] = p == a.stimulus_parameter ? (RR)a.stimulus_value : P[j][p];
+            heun_step<Model, RR, Math, false>(V[j], S[j], L[j], Pk, t, s.dt0, false, a.vstim, nullptr);
+          } else {
+            heun_step<Model, RR, Math, false>(V[j], S[j], L[j], P[j], t, s.dt0, stim, a.vstim, nullptr);
+          }
         }
       }
       if (store_here) {
