@@ -144,6 +144,10 @@ int fdm_get_timing(const fdm_solver *s, double *main_kernel_ms, int64_t *main_ke
                    double *advance_ms, int64_t *kernel_launches);
 int fdm_reset_timing(fdm_solver *s);
 
+/* back to the start of the simulation: time-stepping state, Strang step counter and stimulation machine as
+ * right after fdm_set_stimulation (states and parameters are kept) */
+int fdm_rewind(fdm_solver *s);
+
 int fdm_checkpoint_save(fdm_solver *s);
 int fdm_checkpoint_restore(fdm_solver *s);
 
@@ -168,6 +172,23 @@ int fdm_diffusion_solve(int n_fibers, int64_t n_nodes, const int64_t *d_fiber_of
 int fdm_diffusion_solve_noalloc(int n_fibers, int64_t n_nodes, const int64_t *d_fiber_offsets,
                                 const double *d_element_lengths, const double *d_prefactor, double dt,
                                 int diffusion_scheme, double *d_vm, void *stream);
+
+/* ---- adjoint (no counterpart in the reference: the differentiation extension) ----------------------
+ * Discrete reverse mode of the FP64 split path (method FDM_METHOD_SPLIT, FDM_FP64).
+ * fdm_adjoint_forward: advances over [t_start, t_end] like fdm_advance, records Vm at the sensor nodes after
+ *   every Strang step (read with fdm_get_trace) and saves a checkpoint every checkpoint_every steps.
+ * fdm_adjoint_backward: given trace_grad[step * n_sensors + k] = dL/dVm(sensor k, after step), returns
+ *   dL/dprefactor[fiber], dL/dparameters[p * n_nodes + node] and dL/dstates(t_start)[s * n_nodes + node] (any of
+ *   the three may be NULL).  Each checkpoint segment is replayed storing every Heun substep's input state, then
+ *   reversed: Heun steps through the generated vector-Jacobian product of the model, the diffusion solve through
+ *   the transposed (= same, symmetric) tridiagonal system.  The solver then continues from the forward run's end. */
+int fdm_adjoint_forward(fdm_solver *s, double t_start, double t_end, int checkpoint_every, int n_sensors,
+                        const int64_t *sensor_nodes);
+int fdm_adjoint_backward(fdm_solver *s, const double *trace_grad, double *grad_prefactor, double *grad_parameters,
+                         double *grad_states0);
+int fdm_adjoint_release(fdm_solver *s);
+/* device time of the adjoint backward passes so far (ms) */
+int fdm_adjoint_timing(const fdm_solver *s, double *backward_ms);
 
 /* number of the fused-kernel shapes built into the library and their (threads, nodes per thread) */
 int fdm_fused_shapes(int *threads, int *nodes_per_thread, int capacity);

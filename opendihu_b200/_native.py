@@ -29,7 +29,8 @@ EXPORTED = [
     "fdm_get_clamp_nodes", "fdm_set_algebraics_for_transfer", "fdm_get_algebraics", "fdm_set_trace",
     "fdm_get_trace", "fdm_advance", "fdm_split_steps", "fdm_get_timing", "fdm_reset_timing",
     "fdm_checkpoint_save", "fdm_checkpoint_restore", "fdm_fused_shapes", "fdm_diffusion_solve",
-    "fdm_diffusion_solve_noalloc", "fdm_compat_configure", "fdm_compat_release",
+    "fdm_diffusion_solve_noalloc", "fdm_compat_configure", "fdm_compat_release", "fdm_adjoint_forward",
+    "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind",
 ]
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
@@ -101,6 +102,11 @@ def lib() -> C.CDLL:
         "fdm_diffusion_solve": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_diffusion_solve_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_compat_configure": (C.c_int, [C.c_int] * 13),
+        "fdm_adjoint_forward": (C.c_int, [P, C.c_double, C.c_double, C.c_int, C.c_int, i64]),
+        "fdm_adjoint_backward": (C.c_int, [P, d, d, d, d]),
+        "fdm_adjoint_release": (C.c_int, [P]),
+        "fdm_adjoint_timing": (C.c_int, [P, d]),
+        "fdm_rewind": (C.c_int, [P]),
         "fdm_compat_release": (C.c_int, []),
         "initializeArrays": (None, [d, i32, i32, C.c_char_p, d, i32, i32, d, d, d, d]),
         "computeMonodomain": (None, [C.POINTER(C.c_float), d, d, C.POINTER(C.c_float), C.c_double, C.c_double,

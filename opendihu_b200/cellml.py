@@ -725,6 +725,9 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
         out.append(f"#undef FDM_POW{n}")
     out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
     out.append("  }")
+    # reverse mode (adjoint)
+    out.append("  // vector-Jacobian product: LAM_STATES += J^T LAM_RATES, LAM_PARAMS += (dRATES/dPARAMS)^T LAM_RATES")
+    out.extend(emit_cuda_vjp(model, params_alg, params_const))
     out.append("};")
     out.append("")
     return "\n".join(out)
@@ -799,6 +802,41 @@ VARIANTS = [
 ]
 
 
+def _tree_to_json(e):
+    """Expression tree as nested lists (numbers keep their literal text)."""
+    if e[0] == "num":
+        return ["num", e[1]]
+    if e[0] == "var":
+        return ["var", e[1], e[2]]
+    if e[0] in ("neg", "pos", "not"):
+        return [e[0], _tree_to_json(e[1])]
+    if e[0] == "bin":
+        return ["bin", e[1], _tree_to_json(e[2]), _tree_to_json(e[3])]
+    if e[0] == "tern":
+        return ["tern", _tree_to_json(e[1]), _tree_to_json(e[2]), _tree_to_json(e[3])]
+    if e[0] == "call":
+        return ["call", e[1], [_tree_to_json(a) for a in e[2]]]
+    raise ValueError(e)
+
+
+def tree_from_json(j):
+    """Inverse of _tree_to_json (numbers get their double value back)."""
+    t = j[0]
+    if t == "num":
+        return ("num", j[1], float(j[1]))
+    if t == "var":
+        return ("var", j[1], j[2])
+    if t in ("neg", "pos", "not"):
+        return (t, tree_from_json(j[1]))
+    if t == "bin":
+        return ("bin", j[1], tree_from_json(j[2]), tree_from_json(j[3]))
+    if t == "tern":
+        return ("tern", tree_from_json(j[1]), tree_from_json(j[2]), tree_from_json(j[3]))
+    if t == "call":
+        return ("call", j[1], [tree_from_json(a) for a in j[2]])
+    raise ValueError(j)
+
+
 def generate_all(input_dir: str, cuda_dir: str, c_dir: str) -> List[str]:
     """(Re)generate the device and oracle model sources for every prebuilt variant."""
     written = []
@@ -822,7 +860,8 @@ def generate_all(input_dir: str, cuda_dir: str, c_dir: str) -> List[str]:
                        "constants": model.constants,
                        "state_names": model.state_names, "algebraic_names": model.algebraic_names,
                        "constant_names": model.constant_names, "uses_time": model.uses_voi,
-                       "operations_per_rhs": count_operations(model, pa, pc)},
+                       "operations_per_rhs": count_operations(model, pa, pc),
+                       "rhs_lines": [[k, i, _tree_to_json(e)] for k, i, e in substitute_parameters(model, pa, pc)]},
                       f, indent=1)
         written.append(meta)
     return written
@@ -878,3 +917,189 @@ def count_operations(model: Model, params_alg: Sequence[int] = (), params_const:
     for _, _, e in lines:
         walk(e)
     return c
+
+
+# ----------------------------------------------------------------------------------------------
+# reverse mode: vector-Jacobian product of the right-hand side (for the hand-written adjoint)
+# ----------------------------------------------------------------------------------------------
+
+class _VjpBuilder:
+    """Straight-line forward code with one temporary per operation, then the adjoint accumulation in
+    reverse order (classic reverse-mode differentiation of the expression DAG)."""
+
+    def __init__(self, consts, real="R"):
+        self.consts = consts
+        self.real = real
+        self.fwd: List[str] = []
+        self.ops: List[tuple] = []     # (temp name, op, operands, extra)
+        self.alg_temp: Dict[int, str] = {}
+        self.rate_temp: Dict[int, str] = {}
+        self.n = 0
+        self.plain = _Emitter(real, consts, "cuda")
+
+    def lit(self, v):
+        return ("lit", f"(({self.real}){_hexf(v)})", None)
+
+    def leaf(self, e):
+        t = e[0]
+        if t == "num":
+            return ("lit", f"(({self.real}){e[1]})", None)
+        k, i = e[1], e[2]
+        if k == "C":
+            return self.lit(self.consts[i])
+        if k == "S":
+            return ("ref", f"STATES[{i}]", f"LAM_STATES[{i}]")
+        if k == "P":
+            return ("ref", f"PARAMS[{i}]", f"LAM_PARAMS[{i}]")
+        if k == "T":
+            return ("ref", "VOI", None)
+        if k == "A":
+            tn = self.alg_temp[i]
+            return ("ref", tn, "a_" + tn)
+        if k == "R":
+            tn = self.rate_temp[i]
+            return ("ref", tn, "a_" + tn)
+        raise ValueError(e)
+
+    def temp(self, op, operands, expr_text, extra=None):
+        name = f"t{self.n}"
+        self.n += 1
+        self.fwd.append(f"    const {self.real} {name} = {expr_text};")
+        self.ops.append((name, op, operands, extra))
+        return ("ref", name, "a_" + name)
+
+    def build(self, e):
+        t = e[0]
+        if t in ("num", "var"):
+            return self.leaf(e)
+        if t == "pos":
+            return self.build(e[1])
+        if t == "neg":
+            a = self.build(e[1])
+            return self.temp("neg", [a], f"(-{a[1]})")
+        if t == "bin":
+            op = e[1]
+            if op in "+-*/":
+                a = self.build(e[2])
+                b = self.build(e[3])
+                return self.temp(op, [a, b], f"({a[1]} {op} {b[1]})")
+            raise ValueError("comparison outside a condition")
+        if t == "tern":
+            cond = self.plain.expr(e[1]).replace("ALGEBRAIC[", "ALG[")
+            a = self.build(e[2])
+            b = self.build(e[3])
+            cname = f"c{self.n}"
+            self.fwd.append(f"    const bool {cname} = ({cond});")
+            return self.temp("tern", [a, b], f"({cname} ? {a[1]} : {b[1]})", cname)
+        if t == "call":
+            f = e[1]
+            if f == "pow":
+                n = _int_exponent(e[2][1])
+                a = self.build(e[2][0])
+                if n is not None:
+                    if n > 0:
+                        return self.temp(("powi", n), [a], f"FDM_POW{n}({a[1]})")
+                    return self.temp(("powi", n), [a], f"(({self.real})1.0/FDM_POW{-n}({a[1]}))")
+                b = self.build(e[2][1])
+                return self.temp("pow", [a, b], f"M::pow({a[1]}, {b[1]})")
+            a = self.build(e[2][0])
+            if f == "exp":
+                return self.temp("exp", [a], f"M::exp({a[1]})")
+            if f == "log":
+                return self.temp("log", [a], f"M::log({a[1]})")
+            if f == "fabs":
+                return self.temp("fabs", [a], f"fabs({a[1]})")
+            if f == "sqrt":
+                return self.temp("sqrt", [a], f"sqrt({a[1]})")
+        raise ValueError(f"unsupported node {e}")
+
+    def backward(self):
+        out = []
+        R = self.real
+        for name, op, ops, extra in reversed(self.ops):
+            a = "a_" + name
+
+            def acc(o, term):
+                if o[2] is not None:
+                    out.append(f"    {o[2]} += {term};")
+            if op == "+":
+                acc(ops[0], a)
+                acc(ops[1], a)
+            elif op == "-":
+                acc(ops[0], a)
+                acc(ops[1], f"-{a}")
+            elif op == "*":
+                acc(ops[0], f"{a} * {ops[1][1]}")
+                acc(ops[1], f"{a} * {ops[0][1]}")
+            elif op == "/":
+                acc(ops[0], f"{a} / {ops[1][1]}")
+                acc(ops[1], f"-{a} * {name} / {ops[1][1]}")
+            elif op == "neg":
+                acc(ops[0], f"-{a}")
+            elif op == "exp":
+                acc(ops[0], f"{a} * M::dexp({ops[0][1]}, {name})")
+            elif op == "log":
+                acc(ops[0], f"{a} * M::dlog({ops[0][1]}, {name})")
+            elif op == "fabs":
+                acc(ops[0], f"({ops[0][1]} >= ({R})0 ? {a} : -{a})")
+            elif op == "sqrt":
+                acc(ops[0], f"{a} * ({R})0.5 / {name}")
+            elif op == "pow":
+                acc(ops[0], f"{a} * {ops[1][1]} * {name} / {ops[0][1]}")
+                acc(ops[1], f"{a} * {name} * M::log({ops[0][1]})")
+            elif op == "tern":
+                acc(ops[0], f"({extra} ? {a} : ({R})0)")
+                acc(ops[1], f"({extra} ? ({R})0 : {a})")
+            elif isinstance(op, tuple) and op[0] == "powi":
+                n = op[1]
+                x = ops[0][1]
+                if n > 0:
+                    d = f"(({R}){n})" if n == 1 else (f"(({R}){n} * {x})" if n == 2 else f"(({R}){n} * FDM_POW{n - 1}({x}))")
+                    if n == 1:
+                        d = f"(({R})1)"
+                    acc(ops[0], f"{a} * {d}")
+                else:
+                    acc(ops[0], f"{a} * (({R}){n}) * {name} / {x}")
+            else:
+                raise ValueError(op)
+        return out
+
+
+def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> List[str]:
+    """Lines of the member function ``rates_vjp<R, M>`` (to be placed inside the model struct):
+    given STATES, PARAMS and LAM_RATES it evaluates the right-hand side and adds J^T LAM_RATES to
+    LAM_STATES and (dRATES/dPARAMS)^T LAM_RATES to LAM_PARAMS."""
+    lines = substitute_parameters(model, params_alg, params_const)
+    b = _VjpBuilder(model.constants)
+    for kind, idx, expr in lines:
+        r = b.build(expr)
+        if r[0] == "lit" or (r[0] == "ref" and not r[1].startswith("t")):
+            r = b.temp("+", [r, b.lit(0.0)], f"({r[1]} + (({b.real})0))")
+        if kind == "A":
+            b.alg_temp[idx] = r[1]
+            b.fwd.append(f"    ALG[{idx}] = {r[1]};")
+        else:
+            b.rate_temp[idx] = r[1]
+    out = []
+    out.append("  template<class R, class M>")
+    out.append("  __device__ __forceinline__ static void rates_vjp(const R VOI, const R* __restrict__ STATES,"
+               " const R* __restrict__ PARAMS, const R* __restrict__ LAM_RATES, R* __restrict__ LAM_STATES,"
+               " R* __restrict__ LAM_PARAMS)")
+    out.append("  {")
+    out.append("    (void)VOI; (void)PARAMS;")
+    pows = _collect_int_pows(lines)
+    pows_vjp = sorted(set(pows) | {n - 1 for n in pows if n > 2})
+    for n in pows_vjp:
+        out.append("#define " + _pow_macro_defs([n])[0].split("#define ", 1)[1])
+    out.append(f"    R ALG[{max(model.n_algebraics, 1)}];")
+    out.append("    (void)ALG;")
+    out.extend(b.fwd)
+    for name, *_ in b.ops:
+        out.append(f"    R a_{name} = (R)0;")
+    for idx, tn in sorted(b.rate_temp.items()):
+        out.append(f"    a_{tn} += LAM_RATES[{idx}];")
+    out.extend(b.backward())
+    for n in pows_vjp:
+        out.append(f"#undef FDM_POW{n}")
+    out.append("  }")
+    return out

@@ -122,11 +122,13 @@ struct fdm_solver {
   DevBuf<int> jitter_idx;
   DevBuf<uint32_t> flags;
   DevBuf<SplitStep> steps_d;
-  SplitStep* steps_h = nullptr;   // pinned, 2 slots
+  SplitStep* steps_h = nullptr;   // pinned, 2 slots of step_capacity
+  int step_capacity = 0;
   cudaEvent_t slot_ev[2] = {nullptr, nullptr};
   int slot = 0;
   int firing_rows = 0, firing_cols = 0, n_jitter = 0;
   bool stimulation_set = false;
+  std::vector<double> stim_freq, stim_begin; // for rewinding the stimulation machine
 
   // checkpoint
   DevBuf<double> ck_vm, ck_last, ck_jit;
@@ -150,10 +152,35 @@ struct fdm_solver {
   int n_trace = 0;
   int64_t trace_capacity = 0;
 
+  // adjoint (checkpointed forward, replay + reverse)
+  struct Adjoint {
+    bool ready = false;
+    int kc = 0, n_seg = 0, n_sensors = 0, n0max = 1;
+    std::vector<SplitStep> steps;
+    std::vector<double> dt1s;
+    DevBuf<double> ck_vm, ck_states, ck_last, ck_jit, fin_vm, fin_states, fin_last, fin_jit;
+    DevBuf<int> ck_jidx, fin_jidx;
+    DevBuf<uint8_t> ck_hbs, fin_hbs;
+    Tss fin_strang, fin_heun, fin_diff;
+    int64_t fin_split = 0;
+    DevBuf<double> H, U, X, lam, gP, gpf, mu, tgrad;
+    void release()
+    {
+      for (auto* b : {&ck_vm, &ck_states, &ck_last, &ck_jit, &fin_vm, &fin_states, &fin_last, &fin_jit, &H, &U, &X,
+                      &lam, &gP, &gpf, &mu, &tgrad})
+        b->release();
+      ck_jidx.release();
+      fin_jidx.release();
+      ck_hbs.release();
+      fin_hbs.release();
+      ready = false;
+    }
+  } adj;
+
   // timing
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
-  double main_ms = 0, adv_ms = 0;
+  double main_ms = 0, adv_ms = 0, adj_ms = 0;
   int64_t main_launches = 0, launches = 0;
   cudaEvent_t adv_start = nullptr, adv_stop = nullptr;
 };
@@ -315,6 +342,7 @@ extern "C" int fdm_create(const fdm_config* cfg, fdm_solver** out)
     e = cudaEventCreate(&s->adv_stop);
   if (e == cudaSuccess)
     e = s->steps_d.alloc(s->cfg.steps_per_launch);
+  s->step_capacity = s->cfg.steps_per_launch;
   if (e == cudaSuccess)
     e = s->nonfinite.alloc(1);
   if (e != cudaSuccess) {
@@ -352,6 +380,7 @@ extern "C" int fdm_destroy(fdm_solver* s)
   s->ck_hbs.release();
   s->flags.release();
   s->steps_d.release();
+  s->adj.release();
   if (s->steps_h)
     cudaFreeHost(s->steps_h);
   for (auto ev : s->slot_ev)
@@ -814,6 +843,8 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
     if (n_jitter > 0)
       FDM_CUDA(cudaMemcpyAsync(s->jitter.p, jitter, sizeof(double) * nf * n_jitter, cudaMemcpyHostToDevice,
                                s->stream));
+    s->stim_freq.assign(call_frequency, call_frequency + nf);
+    s->stim_begin.assign(call_enable_begin, call_enable_begin + nf);
     // initial machine state (initialization.tpp:342-344)
     std::vector<double> last(nf), cj(nf, 0.0);
     std::vector<int> ji(nf, 0);
@@ -954,29 +985,45 @@ static int ensure_coefficients(fdm_solver* s, double dt1)
   return FDM_OK;
 }
 
-static int run_window(fdm_solver* s, int n_steps, double dt1, bool store_alg)
+struct WindowInfo {
+  int words = 0, nsub = 1;
+};
+
+static int ensure_step_capacity(fdm_solver* s, int n)
 {
-  if (n_steps == 0 || s->n_fibers == 0)
+  if (n <= s->step_capacity)
     return FDM_OK;
-  int rc = ensure_coefficients(s, dt1);
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  if (s->steps_h)
+    FDM_CUDA(cudaFreeHost(s->steps_h));
+  s->steps_h = nullptr;
+  FDM_CUDA(cudaMallocHost((void**)&s->steps_h, sizeof(SplitStep) * 2 * (size_t)n));
+  FDM_CUDA(s->steps_d.alloc(n));
+  s->step_capacity = n;
+  return FDM_OK;
+}
+
+// uploads a window of split steps (through a pinned slot) and runs the stimulation schedule for it
+static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, WindowInfo* wi)
+{
+  int rc = ensure_step_capacity(s, n_steps);
   if (rc)
     return rc;
-  // upload the window's split steps from a pinned slot (wait until the slot's previous copy finished)
   const int slot = s->slot;
   s->slot ^= 1;
   FDM_CUDA(cudaEventSynchronize(s->slot_ev[slot]));
-  SplitStep* hs = s->steps_h + (size_t)slot * s->cfg.steps_per_launch;
-  // (filled by the caller into s->steps_h slot area before; copy from the staging vector)
-  (void)hs;
+  SplitStep* hs = s->steps_h + (size_t)slot * s->step_capacity;
+  std::memcpy(hs, host_steps, sizeof(SplitStep) * n_steps);
   int nsub = 1;
   for (int j = 0; j < n_steps; j++)
     nsub = std::max(nsub, hs[j].n0);
   const int bits = n_steps * 2 * nsub;
   const int words = (bits + 31) / 32;
-  FDM_CUDA(s->flags.alloc((size_t)words * s->n_fibers));
+  FDM_CUDA(s->flags.alloc((size_t)words * std::max(s->n_fibers, 1)));
   FDM_CUDA(cudaMemcpyAsync(s->steps_d.p, hs, sizeof(SplitStep) * n_steps, cudaMemcpyHostToDevice, s->stream));
   FDM_CUDA(cudaEventRecord(s->slot_ev[slot], s->stream));
-
+  wi->words = words;
+  wi->nsub = nsub;
   StimArgs sa{};
   sa.firing_events = s->firing.p;
   sa.rows = s->firing_rows;
@@ -998,6 +1045,21 @@ static int run_window(fdm_solver* s, int n_steps, double dt1, bool store_alg)
   sa.n_fibers = s->n_fibers;
   FDM_CUDA(launch_schedule(sa, s->steps_d.p, n_steps, s->stream));
   s->launches++;
+  return FDM_OK;
+}
+
+static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, double dt1, bool store_alg)
+{
+  if (n_steps == 0 || s->n_fibers == 0)
+    return FDM_OK;
+  int rc = ensure_coefficients(s, dt1);
+  if (rc)
+    return rc;
+  WindowInfo wi;
+  rc = prepare_window(s, host_steps, n_steps, &wi);
+  if (rc)
+    return rc;
+  const int words = wi.words, nsub = wi.nsub;
 
   const RealKind rk = s->real_bytes == 8 ? REAL_F64 : REAL_F32;
   const MathKind mk = s->cfg.approximate_exponential_function ? MATH_APPROX : MATH_EXACT;
@@ -1095,20 +1157,12 @@ static int run_window(fdm_solver* s, int n_steps, double dt1, bool store_alg)
   return FDM_OK;
 }
 
-extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
+// The split steps of RepeatedCall<FastMonodomainSolver>::advanceTimeSpan over [t_start, t_end]
+// (repeated_call.tpp:43-75, fast_monodomain_solver_compute.tpp:64-129), with the time-step objects'
+// state carried from call to call as the reference's scheme objects carry it.
+static void plan_advance(fdm_solver* s, double t_start, double t_end, std::vector<SplitStep>& steps,
+                         std::vector<double>& dt1s)
 {
-  if (!s)
-    return fail(s, FDM_ERR_ARG, "fdm_advance: null solver");
-  FDM_BIND(s);
-  if (!(t_end >= t_start))
-    return fail(s, FDM_ERR_ARG, "fdm_advance: t_end must be >= t_start");
-  if (s->n_fibers > 0 && !s->stimulation_set)
-    return fail(s, FDM_ERR_ARG, "fdm_advance: call fdm_set_stimulation first");
-  s->ev_used = 0;
-  FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
-  const int64_t launches0 = s->launches;
-
-  // RepeatedCall (repeated_call.tpp:43-75)
   Tss rc;
   rc.init(t_start, t_end, s->cfg.dt_repeated_call);
   rc.set_dt(s->cfg.dt_repeated_call);
@@ -1119,9 +1173,6 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
     s->diff.init(t_start, t_start + s->cfg.dt_1d, s->cfg.dt_1d);
     s->tss_init = true;
   }
-  const int K = s->cfg.steps_per_launch;
-  int filled = 0;
-  double window_dt1 = 0;
   double t = rc.start;
   for (int k = 0; k < rc.n;) {
     s->strang.set_span(t, t + rc.dt);
@@ -1130,19 +1181,8 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
     const int ns = s->strang.n;
     s->heun.set_span(start, start + 0.5 * dts);
     s->diff.set_span(start, start + dts);
-    const double dt1 = s->diff.dt;
     for (int j = 0; j < ns; j++) {
-      if (filled > 0 && (filled == K || std::fabs(dt1 - window_dt1) > 1e-12 * std::fabs(window_dt1))) {
-        int r2 = run_window(s, filled, window_dt1, false);
-        if (r2)
-          return r2;
-        filled = 0;
-      }
-      if (filled == 0) {
-        window_dt1 = dt1;
-        FDM_CUDA(cudaEventSynchronize(s->slot_ev[s->slot]));
-      }
-      SplitStep& st = s->steps_h[(size_t)s->slot * K + filled];
+      SplitStep st;
       const double tc = start + j * dts;
       st.t = tc;
       st.mid = tc + 0.5 * dts;
@@ -1150,14 +1190,34 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
       st.n0 = s->heun.n;
       st.global_no = (int)std::min<int64_t>(s->split_no, 2147483647);
       s->split_no++;
-      filled++;
+      steps.push_back(st);
+      dt1s.push_back(s->diff.dt);
     }
     k++;
     t = rc.start + (double)k / rc.n * span;
   }
-  int r3 = run_window(s, filled, window_dt1, true);
-  if (r3)
-    return r3;
+}
+
+// runs planned steps in windows of at most steps_per_launch steps that share the diffusion step width
+static int run_planned(fdm_solver* s, const std::vector<SplitStep>& steps, const std::vector<double>& dt1s,
+                       size_t begin, size_t end, bool store_at_end)
+{
+  const int K = s->cfg.steps_per_launch;
+  size_t w0 = begin;
+  while (w0 < end) {
+    size_t w1 = w0 + 1;
+    while (w1 < end && (int)(w1 - w0) < K && std::fabs(dt1s[w1] - dt1s[w0]) <= 1e-12 * std::fabs(dt1s[w0]))
+      w1++;
+    int r = run_window(s, steps.data() + w0, (int)(w1 - w0), dt1s[w0], store_at_end && w1 == end);
+    if (r)
+      return r;
+    w0 = w1;
+  }
+  return FDM_OK;
+}
+
+static int finish_advance(fdm_solver* s)
+{
   FDM_CUDA(cudaEventRecord(s->adv_stop, s->stream));
   if (s->cfg.check_nan && s->n_nodes > 0) {
     FDM_CUDA(cudaMemsetAsync(s->nonfinite.p, 0, sizeof(int), s->stream));
@@ -1173,7 +1233,6 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
     s->main_ms += m2;
     s->main_launches++;
   }
-  (void)launches0;
   if (s->cfg.check_nan && s->n_nodes > 0) {
     int bad = 0;
     FDM_CUDA(cudaMemcpy(&bad, s->nonfinite.p, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1183,6 +1242,26 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
   return FDM_OK;
 }
 
+extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
+{
+  if (!s)
+    return fail(s, FDM_ERR_ARG, "fdm_advance: null solver");
+  FDM_BIND(s);
+  if (!(t_end >= t_start))
+    return fail(s, FDM_ERR_ARG, "fdm_advance: t_end must be >= t_start");
+  if (s->n_fibers > 0 && !s->stimulation_set)
+    return fail(s, FDM_ERR_ARG, "fdm_advance: call fdm_set_stimulation first");
+  s->ev_used = 0;
+  FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
+  std::vector<SplitStep> steps;
+  std::vector<double> dt1s;
+  plan_advance(s, t_start, t_end, steps, dt1s);
+  int r = run_planned(s, steps, dt1s, 0, steps.size(), true);
+  if (r)
+    return r;
+  return finish_advance(s);
+}
+
 // Strang steps given explicitly, as the reference's generated computeMonodomain receives them
 // (fast_monodomain_solver_gpu.tpp:478-481, 505-515): currentTime = startTime + j*dtSplit, substeps at
 // currentTime + k*dt0D and midTime + k*dt0D, one diffusion solve with dt1D per step.
@@ -1190,36 +1269,21 @@ static int advance_explicit(fdm_solver* s, double start, double dts, int ns, dou
 {
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
-  const int K = s->cfg.steps_per_launch;
-  int filled = 0;
+  std::vector<SplitStep> steps(ns);
+  std::vector<double> dt1s(ns, dt1);
   for (int j = 0; j < ns; j++) {
-    if (filled == K) {
-      int r = run_window(s, filled, dt1, false);
-      if (r)
-        return r;
-      filled = 0;
-    }
-    if (filled == 0)
-      FDM_CUDA(cudaEventSynchronize(s->slot_ev[s->slot]));
-    SplitStep& st = s->steps_h[(size_t)s->slot * K + filled];
     const double tc = start + j * dts;
-    st.t = tc;
-    st.mid = tc + 0.5 * dts;
-    st.dt0 = dt0;
-    st.n0 = n0;
-    st.global_no = (int)std::min<int64_t>(s->split_no, 2147483647);
+    steps[j].t = tc;
+    steps[j].mid = tc + 0.5 * dts;
+    steps[j].dt0 = dt0;
+    steps[j].n0 = n0;
+    steps[j].global_no = (int)std::min<int64_t>(s->split_no, 2147483647);
     s->split_no++;
-    filled++;
   }
-  int r = run_window(s, filled, dt1, true);
+  int r = run_planned(s, steps, dt1s, 0, steps.size(), true);
   if (r)
     return r;
-  FDM_CUDA(cudaEventRecord(s->adv_stop, s->stream));
-  FDM_CUDA(cudaStreamSynchronize(s->stream));
-  float ms = 0;
-  FDM_CUDA(cudaEventElapsedTime(&ms, s->adv_start, s->adv_stop));
-  s->adv_ms += ms;
-  return FDM_OK;
+  return finish_advance(s);
 }
 
 extern "C" int64_t fdm_split_steps(const fdm_solver* s) { return s ? s->split_no : 0; }
@@ -1244,7 +1308,7 @@ extern "C" int fdm_reset_timing(fdm_solver* s)
 {
   if (!s)
     return FDM_ERR_ARG;
-  s->main_ms = s->adv_ms = 0;
+  s->main_ms = s->adv_ms = s->adj_ms = 0;
   s->main_launches = s->launches = 0;
   return FDM_OK;
 }
@@ -1544,5 +1608,295 @@ extern "C" int fdm_compat_release(void)
   if (g_compat.s)
     fdm_destroy(g_compat.s);
   g_compat = Compat();
+  return FDM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// adjoint: discrete reverse mode of the FP64 split path with checkpointing
+// ---------------------------------------------------------------------------------------------
+
+// device copies of the evolving state: Vm, the other states (FP64) and the stimulation machine
+static int copy_state(fdm_solver* s, double* vm, double* st, double* last, double* jit, int* jidx, uint8_t* hbs,
+                      bool to_snapshot)
+{
+  const int64_t N = s->n_nodes;
+  const int NS = s->model->n_states;
+  const int nf = s->n_fibers;
+  auto cp = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s->stream);
+  };
+  if (to_snapshot) {
+    FDM_CUDA(cp(vm, s->vm.p, sizeof(double) * N));
+    if (NS > 1)
+      FDM_CUDA(cp(st, s->states.p, sizeof(double) * N * (NS - 1)));
+    FDM_CUDA(cp(last, s->last_check.p, sizeof(double) * nf));
+    FDM_CUDA(cp(jit, s->cur_jitter.p, sizeof(double) * nf));
+    FDM_CUDA(cp(jidx, s->jitter_idx.p, sizeof(int) * nf));
+    FDM_CUDA(cp(hbs, s->hbs.p, nf));
+  } else {
+    FDM_CUDA(cp(s->vm.p, vm, sizeof(double) * N));
+    if (NS > 1)
+      FDM_CUDA(cp(s->states.p, st, sizeof(double) * N * (NS - 1)));
+    FDM_CUDA(cp(s->last_check.p, last, sizeof(double) * nf));
+    FDM_CUDA(cp(s->cur_jitter.p, jit, sizeof(double) * nf));
+    FDM_CUDA(cp(s->jitter_idx.p, jidx, sizeof(int) * nf));
+    FDM_CUDA(cp(s->hbs.p, hbs, nf));
+  }
+  return FDM_OK;
+}
+
+extern "C" int fdm_adjoint_forward(fdm_solver* s, double t_start, double t_end, int checkpoint_every, int n_sensors,
+                                   const int64_t* sensor_nodes)
+{
+  if (!s || checkpoint_every < 1 || n_sensors < 0 || (n_sensors > 0 && !sensor_nodes))
+    return fail(s, FDM_ERR_ARG, "fdm_adjoint_forward: bad argument");
+  FDM_BIND(s);
+  if (s->cfg.method != FDM_METHOD_SPLIT || s->real_bytes != 8)
+    return fail(s, FDM_ERR_UNSUPPORTED, "fdm_adjoint_forward: the adjoint runs on the FP64 split path "
+                                        "(method FDM_METHOD_SPLIT, reaction_precision FDM_FP64)");
+  if (s->n_fibers == 0 || !s->stimulation_set)
+    return fail(s, FDM_ERR_ARG, "fdm_adjoint_forward: set fibers and stimulation first");
+  auto& A = s->adj;
+  A.release();
+  A.steps.clear();
+  A.dt1s.clear();
+  plan_advance(s, t_start, t_end, A.steps, A.dt1s);
+  const int64_t NT = (int64_t)A.steps.size();
+  for (int64_t j = 0; j < NT; j++)
+    A.steps[j].global_no = (int)j; // trace rows of this run
+  int rc = fdm_set_trace(s, n_sensors, sensor_nodes, NT);
+  if (rc)
+    return rc;
+  const int64_t N = s->n_nodes;
+  const int NS = s->model->n_states;
+  const int nf = s->n_fibers;
+  A.kc = checkpoint_every;
+  A.n_seg = (int)((NT + A.kc - 1) / A.kc);
+  A.n_sensors = n_sensors;
+  A.n0max = 1;
+  for (auto& st : A.steps)
+    A.n0max = std::max(A.n0max, st.n0);
+  const size_t segs = std::max(A.n_seg, 1);
+  FDM_CUDA(A.ck_vm.alloc(segs * N));
+  FDM_CUDA(A.ck_states.alloc(segs * N * std::max(NS - 1, 1)));
+  FDM_CUDA(A.ck_last.alloc(segs * nf));
+  FDM_CUDA(A.ck_jit.alloc(segs * nf));
+  FDM_CUDA(A.ck_jidx.alloc(segs * nf));
+  FDM_CUDA(A.ck_hbs.alloc(segs * nf));
+  FDM_CUDA(A.fin_vm.alloc(N));
+  FDM_CUDA(A.fin_states.alloc((size_t)N * std::max(NS - 1, 1)));
+  FDM_CUDA(A.fin_last.alloc(nf));
+  FDM_CUDA(A.fin_jit.alloc(nf));
+  FDM_CUDA(A.fin_jidx.alloc(nf));
+  FDM_CUDA(A.fin_hbs.alloc(nf));
+  s->ev_used = 0;
+  FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
+  for (int c = 0; c < A.n_seg; c++) {
+    rc = copy_state(s, A.ck_vm.p + (size_t)c * N, A.ck_states.p + (size_t)c * N * (NS - 1), A.ck_last.p + (size_t)c * nf,
+                    A.ck_jit.p + (size_t)c * nf, A.ck_jidx.p + (size_t)c * nf, A.ck_hbs.p + (size_t)c * nf, true);
+    if (rc)
+      return rc;
+    const size_t b = (size_t)c * A.kc, e = std::min<size_t>(b + A.kc, NT);
+    rc = run_planned(s, A.steps, A.dt1s, b, e, c == A.n_seg - 1);
+    if (rc)
+      return rc;
+  }
+  rc = copy_state(s, A.fin_vm.p, A.fin_states.p, A.fin_last.p, A.fin_jit.p, A.fin_jidx.p, A.fin_hbs.p, true);
+  if (rc)
+    return rc;
+  A.fin_strang = s->strang;
+  A.fin_heun = s->heun;
+  A.fin_diff = s->diff;
+  A.fin_split = s->split_no;
+  rc = finish_advance(s);
+  if (rc)
+    return rc;
+  A.ready = true;
+  return FDM_OK;
+}
+
+extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, double* grad_prefactor,
+                                    double* grad_parameters, double* grad_states0)
+{
+  if (!s || !trace_grad)
+    return fail(s, FDM_ERR_ARG, "fdm_adjoint_backward: bad argument");
+  FDM_BIND(s);
+  auto& A = s->adj;
+  if (!A.ready)
+    return fail(s, FDM_ERR_ARG, "fdm_adjoint_backward: call fdm_adjoint_forward first");
+  const int64_t N = s->n_nodes;
+  const int NS = s->model->n_states;
+  const int NP = s->model->n_parameters;
+  const int nf = s->n_fibers;
+  const int64_t NT = (int64_t)A.steps.size();
+  const size_t hstride = (size_t)A.n0max * NS * N; // one half step of stored substep states
+  FDM_CUDA(A.H.alloc((size_t)A.kc * 2 * hstride));
+  FDM_CUDA(A.U.alloc((size_t)A.kc * N));
+  FDM_CUDA(A.X.alloc((size_t)A.kc * N));
+  FDM_CUDA(A.lam.alloc((size_t)NS * N));
+  FDM_CUDA(A.gP.alloc((size_t)std::max(NP, 1) * N));
+  FDM_CUDA(A.gpf.alloc(nf));
+  FDM_CUDA(A.mu.alloc(N));
+  FDM_CUDA(A.tgrad.alloc(std::max<size_t>((size_t)NT * A.n_sensors, 1)));
+  FDM_CUDA(cudaMemsetAsync(A.lam.p, 0, sizeof(double) * NS * N, s->stream));
+  FDM_CUDA(cudaMemsetAsync(A.gP.p, 0, sizeof(double) * std::max(NP, 1) * N, s->stream));
+  FDM_CUDA(cudaMemsetAsync(A.gpf.p, 0, sizeof(double) * nf, s->stream));
+  if (NT * A.n_sensors > 0)
+    FDM_CUDA(cudaMemcpyAsync(A.tgrad.p, trace_grad, sizeof(double) * NT * A.n_sensors, cudaMemcpyHostToDevice,
+                             s->stream));
+  const MathKind mk = s->cfg.approximate_exponential_function ? MATH_APPROX : MATH_EXACT;
+  const int ie = s->cfg.diffusion_scheme == FDM_IMPLICIT_EULER;
+  s->ev_used = 0;
+  FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
+  for (int c = A.n_seg - 1; c >= 0; c--) {
+    int rc = copy_state(s, A.ck_vm.p + (size_t)c * N, A.ck_states.p + (size_t)c * N * (NS - 1),
+                        A.ck_last.p + (size_t)c * nf, A.ck_jit.p + (size_t)c * nf, A.ck_jidx.p + (size_t)c * nf,
+                        A.ck_hbs.p + (size_t)c * nf, false);
+    if (rc)
+      return rc;
+    const size_t b = (size_t)c * A.kc, e = std::min<size_t>(b + A.kc, NT);
+    const int len = (int)(e - b);
+    rc = ensure_coefficients(s, A.dt1s[b]);
+    if (rc)
+      return rc;
+    WindowInfo wi;
+    rc = prepare_window(s, A.steps.data() + b, len, &wi);
+    if (rc)
+      return rc;
+    // replay the segment, storing every substep's input state and Vm before/after each diffusion solve
+    ReactionArgs ra{};
+    ra.n_nodes = N;
+    ra.stride = N;
+    ra.vm = s->vm.p;
+    ra.states = s->states.p;
+    ra.params = s->params.p;
+    ra.clamp_fiber = s->clamp_fiber.p;
+    ra.flags = s->flags.p;
+    ra.words_per_fiber = wi.words;
+    ra.nsub_stride = wi.nsub;
+    ra.vstim = s->cfg.value_for_stimulated_point;
+    ra.stimulus_mode = s->cfg.stimulus_mode;
+    ra.stimulus_parameter = s->cfg.stimulus_parameter;
+    ra.stimulus_value = s->cfg.stimulus_value;
+    ra.steps = s->steps_d.p;
+    for (int jj = 0; jj < len; jj++) {
+      rc = ensure_coefficients(s, A.dt1s[b + jj]);
+      if (rc)
+        return rc;
+      ra.step = jj;
+      for (int half = 0; half < 2; half++) {
+        ra.half = half;
+        ra.store_states = A.H.p + ((size_t)jj * 2 + half) * hstride;
+        FDM_CUDA(launch_reaction(s->cfg.model, REAL_F64, mk, ra, s->stream));
+        s->launches++;
+        if (half == 0) {
+          FDM_CUDA(cudaMemcpyAsync(A.U.p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+                                   s->stream));
+          FDM_CUDA(launch_diffusion_warp(nf, s->off_d.p, s->coef.p, N, s->vm.p, s->scratch.p, s->stream));
+          s->launches++;
+          FDM_CUDA(cudaMemcpyAsync(A.X.p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+                                   s->stream));
+        }
+      }
+    }
+    // reverse the segment
+    AdjointArgs aa{};
+    aa.n_nodes = N;
+    aa.params = (const double*)s->params.p;
+    aa.lam = A.lam.p;
+    aa.grad_params = A.gP.p;
+    aa.clamp_fiber = s->clamp_fiber.p;
+    aa.flags = s->flags.p;
+    aa.words_per_fiber = wi.words;
+    aa.nsub_stride = wi.nsub;
+    aa.vstim = s->cfg.value_for_stimulated_point;
+    aa.stimulus_mode = s->cfg.stimulus_mode;
+    aa.stimulus_parameter = s->cfg.stimulus_parameter;
+    aa.stimulus_value = s->cfg.stimulus_value;
+    aa.trace_slot = A.n_sensors > 0 ? s->trace_slot.p : nullptr;
+    aa.trace_grad = A.tgrad.p;
+    aa.n_trace = A.n_sensors;
+    for (int jj = len - 1; jj >= 0; jj--) {
+      const size_t j = b + jj;
+      aa.step = A.steps[j];
+      aa.step_in_window = jj;
+      aa.half = 1;
+      aa.trace_row = (int64_t)j;
+      aa.states = A.H.p + ((size_t)jj * 2 + 1) * hstride;
+      FDM_CUDA(launch_adjoint_half(s->cfg.model, mk, aa, s->stream));
+      rc = ensure_coefficients(s, A.dt1s[j]);
+      if (rc)
+        return rc;
+      FDM_CUDA(launch_adjoint_diffusion(nf, s->off_d.p, s->elem_d.p, s->coef.p, N, A.lam.p, A.U.p + (size_t)jj * N,
+                                        A.X.p + (size_t)jj * N, ie, A.gpf.p, s->scratch.p, A.mu.p, s->stream));
+      aa.half = 0;
+      aa.trace_row = -1;
+      aa.states = A.H.p + ((size_t)jj * 2 + 0) * hstride;
+      FDM_CUDA(launch_adjoint_half(s->cfg.model, mk, aa, s->stream));
+      s->launches += 3;
+    }
+  }
+  FDM_CUDA(cudaEventRecord(s->adv_stop, s->stream));
+  if (grad_parameters && NP > 0)
+    FDM_CUDA(cudaMemcpyAsync(grad_parameters, A.gP.p, sizeof(double) * NP * N, cudaMemcpyDeviceToHost, s->stream));
+  if (grad_prefactor)
+    FDM_CUDA(cudaMemcpyAsync(grad_prefactor, A.gpf.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, s->stream));
+  if (grad_states0)
+    FDM_CUDA(cudaMemcpyAsync(grad_states0, A.lam.p, sizeof(double) * NS * N, cudaMemcpyDeviceToHost, s->stream));
+  // the solver continues from the state the forward run ended in
+  int rc = copy_state(s, A.fin_vm.p, A.fin_states.p, A.fin_last.p, A.fin_jit.p, A.fin_jidx.p, A.fin_hbs.p, false);
+  if (rc)
+    return rc;
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  float ms = 0;
+  FDM_CUDA(cudaEventElapsedTime(&ms, s->adv_start, s->adv_stop));
+  s->adj_ms += ms;
+  s->strang = A.fin_strang;
+  s->heun = A.fin_heun;
+  s->diff = A.fin_diff;
+  s->split_no = A.fin_split;
+  return FDM_OK;
+}
+
+extern "C" int fdm_adjoint_release(fdm_solver* s)
+{
+  if (!s)
+    return FDM_ERR_ARG;
+  FDM_BIND(s);
+  s->adj.release();
+  return FDM_OK;
+}
+
+extern "C" int fdm_adjoint_timing(const fdm_solver* s, double* backward_ms)
+{
+  if (!s || !backward_ms)
+    return FDM_ERR_ARG;
+  *backward_ms = s->adj_ms;
+  return FDM_OK;
+}
+
+// back to the start: time-stepping objects, Strang step counter and the stimulation machine as after
+// fdm_set_stimulation (the states are left as they are)
+extern "C" int fdm_rewind(fdm_solver* s)
+{
+  if (!s)
+    return FDM_ERR_ARG;
+  FDM_BIND(s);
+  s->tss_init = false;
+  s->split_no = 0;
+  s->ck_valid = false;
+  const int nf = s->n_fibers;
+  if (s->stimulation_set && nf > 0) {
+    std::vector<double> last(nf), cj(nf, 0.0);
+    std::vector<int> ji(nf, 0);
+    std::vector<uint8_t> h0(nf, 0);
+    for (int f = 0; f < nf; f++)
+      last[f] = s->stim_begin[f] - 1e-13 - 1. / (s->stim_freq[f] + cj[f]);
+    FDM_CUDA(cudaMemcpyAsync(s->last_check.p, last.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->cur_jitter.p, cj.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, ji.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->hbs.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+  }
   return FDM_OK;
 }

@@ -272,6 +272,8 @@ struct ReactionArgs {
   double* trace;                  // [global split no][slot]
   int n_trace;
   int64_t trace_capacity;
+  double* store_states;           // adjoint replay (FP64 only): input state of substep k at
+                                  // store_states[(k*nStates + s)*stride + node], or null
 };
 
 template<class Model, class RR, class Math>
@@ -306,6 +308,12 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
     const double t = xadd(t0, xmul((double)k, s.dt0));
     const bool stim = cf >= 0 && stim_bit(a.flags, a.words_per_fiber, cf, base + k);
     const bool vclamp = stim && a.stimulus_mode == 0;
+    if (a.store_states) {
+      a.store_states[(int64_t)(k * NS) * a.stride + i] = V;
+#pragma unroll
+      for (int s2 = 1; s2 < NS; s2++)
+        a.store_states[(int64_t)(k * NS + s2) * a.stride + i] = (double)S[s2 - 1];
+    }
     RR Pk[NP];
 #pragma unroll
     for (int q = 0; q < NP; q++)
@@ -493,7 +501,205 @@ __global__ void __launch_bounds__(128) diffusion_warp_kernel(int n_fibers, const
   }
 }
 
+// Adjoint of one diffusion solve A x = B u (A, B symmetric tridiagonal): given lam (the adjoint of x) per
+// fiber, mu = A^{-1} lam with the same LU factors, lam_u = B mu written back to lam, and the prefactor
+// gradient  d/dpf = mu^T (dB/dpf u - dA/dpf x)  with K1 v = sum over the node's elements (v_nb - v)/h:
+//   implicit Euler: A = pf K1 - M/dt, B = -M/dt          -> -mu^T K1 x
+//   Crank-Nicolson: A = pf/2 K1 - M/dt, B = -pf/2 K1 - M/dt -> -mu^T K1 (u + x)/2
+__global__ void __launch_bounds__(128) adjoint_diffusion_warp_kernel(
+    int n_fibers, const int64_t* __restrict__ fiber_offsets, const double* __restrict__ element_lengths,
+    const double* __restrict__ coef, int64_t stride, double* __restrict__ lam, const double* __restrict__ u,
+    const double* __restrict__ x, int implicit_euler, double* __restrict__ grad_prefactor,
+    double* __restrict__ scratch, double* __restrict__ mu)
+{
+  const int lane = threadIdx.x & 31;
+  const int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (f >= n_fibers)
+    return;
+  const int64_t o = fiber_offsets[f];
+  const int64_t n = fiber_offsets[f + 1] - o;
+  const int64_t L = (n + 31) / 32;
+  const int64_t lo = o + min((int64_t)lane * L, n);
+  const int64_t hi = o + min((int64_t)(lane + 1) * L, n);
+  const double* h = element_lengths + (o - f);
+  const double* mulF = coef;
+  const double* inv = coef + stride;
+  const double* cp = coef + 2 * stride;
+  const double* cl = coef + 3 * stride;
+  const double* cm = coef + 4 * stride;
+  const double* cr = coef + 5 * stride;
+  Affine acc{1.0, 0.0};
+  for (int64_t i = lo; i < hi; i++)
+    acc = compose(acc, Affine{mulF[i], inv[i] * lam[i]});
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double F = __shfl_up_sync(0xffffffffu, acc.F, off);
+    const double G = __shfl_up_sync(0xffffffffu, acc.G, off);
+    if (lane >= off)
+      acc = compose(Affine{F, G}, acc);
+  }
+  double dp = __shfl_up_sync(0xffffffffu, acc.G, 1);
+  if (lane == 0)
+    dp = 0.0;
+  for (int64_t i = lo; i < hi; i++) {
+    dp = mulF[i] * dp + inv[i] * lam[i];
+    scratch[i] = dp;
+  }
+  __syncwarp();
+  Affine bacc{1.0, 0.0};
+  for (int64_t i = hi - 1; i >= lo; i--)
+    bacc = compose(bacc, Affine{-cp[i], scratch[i]});
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double F = __shfl_down_sync(0xffffffffu, bacc.F, off);
+    const double G = __shfl_down_sync(0xffffffffu, bacc.G, off);
+    if (lane + off < 32)
+      bacc = compose(Affine{F, G}, bacc);
+  }
+  double xx = __shfl_down_sync(0xffffffffu, bacc.G, 1);
+  if (lane == 31)
+    xx = 0.0;
+  for (int64_t i = hi - 1; i >= lo; i--) {
+    xx = -cp[i] * xx + scratch[i];
+    mu[i] = xx;
+  }
+  __syncwarp();
+  // lam_u = B mu, and the prefactor gradient
+  double g = 0.0;
+  for (int64_t i = lo; i < hi; i++) {
+    const int64_t v = i - o;
+    const double mp = v > 0 ? mu[i - 1] : 0.0;
+    const double mn = v < n - 1 ? mu[i + 1] : 0.0;
+    const double newlam = cl[i] * mp + cm[i] * mu[i] + cr[i] * mn;
+    double k1 = 0.0;
+    const double w = implicit_euler ? x[i] : 0.5 * (x[i] + u[i]);
+    if (v > 0)
+      k1 += ((implicit_euler ? x[i - 1] : 0.5 * (x[i - 1] + u[i - 1])) - w) / h[v - 1];
+    if (v < n - 1)
+      k1 += ((implicit_euler ? x[i + 1] : 0.5 * (x[i + 1] + u[i + 1])) - w) / h[v];
+    g -= mu[i] * k1;
+    scratch[i] = newlam;
+  }
+  __syncwarp();
+  for (int64_t i = lo; i < hi; i++)
+    lam[i] = scratch[i];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+    g += __shfl_down_sync(0xffffffffu, g, off);
+  if (lane == 0)
+    grad_prefactor[f] += g;
+}
+
 #endif // FDM_COMMON_KERNELS_TU
+
+// --------------------------------------------------------------------------------------------
+// adjoint (discrete reverse mode of the FP64 split path)
+// --------------------------------------------------------------------------------------------
+struct AdjointArgs {
+  int64_t n_nodes;
+  const double* states;           // stored substep input states of this half step: [(k*nS + s)*N + node]
+  const double* params;           // [p][node]
+  double* lam;                    // adjoint of the state [s][node], in/out
+  double* grad_params;            // [p][node], accumulated
+  const int* clamp_fiber;
+  const uint32_t* flags;
+  int words_per_fiber;
+  int nsub_stride;
+  double vstim;
+  int stimulus_mode;
+  int stimulus_parameter;
+  double stimulus_value;
+  SplitStep step;
+  int step_in_window;             // index of the split step in the flags window
+  int half;
+  const int* trace_slot;          // sensors: adjoint of the recorded Vm is added before half 1 is reversed
+  const double* trace_grad;       // [step][slot]
+  int n_trace;
+  int64_t trace_row;              // row of trace_grad for this split step (or -1)
+};
+
+// reverse of one half step (n0 Heun substeps) for one node:
+//   forward  r = f(y); y* = y + dt r [y*_0 := vStim]; y' = y + dt/2 (r + f(y*)) [y'_0 := vStim]
+//   reverse  (clamp: lam'_0 := 0); lam_* = J(y*)^T dt/2 lam' (clamp: lam_*_0 := 0);
+//            lam_y = lam' + lam_* + J(y)^T (dt/2 lam' + dt lam_*)
+template<class Model, class Math>
+__global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
+{
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_nodes)
+    return;
+  constexpr int NS = Model::nStates;
+  constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
+  const int64_t N = a.n_nodes;
+  double lam[NS], P[NP], gP[NP];
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    lam[s] = a.lam[s * N + i];
+#pragma unroll
+  for (int q = 0; q < Model::nParameters; q++) {
+    P[q] = a.params[q * N + i];
+    gP[q] = 0.0;
+  }
+  if (a.half == 1 && a.trace_slot && a.trace_row >= 0) {
+    const int slot = a.trace_slot[i];
+    if (slot >= 0)
+      lam[0] += a.trace_grad[a.trace_row * a.n_trace + slot];
+  }
+  const int cf = a.clamp_fiber[i];
+  const SplitStep st = a.step;
+  const double t0 = a.half ? st.mid : st.t;
+  const int base = (a.step_in_window * 2 + a.half) * a.nsub_stride;
+  const double dt = st.dt0;
+  for (int k = st.n0 - 1; k >= 0; k--) {
+    const double t = xadd(t0, xmul((double)k, dt));
+    const bool stim = cf >= 0 && stim_bit(a.flags, a.words_per_fiber, cf, base + k);
+    const bool clamp = stim && a.stimulus_mode == 0;
+    double Pk[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+      Pk[q] = (stim && a.stimulus_mode == 1 && q == a.stimulus_parameter) ? a.stimulus_value : P[q];
+    double y[NS], r[NS], ys[NS], alg[Model::nAlgebraics];
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      y[s] = a.states[(int64_t)(k * NS + s) * N + i];
+    Model::template rates<double, Math>(t, y, Pk, r, alg);
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      ys[s] = y[s] + dt * r[s];
+    if (clamp) {
+      ys[0] = a.vstim;
+      lam[0] = 0.0;
+    }
+    double lr2[NS], lys[NS], lr[NS], gPk[NP];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      lr2[s] = 0.5 * dt * lam[s];
+      lys[s] = 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+      gPk[q] = 0.0;
+    Model::template rates_vjp<double, Math>(t, ys, Pk, lr2, lys, gPk);
+    if (clamp)
+      lys[0] = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      lr[s] = 0.5 * dt * lam[s] + dt * lys[s];
+      lam[s] = lam[s] + lys[s];
+    }
+    Model::template rates_vjp<double, Math>(t, y, Pk, lr, lam, gPk);
+#pragma unroll
+    for (int q = 0; q < Model::nParameters; q++)
+      if (!(stim && a.stimulus_mode == 1 && q == a.stimulus_parameter))
+        gP[q] += gPk[q];
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    a.lam[s * N + i] = lam[s];
+#pragma unroll
+  for (int q = 0; q < Model::nParameters; q++)
+    a.grad_params[q * N + i] += gP[q];
+}
 
 // --------------------------------------------------------------------------------------------
 // fused path

@@ -87,6 +87,43 @@ cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, co
   return cudaGetLastError();
 }
 
+template<class Model>
+static cudaError_t adjoint_model(MathKind mk, const AdjointArgs& a, cudaStream_t s)
+{
+  const int T = 128;
+  const int64_t blocks = (a.n_nodes + T - 1) / T;
+  if (blocks == 0)
+    return cudaSuccess;
+  if (mk == MATH_EXACT)
+    adjoint_half_kernel<Model, fdm_math_exact><<<(unsigned)blocks, T, 0, s>>>(a);
+  else
+    adjoint_half_kernel<Model, fdm_math_approx><<<(unsigned)blocks, T, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_half(int model, MathKind mk, const AdjointArgs& a, cudaStream_t s)
+{
+  switch (model) {
+  case 0: return adjoint_model<HH>(mk, a, s);
+  case 1: return adjoint_model<SH>(mk, a, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_adjoint_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths,
+                                     const double* coef, int64_t stride, double* lam, const double* u, const double* x,
+                                     int implicit_euler, double* grad_prefactor, double* scratch, double* mu,
+                                     cudaStream_t s)
+{
+  if (n_fibers == 0)
+    return cudaSuccess;
+  const int T = 128;
+  const int64_t threads = (int64_t)n_fibers * 32;
+  adjoint_diffusion_warp_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, s>>>(
+      n_fibers, fiber_offsets, element_lengths, coef, stride, lam, u, x, implicit_euler, grad_prefactor, scratch, mu);
+  return cudaGetLastError();
+}
+
 __global__ void count_nonfinite_kernel(const double* __restrict__ x, int64_t n, int* count)
 {
   int local = 0;

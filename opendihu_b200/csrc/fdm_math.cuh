@@ -16,6 +16,11 @@
 #include <math.h>
 
 struct fdm_math_exact {
+  // derivatives for the adjoint: d exp(x)/dx = exp(x), d log(x)/dx = 1/x
+  template<class R>
+  __device__ __forceinline__ static R dexp(R x, R ex) { (void)x; return ex; }
+  template<class R>
+  __device__ __forceinline__ static R dlog(R x, R lx) { (void)lx; return (R)1 / x; }
   __device__ __forceinline__ static double exp(double x) { return ::exp(x); }
   __device__ __forceinline__ static float exp(float x) { return __expf(x); }
   __device__ __forceinline__ static double log(double x) { return ::log(x); }
@@ -81,6 +86,11 @@ __device__ __forceinline__ R fdm_approx_log_poly(R x)
 }
 
 struct fdm_math_approx {
+  // d/dx (1 + x/1024)^1024 = (1 + x/1024)^1023; the log approximation is differentiated as 1/x
+  template<class R>
+  __device__ __forceinline__ static R dexp(R x, R ex) { return ex / ((R)1 + x / (R)1024); }
+  template<class R>
+  __device__ __forceinline__ static R dlog(R x, R lx) { (void)lx; return (R)1 / x; }
   __device__ __forceinline__ static double exp(double x) { return fdm_approx_exp_d(x); }
   __device__ __forceinline__ static float exp(float x) { return fdm_approx_exp_f(x); }
   __device__ __forceinline__ static double log(double x)

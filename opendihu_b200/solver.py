@@ -507,6 +507,42 @@ class FastMonodomainSolver:
             self._call(N.lib().fdm_get_trace, N.ptr(out, C.c_double), C.byref(n))
         return out[:n.value, :len(self.trace_nodes)]
 
+    def rewind(self):
+        """Back to the start time: time-stepping state and stimulation machine reset, states kept."""
+        self._call(N.lib().fdm_rewind)
+
+    # -- adjoint ----------------------------------------------------------------------------------
+    def adjoint_forward(self, t_start: float, t_end: float, checkpoint_every: int, sensor_nodes) -> np.ndarray:
+        """Checkpointed FP64 forward run; returns Vm at the sensor nodes after every Strang step."""
+        self.initialize()
+        sn = np.ascontiguousarray(sensor_nodes, np.int64)
+        self._sensors = sn
+        self._call(N.lib().fdm_adjoint_forward, float(t_start), float(t_end), int(checkpoint_every), len(sn),
+                   N.ptr(sn, C.c_int64))
+        n = C.c_int64()
+        self._call(N.lib().fdm_get_trace, None, C.byref(n))
+        out = np.zeros((max(n.value, 1), max(len(sn), 1)))
+        if n.value and len(sn):
+            self._call(N.lib().fdm_get_trace, N.ptr(out, C.c_double), C.byref(n))
+        return out[:n.value, :len(sn)]
+
+    def adjoint_backward(self, trace_grad: np.ndarray) -> Dict[str, np.ndarray]:
+        """Gradients of a loss whose derivative w.r.t. the recorded trace is trace_grad [steps, sensors]."""
+        s = self.system
+        ns, na, npar = model_sizes(s.model)[:3]
+        tg = np.ascontiguousarray(trace_grad, np.float64)
+        gpf = np.zeros(s.n_fibers)
+        gp = np.zeros((max(npar, 1), s.n_nodes))
+        g0 = np.zeros((ns, s.n_nodes))
+        self._call(N.lib().fdm_adjoint_backward, N.ptr(tg, C.c_double), N.ptr(gpf, C.c_double),
+                   N.ptr(gp, C.c_double), N.ptr(g0, C.c_double))
+        return {"prefactor": gpf, "parameters": gp[:npar], "states0": g0}
+
+    def adjoint_timing_ms(self) -> float:
+        v = C.c_double()
+        self._call(N.lib().fdm_adjoint_timing, C.byref(v))
+        return v.value
+
     def clamp_nodes(self):
         nf = self.system.n_fibers
         first = np.zeros(nf, np.int64)

@@ -80,3 +80,30 @@ def subset(system: FiberSystem, fibers) -> FiberSystem:
     if system.states is not None:
         s.states = system.states[:, nodes].copy()
     return s
+
+
+def differentiation_hh(n_fibers: int = 256, n_nodes: int = 1481, end_time: float = 20.0, n_sensors: int = 32,
+                       seed: int = 1, **kw):
+    """Differentiation configuration: HH, 256 fibers x 1481 nodes, per-fiber sigma ~ U[2.5, 5.0] mS/cm and
+    per-fiber g_Na, g_K scaled by U[0.8, 1.2] (seeded), 32 sensor nodes per fiber evenly spaced, 20 ms.
+    Returns (system, sigma, scale_na, scale_k, sensor_nodes); parameters slot 1 = g_Na, slot 2 = g_K."""
+    rng = np.random.default_rng(seed)
+    sigma = rng.uniform(2.5, 5.0, size=n_fibers)
+    s_na = rng.uniform(0.8, 1.2, size=n_fibers)
+    s_k = rng.uniform(0.8, 1.2, size=n_fibers)
+    sysm = plain_hh(n_fibers=n_fibers, n_nodes=n_nodes, end_time=end_time, **kw)
+    sysm.prefactor = sigma / (AM * CM)
+    sysm.parameters = hh_parameters(sysm, s_na, s_k)
+    idx = np.linspace(0, n_nodes - 1, n_sensors).round().astype(np.int64)
+    sensors = (np.asarray(sysm.fiber_offsets[:-1])[:, None] + idx[None, :]).reshape(-1)
+    return sysm, sigma, s_na, s_k, sensors
+
+
+def hh_parameters(system: FiberSystem, s_na, s_k, i_stim: float = 0.0) -> np.ndarray:
+    """Per-node HH parameter slots (I_Stim, g_Na, g_K) with per-fiber scales of the model's 120 and 36 mS/cm^2."""
+    lengths = np.diff(np.asarray(system.fiber_offsets))
+    p = np.zeros((3, system.n_nodes))
+    p[0] = i_stim
+    p[1] = np.repeat(120.0 * np.asarray(s_na), lengths)
+    p[2] = np.repeat(36.0 * np.asarray(s_k), lengths)
+    return p
