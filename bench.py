@@ -44,6 +44,8 @@ def parse_args():
     p.add_argument("--nodes-per-thread", type=int, default=0)
     p.add_argument("--steps-per-launch", type=int, default=0)
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--skip-adjoint", action="store_true")
+    p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
     return p.parse_args()
 
 
@@ -266,6 +268,40 @@ def main():
         fp64_value = n_nodes * (plain.split_steps() - p0) * world / p_s
         plain.close()
 
+    # differentiation: adjoint gradient cost relative to one FP64 forward solve (256 HH fibers x 1481 nodes,
+    # per-fiber sigma, g_Na, g_K; 32 sensors per fiber; checkpoint every 100 Strang steps)
+    adj = None
+    if rank == 0 and not args.skip_adjoint:
+        from opendihu_b200 import adjoint as ADJ
+        dsys, sigma, s_na, s_k, sensors = WL.differentiation_hh(end_time=args.adjoint_ms, seed=1)
+        _, sigma2, s_na2, s_k2, _ = WL.differentiation_hh(end_time=args.adjoint_ms, seed=2)
+        eng = ADJ.AdjointEngine(dsys, sensors, checkpoint_every=100, device=local)
+        target = eng.forward(sigma2 / (WL.AM * WL.CM), WL.hh_parameters(dsys, s_na2, s_k2))
+        eng.solver.reset_timing()
+        trace = eng.forward(dsys.prefactor, dsys.parameters)
+        fwd_ck_ms = eng.solver.timing()["advance_ms"]
+        loss = float(((trace - target) ** 2).sum())
+        g = eng.backward(2.0 * (trace - target))
+        bwd_ms = eng.solver.adjoint_timing_ms()
+        eng.close()
+        with S.FastMonodomainSolver(dsys.copy(), method="split", precision="fp64", device=local) as fw:
+            fw.advanceTimeSpan()
+            fw.reset_timing()
+            fw.rewind()
+            fw.set_states(np.repeat(S.model_sizes(dsys.model)[3][:, None], dsys.n_nodes, axis=1))
+            fw.advanceTimeSpan()
+            plain_fwd_ms = fw.timing()["advance_ms"]
+        lengths = np.diff(dsys.fiber_offsets)
+        fiber_of = np.repeat(np.arange(dsys.n_fibers), lengths)
+        g_na = np.bincount(fiber_of, g["parameters"][1] * 120.0, minlength=dsys.n_fibers)
+        adj = {"workload": "256 HH fibers x 1481 nodes, %g ms, 32 sensors/fiber, checkpoint every 100 steps, "
+                           "768 parameters (sigma, g_Na scale, g_K scale per fiber)" % args.adjoint_ms,
+               "forward_ms": plain_fwd_ms, "checkpointed_forward_ms": fwd_ck_ms, "backward_ms": bwd_ms,
+               "adjoint_over_forward": (fwd_ck_ms + bwd_ms) / plain_fwd_ms,
+               "backward_over_forward": bwd_ms / plain_fwd_ms, "loss": loss,
+               "grad_norm_sigma": float(np.linalg.norm(g["prefactor"] / (WL.AM * WL.CM))),
+               "grad_norm_gna_scale": float(np.linalg.norm(g_na))}
+
     # accuracy against the FP64 oracle on a sample of the batch, and the oracle's CPU throughput
     acc = None
     cpu = None
@@ -320,7 +356,8 @@ def main():
             "fp64_plain": {"value": fp64_value, "unit": "node-steps/s",
                            "speedup_fp32_fused_over_fp64_plain": (value / fp64_value) if fp64_value else None},
             "accuracy_vs_fp64_oracle": acc,
-            "adjoint_over_forward": None,
+            "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
+            "adjoint": adj,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak_hbm, "unit": "GB/s",
                          "frac": (achieved_gbs / peak_hbm) if achieved_gbs else None, "traffic": traffic,
                          "peak_source": peak_kind,

@@ -1098,8 +1098,50 @@ def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequenc
         out.append(f"    R a_{name} = (R)0;")
     for idx, tn in sorted(b.rate_temp.items()):
         out.append(f"    a_{tn} += LAM_RATES[{idx}];")
-    out.extend(b.backward())
+    bwd = b.backward()
+    out.extend(bwd)
+    out.append("  }")
+    # the same split in two: a forward that records every temporary (and condition) on a tape, and a
+    # backward that reads the tape, so that a caller who needs the rates anyway evaluates them only once
+    n_tape = b.n
+    conds = [ln.split("const bool ", 1)[1].split(" =", 1)[0] for ln in b.fwd if "const bool " in ln]
+    out.append(f"  static constexpr int nTape = {n_tape + len(conds)};")
+    out.append("  template<class R, class M>")
+    out.append("  __device__ __forceinline__ static void rates_tape(const R VOI, const R* __restrict__ STATES,"
+               " const R* __restrict__ PARAMS, R* __restrict__ RATES, R* __restrict__ TAPE)")
+    out.append("  {")
+    out.append("    (void)VOI; (void)PARAMS;")
+    out.append(f"    R ALG[{max(model.n_algebraics, 1)}];")
+    out.append("    (void)ALG;")
+    ci = {c: n_tape + k for k, c in enumerate(conds)}
+    for ln in b.fwd:
+        out.append(ln)
+        st = ln.strip()
+        if st.startswith("const R t"):
+            name = st.split()[2]
+            out.append(f"    TAPE[{int(name[1:])}] = {name};")
+        elif st.startswith("const bool c"):
+            name = st.split()[2]
+            out.append(f"    TAPE[{ci[name]}] = {name} ? (R)1 : (R)0;")
+    for idx, tn in sorted(b.rate_temp.items()):
+        out.append(f"    RATES[{idx}] = {tn};")
+    out.append("  }")
+    out.append("  template<class R, class M>")
+    out.append("  __device__ __forceinline__ static void rates_vjp_tape(const R VOI, const R* __restrict__ STATES,"
+               " const R* __restrict__ PARAMS, const R* __restrict__ TAPE, const R* __restrict__ LAM_RATES,"
+               " R* __restrict__ LAM_STATES, R* __restrict__ LAM_PARAMS)")
+    out.append("  {")
+    out.append("    (void)VOI; (void)PARAMS; (void)STATES;")
+    for k in range(n_tape):
+        out.append(f"    const R t{k} = TAPE[{k}];")
+    for c, k in ci.items():
+        out.append(f"    const bool {c} = TAPE[{k}] != (R)0;")
+    for name, *_ in b.ops:
+        out.append(f"    R a_{name} = (R)0;")
+    for idx, tn in sorted(b.rate_temp.items()):
+        out.append(f"    a_{tn} += LAM_RATES[{idx}];")
+    out.extend(bwd)
+    out.append("  }")
     for n in pows_vjp:
         out.append(f"#undef FDM_POW{n}")
-    out.append("  }")
     return out

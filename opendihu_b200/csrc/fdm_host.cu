@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -181,6 +182,7 @@ struct fdm_solver {
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   double main_ms = 0, adv_ms = 0, adj_ms = 0;
+  int adjoint_tape = 1; // FDM_ADJOINT_TAPE=0 selects the re-evaluating reverse step (for measurements)
   int64_t main_launches = 0, launches = 0;
   cudaEvent_t adv_start = nullptr, adv_stop = nullptr;
 };
@@ -329,6 +331,8 @@ extern "C" int fdm_create(const fdm_config* cfg, fdm_solver** out)
     s->cfg.steps_per_launch = 100;
   s->model = m;
   s->real_bytes = cfg->reaction_precision == FDM_FP64 ? 8 : 4;
+  if (const char* env = std::getenv("FDM_ADJOINT_TAPE"))
+    s->adjoint_tape = std::atoi(env) != 0;
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess)
     e = cudaMallocHost((void**)&s->steps_h, sizeof(SplitStep) * 2 * s->cfg.steps_per_launch);
@@ -1816,6 +1820,7 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
     aa.trace_slot = A.n_sensors > 0 ? s->trace_slot.p : nullptr;
     aa.trace_grad = A.tgrad.p;
     aa.n_trace = A.n_sensors;
+    aa.use_tape = s->adjoint_tape;
     for (int jj = len - 1; jj >= 0; jj--) {
       const size_t j = b + jj;
       aa.step = A.steps[j];

@@ -616,6 +616,7 @@ struct AdjointArgs {
   const double* trace_grad;       // [step][slot]
   int n_trace;
   int64_t trace_row;              // row of trace_grad for this split step (or -1)
+  int use_tape;                   // 1: f(y) evaluated once, its temporaries kept for the backward sweep
 };
 
 // reverse of one half step (n0 Heun substeps) for one node:
@@ -662,7 +663,12 @@ __global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
 #pragma unroll
     for (int s = 0; s < NS; s++)
       y[s] = a.states[(int64_t)(k * NS + s) * N + i];
-    Model::template rates<double, Math>(t, y, Pk, r, alg);
+    constexpr bool TAPE_OK = Model::nTape <= 256;
+    double tape[TAPE_OK ? Model::nTape : 1];
+    if (TAPE_OK && a.use_tape)
+      Model::template rates_tape<double, Math>(t, y, Pk, r, tape);
+    else
+      Model::template rates<double, Math>(t, y, Pk, r, alg);
 #pragma unroll
     for (int s = 0; s < NS; s++)
       ys[s] = y[s] + dt * r[s];
@@ -687,7 +693,10 @@ __global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
       lr[s] = 0.5 * dt * lam[s] + dt * lys[s];
       lam[s] = lam[s] + lys[s];
     }
-    Model::template rates_vjp<double, Math>(t, y, Pk, lr, lam, gPk);
+    if (TAPE_OK && a.use_tape)
+      Model::template rates_vjp_tape<double, Math>(t, y, Pk, tape, lr, lam, gPk);
+    else
+      Model::template rates_vjp<double, Math>(t, y, Pk, lr, lam, gPk);
 #pragma unroll
     for (int q = 0; q < Model::nParameters; q++)
       if (!(stim && a.stimulus_mode == 1 && q == a.stimulus_parameter))
