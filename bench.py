@@ -323,9 +323,9 @@ def main():
     n0d = 5
     fp32_flops_node_step = 2 * n0d * (2 * ops["flops"] + 6 + 9)
     fp64_flops_node_step = 2 * n0d * 5 + 15
-    # algorithmic HBM bytes of one fused launch: states (Vm f64 + 3 gates f32) read+write, 3 parameters,
-    # 6 diffusion coefficients (f64) and the clamp map, per node
-    bytes_launch = n_nodes * (2 * (8 + 12) + 12 + 48 + 4)
+    # algorithmic HBM bytes of one fused launch, per node: states read and written once (Vm f64, 3 gates and
+    # their 3 compensation residuals f32), 3 parameters (f32), 6 diffusion coefficients (f64), clamp map (i32)
+    bytes_launch = n_nodes * (2 * (8 + 12 + 12) + 12 + 48 + 4)
     achieved_gbs = bytes_launch / (kernel_avg_ms / 1e3) / 1e9 if kernel_avg_ms > 0 else None
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
     achieved_tf = n_nodes * steps_per_launch * fp32_flops_node_step / (kernel_avg_ms / 1e3) / 1e12 if kernel_avg_ms > 0 else None
