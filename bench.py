@@ -239,7 +239,7 @@ def main():
         fused.set_states(host_states)
         fused.setTimeSpan(t, t + step)
         fused.advanceTimeSpan()
-        host_states = fused.states()
+        host_states = fused.states(out=host_states)
         t += step
     e2e_s = allmax(pg, time.perf_counter() - t0)
     e2e_value = n_nodes * (split_steps / args.steps) * e2e_steps * world / e2e_s
@@ -249,7 +249,7 @@ def main():
     # FP64 split ("plain") solver on the same batch
     fp64_value = None
     if not args.skip_fp64:
-        plain = S.FastMonodomainSolver(system.copy(), method="split", precision="fp64", profile=True, device=local)
+        plain = S.FastMonodomainSolver(system.copy(), method="split", precision="fp64", device=local)
         plain.initialize()
         tp = 0.0
         plain.setTimeSpan(tp, tp + step)
@@ -267,6 +267,22 @@ def main():
         p_s = allmax(pg, tmp["advance_ms"] / 1e3)
         fp64_value = n_nodes * (plain.split_steps() - p0) * world / p_s
         plain.close()
+
+    # plain-method configuration (16 HH fibers x 1481 nodes, implicit Euler, FP64 split path with CUDA graphs,
+    # and the FP32 fused kernel on the same fibers)
+    plain_cfg = None
+    if rank == 0 and not args.skip_fp64:
+        c1 = WL.plain_hh(end_time=10.0)
+        plain_cfg = {"workload": "16 HH fibers x 1481 nodes, implicit Euler, 10 ms"}
+        for name, method, prec in (("fp64_split", "split", "fp64"), ("fp32_fused", "fused", "fp32")):
+            with S.FastMonodomainSolver(c1.copy(), method=method, precision=prec, device=local) as sv:
+                sv.setTimeSpan(0.0, 1.0)
+                sv.advanceTimeSpan()
+                sv.reset_timing()
+                sv.setTimeSpan(1.0, 10.0)
+                sv.advanceTimeSpan()
+                ms = sv.timing()["advance_ms"]
+            plain_cfg[name] = c1.n_nodes * 9000 / (ms / 1e3)
 
     # differentiation: adjoint gradient cost relative to one FP64 forward solve (256 HH fibers x 1481 nodes,
     # per-fiber sigma, g_Na, g_K; 32 sensors per fiber; checkpoint every 100 Strang steps)
@@ -357,6 +373,7 @@ def main():
                            "speedup_fp32_fused_over_fp64_plain": (value / fp64_value) if fp64_value else None},
             "accuracy_vs_fp64_oracle": acc,
             "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
+            "plain_config_node_steps_per_s": plain_cfg,
             "adjoint": adj,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak_hbm, "unit": "GB/s",
                          "frac": (achieved_gbs / peak_hbm) if achieved_gbs else None, "traffic": traffic,

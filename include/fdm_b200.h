@@ -82,6 +82,7 @@ typedef struct fdm_config {
   int check_nan;                 /* 1: fdm_advance fails with FDM_ERR_NAN if Vm is not finite */
   int profile;                   /* 1: time the main kernel launches with CUDA events */
   int device;                    /* CUDA device ordinal the solver lives on */
+  int use_graph;                 /* 1: the split path replays each window's launch sequence as a CUDA graph */
 } fdm_config;
 
 /* fills *cfg with the reference's defaults (HH, implicit Euler, FP64 split, vc rule W=4, 20 mV clamp) */

@@ -52,7 +52,7 @@ class Config(C.Structure):
         ("value_for_stimulated_point", C.c_double), ("dt_repeated_call", C.c_double),
         ("dt_splitting", C.c_double), ("dt_0d", C.c_double), ("dt_1d", C.c_double),
         ("steps_per_launch", C.c_int), ("threads_per_block", C.c_int), ("nodes_per_thread", C.c_int),
-        ("check_nan", C.c_int), ("profile", C.c_int), ("device", C.c_int),
+        ("check_nan", C.c_int), ("profile", C.c_int), ("device", C.c_int), ("use_graph", C.c_int),
     ]
 
 

@@ -17,8 +17,11 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <string>
+#include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fdm_b200.h"
@@ -178,6 +181,13 @@ struct fdm_solver {
     }
   } adj;
 
+  // pinned host staging for the state transfers
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+
+  // split-path window graphs: (steps, words, nsub, flags pointer) -> executable graph
+  std::map<std::tuple<int, int, int, const void*>, cudaGraphExec_t> graphs;
+
   // timing
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
@@ -222,6 +232,14 @@ static int cuda_fail(fdm_solver* s, cudaError_t e, const char* what)
       return cuda_fail(s, e_, #call);           \
   } while (0)
 
+// captured window graphs hold kernel arguments by value: drop them whenever those can change
+static void invalidate_graphs(fdm_solver* s)
+{
+  for (auto& kv : s->graphs)
+    cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+}
+
 extern "C" void fdm_config_default(fdm_config* c)
 {
   std::memset(c, 0, sizeof(*c));
@@ -246,6 +264,8 @@ extern "C" void fdm_config_default(fdm_config* c)
   c->nodes_per_thread = 0;
   c->check_nan = 1;
   c->profile = 0;
+  c->device = 0;
+  c->use_graph = 1;
 }
 
 extern "C" const char* fdm_last_error(const fdm_solver* s)
@@ -385,6 +405,11 @@ extern "C" int fdm_destroy(fdm_solver* s)
   s->flags.release();
   s->steps_d.release();
   s->adj.release();
+  for (auto& kv : s->graphs)
+    cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  if (s->stage)
+    cudaFreeHost(s->stage);
   if (s->steps_h)
     cudaFreeHost(s->steps_h);
   for (auto ev : s->slot_ev)
@@ -484,6 +509,7 @@ extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_
   if (!s || n_fibers < 0 || (n_fibers > 0 && (!fiber_offsets || !element_lengths || !prefactor)))
     return fail(s, FDM_ERR_ARG, "fdm_set_fibers: bad argument");
   FDM_BIND(s);
+  invalidate_graphs(s);
   if (n_fibers > 0 && fiber_offsets[0] != 0)
     return fail(s, FDM_ERR_ARG, "fdm_set_fibers: fiber_offsets[0] must be 0");
   int64_t maxlen = 0;
@@ -598,6 +624,40 @@ extern "C" int fdm_set_prefactor(fdm_solver* s, const double* prefactor)
   return FDM_OK;
 }
 
+// host-side parallel loop for the conversions at the boundary
+template<class F>
+static void parallel_for(size_t n, F fn)
+{
+  unsigned nt = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (n < (1u << 16) || nt == 1) {
+    fn(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (n + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; t++) {
+    const size_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b)
+      th.emplace_back([=] { fn(a, b); });
+  }
+  for (auto& t : th)
+    t.join();
+}
+
+static cudaError_t ensure_stage(fdm_solver* s, size_t bytes)
+{
+  if (bytes <= s->stage_bytes)
+    return cudaSuccess;
+  if (s->stage)
+    cudaFreeHost(s->stage);
+  s->stage = nullptr;
+  s->stage_bytes = 0;
+  cudaError_t e = cudaMallocHost(&s->stage, bytes);
+  if (e == cudaSuccess)
+    s->stage_bytes = bytes;
+  return e;
+}
+
 // SoA host doubles -> device (Vm in FP64, other states in the reaction precision)
 extern "C" int fdm_set_states(fdm_solver* s, const double* states)
 {
@@ -605,26 +665,33 @@ extern "C" int fdm_set_states(fdm_solver* s, const double* states)
     return fail(s, FDM_ERR_ARG, "fdm_set_states: bad argument");
   FDM_BIND(s);
   const int NS = s->model->n_states;
-  const int64_t N = s->n_nodes;
+  const size_t N = (size_t)s->n_nodes;
   if (N == 0)
     return FDM_OK;
-  FDM_CUDA(cudaMemcpyAsync(s->vm.p, states, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream));
-  if (NS > 1) {
+  const size_t M = N * (size_t)std::max(NS - 1, 0);
+  // staging layout: Vm (N doubles), then the other states as FP64 or as FP32 (value, residual) pairs
+  const size_t bytes = N * 8 + (s->real_bytes == 8 ? M * 8 : M * 8);
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  FDM_CUDA(ensure_stage(s, bytes));
+  double* vm = (double*)s->stage;
+  parallel_for(N, [&](size_t a, size_t b) { std::memcpy(vm + a, states + a, (b - a) * sizeof(double)); });
+  FDM_CUDA(cudaMemcpyAsync(s->vm.p, vm, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream));
+  if (M > 0) {
     if (s->real_bytes == 8) {
-      FDM_CUDA(cudaMemcpyAsync(s->states.p, states + N, sizeof(double) * N * (NS - 1), cudaMemcpyHostToDevice,
-                               s->stream));
+      double* st = vm + N;
+      parallel_for(M, [&](size_t a, size_t b) { std::memcpy(st + a, states + N + a, (b - a) * sizeof(double)); });
+      FDM_CUDA(cudaMemcpyAsync(s->states.p, st, sizeof(double) * M, cudaMemcpyHostToDevice, s->stream));
     } else {
-      // each state as an FP32 pair (value, residual) whose sum reproduces the double
-      std::vector<float> hi((size_t)N * (NS - 1)), lo((size_t)N * (NS - 1));
-      for (size_t i = 0; i < hi.size(); i++) {
-        hi[i] = (float)states[N + i];
-        lo[i] = (float)(states[N + i] - (double)hi[i]);
-      }
-      FDM_CUDA(cudaMemcpyAsync(s->states.p, hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice,
-                               s->stream));
-      FDM_CUDA(cudaMemcpyAsync(s->states_lo.p, lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice,
-                               s->stream));
-      FDM_CUDA(cudaStreamSynchronize(s->stream));
+      float* hi = (float*)(vm + N);
+      float* lo = hi + M;
+      parallel_for(M, [&](size_t a, size_t b) {
+        for (size_t i = a; i < b; i++) {
+          hi[i] = (float)states[N + i];
+          lo[i] = (float)(states[N + i] - (double)hi[i]);
+        }
+      });
+      FDM_CUDA(cudaMemcpyAsync(s->states.p, hi, sizeof(float) * M, cudaMemcpyHostToDevice, s->stream));
+      FDM_CUDA(cudaMemcpyAsync(s->states_lo.p, lo, sizeof(float) * M, cudaMemcpyHostToDevice, s->stream));
     }
   }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
@@ -637,27 +704,37 @@ extern "C" int fdm_get_states(fdm_solver* s, double* states)
     return fail(s, FDM_ERR_ARG, "fdm_get_states: bad argument");
   FDM_BIND(s);
   const int NS = s->model->n_states;
-  const int64_t N = s->n_nodes;
+  const size_t N = (size_t)s->n_nodes;
   if (N == 0)
     return FDM_OK;
-  FDM_CUDA(cudaMemcpyAsync(states, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream));
-  if (NS > 1) {
+  const size_t M = N * (size_t)std::max(NS - 1, 0);
+  FDM_CUDA(ensure_stage(s, N * 8 + M * 8));
+  double* vm = (double*)s->stage;
+  FDM_CUDA(cudaMemcpyAsync(vm, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream));
+  if (M > 0) {
     if (s->real_bytes == 8) {
-      FDM_CUDA(cudaMemcpyAsync(states + N, s->states.p, sizeof(double) * N * (NS - 1), cudaMemcpyDeviceToHost,
-                               s->stream));
-      FDM_CUDA(cudaStreamSynchronize(s->stream));
+      FDM_CUDA(cudaMemcpyAsync(vm + N, s->states.p, sizeof(double) * M, cudaMemcpyDeviceToHost, s->stream));
     } else {
-      std::vector<float> hi((size_t)N * (NS - 1)), lo((size_t)N * (NS - 1));
-      FDM_CUDA(cudaMemcpyAsync(hi.data(), s->states.p, sizeof(float) * hi.size(), cudaMemcpyDeviceToHost,
-                               s->stream));
-      FDM_CUDA(cudaMemcpyAsync(lo.data(), s->states_lo.p, sizeof(float) * lo.size(), cudaMemcpyDeviceToHost,
-                               s->stream));
-      FDM_CUDA(cudaStreamSynchronize(s->stream));
-      for (size_t i = 0; i < hi.size(); i++)
-        states[N + i] = (double)hi[i] + (double)lo[i];
+      float* hi = (float*)(vm + N);
+      FDM_CUDA(cudaMemcpyAsync(hi, s->states.p, sizeof(float) * M, cudaMemcpyDeviceToHost, s->stream));
+      FDM_CUDA(cudaMemcpyAsync(hi + M, s->states_lo.p, sizeof(float) * M, cudaMemcpyDeviceToHost, s->stream));
     }
   }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
+  parallel_for(N, [&](size_t a, size_t b) { std::memcpy(states + a, vm + a, (b - a) * sizeof(double)); });
+  if (M > 0) {
+    if (s->real_bytes == 8) {
+      const double* st = vm + N;
+      parallel_for(M, [&](size_t a, size_t b) { std::memcpy(states + N + a, st + a, (b - a) * sizeof(double)); });
+    } else {
+      const float* hi = (const float*)(vm + N);
+      const float* lo = hi + M;
+      parallel_for(M, [&](size_t a, size_t b) {
+        for (size_t i = a; i < b; i++)
+          states[N + i] = (double)hi[i] + (double)lo[i];
+      });
+    }
+  }
   return FDM_OK;
 }
 
@@ -808,6 +885,7 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
   if (!s || rows < 1 || cols < 1 || !firing_events || n_jitter < 0 || (n_jitter > 0 && !jitter))
     return fail(s, FDM_ERR_ARG, "fdm_set_stimulation: bad argument (firing events need at least one row and column)");
   FDM_BIND(s);
+  invalidate_graphs(s);
   const int nf = s->n_fibers;
   if (nf > 0 && (!motor_unit_no || !stimulation_point_index || !call_frequency || !repeat_after_first_call ||
                  !call_enable_begin))
@@ -892,6 +970,7 @@ extern "C" int fdm_set_algebraics_for_transfer(fdm_solver* s, int n, const int* 
   if (!s || n < 0 || (n > 0 && !idx))
     return fail(s, FDM_ERR_ARG, "fdm_set_algebraics_for_transfer: bad argument");
   FDM_BIND(s);
+  invalidate_graphs(s);
   for (int k = 0; k < n; k++)
     if (idx[k] < 0 || idx[k] >= s->model->n_algebraics)
       return fail(s, FDM_ERR_ARG, "fdm_set_algebraics_for_transfer: algebraic index out of range");
@@ -924,6 +1003,7 @@ extern "C" int fdm_set_trace(fdm_solver* s, int n, const int64_t* nodes, int64_t
   if (!s || n < 0 || (n > 0 && !nodes) || capacity < 0)
     return fail(s, FDM_ERR_ARG, "fdm_set_trace: bad argument");
   FDM_BIND(s);
+  invalidate_graphs(s);
   std::vector<int> slot((size_t)std::max<int64_t>(s->n_nodes, 1), -1);
   for (int k = 0; k < n; k++) {
     if (nodes[k] < 0 || nodes[k] >= s->n_nodes)
@@ -1136,6 +1216,40 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
   ra.trace = s->trace.p;
   ra.n_trace = s->n_trace;
   ra.trace_capacity = s->trace_capacity;
+  // without profiling, a window that stores no algebraics replays a captured CUDA graph of its launches
+  const bool graph_ok = s->cfg.use_graph && !prof && !(store_alg && s->n_alg_out > 0);
+  if (graph_ok) {
+    const auto key = std::make_tuple(n_steps, words, nsub, (const void*)s->flags.p);
+    auto it = s->graphs.find(key);
+    if (it == s->graphs.end()) {
+      cudaGraph_t g = nullptr;
+      FDM_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t ce = cudaSuccess;
+      for (int j = 0; j < n_steps && ce == cudaSuccess; j++) {
+        ra.step = j;
+        for (int half = 0; half < 2 && ce == cudaSuccess; half++) {
+          ra.half = half;
+          ra.store_alg = 0;
+          ce = launch_reaction(s->cfg.model, rk, mk, ra, s->stream);
+          if (ce == cudaSuccess && half == 0)
+            ce = launch_diffusion_warp(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
+                                       s->stream);
+        }
+      }
+      cudaError_t ee = cudaStreamEndCapture(s->stream, &g);
+      if (ce != cudaSuccess)
+        return cuda_fail(s, ce, "capture of the window launches");
+      FDM_CUDA(ee);
+      cudaGraphExec_t ex = nullptr;
+      cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      FDM_CUDA(ie);
+      it = s->graphs.emplace(key, ex).first;
+    }
+    FDM_CUDA(cudaGraphLaunch(it->second, s->stream));
+    s->launches += 3 * (int64_t)n_steps;
+    return FDM_OK;
+  }
   for (int j = 0; j < n_steps; j++) {
     ra.step = j;
     for (int half = 0; half < 2; half++) {
@@ -1591,6 +1705,8 @@ extern "C" void computeMonodomain(const float* parameters, double* algebraicsFor
     if (fdm_set_parameters(s, p.data()))
       return;
   }
+  if (s->cfg.value_for_stimulated_point != valueForStimulatedPoint)
+    invalidate_graphs(s);
   s->cfg.value_for_stimulated_point = valueForStimulatedPoint;
   if (advance_explicit(s, startTime, timeStepWidthSplitting, nTimeStepsSplitting, dt0D, nTimeSteps0D, dt1D))
     return;

@@ -462,9 +462,12 @@ class FastMonodomainSolver:
         self._call(N.lib().fdm_checkpoint_restore)
 
     # -- data -------------------------------------------------------------------------------------
-    def states(self) -> np.ndarray:
+    def states(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """All states [state, node] (FP64); ``out`` reuses a C-contiguous float64 array of that shape."""
         ns = model_sizes(self.system.model)[0]
-        out = np.zeros((ns, self.system.n_nodes))
+        if out is None or out.shape != (ns, self.system.n_nodes) or out.dtype != np.float64 \
+                or not out.flags.c_contiguous:
+            out = np.empty((ns, self.system.n_nodes))
         self._call(N.lib().fdm_get_states, N.ptr(out, C.c_double))
         return out
 
