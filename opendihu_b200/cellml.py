@@ -636,17 +636,42 @@ def _exp_groups(lines, consts):
     return repl, groups
 
 
+_LOG2E = 1.4426950408889634
+_LN2 = 0.6931471805599453
+
+
 class _FastEmitter(_Emitter):
-    """FP32 variant: shared exponentials (see _exp_groups)."""
+    """FP32 form of the right-hand side: shared exponentials (see _exp_groups), every exponential as one
+    SFU ex2 of an argument whose log2(e) scaling and affine coefficients are folded at generation time,
+    divisions by constants as multiplications, other divisions as a multiplication by the SFU reciprocal."""
 
     def __init__(self, real, consts, repl):
         super().__init__(real, consts, "cuda")
         self.repl = repl
 
+    def affine_text(self, coeffs, const, scale):
+        terms = [f"(({self.real}){_hexf(v * scale)}) * {self.var(k[0], k[1])}" for k, v in coeffs]
+        if const != 0.0:
+            terms.append(f"(({self.real}){_hexf(const * scale)})")
+        return " + ".join(terms) if terms else f"(({self.real})0)"
+
     def expr(self, e):
-        if e[0] == "call" and e[1] == "exp" and repr(e) in self.repl:
-            g, b = self.repl[repr(e)]
-            return f"(fdm_e{g} * (({self.real}){_hexf(math.exp(b))}))"
+        t = e[0]
+        if t == "call" and e[1] == "exp":
+            if repr(e) in self.repl:
+                g, b = self.repl[repr(e)]
+                return f"(fdm_e{g} * (({self.real}){_hexf(math.exp(b))}))"
+            af = _affine(e[2][0], self.consts)
+            if af is not None:
+                return f"fdm_ex2({self.affine_text(sorted(af[0].items()), af[1], _LOG2E)})"
+            return f"fdm_ex2((({self.real}){_hexf(_LOG2E)}) * {self.expr(e[2][0])})"
+        if t == "call" and e[1] == "log":
+            return f"(fdm_lg2({self.expr(e[2][0])}) * (({self.real}){_hexf(_LN2)}))"
+        if t == "bin" and e[1] == "/":
+            den = _affine(e[3], self.consts)
+            if den is not None and not den[0] and den[1] != 0.0:
+                return f"({self.expr(e[2])} * (({self.real}){_hexf(1.0 / den[1])}))"
+            return f"({self.expr(e[2])} * fdm_rcp({self.expr(e[3])}))"
         return super().expr(e)
 
 
@@ -702,7 +727,8 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     # FP32 variant with shared exponentials
     repl, groups = _exp_groups(lines, model.constants)
     fem = _FastEmitter("R", model.constants, repl)
-    out.append("  // FP32 form: exponentials exp(a.x + b_k) that share a.x are evaluated once as exp(a.x) * e^{b_k}")
+    out.append("  // FP32 form: exponentials exp(a.x + b_k) that share a.x are evaluated once as exp(a.x) * e^{b_k};")
+    out.append("  // exponentials, logarithms and reciprocals as single SFU instructions (fdm_ex2/fdm_lg2/fdm_rcp)")
     out.append(f"  static constexpr int nSharedExponentials = {len(groups)};")
     out.append("  template<class R, class M>")
     out.append("  __device__ __forceinline__ static void rates_fast(const R VOI, const R* __restrict__ STATES,"
@@ -716,8 +742,7 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     out.append("#define FDM_SQRT(x) sqrt(x)")
     out.extend("#define " + s2.split("#define ", 1)[1] for s2 in _pow_macro_defs(pows))
     for g, key in enumerate(groups):
-        terms = " + ".join(f"(({'R'}){_hexf(v)}) * {fem.var(k[0], k[1])}" for k, v in key)
-        out.append(f"    const R fdm_e{g} = FDM_EXP({terms});")
+        out.append(f"    const R fdm_e{g} = fdm_ex2({fem.affine_text(list(key), 0.0, _LOG2E)});")
     for kind, idx, expr in lines:
         tgt = f"ALGEBRAIC[{idx}]" if kind == "A" else f"RATES[{idx}]"
         out.append(f"    {tgt} = {fem.expr(expr)};")

@@ -15,6 +15,27 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+// single SFU instructions for the FP32 form of the right-hand sides (relative error ~2^-22):
+// 2^x, 1/x and log2(x), flushing denormals (the FP32 reaction is compiled with -ftz=true)
+__device__ __forceinline__ float fdm_ex2(float x)
+{
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float fdm_rcp(float x)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float fdm_lg2(float x)
+{
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 struct fdm_math_exact {
   // derivatives for the adjoint: d exp(x)/dx = exp(x), d log(x)/dx = 1/x
   template<class R>
