@@ -126,6 +126,11 @@ int fdm_set_stimulation(fdm_solver *s, const uint8_t *firing_events, int rows, i
                         const double *jitter, int n_jitter);
 /* per fiber: first clamped node (global index, -1 if none), number of clamped nodes, machine evaluated */
 int fdm_get_clamp_nodes(fdm_solver *s, int64_t *first_node, int *count, uint8_t *evaluated);
+/* replaces the clamp nodes fdm_set_stimulation chose (e.g. with a selection made for a larger layout) */
+int fdm_set_clamp_nodes(fdm_solver *s, const int64_t *first_node, const int *count, const uint8_t *evaluated);
+/* host-only: the clamp nodes of a fiber layout under a rule (the selection fdm_set_stimulation makes) */
+int fdm_select_clamp_nodes(int clamp_rule, int vc_width, int n_ranks, int n_fibers, const int64_t *fiber_offsets,
+                           const int *stimulation_point_index, int64_t *first_node, int *count, uint8_t *evaluated);
 
 /* which algebraics to return after each advance ("algebraicsForTransfer") */
 int fdm_set_algebraics_for_transfer(fdm_solver *s, int n, const int *algebraic_indices);

@@ -30,7 +30,8 @@ EXPORTED = [
     "fdm_get_trace", "fdm_advance", "fdm_split_steps", "fdm_get_timing", "fdm_reset_timing",
     "fdm_checkpoint_save", "fdm_checkpoint_restore", "fdm_fused_shapes", "fdm_diffusion_solve",
     "fdm_diffusion_solve_noalloc", "fdm_compat_configure", "fdm_compat_release", "fdm_adjoint_forward",
-    "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind",
+    "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
+    "fdm_select_clamp_nodes",
 ]
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
@@ -107,6 +108,8 @@ def lib() -> C.CDLL:
         "fdm_adjoint_release": (C.c_int, [P]),
         "fdm_adjoint_timing": (C.c_int, [P, d]),
         "fdm_rewind": (C.c_int, [P]),
+        "fdm_set_clamp_nodes": (C.c_int, [P, i64, i32, u8]),
+        "fdm_select_clamp_nodes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, i64, i32, i64, i32, u8]),
         "fdm_compat_release": (C.c_int, []),
         "initializeArrays": (None, [d, i32, i32, C.c_char_p, d, i32, i32, d, d, d, d]),
         "computeMonodomain": (None, [C.POINTER(C.c_float), d, d, C.POINTER(C.c_float), C.c_double, C.c_double,
@@ -150,3 +153,16 @@ def fused_shapes():
     m = np.zeros(64, np.int32)
     n = lib().fdm_fused_shapes(ptr(t, C.c_int), ptr(m, C.c_int), 64)
     return [(int(t[i]), int(m[i])) for i in range(n)]
+
+
+def select_clamp_nodes(rule: int, vc_width: int, n_ranks: int, fiber_offsets, stimulation_point_index):
+    """Host-only junction clamp selection of the library (first node, count, machine evaluated per fiber)."""
+    off = np.ascontiguousarray(fiber_offsets, np.int64)
+    c = np.ascontiguousarray(stimulation_point_index, np.int32)
+    nf = len(off) - 1
+    first = np.zeros(max(nf, 1), np.int64)
+    cnt = np.zeros(max(nf, 1), np.int32)
+    ev = np.zeros(max(nf, 1), np.uint8)
+    check(lib().fdm_select_clamp_nodes(rule, vc_width, n_ranks, nf, ptr(off, C.c_int64), ptr(c, C.c_int),
+                                       ptr(first, C.c_int64), ptr(cnt, C.c_int), ptr(ev, C.c_uint8)))
+    return first[:nf], cnt[:nf], ev[:nf]

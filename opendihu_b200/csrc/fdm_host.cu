@@ -800,20 +800,22 @@ extern "C" int fdm_get_parameters(fdm_solver* s, double* parameters)
 // its fibers concatenated (valuesOffset) and cut into buffers of W lanes; a buffer b is "in the centre"
 // of the fiber its first lane is attributed to by int(b * W / valuesLength[0]) when the junction index
 // falls inside it, and then lanes 0..min(3,W)-1 of b are clamped (compute.tpp:158-166, 03_generator_vc.cpp:1031-1038).
-static void select_clamp_vc(fdm_solver* s, const std::vector<int>& center)
+static void select_clamp_vc(int W, int R, int n_fibers, const int64_t* off, const int* center, int64_t* first_out,
+                            int* count_out, uint8_t* eval_out)
 {
-  const int W = s->cfg.vc_width, R = s->cfg.n_ranks;
-  s->clamp_first.assign(s->n_fibers, -1);
-  s->clamp_count.assign(s->n_fibers, 0);
-  s->evaluated.assign(s->n_fibers, 0);
+  for (int f = 0; f < n_fibers; f++) {
+    first_out[f] = -1;
+    count_out[f] = 0;
+    eval_out[f] = 0;
+  }
   for (int r = 0; r < R; r++) {
     std::vector<int> fib;
     std::vector<int64_t> vo;
     int64_t total = 0;
-    for (int f = r; f < s->n_fibers; f += R) {
+    for (int f = r; f < n_fibers; f += R) {
       fib.push_back(f);
       vo.push_back(total);
-      total += s->off[f + 1] - s->off[f];
+      total += off[f + 1] - off[f];
     }
     if (fib.empty())
       continue;
@@ -828,7 +830,7 @@ static void select_clamp_vc(fdm_solver* s, const std::vector<int>& center)
       const int f = fib[local];
       const int64_t index_in_fiber = b * W - vo[local];
       if ((unsigned long)((long)center[f] - (long)index_in_fiber) < (unsigned long)W) {
-        s->evaluated[f] = 1;
+        eval_out[f] = 1;
         int64_t first = -1;
         int cnt = 0;
         for (int lane = 0; lane < lanes; lane++) {
@@ -836,32 +838,49 @@ static void select_clamp_vc(fdm_solver* s, const std::vector<int>& center)
           if (i >= total)
             break;
           const size_t l2 = (size_t)(std::upper_bound(vo.begin(), vo.end(), i) - vo.begin()) - 1;
-          const int64_t g = s->off[fib[l2]] + (i - vo[l2]);
+          const int64_t g = off[fib[l2]] + (i - vo[l2]);
           if (first < 0)
             first = g;
           cnt++;
         }
-        s->clamp_first[f] = first;
-        s->clamp_count[f] = cnt;
+        first_out[f] = first;
+        count_out[f] = cnt;
       }
     }
   }
 }
 
 // junction node and its two neighbours inside the fiber (fast_monodomain_solver_gpu.tpp:538-540)
-static void select_clamp_center(fdm_solver* s, const std::vector<int>& center)
+static void select_clamp_center(int n_fibers, const int64_t* off, const int* center, int64_t* first_out,
+                                int* count_out, uint8_t* eval_out)
 {
-  s->clamp_first.assign(s->n_fibers, -1);
-  s->clamp_count.assign(s->n_fibers, 0);
-  s->evaluated.assign(s->n_fibers, 1);
-  for (int f = 0; f < s->n_fibers; f++) {
-    const int64_t n = s->off[f + 1] - s->off[f];
+  for (int f = 0; f < n_fibers; f++) {
+    first_out[f] = -1;
+    count_out[f] = 0;
+    eval_out[f] = 1;
+    const int64_t n = off[f + 1] - off[f];
     const int64_t lo = std::max<int64_t>(center[f] - 1, 0), hi = std::min<int64_t>(center[f] + 1, n - 1);
     if (hi < lo)
       continue;
-    s->clamp_first[f] = s->off[f] + lo;
-    s->clamp_count[f] = (int)(hi - lo + 1);
+    first_out[f] = off[f] + lo;
+    count_out[f] = (int)(hi - lo + 1);
   }
+}
+
+extern "C" int fdm_select_clamp_nodes(int clamp_rule, int vc_width, int n_ranks, int n_fibers,
+                                      const int64_t* fiber_offsets, const int* stimulation_point_index,
+                                      int64_t* first_node, int* count, uint8_t* evaluated)
+{
+  if (n_fibers < 0 || vc_width < 1 || n_ranks < 1 ||
+      (n_fibers > 0 && (!fiber_offsets || !stimulation_point_index || !first_node || !count || !evaluated)))
+    return fail(nullptr, FDM_ERR_ARG, "fdm_select_clamp_nodes: bad argument");
+  if (clamp_rule == FDM_CLAMP_VC_LANES)
+    select_clamp_vc(vc_width, n_ranks, n_fibers, fiber_offsets, stimulation_point_index, first_node, count, evaluated);
+  else if (clamp_rule == FDM_CLAMP_CENTER)
+    select_clamp_center(n_fibers, fiber_offsets, stimulation_point_index, first_node, count, evaluated);
+  else
+    return fail(nullptr, FDM_ERR_ARG, "fdm_select_clamp_nodes: unknown clamp rule");
+  return FDM_OK;
 }
 
 static int upload_clamp(fdm_solver* s)
@@ -939,15 +958,36 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
     FDM_CUDA(cudaMemcpyAsync(s->hbs.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaStreamSynchronize(s->stream));
   }
+  s->clamp_first.assign(nf, -1);
+  s->clamp_count.assign(nf, 0);
+  s->evaluated.assign(nf, 0);
   if (s->cfg.clamp_rule == FDM_CLAMP_VC_LANES)
-    select_clamp_vc(s, center);
+    select_clamp_vc(s->cfg.vc_width, s->cfg.n_ranks, nf, s->off.data(), center.data(), s->clamp_first.data(),
+                    s->clamp_count.data(), s->evaluated.data());
   else
-    select_clamp_center(s, center);
+    select_clamp_center(nf, s->off.data(), center.data(), s->clamp_first.data(), s->clamp_count.data(),
+                        s->evaluated.data());
   int rc = upload_clamp(s);
   if (rc)
     return rc;
   s->stimulation_set = true;
   return FDM_OK;
+}
+
+extern "C" int fdm_set_clamp_nodes(fdm_solver* s, const int64_t* first_node, const int* count,
+                                   const uint8_t* evaluated)
+{
+  if (!s || !s->stimulation_set || !first_node || !count || !evaluated)
+    return fail(s, FDM_ERR_ARG, "fdm_set_clamp_nodes: call fdm_set_stimulation first; no null arrays");
+  FDM_BIND(s);
+  for (int f = 0; f < s->n_fibers; f++)
+    if (count[f] < 0 || (count[f] > 0 && (first_node[f] < 0 || first_node[f] + count[f] > s->n_nodes)))
+      return fail(s, FDM_ERR_ARG, "fdm_set_clamp_nodes: clamp nodes out of range");
+  s->clamp_first.assign(first_node, first_node + s->n_fibers);
+  s->clamp_count.assign(count, count + s->n_fibers);
+  s->evaluated.assign(evaluated, evaluated + s->n_fibers);
+  invalidate_graphs(s);
+  return upload_clamp(s);
 }
 
 extern "C" int fdm_get_clamp_nodes(fdm_solver* s, int64_t* first_node, int* count, uint8_t* evaluated)

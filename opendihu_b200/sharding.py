@@ -1,0 +1,297 @@
+"""Fiber sharding across devices (multi-GPU without a data-path collective).
+
+The reference distributes the fibers of a muscle over MPI ranks; its FastMonodomainSolver then gathers every
+fiber onto one rank and solves it there (fast_monodomain_solver_communication.tpp:13-228), so that a fiber is
+always solved whole by one process and fibers never exchange data during a solve.  Here a fiber system is
+split into shards of whole fibers, one shard per GPU, balanced by the longest-processing-time rule on node
+counts (the work of a fiber is proportional to its nodes).  Each shard is an ordinary
+:class:`~opendihu_b200.solver.FastMonodomainSolver` on its own device and stream; nothing crosses devices
+while they run.  The only exchange is the optional end-of-interval gather of Vm / states into the global node
+order (host arrays here, or ``torch.distributed`` gather for one-process-per-GPU jobs).
+
+Results are identical to the unsharded solve: a shard keeps each fiber's geometry, stimulation inputs,
+parameters and states, and its junction clamp nodes are those the unsharded layout selects
+(:func:`opendihu_b200._native.select_clamp_nodes` on the whole system, mapped to shard-local node indices),
+since the "vc" clamp rule depends on how all fibers of a rank are laid out together.
+"""
+from __future__ import annotations
+
+import heapq
+import threading
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from .solver import CLAMP_RULES, FastMonodomainSolver, FiberSystem
+
+
+def lpt_partition(weights: Sequence[int], n_shards: int) -> List[np.ndarray]:
+    """Longest-processing-time assignment: items by decreasing weight (ties by index), each to the shard with
+    the least total so far (ties by shard number).  Returns the item indices of every shard in ascending
+    order.  Deterministic, so every rank of a distributed job computes the same partition."""
+    if n_shards < 1:
+        raise ValueError("n_shards must be >= 1")
+    w = np.asarray(weights, np.int64)
+    order = sorted(range(len(w)), key=lambda i: (-int(w[i]), i))
+    heap = [(0, k) for k in range(n_shards)]
+    parts: List[List[int]] = [[] for _ in range(n_shards)]
+    for i in order:
+        load, k = heapq.heappop(heap)
+        parts[k].append(i)
+        heapq.heappush(heap, (load + int(w[i]), k))
+    return [np.asarray(sorted(p), np.int64) for p in parts]
+
+
+def subset(system: FiberSystem, fibers) -> FiberSystem:
+    """The given fibers of a system, as a system of their own (same per-fiber inputs, node order = the given
+    fiber order)."""
+    fibers = np.asarray(fibers, np.int64)
+    off = np.asarray(system.fiber_offsets, np.int64)
+    lengths = off[fibers + 1] - off[fibers]
+    new_off = np.zeros(len(fibers) + 1, np.int64)
+    new_off[1:] = np.cumsum(lengths)
+    elem = np.asarray(system.element_lengths)
+    elem = np.concatenate([elem[off[f] - f:off[f + 1] - f - 1] for f in fibers]) if len(fibers) else elem[:0]
+    nodes = node_index(off, fibers)
+    s = system.copy()
+    s.fiber_offsets = new_off
+    s.element_lengths = elem
+    for name in ("prefactor", "motor_unit_no", "stimulation_point_index", "call_frequency",
+                 "repeat_after_first_call", "call_enable_begin"):
+        setattr(s, name, np.asarray(getattr(system, name))[fibers].copy())
+    if system.jitter is not None and np.asarray(system.jitter).size:
+        s.jitter = np.asarray(system.jitter)[fibers].copy()
+    else:
+        s.jitter = np.zeros((len(fibers), 0))
+    if system.parameters is not None:
+        s.parameters = np.asarray(system.parameters)[:, nodes].copy()
+    if system.states is not None:
+        s.states = np.asarray(system.states)[:, nodes].copy()
+    return s
+
+
+def node_index(fiber_offsets, fibers) -> np.ndarray:
+    """Global node indices of the given fibers, concatenated in the given order."""
+    off = np.asarray(fiber_offsets, np.int64)
+    fibers = np.asarray(fibers, np.int64)
+    if not len(fibers):
+        return np.zeros(0, np.int64)
+    return np.concatenate([np.arange(off[f], off[f + 1]) for f in fibers])
+
+
+def global_clamp_nodes(system: FiberSystem):
+    """Clamp nodes (first node, count, evaluated per fiber) that the unsharded system selects."""
+    return N.select_clamp_nodes(CLAMP_RULES[system.clamp_rule], int(system.vc_width), int(system.n_ranks),
+                                system.fiber_offsets, system.stimulation_point_index)
+
+
+def shard_clamp_nodes(system: FiberSystem, fibers, clamp):
+    """The global clamp selection restricted to the given fibers, as shard-local node indices."""
+    first, cnt, ev = clamp
+    fibers = np.asarray(fibers, np.int64)
+    off = np.asarray(system.fiber_offsets, np.int64)
+    lengths = off[fibers + 1] - off[fibers]
+    local_off = np.concatenate([[0], np.cumsum(lengths)[:-1]]).astype(np.int64)
+    f_first = first[fibers]
+    local_first = np.where(f_first >= 0, f_first - off[fibers] + local_off, -1).astype(np.int64)
+    return local_first, cnt[fibers].astype(np.int32), ev[fibers].astype(np.uint8)
+
+
+class ShardedSolver:
+    """One fiber system solved as LPT shards on several devices (or several shards on one device).
+
+    Mirrors the operator API of :class:`FastMonodomainSolver` (``initialize``, ``setTimeSpan``,
+    ``advanceTimeSpan``, ``run``, ``states``, ``vm``, ``set_states``, ``parameters``, checkpoints, adjoint) on
+    the global node order.  Each shard's calls run on their own host thread so that devices advance
+    concurrently (the C ABI releases the interpreter lock for the length of every call)."""
+
+    def __init__(self, system: FiberSystem, devices: Sequence[int] = (0,), n_shards: Optional[int] = None,
+                 **solver_kw):
+        self.system = system
+        devices = list(devices)
+        n = int(n_shards or len(devices))
+        if n < 1 or not devices:
+            raise ValueError("need at least one shard and one device")
+        lengths = np.diff(np.asarray(system.fiber_offsets, np.int64))
+        self.fibers = lpt_partition(lengths, n)
+        self.devices = [devices[k % len(devices)] for k in range(n)]
+        clamp = global_clamp_nodes(system)
+        self.nodes = [node_index(system.fiber_offsets, f) for f in self.fibers]
+        self.shards: List[Optional[FastMonodomainSolver]] = []
+        for fib, dev in zip(self.fibers, self.devices):
+            if not len(fib):
+                self.shards.append(None)
+                continue
+            sub = subset(system, fib)
+            sv = FastMonodomainSolver(sub, device=dev, **solver_kw)
+            sv.clamp_override = shard_clamp_nodes(system, fib, clamp)
+            self.shards.append(sv)
+        self._start = system.start_time
+        self._end = system.end_time
+
+    # -- parallel dispatch ------------------------------------------------------------------------
+    def _each(self, fn):
+        """fn(shard_index, solver) on every non-empty shard, one host thread per shard; re-raises the first
+        error after all threads joined."""
+        results: Dict[int, object] = {}
+        errors: List[BaseException] = []
+
+        def work(k, sv):
+            try:
+                results[k] = fn(k, sv)
+            except BaseException as e:  # noqa: BLE001 - re-raised below
+                errors.append(e)
+
+        live = [(k, sv) for k, sv in enumerate(self.shards) if sv is not None]
+        if len(live) == 1:
+            work(*live[0])
+        else:
+            th = [threading.Thread(target=work, args=(k, sv)) for k, sv in live]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+        if errors:
+            raise errors[0]
+        return results
+
+    # -- lifecycle and the operator API ----------------------------------------------------------
+    def initialize(self):
+        self._each(lambda k, sv: sv.initialize())
+
+    def close(self):
+        for sv in self.shards:
+            if sv is not None:
+                sv.close()
+
+    def __enter__(self):
+        self.initialize()
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def setTimeSpan(self, start_time: float, end_time: float):
+        self._start, self._end = float(start_time), float(end_time)
+        for sv in self.shards:
+            if sv is not None:
+                sv.setTimeSpan(start_time, end_time)
+
+    def startTime(self) -> float:
+        return self._start
+
+    def endTime(self) -> float:
+        return self._end
+
+    def advanceTimeSpan(self, withOutputWritersEnabled: bool = True):
+        self._each(lambda k, sv: sv.advanceTimeSpan(withOutputWritersEnabled))
+
+    def run(self):
+        self.initialize()
+        self.advanceTimeSpan()
+
+    def saveFiberDataCheckpoint(self):
+        self._each(lambda k, sv: sv.saveFiberDataCheckpoint())
+
+    def restoreFiberDataCheckpoint(self):
+        self._each(lambda k, sv: sv.restoreFiberDataCheckpoint())
+
+    def rewind(self):
+        self._each(lambda k, sv: sv.rewind())
+
+    # -- gathers into the global node order -----------------------------------------------------
+    def _gather_rows(self, per_shard: Dict[int, np.ndarray], n_rows: int) -> np.ndarray:
+        out = np.zeros((n_rows, self.system.n_nodes))
+        for k, a in per_shard.items():
+            out[:, self.nodes[k]] = a
+        return out
+
+    def states(self) -> np.ndarray:
+        r = self._each(lambda k, sv: sv.states())
+        return self._gather_rows(r, next(iter(r.values())).shape[0])
+
+    def vm(self) -> np.ndarray:
+        r = self._each(lambda k, sv: sv.vm()[None, :])
+        return self._gather_rows(r, 1)[0]
+
+    def algebraics(self) -> np.ndarray:
+        r = self._each(lambda k, sv: sv.algebraics())
+        return self._gather_rows(r, len(self.system.algebraics_for_transfer))
+
+    def parameters(self) -> np.ndarray:
+        r = self._each(lambda k, sv: sv.parameters())
+        return self._gather_rows(r, next(iter(r.values())).shape[0])
+
+    def set_states(self, states: np.ndarray):
+        states = np.asarray(states, np.float64)
+        self._each(lambda k, sv: sv.set_states(states[:, self.nodes[k]]))
+
+    def set_parameters(self, params: np.ndarray):
+        params = np.asarray(params, np.float64)
+        self._each(lambda k, sv: sv.set_parameters(params[:, self.nodes[k]]))
+
+    def set_prefactor(self, prefactor: np.ndarray):
+        prefactor = np.asarray(prefactor, np.float64)
+        self._each(lambda k, sv: sv.set_prefactor(prefactor[self.fibers[k]]))
+
+    def split_steps(self) -> int:
+        return max(sv.split_steps() for sv in self.shards if sv is not None)
+
+    def timing(self) -> List[Dict[str, float]]:
+        return [sv.timing() if sv is not None else None for sv in self.shards]
+
+    # -- adjoint: every shard differentiates its own fibers -------------------------------------
+    def adjoint_forward(self, t_start: float, t_end: float, checkpoint_every: int, sensor_nodes) -> np.ndarray:
+        """Checkpointed forward of every shard; returns the trace [steps, sensors] in the given sensor order."""
+        sensor_nodes = np.asarray(sensor_nodes, np.int64)
+        owner = np.full(self.system.n_nodes, -1, np.int64)
+        local = np.zeros(self.system.n_nodes, np.int64)
+        for k, nodes in enumerate(self.nodes):
+            owner[nodes] = k
+            local[nodes] = np.arange(len(nodes))
+        self._sensor_split = {k: np.nonzero(owner[sensor_nodes] == k)[0] for k in range(len(self.shards))}
+        r = self._each(lambda k, sv: sv.adjoint_forward(t_start, t_end, checkpoint_every,
+                                                        local[sensor_nodes[self._sensor_split[k]]]))
+        steps = max(a.shape[0] for a in r.values())
+        out = np.zeros((steps, len(sensor_nodes)))
+        for k, a in r.items():
+            out[:a.shape[0], self._sensor_split[k]] = a
+        return out
+
+    def adjoint_backward(self, trace_grad: np.ndarray) -> Dict[str, np.ndarray]:
+        tg = np.asarray(trace_grad, np.float64)
+        r = self._each(lambda k, sv: sv.adjoint_backward(tg[:, self._sensor_split[k]]))
+        nf, nn = self.system.n_fibers, self.system.n_nodes
+        any_r = next(iter(r.values()))
+        g = {"prefactor": np.zeros(nf), "parameters": np.zeros((any_r["parameters"].shape[0], nn)),
+             "states0": np.zeros((any_r["states0"].shape[0], nn))}
+        for k, a in r.items():
+            g["prefactor"][self.fibers[k]] = a["prefactor"]
+            g["parameters"][:, self.nodes[k]] = a["parameters"]
+            g["states0"][:, self.nodes[k]] = a["states0"]
+        return g
+
+
+def rank_shard(system: FiberSystem, rank: int, world: int):
+    """The shard of one rank of a one-process-per-GPU job: (fiber indices, shard system, clamp override)."""
+    fibers = lpt_partition(np.diff(np.asarray(system.fiber_offsets, np.int64)), world)[rank]
+    return fibers, subset(system, fibers), shard_clamp_nodes(system, fibers, global_clamp_nodes(system))
+
+
+def gather_to_root(pg, system: FiberSystem, fibers, local_rows: np.ndarray, root: int = 0):
+    """End-of-interval gather of per-rank rows [rows, shard nodes] into the global node order on ``root``
+    (``torch.distributed``; returns None on the other ranks).  Object gather: an end-of-interval copy, not
+    part of the time-stepping."""
+    import torch.distributed as dist
+    rank = dist.get_rank(pg)
+    world = dist.get_world_size(pg)
+    payload = (np.asarray(fibers, np.int64), np.asarray(local_rows))
+    got = [None] * world if rank == root else None
+    dist.gather_object(payload, got, dst=root, group=pg)
+    if rank != root:
+        return None
+    out = np.zeros((payload[1].shape[0], system.n_nodes))
+    for fib, rows in got:
+        out[:, node_index(system.fiber_offsets, fib)] = rows
+    return out

@@ -320,6 +320,9 @@ class FastMonodomainSolver:
         self.device = int(device)
         self.autotune = bool(autotune)
         self.tuning = None
+        #: (first_node, count, evaluated) per fiber replacing the clamp selection of fdm_set_stimulation
+        #: (set by the sharded solver to keep the selection of the unsharded layout)
+        self.clamp_override = None
         self._h = None
         self._start = system.start_time
         self._end = system.end_time
@@ -382,6 +385,11 @@ class FastMonodomainSolver:
                 st = np.ascontiguousarray(s.states, np.float64)
                 self._call(L.fdm_set_states, N.ptr(st, C.c_double))
             self._set_stimulation()
+            if self.clamp_override is not None:
+                first, cnt, ev = (np.ascontiguousarray(a, t) for a, t in
+                                  zip(self.clamp_override, (np.int64, np.int32, np.uint8)))
+                self._call(L.fdm_set_clamp_nodes, N.ptr(first, C.c_int64), N.ptr(cnt, C.c_int),
+                           N.ptr(ev, C.c_uint8))
             if len(s.algebraics_for_transfer):
                 idx = np.ascontiguousarray(s.algebraics_for_transfer, np.int32)
                 self._call(L.fdm_set_algebraics_for_transfer, len(idx), N.ptr(idx, C.c_int))

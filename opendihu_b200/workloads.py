@@ -10,6 +10,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import inputs
+from .sharding import subset  # noqa: F401  (re-exported: the given fibers as a system)
 from .solver import FiberSystem, uniform_fibers
 
 HH = "hodgkin_huxley_1952"
@@ -54,32 +55,6 @@ def shorten_grid(n_fibers: int = 1369, n_nodes: int = 1481, end_time: float = 50
     return uniform_fibers(SHORTEN, [n_nodes] * n_fibers, 0.01, SIGMA / (AM * 0.58), firing_events=firing,
                           motor_unit_no=mus, call_frequency=0.1, repeat_after_first_call=0.1, call_enable_begin=0.0,
                           end_time=end_time, dt_0d=1e-5, dt_1d=5e-4, dt_splitting=5e-4, dt_repeated_call=5e-4, **kw)
-
-
-def subset(system: FiberSystem, fibers) -> FiberSystem:
-    """The given fibers of a system, as a system of their own (same per-fiber inputs)."""
-    fibers = np.asarray(fibers)
-    off = system.fiber_offsets
-    lengths = off[fibers + 1] - off[fibers]
-    new_off = np.zeros(len(fibers) + 1, np.int64)
-    new_off[1:] = np.cumsum(lengths)
-    elem = np.concatenate([system.element_lengths[off[f] - f:off[f + 1] - f - 1] for f in fibers])
-    nodes = np.concatenate([np.arange(off[f], off[f + 1]) for f in fibers])
-    s = system.copy()
-    s.fiber_offsets = new_off
-    s.element_lengths = elem
-    for name in ("prefactor", "motor_unit_no", "stimulation_point_index", "call_frequency",
-                 "repeat_after_first_call", "call_enable_begin"):
-        setattr(s, name, np.asarray(getattr(system, name))[fibers].copy())
-    if system.jitter is not None and np.asarray(system.jitter).size:
-        s.jitter = np.asarray(system.jitter)[fibers].copy()
-    else:
-        s.jitter = np.zeros((len(fibers), 0))
-    if system.parameters is not None:
-        s.parameters = system.parameters[:, nodes].copy()
-    if system.states is not None:
-        s.states = system.states[:, nodes].copy()
-    return s
 
 
 def differentiation_hh(n_fibers: int = 256, n_nodes: int = 1481, end_time: float = 20.0, n_sensors: int = 32,
