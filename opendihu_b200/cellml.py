@@ -640,39 +640,171 @@ _LOG2E = 1.4426950408889634
 _LN2 = 0.6931471805599453
 
 
-class _FastEmitter(_Emitter):
-    """FP32 form of the right-hand side: shared exponentials (see _exp_groups), every exponential as one
-    SFU ex2 of an argument whose log2(e) scaling and affine coefficients are folded at generation time,
-    divisions by constants as multiplications, other divisions as a multiplication by the SFU reciprocal."""
+def _uses_algebraic(e) -> bool:
+    t = e[0]
+    if t == "var":
+        return e[1] in ("A", "R")
+    if t == "call":
+        return any(_uses_algebraic(x) for x in e[2])
+    if t in ("neg", "pos", "not"):
+        return _uses_algebraic(e[1])
+    if t == "bin":
+        return _uses_algebraic(e[2]) or _uses_algebraic(e[3])
+    if t == "tern":
+        return any(_uses_algebraic(x) for x in e[1:4])
+    return False
 
-    def __init__(self, real, consts, repl):
+
+def _batched_denominators(lines, consts, max_group: int = 3):
+    """Denominators of divisions that depend on states, parameters, time and constants only (no algebraic
+    variables) and are not constants, in order of first appearance; grouped by max_group for a batched
+    reciprocal (one SFU reciprocal per group, see fdm_rcp_batch)."""
+    seen = []
+
+    def walk(e):
+        t = e[0]
+        if t == "bin":
+            if e[1] == "/":
+                den = e[3]
+                af = _affine(den, consts)
+                if not (af is not None and not af[0]) and not _uses_algebraic(den) and repr(den) not in seen:
+                    seen.append(repr(den))
+                    found.append(den)
+            walk(e[2])
+            walk(e[3])
+        elif t == "call":
+            for x in e[2]:
+                walk(x)
+        elif t in ("neg", "pos", "not"):
+            walk(e[1])
+        elif t == "tern":
+            for x in e[1:4]:
+                walk(x)
+    found = []
+    for _, _, e in lines:
+        walk(e)
+    groups = [found[i:i + max_group] for i in range(0, len(found), max_group)]
+    return [g for g in groups if len(g) >= 2]
+
+
+class _FastEmitter(_Emitter):
+    """FP32 form of the right-hand side, written for the fewest instructions:
+      - shared exponentials (see _exp_groups); every exponential one SFU ex2 of an argument whose log2(e)
+        scaling and affine coefficients are folded at generation time; a positive constant factor of an
+        exponential goes into its argument (c e^u = e^(u + ln c));
+      - affine subexpressions c (x + k) as one fused multiply-add (c x + c k);
+      - the gate form a (1 - s) - b s as a - (a + b) s;
+      - divisions by constants as multiplications, other divisions as a multiplication by a reciprocal;
+        denominators free of algebraic variables share one SFU reciprocal per group of up to three
+        (fdm_rcp_batch: 1/d_k from 1/(d_0 d_1 d_2) and the other factors)."""
+
+    def __init__(self, real, consts, repl, paired: bool = False, recip=None):
         super().__init__(real, consts, "cuda")
         self.repl = repl
+        self.paired = paired        # fdm_f2 operands: conditional expressions become per-component selects
+        self.recip = recip or {}    # repr(denominator) -> name of its batched reciprocal
+
+    def coef_text(self, v, x):
+        if v == 1.0:
+            return x
+        if v == -1.0:
+            return f"(-{x})"
+        return f"(({self.real}){_hexf(v)}) * {x}"
 
     def affine_text(self, coeffs, const, scale):
-        terms = [f"(({self.real}){_hexf(v * scale)}) * {self.var(k[0], k[1])}" for k, v in coeffs]
+        terms = [self.coef_text(v * scale, self.var(k[0], k[1])) for k, v in coeffs]
         if const != 0.0:
             terms.append(f"(({self.real}){_hexf(const * scale)})")
         return " + ".join(terms) if terms else f"(({self.real})0)"
 
+    def _positive_const(self, e):
+        af = _affine(e, self.consts)
+        if af is not None and not af[0] and af[1] > 0.0:
+            return af[1]
+        return None
+
+    def exp_text(self, e, factor: float = 1.0):
+        """factor * exp(arg) for the exp call node e (factor > 0)"""
+        if repr(e) in self.repl:
+            g, b = self.repl[repr(e)]
+            return f"(fdm_e{g} * (({self.real}){_hexf(math.exp(b) * factor)}))"
+        af = _affine(e[2][0], self.consts)
+        if af is not None:
+            return f"fdm_ex2({self.affine_text(sorted(af[0].items()), af[1] + math.log(factor), _LOG2E)})"
+        arg = f"(({self.real}){_hexf(_LOG2E)}) * {self.expr(e[2][0])}"
+        if factor != 1.0:
+            arg = f"{arg} + (({self.real}){_hexf(math.log(factor) * _LOG2E)})"
+        return f"fdm_ex2({arg})"
+
     def expr(self, e):
         t = e[0]
         if t == "call" and e[1] == "exp":
-            if repr(e) in self.repl:
-                g, b = self.repl[repr(e)]
-                return f"(fdm_e{g} * (({self.real}){_hexf(math.exp(b))}))"
-            af = _affine(e[2][0], self.consts)
-            if af is not None:
-                return f"fdm_ex2({self.affine_text(sorted(af[0].items()), af[1], _LOG2E)})"
-            return f"fdm_ex2((({self.real}){_hexf(_LOG2E)}) * {self.expr(e[2][0])})"
+            return self.exp_text(e)
         if t == "call" and e[1] == "log":
             return f"(fdm_lg2({self.expr(e[2][0])}) * (({self.real}){_hexf(_LN2)}))"
+        if t == "bin" and e[1] == "*":
+            for c_side, x_side in ((e[2], e[3]), (e[3], e[2])):
+                c = self._positive_const(c_side)
+                if c is not None and x_side[0] == "call" and x_side[1] == "exp":
+                    return self.exp_text(x_side, c)
+        if (t == "bin" and e[1] in "*/") or t == "neg":
+            af = _affine(e, self.consts)
+            if af is not None and af[0]:
+                return f"({self.affine_text(sorted(af[0].items()), af[1], 1.0)})"
+        if t == "neg":
+            return self.neg_text(e[1])
+        if t == "bin" and e[1] == "-":
+            # a (1 - s) - b s  ->  a - (a + b) s, for variables a, b, s
+            l, r = e[2], e[3]
+            if l[0] == "bin" and l[1] == "*" and r[0] == "bin" and r[1] == "*":
+                a, one_minus = l[2], l[3]
+                b, s2 = r[2], r[3]
+                if (one_minus[0] == "bin" and one_minus[1] == "-" and _affine(one_minus[2], self.consts) == ({}, 1.0)
+                        and a[0] == "var" and b[0] == "var" and s2[0] == "var" and repr(one_minus[3]) == repr(s2)):
+                    A, B, S = self.expr(a), self.expr(b), self.expr(s2)
+                    return f"({A} - ({A} + {B}) * {S})"
         if t == "bin" and e[1] == "/":
             den = _affine(e[3], self.consts)
             if den is not None and not den[0] and den[1] != 0.0:
+                if den[1] == 1.0:
+                    return self.expr(e[2])
                 return f"({self.expr(e[2])} * (({self.real}){_hexf(1.0 / den[1])}))"
-            return f"({self.expr(e[2])} * fdm_rcp({self.expr(e[3])}))"
+            num = _affine(e[2], self.consts)
+            inv = self.recip.get(repr(e[3])) or f"fdm_rcp({self.expr(e[3])})"
+            if num is not None and not num[0] and num[1] == 1.0:
+                return inv
+            return f"({self.expr(e[2])} * {inv})"
+        if t == "tern" and self.paired:
+            return f"fdm_sel({self.expr(e[1])}, {self.expr(e[2])}, {self.expr(e[3])})"
         return super().expr(e)
+
+    def neg_text(self, e):
+        """-(e) with the negation pushed through sums to a single leaf: -((a + b) - c) = (-a - b) + c"""
+        t = e[0]
+        if t == "neg":
+            return self.expr(e[1])
+        if t == "bin" and e[1] == "+":
+            return f"({self.neg_text(e[2])} - {self.expr(e[3])})"
+        if t == "bin" and e[1] == "-":
+            return f"({self.neg_text(e[2])} + {self.expr(e[3])})"
+        return f"(-{self.expr(e)})"
+
+    def batch_lines(self, groups):
+        """Declarations of the batched reciprocals (after the shared exponentials); fills self.recip."""
+        out = []
+        k = 0
+        for g in groups:
+            names = []
+            for den in g:
+                out.append(f"    const R fdm_d{k} = {self.expr(den)};")
+                names.append(k)
+                k += 1
+            out.append("    R " + ", ".join(f"fdm_r{j}" for j in names) + ";")
+            args = ", ".join(f"fdm_d{j}" for j in names) + ", " + ", ".join(f"fdm_r{j}" for j in names)
+            out.append(f"    fdm_rcp_batch({args});")
+            for j, den in zip(names, g):
+                self.recip[repr(den)] = f"fdm_r{j}"
+        return out
 
 
 def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> str:
@@ -726,6 +858,7 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     out.append("  }")
     # FP32 variant with shared exponentials
     repl, groups = _exp_groups(lines, model.constants)
+    rgroups = _batched_denominators(lines, model.constants)
     fem = _FastEmitter("R", model.constants, repl)
     out.append("  // FP32 form: exponentials exp(a.x + b_k) that share a.x are evaluated once as exp(a.x) * e^{b_k};")
     out.append("  // exponentials, logarithms and reciprocals as single SFU instructions (fdm_ex2/fdm_lg2/fdm_rcp)")
@@ -743,12 +876,36 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     out.extend("#define " + s2.split("#define ", 1)[1] for s2 in _pow_macro_defs(pows))
     for g, key in enumerate(groups):
         out.append(f"    const R fdm_e{g} = fdm_ex2({fem.affine_text(list(key), 0.0, _LOG2E)});")
+    out.extend(fem.batch_lines(rgroups))
     for kind, idx, expr in lines:
         tgt = f"ALGEBRAIC[{idx}]" if kind == "A" else f"RATES[{idx}]"
         out.append(f"    {tgt} = {fem.expr(expr)};")
     for n in pows:
         out.append(f"#undef FDM_POW{n}")
     out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
+    out.append("  }")
+    # the same FP32 form over node pairs (packed FP32 instructions)
+    fem2 = _FastEmitter("R", model.constants, repl, paired=True)
+    out.append("  // paired FP32 form: the FP32 form over two nodes at once (fdm_f2, packed FP32 instructions)")
+    out.append("  template<class M>")
+    out.append("  __device__ __forceinline__ static void rates_fast2(const fdm_f2 VOI, const fdm_f2* __restrict__ STATES,"
+               " const fdm_f2* __restrict__ PARAMS, fdm_f2* __restrict__ RATES, fdm_f2* __restrict__ ALGEBRAIC)")
+    out.append("  {")
+    out.append("    typedef fdm_f2 R;")
+    out.append("    (void)VOI; (void)PARAMS;")
+    out.append("#define FDM_POWF(x, y) fdm_powf_pair(x, y)")
+    out.append("#define FDM_ABS(x) fabs(x)")
+    out.append("#define FDM_SQRT(x) sqrt(x)")
+    out.extend("#define " + s2.split("#define ", 1)[1] for s2 in _pow_macro_defs(pows))
+    for g, key in enumerate(groups):
+        out.append(f"    const R fdm_e{g} = fdm_ex2({fem2.affine_text(list(key), 0.0, _LOG2E)});")
+    out.extend(fem2.batch_lines(rgroups))
+    for kind, idx, expr in lines:
+        tgt = f"ALGEBRAIC[{idx}]" if kind == "A" else f"RATES[{idx}]"
+        out.append(f"    {tgt} = {fem2.expr(expr)};")
+    for n in pows:
+        out.append(f"#undef FDM_POW{n}")
+    out.append("#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
     out.append("  }")
     # reverse mode (adjoint)
     out.append("  // vector-Jacobian product: LAM_STATES += J^T LAM_RATES, LAM_PARAMS += (dRATES/dPARAMS)^T LAM_RATES")

@@ -12,8 +12,10 @@
   X(256, 8)                 \
   X(256, 10)                \
   X(384, 7)                 \
+  X(384, 8)                 \
   X(512, 3)                 \
   X(512, 5)                 \
+  X(512, 6)                 \
   X(640, 4)                 \
   X(768, 4)                 \
   X(1024, 3)

@@ -227,6 +227,58 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __r
   }
 }
 
+// The FP32 Heun step of two nodes at once, over fdm_f2 pairs (packed FP32 instructions): Vm of each
+// node in FP64; every other state is a pair (S, L) whose sum is its value.  Within a half step the
+// increments dt/2 (f + f*) are summed into L and the right-hand side sees S + L; normalize_pair
+// folds L back into S (Fast2Sum) at the end of the half step.  L stays of the size of a few
+// increments, so no increment is lost against S (the stagnation the compensation exists for) at
+// four packed operations per state and substep instead of the seven of a Fast2Sum per substep.
+// Used with the FP32 exact-exponential policy only.
+template<class Model>
+__device__ __forceinline__ void heun_step2(double& V0, double& V1, const fdm_f2* __restrict__ S,
+                                           fdm_f2* __restrict__ L, const fdm_f2* __restrict__ P, double t,
+                                           float dt, bool clamp0, bool clamp1, double vstim)
+{
+  constexpr int NS = Model::nStates;
+  fdm_f2 y[NS], r[NS], ys[NS], r2[NS];
+  fdm_f2 alg[Model::nAlgebraics];
+  y[0] = fdm_f2((float)V0, (float)V1);
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    y[s] = S[s - 1] + L[s - 1];
+  const fdm_f2 tr((float)t);
+  Model::template rates_fast2<fdm_math_exact>(tr, y, P, r, alg);
+  const fdm_f2 dtr(dt);
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    ys[s] = dtr * r[s] + y[s];
+  const float vs = (float)vstim;
+  if (clamp0)
+    ys[0].v.x = vs;
+  if (clamp1)
+    ys[0].v.y = vs;
+  Model::template rates_fast2<fdm_math_exact>(tr, ys, P, r2, alg);
+  const fdm_f2 hdt(0.5f * dt);
+  const fdm_f2 dv = hdt * (r[0] + r2[0]);
+  V0 += (double)dv.v.x;
+  V1 += (double)dv.v.y;
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    L[s - 1] = hdt * (r[s] + r2[s]) + L[s - 1];
+  if (clamp0)
+    V0 = vstim;
+  if (clamp1)
+    V1 = vstim;
+}
+
+// (S, L) -> (S + L rounded, the rounding error): the Fast2Sum normalization of a compensated pair
+__device__ __forceinline__ void normalize_pair(fdm_f2& S, fdm_f2& L)
+{
+  const fdm_f2 t = S + L;
+  L = L - (t - S);
+  S = t;
+}
+
 // algebraicsForTransfer: copy the requested entries (selected at run time) without dynamic
 // register indexing
 template<class Model, class RR>
@@ -821,11 +873,14 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
   constexpr int CAP = T * M;
   extern __shared__ double smem[];
-  double* sc = smem;                 // 6 x CAP coefficients
-  double* vfirst = sc + 6 * CAP;     // T
+  // 5 x CAP coefficients: mulF, cp, and the right-hand side stencil l, m, r premultiplied by inv
+  double* sc = smem;
+  double* vfirst = sc + 5 * CAP;     // T
   double* vlast = vfirst + T;        // T
   double* sF = vlast + T;            // 2 * (T/32)
   double* sG = sF + 2 * (T / 32);    // 2 * (T/32)
+  int* s_cf = (int*)(sG + 2 * (T / 32)); // CAP: clamp fiber of each node (-1: not a junction node)
+  int* s_ts = s_cf + CAP;                // CAP: trace slot of each node (-1: not traced)
   __shared__ int64_t fib_global[FUSED_MAX_FIBERS_PER_BIN];
   __shared__ int fib_local[FUSED_MAX_FIBERS_PER_BIN + 1];
 
@@ -855,13 +910,17 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     return fib_global[k] + (q - fib_local[k]);
   };
 
-  // coefficients into shared memory (zero beyond the bin: those nodes carry x = 0)
+  // coefficients into shared memory (zero beyond the bin: those nodes carry x = 0); the forward sweep's
+  // inv * d is formed as (inv l) u_{i-1} + (inv m) u_i + (inv r) u_{i+1}
   for (int q = tid; q < CAP; q += T) {
     const bool ok = q < nb;
     const int64_t g = ok ? global_node(q) : 0;
+    const double inv = ok ? a.coef[1 * a.stride + g] : 0.0;
+    sc[0 * CAP + q] = ok ? a.coef[0 * a.stride + g] : 0.0;
+    sc[1 * CAP + q] = ok ? a.coef[2 * a.stride + g] : 0.0;
 #pragma unroll
-    for (int k = 0; k < 6; k++)
-      sc[k * CAP + q] = ok ? a.coef[k * a.stride + g] : 0.0;
+    for (int k = 3; k < 6; k++)
+      sc[(k - 1) * CAP + q] = ok ? inv * a.coef[k * a.stride + g] : 0.0;
   }
 
   const RR* pr = (const RR*)a.params;
@@ -871,15 +930,12 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   RR S[M][NS > 1 ? NS - 1 : 1];
   RR L[M][NS > 1 ? NS - 1 : 1];
   RR P[M][NP];
-  int cf[M];
-  int ts[M];
-  int64_t gi[M];
+  unsigned cmask = 0u; // bit j: node j is a junction node (its clamp fiber in s_cf)
 #pragma unroll
   for (int j = 0; j < M; j++) {
     const int q = tid * M + j;
     const bool ok = q < nb;
     const int64_t i = ok ? global_node(q) : 0;
-    gi[j] = i;
     V[j] = ok ? a.vm[i] : 0.0;
 #pragma unroll
     for (int s = 1; s < NS; s++) {
@@ -889,9 +945,92 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 #pragma unroll
     for (int p = 0; p < Model::nParameters; p++)
       P[j][p] = ok ? pr[p * a.stride + i] : (RR)0;
-    cf[j] = ok ? a.clamp_fiber[i] : -1;
-    ts[j] = (ok && a.trace_slot) ? a.trace_slot[i] : -1;
+    const int cfj = ok ? a.clamp_fiber[i] : -1;
+    s_cf[q] = cfj;
+    cmask |= (cfj >= 0 ? 1u : 0u) << j;
+    s_ts[q] = (ok && a.trace_slot) ? a.trace_slot[i] : -1;
   }
+  // stimulation bit of node j at substep bit `bit` (junction nodes only read their fiber's bit)
+  auto node_stim = [&](int j, int bit) -> bool {
+    return ((cmask >> j) & 1u) && stim_bit(a.flags, a.words_per_fiber, s_cf[tid * M + j], bit);
+  };
+  // FP32 exact-exponential reaction: nodes (2p, 2p+1) advance together in packed FP32 (heun_step2);
+  // an odd last node runs alone
+  constexpr bool PAIR = std::is_same<RR, float>::value && std::is_same<Math, fdm_math_exact>::value;
+  constexpr int MP = PAIR ? M / 2 : 0;
+  constexpr int NSM = NS > 1 ? NS - 1 : 1;
+  fdm_f2 S2[MP > 0 ? MP : 1][NSM], L2[MP > 0 ? MP : 1][NSM], P2[MP > 0 ? MP : 1][NP];
+  if constexpr (PAIR) {
+#pragma unroll
+    for (int p = 0; p < MP; p++) {
+#pragma unroll
+      for (int s = 0; s < NSM; s++) {
+        S2[p][s] = fdm_f2((float)S[2 * p][s], (float)S[2 * p + 1][s]);
+        L2[p][s] = fdm_f2((float)L[2 * p][s], (float)L[2 * p + 1][s]);
+      }
+#pragma unroll
+      for (int q = 0; q < NP; q++)
+        P2[p][q] = fdm_f2((float)P[2 * p][q], (float)P[2 * p + 1][q]);
+    }
+  }
+  // the scalar state of node j (from the pair arrays where node j is paired)
+  auto unpack = [&](int j, RR* Sj, RR* Lj, RR* Pj) {
+#pragma unroll
+    for (int s = 0; s < NSM; s++) {
+      Sj[s] = S[j][s];
+      Lj[s] = L[j][s];
+    }
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+      Pj[q] = P[j][q];
+    if constexpr (PAIR) {
+      if (j < 2 * MP) {
+#pragma unroll
+        for (int s = 0; s < NSM; s++) {
+          Sj[s] = (RR)((j & 1) ? S2[j >> 1][s].v.y : S2[j >> 1][s].v.x);
+          Lj[s] = (RR)((j & 1) ? L2[j >> 1][s].v.y : L2[j >> 1][s].v.x);
+        }
+#pragma unroll
+        for (int q = 0; q < NP; q++)
+          Pj[q] = (RR)((j & 1) ? P2[j >> 1][q].v.y : P2[j >> 1][q].v.x);
+      }
+    }
+  };
+  auto repack = [&](int j, const RR* Sj, const RR* Lj) {
+#pragma unroll
+    for (int s = 0; s < NSM; s++) {
+      S[j][s] = Sj[s];
+      L[j][s] = Lj[s];
+    }
+    if constexpr (PAIR) {
+      if (j < 2 * MP) {
+#pragma unroll
+        for (int s = 0; s < NSM; s++) {
+          if (j & 1) {
+            S2[j >> 1][s].v.y = (float)Sj[s];
+            L2[j >> 1][s].v.y = (float)Lj[s];
+          } else {
+            S2[j >> 1][s].v.x = (float)Sj[s];
+            L2[j >> 1][s].v.x = (float)Lj[s];
+          }
+        }
+      }
+    }
+  };
+  // one Heun substep of a node that runs alone
+  auto scalar_node = [&](int j, double t, double dt0, int bit) {
+    const bool stim = node_stim(j, bit);
+    if (stim && a.stimulus_mode == 1) {
+      // stimulus current: the junction nodes see the stimulus parameter while stimulated
+      RR Pk[NP];
+#pragma unroll
+      for (int p = 0; p < NP; p++)
+        Pk[p] = p == a.stimulus_parameter ? (RR)a.stimulus_value : P[j][p];
+      heun_step<Model, RR, Math, false>(V[j], S[j], L[j], Pk, t, dt0, false, a.vstim, nullptr);
+    } else {
+      heun_step<Model, RR, Math, false>(V[j], S[j], L[j], P[j], t, dt0, stim, a.vstim, nullptr);
+    }
+  };
   __syncthreads();
 
   for (int step = 0; step < a.n_steps; step++) {
@@ -906,22 +1045,52 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 #pragma unroll 1
       for (int k = 0; k < k_end; k++) {
         const double t = xadd(t0, xmul((double)k, s.dt0));
+        if constexpr (PAIR) {
+          const float dtf = (float)s.dt0;
 #pragma unroll
-        for (int j = 0; j < M; j++) {
-          if (tid * M + j >= nb)
-            continue;
-          const bool stim = cf[j] >= 0 && stim_bit(a.flags, a.words_per_fiber, cf[j], base + k);
-          if (stim && a.stimulus_mode == 1) {
-            // stimulus current: the junction nodes see the stimulus parameter while stimulated
-            RR Pk[NP];
+          for (int p = 0; p < MP; p++) {
+            const int j0 = 2 * p;
+            if (tid * M + j0 >= nb)
+              continue;
+            const bool stim0 = node_stim(j0, base + k);
+            const bool stim1 = node_stim(j0 + 1, base + k);
+            if ((stim0 || stim1) && a.stimulus_mode == 1) {
+              fdm_f2 Pk[NP];
+              const float sv = (float)a.stimulus_value;
 #pragma unroll
-            for (int p = 0; p < NP; p++)
-              Pk[p] = p == a.stimulus_parameter ? (RR)a.stimulus_value : P[j][p];
-            heun_step<Model, RR, Math, false>(V[j], S[j], L[j], Pk, t, s.dt0, false, a.vstim, nullptr);
-          } else {
-            heun_step<Model, RR, Math, false>(V[j], S[j], L[j], P[j], t, s.dt0, stim, a.vstim, nullptr);
+              for (int q = 0; q < NP; q++) {
+                Pk[q] = P2[p][q];
+                if (q == a.stimulus_parameter) {
+                  if (stim0)
+                    Pk[q].v.x = sv;
+                  if (stim1)
+                    Pk[q].v.y = sv;
+                }
+              }
+              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pk, t, dtf, false, false, a.vstim);
+            } else {
+              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], P2[p], t, dtf, stim0, stim1, a.vstim);
+            }
+          }
+          if constexpr (M % 2 == 1) {
+            if (tid * M + M - 1 < nb)
+              scalar_node(M - 1, t, s.dt0, base + k);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < M; j++) {
+            if (tid * M + j >= nb)
+              continue;
+            scalar_node(j, t, s.dt0, base + k);
           }
         }
+      }
+      if constexpr (PAIR) {
+#pragma unroll
+        for (int p = 0; p < MP; p++)
+#pragma unroll
+          for (int q = 0; q < NSM; q++)
+            normalize_pair(S2[p][q], L2[p][q]);
       }
       if (store_here) {
         const int k = s.n0 - 1;
@@ -930,15 +1099,17 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         for (int j = 0; j < M; j++) {
           if (tid * M + j >= nb)
             continue;
-          const bool stim = cf[j] >= 0 && stim_bit(a.flags, a.words_per_fiber, cf[j], base + k);
+          const bool stim = node_stim(j, base + k);
+          RR Sj[NSM], Lj[NSM], Pj[NP];
+          unpack(j, Sj, Lj, Pj);
           RR Pk[NP];
 #pragma unroll
           for (int p = 0; p < NP; p++)
-            Pk[p] = (stim && a.stimulus_mode == 1 && p == a.stimulus_parameter) ? (RR)a.stimulus_value : P[j][p];
+            Pk[p] = (stim && a.stimulus_mode == 1 && p == a.stimulus_parameter) ? (RR)a.stimulus_value : Pj[p];
           RR alg[Model::nAlgebraics];
-          heun_step<Model, RR, Math, true>(V[j], S[j], L[j], Pk, t, s.dt0, stim && a.stimulus_mode == 0, a.vstim,
-                                           alg);
-          store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, gi[j]);
+          heun_step<Model, RR, Math, true>(V[j], Sj, Lj, Pk, t, s.dt0, stim && a.stimulus_mode == 0, a.vstim, alg);
+          repack(j, Sj, Lj);
+          store_algebraics<Model>(alg, a.n_alg_out, a.alg_indices, a.alg_out, a.n_nodes, global_node(tid * M + j));
         }
       }
       if (half == 1)
@@ -956,33 +1127,33 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         const int q = tid * M + j;
         const double um = j > 0 ? V[j - 1] : vprev;
         const double up = j < M - 1 ? V[j + 1] : vnext;
-        d[j] = sc[3 * CAP + q] * um + sc[4 * CAP + q] * V[j] + sc[5 * CAP + q] * up;
+        d[j] = sc[2 * CAP + q] * um + sc[3 * CAP + q] * V[j] + sc[4 * CAP + q] * up;
       }
       Affine acc{1.0, 0.0};
 #pragma unroll
       for (int j = 0; j < M; j++) {
         const int q = tid * M + j;
-        acc = compose(acc, Affine{sc[0 * CAP + q], sc[1 * CAP + q] * d[j]});
+        acc = compose(acc, Affine{sc[0 * CAP + q], d[j]});
       }
       double dp = block_scan_incoming<T, false>(acc, sF, sG);
 #pragma unroll
       for (int j = 0; j < M; j++) {
         const int q = tid * M + j;
-        dp = sc[0 * CAP + q] * dp + sc[1 * CAP + q] * d[j];
+        dp = sc[0 * CAP + q] * dp + d[j];
         d[j] = dp;
       }
       Affine bacc{1.0, 0.0};
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
         const int q = tid * M + j;
-        bacc = compose(bacc, Affine{-sc[2 * CAP + q], d[j]});
+        bacc = compose(bacc, Affine{-sc[1 * CAP + q], d[j]});
       }
       __syncthreads(); // sF/sG reuse
       double x = block_scan_incoming<T, true>(bacc, sF, sG);
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
         const int q = tid * M + j;
-        x = -sc[2 * CAP + q] * x + d[j];
+        x = -sc[1 * CAP + q] * x + d[j];
         V[j] = x;
       }
       __syncthreads(); // vfirst/vlast and sF/sG reuse
@@ -990,16 +1161,28 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     if (a.trace_slot) {
 #pragma unroll
       for (int j = 0; j < M; j++)
-        if (ts[j] >= 0 && s.global_no < a.trace_capacity)
-          a.trace[(int64_t)s.global_no * a.n_trace + ts[j]] = V[j];
+        if (s_ts[tid * M + j] >= 0 && s.global_no < a.trace_capacity)
+          a.trace[(int64_t)s.global_no * a.n_trace + s_ts[tid * M + j]] = V[j];
     }
   }
 
+  if constexpr (PAIR) {
+#pragma unroll
+    for (int j = 0; j < 2 * MP; j++) {
+      RR Sj[NSM], Lj[NSM], Pj[NP];
+      unpack(j, Sj, Lj, Pj);
+#pragma unroll
+      for (int s = 0; s < NSM; s++) {
+        S[j][s] = Sj[s];
+        L[j][s] = Lj[s];
+      }
+    }
+  }
 #pragma unroll
   for (int j = 0; j < M; j++) {
     const int q = tid * M + j;
     if (q < nb) {
-      const int64_t i = gi[j];
+      const int64_t i = global_node(q);
       a.vm[i] = V[j];
 #pragma unroll
       for (int s = 1; s < NS; s++) {
@@ -1014,7 +1197,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 template<int T, int M>
 constexpr size_t fused_smem_bytes()
 {
-  return sizeof(double) * (6 * T * M + 2 * T + 4 * (T / 32));
+  return sizeof(double) * (5 * T * M + 2 * T + 4 * (T / 32)) + sizeof(int) * 2 * T * M;
 }
 
 } // namespace fdm

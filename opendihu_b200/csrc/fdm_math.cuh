@@ -36,6 +36,107 @@ __device__ __forceinline__ float fdm_lg2(float x)
   return r;
 }
 
+// --------------------------------------------------------------------------------------------
+// fdm_f2: two FP32 values (two nodes) evaluated by one packed sm_100 instruction (FADD2 / FMUL2 /
+// FFMA2 through __fadd2_rn / __fmul2_rn / __ffma2_rn).  The generated paired right-hand side
+// (rates_fast2) is the FP32 form written over this type, so one instruction stream advances two
+// nodes.  A product is kept unevaluated (fdm_f2_prod) until it meets an addend, so a*b + c becomes
+// one FFMA2 as a scalar a*b + c becomes one FFMA.  Transcendentals (ex2, rcp, lg2) have no packed
+// form and run per component.
+// --------------------------------------------------------------------------------------------
+struct fdm_f2 {
+  float2 v;
+  __device__ __forceinline__ fdm_f2() {}
+  __device__ __forceinline__ explicit fdm_f2(double c) : v(make_float2((float)c, (float)c)) {}
+  __device__ __forceinline__ explicit fdm_f2(float c) : v(make_float2(c, c)) {}
+  __device__ __forceinline__ fdm_f2(float a, float b) : v(make_float2(a, b)) {}
+  __device__ __forceinline__ fdm_f2(float2 x) : v(x) {}
+};
+struct fdm_f2_prod {
+  float2 a, b;
+  __device__ __forceinline__ operator fdm_f2() const { return fdm_f2(__fmul2_rn(a, b)); }
+};
+struct fdm_b2 {
+  bool x, y;
+};
+
+__device__ __forceinline__ float2 fdm_neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2 a) { return fdm_f2(fdm_neg2(a.v)); }
+__device__ __forceinline__ fdm_f2 operator+(fdm_f2 a) { return a; }
+__device__ __forceinline__ fdm_f2_prod operator-(fdm_f2_prod p) { return fdm_f2_prod{fdm_neg2(p.a), p.b}; }
+__device__ __forceinline__ fdm_f2_prod operator*(fdm_f2 a, fdm_f2 b) { return fdm_f2_prod{a.v, b.v}; }
+__device__ __forceinline__ fdm_f2 operator+(fdm_f2 a, fdm_f2 b) { return fdm_f2(__fadd2_rn(a.v, b.v)); }
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2 a, fdm_f2 b) { return fdm_f2(__fadd2_rn(a.v, fdm_neg2(b.v))); }
+__device__ __forceinline__ fdm_f2 operator+(fdm_f2_prod p, fdm_f2 c) { return fdm_f2(__ffma2_rn(p.a, p.b, c.v)); }
+__device__ __forceinline__ fdm_f2 operator+(fdm_f2 c, fdm_f2_prod p) { return fdm_f2(__ffma2_rn(p.a, p.b, c.v)); }
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2_prod p, fdm_f2 c)
+{
+  return fdm_f2(__ffma2_rn(p.a, p.b, fdm_neg2(c.v)));
+}
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2 c, fdm_f2_prod p)
+{
+  return fdm_f2(__ffma2_rn(fdm_neg2(p.a), p.b, c.v));
+}
+__device__ __forceinline__ fdm_f2 operator+(fdm_f2_prod p, fdm_f2_prod q) { return p + fdm_f2(q); }
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2_prod p, fdm_f2_prod q) { return p - fdm_f2(q); }
+__device__ __forceinline__ fdm_f2& operator+=(fdm_f2& a, fdm_f2 b) { return a = a + b; }
+__device__ __forceinline__ fdm_f2& operator+=(fdm_f2& a, fdm_f2_prod p) { return a = p + a; }
+__device__ __forceinline__ fdm_f2 fdm_ex2(fdm_f2 x) { return fdm_f2(fdm_ex2(x.v.x), fdm_ex2(x.v.y)); }
+__device__ __forceinline__ fdm_f2 fdm_rcp(fdm_f2 x) { return fdm_f2(fdm_rcp(x.v.x), fdm_rcp(x.v.y)); }
+__device__ __forceinline__ fdm_f2 fdm_lg2(fdm_f2 x) { return fdm_f2(fdm_lg2(x.v.x), fdm_lg2(x.v.y)); }
+__device__ __forceinline__ fdm_f2 operator/(fdm_f2 a, fdm_f2 b) { return a * fdm_rcp(b); }
+__device__ __forceinline__ fdm_f2 fabs(fdm_f2 x) { return fdm_f2(fabsf(x.v.x), fabsf(x.v.y)); }
+__device__ __forceinline__ fdm_f2 sqrt(fdm_f2 x) { return fdm_f2(sqrtf(x.v.x), sqrtf(x.v.y)); }
+__device__ __forceinline__ fdm_f2 fdm_powf_pair(fdm_f2 x, fdm_f2 y)
+{
+  return fdm_f2(__powf(x.v.x, y.v.x), __powf(x.v.y, y.v.y));
+}
+#define FDM_F2_CMP(op)                                                                                   \
+  __device__ __forceinline__ fdm_b2 operator op(fdm_f2 a, fdm_f2 b) { return fdm_b2{a.v.x op b.v.x, a.v.y op b.v.y}; }
+FDM_F2_CMP(<)
+FDM_F2_CMP(<=)
+FDM_F2_CMP(>)
+FDM_F2_CMP(>=)
+FDM_F2_CMP(==)
+FDM_F2_CMP(!=)
+#undef FDM_F2_CMP
+__device__ __forceinline__ fdm_b2 operator&&(fdm_b2 a, fdm_b2 b) { return fdm_b2{a.x && b.x, a.y && b.y}; }
+__device__ __forceinline__ fdm_b2 operator||(fdm_b2 a, fdm_b2 b) { return fdm_b2{a.x || b.x, a.y || b.y}; }
+__device__ __forceinline__ fdm_b2 operator!(fdm_b2 a) { return fdm_b2{!a.x, !a.y}; }
+// per-component select (the paired form of c ? a : b; both operands are evaluated)
+__device__ __forceinline__ fdm_f2 fdm_sel(fdm_b2 c, fdm_f2 a, fdm_f2 b)
+{
+  return fdm_f2(c.x ? a.v.x : b.v.x, c.y ? a.v.y : b.v.y);
+}
+
+// --------------------------------------------------------------------------------------------
+// Batched reciprocals (simultaneous inversion): with q = d0 d1 [d2] one SFU reciprocal gives
+// 1/d_k = (1/q) * (product of the other factors), three multiplications per saved reciprocal.
+// Valid while q stays inside the FP32 range: for the Hodgkin-Huxley denominators
+// exp(-(Vm+k)/10) c -/+ 1 that holds for Vm > -340 mV.  Outside it q is inf or 0 and the
+// reciprocals become NaN, which the solver's non-finite check reports (FDM_ERR_NAN); the
+// FP32-reaction mode is specified for physiological potentials.  No range test is made: a
+// branch inside the right-hand side costs more than the reciprocals it saves.
+// --------------------------------------------------------------------------------------------
+template<class R>
+__device__ __forceinline__ void fdm_rcp_batch(R d0, R d1, R& r0, R& r1)
+{
+  const R iv = fdm_rcp(R(d0 * d1));
+  r0 = iv * d1;
+  r1 = iv * d0;
+}
+
+template<class R>
+__device__ __forceinline__ void fdm_rcp_batch(R d0, R d1, R d2, R& r0, R& r1, R& r2)
+{
+  const R q1 = d0 * d1;
+  const R iv = fdm_rcp(R(q1 * d2));
+  r2 = iv * q1;
+  const R t = iv * d2; // 1/(d0 d1)
+  r0 = t * d1;
+  r1 = t * d0;
+}
+
 struct fdm_math_exact {
   // derivatives for the adjoint: d exp(x)/dx = exp(x), d log(x)/dx = 1/x
   template<class R>
