@@ -754,6 +754,11 @@ class _FastEmitter(_Emitter):
         if t == "neg":
             return self.neg_text(e[1])
         if t == "bin" and e[1] == "-":
+            # x - c for a constant c: x + (-c), so that a product x = a b fuses with it
+            c = _affine(e[3], self.consts)
+            if c is not None and not c[0] and not (e[2][0] == "var" or _affine(e[2], self.consts) is not None):
+                return f"({self.expr(e[2])} + (({self.real}){_hexf(-c[1])}))"
+        if t == "bin" and e[1] == "-":
             # a (1 - s) - b s  ->  a - (a + b) s, for variables a, b, s
             l, r = e[2], e[3]
             if l[0] == "bin" and l[1] == "*" and r[0] == "bin" and r[1] == "*":

@@ -32,7 +32,7 @@ cudaError_t launch_fused_hh_f32_approx(int shape, const FusedArgs& a, cudaStream
 template<class Model, class RR, class Math, int T, int M>
 static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s)
 {
-  constexpr size_t smem = fused_smem_bytes<T, M>();
+  constexpr size_t smem = fused_smem_bytes<Model, RR, Math, T, M>();
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(fused_kernel<Model, RR, Math, T, M>,

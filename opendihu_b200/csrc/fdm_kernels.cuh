@@ -881,6 +881,8 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   double* sG = sF + 2 * (T / 32);    // 2 * (T/32)
   int* s_cf = (int*)(sG + 2 * (T / 32)); // CAP: clamp fiber of each node (-1: not a junction node)
   int* s_ts = s_cf + CAP;                // CAP: trace slot of each node (-1: not traced)
+  // paired FP32 path: the parameters of node pair p of thread tid, parameter k, at (p * NP + k) * T + tid
+  fdm_f2* sP2 = (fdm_f2*)(s_ts + CAP);
   __shared__ int64_t fib_global[FUSED_MAX_FIBERS_PER_BIN];
   __shared__ int fib_local[FUSED_MAX_FIBERS_PER_BIN + 1];
 
@@ -959,7 +961,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   constexpr bool PAIR = std::is_same<RR, float>::value && std::is_same<Math, fdm_math_exact>::value;
   constexpr int MP = PAIR ? M / 2 : 0;
   constexpr int NSM = NS > 1 ? NS - 1 : 1;
-  fdm_f2 S2[MP > 0 ? MP : 1][NSM], L2[MP > 0 ? MP : 1][NSM], P2[MP > 0 ? MP : 1][NP];
+  fdm_f2 S2[MP > 0 ? MP : 1][NSM], L2[MP > 0 ? MP : 1][NSM];
   if constexpr (PAIR) {
 #pragma unroll
     for (int p = 0; p < MP; p++) {
@@ -970,7 +972,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       }
 #pragma unroll
       for (int q = 0; q < NP; q++)
-        P2[p][q] = fdm_f2((float)P[2 * p][q], (float)P[2 * p + 1][q]);
+        sP2[(p * NP + q) * T + tid] = fdm_f2((float)P[2 * p][q], (float)P[2 * p + 1][q]);
     }
   }
   // the scalar state of node j (from the pair arrays where node j is paired)
@@ -992,7 +994,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         }
 #pragma unroll
         for (int q = 0; q < NP; q++)
-          Pj[q] = (RR)((j & 1) ? P2[j >> 1][q].v.y : P2[j >> 1][q].v.x);
+          Pj[q] = (RR)((j & 1) ? sP2[((j >> 1) * NP + q) * T + tid].v.y : sP2[((j >> 1) * NP + q) * T + tid].v.x);
       }
     }
   };
@@ -1054,12 +1056,16 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
               continue;
             const bool stim0 = node_stim(j0, base + k);
             const bool stim1 = node_stim(j0 + 1, base + k);
+            fdm_f2 Pp[NP];
+#pragma unroll
+            for (int q = 0; q < NP; q++)
+              Pp[q] = sP2[(p * NP + q) * T + tid];
             if ((stim0 || stim1) && a.stimulus_mode == 1) {
               fdm_f2 Pk[NP];
               const float sv = (float)a.stimulus_value;
 #pragma unroll
               for (int q = 0; q < NP; q++) {
-                Pk[q] = P2[p][q];
+                Pk[q] = Pp[q];
                 if (q == a.stimulus_parameter) {
                   if (stim0)
                     Pk[q].v.x = sv;
@@ -1069,7 +1075,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
               }
               heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pk, t, dtf, false, false, a.vstim);
             } else {
-              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], P2[p], t, dtf, stim0, stim1, a.vstim);
+              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pp, t, dtf, stim0, stim1, a.vstim);
             }
           }
           if constexpr (M % 2 == 1) {
@@ -1194,10 +1200,13 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   }
 }
 
-template<int T, int M>
+template<class Model, class RR, class Math, int T, int M>
 constexpr size_t fused_smem_bytes()
 {
-  return sizeof(double) * (5 * T * M + 2 * T + 4 * (T / 32)) + sizeof(int) * 2 * T * M;
+  constexpr bool PAIR = std::is_same<RR, float>::value && std::is_same<Math, fdm_math_exact>::value;
+  constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
+  return sizeof(double) * (5 * T * M + 2 * T + 4 * (T / 32)) + sizeof(int) * 2 * T * M +
+         (PAIR ? sizeof(fdm_f2) * (M / 2) * NP * T : 0);
 }
 
 } // namespace fdm

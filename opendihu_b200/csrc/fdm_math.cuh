@@ -14,6 +14,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 
 // single SFU instructions for the FP32 form of the right-hand sides (relative error ~2^-22):
 // 2^x, 1/x and log2(x), flushing denormals (the FP32 reaction is compiled with -ftz=true)
@@ -60,23 +61,31 @@ struct fdm_b2 {
   bool x, y;
 };
 
-__device__ __forceinline__ float2 fdm_neg2(float2 a) { return make_float2(-a.x, -a.y); }
+// a - b as one packed subtraction (PTX sub.f32x2; there is no packed-subtract intrinsic)
+__device__ __forceinline__ float2 fdm_sub2(float2 a, float2 b)
+{
+  unsigned long long ra, rb, rd;
+  memcpy(&ra, &a, 8);
+  memcpy(&rb, &b, 8);
+  asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+  float2 d;
+  memcpy(&d, &rd, 8);
+  return d;
+}
+// -a: one packed subtraction from zero (two scalar negations would cost two instructions)
+__device__ __forceinline__ float2 fdm_neg2(float2 a) { return fdm_sub2(make_float2(0.f, 0.f), a); }
 __device__ __forceinline__ fdm_f2 operator-(fdm_f2 a) { return fdm_f2(fdm_neg2(a.v)); }
 __device__ __forceinline__ fdm_f2 operator+(fdm_f2 a) { return a; }
 __device__ __forceinline__ fdm_f2_prod operator-(fdm_f2_prod p) { return fdm_f2_prod{fdm_neg2(p.a), p.b}; }
 __device__ __forceinline__ fdm_f2_prod operator*(fdm_f2 a, fdm_f2 b) { return fdm_f2_prod{a.v, b.v}; }
 __device__ __forceinline__ fdm_f2 operator+(fdm_f2 a, fdm_f2 b) { return fdm_f2(__fadd2_rn(a.v, b.v)); }
-__device__ __forceinline__ fdm_f2 operator-(fdm_f2 a, fdm_f2 b) { return fdm_f2(__fadd2_rn(a.v, fdm_neg2(b.v))); }
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2 a, fdm_f2 b) { return fdm_f2(fdm_sub2(a.v, b.v)); }
 __device__ __forceinline__ fdm_f2 operator+(fdm_f2_prod p, fdm_f2 c) { return fdm_f2(__ffma2_rn(p.a, p.b, c.v)); }
 __device__ __forceinline__ fdm_f2 operator+(fdm_f2 c, fdm_f2_prod p) { return fdm_f2(__ffma2_rn(p.a, p.b, c.v)); }
-__device__ __forceinline__ fdm_f2 operator-(fdm_f2_prod p, fdm_f2 c)
-{
-  return fdm_f2(__ffma2_rn(p.a, p.b, fdm_neg2(c.v)));
-}
-__device__ __forceinline__ fdm_f2 operator-(fdm_f2 c, fdm_f2_prod p)
-{
-  return fdm_f2(__ffma2_rn(fdm_neg2(p.a), p.b, c.v));
-}
+// a b - c and c - a b: a product and a packed subtraction (the negated operand of a fused form would
+// cost a separate instruction as well); the generator writes constant subtrahends as negative addends
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2_prod p, fdm_f2 c) { return fdm_f2(fdm_sub2(__fmul2_rn(p.a, p.b), c.v)); }
+__device__ __forceinline__ fdm_f2 operator-(fdm_f2 c, fdm_f2_prod p) { return fdm_f2(fdm_sub2(c.v, __fmul2_rn(p.a, p.b))); }
 __device__ __forceinline__ fdm_f2 operator+(fdm_f2_prod p, fdm_f2_prod q) { return p + fdm_f2(q); }
 __device__ __forceinline__ fdm_f2 operator-(fdm_f2_prod p, fdm_f2_prod q) { return p - fdm_f2(q); }
 __device__ __forceinline__ fdm_f2& operator+=(fdm_f2& a, fdm_f2 b) { return a = a + b; }
