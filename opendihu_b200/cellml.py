@@ -915,6 +915,8 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     # reverse mode (adjoint)
     out.append("  // vector-Jacobian product: LAM_STATES += J^T LAM_RATES, LAM_PARAMS += (dRATES/dPARAMS)^T LAM_RATES")
     out.extend(emit_cuda_vjp(model, params_alg, params_const))
+    out.append("  // the same in the fast form (exact exponentials): shared exponentials, reciprocals")
+    out.extend(emit_cuda_vjp(model, params_alg, params_const, fast=True))
     out.append("};")
     out.append("")
     return "\n".join(out)
@@ -1114,7 +1116,7 @@ class _VjpBuilder:
     """Straight-line forward code with one temporary per operation, then the adjoint accumulation in
     reverse order (classic reverse-mode differentiation of the expression DAG)."""
 
-    def __init__(self, consts, real="R"):
+    def __init__(self, consts, real="R", repl=None, groups=None):
         self.consts = consts
         self.real = real
         self.fwd: List[str] = []
@@ -1123,6 +1125,13 @@ class _VjpBuilder:
         self.rate_temp: Dict[int, str] = {}
         self.n = 0
         self.plain = _Emitter(real, consts, "cuda")
+        # fast form (exact exponentials only): shared exponentials exp(a.x + b) = exp(a.x) e^b
+        # (repl/groups from _exp_groups), divisions by constants as multiplications, one reciprocal per
+        # division by a variable (its derivative -1/d^2 from the same reciprocal)
+        self.fast = repl is not None
+        self.repl = repl or {}
+        self.groups = groups or []
+        self.group_temp: Dict[int, tuple] = {}
 
     def lit(self, v):
         return ("lit", f"(({self.real}){_hexf(v)})", None)
@@ -1166,6 +1175,15 @@ class _VjpBuilder:
             return self.temp("neg", [a], f"(-{a[1]})")
         if t == "bin":
             op = e[1]
+            if op == "/" and self.fast:
+                a = self.build(e[2])
+                den = _affine(e[3], self.consts)
+                if den is not None and not den[0] and den[1] != 0.0:
+                    c = self.lit(1.0 / den[1])
+                    return self.temp("*", [a, c], f"({a[1]} * {c[1]})")
+                b = self.build(e[3])
+                r = self.temp("rcp", [b], f"((({self.real})1) / {b[1]})")
+                return self.temp("*", [a, r], f"({a[1]} * {r[1]})")
             if op in "+-*/":
                 a = self.build(e[2])
                 b = self.build(e[3])
@@ -1189,6 +1207,18 @@ class _VjpBuilder:
                     return self.temp(("powi", n), [a], f"(({self.real})1.0/FDM_POW{-n}({a[1]}))")
                 b = self.build(e[2][1])
                 return self.temp("pow", [a, b], f"M::pow({a[1]}, {b[1]})")
+            if f == "exp" and repr(e) in self.repl:
+                g, off = self.repl[repr(e)]
+                if g not in self.group_temp:
+                    arg = None
+                    for (kind, idx), coef in self.groups[g]:
+                        term = ("bin", "*", ("num", _hexf(coef), coef), ("var", kind, idx))
+                        arg = term if arg is None else ("bin", "+", arg, term)
+                    x = self.build(arg)
+                    self.group_temp[g] = self.temp("exp", [x], f"M::exp({x[1]})")
+                ge = self.group_temp[g]
+                c = self.lit(math.exp(off))
+                return self.temp("*", [ge, c], f"({ge[1]} * {c[1]})")
             a = self.build(e[2][0])
             if f == "exp":
                 return self.temp("exp", [a], f"M::exp({a[1]})")
@@ -1221,6 +1251,8 @@ class _VjpBuilder:
             elif op == "/":
                 acc(ops[0], f"{a} / {ops[1][1]}")
                 acc(ops[1], f"-{a} * {name} / {ops[1][1]}")
+            elif op == "rcp":
+                acc(ops[0], f"-{a} * {name} * {name}")
             elif op == "neg":
                 acc(ops[0], f"-{a}")
             elif op == "exp":
@@ -1252,12 +1284,19 @@ class _VjpBuilder:
         return out
 
 
-def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> List[str]:
+def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequence[int], fast: bool = False) -> List[str]:
     """Lines of the member function ``rates_vjp<R, M>`` (to be placed inside the model struct):
     given STATES, PARAMS and LAM_RATES it evaluates the right-hand side and adds J^T LAM_RATES to
-    LAM_STATES and (dRATES/dPARAMS)^T LAM_RATES to LAM_PARAMS."""
+    LAM_STATES and (dRATES/dPARAMS)^T LAM_RATES to LAM_PARAMS; ``rates_tape`` / ``rates_vjp_tape``
+    split it in a recording forward and a backward.  ``fast``: the same functions with the suffix
+    ``_fast`` in the fast form of _VjpBuilder (shared exponentials, reciprocals; exact exponentials)."""
     lines = substitute_parameters(model, params_alg, params_const)
-    b = _VjpBuilder(model.constants)
+    sfx = "_fast" if fast else ""
+    if fast:
+        repl, groups = _exp_groups(lines, model.constants)
+        b = _VjpBuilder(model.constants, repl=repl, groups=groups)
+    else:
+        b = _VjpBuilder(model.constants)
     for kind, idx, expr in lines:
         r = b.build(expr)
         if r[0] == "lit" or (r[0] == "ref" and not r[1].startswith("t")):
@@ -1269,7 +1308,7 @@ def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequenc
             b.rate_temp[idx] = r[1]
     out = []
     out.append("  template<class R, class M>")
-    out.append("  __device__ __forceinline__ static void rates_vjp(const R VOI, const R* __restrict__ STATES,"
+    out.append(f"  __device__ __forceinline__ static void rates_vjp{sfx}(const R VOI, const R* __restrict__ STATES,"
                " const R* __restrict__ PARAMS, const R* __restrict__ LAM_RATES, R* __restrict__ LAM_STATES,"
                " R* __restrict__ LAM_PARAMS)")
     out.append("  {")
@@ -1292,9 +1331,9 @@ def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequenc
     # backward that reads the tape, so that a caller who needs the rates anyway evaluates them only once
     n_tape = b.n
     conds = [ln.split("const bool ", 1)[1].split(" =", 1)[0] for ln in b.fwd if "const bool " in ln]
-    out.append(f"  static constexpr int nTape = {n_tape + len(conds)};")
+    out.append(f"  static constexpr int nTape{sfx.title().replace('_', '')} = {n_tape + len(conds)};")
     out.append("  template<class R, class M>")
-    out.append("  __device__ __forceinline__ static void rates_tape(const R VOI, const R* __restrict__ STATES,"
+    out.append(f"  __device__ __forceinline__ static void rates_tape{sfx}(const R VOI, const R* __restrict__ STATES,"
                " const R* __restrict__ PARAMS, R* __restrict__ RATES, R* __restrict__ TAPE)")
     out.append("  {")
     out.append("    (void)VOI; (void)PARAMS;")
@@ -1314,7 +1353,7 @@ def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequenc
         out.append(f"    RATES[{idx}] = {tn};")
     out.append("  }")
     out.append("  template<class R, class M>")
-    out.append("  __device__ __forceinline__ static void rates_vjp_tape(const R VOI, const R* __restrict__ STATES,"
+    out.append(f"  __device__ __forceinline__ static void rates_vjp_tape{sfx}(const R VOI, const R* __restrict__ STATES,"
                " const R* __restrict__ PARAMS, const R* __restrict__ TAPE, const R* __restrict__ LAM_RATES,"
                " R* __restrict__ LAM_STATES, R* __restrict__ LAM_PARAMS)")
     out.append("  {")

@@ -671,18 +671,62 @@ struct AdjointArgs {
   int use_tape;                   // 1: f(y) evaluated once, its temporaries kept for the backward sweep
 };
 
+// The right-hand side forms the adjoint uses: with exact exponentials the generated fast form
+// (shared exponentials, one reciprocal per division; values equal to the plain form's to a few
+// ulps, which moves the linearization point by that much), else the plain form.
+template<class Model, class Math, bool FAST = std::is_same<Math, fdm_math_exact>::value>
+struct AdjointForms {
+  static constexpr int nTape = Model::nTape;
+  __device__ __forceinline__ static void tape(double t, const double* y, const double* P, double* r, double* tp)
+  {
+    Model::template rates_tape<double, Math>(t, y, P, r, tp);
+  }
+  __device__ __forceinline__ static void vjp(double t, const double* y, const double* P, const double* lr, double* ly,
+                                             double* lp)
+  {
+    Model::template rates_vjp<double, Math>(t, y, P, lr, ly, lp);
+  }
+  __device__ __forceinline__ static void vjp_tape(double t, const double* y, const double* P, const double* tp,
+                                                  const double* lr, double* ly, double* lp)
+  {
+    Model::template rates_vjp_tape<double, Math>(t, y, P, tp, lr, ly, lp);
+  }
+};
+template<class Model, class Math>
+struct AdjointForms<Model, Math, true> {
+  static constexpr int nTape = Model::nTapeFast;
+  __device__ __forceinline__ static void tape(double t, const double* y, const double* P, double* r, double* tp)
+  {
+    Model::template rates_tape_fast<double, Math>(t, y, P, r, tp);
+  }
+  __device__ __forceinline__ static void vjp(double t, const double* y, const double* P, const double* lr, double* ly,
+                                             double* lp)
+  {
+    Model::template rates_vjp_fast<double, Math>(t, y, P, lr, ly, lp);
+  }
+  __device__ __forceinline__ static void vjp_tape(double t, const double* y, const double* P, const double* tp,
+                                                  const double* lr, double* ly, double* lp)
+  {
+    Model::template rates_vjp_tape_fast<double, Math>(t, y, P, tp, lr, ly, lp);
+  }
+};
+
 // reverse of one half step (n0 Heun substeps) for one node:
 //   forward  r = f(y); y* = y + dt r [y*_0 := vStim]; y' = y + dt/2 (r + f(y*)) [y'_0 := vStim]
 //   reverse  (clamp: lam'_0 := 0); lam_* = J(y*)^T dt/2 lam' (clamp: lam_*_0 := 0);
 //            lam_y = lam' + lam_* + J(y)^T (dt/2 lam' + dt lam_*)
+// The stored input state of the next substep in reverse order is loaded while the current one is
+// differentiated (models with at most 8 states).
 template<class Model, class Math>
-__global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
+__global__ void __launch_bounds__(128, 4) adjoint_half_kernel(AdjointArgs a)
 {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n_nodes)
     return;
+  using F = AdjointForms<Model, Math>;
   constexpr int NS = Model::nStates;
   constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
+  constexpr bool PREFETCH = NS <= 8;
   const int64_t N = a.n_nodes;
   double lam[NS], P[NP], gP[NP];
 #pragma unroll
@@ -703,6 +747,12 @@ __global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
   const double t0 = a.half ? st.mid : st.t;
   const int base = (a.step_in_window * 2 + a.half) * a.nsub_stride;
   const double dt = st.dt0;
+  double ynext[PREFETCH ? NS : 1];
+  if (PREFETCH && st.n0 > 0) {
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      ynext[s] = a.states[(int64_t)((st.n0 - 1) * NS + s) * N + i];
+  }
   for (int k = st.n0 - 1; k >= 0; k--) {
     const double t = xadd(t0, xmul((double)k, dt));
     const bool stim = cf >= 0 && stim_bit(a.flags, a.words_per_fiber, cf, base + k);
@@ -711,16 +761,29 @@ __global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
 #pragma unroll
     for (int q = 0; q < NP; q++)
       Pk[q] = (stim && a.stimulus_mode == 1 && q == a.stimulus_parameter) ? a.stimulus_value : P[q];
-    double y[NS], r[NS], ys[NS], alg[Model::nAlgebraics];
+    double y[NS], r[NS], ys[NS];
+    if (PREFETCH) {
 #pragma unroll
-    for (int s = 0; s < NS; s++)
-      y[s] = a.states[(int64_t)(k * NS + s) * N + i];
-    constexpr bool TAPE_OK = Model::nTape <= 256;
-    double tape[TAPE_OK ? Model::nTape : 1];
-    if (TAPE_OK && a.use_tape)
-      Model::template rates_tape<double, Math>(t, y, Pk, r, tape);
-    else
+      for (int s = 0; s < NS; s++)
+        y[s] = ynext[s];
+      if (k > 0) {
+#pragma unroll
+        for (int s = 0; s < NS; s++)
+          ynext[s] = a.states[(int64_t)((k - 1) * NS + s) * N + i];
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < NS; s++)
+        y[s] = a.states[(int64_t)(k * NS + s) * N + i];
+    }
+    constexpr bool TAPE_OK = F::nTape <= 256;
+    double tape[TAPE_OK ? F::nTape : 1];
+    if (TAPE_OK && a.use_tape) {
+      F::tape(t, y, Pk, r, tape);
+    } else {
+      double alg[Model::nAlgebraics];
       Model::template rates<double, Math>(t, y, Pk, r, alg);
+    }
 #pragma unroll
     for (int s = 0; s < NS; s++)
       ys[s] = y[s] + dt * r[s];
@@ -737,7 +800,7 @@ __global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
 #pragma unroll
     for (int q = 0; q < NP; q++)
       gPk[q] = 0.0;
-    Model::template rates_vjp<double, Math>(t, ys, Pk, lr2, lys, gPk);
+    F::vjp(t, ys, Pk, lr2, lys, gPk);
     if (clamp)
       lys[0] = 0.0;
 #pragma unroll
@@ -746,9 +809,9 @@ __global__ void __launch_bounds__(128) adjoint_half_kernel(AdjointArgs a)
       lam[s] = lam[s] + lys[s];
     }
     if (TAPE_OK && a.use_tape)
-      Model::template rates_vjp_tape<double, Math>(t, y, Pk, tape, lr, lam, gPk);
+      F::vjp_tape(t, y, Pk, tape, lr, lam, gPk);
     else
-      Model::template rates_vjp<double, Math>(t, y, Pk, lr, lam, gPk);
+      F::vjp(t, y, Pk, lr, lam, gPk);
 #pragma unroll
     for (int q = 0; q < Model::nParameters; q++)
       if (!(stim && a.stimulus_mode == 1 && q == a.stimulus_parameter))
