@@ -167,16 +167,34 @@ struct fdm_solver {
     DevBuf<uint8_t> ck_hbs, fin_hbs;
     Tss fin_strang, fin_heun, fin_diff;
     int64_t fin_split = 0;
-    DevBuf<double> H, U, X, lam, gP, gpf, mu, tgrad;
+    // two buffer sets (stored substep states H, Vm before/after each diffusion solve U/X, stimulation bits)
+    // so that the replay of one segment overlaps the reverse sweep of the next one in reverse order
+    DevBuf<double> H[2], U[2], X[2], lam, gP, gpf, mu, ascratch, tgrad;
+    DevBuf<uint32_t> flags[2];
+    cudaStream_t rstream = nullptr;                 // reverse sweeps
+    cudaEvent_t replayed[2] = {nullptr, nullptr};   // buffer k filled by a replay
+    cudaEvent_t reversed[2] = {nullptr, nullptr};   // buffer k consumed by a reverse sweep
     void release()
     {
-      for (auto* b : {&ck_vm, &ck_states, &ck_last, &ck_jit, &fin_vm, &fin_states, &fin_last, &fin_jit, &H, &U, &X,
-                      &lam, &gP, &gpf, &mu, &tgrad})
+      for (auto* b : {&ck_vm, &ck_states, &ck_last, &ck_jit, &fin_vm, &fin_states, &fin_last, &fin_jit, &H[0], &H[1],
+                      &U[0], &U[1], &X[0], &X[1], &lam, &gP, &gpf, &mu, &ascratch, &tgrad})
         b->release();
+      flags[0].release();
+      flags[1].release();
       ck_jidx.release();
       fin_jidx.release();
       ck_hbs.release();
       fin_hbs.release();
+      for (int k = 0; k < 2; k++) {
+        if (replayed[k])
+          cudaEventDestroy(replayed[k]);
+        if (reversed[k])
+          cudaEventDestroy(reversed[k]);
+        replayed[k] = reversed[k] = nullptr;
+      }
+      if (rstream)
+        cudaStreamDestroy(rstream);
+      rstream = nullptr;
       ready = false;
     }
   } adj;
@@ -1128,7 +1146,8 @@ static int ensure_step_capacity(fdm_solver* s, int n)
 }
 
 // uploads a window of split steps (through a pinned slot) and runs the stimulation schedule for it
-static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, WindowInfo* wi)
+static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, WindowInfo* wi,
+                          uint32_t* flags_buf = nullptr)
 {
   int rc = ensure_step_capacity(s, n_steps);
   if (rc)
@@ -1143,7 +1162,8 @@ static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_step
     nsub = std::max(nsub, hs[j].n0);
   const int bits = n_steps * 2 * nsub;
   const int words = (bits + 31) / 32;
-  FDM_CUDA(s->flags.alloc((size_t)words * std::max(s->n_fibers, 1)));
+  if (!flags_buf)
+    FDM_CUDA(s->flags.alloc((size_t)words * std::max(s->n_fibers, 1)));
   FDM_CUDA(cudaMemcpyAsync(s->steps_d.p, hs, sizeof(SplitStep) * n_steps, cudaMemcpyHostToDevice, s->stream));
   FDM_CUDA(cudaEventRecord(s->slot_ev[slot], s->stream));
   wi->words = words;
@@ -1163,7 +1183,7 @@ static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_step
   sa.current_jitter = s->cur_jitter.p;
   sa.jitter_index = s->jitter_idx.p;
   sa.has_been_stimulated = s->hbs.p;
-  sa.flags = s->flags.p;
+  sa.flags = flags_buf ? flags_buf : s->flags.p;
   sa.words_per_fiber = words;
   sa.nsub_stride = nsub;
   sa.n_fibers = s->n_fibers;
@@ -1890,13 +1910,31 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
   const int nf = s->n_fibers;
   const int64_t NT = (int64_t)A.steps.size();
   const size_t hstride = (size_t)A.n0max * NS * N; // one half step of stored substep states
-  FDM_CUDA(A.H.alloc((size_t)A.kc * 2 * hstride));
-  FDM_CUDA(A.U.alloc((size_t)A.kc * N));
-  FDM_CUDA(A.X.alloc((size_t)A.kc * N));
+  int max_words = 1;
+  for (int c = 0; c < A.n_seg; c++) {
+    const size_t b = (size_t)c * A.kc, e = std::min<size_t>(b + A.kc, NT);
+    int nsub = 1;
+    for (size_t j = b; j < e; j++)
+      nsub = std::max(nsub, A.steps[j].n0);
+    max_words = std::max(max_words, (int)(((e - b) * 2 * nsub + 31) / 32));
+  }
+  for (int k = 0; k < 2; k++) {
+    FDM_CUDA(A.H[k].alloc((size_t)A.kc * 2 * hstride));
+    FDM_CUDA(A.U[k].alloc((size_t)A.kc * N));
+    FDM_CUDA(A.X[k].alloc((size_t)A.kc * N));
+    FDM_CUDA(A.flags[k].alloc((size_t)max_words * std::max(nf, 1)));
+    if (!A.replayed[k])
+      FDM_CUDA(cudaEventCreateWithFlags(&A.replayed[k], cudaEventDisableTiming));
+    if (!A.reversed[k])
+      FDM_CUDA(cudaEventCreateWithFlags(&A.reversed[k], cudaEventDisableTiming));
+  }
+  if (!A.rstream)
+    FDM_CUDA(cudaStreamCreateWithFlags(&A.rstream, cudaStreamNonBlocking));
   FDM_CUDA(A.lam.alloc((size_t)NS * N));
   FDM_CUDA(A.gP.alloc((size_t)std::max(NP, 1) * N));
   FDM_CUDA(A.gpf.alloc(nf));
   FDM_CUDA(A.mu.alloc(N));
+  FDM_CUDA(A.ascratch.alloc(N));
   FDM_CUDA(A.tgrad.alloc(std::max<size_t>((size_t)NT * A.n_sensors, 1)));
   FDM_CUDA(cudaMemsetAsync(A.lam.p, 0, sizeof(double) * NS * N, s->stream));
   FDM_CUDA(cudaMemsetAsync(A.gP.p, 0, sizeof(double) * std::max(NP, 1) * N, s->stream));
@@ -1906,9 +1944,27 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
                              s->stream));
   const MathKind mk = s->cfg.approximate_exponential_function ? MATH_APPROX : MATH_EXACT;
   const int ie = s->cfg.diffusion_scheme == FDM_IMPLICIT_EULER;
+  // Replay and reverse sweeps run on two streams when the diffusion step width (and so the factorized
+  // coefficients both read) is the same for every split step; otherwise everything runs in order on one
+  // stream and the coefficients are refactorized where the step width changes.
+  bool uniform_dt1 = true;
+  for (int64_t j = 0; j < NT; j++)
+    if (std::fabs(A.dt1s[j] - A.dt1s[0]) > 1e-12 * std::fabs(A.dt1s[0]))
+      uniform_dt1 = false;
+  cudaStream_t rs = uniform_dt1 ? A.rstream : s->stream;
+  if (uniform_dt1 && NT > 0) {
+    int rc = ensure_coefficients(s, A.dt1s[0]);
+    if (rc)
+      return rc;
+  }
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
-  for (int c = A.n_seg - 1; c >= 0; c--) {
+  std::vector<WindowInfo> win(A.n_seg);
+
+  // replay of segment c into buffer k (stream s->stream): every substep's input state and Vm before/after
+  // each diffusion solve
+  auto replay = [&](int c, int k) -> int {
+    FDM_CUDA(cudaStreamWaitEvent(s->stream, A.reversed[k], 0));
     int rc = copy_state(s, A.ck_vm.p + (size_t)c * N, A.ck_states.p + (size_t)c * N * (NS - 1),
                         A.ck_last.p + (size_t)c * nf, A.ck_jit.p + (size_t)c * nf, A.ck_jidx.p + (size_t)c * nf,
                         A.ck_hbs.p + (size_t)c * nf, false);
@@ -1919,11 +1975,9 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
     rc = ensure_coefficients(s, A.dt1s[b]);
     if (rc)
       return rc;
-    WindowInfo wi;
-    rc = prepare_window(s, A.steps.data() + b, len, &wi);
+    rc = prepare_window(s, A.steps.data() + b, len, &win[c], A.flags[k].p);
     if (rc)
       return rc;
-    // replay the segment, storing every substep's input state and Vm before/after each diffusion solve
     ReactionArgs ra{};
     ra.n_nodes = N;
     ra.stride = N;
@@ -1931,9 +1985,9 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
     ra.states = s->states.p;
     ra.params = s->params.p;
     ra.clamp_fiber = s->clamp_fiber.p;
-    ra.flags = s->flags.p;
-    ra.words_per_fiber = wi.words;
-    ra.nsub_stride = wi.nsub;
+    ra.flags = A.flags[k].p;
+    ra.words_per_fiber = win[c].words;
+    ra.nsub_stride = win[c].nsub;
     ra.vstim = s->cfg.value_for_stimulated_point;
     ra.stimulus_mode = s->cfg.stimulus_mode;
     ra.stimulus_parameter = s->cfg.stimulus_parameter;
@@ -1946,29 +2000,37 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       ra.step = jj;
       for (int half = 0; half < 2; half++) {
         ra.half = half;
-        ra.store_states = A.H.p + ((size_t)jj * 2 + half) * hstride;
+        ra.store_states = A.H[k].p + ((size_t)jj * 2 + half) * hstride;
         FDM_CUDA(launch_reaction(s->cfg.model, REAL_F64, mk, ra, s->stream));
         s->launches++;
         if (half == 0) {
-          FDM_CUDA(cudaMemcpyAsync(A.U.p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+          FDM_CUDA(cudaMemcpyAsync(A.U[k].p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
                                    s->stream));
           FDM_CUDA(launch_diffusion_warp(nf, s->off_d.p, s->coef.p, N, s->vm.p, s->scratch.p, s->stream));
           s->launches++;
-          FDM_CUDA(cudaMemcpyAsync(A.X.p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+          FDM_CUDA(cudaMemcpyAsync(A.X[k].p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
                                    s->stream));
         }
       }
     }
-    // reverse the segment
+    FDM_CUDA(cudaEventRecord(A.replayed[k], s->stream));
+    return FDM_OK;
+  };
+
+  // reverse sweep of segment c from buffer k (stream A.rstream)
+  auto reverse = [&](int c, int k) -> int {
+    FDM_CUDA(cudaStreamWaitEvent(rs, A.replayed[k], 0));
+    const size_t b = (size_t)c * A.kc, e = std::min<size_t>(b + A.kc, NT);
+    const int len = (int)(e - b);
     AdjointArgs aa{};
     aa.n_nodes = N;
     aa.params = (const double*)s->params.p;
     aa.lam = A.lam.p;
     aa.grad_params = A.gP.p;
     aa.clamp_fiber = s->clamp_fiber.p;
-    aa.flags = s->flags.p;
-    aa.words_per_fiber = wi.words;
-    aa.nsub_stride = wi.nsub;
+    aa.flags = A.flags[k].p;
+    aa.words_per_fiber = win[c].words;
+    aa.nsub_stride = win[c].nsub;
     aa.vstim = s->cfg.value_for_stimulated_point;
     aa.stimulus_mode = s->cfg.stimulus_mode;
     aa.stimulus_parameter = s->cfg.stimulus_parameter;
@@ -1983,20 +2045,48 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       aa.step_in_window = jj;
       aa.half = 1;
       aa.trace_row = (int64_t)j;
-      aa.states = A.H.p + ((size_t)jj * 2 + 1) * hstride;
-      FDM_CUDA(launch_adjoint_half(s->cfg.model, mk, aa, s->stream));
-      rc = ensure_coefficients(s, A.dt1s[j]);
-      if (rc)
-        return rc;
-      FDM_CUDA(launch_adjoint_diffusion(nf, s->off_d.p, s->elem_d.p, s->coef.p, N, A.lam.p, A.U.p + (size_t)jj * N,
-                                        A.X.p + (size_t)jj * N, ie, A.gpf.p, s->scratch.p, A.mu.p, s->stream));
+      aa.states = A.H[k].p + ((size_t)jj * 2 + 1) * hstride;
+      FDM_CUDA(launch_adjoint_half(s->cfg.model, mk, aa, rs));
+      if (!uniform_dt1) {
+        int rc = ensure_coefficients(s, A.dt1s[j]);
+        if (rc)
+          return rc;
+      }
+      FDM_CUDA(launch_adjoint_diffusion(nf, s->off_d.p, s->elem_d.p, s->coef.p, N, A.lam.p, A.U[k].p + (size_t)jj * N,
+                                        A.X[k].p + (size_t)jj * N, ie, A.gpf.p, A.ascratch.p, A.mu.p,
+                                        s->max_fiber_len, rs));
       aa.half = 0;
       aa.trace_row = -1;
-      aa.states = A.H.p + ((size_t)jj * 2 + 0) * hstride;
-      FDM_CUDA(launch_adjoint_half(s->cfg.model, mk, aa, s->stream));
+      aa.states = A.H[k].p + ((size_t)jj * 2 + 0) * hstride;
+      FDM_CUDA(launch_adjoint_half(s->cfg.model, mk, aa, rs));
       s->launches += 3;
     }
+    FDM_CUDA(cudaEventRecord(A.reversed[k], rs));
+    return FDM_OK;
+  };
+
+  // the reverse stream starts after the gradient buffers are cleared; buffers start free
+  FDM_CUDA(cudaEventRecord(A.reversed[0], s->stream));
+  FDM_CUDA(cudaEventRecord(A.reversed[1], s->stream));
+  FDM_CUDA(cudaStreamWaitEvent(rs, A.reversed[0], 0));
+  if (A.n_seg > 0) {
+    int rc = replay(A.n_seg - 1, (A.n_seg - 1) & 1);
+    if (rc)
+      return rc;
   }
+  for (int c = A.n_seg - 1; c >= 0; c--) {
+    if (c > 0) {
+      int rc = replay(c - 1, (c - 1) & 1);
+      if (rc)
+        return rc;
+    }
+    int rc = reverse(c, c & 1);
+    if (rc)
+      return rc;
+  }
+  // join: the gradients are complete when the last reverse sweep is
+  FDM_CUDA(cudaEventRecord(A.reversed[0], rs));
+  FDM_CUDA(cudaStreamWaitEvent(s->stream, A.reversed[0], 0));
   FDM_CUDA(cudaEventRecord(s->adv_stop, s->stream));
   if (grad_parameters && NP > 0)
     FDM_CUDA(cudaMemcpyAsync(grad_parameters, A.gP.p, sizeof(double) * NP * N, cudaMemcpyDeviceToHost, s->stream));

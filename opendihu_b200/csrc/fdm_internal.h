@@ -40,7 +40,7 @@ cudaError_t launch_adjoint_half(int model, MathKind mk, const AdjointArgs& a, cu
 cudaError_t launch_adjoint_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths,
                                      const double* coef, int64_t stride, double* lam, const double* u, const double* x,
                                      int implicit_euler, double* grad_prefactor, double* scratch, double* mu,
-                                     cudaStream_t s);
+                                     int64_t max_fiber_len, cudaStream_t s);
 // counts non-finite entries of x[0..n) into *count (device int, must be zeroed by the caller)
 cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t s);
 

@@ -929,6 +929,111 @@ __device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, do
   return ex.G; // applied to the zero entering the first node of the bin
 }
 
+// Adjoint of one diffusion solve (see adjoint_diffusion_warp_kernel for the algebra) with one CTA per
+// fiber of at most T*M nodes: thread tid owns nodes tid*M .. tid*M+M-1 in registers, the two sweeps of the
+// LU solve are block-wide scans of affine maps (as in the fused kernel), neighbours across threads go
+// through shared memory, and the prefactor gradient is a block reduction.  Used when the fibers are few
+// (a warp per fiber would leave most of the GPU idle).
+template<int T, int M>
+__global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
+    const int64_t* __restrict__ fiber_offsets, const double* __restrict__ element_lengths,
+    const double* __restrict__ coef, int64_t stride, double* __restrict__ lam, const double* __restrict__ u,
+    const double* __restrict__ x, int implicit_euler, double* __restrict__ grad_prefactor)
+{
+  __shared__ double sF[2 * (T / 32)], sG[2 * (T / 32)];
+  __shared__ double sfirst[T], slast[T], sred[T / 32];
+  const int f = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int64_t o = fiber_offsets[f];
+  const int n = (int)(fiber_offsets[f + 1] - o);
+  const double* h = element_lengths + (o - f);
+  const double* mulF = coef;
+  const double* inv = coef + stride;
+  const double* cp = coef + 2 * stride;
+  const double* cl = coef + 3 * stride;
+  const double* cm = coef + 4 * stride;
+  const double* cr = coef + 5 * stride;
+  double d[M], mu[M], w[M];
+  // forward sweep of A^{-1} lam
+  Affine acc{1.0, 0.0};
+#pragma unroll
+  for (int j = 0; j < M; j++) {
+    const int q = tid * M + j;
+    if (q < n) {
+      d[j] = inv[o + q] * lam[o + q];
+      acc = compose(acc, Affine{mulF[o + q], d[j]});
+    } else {
+      d[j] = 0.0;
+    }
+  }
+  double dp = block_scan_incoming<T, false>(acc, sF, sG);
+#pragma unroll
+  for (int j = 0; j < M; j++) {
+    const int q = tid * M + j;
+    if (q < n) {
+      dp = mulF[o + q] * dp + d[j];
+      d[j] = dp;
+    }
+  }
+  // backward sweep (nodes beyond the fiber carry x = 0 into its last node)
+  Affine bacc{1.0, 0.0};
+#pragma unroll
+  for (int j = M - 1; j >= 0; j--) {
+    const int q = tid * M + j;
+    bacc = compose(bacc, q < n ? Affine{-cp[o + q], d[j]} : Affine{0.0, 0.0});
+  }
+  __syncthreads(); // sF/sG reuse
+  double xx = block_scan_incoming<T, true>(bacc, sF, sG);
+#pragma unroll
+  for (int j = M - 1; j >= 0; j--) {
+    const int q = tid * M + j;
+    xx = q < n ? -cp[o + q] * xx + d[j] : 0.0;
+    mu[j] = xx;
+    w[j] = q < n ? (implicit_euler ? x[o + q] : 0.5 * (x[o + q] + u[o + q])) : 0.0;
+  }
+  // neighbours of the thread's first and last node: mu and w
+  sfirst[tid] = mu[0];
+  slast[tid] = mu[M - 1];
+  __syncthreads();
+  const double mu_prev = tid > 0 ? slast[tid - 1] : 0.0;
+  const double mu_next = tid < T - 1 ? sfirst[tid + 1] : 0.0;
+  __syncthreads();
+  sfirst[tid] = w[0];
+  slast[tid] = w[M - 1];
+  __syncthreads();
+  const double w_prev = tid > 0 ? slast[tid - 1] : 0.0;
+  const double w_next = tid < T - 1 ? sfirst[tid + 1] : 0.0;
+  // lam_u = B mu and the prefactor gradient -mu^T K1 w
+  double g = 0.0;
+#pragma unroll
+  for (int j = 0; j < M; j++) {
+    const int q = tid * M + j;
+    if (q >= n)
+      continue;
+    const double mp = q > 0 ? (j > 0 ? mu[j - 1] : mu_prev) : 0.0;
+    const double mn = q < n - 1 ? (j < M - 1 ? mu[j + 1] : mu_next) : 0.0;
+    lam[o + q] = cl[o + q] * mp + cm[o + q] * mu[j] + cr[o + q] * mn;
+    double k1 = 0.0;
+    if (q > 0)
+      k1 += ((j > 0 ? w[j - 1] : w_prev) - w[j]) / h[q - 1];
+    if (q < n - 1)
+      k1 += ((j < M - 1 ? w[j + 1] : w_next) - w[j]) / h[q];
+    g -= mu[j] * k1;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+    g += __shfl_down_sync(0xffffffffu, g, off);
+  if ((tid & 31) == 0)
+    sred[tid >> 5] = g;
+  __syncthreads();
+  if (tid == 0) {
+    double sum = 0.0;
+    for (int k = 0; k < T / 32; k++)
+      sum += sred[k];
+    grad_prefactor[f] += sum;
+  }
+}
+
 template<class Model, class RR, class Math, int T, int M>
 __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 {

@@ -110,13 +110,39 @@ cudaError_t launch_adjoint_half(int model, MathKind mk, const AdjointArgs& a, cu
   }
 }
 
+template<int T, int M>
+static cudaError_t adjoint_diffusion_block(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths,
+                                           const double* coef, int64_t stride, double* lam, const double* u,
+                                           const double* x, int implicit_euler, double* grad_prefactor,
+                                           cudaStream_t s)
+{
+  adjoint_diffusion_block_kernel<T, M><<<(unsigned)n_fibers, T, 0, s>>>(fiber_offsets, element_lengths, coef, stride,
+                                                                       lam, u, x, implicit_euler, grad_prefactor);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_adjoint_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths,
                                      const double* coef, int64_t stride, double* lam, const double* u, const double* x,
                                      int implicit_euler, double* grad_prefactor, double* scratch, double* mu,
-                                     cudaStream_t s)
+                                     int64_t max_fiber_len, cudaStream_t s)
 {
   if (n_fibers == 0)
     return cudaSuccess;
+  // few fibers: one CTA per fiber (block-wide scans); many fibers: one warp per fiber fills the GPU
+  if (n_fibers < 4 * 148) {
+    if (max_fiber_len <= 512)
+      return adjoint_diffusion_block<128, 4>(n_fibers, fiber_offsets, element_lengths, coef, stride, lam, u, x,
+                                             implicit_euler, grad_prefactor, s);
+    if (max_fiber_len <= 1024)
+      return adjoint_diffusion_block<256, 4>(n_fibers, fiber_offsets, element_lengths, coef, stride, lam, u, x,
+                                             implicit_euler, grad_prefactor, s);
+    if (max_fiber_len <= 2048)
+      return adjoint_diffusion_block<256, 8>(n_fibers, fiber_offsets, element_lengths, coef, stride, lam, u, x,
+                                             implicit_euler, grad_prefactor, s);
+    if (max_fiber_len <= 4096)
+      return adjoint_diffusion_block<512, 8>(n_fibers, fiber_offsets, element_lengths, coef, stride, lam, u, x,
+                                             implicit_euler, grad_prefactor, s);
+  }
   const int T = 128;
   const int64_t threads = (int64_t)n_fibers * 32;
   adjoint_diffusion_warp_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, s>>>(
