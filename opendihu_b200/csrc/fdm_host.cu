@@ -170,6 +170,7 @@ struct fdm_solver {
     // two buffer sets (stored substep states H, Vm before/after each diffusion solve U/X, stimulation bits)
     // so that the replay of one segment overlaps the reverse sweep of the next one in reverse order
     DevBuf<double> H[2], U[2], X[2], lam, gP, gpf, mu, ascratch, tgrad;
+    DevBuf<double> coefs;                           // one factorization per distinct diffusion step width
     DevBuf<uint32_t> flags[2];
     cudaStream_t rstream = nullptr;                 // reverse sweeps
     cudaEvent_t replayed[2] = {nullptr, nullptr};   // buffer k filled by a replay
@@ -177,7 +178,7 @@ struct fdm_solver {
     void release()
     {
       for (auto* b : {&ck_vm, &ck_states, &ck_last, &ck_jit, &fin_vm, &fin_states, &fin_last, &fin_jit, &H[0], &H[1],
-                      &U[0], &U[1], &X[0], &X[1], &lam, &gP, &gpf, &mu, &ascratch, &tgrad})
+                      &U[0], &U[1], &X[0], &X[1], &lam, &gP, &gpf, &mu, &ascratch, &tgrad, &coefs})
         b->release();
       flags[0].release();
       flags[1].release();
@@ -1944,19 +1945,30 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
                              s->stream));
   const MathKind mk = s->cfg.approximate_exponential_function ? MATH_APPROX : MATH_EXACT;
   const int ie = s->cfg.diffusion_scheme == FDM_IMPLICIT_EULER;
-  // Replay and reverse sweeps run on two streams when the diffusion step width (and so the factorized
-  // coefficients both read) is the same for every split step; otherwise everything runs in order on one
-  // stream and the coefficients are refactorized where the step width changes.
-  bool uniform_dt1 = true;
-  for (int64_t j = 0; j < NT; j++)
-    if (std::fabs(A.dt1s[j] - A.dt1s[0]) > 1e-12 * std::fabs(A.dt1s[0]))
-      uniform_dt1 = false;
-  cudaStream_t rs = uniform_dt1 ? A.rstream : s->stream;
-  if (uniform_dt1 && NT > 0) {
-    int rc = ensure_coefficients(s, A.dt1s[0]);
-    if (rc)
-      return rc;
+  // The diffusion step width dt1D = ((t + dtSplit) - t)/n1D drifts in its last bits as t grows; the
+  // factorization in use is replaced when dt1D leaves a relative 1e-12 of it (ensure_coefficients).  The
+  // same rule applied to the run's step widths gives the factorizations ("epochs") of every split step;
+  // each is computed once into its own buffer, so that replay and reverse sweeps, which both read them,
+  // can run on two streams.  With many epochs (a step width changing at every step) everything runs in
+  // order on one stream and the coefficients are refactorized where the width changes.
+  std::vector<int> epoch(NT, 0);
+  std::vector<double> edt;
+  for (int64_t j = 0; j < NT; j++) {
+    if (edt.empty() || std::fabs(A.dt1s[j] - edt.back()) > 1e-12 * std::fabs(edt.back()))
+      edt.push_back(A.dt1s[j]);
+    epoch[j] = (int)edt.size() - 1;
   }
+  const bool pipelined = !edt.empty() && edt.size() <= 16;
+  cudaStream_t rs = pipelined ? A.rstream : s->stream;
+  if (pipelined) {
+    FDM_CUDA(A.coefs.alloc(edt.size() * 6 * (size_t)N));
+    for (size_t e = 0; e < edt.size(); e++) {
+      FDM_CUDA(launch_coefficients(nf, s->off_d.p, s->elem_d.p, s->prefactor_d.p, edt[e], ie, A.coefs.p + e * 6 * N, N,
+                                   s->stream));
+      s->launches++;
+    }
+  }
+  auto coef_of = [&](size_t j) -> const double* { return pipelined ? A.coefs.p + (size_t)epoch[j] * 6 * N : s->coef.p; };
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
   std::vector<WindowInfo> win(A.n_seg);
@@ -1972,9 +1984,6 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       return rc;
     const size_t b = (size_t)c * A.kc, e = std::min<size_t>(b + A.kc, NT);
     const int len = (int)(e - b);
-    rc = ensure_coefficients(s, A.dt1s[b]);
-    if (rc)
-      return rc;
     rc = prepare_window(s, A.steps.data() + b, len, &win[c], A.flags[k].p);
     if (rc)
       return rc;
@@ -1994,9 +2003,11 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
     ra.stimulus_value = s->cfg.stimulus_value;
     ra.steps = s->steps_d.p;
     for (int jj = 0; jj < len; jj++) {
-      rc = ensure_coefficients(s, A.dt1s[b + jj]);
-      if (rc)
-        return rc;
+      if (!pipelined) {
+        rc = ensure_coefficients(s, A.dt1s[b + jj]);
+        if (rc)
+          return rc;
+      }
       ra.step = jj;
       for (int half = 0; half < 2; half++) {
         ra.half = half;
@@ -2006,7 +2017,7 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
         if (half == 0) {
           FDM_CUDA(cudaMemcpyAsync(A.U[k].p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
                                    s->stream));
-          FDM_CUDA(launch_diffusion_warp(nf, s->off_d.p, s->coef.p, N, s->vm.p, s->scratch.p, s->stream));
+          FDM_CUDA(launch_diffusion_warp(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream));
           s->launches++;
           FDM_CUDA(cudaMemcpyAsync(A.X[k].p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
                                    s->stream));
@@ -2047,12 +2058,12 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       aa.trace_row = (int64_t)j;
       aa.states = A.H[k].p + ((size_t)jj * 2 + 1) * hstride;
       FDM_CUDA(launch_adjoint_half(s->cfg.model, mk, aa, rs));
-      if (!uniform_dt1) {
+      if (!pipelined) {
         int rc = ensure_coefficients(s, A.dt1s[j]);
         if (rc)
           return rc;
       }
-      FDM_CUDA(launch_adjoint_diffusion(nf, s->off_d.p, s->elem_d.p, s->coef.p, N, A.lam.p, A.U[k].p + (size_t)jj * N,
+      FDM_CUDA(launch_adjoint_diffusion(nf, s->off_d.p, s->elem_d.p, coef_of(j), N, A.lam.p, A.U[k].p + (size_t)jj * N,
                                         A.X[k].p + (size_t)jj * N, ie, A.gpf.p, A.ascratch.p, A.mu.p,
                                         s->max_fiber_len, rs));
       aa.half = 0;
