@@ -83,6 +83,9 @@ typedef struct fdm_config {
   int profile;                   /* 1: time the main kernel launches with CUDA events */
   int device;                    /* CUDA device ordinal the solver lives on */
   int use_graph;                 /* 1: the split path replays each window's launch sequence as a CUDA graph */
+  int only_compute_if_stimulated; /* "onlyComputeIfHasBeenStimulated" (compute.tpp:201-205): a node's Heun
+                                     substeps are skipped while the fiber its point buffer is attributed to
+                                     has not been stimulated (0: every node computed, the parity setting) */
 } fdm_config;
 
 /* fills *cfg with the reference's defaults (HH, implicit Euler, FP64 split, vc rule W=4, 20 mV clamp) */
@@ -128,6 +131,13 @@ int fdm_set_stimulation(fdm_solver *s, const uint8_t *firing_events, int rows, i
 int fdm_get_clamp_nodes(fdm_solver *s, int64_t *first_node, int *count, uint8_t *evaluated);
 /* replaces the clamp nodes fdm_set_stimulation chose (e.g. with a selection made for a larger layout) */
 int fdm_set_clamp_nodes(fdm_solver *s, const int64_t *first_node, const int *count, const uint8_t *evaluated);
+/* host-only: per node, the code (attributed fiber) * 4 + class that onlyComputeIfHasBeenStimulated uses:
+ * class 0/1/2 = the node's point buffer lies before / is / lies after the junction buffer of the fiber it
+ * is attributed to (compute.tpp:158-205 processes buffers in order and the junction buffer sets the flag) */
+int fdm_select_gate_codes(int clamp_rule, int vc_width, int n_ranks, int n_fibers, const int64_t *fiber_offsets,
+                          const int *stimulation_point_index, int *codes);
+/* replaces the codes fdm_set_stimulation chose (a selection made for a larger layout) */
+int fdm_set_gate_codes(fdm_solver *s, const int *codes);
 /* host-only: the clamp nodes of a fiber layout under a rule (the selection fdm_set_stimulation makes) */
 int fdm_select_clamp_nodes(int clamp_rule, int vc_width, int n_ranks, int n_fibers, const int64_t *fiber_offsets,
                            const int *stimulation_point_index, int64_t *first_node, int *count, uint8_t *evaluated);

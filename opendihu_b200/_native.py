@@ -31,7 +31,7 @@ EXPORTED = [
     "fdm_checkpoint_save", "fdm_checkpoint_restore", "fdm_fused_shapes", "fdm_diffusion_solve",
     "fdm_diffusion_solve_noalloc", "fdm_compat_configure", "fdm_compat_release", "fdm_adjoint_forward",
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
-    "fdm_select_clamp_nodes",
+    "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes",
 ]
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
@@ -54,6 +54,7 @@ class Config(C.Structure):
         ("dt_splitting", C.c_double), ("dt_0d", C.c_double), ("dt_1d", C.c_double),
         ("steps_per_launch", C.c_int), ("threads_per_block", C.c_int), ("nodes_per_thread", C.c_int),
         ("check_nan", C.c_int), ("profile", C.c_int), ("device", C.c_int), ("use_graph", C.c_int),
+        ("only_compute_if_stimulated", C.c_int),
     ]
 
 
@@ -110,6 +111,8 @@ def lib() -> C.CDLL:
         "fdm_rewind": (C.c_int, [P]),
         "fdm_set_clamp_nodes": (C.c_int, [P, i64, i32, u8]),
         "fdm_select_clamp_nodes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, i64, i32, i64, i32, u8]),
+        "fdm_select_gate_codes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, i64, i32, i32]),
+        "fdm_set_gate_codes": (C.c_int, [P, i32]),
         "fdm_compat_release": (C.c_int, []),
         "initializeArrays": (None, [d, i32, i32, C.c_char_p, d, i32, i32, d, d, d, d]),
         "computeMonodomain": (None, [C.POINTER(C.c_float), d, d, C.POINTER(C.c_float), C.c_double, C.c_double,
@@ -166,3 +169,14 @@ def select_clamp_nodes(rule: int, vc_width: int, n_ranks: int, fiber_offsets, st
     check(lib().fdm_select_clamp_nodes(rule, vc_width, n_ranks, nf, ptr(off, C.c_int64), ptr(c, C.c_int),
                                        ptr(first, C.c_int64), ptr(cnt, C.c_int), ptr(ev, C.c_uint8)))
     return first[:nf], cnt[:nf], ev[:nf]
+
+
+def select_gate_codes(rule: int, vc_width: int, n_ranks: int, fiber_offsets, stimulation_point_index):
+    """Host-only per-node codes (attributed fiber * 4 + class) of onlyComputeIfHasBeenStimulated."""
+    off = np.ascontiguousarray(fiber_offsets, np.int64)
+    c = np.ascontiguousarray(stimulation_point_index, np.int32)
+    n = int(off[-1]) if len(off) else 0
+    codes = np.zeros(max(n, 1), np.int32)
+    check(lib().fdm_select_gate_codes(rule, vc_width, n_ranks, len(off) - 1, ptr(off, C.c_int64), ptr(c, C.c_int),
+                                      ptr(codes, C.c_int)))
+    return codes[:n]

@@ -4,6 +4,8 @@
 namespace fdm {
 cudaError_t launch_fused_hh_f32_approx(int shape, const FusedArgs& a, cudaStream_t s)
 {
-  return fused_shape<FusedHH, float, fdm_math_approx>(shape, a, s);
+  if (a.gate)
+    return launch_fused_hh_f32_approx_gate(shape, a, s);
+  return fused_shape<FusedHH, float, fdm_math_approx, false>(shape, a, s);
 }
 } // namespace fdm

@@ -4,6 +4,8 @@
 namespace fdm {
 cudaError_t launch_fused_hh_f32_exact(int shape, const FusedArgs& a, cudaStream_t s)
 {
-  return fused_shape<FusedHH, float, fdm_math_exact>(shape, a, s);
+  if (a.gate)
+    return launch_fused_hh_f32_exact_gate(shape, a, s);
+  return fused_shape<FusedHH, float, fdm_math_exact, false>(shape, a, s);
 }
 } // namespace fdm

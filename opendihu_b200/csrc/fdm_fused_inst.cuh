@@ -28,14 +28,19 @@ cudaError_t launch_fused_hh_f64_exact(int shape, const FusedArgs& a, cudaStream_
 cudaError_t launch_fused_hh_f64_approx(int shape, const FusedArgs& a, cudaStream_t s);
 cudaError_t launch_fused_hh_f32_exact(int shape, const FusedArgs& a, cudaStream_t s);
 cudaError_t launch_fused_hh_f32_approx(int shape, const FusedArgs& a, cudaStream_t s);
+// the same with onlyComputeIfHasBeenStimulated (fdm_fused_*_gate.cu)
+cudaError_t launch_fused_hh_f64_exact_gate(int shape, const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_hh_f64_approx_gate(int shape, const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_hh_f32_exact_gate(int shape, const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_hh_f32_approx_gate(int shape, const FusedArgs& a, cudaStream_t s);
 
-template<class Model, class RR, class Math, int T, int M>
+template<class Model, class RR, class Math, int T, int M, bool GATE>
 static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s)
 {
   constexpr size_t smem = fused_smem_bytes<Model, RR, Math, T, M>();
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(fused_kernel<Model, RR, Math, T, M>,
+    cudaError_t e = cudaFuncSetAttribute(fused_kernel<Model, RR, Math, T, M, GATE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
       return e;
@@ -43,17 +48,17 @@ static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s)
   }
   if (a.n_bins == 0)
     return cudaSuccess;
-  fused_kernel<Model, RR, Math, T, M><<<a.n_bins, T, smem, s>>>(a);
+  fused_kernel<Model, RR, Math, T, M, GATE><<<a.n_bins, T, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template<class Model, class RR, class Math>
+template<class Model, class RR, class Math, bool GATE>
 static cudaError_t fused_shape(int shape, const FusedArgs& a, cudaStream_t s)
 {
   int k = 0;
-#define FDM_SHAPE_CASE(T, M)                       \
-  if (shape == k)                                  \
-    return fused_one<Model, RR, Math, T, M>(a, s); \
+#define FDM_SHAPE_CASE(T, M)                             \
+  if (shape == k)                                        \
+    return fused_one<Model, RR, Math, T, M, GATE>(a, s); \
   k++;
   FDM_FUSED_SHAPES(FDM_SHAPE_CASE)
 #undef FDM_SHAPE_CASE

@@ -120,6 +120,12 @@ struct fdm_solver {
   DevBuf<unsigned char> states, states_lo, params;
   DevBuf<int64_t> off_d, elem_off_d;
   DevBuf<int> clamp_fiber, bin_start_d, bin_fibers_d, alg_idx, trace_slot, nonfinite;
+  // onlyComputeIfHasBeenStimulated: per node code (attributed fiber * 4 + class), per fiber and half step of
+  // a window the first substep a junction-class node computes (0 = all, 255 = none)
+  DevBuf<int> gate;
+  DevBuf<uint8_t> gate_start;
+  std::vector<int> gate_h;
+  bool gate_set = false;
   DevBuf<uint8_t> firing, evaluated_d, hbs;
   DevBuf<int> mu;
   DevBuf<double> freq, repeat, begin, jitter, last_check, cur_jitter;
@@ -172,6 +178,7 @@ struct fdm_solver {
     DevBuf<double> H[2], U[2], X[2], lam, gP, gpf, mu, ascratch, tgrad;
     DevBuf<double> coefs;                           // one factorization per distinct diffusion step width
     DevBuf<uint32_t> flags[2];
+    DevBuf<uint8_t> gates[2];
     cudaStream_t rstream = nullptr;                 // reverse sweeps
     cudaEvent_t replayed[2] = {nullptr, nullptr};   // buffer k filled by a replay
     cudaEvent_t reversed[2] = {nullptr, nullptr};   // buffer k consumed by a reverse sweep
@@ -182,6 +189,8 @@ struct fdm_solver {
         b->release();
       flags[0].release();
       flags[1].release();
+      gates[0].release();
+      gates[1].release();
       ck_jidx.release();
       fin_jidx.release();
       ck_hbs.release();
@@ -521,6 +530,7 @@ static int choose_shape(fdm_solver* s)
 }
 
 static int upload_clamp(fdm_solver* s);
+static int upload_gate(fdm_solver* s);
 
 extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_offsets,
                               const double* element_lengths, const double* prefactor)
@@ -619,6 +629,7 @@ extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_
                              cudaMemcpyHostToDevice, s->stream));
   }
   s->stimulation_set = false;
+  s->gate_set = false;
   s->split_no = 0;
   s->tss_init = false;
   s->ck_valid = false;
@@ -886,6 +897,80 @@ static void select_clamp_center(int n_fibers, const int64_t* off, const int* cen
   }
 }
 
+// onlyComputeIfHasBeenStimulated (compute.tpp:158-205): the reference walks the point buffers of a rank in
+// order; a buffer is skipped while the flag of the fiber it is attributed to (int(b * W / valuesLength[0]))
+// is false, and that flag is set by the fiber's junction buffer when its machine first stimulates.  So a
+// node computes every substep once the flag was set before the call (code class any), and within the call
+// of the first stimulation: nothing if its buffer lies before the junction buffer (class 0), from the
+// stimulating substep on if it is the junction buffer (class 1), everything if it lies after it (class 2).
+static void select_gate_vc(int W, int R, int n_fibers, const int64_t* off, const int* center, int* codes)
+{
+  for (int r = 0; r < R; r++) {
+    std::vector<int> fib;
+    std::vector<int64_t> vo;
+    int64_t total = 0;
+    for (int f = r; f < n_fibers; f += R) {
+      fib.push_back(f);
+      vo.push_back(total);
+      total += off[f + 1] - off[f];
+    }
+    if (fib.empty())
+      continue;
+    vo.push_back(total);
+    const int nl = (int)fib.size();
+    const int64_t nbuf = (total + W - 1) / W;
+    const double factor = (double)W / (double)(vo[1] - vo[0]);
+    auto attributed = [&](int64_t b) {
+      int local = (int)(b * factor);
+      return local >= nl ? nl - 1 : local;
+    };
+    std::vector<int64_t> jb(nl, -1);
+    for (int64_t b = 0; b < nbuf; b++) {
+      const int local = attributed(b);
+      const int64_t index_in_fiber = b * W - vo[local];
+      if ((unsigned long)((long)center[fib[local]] - (long)index_in_fiber) < (unsigned long)W)
+        jb[local] = b;
+    }
+    int l2 = 0;
+    for (int64_t b = 0; b < nbuf; b++) {
+      const int local = attributed(b);
+      const int cls = jb[local] < 0 ? 0 : (b < jb[local] ? 0 : (b == jb[local] ? 1 : 2));
+      for (int lane = 0; lane < W; lane++) {
+        const int64_t i = b * W + lane;
+        if (i >= total)
+          break;
+        while (i >= vo[l2 + 1])
+          l2++;
+        codes[off[fib[l2]] + (i - vo[l2])] = fib[local] * 4 + cls;
+      }
+    }
+  }
+}
+
+// the centre-1..centre+1 rule: every node of a fiber follows its own fiber's flag from the substep on
+// that sets it
+static void select_gate_center(int n_fibers, const int64_t* off, int* codes)
+{
+  for (int f = 0; f < n_fibers; f++)
+    for (int64_t i = off[f]; i < off[f + 1]; i++)
+      codes[i] = f * 4 + 1;
+}
+
+extern "C" int fdm_select_gate_codes(int clamp_rule, int vc_width, int n_ranks, int n_fibers,
+                                     const int64_t* fiber_offsets, const int* stimulation_point_index, int* codes)
+{
+  if (n_fibers < 0 || vc_width < 1 || n_ranks < 1 ||
+      (n_fibers > 0 && (!fiber_offsets || !stimulation_point_index || !codes)))
+    return fail(nullptr, FDM_ERR_ARG, "fdm_select_gate_codes: bad argument");
+  if (clamp_rule == FDM_CLAMP_VC_LANES)
+    select_gate_vc(vc_width, n_ranks, n_fibers, fiber_offsets, stimulation_point_index, codes);
+  else if (clamp_rule == FDM_CLAMP_CENTER)
+    select_gate_center(n_fibers, fiber_offsets, codes);
+  else
+    return fail(nullptr, FDM_ERR_ARG, "fdm_select_gate_codes: unknown clamp rule");
+  return FDM_OK;
+}
+
 extern "C" int fdm_select_clamp_nodes(int clamp_rule, int vc_width, int n_ranks, int n_fibers,
                                       const int64_t* fiber_offsets, const int* stimulation_point_index,
                                       int64_t* first_node, int* count, uint8_t* evaluated)
@@ -899,6 +984,15 @@ extern "C" int fdm_select_clamp_nodes(int clamp_rule, int vc_width, int n_ranks,
     select_clamp_center(n_fibers, fiber_offsets, stimulation_point_index, first_node, count, evaluated);
   else
     return fail(nullptr, FDM_ERR_ARG, "fdm_select_clamp_nodes: unknown clamp rule");
+  return FDM_OK;
+}
+
+static int upload_gate(fdm_solver* s)
+{
+  FDM_CUDA(s->gate.alloc((size_t)std::max<int64_t>(s->n_nodes, 1)));
+  FDM_CUDA(cudaMemcpyAsync(s->gate.p, s->gate_h.data(), sizeof(int) * s->n_nodes, cudaMemcpyHostToDevice, s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  s->gate_set = true;
   return FDM_OK;
 }
 
@@ -989,8 +1083,31 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
   int rc = upload_clamp(s);
   if (rc)
     return rc;
+  if (s->cfg.only_compute_if_stimulated) {
+    s->gate_h.assign((size_t)std::max<int64_t>(s->n_nodes, 1), 0);
+    if (s->cfg.clamp_rule == FDM_CLAMP_VC_LANES)
+      select_gate_vc(s->cfg.vc_width, s->cfg.n_ranks, nf, s->off.data(), center.data(), s->gate_h.data());
+    else
+      select_gate_center(nf, s->off.data(), s->gate_h.data());
+    rc = upload_gate(s);
+    if (rc)
+      return rc;
+  }
   s->stimulation_set = true;
   return FDM_OK;
+}
+
+extern "C" int fdm_set_gate_codes(fdm_solver* s, const int* codes)
+{
+  if (!s || !s->stimulation_set || !codes || !s->cfg.only_compute_if_stimulated)
+    return fail(s, FDM_ERR_ARG, "fdm_set_gate_codes: needs only_compute_if_stimulated and fdm_set_stimulation first");
+  FDM_BIND(s);
+  for (int64_t i = 0; i < s->n_nodes; i++)
+    if (codes[i] < 0 || codes[i] / 4 >= s->n_fibers || codes[i] % 4 > 2)
+      return fail(s, FDM_ERR_ARG, "fdm_set_gate_codes: code out of range");
+  s->gate_h.assign(codes, codes + s->n_nodes);
+  invalidate_graphs(s);
+  return upload_gate(s);
 }
 
 extern "C" int fdm_set_clamp_nodes(fdm_solver* s, const int64_t* first_node, const int* count,
@@ -1130,6 +1247,8 @@ static int ensure_coefficients(fdm_solver* s, double dt1)
 
 struct WindowInfo {
   int words = 0, nsub = 1;
+  const uint8_t* gate_start = nullptr; // onlyComputeIfHasBeenStimulated: first substeps of the window
+  int gate_stride = 0;
 };
 
 static int ensure_step_capacity(fdm_solver* s, int n)
@@ -1148,7 +1267,7 @@ static int ensure_step_capacity(fdm_solver* s, int n)
 
 // uploads a window of split steps (through a pinned slot) and runs the stimulation schedule for it
 static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, WindowInfo* wi,
-                          uint32_t* flags_buf = nullptr)
+                          uint32_t* flags_buf = nullptr, uint8_t* gate_buf = nullptr)
 {
   int rc = ensure_step_capacity(s, n_steps);
   if (rc)
@@ -1188,6 +1307,23 @@ static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_step
   sa.words_per_fiber = words;
   sa.nsub_stride = nsub;
   sa.n_fibers = s->n_fibers;
+  if (s->gate_set) {
+    if (nsub > 253)
+      return fail(s, FDM_ERR_UNSUPPORTED, "onlyComputeIfHasBeenStimulated supports at most 253 Heun substeps per half step");
+    if (!gate_buf) {
+      const size_t need = (size_t)std::max(s->n_fibers, 1) * 2 * s->step_capacity;
+      if (s->gate_start.n < need) {
+        FDM_CUDA(cudaStreamSynchronize(s->stream));
+        FDM_CUDA(s->gate_start.alloc(need));
+        invalidate_graphs(s);
+      }
+      gate_buf = s->gate_start.p;
+    }
+    sa.gate_start = gate_buf;
+    sa.gate_stride = 2 * s->step_capacity;
+  }
+  wi->gate_start = sa.gate_start;
+  wi->gate_stride = sa.gate_stride;
   FDM_CUDA(launch_schedule(sa, s->steps_d.p, n_steps, s->stream));
   s->launches++;
   return FDM_OK;
@@ -1225,6 +1361,9 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
     fa.clamp_fiber = s->clamp_fiber.p;
     fa.flags = s->flags.p;
     fa.words_per_fiber = words;
+    fa.gate = s->gate_set ? s->gate.p : nullptr;
+    fa.gate_start = wi.gate_start;
+    fa.gate_stride = wi.gate_stride;
     fa.nsub_stride = nsub;
     fa.vstim = s->cfg.value_for_stimulated_point;
     fa.stimulus_mode = s->cfg.stimulus_mode;
@@ -1264,6 +1403,9 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
   ra.clamp_fiber = s->clamp_fiber.p;
   ra.flags = s->flags.p;
   ra.words_per_fiber = words;
+  ra.gate = s->gate_set ? s->gate.p : nullptr;
+  ra.gate_start = wi.gate_start;
+  ra.gate_stride = wi.gate_stride;
   ra.nsub_stride = nsub;
   ra.vstim = s->cfg.value_for_stimulated_point;
   ra.stimulus_mode = s->cfg.stimulus_mode;
@@ -1919,7 +2061,14 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       nsub = std::max(nsub, A.steps[j].n0);
     max_words = std::max(max_words, (int)(((e - b) * 2 * nsub + 31) / 32));
   }
+  {
+    int rc = ensure_step_capacity(s, A.kc);
+    if (rc)
+      return rc;
+  }
   for (int k = 0; k < 2; k++) {
+    if (s->gate_set)
+      FDM_CUDA(A.gates[k].alloc((size_t)std::max(nf, 1) * 2 * s->step_capacity));
     FDM_CUDA(A.H[k].alloc((size_t)A.kc * 2 * hstride));
     FDM_CUDA(A.U[k].alloc((size_t)A.kc * N));
     FDM_CUDA(A.X[k].alloc((size_t)A.kc * N));
@@ -1984,7 +2133,7 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       return rc;
     const size_t b = (size_t)c * A.kc, e = std::min<size_t>(b + A.kc, NT);
     const int len = (int)(e - b);
-    rc = prepare_window(s, A.steps.data() + b, len, &win[c], A.flags[k].p);
+    rc = prepare_window(s, A.steps.data() + b, len, &win[c], A.flags[k].p, s->gate_set ? A.gates[k].p : nullptr);
     if (rc)
       return rc;
     ReactionArgs ra{};
@@ -1996,6 +2145,9 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
     ra.clamp_fiber = s->clamp_fiber.p;
     ra.flags = A.flags[k].p;
     ra.words_per_fiber = win[c].words;
+    ra.gate = s->gate_set ? s->gate.p : nullptr;
+    ra.gate_start = win[c].gate_start;
+    ra.gate_stride = win[c].gate_stride;
     ra.nsub_stride = win[c].nsub;
     ra.vstim = s->cfg.value_for_stimulated_point;
     ra.stimulus_mode = s->cfg.stimulus_mode;
@@ -2041,6 +2193,9 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
     aa.clamp_fiber = s->clamp_fiber.p;
     aa.flags = A.flags[k].p;
     aa.words_per_fiber = win[c].words;
+    aa.gate = s->gate_set ? s->gate.p : nullptr;
+    aa.gate_start = win[c].gate_start;
+    aa.gate_stride = win[c].gate_stride;
     aa.nsub_stride = win[c].nsub;
     aa.vstim = s->cfg.value_for_stimulated_point;
     aa.stimulus_mode = s->cfg.stimulus_mode;

@@ -58,7 +58,25 @@ struct StimArgs {
   int words_per_fiber;
   int nsub_stride;                // bit index = (step*2 + half)*nsub_stride + substep
   int n_fibers;
+  uint8_t* gate_start;            // onlyComputeIfHasBeenStimulated (or null): per fiber and half step of the
+  int gate_stride;                // window, 0 if the fiber's flag was set before the half step, 1 + the
+                                  // substep that sets it, 255 if it stays unset:
+                                  // [fiber * gate_stride + step*2 + half]
 };
+
+// onlyComputeIfHasBeenStimulated: the first substep of half step hs that a node with gate code `code`
+// (attributed fiber * 4 + class, class 0/1/2 = buffer before / at / after the junction buffer) computes;
+// 255 = none (compute.tpp:201-205 in the reference's buffer order: a buffer before the junction buffer
+// still sees the flag unset, the junction buffer computes from the stimulating substep on, a buffer after
+// it sees the flag set)
+__device__ __forceinline__ int gate_first(const uint8_t* __restrict__ gate_start, int gate_stride, int code, int hs)
+{
+  const int st = gate_start[(int64_t)(code >> 2) * gate_stride + hs];
+  const int cls = code & 3;
+  if (st == 0 || st == 255)
+    return st;
+  return cls == 1 ? st - 1 : (cls == 0 ? 255 : 0);
+}
 
 // isCurrentPointStimulated (compute.tpp:509-627), one fiber, one substep
 __device__ __forceinline__ bool stimulation_machine(const StimArgs& a, int f, double t, double& last, double& jit,
@@ -97,8 +115,14 @@ __global__ void stimulation_schedule_kernel(StimArgs a, const SplitStep* __restr
   uint32_t* fl = a.flags + (int64_t)f * a.words_per_fiber;
   for (int w = 0; w < a.words_per_fiber; w++)
     fl[w] = 0u;
-  if (!a.evaluated[f])
+  if (!a.evaluated[f]) {
+    if (a.gate_start) {
+      const uint8_t g = a.has_been_stimulated[f] ? 0 : 255;
+      for (int hs = 0; hs < 2 * n_steps; hs++)
+        a.gate_start[(int64_t)f * a.gate_stride + hs] = g;
+    }
     return;
+  }
   double last = a.last_check_time[f], jit = a.current_jitter[f];
   int jidx = a.jitter_index[f];
   uint8_t hbs = a.has_been_stimulated[f];
@@ -108,10 +132,13 @@ __global__ void stimulation_schedule_kernel(StimArgs a, const SplitStep* __restr
       const double t0 = h ? s.mid : s.t;
       uint32_t word = 0u;
       int word_no = -1;
+      int first = hbs ? 0 : 255;
       for (int k = 0; k < s.n0; k++) {
         const double t = xadd(t0, xmul((double)k, s.dt0));
         const bool st = stimulation_machine(a, f, t, last, jit, jidx);
         if (st) {
+          if (first == 255)
+            first = k + 1;
           hbs = 1;
           const int bit = (j * 2 + h) * a.nsub_stride + k;
           if (bit / 32 != word_no) {
@@ -125,6 +152,8 @@ __global__ void stimulation_schedule_kernel(StimArgs a, const SplitStep* __restr
       }
       if (word_no >= 0)
         fl[word_no] |= word;
+      if (a.gate_start)
+        a.gate_start[(int64_t)f * a.gate_stride + j * 2 + h] = (uint8_t)first;
     }
   }
   a.last_check_time[f] = last;
@@ -228,7 +257,9 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __r
 }
 
 // The FP32 Heun step of two nodes at once, over fdm_f2 pairs (packed FP32 instructions): Vm of each
-// node in FP64; every other state is a pair (S, L) whose sum is its value.  Within a half step the
+// node in FP64; every other state is a pair (S, L) whose sum is its value.  dtr / hdt are the step width
+// and its half per node (a node that skips the substep has 0: y* = y, and S, L, Vm stay as they are).
+// Within a half step the
 // increments dt/2 (f + f*) are summed into L and the right-hand side sees S + L; normalize_pair
 // folds L back into S (Fast2Sum) at the end of the half step.  L stays of the size of a few
 // increments, so no increment is lost against S (the stagnation the compensation exists for) at
@@ -237,7 +268,7 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __r
 template<class Model>
 __device__ __forceinline__ void heun_step2(double& V0, double& V1, const fdm_f2* __restrict__ S,
                                            fdm_f2* __restrict__ L, const fdm_f2* __restrict__ P, double t,
-                                           float dt, bool clamp0, bool clamp1, double vstim)
+                                           fdm_f2 dtr, fdm_f2 hdt, bool clamp0, bool clamp1, double vstim)
 {
   constexpr int NS = Model::nStates;
   fdm_f2 y[NS], r[NS], ys[NS], r2[NS];
@@ -248,7 +279,6 @@ __device__ __forceinline__ void heun_step2(double& V0, double& V1, const fdm_f2*
     y[s] = S[s - 1] + L[s - 1];
   const fdm_f2 tr((float)t);
   Model::template rates_fast2<fdm_math_exact>(tr, y, P, r, alg);
-  const fdm_f2 dtr(dt);
 #pragma unroll
   for (int s = 0; s < NS; s++)
     ys[s] = dtr * r[s] + y[s];
@@ -258,7 +288,6 @@ __device__ __forceinline__ void heun_step2(double& V0, double& V1, const fdm_f2*
   if (clamp1)
     ys[0].v.y = vs;
   Model::template rates_fast2<fdm_math_exact>(tr, ys, P, r2, alg);
-  const fdm_f2 hdt(0.5f * dt);
   const fdm_f2 dv = hdt * (r[0] + r2[0]);
   V0 += (double)dv.v.x;
   V1 += (double)dv.v.y;
@@ -326,6 +355,9 @@ struct ReactionArgs {
   int64_t trace_capacity;
   double* store_states;           // adjoint replay (FP64 only): input state of substep k at
                                   // store_states[(k*nStates + s)*stride + node], or null
+  const int* gate;                // onlyComputeIfHasBeenStimulated: per node gate code, or null
+  const uint8_t* gate_start;
+  int gate_stride;
 };
 
 template<class Model, class RR, class Math>
@@ -356,6 +388,7 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
   const SplitStep s = a.steps[a.step];
   const double t0 = a.half ? s.mid : s.t;
   const int base = (a.step * 2 + a.half) * a.nsub_stride;
+  const int first = a.gate ? gate_first(a.gate_start, a.gate_stride, a.gate[i], a.step * 2 + a.half) : 0;
   for (int k = 0; k < s.n0; k++) {
     const double t = xadd(t0, xmul((double)k, s.dt0));
     const bool stim = cf >= 0 && stim_bit(a.flags, a.words_per_fiber, cf, base + k);
@@ -366,6 +399,8 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
       for (int s2 = 1; s2 < NS; s2++)
         a.store_states[(int64_t)(k * NS + s2) * a.stride + i] = (double)S[s2 - 1];
     }
+    if (k < first)
+      continue; // not computed before the attributed fiber was stimulated
     RR Pk[NP];
 #pragma unroll
     for (int q = 0; q < NP; q++)
@@ -669,6 +704,9 @@ struct AdjointArgs {
   int n_trace;
   int64_t trace_row;              // row of trace_grad for this split step (or -1)
   int use_tape;                   // 1: f(y) evaluated once, its temporaries kept for the backward sweep
+  const int* gate;                // onlyComputeIfHasBeenStimulated: skipped substeps are the identity
+  const uint8_t* gate_start;
+  int gate_stride;
 };
 
 // The right-hand side forms the adjoint uses: with exact exponentials the generated fast form
@@ -747,6 +785,7 @@ __global__ void __launch_bounds__(128, 4) adjoint_half_kernel(AdjointArgs a)
   const double t0 = a.half ? st.mid : st.t;
   const int base = (a.step_in_window * 2 + a.half) * a.nsub_stride;
   const double dt = st.dt0;
+  const int first = a.gate ? gate_first(a.gate_start, a.gate_stride, a.gate[i], a.step_in_window * 2 + a.half) : 0;
   double ynext[PREFETCH ? NS : 1];
   if (PREFETCH && st.n0 > 0) {
 #pragma unroll
@@ -776,6 +815,8 @@ __global__ void __launch_bounds__(128, 4) adjoint_half_kernel(AdjointArgs a)
       for (int s = 0; s < NS; s++)
         y[s] = a.states[(int64_t)(k * NS + s) * N + i];
     }
+    if (k < first)
+      continue; // the forward substep was skipped: its reverse is the identity
     constexpr bool TAPE_OK = F::nTape <= 256;
     double tape[TAPE_OK ? F::nTape : 1];
     if (TAPE_OK && a.use_tape) {
@@ -860,6 +901,9 @@ struct FusedArgs {
   double* trace;
   int n_trace;
   int64_t trace_capacity;
+  const int* gate;                // onlyComputeIfHasBeenStimulated: per node gate code, or null
+  const uint8_t* gate_start;
+  int gate_stride;
 };
 
 // block-wide exclusive scan of affine maps in thread order (REVERSE: from the last thread down)
@@ -1034,7 +1078,9 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
   }
 }
 
-template<class Model, class RR, class Math, int T, int M>
+// GATE: onlyComputeIfHasBeenStimulated is on (a.gate is set); a separate instantiation so that the
+// default path carries none of its per-substep checks
+template<class Model, class RR, class Math, int T, int M, bool GATE>
 __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 {
   constexpr int NS = Model::nStates;
@@ -1049,8 +1095,9 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   double* sG = sF + 2 * (T / 32);    // 2 * (T/32)
   int* s_cf = (int*)(sG + 2 * (T / 32)); // CAP: clamp fiber of each node (-1: not a junction node)
   int* s_ts = s_cf + CAP;                // CAP: trace slot of each node (-1: not traced)
+  int* s_gate = s_ts + CAP;              // CAP: gate code of each node (onlyComputeIfHasBeenStimulated)
   // paired FP32 path: the parameters of node pair p of thread tid, parameter k, at (p * NP + k) * T + tid
-  fdm_f2* sP2 = (fdm_f2*)(s_ts + CAP);
+  fdm_f2* sP2 = (fdm_f2*)(s_gate + CAP);
   __shared__ int64_t fib_global[FUSED_MAX_FIBERS_PER_BIN];
   __shared__ int fib_local[FUSED_MAX_FIBERS_PER_BIN + 1];
 
@@ -1119,6 +1166,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     s_cf[q] = cfj;
     cmask |= (cfj >= 0 ? 1u : 0u) << j;
     s_ts[q] = (ok && a.trace_slot) ? a.trace_slot[i] : -1;
+    s_gate[q] = (ok && a.gate) ? a.gate[i] : 0;
   }
   // stimulation bit of node j at substep bit `bit` (junction nodes only read their fiber's bit)
   auto node_stim = [&](int j, int bit) -> bool {
@@ -1212,16 +1260,48 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       // the substep after which algebraicsForTransfer are stored runs outside the hot loop
       const bool store_here = a.store_alg && half == 1 && step == a.n_steps - 1;
       const int k_end = store_here ? s.n0 - 1 : s.n0;
+      // onlyComputeIfHasBeenStimulated: each node's first computed substep of this half step, 8 bits each
+      constexpr bool gate_on = GATE;
+      unsigned gfirst[(M + 3) / 4];
+#pragma unroll
+      for (int w = 0; w < (M + 3) / 4; w++)
+        gfirst[w] = 0u;
+      if constexpr (gate_on) {
+#pragma unroll
+        for (int j = 0; j < M; j++)
+          gfirst[j >> 2] |= (unsigned)gate_first(a.gate_start, a.gate_stride, s_gate[tid * M + j], step * 2 + half)
+                            << (8 * (j & 3));
+      }
+      auto node_on = [&](int j, int k) -> bool { return k >= (int)((gfirst[j >> 2] >> (8 * (j & 3))) & 0xffu); };
 #pragma unroll 1
       for (int k = 0; k < k_end; k++) {
         const double t = xadd(t0, xmul((double)k, s.dt0));
+        if constexpr (gate_on) {
+          // a substep that no node of the warp computes is skipped by the whole warp
+          bool any = false;
+#pragma unroll
+          for (int j = 0; j < M; j++)
+            any = any || (tid * M + j < nb && node_on(j, k));
+          if (!__any_sync(0xffffffffu, any))
+            continue;
+        }
         if constexpr (PAIR) {
           const float dtf = (float)s.dt0;
+          const fdm_f2 dt_all(dtf), hdt_all(0.5f * dtf);
 #pragma unroll
           for (int p = 0; p < MP; p++) {
             const int j0 = 2 * p;
             if (tid * M + j0 >= nb)
               continue;
+            // a node that does not compute this substep gets step width 0 (its state stays as it is)
+            fdm_f2 dtr = dt_all, hdt = hdt_all;
+            if constexpr (gate_on) {
+              const bool c0 = node_on(j0, k), c1 = node_on(j0 + 1, k);
+              if (!c0 && !c1)
+                continue;
+              dtr = fdm_f2(c0 ? dtf : 0.f, c1 ? dtf : 0.f);
+              hdt = fdm_f2(c0 ? 0.5f * dtf : 0.f, c1 ? 0.5f * dtf : 0.f);
+            }
             const bool stim0 = node_stim(j0, base + k);
             const bool stim1 = node_stim(j0 + 1, base + k);
             fdm_f2 Pp[NP];
@@ -1241,19 +1321,19 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
                     Pk[q].v.y = sv;
                 }
               }
-              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pk, t, dtf, false, false, a.vstim);
+              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pk, t, dtr, hdt, false, false, a.vstim);
             } else {
-              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pp, t, dtf, stim0, stim1, a.vstim);
+              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pp, t, dtr, hdt, stim0, stim1, a.vstim);
             }
           }
           if constexpr (M % 2 == 1) {
-            if (tid * M + M - 1 < nb)
+            if (tid * M + M - 1 < nb && (!gate_on || node_on(M - 1, k)))
               scalar_node(M - 1, t, s.dt0, base + k);
           }
         } else {
 #pragma unroll
           for (int j = 0; j < M; j++) {
-            if (tid * M + j >= nb)
+            if (tid * M + j >= nb || (gate_on && !node_on(j, k)))
               continue;
             scalar_node(j, t, s.dt0, base + k);
           }
@@ -1271,7 +1351,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         const double t = xadd(t0, xmul((double)k, s.dt0));
 #pragma unroll
         for (int j = 0; j < M; j++) {
-          if (tid * M + j >= nb)
+          if (tid * M + j >= nb || (gate_on && !node_on(j, k)))
             continue;
           const bool stim = node_stim(j, base + k);
           RR Sj[NSM], Lj[NSM], Pj[NP];
@@ -1373,7 +1453,7 @@ constexpr size_t fused_smem_bytes()
 {
   constexpr bool PAIR = std::is_same<RR, float>::value && std::is_same<Math, fdm_math_exact>::value;
   constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
-  return sizeof(double) * (5 * T * M + 2 * T + 4 * (T / 32)) + sizeof(int) * 2 * T * M +
+  return sizeof(double) * (5 * T * M + 2 * T + 4 * (T / 32)) + sizeof(int) * 3 * T * M +
          (PAIR ? sizeof(fdm_f2) * (M / 2) * NP * T : 0);
 }
 

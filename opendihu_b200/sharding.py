@@ -86,6 +86,27 @@ def global_clamp_nodes(system: FiberSystem):
                                 system.fiber_offsets, system.stimulation_point_index)
 
 
+def global_gate_codes(system: FiberSystem) -> np.ndarray:
+    """onlyComputeIfHasBeenStimulated codes (attributed fiber * 4 + class per node) of the unsharded system."""
+    return N.select_gate_codes(CLAMP_RULES[system.clamp_rule], int(system.vc_width), int(system.n_ranks),
+                               system.fiber_offsets, system.stimulation_point_index)
+
+
+def shard_gate_codes(system: FiberSystem, fibers, codes) -> np.ndarray:
+    """The global codes of the shard's nodes with the attributed fibers renumbered shard-locally; a node
+    attributed to a fiber of another shard (possible with the vc rule and uneven lengths) cannot be gated
+    without an exchange, so that raises."""
+    fibers = np.asarray(fibers, np.int64)
+    local = np.full(len(system.fiber_offsets) - 1, -1, np.int64)
+    local[fibers] = np.arange(len(fibers))
+    c = np.asarray(codes, np.int64)[node_index(system.fiber_offsets, fibers)]
+    att = local[c >> 2]
+    if np.any(att < 0):
+        raise ValueError("onlyComputeIfHasBeenStimulated: a point buffer of this shard is attributed to a fiber of "
+                         "another shard (vc rule with uneven fiber lengths); use the centre rule or one shard")
+    return (att * 4 + (c & 3)).astype(np.int32)
+
+
 def shard_clamp_nodes(system: FiberSystem, fibers, clamp):
     """The global clamp selection restricted to the given fibers, as shard-local node indices."""
     first, cnt, ev = clamp
@@ -117,6 +138,7 @@ class ShardedSolver:
         self.fibers = lpt_partition(lengths, n)
         self.devices = [devices[k % len(devices)] for k in range(n)]
         clamp = global_clamp_nodes(system)
+        gate = global_gate_codes(system) if system.only_compute_if_has_been_stimulated else None
         self.nodes = [node_index(system.fiber_offsets, f) for f in self.fibers]
         self.shards: List[Optional[FastMonodomainSolver]] = []
         for fib, dev in zip(self.fibers, self.devices):
@@ -126,6 +148,8 @@ class ShardedSolver:
             sub = subset(system, fib)
             sv = FastMonodomainSolver(sub, device=dev, **solver_kw)
             sv.clamp_override = shard_clamp_nodes(system, fib, clamp)
+            if gate is not None:
+                sv.gate_override = shard_gate_codes(system, fib, gate)
             self.shards.append(sv)
         self._start = system.start_time
         self._end = system.end_time

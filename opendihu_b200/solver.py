@@ -71,6 +71,7 @@ class FiberSystem:
     stimulus_value: float = 0.0
     algebraics_for_transfer: Sequence[int] = ()
     states_for_transfer: Sequence[int] = (0,)
+    only_compute_if_has_been_stimulated: bool = False   # "onlyComputeIfHasBeenStimulated"
 
     @property
     def n_fibers(self) -> int:
@@ -269,10 +270,11 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         rng = np.random.default_rng(int(b200.get("neuromuscularJunctionSeed", 0)))
         u = rng.uniform(0.5 - nmj_size / 2, 0.5 + nmj_size / 2, size=nf)
         center = (lengths * u).astype(np.int32)
-    for opt in ("onlyComputeIfHasBeenStimulated", "disableComputationWhenStatesAreCloseToEquilibrium"):
-        if fast.get(opt, True):
-            warnings.warn(f"{opt}=True is not implemented by the B200 solver; every node is computed every step "
-                          "(the reference's own tests set it to False)")
+    # both options default to True in the reference (fast_monodomain_solver_initialization.tpp:68-69)
+    only_if_stimulated = bool(fast.get("onlyComputeIfHasBeenStimulated", True))
+    if fast.get("disableComputationWhenStatesAreCloseToEquilibrium", True):
+        warnings.warn("disableComputationWhenStatesAreCloseToEquilibrium=True is not implemented by the B200 solver; "
+                      "nodes close to equilibrium are computed (the reference's own tests set it to False)")
 
     precision = b200.get("precision", "fp32" if fast.get("useSinglePrecision", False) else "fp64")
     sys_ = FiberSystem(
@@ -290,7 +292,8 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         stimulus_mode=b200.get("stimulusMode", "clamp"), stimulus_parameter=int(b200.get("stimulusParameter", 0)),
         stimulus_value=float(b200.get("stimulusValue", 0.0)),
         algebraics_for_transfer=[int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))],
-        states_for_transfer=[int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))] or [0])
+        states_for_transfer=[int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))] or [0],
+        only_compute_if_has_been_stimulated=only_if_stimulated)
     sys_.method = b200.get("method", "split")
     sys_.precision = precision
     return sys_
@@ -323,6 +326,8 @@ class FastMonodomainSolver:
         #: (first_node, count, evaluated) per fiber replacing the clamp selection of fdm_set_stimulation
         #: (set by the sharded solver to keep the selection of the unsharded layout)
         self.clamp_override = None
+        #: per-node onlyComputeIfHasBeenStimulated codes replacing the library's selection (sharded solver)
+        self.gate_override = None
         self._h = None
         self._start = system.start_time
         self._end = system.end_time
@@ -369,6 +374,7 @@ class FastMonodomainSolver:
         cfg.check_nan = int(bool(self.check_nan))
         cfg.profile = int(bool(self.profile))
         cfg.device = self.device
+        cfg.only_compute_if_stimulated = int(bool(s.only_compute_if_has_been_stimulated))
         h = C.c_void_p()
         N.check(L.fdm_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -390,6 +396,9 @@ class FastMonodomainSolver:
                                   zip(self.clamp_override, (np.int64, np.int32, np.uint8)))
                 self._call(L.fdm_set_clamp_nodes, N.ptr(first, C.c_int64), N.ptr(cnt, C.c_int),
                            N.ptr(ev, C.c_uint8))
+            if self.gate_override is not None and s.only_compute_if_has_been_stimulated:
+                codes = np.ascontiguousarray(self.gate_override, np.int32)
+                self._call(L.fdm_set_gate_codes, N.ptr(codes, C.c_int))
             if len(s.algebraics_for_transfer):
                 idx = np.ascontiguousarray(s.algebraics_for_transfer, np.int32)
                 self._call(L.fdm_set_algebraics_for_transfer, len(idx), N.ptr(idx, C.c_int))

@@ -172,6 +172,10 @@ typedef struct {
   const int64_t *trace_nodes;
   double *trace;                  /* [split step][trace node], Vm after each split step */
   int64_t trace_capacity;         /* number of split steps the trace buffer holds */
+  /* onlyComputeIfHasBeenStimulated (compute.tpp:201-205): a point buffer is not computed while the
+   * fiber it is attributed to has not been stimulated; the flag per fiber is in/out (NULL: all 0) */
+  int only_if_stimulated;
+  int *has_been_stimulated;
 } oracle_problem;
 
 typedef struct {
@@ -270,8 +274,11 @@ static void compute0d(const oracle_problem *p, oracle_rank *r, oracle_fiber_stat
   const int64_t N = r->n_buffers * W;
   const double factor = (double)W / (double)(r->values_offset[1] - r->values_offset[0]);
   /* buffers are independent; each fiber's stimulation machine is advanced only by the one buffer
-   * that holds its junction, so the loop runs in parallel without changing the result */
-#pragma omp parallel for num_threads(p->n_threads > 0 ? p->n_threads : 1) schedule(static)
+   * that holds its junction, so the loop runs in parallel without changing the result.  With
+   * onlyComputeIfHasBeenStimulated a buffer reads the flag its fiber's junction buffer sets, so the
+   * buffers run in the reference's order, one after the other. */
+  const int serial = p->only_if_stimulated != 0;
+#pragma omp parallel for num_threads(serial ? 1 : (p->n_threads > 0 ? p->n_threads : 1)) schedule(static)
   for (int64_t b = 0; b < r->n_buffers; b++) {
     double y[ORACLE_MAX_STATES], prm[ORACLE_MAX_PARAMETERS];
     int local = (int)(b * factor);
@@ -290,6 +297,8 @@ static void compute0d(const oracle_problem *p, oracle_rank *r, oracle_fiber_stat
       int stim = 0;
       if (in_center)
         stim = stimulation_machine(p, f, &fs[f], t);
+      if (p->only_if_stimulated && !fs[f].has_been_stimulated)
+        continue; /* compute.tpp:201-205 */
       const int store_now = store && k == n_steps - 1;
       for (int lane = 0; lane < W; lane++) {
         const int64_t i = b * W + lane;
@@ -326,13 +335,16 @@ static void compute0d_center(const oracle_problem *p, oracle_rank *r, oracle_fib
   {
   double y[ORACLE_MAX_STATES], prm[ORACLE_MAX_PARAMETERS], prm_stim[ORACLE_MAX_PARAMETERS];
   int *stim = (int *)malloc(sizeof(int) * (n_steps > 0 ? n_steps : 1));
+  int *stim_seen = (int *)malloc(sizeof(int) * (n_steps > 0 ? n_steps : 1));
 #pragma omp for schedule(dynamic, 1)
   for (int lf = 0; lf < r->n_fibers; lf++) {
     const int f = r->fibers[lf];
     const int64_t n = p->fiber_offsets[f + 1] - p->fiber_offsets[f];
     const int64_t center = p->stimulation_point_index[f];
-    for (int k = 0; k < n_steps; k++)
+    for (int k = 0; k < n_steps; k++) {
       stim[k] = stimulation_machine(p, f, &fs[f], t0 + k * dt);
+      stim_seen[k] = fs[f].has_been_stimulated; /* the flag after the machine's substep k */
+    }
     for (int64_t j = 0; j < n; j++) {
       const int64_t i = r->values_offset[lf] + j;
       for (int s = 0; s < m->n_states; s++)
@@ -344,6 +356,8 @@ static void compute0d_center(const oracle_problem *p, oracle_rank *r, oracle_fib
         prm_stim[p->stimulus_parameter] = p->stimulus_value;
       for (int k = 0; k < n_steps; k++) {
         const double t = t0 + k * dt;
+        if (p->only_if_stimulated && !stim_seen[k])
+          continue;
         const int on = stim[k] && clamp;
         heun_step(m, y, (p->stimulus_mode == 1 && on) ? prm_stim : prm, t, dt, on, p->stimulus_mode == 0, p->value_for_stimulated_point,
                   store && k == n_steps - 1, p, r->alg_out + i, N);
@@ -353,6 +367,7 @@ static void compute0d_center(const oracle_problem *p, oracle_rank *r, oracle_fib
     }
   }
   free(stim);
+  free(stim_seen);
   }
 }
 
@@ -531,6 +546,7 @@ int64_t oracle_run(const oracle_problem *p, double *states, double *last_check_t
     fs[f].last_check_time = last_check_time[f];
     fs[f].current_jitter = current_jitter[f];
     fs[f].jitter_index = jitter_index[f];
+    fs[f].has_been_stimulated = p->has_been_stimulated ? p->has_been_stimulated[f] : 0;
   }
 
   /* RepeatedCall (repeated_call.tpp:43-75) */
@@ -614,6 +630,8 @@ int64_t oracle_run(const oracle_problem *p, double *states, double *last_check_t
     last_check_time[f] = fs[f].last_check_time;
     current_jitter[f] = fs[f].current_jitter;
     jitter_index[f] = fs[f].jitter_index;
+    if (p->has_been_stimulated)
+      p->has_been_stimulated[f] = fs[f].has_been_stimulated;
   }
   free_ranks(p, ranks);
   free(ranks);

@@ -53,6 +53,7 @@ class Problem(C.Structure):
         ("algebraics_out", C.POINTER(C.c_double)),
         ("n_trace_nodes", C.c_int), ("trace_nodes", C.POINTER(C.c_int64)), ("trace", C.POINTER(C.c_double)),
         ("trace_capacity", C.c_int64),
+        ("only_if_stimulated", C.c_int), ("has_been_stimulated", C.POINTER(C.c_int)),
     ]
 
 
@@ -166,8 +167,11 @@ class OracleRun:
         self.trace = np.full((max(cap, 1), max(len(tn), 1)), np.nan)
         p.trace = _p(self.trace, C.c_double)
         p.trace_capacity = cap
-        self.p = p
+        p.only_if_stimulated = int(bool(spec.get("only_if_stimulated", False)))
         nf = p.n_fibers
+        self.has_been_stimulated = np.zeros(max(nf, 1), np.int32)
+        p.has_been_stimulated = _p(self.has_been_stimulated, C.c_int)
+        self.p = p
         self.last_check_time = np.zeros(nf)
         self.current_jitter = np.zeros(nf)
         self.jitter_index = np.zeros(nf, np.int32)

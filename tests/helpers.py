@@ -62,6 +62,7 @@ def oracle_spec(system: S.FiberSystem, n_threads: int = 0, trace_nodes=(), trace
         "n_threads": n_threads or (os.cpu_count() or 1),
         "algebraic_indices": list(system.algebraics_for_transfer),
         "trace_nodes": list(trace_nodes), "trace_capacity": trace_capacity,
+        "only_if_stimulated": bool(getattr(system, "only_compute_if_has_been_stimulated", False)),
     }
 
 

@@ -55,3 +55,14 @@ def test_sharded_adjoint_equals_unsharded():
     np.testing.assert_array_equal(tr2, tr)
     for k in ("prefactor", "parameters", "states0"):
         np.testing.assert_allclose(g2[k], g[k], rtol=1e-12, atol=1e-300)
+
+
+def test_sharded_only_if_stimulated_equals_unsharded():
+    s = _system(clamp_rule="center")
+    s.only_compute_if_has_been_stimulated = True
+    s.call_enable_begin = np.linspace(0.0, 2.0, s.n_fibers)
+    ref = _unsharded(s)
+    with SH.ShardedSolver(s.copy(), devices=[0], n_shards=3) as sh:
+        sh.advanceTimeSpan()
+        st = sh.states()
+    np.testing.assert_array_equal(st, ref)

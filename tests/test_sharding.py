@@ -140,3 +140,20 @@ def test_two_gloo_ranks_gather_shards():
     full, _, _, _ = H.run_oracle(s.copy(), n_threads=1)
     assert sorted(out[0] + out[1]) == list(range(6))
     np.testing.assert_array_equal(out["vm"], full[0])
+
+
+def test_shard_gate_codes_map_fibers():
+    s = WL.batched_hh(n_fibers=9, min_nodes=20, max_nodes=40, seed=6, end_time=0.0, clamp_rule="center")
+    codes = SH.global_gate_codes(s)
+    for fib in SH.lpt_partition(np.diff(s.fiber_offsets), 3):
+        c = SH.shard_gate_codes(s, fib, codes)
+        sub = SH.subset(s, fib)
+        want = N.select_gate_codes(S.CLAMP_RULES["center"], 4, 1, sub.fiber_offsets, sub.stimulation_point_index)
+        np.testing.assert_array_equal(c, want)
+    # vc rule, uneven lengths: some buffer is attributed across a shard boundary
+    s.clamp_rule = "vc"
+    codes = SH.global_gate_codes(s)
+    if np.any((codes >> 2) != np.repeat(np.arange(9), np.diff(s.fiber_offsets))):
+        with pytest.raises(ValueError):
+            for fib in SH.lpt_partition(np.diff(s.fiber_offsets), 3):
+                SH.shard_gate_codes(s, fib, codes)

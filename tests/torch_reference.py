@@ -175,9 +175,11 @@ class Machine:
         return check and bool(self.fe[row, self.mu % self.fe.shape[1]])
 
 
-def forward(system, prefactor, params, sensors, clamp_first, clamp_count):
+def forward(system, prefactor, params, sensors, clamp_first, clamp_count, gate_codes=None):
     """Differentiable trace [steps, sensors]; prefactor [n_fibers] and params [n_params, n_nodes] are torch
-    tensors (float64), states start from system.states."""
+    tensors (float64), states start from system.states.  gate_codes (per node attributed fiber * 4 + class,
+    from the library's host-only selection): onlyComputeIfHasBeenStimulated, a node keeps its state at the
+    substeps its attributed fiber's flag does not yet allow (compute.tpp:201-205 in buffer order)."""
     model = TorchModel(system.model)
     off = np.asarray(system.fiber_offsets)
     nf = len(off) - 1
@@ -193,20 +195,39 @@ def forward(system, prefactor, params, sensors, clamp_first, clamp_count):
     trace = []
     sensors_t = torch.as_tensor(np.asarray(sensors), dtype=torch.long)
 
+    evaluated = [len(c) > 0 for c in clamp_nodes]
+    hbs = [False] * nf
+
     def half(t0, dt0, n0, y):
+        stims = []
+        for k in range(n0):
+            t = t0 + k * dt0
+            stims.append([machines[f](t) if evaluated[f] else False for f in range(nf)])
+        first = np.zeros(N, np.int64)
+        if gate_codes is not None:
+            start = []
+            for f in range(nf):
+                ks = [k for k in range(n0) if stims[k][f]]
+                start.append(0 if hbs[f] else (ks[0] + 1 if ks else 255))
+                hbs[f] = hbs[f] or bool(ks)
+            for i in range(N):
+                st, cls = start[gate_codes[i] >> 2], gate_codes[i] & 3
+                first[i] = st if st in (0, 255) else (st - 1 if cls == 1 else (255 if cls == 0 else 0))
         for k in range(n0):
             t = t0 + k * dt0
             mask = np.zeros(N, bool)
             for f in range(nf):
-                if machines[f](t):
+                if stims[k][f]:
                     mask[clamp_nodes[f]] = True
             m = torch.as_tensor(mask)
             r = model.rates(t, y, P)
             ys = [y[s] + dt0 * r[s] for s in range(model.n_states)]
             ys[0] = torch.where(m, torch.full_like(ys[0], vstim), ys[0])
             r2 = model.rates(t, ys, P)
-            y = [y[s] + 0.5 * dt0 * (r[s] + r2[s]) for s in range(model.n_states)]
-            y[0] = torch.where(m, torch.full_like(y[0], vstim), y[0])
+            yn = [y[s] + 0.5 * dt0 * (r[s] + r2[s]) for s in range(model.n_states)]
+            yn[0] = torch.where(m, torch.full_like(yn[0], vstim), yn[0])
+            on = torch.as_tensor(k >= first)
+            y = [torch.where(on, yn[s], y[s]) for s in range(model.n_states)]
         return y
 
     def diffusion(u, dt):
