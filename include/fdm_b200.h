@@ -86,6 +86,10 @@ typedef struct fdm_config {
   int only_compute_if_stimulated; /* "onlyComputeIfHasBeenStimulated" (compute.tpp:201-205): a node's Heun
                                      substeps are skipped while the fiber its point buffer is attributed to
                                      has not been stimulated (0: every node computed, the parity setting) */
+  int skip_close_to_equilibrium;  /* "disableComputationWhenStatesAreCloseToEquilibrium" (compute.tpp:130-265,
+                                     630-797): point buffers whose states stop changing are skipped and a rank
+                                     whose buffers are all counted inactive skips its diffusion solve; split
+                                     method with the vc clamp rule only (0: off, the parity setting) */
 } fdm_config;
 
 /* fills *cfg with the reference's defaults (HH, implicit Euler, FP64 split, vc rule W=4, 20 mV clamp) */
@@ -131,6 +135,11 @@ int fdm_set_stimulation(fdm_solver *s, const uint8_t *firing_events, int rows, i
 int fdm_get_clamp_nodes(fdm_solver *s, int64_t *first_node, int *count, uint8_t *evaluated);
 /* replaces the clamp nodes fdm_set_stimulation chose (e.g. with a selection made for a larger layout) */
 int fdm_set_clamp_nodes(fdm_solver *s, const int64_t *first_node, const int *count, const uint8_t *evaluated);
+/* disableComputationWhenStatesAreCloseToEquilibrium: the number of point buffers (all ranks, rank after rank),
+ * their statuses (0 inactive, 1 neighbor_is_active, 2 active; may be NULL) and the per-rank counts of
+ * inactive buffers (n_ranks entries; may be NULL) -- the "computeStateInformation" data of
+ * fast_monodomain_solver_communication.tpp:280-290 */
+int fdm_get_equilibrium_state(fdm_solver *s, int64_t *n_buffers, uint8_t *status, int *counter);
 /* host-only: per node, the code (attributed fiber) * 4 + class that onlyComputeIfHasBeenStimulated uses:
  * class 0/1/2 = the node's point buffer lies before / is / lies after the junction buffer of the fiber it
  * is attributed to (compute.tpp:158-205 processes buffers in order and the junction buffer sets the flag) */

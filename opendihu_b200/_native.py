@@ -31,7 +31,7 @@ EXPORTED = [
     "fdm_checkpoint_save", "fdm_checkpoint_restore", "fdm_fused_shapes", "fdm_diffusion_solve",
     "fdm_diffusion_solve_noalloc", "fdm_compat_configure", "fdm_compat_release", "fdm_adjoint_forward",
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
-    "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes",
+    "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes", "fdm_get_equilibrium_state",
 ]
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
@@ -54,7 +54,7 @@ class Config(C.Structure):
         ("dt_splitting", C.c_double), ("dt_0d", C.c_double), ("dt_1d", C.c_double),
         ("steps_per_launch", C.c_int), ("threads_per_block", C.c_int), ("nodes_per_thread", C.c_int),
         ("check_nan", C.c_int), ("profile", C.c_int), ("device", C.c_int), ("use_graph", C.c_int),
-        ("only_compute_if_stimulated", C.c_int),
+        ("only_compute_if_stimulated", C.c_int), ("skip_close_to_equilibrium", C.c_int),
     ]
 
 
@@ -113,6 +113,7 @@ def lib() -> C.CDLL:
         "fdm_select_clamp_nodes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, i64, i32, i64, i32, u8]),
         "fdm_select_gate_codes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, i64, i32, i32]),
         "fdm_set_gate_codes": (C.c_int, [P, i32]),
+        "fdm_get_equilibrium_state": (C.c_int, [P, i64, u8, i32]),
         "fdm_compat_release": (C.c_int, []),
         "initializeArrays": (None, [d, i32, i32, C.c_char_p, d, i32, i32, d, d, d, d]),
         "computeMonodomain": (None, [C.POINTER(C.c_float), d, d, C.POINTER(C.c_float), C.c_double, C.c_double,

@@ -126,6 +126,23 @@ struct fdm_solver {
   DevBuf<uint8_t> gate_start;
   std::vector<int> gate_h;
   bool gate_set = false;
+
+  // disableComputationWhenStatesAreCloseToEquilibrium (fdm_equilibrium.cuh): buffer layout of the ranks,
+  // statuses (double-buffered per half step), counts, padding lanes and the speculative results
+  struct Equilibrium {
+    bool on = false;
+    int64_t n_buffers = 0;
+    int n_pad = 0;
+    std::vector<int> pad_src;       // per padding lane: node whose parameters it holds
+    DevBuf<int> buf_of, lane_node, jfiber, buf_rank, rank_first, counter, nbuf, pad_clamp, pad_gate;
+    DevBuf<uint8_t> st[2], info, prefix, block_agg, ran_b;
+    DevBuf<double> vm_pad, vm_a, vm_b, alg_a, alg_b;
+    DevBuf<uint8_t> states_pad, states_lo_pad, params_pad, st_a, stl_a, st_b, stl_b; // reaction precision
+    DevBuf<uint8_t> ck_st, ck_states_pad, ck_states_lo_pad;
+    DevBuf<int> ck_counter;
+    DevBuf<double> ck_vm_pad;
+    bool ck_valid = false;
+  } eq;
   DevBuf<uint8_t> firing, evaluated_d, hbs;
   DevBuf<int> mu;
   DevBuf<double> freq, repeat, begin, jitter, last_check, cur_jitter;
@@ -366,6 +383,10 @@ extern "C" int fdm_create(const fdm_config* cfg, fdm_solver** out)
     return fail(nullptr, FDM_ERR_ARG, "fdm_create: stimulus_parameter out of range");
   if (!(cfg->dt_repeated_call > 0) || !(cfg->dt_splitting > 0) || !(cfg->dt_0d > 0) || !(cfg->dt_1d > 0))
     return fail(nullptr, FDM_ERR_ARG, "fdm_create: time step widths must be positive");
+  if (cfg->skip_close_to_equilibrium &&
+      (cfg->method != FDM_METHOD_SPLIT || cfg->clamp_rule != FDM_CLAMP_VC_LANES))
+    return fail(nullptr, FDM_ERR_UNSUPPORTED, "fdm_create: the equilibrium skip (point buffers of the vc path) "
+                                              "needs FDM_METHOD_SPLIT and FDM_CLAMP_VC_LANES");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(nullptr, FDM_ERR_NO_DEVICE, "fdm_create: no CUDA device");
@@ -531,6 +552,8 @@ static int choose_shape(fdm_solver* s)
 
 static int upload_clamp(fdm_solver* s);
 static int upload_gate(fdm_solver* s);
+static int eq_copy_pad_params(fdm_solver* s);
+static int eq_reset(fdm_solver* s);
 
 extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_offsets,
                               const double* element_lengths, const double* prefactor)
@@ -797,6 +820,11 @@ extern "C" int fdm_set_parameters(fdm_solver* s, const double* parameters)
       tmp[i] = (float)parameters[i];
     FDM_CUDA(cudaMemcpyAsync(s->params.p, tmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
   }
+  if (s->eq.on) {
+    int rc = eq_copy_pad_params(s);
+    if (rc)
+      return rc;
+  }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
   return FDM_OK;
 }
@@ -996,6 +1024,169 @@ static int upload_gate(fdm_solver* s)
   return FDM_OK;
 }
 
+// equilibrium skip: padding lanes hold the parameters of their rank's first node (the reference fills
+// every lane with the first instance's values before it copies the fibers' values in)
+static int eq_copy_pad_params(fdm_solver* s)
+{
+  auto& E = s->eq;
+  const int NP = s->model->n_parameters;
+  const int rb = s->real_bytes;
+  for (int p = 0; p < E.n_pad; p++)
+    for (int q = 0; q < NP; q++)
+      FDM_CUDA(cudaMemcpyAsync(E.params_pad.p + ((size_t)q * E.n_pad + p) * rb,
+                               (const uint8_t*)s->params.p + ((size_t)q * s->n_nodes + E.pad_src[p]) * rb, rb,
+                               cudaMemcpyDeviceToDevice, s->stream));
+  return FDM_OK;
+}
+
+// statuses all active, counts 0, padding lanes at the model's initial values (initialization.tpp:128-134, 430-431)
+static int eq_reset(fdm_solver* s)
+{
+  auto& E = s->eq;
+  const int NS = s->model->n_states;
+  const int R = s->cfg.n_ranks;
+  for (int k = 0; k < 2; k++)
+    FDM_CUDA(cudaMemsetAsync(E.st[k].p, EQ_ACTIVE, std::max<int64_t>(E.n_buffers, 1), s->stream));
+  FDM_CUDA(cudaMemsetAsync(E.counter.p, 0, sizeof(int) * R, s->stream));
+  if (E.n_pad > 0) {
+    std::vector<double> vm(E.n_pad, s->model->states_initial[0]);
+    std::vector<uint8_t> st((size_t)std::max(NS - 1, 1) * E.n_pad * s->real_bytes, 0);
+    for (int q = 1; q < NS; q++)
+      for (int p = 0; p < E.n_pad; p++) {
+        const size_t at = ((size_t)(q - 1) * E.n_pad + p) * s->real_bytes;
+        if (s->real_bytes == 8) {
+          const double v = s->model->states_initial[q];
+          std::memcpy(&st[at], &v, 8);
+        } else {
+          const float v = (float)s->model->states_initial[q];
+          std::memcpy(&st[at], &v, 4);
+        }
+      }
+    FDM_CUDA(cudaMemcpyAsync(E.vm_pad.p, vm.data(), sizeof(double) * E.n_pad, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.states_pad.p, st.data(), st.size(), cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemsetAsync(E.states_lo_pad.p, 0, st.size(), s->stream));
+  }
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
+// the point-buffer layout of the vc path: rank r holds fibers r, r+R, ... concatenated, cut into buffers of W
+// lanes; the buffer's attributed fiber int(b W / len0), its junction fiber, and the padding lanes
+static int eq_build(fdm_solver* s, const std::vector<int>& center)
+{
+  auto& E = s->eq;
+  const int W = s->cfg.vc_width, R = s->cfg.n_ranks, nf = s->n_fibers;
+  const int64_t N = s->n_nodes;
+  const int NS = s->model->n_states, NP = s->model->n_parameters;
+  std::vector<int> rank_first(R + 1, 0), nbuf(R, 0), buf_rank, jfiber, lane_node, buf_of(N, 0), pad_clamp, pad_gate;
+  std::vector<int> buf_code; // onlyComputeIfHasBeenStimulated code of each buffer (for its padding lanes)
+  E.pad_src.clear();
+  int n_pad = 0;
+  for (int r = 0; r < R; r++) {
+    rank_first[r] = (int)buf_rank.size();
+    std::vector<int> fib;
+    std::vector<int64_t> vo;
+    int64_t total = 0;
+    for (int f = r; f < nf; f += R) {
+      fib.push_back(f);
+      vo.push_back(total);
+      total += s->off[f + 1] - s->off[f];
+    }
+    if (fib.empty())
+      continue;
+    vo.push_back(total);
+    const int nl = (int)fib.size();
+    const int64_t nb = (total + W - 1) / W;
+    nbuf[r] = (int)nb;
+    const double factor = (double)W / (double)(vo[1] - vo[0]);
+    std::vector<int64_t> jb(nl, -1);
+    std::vector<int> att(nb);
+    for (int64_t b = 0; b < nb; b++) {
+      int local = (int)(b * factor);
+      if (local >= nl)
+        local = nl - 1;
+      att[b] = local;
+      const int64_t index_in_fiber = b * W - vo[local];
+      if ((unsigned long)((long)center[fib[local]] - (long)index_in_fiber) < (unsigned long)W)
+        jb[local] = b;
+    }
+    int l2 = 0;
+    for (int64_t b = 0; b < nb; b++) {
+      const int gb = (int)buf_rank.size();
+      buf_rank.push_back(r);
+      const int local = att[b];
+      jfiber.push_back(jb[local] == b ? fib[local] : -1);
+      const int cls = jb[local] < 0 ? 0 : (b < jb[local] ? 0 : (b == jb[local] ? 1 : 2));
+      buf_code.push_back(fib[local] * 4 + cls);
+      for (int lane = 0; lane < W; lane++) {
+        const int64_t i = b * W + lane;
+        if (i < total) {
+          while (i >= vo[l2 + 1])
+            l2++;
+          const int64_t g = s->off[fib[l2]] + (i - vo[l2]);
+          lane_node.push_back((int)g);
+          buf_of[g] = gb;
+        } else {
+          lane_node.push_back((int)(N + n_pad));
+          buf_of.push_back(gb);
+          pad_clamp.push_back((jb[local] == b && lane < std::min(3, W)) ? fib[local] : -1);
+          pad_gate.push_back(fib[local] * 4 + cls);
+          E.pad_src.push_back((int)s->off[fib[0]]);
+          n_pad++;
+        }
+      }
+    }
+  }
+  rank_first[R] = (int)buf_rank.size();
+  E.n_buffers = (int64_t)buf_rank.size();
+  E.n_pad = n_pad;
+  const int64_t nt = N + n_pad;
+  const size_t nsm = (size_t)std::max(NS - 1, 1), rb = (size_t)s->real_bytes;
+  auto up = [&](DevBuf<int>& d, const std::vector<int>& h) -> cudaError_t {
+    cudaError_t e = d.alloc(std::max<size_t>(h.size(), 1));
+    if (e == cudaSuccess && !h.empty())
+      e = cudaMemcpyAsync(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, s->stream);
+    return e;
+  };
+  FDM_CUDA(up(E.buf_of, buf_of));
+  FDM_CUDA(up(E.lane_node, lane_node));
+  FDM_CUDA(up(E.jfiber, jfiber));
+  FDM_CUDA(up(E.buf_rank, buf_rank));
+  FDM_CUDA(up(E.rank_first, rank_first));
+  FDM_CUDA(up(E.nbuf, nbuf));
+  FDM_CUDA(up(E.pad_clamp, pad_clamp));
+  FDM_CUDA(up(E.pad_gate, pad_gate));
+  FDM_CUDA(E.counter.alloc(R));
+  for (int k = 0; k < 2; k++)
+    FDM_CUDA(E.st[k].alloc(std::max<int64_t>(E.n_buffers, 1)));
+  FDM_CUDA(E.info.alloc(std::max<int64_t>(E.n_buffers, 1)));
+  FDM_CUDA(E.prefix.alloc(std::max<int64_t>(E.n_buffers, 1)));
+  FDM_CUDA(E.block_agg.alloc(std::max<int64_t>((E.n_buffers + EQ_SCAN_T - 1) / EQ_SCAN_T, 1)));
+  FDM_CUDA(E.ran_b.alloc(std::max<int64_t>(nt, 1)));
+  FDM_CUDA(E.vm_pad.alloc(std::max(n_pad, 1)));
+  FDM_CUDA(E.states_pad.alloc(nsm * std::max(n_pad, 1) * rb));
+  FDM_CUDA(E.states_lo_pad.alloc(nsm * std::max(n_pad, 1) * rb));
+  FDM_CUDA(E.params_pad.alloc((size_t)std::max(NP, 1) * std::max(n_pad, 1) * rb));
+  FDM_CUDA(E.vm_a.alloc(std::max<int64_t>(nt, 1)));
+  FDM_CUDA(E.vm_b.alloc(std::max<int64_t>(nt, 1)));
+  FDM_CUDA(E.st_a.alloc(nsm * std::max<int64_t>(nt, 1) * rb));
+  FDM_CUDA(E.stl_a.alloc(nsm * std::max<int64_t>(nt, 1) * rb));
+  FDM_CUDA(E.st_b.alloc(nsm * std::max<int64_t>(nt, 1) * rb));
+  FDM_CUDA(E.stl_b.alloc(nsm * std::max<int64_t>(nt, 1) * rb));
+  FDM_CUDA(E.alg_a.alloc((size_t)std::max(s->n_alg_out, 1) * std::max<int64_t>(nt, 1)));
+  FDM_CUDA(E.alg_b.alloc((size_t)std::max(s->n_alg_out, 1) * std::max<int64_t>(nt, 1)));
+  int rc = eq_copy_pad_params(s);
+  if (rc)
+    return rc;
+  rc = eq_reset(s);
+  if (rc)
+    return rc;
+  E.on = true;
+  E.ck_valid = false;
+  (void)buf_code;
+  return FDM_OK;
+}
+
 static int upload_clamp(fdm_solver* s)
 {
   std::vector<int> cf((size_t)std::max<int64_t>(s->n_nodes, 1), -1);
@@ -1083,6 +1274,11 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
   int rc = upload_clamp(s);
   if (rc)
     return rc;
+  if (s->cfg.skip_close_to_equilibrium) {
+    rc = eq_build(s, center);
+    if (rc)
+      return rc;
+  }
   if (s->cfg.only_compute_if_stimulated) {
     s->gate_h.assign((size_t)std::max<int64_t>(s->n_nodes, 1), 0);
     if (s->cfg.clamp_rule == FDM_CLAMP_VC_LANES)
@@ -1094,6 +1290,23 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
       return rc;
   }
   s->stimulation_set = true;
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_equilibrium_state(fdm_solver* s, int64_t* n_buffers, uint8_t* status, int* counter)
+{
+  if (!s || !s->eq.on)
+    return fail(s, FDM_ERR_ARG, "fdm_get_equilibrium_state: the equilibrium skip is not on (or fdm_set_stimulation "
+                                "was not called)");
+  FDM_BIND(s);
+  if (n_buffers)
+    *n_buffers = s->eq.n_buffers;
+  if (status && s->eq.n_buffers > 0)
+    FDM_CUDA(cudaMemcpyAsync(status, s->eq.st[0].p, s->eq.n_buffers, cudaMemcpyDeviceToHost, s->stream));
+  if (counter)
+    FDM_CUDA(cudaMemcpyAsync(counter, s->eq.counter.p, sizeof(int) * s->cfg.n_ranks, cudaMemcpyDeviceToHost,
+                             s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
   return FDM_OK;
 }
 
@@ -1419,6 +1632,63 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
   ra.trace = s->trace.p;
   ra.n_trace = s->n_trace;
   ra.trace_capacity = s->trace_capacity;
+  if (s->eq.on) {
+    // equilibrium skip: every half step is a speculative reaction, the buffer scan and a commit; the statuses
+    // alternate between the two status arrays, and a window has an even number of half steps
+    auto& E = s->eq;
+    const int64_t nt = s->n_nodes + E.n_pad;
+    FDM_CUDA(E.alg_a.alloc((size_t)std::max(s->n_alg_out, 1) * std::max<int64_t>(nt, 1)));
+    FDM_CUDA(E.alg_b.alloc((size_t)std::max(s->n_alg_out, 1) * std::max<int64_t>(nt, 1)));
+    EqLayout L{};
+    L.W = s->cfg.vc_width;
+    L.n_ranks = s->cfg.n_ranks;
+    L.n_nodes = s->n_nodes;
+    L.n_pad = E.n_pad;
+    L.n_buffers = E.n_buffers;
+    L.buf_of = E.buf_of.p;
+    L.lane_node = E.lane_node.p;
+    L.jfiber = E.jfiber.p;
+    L.buf_rank = E.buf_rank.p;
+    L.rank_first = E.rank_first.p;
+    L.counter = E.counter.p;
+    EqSpec e{};
+    e.nt = nt;
+    e.vm_pad = E.vm_pad.p;
+    e.states_pad = E.states_pad.p;
+    e.states_lo_pad = E.states_lo_pad.p;
+    e.params_pad = E.params_pad.p;
+    e.pad_clamp = E.pad_clamp.p;
+    e.pad_gate = E.pad_gate.p;
+    e.vm_a = E.vm_a.p;
+    e.st_a = E.st_a.p;
+    e.stl_a = E.stl_a.p;
+    e.alg_a = E.alg_a.p;
+    e.vm_b = E.vm_b.p;
+    e.st_b = E.st_b.p;
+    e.stl_b = E.stl_b.p;
+    e.alg_b = E.alg_b.p;
+    e.ran_b = E.ran_b.p;
+    int cur = 0;
+    for (int j = 0; j < n_steps; j++) {
+      ra.step = j;
+      for (int half = 0; half < 2; half++) {
+        ra.half = half;
+        ra.store_alg = (store_alg && s->n_alg_out > 0 && half == 1 && j == n_steps - 1) ? 1 : 0;
+        L.st_in = E.st[cur].p;
+        L.st_out = E.st[cur ^ 1].p;
+        FDM_CUDA(launch_equilibrium_half(s->cfg.model, rk, mk, ra, L, e, E.info.p, E.prefix.p, E.block_agg.p,
+                                         s->model->n_states, half == 1, s->stream));
+        s->launches += 6;
+        cur ^= 1;
+        if (half == 0) {
+          FDM_CUDA(launch_diffusion_warp(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
+                                         s->stream, E.counter.p, E.nbuf.p, s->cfg.n_ranks));
+          s->launches++;
+        }
+      }
+    }
+    return FDM_OK;
+  }
   // without profiling, a window that stores no algebraics replays a captured CUDA graph of its launches
   const bool graph_ok = s->cfg.use_graph && !prof && !(store_alg && s->n_alg_out > 0);
   if (graph_ok) {
@@ -1668,6 +1938,24 @@ extern "C" int fdm_checkpoint_save(fdm_solver* s)
     FDM_CUDA(cudaMemcpyAsync(s->ck_jidx.p, s->jitter_idx.p, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->ck_hbs.p, s->hbs.p, nf, cudaMemcpyDeviceToDevice, s->stream));
   }
+  if (s->eq.on) {
+    auto& E = s->eq;
+    const size_t nsb = (size_t)std::max(NS - 1, 1) * std::max(E.n_pad, 1) * s->real_bytes;
+    FDM_CUDA(E.ck_st.alloc(std::max<int64_t>(E.n_buffers, 1)));
+    FDM_CUDA(E.ck_counter.alloc(s->cfg.n_ranks));
+    FDM_CUDA(E.ck_vm_pad.alloc(std::max(E.n_pad, 1)));
+    FDM_CUDA(E.ck_states_pad.alloc(nsb));
+    FDM_CUDA(E.ck_states_lo_pad.alloc(nsb));
+    FDM_CUDA(cudaMemcpyAsync(E.ck_st.p, E.st[0].p, std::max<int64_t>(E.n_buffers, 1), cudaMemcpyDeviceToDevice,
+                             s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.ck_counter.p, E.counter.p, sizeof(int) * s->cfg.n_ranks, cudaMemcpyDeviceToDevice,
+                             s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.ck_vm_pad.p, E.vm_pad.p, sizeof(double) * std::max(E.n_pad, 1),
+                             cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.ck_states_pad.p, E.states_pad.p, nsb, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.ck_states_lo_pad.p, E.states_lo_pad.p, nsb, cudaMemcpyDeviceToDevice, s->stream));
+    E.ck_valid = true;
+  }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
   s->ck_strang = s->strang;
   s->ck_heun = s->heun;
@@ -1700,6 +1988,18 @@ extern "C" int fdm_checkpoint_restore(fdm_solver* s)
     FDM_CUDA(cudaMemcpyAsync(s->cur_jitter.p, s->ck_jit.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, s->ck_jidx.p, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->hbs.p, s->ck_hbs.p, nf, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  if (s->eq.on && s->eq.ck_valid) {
+    auto& E = s->eq;
+    const size_t nsb = (size_t)std::max(NS - 1, 1) * std::max(E.n_pad, 1) * s->real_bytes;
+    FDM_CUDA(cudaMemcpyAsync(E.st[0].p, E.ck_st.p, std::max<int64_t>(E.n_buffers, 1), cudaMemcpyDeviceToDevice,
+                             s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.counter.p, E.ck_counter.p, sizeof(int) * s->cfg.n_ranks, cudaMemcpyDeviceToDevice,
+                             s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.vm_pad.p, E.ck_vm_pad.p, sizeof(double) * std::max(E.n_pad, 1),
+                             cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.states_pad.p, E.ck_states_pad.p, nsb, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(E.states_lo_pad.p, E.ck_states_lo_pad.p, nsb, cudaMemcpyDeviceToDevice, s->stream));
   }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
   s->strang = s->ck_strang;
@@ -1971,6 +2271,9 @@ static int copy_state(fdm_solver* s, double* vm, double* st, double* last, doubl
 extern "C" int fdm_adjoint_forward(fdm_solver* s, double t_start, double t_end, int checkpoint_every, int n_sensors,
                                    const int64_t* sensor_nodes)
 {
+  if (s && s->eq.on)
+    return fail(s, FDM_ERR_UNSUPPORTED, "fdm_adjoint_forward: the equilibrium skip's decisions are not differentiable; "
+                                        "switch it off for the adjoint");
   if (!s || checkpoint_every < 1 || n_sensors < 0 || (n_sensors > 0 && !sensor_nodes))
     return fail(s, FDM_ERR_ARG, "fdm_adjoint_forward: bad argument");
   FDM_BIND(s);
@@ -2314,6 +2617,11 @@ extern "C" int fdm_rewind(fdm_solver* s)
     FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, ji.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->hbs.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  if (s->eq.on) {
+    int rc = eq_reset(s);
+    if (rc)
+      return rc;
   }
   return FDM_OK;
 }

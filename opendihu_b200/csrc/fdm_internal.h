@@ -7,6 +7,7 @@
 #include <string>
 
 #include "fdm_kernels.cuh"
+#include "fdm_equilibrium.cuh"
 
 namespace fdm {
 
@@ -34,7 +35,13 @@ cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_ste
 cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
                                 double* coef, int64_t stride, cudaStream_t s);
 cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
-                                  double* vm, double* scratch, cudaStream_t s);
+                                  double* vm, double* scratch, cudaStream_t s, const int* eq_counter = nullptr,
+                                  const int* eq_nbuf = nullptr, int n_ranks = 1);
+// one half step with the equilibrium skip (fdm_equilibrium.cuh): speculative reaction, equilibrium tests,
+// scan of the buffers, commit (and the trace after half 1)
+cudaError_t launch_equilibrium_half(int model, RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L,
+                                    const EqSpec& e, uint8_t* info, uint8_t* prefix, uint8_t* block_agg, int n_states,
+                                    bool trace, cudaStream_t s);
 // adjoint (FP64)
 cudaError_t launch_adjoint_half(int model, MathKind mk, const AdjointArgs& a, cudaStream_t s);
 cudaError_t launch_adjoint_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths,

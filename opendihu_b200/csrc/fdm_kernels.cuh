@@ -523,13 +523,19 @@ __device__ __forceinline__ Affine compose(const Affine& first, const Affine& sec
 #ifdef FDM_COMMON_KERNELS_TU
 // split path: one warp per fiber; each lane owns a contiguous chunk of the fiber.
 // Forward sweep results d' go to `scratch` (one double per node) for the backward sweep.
+// eq_counter / eq_nbuf (or null): the equilibrium skip's per-rank count of inactive buffers and number of
+// buffers; a fiber of a rank whose buffers are all counted inactive is not solved (compute.tpp:261-265)
 __global__ void __launch_bounds__(128) diffusion_warp_kernel(int n_fibers, const int64_t* __restrict__ fiber_offsets,
                                                              const double* __restrict__ coef, int64_t stride,
-                                                             double* __restrict__ vm, double* __restrict__ scratch)
+                                                             double* __restrict__ vm, double* __restrict__ scratch,
+                                                             const int* __restrict__ eq_counter,
+                                                             const int* __restrict__ eq_nbuf, int n_ranks)
 {
   const int lane = threadIdx.x & 31;
   const int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (f >= n_fibers)
+    return;
+  if (eq_counter && eq_counter[f % n_ranks] == eq_nbuf[f % n_ranks])
     return;
   const int64_t o = fiber_offsets[f];
   const int64_t n = fiber_offsets[f + 1] - o;

@@ -1,6 +1,7 @@
 // Split-path kernels (reaction, diffusion, stimulation schedule) and the model table.
 #define FDM_COMMON_KERNELS_TU
 #include "fdm_internal.h"
+#include "fdm_equilibrium.cuh"
 
 #include "generated/hodgkin_huxley_1952_anone_c2_3_4.cuh"
 #include "generated/shorten_ocallaghan_davidson_soboleva_2007_a32_c65.cuh"
@@ -76,14 +77,69 @@ cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, cons
 }
 
 cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
-                                  double* vm, double* scratch, cudaStream_t s)
+                                  double* vm, double* scratch, cudaStream_t s, const int* eq_counter,
+                                  const int* eq_nbuf, int n_ranks)
 {
   if (n_fibers == 0)
     return cudaSuccess;
   const int T = 128;
   const int64_t threads = (int64_t)n_fibers * 32;
   diffusion_warp_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, s>>>(n_fibers, fiber_offsets, coef, stride, vm,
-                                                                        scratch);
+                                                                        scratch, eq_counter, eq_nbuf,
+                                                                        n_ranks > 0 ? n_ranks : 1);
+  return cudaGetLastError();
+}
+
+// ---- equilibrium skip ----
+template<class Model, class RR, class Math>
+static cudaError_t reaction_eq_one(const ReactionArgs& a, const EqLayout& L, const EqSpec& e, cudaStream_t s)
+{
+  const int T = 128;
+  const int64_t blocks = (e.nt + T - 1) / T;
+  if (blocks == 0)
+    return cudaSuccess;
+  reaction_eq_kernel<Model, RR, Math><<<(unsigned)blocks, T, 0, s>>>(a, L, e);
+  return cudaGetLastError();
+}
+
+template<class Model>
+static cudaError_t reaction_eq_model(RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L,
+                                     const EqSpec& e, cudaStream_t s)
+{
+  if (rk == REAL_F64)
+    return mk == MATH_EXACT ? reaction_eq_one<Model, double, fdm_math_exact>(a, L, e, s)
+                            : reaction_eq_one<Model, double, fdm_math_approx>(a, L, e, s);
+  return mk == MATH_EXACT ? reaction_eq_one<Model, float, fdm_math_exact>(a, L, e, s)
+                          : reaction_eq_one<Model, float, fdm_math_approx>(a, L, e, s);
+}
+
+cudaError_t launch_equilibrium_half(int model, RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L,
+                                    const EqSpec& e, uint8_t* info, uint8_t* prefix, uint8_t* block_agg, int n_states,
+                                    bool trace, cudaStream_t s)
+{
+  cudaError_t ce = cudaSuccess;
+  switch (model) {
+  case 0: ce = reaction_eq_model<HH>(rk, mk, a, L, e, s); break;
+  case 1: ce = reaction_eq_model<SH>(rk, mk, a, L, e, s); break;
+  default: return cudaErrorInvalidValue;
+  }
+  if (ce != cudaSuccess || L.n_buffers == 0)
+    return ce;
+  const int T = 128;
+  const unsigned bb = (unsigned)((L.n_buffers + T - 1) / T);
+  if (rk == REAL_F64)
+    eq_changed_kernel<double><<<bb, T, 0, s>>>(a, L, e, n_states, info);
+  else
+    eq_changed_kernel<float><<<bb, T, 0, s>>>(a, L, e, n_states, info);
+  const int64_t nblk = (L.n_buffers + EQ_SCAN_T - 1) / EQ_SCAN_T;
+  eq_scan_block_kernel<<<(unsigned)nblk, EQ_SCAN_T, 0, s>>>(L, info, prefix, block_agg);
+  eq_scan_top_kernel<<<1, 1, 0, s>>>(block_agg, nblk);
+  if (rk == REAL_F64)
+    eq_commit_kernel<double><<<bb, T, 0, s>>>(a, L, e, info, prefix, block_agg, n_states);
+  else
+    eq_commit_kernel<float><<<bb, T, 0, s>>>(a, L, e, info, prefix, block_agg, n_states);
+  if (trace && a.trace_slot)
+    eq_trace_kernel<<<(unsigned)((a.n_nodes + T - 1) / T), T, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -72,6 +72,7 @@ class FiberSystem:
     algebraics_for_transfer: Sequence[int] = ()
     states_for_transfer: Sequence[int] = (0,)
     only_compute_if_has_been_stimulated: bool = False   # "onlyComputeIfHasBeenStimulated"
+    skip_close_to_equilibrium: bool = False   # "disableComputationWhenStatesAreCloseToEquilibrium" (split, vc)
 
     @property
     def n_fibers(self) -> int:
@@ -270,11 +271,11 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         rng = np.random.default_rng(int(b200.get("neuromuscularJunctionSeed", 0)))
         u = rng.uniform(0.5 - nmj_size / 2, 0.5 + nmj_size / 2, size=nf)
         center = (lengths * u).astype(np.int32)
-    # both options default to True in the reference (fast_monodomain_solver_initialization.tpp:68-69)
-    only_if_stimulated = bool(fast.get("onlyComputeIfHasBeenStimulated", True))
-    if fast.get("disableComputationWhenStatesAreCloseToEquilibrium", True):
-        warnings.warn("disableComputationWhenStatesAreCloseToEquilibrium=True is not implemented by the B200 solver; "
-                      "nodes close to equilibrium are computed (the reference's own tests set it to False)")
+    # both options default to True in the reference (fast_monodomain_solver_initialization.tpp:68-69); its
+    # "gpu" optimizationType ignores them (fast_monodomain_solver_gpu.tpp computes every node)
+    vc_path = cellml.get("optimizationType", "vc") == "vc"
+    only_if_stimulated = vc_path and bool(fast.get("onlyComputeIfHasBeenStimulated", True))
+    skip_equilibrium = vc_path and bool(fast.get("disableComputationWhenStatesAreCloseToEquilibrium", True))
 
     precision = b200.get("precision", "fp32" if fast.get("useSinglePrecision", False) else "fp64")
     sys_ = FiberSystem(
@@ -293,7 +294,7 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         stimulus_value=float(b200.get("stimulusValue", 0.0)),
         algebraics_for_transfer=[int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))],
         states_for_transfer=[int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))] or [0],
-        only_compute_if_has_been_stimulated=only_if_stimulated)
+        only_compute_if_has_been_stimulated=only_if_stimulated, skip_close_to_equilibrium=skip_equilibrium)
     sys_.method = b200.get("method", "split")
     sys_.precision = precision
     return sys_
@@ -375,6 +376,7 @@ class FastMonodomainSolver:
         cfg.profile = int(bool(self.profile))
         cfg.device = self.device
         cfg.only_compute_if_stimulated = int(bool(s.only_compute_if_has_been_stimulated))
+        cfg.skip_close_to_equilibrium = int(bool(s.skip_close_to_equilibrium))
         h = C.c_void_p()
         N.check(L.fdm_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -562,6 +564,16 @@ class FastMonodomainSolver:
         v = C.c_double()
         self._call(N.lib().fdm_adjoint_timing, C.byref(v))
         return v.value
+
+    def equilibrium_state(self):
+        """(statuses of all point buffers, per-rank counts of inactive buffers) of the equilibrium skip
+        (0 inactive, 1 neighbor_is_active, 2 active)."""
+        n = C.c_int64()
+        self._call(N.lib().fdm_get_equilibrium_state, C.byref(n), None, None)
+        st = np.zeros(max(n.value, 1), np.uint8)
+        cnt = np.zeros(max(self.system.n_ranks, 1), np.int32)
+        self._call(N.lib().fdm_get_equilibrium_state, C.byref(n), N.ptr(st, C.c_uint8), N.ptr(cnt, C.c_int))
+        return st[:n.value], cnt
 
     def clamp_nodes(self):
         nf = self.system.n_fibers

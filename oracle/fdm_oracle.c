@@ -51,6 +51,7 @@ static const oracle_model oracle_models[] = {
 };
 #define ORACLE_N_MODELS ((int)(sizeof(oracle_models) / sizeof(oracle_models[0])))
 #define ORACLE_MAX_STATES 64
+#define ORACLE_MAX_VC_WIDTH 16
 #define ORACLE_MAX_ALGEBRAICS 80
 #define ORACLE_MAX_PARAMETERS 8
 
@@ -176,7 +177,19 @@ typedef struct {
    * fiber it is attributed to has not been stimulated; the flag per fiber is in/out (NULL: all 0) */
   int only_if_stimulated;
   int *has_been_stimulated;
+  /* disableComputationWhenStatesAreCloseToEquilibrium (compute.tpp:630-797): every point buffer carries a
+   * status (0 inactive, 1 neighbor_is_active, 2 active), a rank counts its buffers set inactive, and a
+   * rank whose count equals its number of buffers skips compute1D (compute.tpp:261-265).  In/out, per
+   * rank: eq_status (the ranks' buffers one after the other; NULL: all active), eq_counter (NULL: 0),
+   * pad_states [rank][lane][state] for the lanes of a rank's last buffer past its last node, which the
+   * reference computes like the others and includes in the equilibrium test (NULL: initial values). */
+  int equilibrium;
+  uint8_t *eq_status;
+  int *eq_counter;
+  double *pad_states;
 } oracle_problem;
+
+enum { EQ_INACTIVE = 0, EQ_NEIGHBOR_IS_ACTIVE = 1, EQ_ACTIVE = 2 };
 
 typedef struct {
   double last_check_time, current_jitter;
@@ -241,6 +254,8 @@ typedef struct {
   double *params;        /* [p][n_buffers*W] */
   double *alg_out;       /* [k][n_buffers*W] */
   double *c_prime, *d_prime;
+  uint8_t *eq_status;    /* n_buffers (points into the problem's eq_status or a local array) */
+  int eq_counter;
 } oracle_rank;
 
 static void heun_step(const oracle_model *m, double *y, const double *prm, double t, double dt, int stimulate,
@@ -265,7 +280,62 @@ static void heun_step(const oracle_model *m, double *y, const double *prm, doubl
       alg_store[k * stride] = alg2[p->algebraic_indices[k]];
 }
 
-/* compute0D for one rank (compute.tpp:131-254 with the equilibrium skips disabled) */
+/* equilibriumAccelerationUpdate (compute.tpp:630-762) for buffer b after its substeps: the buffer is at
+ * equilibrium if no state of any lane changed by more than 1e-6 (relative, or absolute when the smallest
+ * lane value of the state is below 1e-11 in magnitude); statuses and the rank's count follow the
+ * reference's three-state rules */
+static void equilibrium_update(const oracle_model *m, oracle_rank *r, int64_t b, int W, int64_t N,
+                               const double *previous)
+{
+  uint8_t *st = r->eq_status;
+  const int64_t nb = r->n_buffers;
+  int at_equilibrium = 1;
+  if (st[b] != EQ_INACTIVE) {
+    for (int s = 0; s < m->n_states && at_equilibrium; s++) {
+      double vmin = r->states[s * N + b * W];
+      for (int lane = 1; lane < W; lane++)
+        if (r->states[s * N + b * W + lane] < vmin)
+          vmin = r->states[s * N + b * W + lane];
+      double change = 0.0;
+      for (int lane = 0; lane < W; lane++) {
+        const double nv = r->states[s * N + b * W + lane], ov = previous[s * W + lane];
+        const double c = fabs(vmin) < 1e-11 ? fabs(nv - ov) : fabs((nv - ov) / nv);
+        if (c > change || c != c)
+          change = c != c ? INFINITY : c;
+      }
+      if (change > 1e-6)
+        at_equilibrium = 0;
+    }
+  }
+  if (st[b] == EQ_NEIGHBOR_IS_ACTIVE && at_equilibrium) {
+    if (b > 0 && st[b - 1] != EQ_ACTIVE && st[b] != EQ_INACTIVE) {
+      st[b] = EQ_INACTIVE;
+      r->eq_counter++;
+    }
+    if (b < nb - 1 && st[b + 1] != EQ_ACTIVE && st[b] != EQ_INACTIVE) {
+      st[b] = EQ_INACTIVE;
+      r->eq_counter++;
+    }
+  }
+  if (st[b] == EQ_ACTIVE || st[b] == EQ_NEIGHBOR_IS_ACTIVE) {
+    if (at_equilibrium) {
+      st[b] = EQ_INACTIVE;
+      r->eq_counter++;
+    } else {
+      st[b] = EQ_ACTIVE;
+      if (b > 0 && st[b - 1] == EQ_INACTIVE) {
+        r->eq_counter--;
+        st[b - 1] = EQ_NEIGHBOR_IS_ACTIVE;
+      }
+      if (b < nb - 1 && st[b + 1] == EQ_INACTIVE) {
+        r->eq_counter--;
+        st[b + 1] = EQ_NEIGHBOR_IS_ACTIVE;
+      }
+    }
+  }
+}
+
+/* compute0D for one rank (compute.tpp:131-254) */
 static void compute0d(const oracle_problem *p, oracle_rank *r, oracle_fiber_state *fs, double t0, double dt,
                       int n_steps, int store)
 {
@@ -277,10 +347,24 @@ static void compute0d(const oracle_problem *p, oracle_rank *r, oracle_fiber_stat
    * that holds its junction, so the loop runs in parallel without changing the result.  With
    * onlyComputeIfHasBeenStimulated a buffer reads the flag its fiber's junction buffer sets, so the
    * buffers run in the reference's order, one after the other. */
-  const int serial = p->only_if_stimulated != 0;
+  const int eq = p->equilibrium != 0;
+  const int serial = p->only_if_stimulated != 0 || eq;
+  const int64_t nb = r->n_buffers;
+  uint8_t *status = r->eq_status;
+  if (eq && nb > 0) {
+    /* compute.tpp:154-156: the first and the last buffer of the rank are set active (the count is not
+     * adjusted) */
+    status[0] = EQ_ACTIVE;
+    status[nb - 1] = EQ_ACTIVE;
+  }
 #pragma omp parallel for num_threads(serial ? 1 : (p->n_threads > 0 ? p->n_threads : 1)) schedule(static)
   for (int64_t b = 0; b < r->n_buffers; b++) {
     double y[ORACLE_MAX_STATES], prm[ORACLE_MAX_PARAMETERS];
+    double previous[ORACLE_MAX_STATES * ORACLE_MAX_VC_WIDTH];
+    if (eq)
+      for (int lane = 0; lane < W; lane++)
+        for (int s = 0; s < m->n_states; s++)
+          previous[s * W + lane] = r->states[s * N + b * W + lane];
     int local = (int)(b * factor);
     if (local >= r->n_fibers)
       local = r->n_fibers - 1;
@@ -297,13 +381,29 @@ static void compute0d(const oracle_problem *p, oracle_rank *r, oracle_fiber_stat
       int stim = 0;
       if (in_center)
         stim = stimulation_machine(p, f, &fs[f], t);
+      if (eq) {
+        /* isEquilibriumAccelerationCurrentPointDisabled (compute.tpp:764-797) */
+        if (stim) {
+          status[b] = EQ_ACTIVE;
+          if (b > 0 && status[b - 1] == EQ_INACTIVE) {
+            r->eq_counter--;
+            status[b - 1] = EQ_NEIGHBOR_IS_ACTIVE;
+          }
+          if (b < nb - 1 && status[b + 1] == EQ_INACTIVE) {
+            r->eq_counter--;
+            status[b + 1] = EQ_NEIGHBOR_IS_ACTIVE;
+          }
+        }
+        if (status[b] == EQ_INACTIVE)
+          continue;
+      }
       if (p->only_if_stimulated && !fs[f].has_been_stimulated)
         continue; /* compute.tpp:201-205 */
       const int store_now = store && k == n_steps - 1;
       for (int lane = 0; lane < W; lane++) {
         const int64_t i = b * W + lane;
-        if (r->node_of[i] < 0)
-          continue; /* padding lane */
+        if (r->node_of[i] < 0 && !eq)
+          continue; /* padding lane (computed by the reference, but it only matters to the equilibrium test) */
         for (int s = 0; s < m->n_states; s++)
           y[s] = r->states[s * N + i];
         for (int q = 0; q < m->n_parameters; q++)
@@ -320,6 +420,8 @@ static void compute0d(const oracle_problem *p, oracle_rank *r, oracle_fiber_stat
           r->states[s * N + i] = y[s];
       }
     }
+    if (eq)
+      equilibrium_update(m, r, b, W, N, previous);
   }
 }
 
@@ -507,11 +609,20 @@ static void build_ranks(const oracle_problem *p, oracle_rank *ranks, const doubl
           r->params[q * N + i] = p->parameters[q * n_nodes + g];
       }
     }
-    /* padding lanes hold the initial values (initializeStates runs on every buffer) */
+    /* padding lanes hold the initial values (initializeStates runs on every buffer) or, for the
+     * equilibrium test, the values they reached in earlier runs; their parameters are those of the rank's
+     * first instance (initialization.tpp:436-441 fills every lane with them before the fibers' values) */
     for (int64_t i = 0; i < N; i++)
-      if (r->node_of[i] < 0)
+      if (r->node_of[i] < 0) {
+        const int lane = (int)(i % W);
         for (int s = 0; s < m->n_states; s++)
-          r->states[s * N + i] = m->states_initial[s];
+          r->states[s * N + i] = (p->equilibrium && p->pad_states)
+                                     ? p->pad_states[((int64_t)rk * W + lane) * m->n_states + s]
+                                     : m->states_initial[s];
+        if (r->n_fibers > 0)
+          for (int q = 0; q < m->n_parameters; q++)
+            r->params[q * N + i] = p->parameters[q * n_nodes + p->fiber_offsets[r->fibers[0]]];
+      }
   }
 }
 
@@ -539,8 +650,28 @@ int64_t oracle_run(const oracle_problem *p, double *states, double *last_check_t
     return -1;
   const oracle_model *m = &oracle_models[p->model];
   const int64_t n_nodes = p->fiber_offsets[p->n_fibers];
+  if (p->equilibrium && p->vc_width > ORACLE_MAX_VC_WIDTH)
+    return -1;
   oracle_rank *ranks = (oracle_rank *)calloc(p->n_ranks, sizeof(oracle_rank));
   build_ranks(p, ranks, states);
+  uint8_t *local_status = NULL;
+  if (p->equilibrium) {
+    int64_t total_buffers = 0;
+    for (int rk = 0; rk < p->n_ranks; rk++)
+      total_buffers += ranks[rk].n_buffers;
+    uint8_t *st = p->eq_status;
+    if (!st) {
+      local_status = (uint8_t *)malloc(total_buffers > 0 ? total_buffers : 1);
+      memset(local_status, EQ_ACTIVE, total_buffers > 0 ? total_buffers : 1);
+      st = local_status;
+    }
+    int64_t o = 0;
+    for (int rk = 0; rk < p->n_ranks; rk++) {
+      ranks[rk].eq_status = st + o;
+      ranks[rk].eq_counter = p->eq_counter ? p->eq_counter[rk] : 0;
+      o += ranks[rk].n_buffers;
+    }
+  }
   oracle_fiber_state *fs = (oracle_fiber_state *)calloc(p->n_fibers > 0 ? p->n_fibers : 1, sizeof(oracle_fiber_state));
   for (int f = 0; f < p->n_fibers; f++) {
     fs[f].last_check_time = last_check_time[f];
@@ -582,7 +713,9 @@ int64_t oracle_run(const oracle_problem *p, double *states, double *last_check_t
           compute0d(p, r, fs, tc, dt0, n0, 0);
         else
           compute0d_center(p, r, fs, tc, dt0, n0, 0);
-        compute1d(p, r, dt1);
+        /* compute.tpp:261-265: no 1D solve when every buffer of the rank is counted inactive */
+        if (!(p->equilibrium && p->clamp_rule == 0 && r->eq_counter == (int)r->n_buffers))
+          compute1d(p, r, dt1);
         if (p->clamp_rule == 0)
           compute0d(p, r, fs, mid, dt0, n0, store);
         else
@@ -632,6 +765,22 @@ int64_t oracle_run(const oracle_problem *p, double *states, double *last_check_t
     jitter_index[f] = fs[f].jitter_index;
     if (p->has_been_stimulated)
       p->has_been_stimulated[f] = fs[f].has_been_stimulated;
+  }
+  if (p->equilibrium) {
+    for (int rk = 0; rk < p->n_ranks; rk++) {
+      oracle_rank *r = &ranks[rk];
+      if (p->eq_counter)
+        p->eq_counter[rk] = r->eq_counter;
+      if (p->pad_states) {
+        const int W = p->vc_width;
+        const int64_t N = r->n_buffers * W;
+        for (int64_t i = 0; i < N; i++)
+          if (r->node_of[i] < 0)
+            for (int s = 0; s < m->n_states; s++)
+              p->pad_states[((int64_t)rk * W + (i % W)) * m->n_states + s] = r->states[s * N + i];
+      }
+    }
+    free(local_status);
   }
   free_ranks(p, ranks);
   free(ranks);

@@ -54,6 +54,8 @@ class Problem(C.Structure):
         ("n_trace_nodes", C.c_int), ("trace_nodes", C.POINTER(C.c_int64)), ("trace", C.POINTER(C.c_double)),
         ("trace_capacity", C.c_int64),
         ("only_if_stimulated", C.c_int), ("has_been_stimulated", C.POINTER(C.c_int)),
+        ("equilibrium", C.c_int), ("eq_status", C.POINTER(C.c_uint8)), ("eq_counter", C.POINTER(C.c_int)),
+        ("pad_states", C.POINTER(C.c_double)),
     ]
 
 
@@ -169,6 +171,19 @@ class OracleRun:
         p.trace_capacity = cap
         p.only_if_stimulated = int(bool(spec.get("only_if_stimulated", False)))
         nf = p.n_fibers
+        # equilibrium skip: statuses of every rank's buffers (all active), counters, padding-lane states
+        p.equilibrium = int(bool(spec.get("equilibrium", False)))
+        W, R = p.vc_width, p.n_ranks
+        lengths = np.diff(offsets)
+        n_buf = [int((lengths[r::R].sum() + W - 1) // W) for r in range(R)]
+        self.eq_status = np.full(max(sum(n_buf), 1), 2, np.uint8)
+        self.eq_counter = np.zeros(R, np.int32)
+        ns = model_info(spec["model"])[0]
+        init = model_info(spec["model"])[3]
+        self.pad_states = np.tile(init, R * W).astype(np.float64)
+        p.eq_status = _p(self.eq_status, C.c_uint8)
+        p.eq_counter = _p(self.eq_counter, C.c_int)
+        p.pad_states = _p(self.pad_states, C.c_double)
         self.has_been_stimulated = np.zeros(max(nf, 1), np.int32)
         p.has_been_stimulated = _p(self.has_been_stimulated, C.c_int)
         self.p = p

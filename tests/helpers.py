@@ -63,6 +63,7 @@ def oracle_spec(system: S.FiberSystem, n_threads: int = 0, trace_nodes=(), trace
         "algebraic_indices": list(system.algebraics_for_transfer),
         "trace_nodes": list(trace_nodes), "trace_capacity": trace_capacity,
         "only_if_stimulated": bool(getattr(system, "only_compute_if_has_been_stimulated", False)),
+        "equilibrium": bool(getattr(system, "skip_close_to_equilibrium", False)),
     }
 
 

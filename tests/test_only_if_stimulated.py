@@ -133,12 +133,11 @@ def reference_settings(n_fibers=2, n_elements=20, **fast):
 
 
 def test_settings_key():
-    with pytest.warns(UserWarning, match="disableComputationWhenStatesAreCloseToEquilibrium"):
-        s = S.parse_settings(reference_settings())          # the reference's defaults: both True
-    assert s.only_compute_if_has_been_stimulated
+    s = S.parse_settings(reference_settings())          # the reference's defaults: both True
+    assert s.only_compute_if_has_been_stimulated and s.skip_close_to_equilibrium
     s = S.parse_settings(reference_settings(onlyComputeIfHasBeenStimulated=False,
                                             disableComputationWhenStatesAreCloseToEquilibrium=False))
-    assert not s.only_compute_if_has_been_stimulated
+    assert not s.only_compute_if_has_been_stimulated and not s.skip_close_to_equilibrium
     assert s.n_fibers == 2 and s.n_nodes == 42
     np.testing.assert_allclose(s.element_lengths, 0.01)
     np.testing.assert_allclose(s.parameters[:, 0], [0.0, 120.0, 36.0])
