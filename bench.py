@@ -323,9 +323,9 @@ def main():
     cpu = None
     if rank == 0 and not args.skip_accuracy:
         threads = os.cpu_count() or 1
-        sub, ref, n_ref, rate, cpu_s = cpu_baseline(system, 8, 15.0, threads)
+        sub, ref, n_ref, rate, cpu_s = cpu_baseline(system, 10, 20.0, threads)
         cpu = {"value": rate, "unit": "node-steps/s", "cores": threads, "kind": "port",
-               "sample": f"first 8 fibers of the batch ({sub.n_nodes} nodes) x 15 ms ({n_ref} Strang steps), "
+               "sample": f"first 10 fibers of the batch ({sub.n_nodes} nodes) x 20 ms ({n_ref} Strang steps), "
                          f"{cpu_s:.1f} s"}
         acc = {}
         for name, method, prec in (("fp32_fused", "fused", "fp32"), ("fp64_split", "split", "fp64")):
