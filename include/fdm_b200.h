@@ -229,6 +229,19 @@ int fdm_compat_configure(int model, int n_fibers, int n_instances_per_fiber, int
                          int firing_rows, int firing_cols, int n_jitter_per_fiber, int n_algebraics_for_transfer,
                          int n_states_for_transfer, int diffusion_scheme, int approximate_exponential_function,
                          int reaction_precision, int method);
+/* The CellmlAdapter's generic right-hand side (the non-fast nested solver path), structure of arrays
+ * var[index * n_instances + i] as the reference's generated "gpu" source (04_generator_gpu.cpp:13-113):
+ * states[n_states * n], parameters[n_parameters * n] (the variant's parameter slots) in; rates[n_states * n]
+ * and algebraics[n_algebraics * n] (may be NULL) out.  Device pointers, on stream (a cudaStream_t, NULL:
+ * the legacy default stream). */
+int fdm_cellml_rhs_device(int model, int approximate_exponential_function, int64_t n_instances, double t,
+                          const double *states, const double *parameters, double *rates, double *algebraics,
+                          void *stream);
+/* the reference's generated entry point with its signature (04_generator_gpu.cpp:25-26), host arrays, sized by a
+ * preceding fdm_cellml_rhs_configure (the reference bakes n_instances into the source); process-wide */
+int fdm_cellml_rhs_configure(int model, int64_t n_instances, int approximate_exponential_function, int device);
+void computeCellMLRightHandSide(void *context, double t, double *states, double *rates, double *algebraics,
+                                double *parameters);
 /* fast_monodomain_solver_gpu.tpp:361-365 */
 void initializeArrays(const double *statesOneInstance, const int *algebraicsForTransferIndices,
                       const int *statesForTransferIndices, const char *firingEvents,

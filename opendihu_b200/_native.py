@@ -32,6 +32,7 @@ EXPORTED = [
     "fdm_diffusion_solve_noalloc", "fdm_compat_configure", "fdm_compat_release", "fdm_adjoint_forward",
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
     "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes", "fdm_get_equilibrium_state",
+    "fdm_cellml_rhs_device", "fdm_cellml_rhs_configure",
 ]
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
@@ -114,6 +115,9 @@ def lib() -> C.CDLL:
         "fdm_select_gate_codes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, i64, i32, i32]),
         "fdm_set_gate_codes": (C.c_int, [P, i32]),
         "fdm_get_equilibrium_state": (C.c_int, [P, i64, u8, i32]),
+        "fdm_cellml_rhs_device": (C.c_int, [C.c_int, C.c_int, C.c_int64, C.c_double, P, P, P, P, P]),
+        "fdm_cellml_rhs_configure": (C.c_int, [C.c_int, C.c_int64, C.c_int, C.c_int]),
+        "computeCellMLRightHandSide": (None, [P, C.c_double, d, d, d, d]),
         "fdm_compat_release": (C.c_int, []),
         "initializeArrays": (None, [d, i32, i32, C.c_char_p, d, i32, i32, d, d, d, d]),
         "computeMonodomain": (None, [C.POINTER(C.c_float), d, d, C.POINTER(C.c_float), C.c_double, C.c_double,

@@ -2078,6 +2078,110 @@ Compat g_compat;
 std::mutex g_compat_mu;
 } // namespace
 
+// ---------------------------------------------------------------------------------------------
+// the CellmlAdapter's generic right-hand side (04_generator_gpu.cpp:13-113)
+// ---------------------------------------------------------------------------------------------
+extern "C" int fdm_cellml_rhs_device(int model, int approximate_exponential_function, int64_t n_instances, double t,
+                                     const double* states, const double* parameters, double* rates,
+                                     double* algebraics, void* stream)
+{
+  const ModelDesc* m = model_desc(model);
+  if (!m || n_instances < 0 || (n_instances > 0 && (!states || !rates || (m->n_parameters > 0 && !parameters))))
+    return fail(nullptr, FDM_ERR_ARG, "fdm_cellml_rhs_device: bad argument");
+  const cudaError_t e = launch_cellml_rhs(model, approximate_exponential_function ? MATH_APPROX : MATH_EXACT,
+                                          n_instances, t, states, parameters, rates, algebraics,
+                                          (cudaStream_t)stream);
+  if (e != cudaSuccess)
+    return fail(nullptr, FDM_ERR_CUDA, std::string("fdm_cellml_rhs_device: ") + cudaGetErrorString(e));
+  return FDM_OK;
+}
+
+namespace {
+struct CellmlRhs {
+  int model = -1, approx = 0, device = 0;
+  int64_t n = 0;
+  double *states = nullptr, *params = nullptr, *rates = nullptr, *alg = nullptr;
+  cudaStream_t stream = nullptr;
+  void release()
+  {
+    for (double* p : {states, params, rates, alg})
+      if (p)
+        cudaFree(p);
+    states = params = rates = alg = nullptr;
+    if (stream)
+      cudaStreamDestroy(stream);
+    stream = nullptr;
+    model = -1;
+  }
+};
+CellmlRhs g_rhs;
+std::mutex g_rhs_mu;
+} // namespace
+
+extern "C" int fdm_cellml_rhs_configure(int model, int64_t n_instances, int approximate_exponential_function,
+                                        int device)
+{
+  std::lock_guard<std::mutex> lock(g_rhs_mu);
+  const ModelDesc* m = model_desc(model);
+  if (!m || n_instances < 0)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_cellml_rhs_configure: bad argument");
+  if (cudaSetDevice(device) != cudaSuccess)
+    return fail(nullptr, FDM_ERR_NO_DEVICE, "fdm_cellml_rhs_configure: no such CUDA device");
+  g_rhs.release();
+  const size_t n = (size_t)std::max<int64_t>(n_instances, 1);
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&g_rhs.states, sizeof(double) * n * m->n_states);
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&g_rhs.params, sizeof(double) * n * std::max(m->n_parameters, 1));
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&g_rhs.rates, sizeof(double) * n * m->n_states);
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&g_rhs.alg, sizeof(double) * n * std::max(m->n_algebraics, 1));
+  if (e == cudaSuccess)
+    e = cudaStreamCreateWithFlags(&g_rhs.stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    g_rhs.release();
+    return fail(nullptr, FDM_ERR_CUDA, std::string("fdm_cellml_rhs_configure: ") + cudaGetErrorString(e));
+  }
+  g_rhs.model = model;
+  g_rhs.n = n_instances;
+  g_rhs.approx = approximate_exponential_function;
+  g_rhs.device = device;
+  return FDM_OK;
+}
+
+// host arrays in and out, as the reference's OpenMP-offload code maps them (map(to: states, parameters)
+// map(from: rates, algebraics)); a failure is reported through fdm_last_error(NULL) and leaves rates untouched
+extern "C" void computeCellMLRightHandSide(void* context, double t, double* states, double* rates, double* algebraics,
+                                           double* parameters)
+{
+  (void)context;
+  std::lock_guard<std::mutex> lock(g_rhs_mu);
+  if (g_rhs.model < 0 || !states || !rates) {
+    fail(nullptr, FDM_ERR_ARG, "computeCellMLRightHandSide: call fdm_cellml_rhs_configure first");
+    return;
+  }
+  const ModelDesc* m = model_desc(g_rhs.model);
+  const int64_t n = g_rhs.n;
+  cudaSetDevice(g_rhs.device);
+  cudaStream_t st = g_rhs.stream;
+  cudaError_t e = cudaMemcpyAsync(g_rhs.states, states, sizeof(double) * n * m->n_states, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && m->n_parameters > 0 && parameters)
+    e = cudaMemcpyAsync(g_rhs.params, parameters, sizeof(double) * n * m->n_parameters, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = launch_cellml_rhs(g_rhs.model, g_rhs.approx ? MATH_APPROX : MATH_EXACT, n, t, g_rhs.states, g_rhs.params,
+                          g_rhs.rates, algebraics ? g_rhs.alg : nullptr, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(rates, g_rhs.rates, sizeof(double) * n * m->n_states, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && algebraics && m->n_algebraics > 0)
+    e = cudaMemcpyAsync(algebraics, g_rhs.alg, sizeof(double) * n * m->n_algebraics, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess)
+    fail(nullptr, FDM_ERR_CUDA, std::string("computeCellMLRightHandSide: ") + cudaGetErrorString(e));
+}
+
 extern "C" int fdm_compat_configure(int model, int n_fibers, int n_instances_per_fiber, int n_parameters_per_instance,
                                     int firing_rows, int firing_cols, int n_jitter_per_fiber,
                                     int n_algebraics_for_transfer, int n_states_for_transfer, int diffusion_scheme,

@@ -48,6 +48,9 @@ cudaError_t launch_adjoint_diffusion(int n_fibers, const int64_t* fiber_offsets,
                                      const double* coef, int64_t stride, double* lam, const double* u, const double* x,
                                      int implicit_euler, double* grad_prefactor, double* scratch, double* mu,
                                      int64_t max_fiber_len, cudaStream_t s);
+// the CellmlAdapter's generic right-hand side on device arrays (SoA, index * n + instance)
+cudaError_t launch_cellml_rhs(int model, MathKind mk, int64_t n, double t, const double* states, const double* params,
+                              double* rates, double* algebraics, cudaStream_t s);
 // counts non-finite entries of x[0..n) into *count (device int, must be zeroed by the caller)
 cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t s);
 

@@ -308,6 +308,38 @@ __device__ __forceinline__ void normalize_pair(fdm_f2& S, fdm_f2& L)
   S = t;
 }
 
+// the CellmlAdapter's generic right-hand side: one thread per instance, SoA var[index * n + i]
+template<class Model, class Math>
+__global__ void __launch_bounds__(128) cellml_rhs_kernel(int64_t n, double t, const double* __restrict__ states,
+                                                        const double* __restrict__ params, double* __restrict__ rates,
+                                                        double* __restrict__ algebraics)
+{
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  constexpr int NS = Model::nStates;
+  constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
+  double y[NS], r[NS], P[NP], alg[Model::nAlgebraics];
+#pragma unroll
+  for (int k = 0; k < Model::nAlgebraics; k++)
+    alg[k] = 0.0; // algebraics replaced by parameters are not assigned
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    y[s] = states[s * n + i];
+#pragma unroll
+  for (int q = 0; q < Model::nParameters; q++)
+    P[q] = params[q * n + i];
+  Model::template rates<double, Math>(t, y, P, r, alg);
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    rates[s * n + i] = r[s];
+  if (algebraics) {
+#pragma unroll
+    for (int k = 0; k < Model::nAlgebraics; k++)
+      algebraics[k * n + i] = alg[k];
+  }
+}
+
 // algebraicsForTransfer: copy the requested entries (selected at run time) without dynamic
 // register indexing
 template<class Model, class RR>

@@ -55,6 +55,31 @@ cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionA
   }
 }
 
+template<class Model>
+static cudaError_t cellml_rhs_model(MathKind mk, int64_t n, double t, const double* st, const double* p, double* r,
+                                    double* alg, cudaStream_t s)
+{
+  const int T = 128;
+  const unsigned blocks = (unsigned)((n + T - 1) / T);
+  if (mk == MATH_EXACT)
+    cellml_rhs_kernel<Model, fdm_math_exact><<<blocks, T, 0, s>>>(n, t, st, p, r, alg);
+  else
+    cellml_rhs_kernel<Model, fdm_math_approx><<<blocks, T, 0, s>>>(n, t, st, p, r, alg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cellml_rhs(int model, MathKind mk, int64_t n, double t, const double* states, const double* params,
+                              double* rates, double* algebraics, cudaStream_t s)
+{
+  if (n == 0)
+    return cudaSuccess;
+  switch (model) {
+  case 0: return cellml_rhs_model<HH>(mk, n, t, states, params, rates, algebraics, s);
+  case 1: return cellml_rhs_model<SH>(mk, n, t, states, params, rates, algebraics, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s)
 {
   if (a.n_fibers == 0)

@@ -16,7 +16,7 @@ def declared_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(fdm_[a-z0-9_]+)\s*\(", text)) | set(
-        re.findall(r"\b(initializeArrays|computeMonodomain)\s*\(", text)))
+        re.findall(r"\b(initializeArrays|computeMonodomain|computeCellMLRightHandSide)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():
