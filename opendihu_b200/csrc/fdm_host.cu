@@ -714,8 +714,10 @@ static cudaError_t ensure_stage(fdm_solver* s, size_t bytes)
 // SoA host doubles -> device (Vm in FP64, other states in the reaction precision)
 extern "C" int fdm_set_states(fdm_solver* s, const double* states)
 {
-  if (!s || !states)
+  if (!s || (!states && s->n_nodes > 0))
     return fail(s, FDM_ERR_ARG, "fdm_set_states: bad argument");
+  if (s->n_nodes == 0)
+    return FDM_OK;
   FDM_BIND(s);
   const int NS = s->model->n_states;
   const size_t N = (size_t)s->n_nodes;
@@ -753,8 +755,10 @@ extern "C" int fdm_set_states(fdm_solver* s, const double* states)
 
 extern "C" int fdm_get_states(fdm_solver* s, double* states)
 {
-  if (!s || !states)
+  if (!s || (!states && s->n_nodes > 0))
     return fail(s, FDM_ERR_ARG, "fdm_get_states: bad argument");
+  if (s->n_nodes == 0)
+    return FDM_OK;
   FDM_BIND(s);
   const int NS = s->model->n_states;
   const size_t N = (size_t)s->n_nodes;
@@ -793,8 +797,10 @@ extern "C" int fdm_get_states(fdm_solver* s, double* states)
 
 extern "C" int fdm_get_vm(fdm_solver* s, double* vm)
 {
-  if (!s || !vm)
+  if (!s || (!vm && s->n_nodes > 0))
     return fail(s, FDM_ERR_ARG, "fdm_get_vm: bad argument");
+  if (s->n_nodes == 0)
+    return FDM_OK;
   FDM_BIND(s);
   if (s->n_nodes == 0)
     return FDM_OK;
@@ -805,8 +811,10 @@ extern "C" int fdm_get_vm(fdm_solver* s, double* vm)
 
 extern "C" int fdm_set_parameters(fdm_solver* s, const double* parameters)
 {
-  if (!s || !parameters)
+  if (!s || (!parameters && s->n_nodes > 0))
     return fail(s, FDM_ERR_ARG, "fdm_set_parameters: bad argument");
+  if (s->n_nodes == 0)
+    return FDM_OK;
   FDM_BIND(s);
   const int NP = s->model->n_parameters;
   const size_t n = (size_t)NP * s->n_nodes;
@@ -831,8 +839,10 @@ extern "C" int fdm_set_parameters(fdm_solver* s, const double* parameters)
 
 extern "C" int fdm_get_parameters(fdm_solver* s, double* parameters)
 {
-  if (!s || !parameters)
+  if (!s || (!parameters && s->n_nodes > 0))
     return fail(s, FDM_ERR_ARG, "fdm_get_parameters: bad argument");
+  if (s->n_nodes == 0)
+    return FDM_OK;
   FDM_BIND(s);
   const size_t n = (size_t)s->model->n_parameters * s->n_nodes;
   if (n == 0)
