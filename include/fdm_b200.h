@@ -90,6 +90,9 @@ typedef struct fdm_config {
                                      630-797): point buffers whose states stop changing are skipped and a rank
                                      whose buffers are all counted inactive skips its diffusion solve; split
                                      method with the vc clamp rule only (0: off, the parity setting) */
+  int cluster_size;               /* fused method: a fiber spread over this many CTAs of one thread-block cluster
+                                     (2..8; HH, exact exponentials, every node computed), for few fibers that
+                                     would leave most SMs idle; 0 = chosen automatically, 1 = off */
 } fdm_config;
 
 /* fills *cfg with the reference's defaults (HH, implicit Euler, FP64 split, vc rule W=4, 20 mV clamp) */
@@ -217,6 +220,11 @@ int fdm_adjoint_timing(const fdm_solver *s, double *backward_ms);
 
 /* number of the fused-kernel shapes built into the library and their (threads, nodes per thread) */
 int fdm_fused_shapes(int *threads, int *nodes_per_thread, int capacity);
+/* the same for the cluster mode of the fused kernel (a fiber spread over up to 8 CTAs of one cluster) */
+int fdm_fused_cluster_shapes(int *threads, int *nodes_per_thread, int capacity);
+/* the fused launch fdm_set_fibers chose: CTA size, nodes per thread, CTAs per fiber (1: bins of whole
+ * fibers, > 1: cluster mode), number of CTAs */
+int fdm_fused_layout(const fdm_solver *s, int *threads, int *nodes_per_thread, int *cluster_size, int *n_blocks);
 
 /* ---- compatibility export of the reference's generated-library ABI ---------------------------------
  * The reference's FastMonodomainSolver with optimizationType "gpu" dlopens a library and binds

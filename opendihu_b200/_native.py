@@ -32,7 +32,7 @@ EXPORTED = [
     "fdm_diffusion_solve_noalloc", "fdm_compat_configure", "fdm_compat_release", "fdm_adjoint_forward",
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
     "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes", "fdm_get_equilibrium_state",
-    "fdm_cellml_rhs_device", "fdm_cellml_rhs_configure",
+    "fdm_cellml_rhs_device", "fdm_cellml_rhs_configure", "fdm_fused_cluster_shapes", "fdm_fused_layout",
 ]
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
@@ -56,6 +56,7 @@ class Config(C.Structure):
         ("steps_per_launch", C.c_int), ("threads_per_block", C.c_int), ("nodes_per_thread", C.c_int),
         ("check_nan", C.c_int), ("profile", C.c_int), ("device", C.c_int), ("use_graph", C.c_int),
         ("only_compute_if_stimulated", C.c_int), ("skip_close_to_equilibrium", C.c_int),
+        ("cluster_size", C.c_int),
     ]
 
 
@@ -102,6 +103,8 @@ def lib() -> C.CDLL:
         "fdm_checkpoint_save": (C.c_int, [P]),
         "fdm_checkpoint_restore": (C.c_int, [P]),
         "fdm_fused_shapes": (C.c_int, [i32, i32, C.c_int]),
+        "fdm_fused_cluster_shapes": (C.c_int, [i32, i32, C.c_int]),
+        "fdm_fused_layout": (C.c_int, [P, i32, i32, i32, i32]),
         "fdm_diffusion_solve": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_diffusion_solve_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_compat_configure": (C.c_int, [C.c_int] * 13),
@@ -156,10 +159,12 @@ def model_info(model: int):
     return ns.value, na.value, npar.value, init[:ns.value].copy(), defaults[:npar.value].copy()
 
 
-def fused_shapes():
+def fused_shapes(cluster: bool = False):
+    """(threads, nodes per thread) of the built fused-kernel shapes (``cluster``: of its cluster mode)."""
     t = np.zeros(64, np.int32)
     m = np.zeros(64, np.int32)
-    n = lib().fdm_fused_shapes(ptr(t, C.c_int), ptr(m, C.c_int), 64)
+    fn = lib().fdm_fused_cluster_shapes if cluster else lib().fdm_fused_shapes
+    n = fn(ptr(t, C.c_int), ptr(m, C.c_int), 64)
     return [(int(t[i]), int(m[i])) for i in range(n)]
 
 

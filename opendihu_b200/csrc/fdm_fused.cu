@@ -19,6 +19,30 @@ int fused_shapes(FusedShape* out, int capacity)
   return n;
 }
 
+static const FusedShape g_cluster_shapes[] = {
+#define FDM_SHAPE_ENTRY(T, M) {T, M},
+  FDM_CLUSTER_SHAPES(FDM_SHAPE_ENTRY)
+#undef FDM_SHAPE_ENTRY
+};
+
+int cluster_shapes(FusedShape* out, int capacity)
+{
+  const int n = (int)(sizeof(g_cluster_shapes) / sizeof(g_cluster_shapes[0]));
+  for (int i = 0; i < n && i < capacity; i++)
+    out[i] = g_cluster_shapes[i];
+  return n;
+}
+
+cudaError_t launch_fused_cluster_hh_f32(int shape, int csize, const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_cluster_hh_f64(int shape, int csize, const FusedArgs& a, cudaStream_t s);
+
+cudaError_t launch_fused_cluster(int model, RealKind rk, int shape, int csize, const FusedArgs& a, cudaStream_t s)
+{
+  if (model != 0 || csize < 1 || csize > FDM_MAX_CLUSTER)
+    return cudaErrorInvalidValue;
+  return rk == REAL_F64 ? launch_fused_cluster_hh_f64(shape, csize, a, s) : launch_fused_cluster_hh_f32(shape, csize, a, s);
+}
+
 cudaError_t launch_fused(int model, RealKind rk, MathKind mk, int shape, const FusedArgs& a, cudaStream_t s)
 {
   if (model != 0)

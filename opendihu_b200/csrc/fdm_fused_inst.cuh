@@ -40,7 +40,7 @@ static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s)
   constexpr size_t smem = fused_smem_bytes<Model, RR, Math, T, M>();
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(fused_kernel<Model, RR, Math, T, M, GATE>,
+    cudaError_t e = cudaFuncSetAttribute(fused_kernel<Model, RR, Math, T, M, GATE, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
       return e;
@@ -48,7 +48,7 @@ static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s)
   }
   if (a.n_bins == 0)
     return cudaSuccess;
-  fused_kernel<Model, RR, Math, T, M, GATE><<<a.n_bins, T, smem, s>>>(a);
+  fused_kernel<Model, RR, Math, T, M, GATE, false><<<a.n_bins, T, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -62,6 +62,49 @@ static cudaError_t fused_shape(int shape, const FusedArgs& a, cudaStream_t s)
   k++;
   FDM_FUSED_SHAPES(FDM_SHAPE_CASE)
 #undef FDM_SHAPE_CASE
+  return cudaErrorInvalidValue;
+}
+
+// cluster mode (one fiber per thread-block cluster of csize CTAs; FDM_CLUSTER_SHAPES in fdm_internal.h)
+template<class Model, class RR, class Math, int T, int M>
+static cudaError_t fused_cluster_one(const FusedArgs& a, int csize, cudaStream_t s)
+{
+  constexpr size_t smem = fused_smem_bytes<Model, RR, Math, T, M>();
+  auto kernel = fused_kernel<Model, RR, Math, T, M, false, true>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return e;
+    attr_set = true;
+  }
+  if (a.n_bins == 0)
+    return cudaSuccess;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(a.n_bins * csize), 1, 1);
+  cfg.blockDim = dim3(T, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)csize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
+template<class Model, class RR, class Math>
+static cudaError_t fused_cluster_shape(int shape, int csize, const FusedArgs& a, cudaStream_t s)
+{
+  int k = 0;
+#define FDM_CLUSTER_CASE(T, M)                                   \
+  if (shape == k)                                                \
+    return fused_cluster_one<Model, RR, Math, T, M>(a, csize, s); \
+  k++;
+  FDM_CLUSTER_SHAPES(FDM_CLUSTER_CASE)
+#undef FDM_CLUSTER_CASE
   return cudaErrorInvalidValue;
 }
 

@@ -106,7 +106,8 @@ struct fdm_solver {
   int64_t max_fiber_len = 0;
 
   // fused bins
-  int shape = -1;
+  int shape = -1;    // index into fused_shapes, or into cluster_shapes when cluster > 1
+  int cluster = 1;   // CTAs per fiber (thread-block cluster mode when > 1)
   int n_bins = 0;
   std::vector<int> bin_start, bin_fibers;
 
@@ -343,6 +344,40 @@ extern "C" int fdm_model_info(int model, int* n_states, int* n_algebraics, int* 
   return FDM_OK;
 }
 
+extern "C" int fdm_fused_cluster_shapes(int* threads, int* nodes_per_thread, int capacity)
+{
+  FusedShape sh[64];
+  const int n = cluster_shapes(sh, 64);
+  for (int i = 0; i < n && i < capacity; i++) {
+    if (threads)
+      threads[i] = sh[i].threads;
+    if (nodes_per_thread)
+      nodes_per_thread[i] = sh[i].nodes_per_thread;
+  }
+  return n;
+}
+
+extern "C" int fdm_fused_layout(const fdm_solver* s, int* threads, int* nodes_per_thread, int* cluster_size,
+                                int* n_blocks)
+{
+  if (!s || s->cfg.method != FDM_METHOD_FUSED || s->shape < 0)
+    return fail(const_cast<fdm_solver*>(s), FDM_ERR_ARG, "fdm_fused_layout: no fused launch set up");
+  FusedShape sh[64];
+  if (s->cluster > 1)
+    cluster_shapes(sh, 64);
+  else
+    fused_shapes(sh, 64);
+  if (threads)
+    *threads = sh[s->shape].threads;
+  if (nodes_per_thread)
+    *nodes_per_thread = sh[s->shape].nodes_per_thread;
+  if (cluster_size)
+    *cluster_size = s->cluster;
+  if (n_blocks)
+    *n_blocks = s->n_bins * s->cluster;
+  return FDM_OK;
+}
+
 extern "C" int fdm_fused_shapes(int* threads, int* nodes_per_thread, int capacity)
 {
   FusedShape sh[64];
@@ -383,6 +418,13 @@ extern "C" int fdm_create(const fdm_config* cfg, fdm_solver** out)
     return fail(nullptr, FDM_ERR_ARG, "fdm_create: stimulus_parameter out of range");
   if (!(cfg->dt_repeated_call > 0) || !(cfg->dt_splitting > 0) || !(cfg->dt_0d > 0) || !(cfg->dt_1d > 0))
     return fail(nullptr, FDM_ERR_ARG, "fdm_create: time step widths must be positive");
+  if (cfg->cluster_size < 0 || cfg->cluster_size > FDM_MAX_CLUSTER)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_create: cluster_size must be in [0, 8]");
+  if (cfg->cluster_size >= 2 &&
+      (cfg->method != FDM_METHOD_FUSED || cfg->model != FDM_MODEL_HODGKIN_HUXLEY_1952 ||
+       cfg->approximate_exponential_function || cfg->only_compute_if_stimulated))
+    return fail(nullptr, FDM_ERR_UNSUPPORTED, "fdm_create: cluster mode needs FDM_METHOD_FUSED, the HH model, exact "
+                                              "exponentials and only_compute_if_stimulated off");
   if (cfg->skip_close_to_equilibrium &&
       (cfg->method != FDM_METHOD_SPLIT || cfg->clamp_rule != FDM_CLAMP_VC_LANES))
     return fail(nullptr, FDM_ERR_UNSUPPORTED, "fdm_create: the equilibrium skip (point buffers of the vc path) "
@@ -550,6 +592,53 @@ static int choose_shape(fdm_solver* s)
   return best;
 }
 
+// Cluster mode: a fiber spread over the CTAs of one thread-block cluster. Chosen automatically when the
+// regular packing gives fewer CTAs than half the SMs (or no regular shape holds the longest fiber); returns
+// the index into cluster_shapes and the CTAs per fiber, or -1 (regular packing), or -2 (a forced cluster
+// size or shape that cannot hold the longest fiber).
+static int choose_cluster(fdm_solver* s, int regular_bins, int* csize_out)
+{
+  const fdm_config& c = s->cfg;
+  const bool forced = c.cluster_size >= 2;
+  const bool shape_forced = c.threads_per_block > 0 || c.nodes_per_thread > 0;
+  if (c.cluster_size == 1 || c.method != FDM_METHOD_FUSED || c.model != FDM_MODEL_HODGKIN_HUXLEY_1952 ||
+      c.approximate_exponential_function || c.only_compute_if_stimulated)
+    return -1;
+  int n_sm = 148;
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, c.device);
+  if (!forced && (shape_forced || (regular_bins > 0 && 2 * regular_bins > n_sm)))
+    return -1;
+  FusedShape sh[64];
+  const int n = cluster_shapes(sh, 64);
+  int best = -1, best_cs = 0;
+  int64_t best_key = 0;
+  for (int i = 0; i < n; i++) {
+    if (shape_forced && (sh[i].threads != c.threads_per_block || sh[i].nodes_per_thread != c.nodes_per_thread))
+      continue;
+    const int64_t cap = (int64_t)sh[i].threads * sh[i].nodes_per_thread;
+    int64_t cs = (s->max_fiber_len + cap - 1) / cap;
+    if (forced) {
+      if (cs > c.cluster_size)
+        continue;
+      cs = c.cluster_size;
+    } else if (cs < 2 || cs > FDM_MAX_CLUSTER) {
+      continue;
+    }
+    // prefer: all CTAs resident at once, fewer nodes per thread, then more CTAs
+    const int64_t ctas = (int64_t)s->n_fibers * cs;
+    const int64_t key = (ctas <= n_sm ? 0 : (int64_t)1 << 40) + ((int64_t)sh[i].nodes_per_thread << 20) - ctas;
+    if (best < 0 || key < best_key) {
+      best = i;
+      best_cs = (int)cs;
+      best_key = key;
+    }
+  }
+  if (best < 0)
+    return forced ? -2 : -1;
+  *csize_out = best_cs;
+  return best;
+}
+
 static int upload_clamp(fdm_solver* s);
 static int upload_gate(fdm_solver* s);
 static int eq_copy_pad_params(fdm_solver* s);
@@ -635,14 +724,33 @@ extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_
   }
 
   // fused bins
+  s->cluster = 1;
   if (s->cfg.method == FDM_METHOD_FUSED && n_fibers > 0) {
-    s->shape = choose_shape(s);
-    if (s->shape < 0)
+    const int regular = s->cfg.cluster_size >= 2 ? -1 : choose_shape(s);
+    if (regular >= 0) {
+      FusedShape sh[64];
+      fused_shapes(sh, 64);
+      pack_bins(s->off, (int64_t)sh[regular].threads * sh[regular].nodes_per_thread, s->bin_start, s->bin_fibers);
+    }
+    int csize = 1;
+    const int cshape = choose_cluster(s, regular >= 0 ? (int)s->bin_start.size() - 1 : 0, &csize);
+    if (cshape >= 0) {
+      // one fiber per cluster
+      s->shape = cshape;
+      s->cluster = csize;
+      s->bin_start.resize(n_fibers + 1);
+      s->bin_fibers.resize(n_fibers);
+      for (int f = 0; f <= n_fibers; f++)
+        s->bin_start[f] = f;
+      for (int f = 0; f < n_fibers; f++)
+        s->bin_fibers[f] = f;
+    } else if (regular >= 0 && cshape == -1) {
+      s->shape = regular;
+    } else {
       return fail(s, FDM_ERR_UNSUPPORTED, "fdm_set_fibers: no fused kernel shape holds the longest fiber (" +
-                                              std::to_string(maxlen) + " nodes) with the requested threads/nodes");
-    FusedShape sh[64];
-    fused_shapes(sh, 64);
-    pack_bins(s->off, (int64_t)sh[s->shape].threads * sh[s->shape].nodes_per_thread, s->bin_start, s->bin_fibers);
+                                              std::to_string(maxlen) +
+                                              " nodes) with the requested threads/nodes/cluster size");
+    }
     s->n_bins = (int)s->bin_start.size() - 1;
     FDM_CUDA(s->bin_start_d.alloc(s->bin_start.size()));
     FDM_CUDA(s->bin_fibers_d.alloc(std::max<size_t>(s->bin_fibers.size(), 1)));
@@ -1609,7 +1717,10 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
       e1 = next_event(s);
       FDM_CUDA(cudaEventRecord(e0, s->stream));
     }
-    FDM_CUDA(launch_fused(s->cfg.model, rk, mk, s->shape, fa, s->stream));
+    if (s->cluster > 1)
+      FDM_CUDA(launch_fused_cluster(s->cfg.model, rk, s->shape, s->cluster, fa, s->stream));
+    else
+      FDM_CUDA(launch_fused(s->cfg.model, rk, mk, s->shape, fa, s->stream));
     s->launches++;
     if (prof)
       FDM_CUDA(cudaEventRecord(e1, s->stream));

@@ -59,6 +59,16 @@ struct FusedShape {
   int threads, nodes_per_thread;
 };
 int fused_shapes(FusedShape* out, int capacity);
+// cluster mode shapes (threads per CTA, nodes per thread); a fiber spans up to 8 CTAs of one cluster
+#define FDM_CLUSTER_SHAPES(X) \
+  X(128, 2)                   \
+  X(256, 2)                   \
+  X(512, 2)                   \
+  X(256, 4)
+constexpr int FDM_MAX_CLUSTER = 8;
+int cluster_shapes(FusedShape* out, int capacity);
+// one fiber per cluster of csize CTAs (FP32/FP64 reaction with exact exponentials, no onlyComputeIfHasBeenStimulated)
+cudaError_t launch_fused_cluster(int model, RealKind rk, int shape, int csize, const FusedArgs& a, cudaStream_t s);
 // shape index into fused_shapes(); returns cudaErrorInvalidValue if the combination is not built
 cudaError_t launch_fused(int model, RealKind rk, MathKind mk, int shape, const FusedArgs& a, cudaStream_t s);
 

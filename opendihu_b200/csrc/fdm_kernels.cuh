@@ -18,9 +18,13 @@
 
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "fdm_math.cuh"
 
 namespace fdm {
+
+namespace cg = cooperative_groups;
 
 // --------------------------------------------------------------------------------------------
 // exact (never contracted) FP64 arithmetic for time values, so that the discrete stimulation
@@ -944,9 +948,11 @@ struct FusedArgs {
   int gate_stride;
 };
 
-// block-wide exclusive scan of affine maps in thread order (REVERSE: from the last thread down)
+// block-wide exclusive scan of affine maps in thread order (REVERSE: from the last thread down): returns the
+// composition of the maps of the threads before this one in scan order, and in *total (if given) the
+// composition of all threads' maps; sF/sG hold 2 * (T/32) + 1 doubles each
 template<int T, bool REVERSE>
-__device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, double* sG)
+__device__ __forceinline__ Affine block_scan_map(Affine acc, double* sF, double* sG, Affine* total)
 {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -1004,11 +1010,22 @@ __device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, do
       sF[NW + w] = pF;
       sG[NW + w] = pG;
     }
+    if (lane == NW - 1) {
+      sF[2 * NW] = v.F;
+      sG[2 * NW] = v.G;
+    }
   }
   __syncthreads();
   const Affine wp{sF[NW + warp], sG[NW + warp]};
-  const Affine ex = compose(wp, Affine{exF, exG});
-  return ex.G; // applied to the zero entering the first node of the bin
+  if (total)
+    *total = Affine{sF[2 * NW], sG[2 * NW]};
+  return compose(wp, Affine{exF, exG});
+}
+
+template<int T, bool REVERSE>
+__device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, double* sG)
+{
+  return block_scan_map<T, REVERSE>(acc, sF, sG, nullptr).G; // applied to the zero entering the first node
 }
 
 // Adjoint of one diffusion solve (see adjoint_diffusion_warp_kernel for the algebra) with one CTA per
@@ -1022,7 +1039,7 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
     const double* __restrict__ coef, int64_t stride, double* __restrict__ lam, const double* __restrict__ u,
     const double* __restrict__ x, int implicit_euler, double* __restrict__ grad_prefactor)
 {
-  __shared__ double sF[2 * (T / 32)], sG[2 * (T / 32)];
+  __shared__ double sF[2 * (T / 32) + 1], sG[2 * (T / 32) + 1];
   __shared__ double sfirst[T], slast[T], sred[T / 32];
   const int f = blockIdx.x;
   const int tid = threadIdx.x;
@@ -1117,8 +1134,12 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
 }
 
 // GATE: onlyComputeIfHasBeenStimulated is on (a.gate is set); a separate instantiation so that the
-// default path carries none of its per-substep checks
-template<class Model, class RR, class Math, int T, int M, bool GATE>
+// default path carries none of its per-substep checks.
+// CLUSTER: for few fibers (the GPU would be mostly idle with one CTA per bin), one fiber per thread-block
+// cluster: CTA r of the cluster holds the fiber's nodes [r * T*M, (r+1) * T*M); the CTAs exchange the Vm of
+// their edge nodes and the totals of their scans through distributed shared memory, with three cluster
+// barriers per Strang step (every CTA of a cluster takes every barrier: no CTA returns early).
+template<class Model, class RR, class Math, int T, int M, bool GATE, bool CLUSTER>
 __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 {
   constexpr int NS = Model::nStates;
@@ -1129,9 +1150,9 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   double* sc = smem;
   double* vfirst = sc + 5 * CAP;     // T
   double* vlast = vfirst + T;        // T
-  double* sF = vlast + T;            // 2 * (T/32)
-  double* sG = sF + 2 * (T / 32);    // 2 * (T/32)
-  int* s_cf = (int*)(sG + 2 * (T / 32)); // CAP: clamp fiber of each node (-1: not a junction node)
+  double* sF = vlast + T;            // 2 * (T/32) + 1
+  double* sG = sF + 2 * (T / 32) + 1; // 2 * (T/32) + 1
+  int* s_cf = (int*)(sG + 2 * (T / 32) + 1); // CAP: clamp fiber of each node (-1: not a junction node)
   int* s_ts = s_cf + CAP;                // CAP: trace slot of each node (-1: not traced)
   int* s_gate = s_ts + CAP;              // CAP: gate code of each node (onlyComputeIfHasBeenStimulated)
   // paired FP32 path: the parameters of node pair p of thread tid, parameter k, at (p * NP + k) * T + tid
@@ -1139,24 +1160,82 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   __shared__ int64_t fib_global[FUSED_MAX_FIBERS_PER_BIN];
   __shared__ int fib_local[FUSED_MAX_FIBERS_PER_BIN + 1];
 
+  __shared__ double ctot[4];      // cluster mode: this CTA's forward and backward scan totals (F, G)
+  __shared__ double cpre[2 * 16]; // cluster mode: the other CTAs' totals this CTA composes
   const int tid = threadIdx.x;
-  const int bin = blockIdx.x;
-  if (bin >= a.n_bins)
-    return;
-  // the bin's fibers, concatenated in bin-local node numbering
+  int bin = blockIdx.x, crank = 0, csize = 1;
+  if constexpr (CLUSTER) {
+    cg::cluster_group cl = cg::this_cluster();
+    crank = (int)cl.block_rank();
+    csize = (int)cl.num_blocks();
+    bin = blockIdx.x / csize;
+  } else {
+    if (bin >= a.n_bins)
+      return;
+  }
+  // the bin's fibers, concatenated in bin-local node numbering (cluster mode: this CTA's part of one fiber)
   const int f0 = a.bin_fiber_start[bin];
-  const int nf = a.bin_fiber_start[bin + 1] - f0;
+  const int nf = CLUSTER ? 1 : a.bin_fiber_start[bin + 1] - f0;
   if (tid == 0) {
-    int loc = 0;
-    for (int k = 0; k < nf; k++) {
-      const int fib = a.bin_fibers[f0 + k];
-      fib_global[k] = a.fiber_offsets[fib];
-      fib_local[k] = loc;
-      loc += (int)(a.fiber_offsets[fib + 1] - a.fiber_offsets[fib]);
+    if (CLUSTER) {
+      const int fib = a.bin_fibers[f0];
+      const int64_t len = a.fiber_offsets[fib + 1] - a.fiber_offsets[fib];
+      const int64_t lo = (int64_t)crank * CAP;
+      fib_global[0] = a.fiber_offsets[fib] + lo;
+      fib_local[0] = 0;
+      fib_local[1] = (int)max((int64_t)0, min((int64_t)CAP, len - lo));
+    } else {
+      int loc = 0;
+      for (int k = 0; k < nf; k++) {
+        const int fib = a.bin_fibers[f0 + k];
+        fib_global[k] = a.fiber_offsets[fib];
+        fib_local[k] = loc;
+        loc += (int)(a.fiber_offsets[fib + 1] - a.fiber_offsets[fib]);
+      }
+      fib_local[nf] = loc;
     }
-    fib_local[nf] = loc;
   }
   __syncthreads();
+  // cluster mode: barrier over the cluster's CTAs (and of this CTA's threads)
+  auto cluster_sync = [&]() {
+    if constexpr (CLUSTER)
+      cg::this_cluster().sync();
+    else
+      __syncthreads();
+  };
+  // cluster mode: the value entering this thread's first node of a sweep, from the CTA's own scan (ex, total)
+  // and the totals of the CTAs before it in sweep order
+  auto cluster_incoming = [&](Affine ex, Affine total, bool reverse) -> double {
+    if constexpr (!CLUSTER) {
+      (void)total;
+      (void)reverse;
+      return ex.G;
+    } else {
+      cg::cluster_group cl = cg::this_cluster();
+      const int slot = reverse ? 2 : 0;
+      if (tid == 0) {
+        ctot[slot] = total.F;
+        ctot[slot + 1] = total.G;
+      }
+      cl.sync();
+      // thread k < csize fetches CTA k's total (the ranks before this one in sweep order are used)
+      if (tid < csize) {
+        const double* remote = cl.map_shared_rank(ctot, tid);
+        cpre[2 * tid] = remote[slot];
+        cpre[2 * tid + 1] = remote[slot + 1];
+      }
+      __syncthreads();
+      Affine pre{1.0, 0.0};
+      if (!reverse) {
+        for (int k = 0; k < crank; k++)
+          pre = compose(pre, Affine{cpre[2 * k], cpre[2 * k + 1]});
+      } else {
+        for (int k = csize - 1; k > crank; k--)
+          pre = compose(pre, Affine{cpre[2 * k], cpre[2 * k + 1]});
+      }
+      return compose(pre, ex).G;
+    }
+  };
   const int nb = fib_local[nf];
   auto global_node = [&](int q) -> int64_t {
     int k = 0;
@@ -1410,9 +1489,16 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       // ---- diffusion: block-wide tridiagonal solve in FP64 ----
       vfirst[tid] = V[0];
       vlast[tid] = V[M - 1];
-      __syncthreads();
-      const double vprev = tid > 0 ? vlast[tid - 1] : 0.0;
-      const double vnext = tid < T - 1 ? vfirst[tid + 1] : 0.0;
+      cluster_sync();
+      double vprev = tid > 0 ? vlast[tid - 1] : 0.0;
+      double vnext = tid < T - 1 ? vfirst[tid + 1] : 0.0;
+      if constexpr (CLUSTER) {
+        cg::cluster_group cl = cg::this_cluster();
+        if (tid == 0 && crank > 0)
+          vprev = cl.map_shared_rank(vlast, crank - 1)[T - 1];
+        if (tid == T - 1 && crank < csize - 1)
+          vnext = cl.map_shared_rank(vfirst, crank + 1)[0];
+      }
       double d[M];
 #pragma unroll
       for (int j = 0; j < M; j++) {
@@ -1427,7 +1513,9 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         const int q = tid * M + j;
         acc = compose(acc, Affine{sc[0 * CAP + q], d[j]});
       }
-      double dp = block_scan_incoming<T, false>(acc, sF, sG);
+      Affine tot_f;
+      const Affine ex_f = block_scan_map<T, false>(acc, sF, sG, &tot_f);
+      double dp = cluster_incoming(ex_f, tot_f, false);
 #pragma unroll
       for (int j = 0; j < M; j++) {
         const int q = tid * M + j;
@@ -1441,7 +1529,9 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         bacc = compose(bacc, Affine{-sc[1 * CAP + q], d[j]});
       }
       __syncthreads(); // sF/sG reuse
-      double x = block_scan_incoming<T, true>(bacc, sF, sG);
+      Affine tot_b;
+      const Affine ex_b = block_scan_map<T, true>(bacc, sF, sG, &tot_b);
+      double x = cluster_incoming(ex_b, tot_b, true);
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
         const int q = tid * M + j;
@@ -1458,6 +1548,9 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     }
   }
 
+  // cluster mode: no CTA leaves while another may still read its shared memory
+  if constexpr (CLUSTER)
+    cg::this_cluster().sync();
   if constexpr (PAIR) {
 #pragma unroll
     for (int j = 0; j < 2 * MP; j++) {
@@ -1491,7 +1584,7 @@ constexpr size_t fused_smem_bytes()
 {
   constexpr bool PAIR = std::is_same<RR, float>::value && std::is_same<Math, fdm_math_exact>::value;
   constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
-  return sizeof(double) * (5 * T * M + 2 * T + 4 * (T / 32)) + sizeof(int) * 3 * T * M +
+  return sizeof(double) * (5 * T * M + 2 * T + 4 * (T / 32) + 2) + sizeof(int) * 3 * T * M +
          (PAIR ? sizeof(fdm_f2) * (M / 2) * NP * T : 0);
 }
 

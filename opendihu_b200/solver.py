@@ -310,7 +310,7 @@ class FastMonodomainSolver:
     def __init__(self, system: FiberSystem, method: Optional[str] = None, precision: Optional[str] = None,
                  steps_per_launch: int = 0, threads_per_block: int = 0, nodes_per_thread: int = 0,
                  check_nan: bool = True, profile: bool = False, trace_nodes: Sequence[int] = (),
-                 trace_capacity: int = 0, device: int = 0, autotune: bool = False):
+                 trace_capacity: int = 0, device: int = 0, autotune: bool = False, cluster_size: int = 0):
         self.system = system
         self.method = method or getattr(system, "method", "split")
         self.precision = precision or getattr(system, "precision", "fp64")
@@ -323,6 +323,8 @@ class FastMonodomainSolver:
         self.trace_capacity = int(trace_capacity)
         self.device = int(device)
         self.autotune = bool(autotune)
+        #: fused method: CTAs of one thread-block cluster per fiber (0: chosen by the library, 1: off)
+        self.cluster_size = int(cluster_size)
         self.tuning = None
         #: (first_node, count, evaluated) per fiber replacing the clamp selection of fdm_set_stimulation
         #: (set by the sharded solver to keep the selection of the unsharded layout)
@@ -377,6 +379,7 @@ class FastMonodomainSolver:
         cfg.device = self.device
         cfg.only_compute_if_stimulated = int(bool(s.only_compute_if_has_been_stimulated))
         cfg.skip_close_to_equilibrium = int(bool(s.skip_close_to_equilibrium))
+        cfg.cluster_size = int(self.cluster_size)
         h = C.c_void_p()
         N.check(L.fdm_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -582,6 +585,12 @@ class FastMonodomainSolver:
         ev = np.zeros(nf, np.uint8)
         self._call(N.lib().fdm_get_clamp_nodes, N.ptr(first, C.c_int64), N.ptr(cnt, C.c_int), N.ptr(ev, C.c_uint8))
         return first, cnt, ev
+
+    def fused_layout(self) -> Dict[str, int]:
+        """The fused kernel's launch: CTA size, nodes per thread, CTAs per fiber (> 1: cluster mode), CTAs."""
+        t, m, c, b = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self._call(N.lib().fdm_fused_layout, C.byref(t), C.byref(m), C.byref(c), C.byref(b))
+        return {"threads": t.value, "nodes_per_thread": m.value, "cluster_size": c.value, "n_blocks": b.value}
 
     def split_steps(self) -> int:
         return int(N.lib().fdm_split_steps(self._h))

@@ -59,9 +59,15 @@ def test_no_fibers():
         assert slv.states().shape == (4, 0)
 
 
-def test_fiber_longer_than_every_fused_bin_fails_loudly():
+def test_fiber_longer_than_every_fused_launch_fails_loudly():
     longest = max(t * m for t, m in S.N.fused_shapes())
     s = S.uniform_fibers(H.HH, [longest + 1], 0.01, 3.828 / 500, end_time=0.01)
+    with pytest.raises(S.N.FdmError) as e:
+        S.FastMonodomainSolver(H.complete(s.copy()), method="fused", cluster_size=1).initialize()
+    assert e.value.code == S.N.FDM_ERR_UNSUPPORTED
+    # cluster mode holds up to 8 CTAs of its largest shape per fiber
+    longest_cluster = 8 * max(t * m for t, m in S.N.fused_shapes(cluster=True))
+    s = S.uniform_fibers(H.HH, [longest_cluster + 1], 0.01, 3.828 / 500, end_time=0.01)
     with pytest.raises(S.N.FdmError) as e:
         S.FastMonodomainSolver(H.complete(s), method="fused").initialize()
     assert e.value.code == S.N.FDM_ERR_UNSUPPORTED

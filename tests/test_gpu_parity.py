@@ -18,6 +18,10 @@ VM_TOL_FP32 = 0.1
 
 
 def run_gpu(system, method="split", precision="fp64", trace_nodes=(), trace_capacity=0, **kw):
+    # "fused" lets the library choose (cluster mode for few fibers); "fused_bins" keeps bins of whole fibers
+    if method == "fused_bins":
+        method = "fused"
+        kw["cluster_size"] = 1
     H.complete(system)
     with S.FastMonodomainSolver(system, method=method, precision=precision, trace_nodes=trace_nodes,
                                 trace_capacity=trace_capacity, **kw) as slv:
@@ -43,18 +47,18 @@ def small_system(**kw):
     return H.c1_system(n_fibers=3, n_nodes=301, end_time=kw.pop("end_time", 2.0), **kw)
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_fp64_matches_oracle(method):
     st, ref, dv = compare(small_system(), method, "fp64", VM_TOL_FP64, 1e-8)
     assert ref[0].max() > 0  # an action potential happened
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_fp32_reaction_within_01mV(method):
     compare(small_system(), method, "fp32", VM_TOL_FP32, 1e-3)
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_crank_nicolson(method):
     compare(small_system(diffusion_scheme="CrankNicolson"), method, "fp64", VM_TOL_FP64, 1e-8)
 
@@ -65,7 +69,7 @@ def test_approximate_exponential(method):
     compare(small_system(approximate_exponential_function=True), method, "fp32", VM_TOL_FP32, 1e-3)
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_uneven_lengths_center_rule_and_jitter(method):
     rng = np.random.default_rng(3)
     lengths = rng.integers(40, 400, size=7)
@@ -95,7 +99,7 @@ def test_clamp_nodes_match_oracle():
     assert first[0] == 740 and first[1] == 1481 + 739  # the W=4 buffer rule shifts the clamp per fiber
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_current_stimulus_mode(method):
     # the benchmark's 1200 uA/cm^2 current at the junction for 0.1 ms every 10 ms (parameter 0 = I_Stim)
     sysm = small_system(stimulus_mode="current", stimulus_parameter=0, stimulus_value=1200.0)
@@ -103,7 +107,7 @@ def test_current_stimulus_mode(method):
     assert ref[0].max() > 0
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_per_node_parameters_and_prefactor(method):
     sysm = small_system()
     H.complete(sysm)
@@ -115,7 +119,7 @@ def test_per_node_parameters_and_prefactor(method):
     compare(sysm, method, "fp64", VM_TOL_FP64, 1e-8)
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_algebraics_for_transfer(method):
     sysm = small_system(end_time=0.5, algebraics_for_transfer=[0, 4, 8])
     ref, ref_alg, _, _ = H.run_oracle(sysm.copy())
@@ -123,11 +127,12 @@ def test_algebraics_for_transfer(method):
     np.testing.assert_allclose(alg, ref_alg, rtol=1e-9, atol=1e-9)
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_repeated_advances_and_checkpoint(method):
     sysm = small_system(end_time=1.0)
     H.complete(sysm)
-    with S.FastMonodomainSolver(sysm, method=method, steps_per_launch=37) as slv:
+    kw = {"method": "fused", "cluster_size": 1} if method == "fused_bins" else {"method": method}
+    with S.FastMonodomainSolver(sysm, steps_per_launch=37, **kw) as slv:
         slv.setTimeSpan(0.0, 0.4)
         slv.advanceTimeSpan()
         slv.saveFiberDataCheckpoint()
@@ -148,7 +153,7 @@ def test_repeated_advances_and_checkpoint(method):
     assert np.max(np.abs(a[0] - st[0])) <= VM_TOL_FP64
 
 
-@pytest.mark.parametrize("method", ["split", "fused"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
 def test_window_sizes_do_not_change_results(method):
     sysm = small_system(end_time=0.7)
     H.complete(sysm)
@@ -188,7 +193,8 @@ def test_nan_is_reported():
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("method,precision", [("split", "fp64"), ("fused", "fp64"), ("fused", "fp32")])
+@pytest.mark.parametrize("method,precision", [("split", "fp64"), ("fused", "fp64"), ("fused", "fp32"),
+                                              ("fused_bins", "fp64")])
 def test_plain_method_config_10ms(method, precision):
     """16 HH fibers x 1481 nodes, 10 ms: Vm after 10 ms and activation times against the oracle."""
     sysm = H.c1_system(end_time=10.0)

@@ -53,3 +53,20 @@ def test_create_fails_loudly_without_device_or_with_bad_config():
 def test_fused_shapes_listed():
     shapes = N.fused_shapes()
     assert len(shapes) >= 4 and all(t % 32 == 0 and m >= 1 for t, m in shapes)
+    cl = N.fused_shapes(cluster=True)
+    assert len(cl) >= 1 and all(t % 32 == 0 and m >= 1 for t, m in cl)
+
+
+@pytest.mark.parametrize("field,value,code", [
+    ("cluster_size", 9, N.FDM_ERR_ARG), ("cluster_size", -1, N.FDM_ERR_ARG),
+    ("method", 0, N.FDM_ERR_UNSUPPORTED),                             # cluster mode is a fused-kernel mode
+    ("approximate_exponential_function", 1, N.FDM_ERR_UNSUPPORTED),
+    ("only_compute_if_stimulated", 1, N.FDM_ERR_UNSUPPORTED)])
+def test_cluster_mode_config_checked_before_the_device(field, value, code):
+    cfg = N.default_config()
+    cfg.method = 1
+    cfg.cluster_size = 4
+    setattr(cfg, field, value)
+    h = C.c_void_p()
+    assert N.lib().fdm_create(C.byref(cfg), C.byref(h)) == code
+    assert b"cluster" in N.lib().fdm_last_error(None)
