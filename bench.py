@@ -274,7 +274,8 @@ def main():
     if rank == 0 and not args.skip_fp64:
         c1 = WL.plain_hh(end_time=10.0)
         plain_cfg = {"workload": "16 HH fibers x 1481 nodes, implicit Euler, 10 ms"}
-        for name, method, prec in (("fp64_split", "split", "fp64"), ("fp32_fused", "fused", "fp32")):
+        for name, method, prec in (("fp64_split", "split", "fp64"), ("fp64_fused", "fused", "fp64"),
+                                   ("fp32_fused", "fused", "fp32")):
             with S.FastMonodomainSolver(c1.copy(), method=method, precision=prec, device=local) as sv:
                 sv.setTimeSpan(0.0, 1.0)
                 sv.advanceTimeSpan()
@@ -282,6 +283,9 @@ def main():
                 sv.setTimeSpan(1.0, 10.0)
                 sv.advanceTimeSpan()
                 ms = sv.timing()["advance_ms"]
+                if method == "fused":
+                    # few fibers: each fiber spread over the CTAs of a thread-block cluster
+                    plain_cfg["fused_layout"] = sv.fused_layout()
             plain_cfg[name] = c1.n_nodes * 9000 / (ms / 1e3)
 
     # differentiation: adjoint gradient cost relative to one FP64 forward solve (256 HH fibers x 1481 nodes,
