@@ -143,6 +143,10 @@ int fdm_set_clamp_nodes(fdm_solver *s, const int64_t *first_node, const int *cou
  * inactive buffers (n_ranks entries; may be NULL) -- the "computeStateInformation" data of
  * fast_monodomain_solver_communication.tpp:280-290 */
 int fdm_get_equilibrium_state(fdm_solver *s, int64_t *n_buffers, uint8_t *status, int *counter);
+/* "computeStateInformation" per node (the extra transfer slot, communication.tpp:277-290): the status of the
+ * node's point buffer (0 inactive, 1 neighbor_is_active, 2 active; 2 everywhere while the equilibrium skip
+ * is off), -1 on the nodes of a fiber not stimulated yet under onlyComputeIfHasBeenStimulated */
+int fdm_get_compute_state_information(fdm_solver *s, double *out /* [n_nodes] */);
 /* host-only: per node, the code (attributed fiber) * 4 + class that onlyComputeIfHasBeenStimulated uses:
  * class 0/1/2 = the node's point buffer lies before / is / lies after the junction buffer of the fiber it
  * is attributed to (compute.tpp:158-205 processes buffers in order and the junction buffer sets the flag) */

@@ -33,6 +33,7 @@ EXPORTED = [
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
     "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes", "fdm_get_equilibrium_state",
     "fdm_cellml_rhs_device", "fdm_cellml_rhs_configure", "fdm_fused_cluster_shapes", "fdm_fused_layout",
+    "fdm_get_compute_state_information",
 ]
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
@@ -105,6 +106,7 @@ def lib() -> C.CDLL:
         "fdm_fused_shapes": (C.c_int, [i32, i32, C.c_int]),
         "fdm_fused_cluster_shapes": (C.c_int, [i32, i32, C.c_int]),
         "fdm_fused_layout": (C.c_int, [P, i32, i32, i32, i32]),
+        "fdm_get_compute_state_information": (C.c_int, [P, d]),
         "fdm_diffusion_solve": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_diffusion_solve_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_compat_configure": (C.c_int, [C.c_int] * 13),

@@ -1428,6 +1428,38 @@ extern "C" int fdm_get_equilibrium_state(fdm_solver* s, int64_t* n_buffers, uint
   return FDM_OK;
 }
 
+extern "C" int fdm_get_compute_state_information(fdm_solver* s, double* out)
+{
+  if (!s || (!out && s->n_nodes > 0) || !s->stimulation_set)
+    return fail(s, FDM_ERR_ARG, "fdm_get_compute_state_information: call fdm_set_stimulation first; no null array");
+  FDM_BIND(s);
+  const int64_t N = s->n_nodes;
+  if (N == 0)
+    return FDM_OK;
+  // the status of the node's point buffer (2 = active for every buffer while the equilibrium skip is off)
+  if (s->eq.on) {
+    std::vector<int> buf_of(N);
+    std::vector<uint8_t> st(s->eq.n_buffers);
+    FDM_CUDA(cudaMemcpyAsync(buf_of.data(), s->eq.buf_of.p, sizeof(int) * N, cudaMemcpyDeviceToHost, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(st.data(), s->eq.st[0].p, s->eq.n_buffers, cudaMemcpyDeviceToHost, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+    for (int64_t i = 0; i < N; i++)
+      out[i] = (double)st[buf_of[i]];
+  } else {
+    std::fill(out, out + N, 2.0);
+  }
+  // -1 on every node of a fiber that has not been stimulated yet (own fiber, onlyComputeIfHasBeenStimulated)
+  if (s->cfg.only_compute_if_stimulated) {
+    std::vector<uint8_t> hbs(s->n_fibers);
+    FDM_CUDA(cudaMemcpyAsync(hbs.data(), s->hbs.p, s->n_fibers, cudaMemcpyDeviceToHost, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+    for (int f = 0; f < s->n_fibers; f++)
+      if (!hbs[f])
+        std::fill(out + s->off[f], out + s->off[f + 1], -1.0);
+  }
+  return FDM_OK;
+}
+
 extern "C" int fdm_set_gate_codes(fdm_solver* s, const int* codes)
 {
   if (!s || !s->stimulation_set || !codes || !s->cfg.only_compute_if_stimulated)

@@ -18,8 +18,10 @@ import numpy as np
 
 
 def fiber_dict(values: Dict[str, np.ndarray], geometry: Optional[np.ndarray], time_step_no: int,
-               current_time: float, field_name: str = "solution") -> dict:
-    """The dict of one fiber (StructuredDeformable 1D mesh with linear Lagrange basis)."""
+               current_time: float, field_name: str = "solution",
+               additional: Optional[Dict[str, np.ndarray]] = None) -> dict:
+    """The dict of one fiber (StructuredDeformable 1D mesh with linear Lagrange basis); ``additional`` adds
+    one single-component field variable per entry (transferred algebraics, computeStateInformation)."""
     n_nodes = len(next(iter(values.values())))
     if geometry is None:
         geometry = np.zeros((n_nodes, 3))
@@ -33,16 +35,19 @@ def fiber_dict(values: Dict[str, np.ndarray], geometry: Optional[np.ndarray], ti
                                                 for i, c in enumerate("xyz")]},
             {"name": field_name, "components": [{"name": k, "values": np.asarray(v, np.float64).tolist()}
                                                 for k, v in values.items()]},
-        ],
+        ] + [{"name": k, "components": [{"name": "0", "values": np.asarray(v, np.float64).tolist()}]}
+             for k, v in (additional or {}).items()],
         "timeStepNo": int(time_step_no), "currentTime": float(current_time),
     }
 
 
 def write_fibers(filename: str, output_no: int, system, states: np.ndarray, state_names: Sequence[str],
                  states_for_transfer: Sequence[int] = (0,), time_step_no: int = 0, current_time: float = 0.0,
-                 binary: bool = False, fibers: Optional[Sequence[int]] = None) -> list:
+                 binary: bool = False, fibers: Optional[Sequence[int]] = None,
+                 additional: Optional[Dict[str, np.ndarray]] = None) -> list:
     """Write ``<filename>_<fiber>_<output_no:07d>.py`` for the given fibers (default all) with the chosen
-    states; node coordinates are the cumulative element lengths along x.  Returns the written paths."""
+    states; node coordinates are the cumulative element lengths along x; ``additional`` maps field names to
+    per-node arrays over all fibers (e.g. "computeStateInformation").  Returns the written paths."""
     off = np.asarray(system.fiber_offsets)
     fibers = range(len(off) - 1) if fibers is None else fibers
     paths = []
@@ -55,7 +60,8 @@ def write_fibers(filename: str, output_no: int, system, states: np.ndarray, stat
         x = np.concatenate([[0.0], np.cumsum(h)])
         geom = np.stack([x, np.zeros_like(x), np.zeros_like(x)], axis=1)
         vals = {state_names[s]: states[s, a:b] for s in states_for_transfer}
-        data = fiber_dict(vals, geom, time_step_no, current_time)
+        extra = {k: np.asarray(v)[a:b] for k, v in (additional or {}).items()}
+        data = fiber_dict(vals, geom, time_step_no, current_time, additional=extra)
         path = f"{filename}_{f}_{output_no:07d}.py"
         if binary:
             with open(path, "wb") as fh:

@@ -73,6 +73,9 @@ class FiberSystem:
     states_for_transfer: Sequence[int] = (0,)
     only_compute_if_has_been_stimulated: bool = False   # "onlyComputeIfHasBeenStimulated"
     skip_close_to_equilibrium: bool = False   # "disableComputationWhenStatesAreCloseToEquilibrium" (split, vc)
+    # the diffusion solver has one more additional field variable than algebraicsForTransfer: the
+    # "computeStateInformation" slot is transferred too (initialization.tpp:572-587)
+    compute_state_information: bool = False
 
     @property
     def n_fibers(self) -> int:
@@ -295,6 +298,8 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         algebraics_for_transfer=[int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))],
         states_for_transfer=[int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))] or [0],
         only_compute_if_has_been_stimulated=only_if_stimulated, skip_close_to_equilibrium=skip_equilibrium)
+    sys_.compute_state_information = \
+        int(f0["diff"].get("nAdditionalFieldVariables", 0)) > len(sys_.algebraics_for_transfer)
     sys_.method = b200.get("method", "split")
     sys_.precision = precision
     return sys_
@@ -604,7 +609,19 @@ class FastMonodomainSolver:
     def reset_timing(self):
         self._call(N.lib().fdm_reset_timing)
 
+    def compute_state_information(self) -> np.ndarray:
+        """"computeStateInformation" per node (communication.tpp:277-290): the status of the node's point
+        buffer (0 inactive, 1 neighbor_is_active, 2 active), -1 on fibers not stimulated yet under
+        onlyComputeIfHasBeenStimulated."""
+        out = np.empty(self.system.n_nodes, np.float64)
+        self._call(N.lib().fdm_get_compute_state_information, N.ptr(out, C.c_double))
+        return out
+
     def data(self) -> Dict[str, np.ndarray]:
-        """The fiber data the reference transfers out (statesForTransfer / algebraicsForTransfer)."""
+        """The fiber data the reference transfers out (statesForTransfer / algebraicsForTransfer, and
+        computeStateInformation when the diffusion solver has the extra slot)."""
         st = self.states()
-        return {"Vm": st[0], "states": st[list(self.system.states_for_transfer)], "algebraics": self.algebraics()}
+        d = {"Vm": st[0], "states": st[list(self.system.states_for_transfer)], "algebraics": self.algebraics()}
+        if self.system.compute_state_information:
+            d["computeStateInformation"] = self.compute_state_information()
+        return d

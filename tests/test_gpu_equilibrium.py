@@ -99,3 +99,43 @@ def test_unsupported_combinations_fail_loudly():
     s.clamp_rule = "center"
     with pytest.raises(S.N.FdmError):
         S.FastMonodomainSolver(s.copy(), method="split").initialize()
+
+
+def _state_information(system, status, has_been_stimulated):
+    """computeStateInformation per node as communication.tpp:249-290 forms it: the status of the point buffer
+    (valuesOffset + valueNo) / W of the rank that computes the fiber (fiber % nRanks), -1 on a fiber not
+    stimulated yet under onlyComputeIfHasBeenStimulated."""
+    off = np.asarray(system.fiber_offsets)
+    lengths = np.diff(off)
+    W, R = system.vc_width, system.n_ranks
+    first = np.concatenate([[0], np.cumsum([(lengths[r::R].sum() + W - 1) // W for r in range(R)])])
+    out = np.empty(system.n_nodes)
+    offset = np.zeros(R, np.int64)
+    for f in range(system.n_fibers):
+        r = f % R
+        buf = first[r] + (offset[r] + np.arange(lengths[f])) // W
+        out[off[f]:off[f + 1]] = status[buf]
+        if system.only_compute_if_has_been_stimulated and not has_been_stimulated[f]:
+            out[off[f]:off[f + 1]] = -1.0
+        offset[r] += lengths[f]
+    return out
+
+
+@pytest.mark.parametrize("skip,only,n_ranks,width", [(True, False, 1, 4), (True, True, 3, 8), (False, True, 2, 4),
+                                                     (False, False, 1, 4)])
+def test_compute_state_information(skip, only, n_ranks, width):
+    s = _system(True, only, n_ranks, width, end_time=1.0)
+    s.skip_close_to_equilibrium = skip
+    s.compute_state_information = True
+    run = O.OracleRun(H.oracle_spec(s.copy()))
+    st = np.ascontiguousarray(s.states, np.float64).copy()
+    run.run(st)
+    want = _state_information(s, run.eq_status, run.has_been_stimulated)
+    with S.FastMonodomainSolver(s.copy(), method="split", precision="fp64") as slv:
+        slv.advanceTimeSpan()
+        got = slv.data()["computeStateInformation"]
+    np.testing.assert_array_equal(got, want)
+    if skip and n_ranks == 1:
+        assert np.any(got == 0)       # buffers at rest were counted inactive
+    if only:
+        assert np.any(got == -1)      # fiber 3 starts at 1.2345 ms

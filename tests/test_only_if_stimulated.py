@@ -141,3 +141,18 @@ def test_settings_key():
     assert s.n_fibers == 2 and s.n_nodes == 42
     np.testing.assert_allclose(s.element_lengths, 0.01)
     np.testing.assert_allclose(s.parameters[:, 0], [0.0, 120.0, 36.0])
+
+
+def test_compute_state_information_slot_from_settings():
+    # the extra slot exists when the diffusion solver has more additional field variables than
+    # algebraicsForTransfer (initialization.tpp:572-587)
+    cfg = reference_settings()
+    assert not S.parse_settings(cfg).compute_state_information
+    for inst in cfg["RepeatedCall"]["MultipleInstances"]["instances"][0]["StrangSplitting"]["Term2"][
+            "MultipleInstances"]["instances"]:
+        inst["ImplicitEuler"]["nAdditionalFieldVariables"] = 1
+    assert S.parse_settings(cfg).compute_state_information
+    for inst in cfg["RepeatedCall"]["MultipleInstances"]["instances"][0]["StrangSplitting"]["Term1"][
+            "MultipleInstances"]["instances"]:
+        inst["Heun"]["CellML"]["algebraicsForTransfer"] = [4]
+    assert not S.parse_settings(cfg).compute_state_information
