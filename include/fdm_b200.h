@@ -230,6 +230,55 @@ int fdm_fused_cluster_shapes(int *threads, int *nodes_per_thread, int capacity);
  * fibers, > 1: cluster mode), number of CTAs */
 int fdm_fused_layout(const fdm_solver *s, int *threads, int *nodes_per_thread, int *cluster_size, int *n_blocks);
 
+/* ---- fibers -> 3D static bidomain (EMG) -------------------------------------------------------------
+ * The caller downstream of the fiber solver in the reference's fibers_emg example (fast_fibers_emg.cpp:17-63:
+ * Control::Coupling of the FastMonodomainSolver with TimeSteppingScheme::StaticBidomainSolver,
+ * static_bidomain_solver.tpp).  Structured hexahedral mesh with trilinear elements: node_positions[n][3] for
+ * the nx*ny*nz nodes numbered i + nx*(j + ny*k); element dofs in the reference's order (x fastest).
+ * fdm_emg_potential_flow: Laplace with Dirichlet values ("PotentialFlow", static_bidomain_solver.tpp:102-130),
+ *   nodal gradients averaged over adjacent elements and normalised into the fiber direction
+ *   (08_field_variable_gradient.tpp:59-115); or fdm_emg_set_direction gives the directions.
+ * fdm_emg_set_conductivity: "diffusionTensor" sigma_i and "extracellularDiffusionTensor" sigma_e (9 values,
+ *   row-major, in fiber coordinates: first axis along the fiber), one for all elements or one per element;
+ *   assembles K(sigma_i) and K(sigma_i + sigma_e) with the tensors rotated onto the interpolated direction
+ *   (diffusion_tensor_directional.tpp:72-110) and gauss_points^3 Gauss points per element.
+ * fdm_emg_set_fiber_mapping: positions[n_source][3] of the fiber nodes (in the fiber solver's node order);
+ *   each node inside an element (xi outside [0,1] by at most xi_tolerance, <= 0: 0.1) adds phi_m(xi) times its
+ *   value to the element's 8 nodes, each 3D node divides by its factor sum (|sum| <= 1e-12: default_value)
+ *   (mapping_between_meshes 00_construct.tpp:90-160, 03_manager_implementation.tpp:239-300).
+ * fdm_emg_map_fibers: maps the fiber solver's current Vm (on the device, ordered after its work);
+ *   fdm_emg_map_values maps host values; fdm_emg_set_vm sets the 3D Vm directly.
+ * fdm_emg_solve: K(sigma_i + sigma_e) phi_e = -K(sigma_i) Vm (static_bidomain_solver.tpp:37-55), constants as
+ *   null space, conjugate gradients with a Jacobi preconditioner until ||r||_2 <= max(rtol ||b||_2, atol);
+ *   phi_e is the zero-mean solution; initial_guess_nonzero starts from the previous phi_e. */
+typedef struct fdm_emg fdm_emg;
+#define FDM_EMG_PHI_E 0          /* extracellular potential phi_e [N] */
+#define FDM_EMG_VM 1             /* transmembrane potential on the 3D mesh [N] */
+#define FDM_EMG_RHS 2            /* -K(sigma_i) Vm [N] */
+#define FDM_EMG_FLOW_POTENTIAL 3 /* potential flow solution [N] */
+#define FDM_EMG_DIRECTION 4      /* fiber direction [N][3] */
+int fdm_emg_create(int nx, int ny, int nz, const double *node_positions, int device, fdm_emg **out);
+int fdm_emg_destroy(fdm_emg *m);
+const char *fdm_emg_last_error(const fdm_emg *m);
+int fdm_emg_potential_flow(fdm_emg *m, int64_t n_dirichlet, const int64_t *nodes, const double *values,
+                           int gauss_points, double rtol, double atol, int max_iterations, int *iterations);
+int fdm_emg_set_direction(fdm_emg *m, const double *direction /* [N][3] */);
+int fdm_emg_set_conductivity(fdm_emg *m, int64_t n_sigma_i, const double *sigma_i, int64_t n_sigma_e,
+                             const double *sigma_e, int gauss_points);
+int fdm_emg_set_fiber_mapping(fdm_emg *m, int64_t n_source, const double *positions, double xi_tolerance,
+                              double default_value, int64_t *n_mapped);
+int fdm_emg_map_fibers(fdm_emg *m, fdm_solver *s);
+int fdm_emg_map_values(fdm_emg *m, const double *fiber_values);
+int fdm_emg_set_vm(fdm_emg *m, const double *vm);
+int fdm_emg_solve(fdm_emg *m, double rtol, double atol, int max_iterations, int initial_guess_nonzero,
+                  int *iterations, double *residual);
+int fdm_emg_get(fdm_emg *m, int field, double *out);
+/* the assembled stencils, coef[q * N + node] with q = (dx+1) + 3(dy+1) + 9(dz+1); which: 0 K(sigma_i),
+ * 1 K(sigma_i + sigma_e) */
+int fdm_emg_get_stencil(fdm_emg *m, int which, double *out /* [27 * N] */);
+/* device time, iterations and residual norm of the last fdm_emg_solve */
+int fdm_emg_timing(const fdm_emg *m, double *last_solve_ms, int *last_iterations, double *last_residual);
+
 /* ---- compatibility export of the reference's generated-library ABI ---------------------------------
  * The reference's FastMonodomainSolver with optimizationType "gpu" dlopens a library and binds
  * initializeArrays and computeMonodomain (fast_monodomain_solver_gpu.tpp:185-196); pointing its

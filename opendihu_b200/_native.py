@@ -33,8 +33,14 @@ EXPORTED = [
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
     "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes", "fdm_get_equilibrium_state",
     "fdm_cellml_rhs_device", "fdm_cellml_rhs_configure", "fdm_fused_cluster_shapes", "fdm_fused_layout",
-    "fdm_get_compute_state_information",
+    "fdm_get_compute_state_information", "fdm_emg_create", "fdm_emg_destroy", "fdm_emg_last_error",
+    "fdm_emg_potential_flow", "fdm_emg_set_direction", "fdm_emg_set_conductivity", "fdm_emg_set_fiber_mapping",
+    "fdm_emg_map_fibers", "fdm_emg_map_values", "fdm_emg_set_vm", "fdm_emg_solve", "fdm_emg_get",
+    "fdm_emg_get_stencil", "fdm_emg_timing",
 ]
+
+#: fdm_emg_get fields of include/fdm_b200.h
+EMG_PHI_E, EMG_VM, EMG_RHS, EMG_FLOW_POTENTIAL, EMG_DIRECTION = 0, 1, 2, 3, 4
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
 NOALLOC_MAX_NODES = 262144
@@ -107,6 +113,20 @@ def lib() -> C.CDLL:
         "fdm_fused_cluster_shapes": (C.c_int, [i32, i32, C.c_int]),
         "fdm_fused_layout": (C.c_int, [P, i32, i32, i32, i32]),
         "fdm_get_compute_state_information": (C.c_int, [P, d]),
+        "fdm_emg_create": (C.c_int, [C.c_int, C.c_int, C.c_int, d, C.c_int, C.POINTER(P)]),
+        "fdm_emg_destroy": (C.c_int, [P]),
+        "fdm_emg_last_error": (C.c_char_p, [P]),
+        "fdm_emg_potential_flow": (C.c_int, [P, C.c_int64, i64, d, C.c_int, C.c_double, C.c_double, C.c_int, i32]),
+        "fdm_emg_set_direction": (C.c_int, [P, d]),
+        "fdm_emg_set_conductivity": (C.c_int, [P, C.c_int64, d, C.c_int64, d, C.c_int]),
+        "fdm_emg_set_fiber_mapping": (C.c_int, [P, C.c_int64, d, C.c_double, C.c_double, i64]),
+        "fdm_emg_map_fibers": (C.c_int, [P, P]),
+        "fdm_emg_map_values": (C.c_int, [P, d]),
+        "fdm_emg_set_vm": (C.c_int, [P, d]),
+        "fdm_emg_solve": (C.c_int, [P, C.c_double, C.c_double, C.c_int, C.c_int, i32, d]),
+        "fdm_emg_get": (C.c_int, [P, C.c_int, d]),
+        "fdm_emg_get_stencil": (C.c_int, [P, C.c_int, d]),
+        "fdm_emg_timing": (C.c_int, [P, d, i32, d]),
         "fdm_diffusion_solve": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_diffusion_solve_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_compat_configure": (C.c_int, [C.c_int] * 13),

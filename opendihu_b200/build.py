@@ -25,7 +25,7 @@ LIB = os.path.join(PKG, "libfdm_b200.so")
 SOURCES = ["fdm_host.cu", "fdm_kernels_split.cu", "fdm_fused.cu", "fdm_fused_f64_exact.cu", "fdm_fused_f64_approx.cu",
            "fdm_fused_f32_exact.cu", "fdm_fused_f32_approx.cu", "fdm_fused_f64_exact_gate.cu",
            "fdm_fused_f64_approx_gate.cu", "fdm_fused_f32_exact_gate.cu", "fdm_fused_f32_approx_gate.cu",
-           "fdm_fused_cluster_f32.cu", "fdm_fused_cluster_f64.cu", "fdm_noalloc.cu"]
+           "fdm_fused_cluster_f32.cu", "fdm_fused_cluster_f64.cu", "fdm_noalloc.cu", "fdm_emg.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",

@@ -1,0 +1,1184 @@
+// Fibers -> 3D static bidomain (EMG): the caller downstream of the fiber solver in the reference's
+// fibers_emg example (examples/electrophysiology/fibers/fibers_emg/src/fast_fibers_emg.cpp:17-63,
+// Control::Coupling of the FastMonodomainSolver with TimeSteppingScheme::StaticBidomainSolver).
+//
+//  * mesh: structured hexahedral mesh (StructuredDeformableOfDimension<3>, linear Lagrange), nodes numbered
+//    i + nx*(j + ny*k), element dofs a + 2b + 4c (the reference's dof order within an element);
+//  * operators: stiffness matrices K(sigma) = int grad(phi_l) . sigma . grad(phi_m) stored as a 27-point
+//    stencil per node (SoA: coef[q * N + node], q = (dx+1) + 3(dy+1) + 9(dz+1)), assembled per node in a fixed
+//    order (deterministic) with Gauss-Legendre quadrature;
+//  * potential flow (static_bidomain_solver.tpp:102-130): Laplace with Dirichlet values, the nodal gradient
+//    averaged over the adjacent elements (08_field_variable_gradient.tpp:59-115), normalised to the fiber
+//    direction (diffusion_tensor_directional.tpp:27-37);
+//  * directional tensors (diffusion_tensor_directional.tpp:72-110, math_utility.tpp:587-655): the tensor
+//    given in fiber coordinates, sigma_i or sigma_i + sigma_e, rotated onto the interpolated direction;
+//  * transfer of Vm from the fibers (mapping_between_meshes 00_construct.tpp:90-160, 01_implementation.tpp:15-60,
+//    03_manager_implementation.tpp:239-300): each fiber node adds phi_m(xi) * Vm to the 8 nodes of the element
+//    it lies in, each 3D node divides by the sum of its factors (|sum| <= 1e-12: the default value);
+//  * solve (static_bidomain_solver.tpp:37-55): K(sigma_i + sigma_e) phi_e = -K(sigma_i) Vm with the constant
+//    functions as null space, by conjugate gradients with a Jacobi preconditioner, all on the device; the
+//    result is the zero-mean solution.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fdm_b200.h"
+#include "fdm_internal.h"
+
+namespace {
+
+constexpr int EMG_T = 256;          // threads per block of the vector kernels
+constexpr int EMG_MAX_BLOCKS = 1184; // 148 SMs x 8 resident blocks: grid-stride loops, one partial per block
+constexpr int EMG_MAX_GAUSS = 7;
+
+template<class T>
+struct Buf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t k)
+  {
+    if (k <= n && p)
+      return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(k, 1) * sizeof(T));
+    if (e == cudaSuccess)
+      n = k;
+    return e;
+  }
+  void release()
+  {
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~Buf() { release(); }
+};
+
+struct Quad {
+  int n;
+  double x[EMG_MAX_GAUSS], w[EMG_MAX_GAUSS];
+};
+
+// Gauss-Legendre points and weights on [0, 1]: Newton's method on the Legendre polynomial P_n from the
+// Chebyshev-node guesses, P_n and P_n' by the three-term recurrence.
+Quad gauss_legendre(int n)
+{
+  Quad q{};
+  q.n = n;
+  for (int i = 0; i < n; i++) {
+    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; k++) {
+        const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      if (n == 1) {
+        p1 = z;
+        p0 = 1.0;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16)
+        break;
+    }
+    q.x[i] = 0.5 * (1.0 - z);
+    q.w[i] = 1.0 / ((1.0 - z * z) * dp * dp); // 2/((1-z^2) P'^2) on [-1,1], halved on [0,1]
+  }
+  return q;
+}
+
+// ---- element geometry ------------------------------------------------------------------------------
+
+struct Grid {
+  int nx, ny, nz;
+  __host__ __device__ int64_t n_nodes() const { return (int64_t)nx * ny * nz; }
+  __host__ __device__ int64_t n_elements() const { return (int64_t)(nx - 1) * (ny - 1) * (nz - 1); }
+  __host__ __device__ int64_t node(int i, int j, int k) const { return i + (int64_t)nx * (j + (int64_t)ny * k); }
+  __host__ __device__ int64_t element(int i, int j, int k) const
+  {
+    return i + (int64_t)(nx - 1) * (j + (int64_t)(ny - 1) * k);
+  }
+};
+
+// shape functions of the trilinear element and their derivatives at xi
+__host__ __device__ inline void shape(const double xi[3], double phi[8], double dphi[8][3])
+{
+  for (int l = 0; l < 8; l++) {
+    const int a = l & 1, b = (l >> 1) & 1, c = l >> 2;
+    const double fx = a ? xi[0] : 1.0 - xi[0], fy = b ? xi[1] : 1.0 - xi[1], fz = c ? xi[2] : 1.0 - xi[2];
+    const double gx = a ? 1.0 : -1.0, gy = b ? 1.0 : -1.0, gz = c ? 1.0 : -1.0;
+    phi[l] = fx * fy * fz;
+    dphi[l][0] = gx * fy * fz;
+    dphi[l][1] = fx * gy * fz;
+    dphi[l][2] = fx * fy * gz;
+  }
+}
+
+// J[i][d] = d x_i / d xi_d; returns det J, writes the inverse
+__host__ __device__ inline double jacobian(const double P[8][3], const double dphi[8][3], double inv[3][3])
+{
+  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int l = 0; l < 8; l++)
+    for (int i = 0; i < 3; i++)
+      for (int d = 0; d < 3; d++)
+        J[i][d] += P[l][i] * dphi[l][d];
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  const double id = 1.0 / det;
+  inv[0][0] = c00 * id;
+  inv[1][0] = c01 * id;
+  inv[2][0] = c02 * id;
+  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  return det;
+}
+
+// world-space gradient: grad_x phi = J^-T grad_xi phi  (inv = J^-1, inv[d][i] = d xi_d / d x_i)
+__host__ __device__ inline void world_gradient(const double inv[3][3], const double g[3], double out[3])
+{
+  for (int i = 0; i < 3; i++)
+    out[i] = inv[0][i] * g[0] + inv[1][i] * g[1] + inv[2][i] * g[2];
+}
+
+// the reference's rotation of a tensor given in fiber coordinates onto direction b (math_utility.tpp:587-655),
+// its formulas kept as they are: for b along e_3 the basis is built from e_2, with its norm expression for
+// the third basis vector (exact for |b| = 1, as nodal directions are)
+__host__ __device__ inline void rotate_tensor(double S[3][3], const double b[3])
+{
+  const double b1 = b[0], b2 = b[1], b3 = b[2];
+  const double bNorm = sqrt(b1 * b1 + b2 * b2 + b3 * b3);
+  const double e3bNorm = sqrt(b1 * b1 + b2 * b2);
+  const double be3bNorm = sqrt(b1 * b1 * b3 * b3 + b2 * b2 * b3 * b3 + (b1 * b1 + b2 * b2) * (b1 * b1 + b2 * b2));
+  if (fabs(bNorm) < 1e-15)
+    return;
+  double B[3][3];
+  if (fabs(e3bNorm) < 1e-15 || fabs(be3bNorm) < 1e-15) {
+    const double e2bNorm = sqrt(b3 * b3 + b1 * b1);
+    const double be2bNorm = sqrt(b1 * b1 * b2 * b2 + (b1 * b1 * b3 * b3) * (b1 * b1 * b3 * b3) + b2 * b2 + b3 * b3);
+    if (fabs(e2bNorm) < 1e-15 || fabs(be2bNorm) < 1e-15)
+      return;
+    const double Bv[3][3] = {{b1 / bNorm, b3 / e2bNorm, -b1 * b2 / be2bNorm},
+                             {b2 / bNorm, 0.0, (b1 * b1 + b3 * b3) / be2bNorm},
+                             {b3 / bNorm, -b1 / e2bNorm, -b2 * b3 / be2bNorm}};
+    memcpy(B, Bv, sizeof(B));
+  } else {
+    const double Bv[3][3] = {{b1 / bNorm, -b2 / e3bNorm, -b1 * b3 / be3bNorm},
+                             {b2 / bNorm, b1 / e3bNorm, -b2 * b3 / be3bNorm},
+                             {b3 / bNorm, 0.0, (b1 * b1 + b2 * b2) / be3bNorm}};
+    memcpy(B, Bv, sizeof(B));
+  }
+  double T[3][3], R[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      T[i][j] = B[i][0] * S[0][j] + B[i][1] * S[1][j] + B[i][2] * S[2][j];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      R[i][j] = T[i][0] * B[j][0] + T[i][1] * B[j][1] + T[i][2] * B[j][2];
+  memcpy(S, R, sizeof(R));
+}
+
+__device__ inline void element_nodes(const Grid& g, int ei, int ej, int ek, int64_t nodes[8])
+{
+  for (int l = 0; l < 8; l++)
+    nodes[l] = g.node(ei + (l & 1), ej + ((l >> 1) & 1), ek + (l >> 2));
+}
+
+// ---- kernels -----------------------------------------------------------------------------------------
+
+struct AssembleArgs {
+  Grid g;
+  const double* pos;       // [N][3]
+  const double* dir;       // [N][3] normalised nodal directions, or null (tensor used as given)
+  const double* tensor;    // 9 per element, or 9 for all (n_tensor == 1)
+  const double* tensor2;   // added to tensor before the rotation (sigma_e), or null
+  int64_t n_tensor, n_tensor2;
+  double prefactor;
+  Quad q;
+  double* coef;            // [27][N]
+  double* diag;            // [N] (may be null)
+};
+
+// row of node n of the assembled stiffness matrix: the sum over its adjacent elements (in element order) of the
+// element matrix row, each integrated over the element's Gauss points in order
+__global__ void __launch_bounds__(128) assemble_kernel(AssembleArgs a)
+{
+  const int64_t N = a.g.n_nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % a.g.nx), j = (int)((n / a.g.nx) % a.g.ny), k = (int)(n / ((int64_t)a.g.nx * a.g.ny));
+    double row[27];
+    for (int q = 0; q < 27; q++)
+      row[q] = 0.0;
+    for (int c = 1; c >= 0; c--)
+      for (int b = 1; b >= 0; b--)
+        for (int aa = 1; aa >= 0; aa--) {
+          // element whose local node (aa, b, c) is this node
+          const int ei = i - aa, ej = j - b, ek = k - c;
+          if (ei < 0 || ej < 0 || ek < 0 || ei >= a.g.nx - 1 || ej >= a.g.ny - 1 || ek >= a.g.nz - 1)
+            continue;
+          const int l = aa + 2 * b + 4 * c;
+          int64_t nodes[8];
+          element_nodes(a.g, ei, ej, ek, nodes);
+          double P[8][3], D[8][3];
+          for (int m = 0; m < 8; m++)
+            for (int d = 0; d < 3; d++) {
+              P[m][d] = a.pos[nodes[m] * 3 + d];
+              D[m][d] = a.dir ? a.dir[nodes[m] * 3 + d] : 0.0;
+            }
+          const int64_t e = a.g.element(ei, ej, ek);
+          const double* t1 = a.tensor + 9 * (a.n_tensor == 1 ? 0 : e);
+          const double* t2 = a.tensor2 ? a.tensor2 + 9 * (a.n_tensor2 == 1 ? 0 : e) : nullptr;
+          for (int qz = 0; qz < a.q.n; qz++)
+            for (int qy = 0; qy < a.q.n; qy++)
+              for (int qx = 0; qx < a.q.n; qx++) {
+                const double xi[3] = {a.q.x[qx], a.q.x[qy], a.q.x[qz]};
+                const double w = a.q.w[qx] * a.q.w[qy] * a.q.w[qz];
+                double phi[8], dphi[8][3], inv[3][3];
+                shape(xi, phi, dphi);
+                const double det = jacobian(P, dphi, inv);
+                double S[3][3];
+                for (int r = 0; r < 3; r++)
+                  for (int s = 0; s < 3; s++)
+                    S[r][s] = t1[3 * r + s] + (t2 ? t2[3 * r + s] : 0.0);
+                if (a.dir) {
+                  double bvec[3] = {0.0, 0.0, 0.0};
+                  for (int m = 0; m < 8; m++)
+                    for (int d = 0; d < 3; d++)
+                      bvec[d] += phi[m] * D[m][d];
+                  if (!isfinite(bvec[0]) || !isfinite(bvec[1]) || !isfinite(bvec[2])) {
+                    bvec[0] = 0.0;
+                    bvec[1] = 0.0;
+                    bvec[2] = 1.0;
+                  }
+                  rotate_tensor(S, bvec);
+                }
+                double gl[3], sg[3];
+                world_gradient(inv, dphi[l], gl);
+                for (int r = 0; r < 3; r++)
+                  sg[r] = S[r][0] * gl[0] + S[r][1] * gl[1] + S[r][2] * gl[2];
+                const double f = a.prefactor * w * fabs(det);
+                for (int m = 0; m < 8; m++) {
+                  double gm[3];
+                  world_gradient(inv, dphi[m], gm);
+                  const int dx = (m & 1) - aa, dy = ((m >> 1) & 1) - b, dz = (m >> 2) - c;
+                  row[(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)] += f * (sg[0] * gm[0] + sg[1] * gm[1] + sg[2] * gm[2]);
+                }
+              }
+        }
+    for (int q = 0; q < 27; q++)
+      a.coef[q * N + n] = row[q];
+    if (a.diag)
+      a.diag[n] = row[13];
+  }
+}
+
+// nodal gradient of u: per adjacent element the gradient at the node's corner, divided by the number of
+// adjacent elements, summed; then normalised (a zero gradient gives a non-finite direction, which the
+// assembly replaces by (0, 0, 1) as the reference does)
+__global__ void gradient_direction_kernel(Grid g, const double* pos, const double* u, double* dir)
+{
+  const int64_t N = g.n_nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / ((int64_t)g.nx * g.ny));
+    int n_adj = 0;
+    for (int c = 0; c < 2; c++)
+      for (int b = 0; b < 2; b++)
+        for (int aa = 0; aa < 2; aa++) {
+          const int ei = i - aa, ej = j - b, ek = k - c;
+          n_adj += (ei >= 0 && ej >= 0 && ek >= 0 && ei < g.nx - 1 && ej < g.ny - 1 && ek < g.nz - 1) ? 1 : 0;
+        }
+    double grad[3] = {0.0, 0.0, 0.0};
+    // elements in element order (the reference loops over elements and adds into the node)
+    for (int c = 1; c >= 0; c--)
+      for (int b = 1; b >= 0; b--)
+        for (int aa = 1; aa >= 0; aa--) {
+          const int ei = i - aa, ej = j - b, ek = k - c;
+          if (ei < 0 || ej < 0 || ek < 0 || ei >= g.nx - 1 || ej >= g.ny - 1 || ek >= g.nz - 1)
+            continue;
+          int64_t nodes[8];
+          element_nodes(g, ei, ej, ek, nodes);
+          double P[8][3], uv[8];
+          for (int m = 0; m < 8; m++) {
+            for (int d = 0; d < 3; d++)
+              P[m][d] = pos[nodes[m] * 3 + d];
+            uv[m] = u[nodes[m]];
+          }
+          const double xi[3] = {(double)aa, (double)b, (double)c};
+          double phi[8], dphi[8][3], inv[3][3];
+          shape(xi, phi, dphi);
+          jacobian(P, dphi, inv);
+          double gxi[3] = {0.0, 0.0, 0.0};
+          for (int m = 0; m < 8; m++)
+            for (int d = 0; d < 3; d++)
+              gxi[d] += uv[m] * dphi[m][d];
+          double gw[3];
+          world_gradient(inv, gxi, gw);
+          for (int d = 0; d < 3; d++)
+            grad[d] += gw[d] / n_adj;
+        }
+    const double nrm = sqrt(grad[0] * grad[0] + grad[1] * grad[1] + grad[2] * grad[2]);
+    for (int d = 0; d < 3; d++)
+      dir[n * 3 + d] = grad[d] / nrm;
+  }
+}
+
+// y = A x on the 27-point stencil; rows with mask[n] set give y = 0 (Dirichlet rows); partial[block] = sum p.y
+// when dot is set
+__global__ void __launch_bounds__(EMG_T) spmv_kernel(Grid g, const double* __restrict__ coef,
+                                                     const double* __restrict__ x, double* __restrict__ y,
+                                                     const unsigned char* __restrict__ mask, double* partial)
+{
+  __shared__ double red[EMG_T / 32];
+  const int64_t N = g.n_nodes();
+  const int64_t sx = 1, sy = g.nx, sz = (int64_t)g.nx * g.ny;
+  double acc = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / sz);
+    double s = 0.0;
+    if (!(mask && mask[n])) {
+#pragma unroll
+      for (int dz = -1; dz <= 1; dz++) {
+        if (k + dz < 0 || k + dz >= g.nz)
+          continue;
+#pragma unroll
+        for (int dy = -1; dy <= 1; dy++) {
+          if (j + dy < 0 || j + dy >= g.ny)
+            continue;
+#pragma unroll
+          for (int dx = -1; dx <= 1; dx++) {
+            if (i + dx < 0 || i + dx >= g.nx)
+              continue;
+            const int q = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+            s += coef[q * N + n] * x[n + dx * sx + dy * sy + dz * sz];
+          }
+        }
+      }
+    }
+    y[n] = s;
+    acc += x[n] * s;
+  }
+  if (partial) {
+    for (int o = 16; o > 0; o >>= 1)
+      acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0)
+      red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < EMG_T / 32; w++)
+        t += red[w];
+      partial[blockIdx.x] = t;
+    }
+  }
+}
+
+// sums nb partials of each of k rows (partial[r * EMG_MAX_BLOCKS + b]) in a fixed order into out[r]
+__global__ void reduce_kernel(const double* partial, int nb, int k, double* out)
+{
+  __shared__ double red[EMG_T / 32];
+  for (int r = 0; r < k; r++) {
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+      acc += partial[r * EMG_MAX_BLOCKS + b];
+    for (int o = 16; o > 0; o >>= 1)
+      acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0)
+      red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < EMG_T / 32; w++)
+        t += red[w];
+      out[r] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// CG scalars on the device: s[0] = r.z, s[1] = p.Ap, s[2] = r.z new, s[3] = r.r, s[4] = alpha, s[5] = beta
+__global__ void update_kernel(int64_t N, double* x, double* r, double* z, const double* p, const double* q,
+                              const double* dinv, const double* s, double* partial)
+{
+  __shared__ double red[2][EMG_T / 32];
+  const double alpha = s[1] != 0.0 ? s[0] / s[1] : 0.0;
+  double rz = 0.0, rr = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    x[n] += alpha * p[n];
+    const double rn = r[n] - alpha * q[n];
+    r[n] = rn;
+    const double zn = rn * dinv[n];
+    z[n] = zn;
+    rz += rn * zn;
+    rr += rn * rn;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rz += __shfl_down_sync(0xffffffffu, rz, o);
+    rr += __shfl_down_sync(0xffffffffu, rr, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = rz;
+    red[1][threadIdx.x >> 5] = rr;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < EMG_T / 32; w++) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    partial[blockIdx.x] = a;
+    partial[EMG_MAX_BLOCKS + blockIdx.x] = b;
+  }
+}
+
+// p = z + (rz_new / rz) p; then rz = rz_new
+__global__ void direction_kernel(int64_t N, double* p, const double* z, const double* s)
+{
+  const double beta = s[0] != 0.0 ? s[2] / s[0] : 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+    p[n] = z[n] + beta * p[n];
+}
+
+__global__ void shift_scalar_kernel(double* s)
+{
+  s[0] = s[2];
+}
+
+// r = b - y, z = dinv r, p = z; partials of r.z and r.r
+__global__ void init_residual_kernel(int64_t N, const double* b, const double* y, double* r, double* z, double* p,
+                                     const double* dinv, double* partial)
+{
+  __shared__ double red[2][EMG_T / 32];
+  double rz = 0.0, rr = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    const double rn = b[n] - y[n];
+    r[n] = rn;
+    const double zn = rn * dinv[n];
+    z[n] = zn;
+    p[n] = zn;
+    rz += rn * zn;
+    rr += rn * rn;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rz += __shfl_down_sync(0xffffffffu, rz, o);
+    rr += __shfl_down_sync(0xffffffffu, rr, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = rz;
+    red[1][threadIdx.x >> 5] = rr;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, c = 0.0;
+    for (int w = 0; w < EMG_T / 32; w++) {
+      a += red[0][w];
+      c += red[1][w];
+    }
+    partial[blockIdx.x] = a;
+    partial[EMG_MAX_BLOCKS + blockIdx.x] = c;
+  }
+}
+
+// partial sums of x (for the mean) and of b.b
+__global__ void sum_kernel(int64_t N, const double* x, const double* b, double* partial)
+{
+  __shared__ double red[2][EMG_T / 32];
+  double sx = 0.0, bb = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    sx += x[n];
+    if (b)
+      bb += b[n] * b[n];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_down_sync(0xffffffffu, sx, o);
+    bb += __shfl_down_sync(0xffffffffu, bb, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = sx;
+    red[1][threadIdx.x >> 5] = bb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, c = 0.0;
+    for (int w = 0; w < EMG_T / 32; w++) {
+      a += red[0][w];
+      c += red[1][w];
+    }
+    partial[blockIdx.x] = a;
+    partial[EMG_MAX_BLOCKS + blockIdx.x] = c;
+  }
+}
+
+__global__ void subtract_mean_kernel(int64_t N, double* x, const double* sum)
+{
+  const double m = sum[0] / (double)N;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+    x[n] -= m;
+}
+
+__global__ void negate_kernel(int64_t N, double* x)
+{
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+    x[n] = -x[n];
+}
+
+__global__ void inverse_diag_kernel(int64_t N, const double* diag, const unsigned char* mask, double* dinv)
+{
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+    dinv[n] = (mask && mask[n]) ? 0.0 : (diag[n] != 0.0 ? 1.0 / diag[n] : 1.0);
+}
+
+// 3D node n: sum over its contributions (fiber node, factor) in fiber-node order, divided by the factor sum
+__global__ void map_kernel(int64_t N, const int64_t* ptr, const int64_t* src, const double* w, const double* fsum,
+                           const double* vm, double default_value, double* out)
+{
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int64_t e = ptr[n]; e < ptr[n + 1]; e++)
+      v += w[e] * vm[src[e]];
+    out[n] = fabs(fsum[n]) > 1e-12 ? v / fsum[n] : default_value;
+  }
+}
+
+int blocks_for(int64_t n)
+{
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + EMG_T - 1) / EMG_T, EMG_MAX_BLOCKS));
+}
+
+// ---- host: trilinear inversion and element search ------------------------------------------------------
+
+struct HostMesh {
+  Grid g;
+  std::vector<double> pos; // [N][3]
+  void element_points(int64_t e, double P[8][3]) const
+  {
+    const int ex = (int)(e % (g.nx - 1)), ey = (int)((e / (g.nx - 1)) % (g.ny - 1)),
+              ez = (int)(e / ((int64_t)(g.nx - 1) * (g.ny - 1)));
+    for (int l = 0; l < 8; l++) {
+      const int64_t n = g.node(ex + (l & 1), ey + ((l >> 1) & 1), ez + (l >> 2));
+      for (int d = 0; d < 3; d++)
+        P[l][d] = pos[n * 3 + d];
+    }
+  }
+  // xi of point x in element e by Newton's method on the trilinear map; returns the largest distance of xi
+  // outside [0, 1] (0 inside)
+  double locate(int64_t e, const double x[3], double xi[3]) const
+  {
+    double P[8][3];
+    element_points(e, P);
+    xi[0] = xi[1] = xi[2] = 0.5;
+    for (int it = 0; it < 50; it++) {
+      double phi[8], dphi[8][3], inv[3][3];
+      shape(xi, phi, dphi);
+      jacobian(P, dphi, inv);
+      double r[3] = {-x[0], -x[1], -x[2]};
+      for (int l = 0; l < 8; l++)
+        for (int d = 0; d < 3; d++)
+          r[d] += phi[l] * P[l][d];
+      double dmax = 0.0;
+      for (int d = 0; d < 3; d++) {
+        const double dx = inv[d][0] * r[0] + inv[d][1] * r[1] + inv[d][2] * r[2];
+        xi[d] -= dx;
+        dmax = std::max(dmax, std::fabs(dx));
+      }
+      if (!(dmax > 1e-15) || !std::isfinite(dmax))
+        break;
+    }
+    double out = 0.0;
+    for (int d = 0; d < 3; d++)
+      out = std::max(out, std::max(-xi[d], xi[d] - 1.0));
+    return std::isfinite(out) ? out : 1e300;
+  }
+};
+
+} // namespace
+
+// ---- the solver object -----------------------------------------------------------------------------------
+
+struct fdm_emg {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  HostMesh hm;
+  int64_t N = 0;
+  Buf<double> pos, dir, flow, coef_i, coef_ie, coef_lap, diag_ie, diag_lap, dinv, vm, rhs, phi, r, z, p, q, partial,
+      scal, tensor_i, tensor_e, tmp;
+  Buf<unsigned char> mask;
+  bool have_dir = false, have_ops = false, have_map = false;
+  int64_t n_tensor_i = 0, n_tensor_e = 0;
+  // fiber -> mesh transfer (CSR over 3D nodes)
+  Buf<int64_t> map_ptr, map_src;
+  Buf<double> map_w, map_fsum;
+  int64_t n_source = 0, n_mapped = 0;
+  double default_value = 0.0;
+  int last_iterations = 0;
+  double last_residual = 0.0;
+  float last_solve_ms = 0.f;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int emg_fail(fdm_emg* m, int code, const std::string& msg)
+{
+  if (m)
+    m->err = msg;
+  else
+    fdm::fdm_report_error(code, msg);
+  return code;
+}
+
+#define EMG_CUDA(m, call)                                                                                   \
+  do {                                                                                                      \
+    cudaError_t e_ = (call);                                                                                \
+    if (e_ != cudaSuccess)                                                                                  \
+      return emg_fail(m, FDM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+#define EMG_BIND(m) EMG_CUDA(m, cudaSetDevice((m)->device))
+
+// conjugate gradients on A x = b with A the stencil coef (Dirichlet rows in mask: x keeps its value there and
+// p, r vanish), Jacobi preconditioner dinv; nullspace: b's and x's mean removed (constant null space).
+// Convergence: ||r||_2 <= max(rtol ||b||_2, atol) (unpreconditioned residual), checked every 8 iterations.
+int cg_solve(fdm_emg* m, const double* coef, const unsigned char* mask, bool nullspace, const double* b, double* x,
+             double rtol, double atol, int max_it, int* iterations, double* residual)
+{
+  const int64_t N = m->N;
+  const Grid g = m->hm.g;
+  const int nb = blocks_for(N);
+  cudaStream_t s = m->stream;
+  double* S = m->scal.p; // [0] r.z [1] p.Ap [2] r.z new [3] r.r [4] sum x [5] b.b
+  double* P = m->partial.p;
+  const double* bb = b;
+  if (nullspace) {
+    // b <- b - mean(b) (consistency of the singular system), into tmp
+    sum_kernel<<<nb, EMG_T, 0, s>>>(N, b, nullptr, P);
+    reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 4);
+    EMG_CUDA(m, cudaMemcpyAsync(m->tmp.p, b, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    subtract_mean_kernel<<<nb, EMG_T, 0, s>>>(N, m->tmp.p, S + 4);
+    bb = m->tmp.p;
+  }
+  sum_kernel<<<nb, EMG_T, 0, s>>>(N, bb, bb, P);
+  reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 2, S + 4);
+  // r = b - A x
+  spmv_kernel<<<nb, EMG_T, 0, s>>>(g, coef, x, m->q.p, mask, nullptr);
+  init_residual_kernel<<<nb, EMG_T, 0, s>>>(N, bb, m->q.p, m->r.p, m->z.p, m->p.p, m->dinv.p, P);
+  reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 0);
+  reduce_kernel<<<1, EMG_T, 0, s>>>(P + EMG_MAX_BLOCKS, nb, 1, S + 3);
+  double hs[6];
+  EMG_CUDA(m, cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  EMG_CUDA(m, cudaStreamSynchronize(s));
+  // relative to ||b|| (to the initial residual where b vanishes: the Dirichlet problem, whose right-hand side
+  // -K_fd u_d sits in the initial residual)
+  const double bnorm = hs[5] > 0 ? std::sqrt(hs[5]) : std::sqrt(hs[3]);
+  const double target = std::max(rtol * bnorm, atol);
+  double rn = std::sqrt(hs[3]);
+  int it = 0;
+  while (rn > target && it < max_it) {
+    const int chunk = std::min(8, max_it - it);
+    for (int c = 0; c < chunk; c++) {
+      spmv_kernel<<<nb, EMG_T, 0, s>>>(g, coef, m->p.p, m->q.p, mask, P);
+      reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 1);
+      update_kernel<<<nb, EMG_T, 0, s>>>(N, x, m->r.p, m->z.p, m->p.p, m->q.p, m->dinv.p, S, P);
+      reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 2);
+      reduce_kernel<<<1, EMG_T, 0, s>>>(P + EMG_MAX_BLOCKS, nb, 1, S + 3);
+      direction_kernel<<<nb, EMG_T, 0, s>>>(N, m->p.p, m->z.p, S);
+      shift_scalar_kernel<<<1, 1, 0, s>>>(S);
+    }
+    it += chunk;
+    EMG_CUDA(m, cudaGetLastError());
+    EMG_CUDA(m, cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    EMG_CUDA(m, cudaStreamSynchronize(s));
+    rn = std::sqrt(hs[3]);
+    if (!std::isfinite(rn))
+      return emg_fail(m, FDM_ERR_NAN, "conjugate gradients: non-finite residual");
+  }
+  if (nullspace) {
+    sum_kernel<<<nb, EMG_T, 0, s>>>(N, x, nullptr, P);
+    reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 4);
+    subtract_mean_kernel<<<nb, EMG_T, 0, s>>>(N, x, S + 4);
+  }
+  EMG_CUDA(m, cudaGetLastError());
+  EMG_CUDA(m, cudaStreamSynchronize(s));
+  if (iterations)
+    *iterations = it;
+  if (residual)
+    *residual = rn;
+  return FDM_OK;
+}
+
+int assemble(fdm_emg* m, const double* tensor, int64_t nt, const double* tensor2, int64_t nt2, double prefactor,
+             int gauss, bool directional, double* coef, double* diag)
+{
+  AssembleArgs a{};
+  a.g = m->hm.g;
+  a.pos = m->pos.p;
+  a.dir = directional ? m->dir.p : nullptr;
+  a.tensor = tensor;
+  a.tensor2 = tensor2;
+  a.n_tensor = nt;
+  a.n_tensor2 = nt2;
+  a.prefactor = prefactor;
+  a.q = gauss_legendre(gauss);
+  a.coef = coef;
+  a.diag = diag;
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((m->N + 127) / 128, 148 * 16));
+  assemble_kernel<<<nb, 128, 0, m->stream>>>(a);
+  EMG_CUDA(m, cudaGetLastError());
+  return FDM_OK;
+}
+
+} // namespace
+
+namespace fdm {
+// the fiber solver's Vm on the device, its node count and stream (fdm_host.cu)
+int solver_vm_device(fdm_solver* s, const double** vm, int64_t* n_nodes, cudaStream_t* stream, int* device);
+} // namespace fdm
+
+extern "C" int fdm_emg_create(int nx, int ny, int nz, const double* node_positions, int device, fdm_emg** out)
+{
+  if (!out || !node_positions || nx < 2 || ny < 2 || nz < 2)
+    return emg_fail(nullptr, FDM_ERR_ARG, "fdm_emg_create: at least 2 nodes per direction and node positions needed");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return emg_fail(nullptr, FDM_ERR_NO_DEVICE, "fdm_emg_create: no CUDA device");
+  if (device < 0 || device >= ndev)
+    return emg_fail(nullptr, FDM_ERR_ARG, "fdm_emg_create: device ordinal out of range");
+  if (cudaSetDevice(device) != cudaSuccess)
+    return emg_fail(nullptr, FDM_ERR_CUDA, "fdm_emg_create: cudaSetDevice failed");
+  fdm_emg* m = new fdm_emg();
+  m->device = device;
+  m->hm.g = Grid{nx, ny, nz};
+  m->N = m->hm.g.n_nodes();
+  m->hm.pos.assign(node_positions, node_positions + 3 * m->N);
+  // every element must have a positive Jacobian determinant at its corners
+  for (int64_t e = 0; e < m->hm.g.n_elements(); e++) {
+    double P[8][3];
+    m->hm.element_points(e, P);
+    for (int l = 0; l < 8; l++) {
+      const double xi[3] = {(double)(l & 1), (double)((l >> 1) & 1), (double)(l >> 2)};
+      double phi[8], dphi[8][3], inv[3][3];
+      shape(xi, phi, dphi);
+      const double det = jacobian(P, dphi, inv);
+      if (!(det > 0) || !std::isfinite(det)) {
+        delete m;
+        return emg_fail(nullptr, FDM_ERR_ARG, "fdm_emg_create: element " + std::to_string(e) +
+                                                  " is degenerate or inverted (node order: x fastest, then y, z)");
+      }
+    }
+  }
+  const int64_t N = m->N;
+  cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&m->ev0);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&m->ev1);
+  for (auto* b : {&m->pos, &m->dir})
+    if (e == cudaSuccess)
+      e = b->alloc(3 * N);
+  for (auto* b : {&m->coef_i, &m->coef_ie})
+    if (e == cudaSuccess)
+      e = b->alloc(27 * N);
+  for (auto* b : {&m->flow, &m->diag_ie, &m->dinv, &m->vm, &m->rhs, &m->phi, &m->r, &m->z, &m->p, &m->q, &m->tmp})
+    if (e == cudaSuccess)
+      e = b->alloc(N);
+  if (e == cudaSuccess)
+    e = m->partial.alloc(2 * EMG_MAX_BLOCKS);
+  if (e == cudaSuccess)
+    e = m->scal.alloc(8);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->pos.p, node_positions, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(m->vm.p, 0, sizeof(double) * N, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(m->phi.p, 0, sizeof(double) * N, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(m->scal.p, 0, sizeof(double) * 8, m->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(m->stream);
+  if (e != cudaSuccess) {
+    std::string msg = std::string("fdm_emg_create: ") + cudaGetErrorString(e);
+    fdm_emg_destroy(m);
+    return emg_fail(nullptr, FDM_ERR_CUDA, msg);
+  }
+  *out = m;
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_destroy(fdm_emg* m)
+{
+  if (!m)
+    return FDM_OK;
+  cudaSetDevice(m->device);
+  if (m->stream)
+    cudaStreamSynchronize(m->stream);
+  for (auto* b : {&m->pos, &m->dir, &m->flow, &m->coef_i, &m->coef_ie, &m->coef_lap, &m->diag_ie, &m->diag_lap,
+                  &m->dinv, &m->vm, &m->rhs, &m->phi, &m->r, &m->z, &m->p, &m->q, &m->partial, &m->scal,
+                  &m->tensor_i, &m->tensor_e, &m->tmp, &m->map_w, &m->map_fsum})
+    b->release();
+  m->mask.release();
+  m->map_ptr.release();
+  m->map_src.release();
+  if (m->ev0)
+    cudaEventDestroy(m->ev0);
+  if (m->ev1)
+    cudaEventDestroy(m->ev1);
+  if (m->stream)
+    cudaStreamDestroy(m->stream);
+  delete m;
+  return FDM_OK;
+}
+
+extern "C" const char* fdm_emg_last_error(const fdm_emg* m)
+{
+  return m ? m->err.c_str() : fdm_last_error(nullptr);
+}
+
+extern "C" int fdm_emg_potential_flow(fdm_emg* m, int64_t n_dirichlet, const int64_t* nodes, const double* values,
+                                      int gauss_points, double rtol, double atol, int max_iterations,
+                                      int* iterations)
+{
+  if (!m || n_dirichlet < 1 || !nodes || !values || gauss_points < 1 || gauss_points > EMG_MAX_GAUSS ||
+      max_iterations < 1)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_potential_flow: Dirichlet nodes and values, 1..7 Gauss points needed");
+  EMG_BIND(m);
+  const int64_t N = m->N;
+  std::vector<unsigned char> mk(N, 0);
+  std::vector<double> x0(N, 0.0);
+  for (int64_t d = 0; d < n_dirichlet; d++) {
+    if (nodes[d] < 0 || nodes[d] >= N)
+      return emg_fail(m, FDM_ERR_ARG, "fdm_emg_potential_flow: Dirichlet node out of range");
+    mk[nodes[d]] = 1;
+    x0[nodes[d]] = values[d];
+  }
+  EMG_CUDA(m, m->coef_lap.alloc(27 * N));
+  EMG_CUDA(m, m->diag_lap.alloc(N));
+  EMG_CUDA(m, m->mask.alloc(N));
+  EMG_CUDA(m, m->tensor_i.alloc(9));
+  const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  EMG_CUDA(m, cudaMemcpyAsync(m->tensor_i.p, eye, sizeof(eye), cudaMemcpyHostToDevice, m->stream));
+  EMG_CUDA(m, cudaMemcpyAsync(m->mask.p, mk.data(), N, cudaMemcpyHostToDevice, m->stream));
+  EMG_CUDA(m, cudaMemcpyAsync(m->flow.p, x0.data(), sizeof(double) * N, cudaMemcpyHostToDevice, m->stream));
+  int rc = assemble(m, m->tensor_i.p, 1, nullptr, 0, 1.0, gauss_points, false, m->coef_lap.p, m->diag_lap.p);
+  if (rc)
+    return rc;
+  const int nb = blocks_for(N);
+  inverse_diag_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->diag_lap.p, m->mask.p, m->dinv.p);
+  // free rows: K_ff u_f = -K_fd u_d (b = 0, x0 holding the Dirichlet values; Dirichlet rows masked)
+  EMG_CUDA(m, cudaMemsetAsync(m->rhs.p, 0, sizeof(double) * N, m->stream));
+  int its = 0;
+  double res = 0.0;
+  rc = cg_solve(m, m->coef_lap.p, m->mask.p, false, m->rhs.p, m->flow.p, rtol, atol, max_iterations, &its, &res);
+  if (rc)
+    return rc;
+  gradient_direction_kernel<<<nb, EMG_T, 0, m->stream>>>(m->hm.g, m->pos.p, m->flow.p, m->dir.p);
+  EMG_CUDA(m, cudaGetLastError());
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  m->coef_lap.release();
+  m->diag_lap.release();
+  m->have_dir = true;
+  m->have_ops = false;
+  if (iterations)
+    *iterations = its;
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_set_direction(fdm_emg* m, const double* direction)
+{
+  if (!m || !direction)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_set_direction: bad argument");
+  EMG_BIND(m);
+  EMG_CUDA(m, cudaMemcpyAsync(m->dir.p, direction, sizeof(double) * 3 * m->N, cudaMemcpyHostToDevice, m->stream));
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  m->have_dir = true;
+  m->have_ops = false;
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_set_conductivity(fdm_emg* m, int64_t n_sigma_i, const double* sigma_i, int64_t n_sigma_e,
+                                        const double* sigma_e, int gauss_points)
+{
+  if (!m || !sigma_i || !sigma_e || gauss_points < 1 || gauss_points > EMG_MAX_GAUSS)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_set_conductivity: bad argument");
+  const int64_t ne = m->hm.g.n_elements();
+  if ((n_sigma_i != 1 && n_sigma_i != ne) || (n_sigma_e != 1 && n_sigma_e != ne))
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_set_conductivity: one tensor for all elements or one per element");
+  if (!m->have_dir)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_set_conductivity: call fdm_emg_potential_flow or fdm_emg_set_direction "
+                                    "first");
+  EMG_BIND(m);
+  EMG_CUDA(m, m->tensor_i.alloc(9 * n_sigma_i));
+  EMG_CUDA(m, m->tensor_e.alloc(9 * n_sigma_e));
+  EMG_CUDA(m, cudaMemcpyAsync(m->tensor_i.p, sigma_i, sizeof(double) * 9 * n_sigma_i, cudaMemcpyHostToDevice,
+                              m->stream));
+  EMG_CUDA(m, cudaMemcpyAsync(m->tensor_e.p, sigma_e, sizeof(double) * 9 * n_sigma_e, cudaMemcpyHostToDevice,
+                              m->stream));
+  int rc = assemble(m, m->tensor_i.p, n_sigma_i, nullptr, 0, 1.0, gauss_points, true, m->coef_i.p, nullptr);
+  if (!rc)
+    rc = assemble(m, m->tensor_i.p, n_sigma_i, m->tensor_e.p, n_sigma_e, 1.0, gauss_points, true, m->coef_ie.p,
+                  m->diag_ie.p);
+  if (rc)
+    return rc;
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  m->n_tensor_i = n_sigma_i;
+  m->n_tensor_e = n_sigma_e;
+  m->have_ops = true;
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_set_fiber_mapping(fdm_emg* m, int64_t n_source, const double* positions, double xi_tolerance,
+                                         double default_value, int64_t* n_mapped)
+{
+  if (!m || n_source < 0 || (n_source > 0 && !positions))
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_set_fiber_mapping: bad argument");
+  EMG_BIND(m);
+  if (xi_tolerance <= 0)
+    xi_tolerance = 1e-1; // 00_construct.tpp:78-79
+  const Grid g = m->hm.g;
+  const int64_t ne = g.n_elements();
+  // CSR over 3D nodes of (fiber node, factor), fiber nodes in increasing order per 3D node
+  std::vector<std::vector<std::pair<int64_t, double>>> lists(m->N);
+  int64_t mapped = 0, guess = 0;
+  for (int64_t s = 0; s < n_source; s++) {
+    const double* x = positions + 3 * s;
+    double xi[3];
+    // walk from the previous element towards the point, then fall back to all elements
+    int64_t e = guess;
+    double out = m->hm.locate(e, x, xi);
+    for (int step = 0; step < g.nx + g.ny + g.nz && out > 1e-12; step++) {
+      int ex = (int)(e % (g.nx - 1)), ey = (int)((e / (g.nx - 1)) % (g.ny - 1)),
+          ez = (int)(e / ((int64_t)(g.nx - 1) * (g.ny - 1)));
+      const int ox = ex, oy = ey, oz = ez;
+      ex = std::min(std::max(ex + (xi[0] < 0 ? -1 : xi[0] > 1 ? 1 : 0), 0), g.nx - 2);
+      ey = std::min(std::max(ey + (xi[1] < 0 ? -1 : xi[1] > 1 ? 1 : 0), 0), g.ny - 2);
+      ez = std::min(std::max(ez + (xi[2] < 0 ? -1 : xi[2] > 1 ? 1 : 0), 0), g.nz - 2);
+      if (ex == ox && ey == oy && ez == oz)
+        break;
+      e = g.element(ex, ey, ez);
+      out = m->hm.locate(e, x, xi);
+    }
+    if (out > 1e-12) {
+      double best = 1e300;
+      int64_t be = 0;
+      for (int64_t c = 0; c < ne; c++) {
+        double t[3];
+        const double o = m->hm.locate(c, x, t);
+        if (o < best - 1e-15) {
+          best = o;
+          be = c;
+          if (o <= 1e-12)
+            break;
+        }
+      }
+      e = be;
+      out = m->hm.locate(e, x, xi);
+    }
+    if (out <= 1e-12) {
+      // the lowest-numbered element containing the point (points on shared faces and edges)
+      const int ex = (int)(e % (g.nx - 1)), ey = (int)((e / (g.nx - 1)) % (g.ny - 1)),
+                ez = (int)(e / ((int64_t)(g.nx - 1) * (g.ny - 1)));
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            const int cx = ex + dx, cy = ey + dy, cz = ez + dz;
+            if (cx < 0 || cy < 0 || cz < 0 || cx > g.nx - 2 || cy > g.ny - 2 || cz > g.nz - 2)
+              continue;
+            const int64_t c = g.element(cx, cy, cz);
+            if (c >= e)
+              continue;
+            double t[3];
+            if (m->hm.locate(c, x, t) <= 1e-12)
+              e = c;
+          }
+      out = m->hm.locate(e, x, xi);
+    }
+    guess = e;
+    if (out > xi_tolerance)
+      continue; // outside the mesh: this fiber node maps nowhere
+    mapped++;
+    double phi[8], dphi[8][3];
+    shape(xi, phi, dphi);
+    const int ex = (int)(e % (g.nx - 1)), ey = (int)((e / (g.nx - 1)) % (g.ny - 1)),
+              ez = (int)(e / ((int64_t)(g.nx - 1) * (g.ny - 1)));
+    for (int l = 0; l < 8; l++) {
+      double f = phi[l];
+      if (std::fabs(f) < 1e-14)
+        f = f >= 0 ? 1e-14 : -1e-14; // 00_construct.tpp:127-137
+      lists[g.node(ex + (l & 1), ey + ((l >> 1) & 1), ez + (l >> 2))].push_back({s, f});
+    }
+  }
+  std::vector<int64_t> ptr(m->N + 1, 0), src;
+  std::vector<double> w, fsum(m->N, 0.0);
+  for (int64_t n = 0; n < m->N; n++) {
+    ptr[n + 1] = ptr[n] + (int64_t)lists[n].size();
+    for (auto& pr : lists[n]) {
+      src.push_back(pr.first);
+      w.push_back(pr.second);
+      fsum[n] += pr.second;
+    }
+  }
+  EMG_CUDA(m, m->map_ptr.alloc(m->N + 1));
+  EMG_CUDA(m, m->map_src.alloc(std::max<size_t>(src.size(), 1)));
+  EMG_CUDA(m, m->map_w.alloc(std::max<size_t>(w.size(), 1)));
+  EMG_CUDA(m, m->map_fsum.alloc(m->N));
+  EMG_CUDA(m, cudaMemcpyAsync(m->map_ptr.p, ptr.data(), sizeof(int64_t) * (m->N + 1), cudaMemcpyHostToDevice,
+                              m->stream));
+  if (!src.empty()) {
+    EMG_CUDA(m, cudaMemcpyAsync(m->map_src.p, src.data(), sizeof(int64_t) * src.size(), cudaMemcpyHostToDevice,
+                                m->stream));
+    EMG_CUDA(m, cudaMemcpyAsync(m->map_w.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, m->stream));
+  }
+  EMG_CUDA(m, cudaMemcpyAsync(m->map_fsum.p, fsum.data(), sizeof(double) * m->N, cudaMemcpyHostToDevice, m->stream));
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  m->n_source = n_source;
+  m->n_mapped = mapped;
+  m->default_value = default_value;
+  m->have_map = true;
+  if (n_mapped)
+    *n_mapped = mapped;
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_map_fibers(fdm_emg* m, fdm_solver* s)
+{
+  if (!m || !s || !m->have_map)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_map_fibers: call fdm_emg_set_fiber_mapping first");
+  const double* vm = nullptr;
+  int64_t n = 0;
+  cudaStream_t ss = nullptr;
+  int dev = 0;
+  int rc = fdm::solver_vm_device(s, &vm, &n, &ss, &dev);
+  if (rc)
+    return emg_fail(m, rc, "fdm_emg_map_fibers: the fiber solver has no state");
+  if (dev != m->device || n != m->n_source)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_map_fibers: the fiber solver's device or node count differs from the "
+                                    "mapping's");
+  EMG_BIND(m);
+  // order after the fiber solver's work
+  EMG_CUDA(m, cudaEventRecord(m->ev0, ss));
+  EMG_CUDA(m, cudaStreamWaitEvent(m->stream, m->ev0, 0));
+  map_kernel<<<blocks_for(m->N), EMG_T, 0, m->stream>>>(m->N, m->map_ptr.p, m->map_src.p, m->map_w.p, m->map_fsum.p, vm,
+                                                         m->default_value, m->vm.p);
+  EMG_CUDA(m, cudaGetLastError());
+  // the fiber solver may overwrite Vm only after the transfer
+  EMG_CUDA(m, cudaEventRecord(m->ev1, m->stream));
+  EMG_CUDA(m, cudaStreamWaitEvent(ss, m->ev1, 0));
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_map_values(fdm_emg* m, const double* fiber_values)
+{
+  if (!m || !m->have_map || (m->n_source > 0 && !fiber_values))
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_map_values: call fdm_emg_set_fiber_mapping first");
+  EMG_BIND(m);
+  Buf<double> src;
+  EMG_CUDA(m, src.alloc(std::max<int64_t>(m->n_source, 1)));
+  if (m->n_source > 0)
+    EMG_CUDA(m, cudaMemcpyAsync(src.p, fiber_values, sizeof(double) * m->n_source, cudaMemcpyHostToDevice,
+                                m->stream));
+  map_kernel<<<blocks_for(m->N), EMG_T, 0, m->stream>>>(m->N, m->map_ptr.p, m->map_src.p, m->map_w.p, m->map_fsum.p,
+                                                         src.p, m->default_value, m->vm.p);
+  EMG_CUDA(m, cudaGetLastError());
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_set_vm(fdm_emg* m, const double* vm)
+{
+  if (!m || !vm)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_set_vm: bad argument");
+  EMG_BIND(m);
+  EMG_CUDA(m, cudaMemcpyAsync(m->vm.p, vm, sizeof(double) * m->N, cudaMemcpyHostToDevice, m->stream));
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_solve(fdm_emg* m, double rtol, double atol, int max_iterations, int initial_guess_nonzero,
+                             int* iterations, double* residual)
+{
+  if (!m || !m->have_ops || max_iterations < 1)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_solve: call fdm_emg_set_conductivity first; max_iterations >= 1");
+  EMG_BIND(m);
+  const int64_t N = m->N;
+  const int nb = blocks_for(N);
+  EMG_CUDA(m, cudaEventRecord(m->ev0, m->stream));
+  // rhs = -K(sigma_i) Vm
+  spmv_kernel<<<nb, EMG_T, 0, m->stream>>>(m->hm.g, m->coef_i.p, m->vm.p, m->rhs.p, nullptr, nullptr);
+  negate_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->rhs.p);
+  inverse_diag_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->diag_ie.p, nullptr, m->dinv.p);
+  if (!initial_guess_nonzero)
+    EMG_CUDA(m, cudaMemsetAsync(m->phi.p, 0, sizeof(double) * N, m->stream));
+  int its = 0;
+  double res = 0.0;
+  int rc = cg_solve(m, m->coef_ie.p, nullptr, true, m->rhs.p, m->phi.p, rtol, atol, max_iterations, &its, &res);
+  if (rc)
+    return rc;
+  EMG_CUDA(m, cudaEventRecord(m->ev1, m->stream));
+  EMG_CUDA(m, cudaEventSynchronize(m->ev1));
+  EMG_CUDA(m, cudaEventElapsedTime(&m->last_solve_ms, m->ev0, m->ev1));
+  m->last_iterations = its;
+  m->last_residual = res;
+  if (iterations)
+    *iterations = its;
+  if (residual)
+    *residual = res;
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_get(fdm_emg* m, int field, double* out)
+{
+  if (!m || !out)
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_get: bad argument");
+  EMG_BIND(m);
+  const double* src = nullptr;
+  int64_t n = m->N;
+  switch (field) {
+  case FDM_EMG_PHI_E: src = m->phi.p; break;
+  case FDM_EMG_VM: src = m->vm.p; break;
+  case FDM_EMG_RHS: src = m->rhs.p; break;
+  case FDM_EMG_FLOW_POTENTIAL: src = m->flow.p; break;
+  case FDM_EMG_DIRECTION: src = m->dir.p; n = 3 * m->N; break;
+  default: return emg_fail(m, FDM_ERR_ARG, "fdm_emg_get: unknown field");
+  }
+  EMG_CUDA(m, cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, m->stream));
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_get_stencil(fdm_emg* m, int which, double* out)
+{
+  if (!m || !out || !m->have_ops || (which != 0 && which != 1))
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_get_stencil: operators not assembled or bad argument");
+  EMG_BIND(m);
+  EMG_CUDA(m, cudaMemcpyAsync(out, which == 0 ? m->coef_i.p : m->coef_ie.p, sizeof(double) * 27 * m->N,
+                              cudaMemcpyDeviceToHost, m->stream));
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_timing(const fdm_emg* m, double* last_solve_ms, int* last_iterations, double* last_residual)
+{
+  if (!m)
+    return FDM_ERR_ARG;
+  if (last_solve_ms)
+    *last_solve_ms = m->last_solve_ms;
+  if (last_iterations)
+    *last_iterations = m->last_iterations;
+  if (last_residual)
+    *last_residual = m->last_residual;
+  return FDM_OK;
+}

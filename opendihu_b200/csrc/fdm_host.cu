@@ -1428,6 +1428,19 @@ extern "C" int fdm_get_equilibrium_state(fdm_solver* s, int64_t* n_buffers, uint
   return FDM_OK;
 }
 
+namespace fdm {
+int solver_vm_device(fdm_solver* s, const double** vm, int64_t* n_nodes, cudaStream_t* stream, int* device)
+{
+  if (!s || !s->vm.p)
+    return FDM_ERR_ARG;
+  *vm = s->vm.p;
+  *n_nodes = s->n_nodes;
+  *stream = s->stream;
+  *device = s->cfg.device;
+  return FDM_OK;
+}
+} // namespace fdm
+
 extern "C" int fdm_get_compute_state_information(fdm_solver* s, double* out)
 {
   if (!s || (!out && s->n_nodes > 0) || !s->stimulation_set)

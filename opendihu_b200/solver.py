@@ -76,6 +76,8 @@ class FiberSystem:
     # the diffusion solver has one more additional field variable than algebraicsForTransfer: the
     # "computeStateInformation" slot is transferred too (initialization.tpp:572-587)
     compute_state_information: bool = False
+    # names of the fibers' meshes in the settings ("Meshes"), in fiber order (for their node positions)
+    fiber_mesh_names: Sequence[str] = ()
 
     @property
     def n_fibers(self) -> int:
@@ -298,6 +300,7 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         algebraics_for_transfer=[int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))],
         states_for_transfer=[int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))] or [0],
         only_compute_if_has_been_stimulated=only_if_stimulated, skip_close_to_equilibrium=skip_equilibrium)
+    sys_.fiber_mesh_names = [fb["fem"].get("meshName", fb["cellml"].get("meshName")) for fb in fibers]
     sys_.compute_state_information = \
         int(f0["diff"].get("nAdditionalFieldVariables", 0)) > len(sys_.algebraics_for_transfer)
     sys_.method = b200.get("method", "split")

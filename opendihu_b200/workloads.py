@@ -82,3 +82,39 @@ def hh_parameters(system: FiberSystem, s_na, s_k, i_stim: float = 0.0) -> np.nda
     p[1] = np.repeat(120.0 * np.asarray(s_na), lengths)
     p[2] = np.repeat(36.0 * np.asarray(s_k), lengths)
     return p
+
+
+# fibers_emg conductivities (settings_fibers_emg.py "Activation"): sigma_i in fiber coordinates, sigma_e
+EMG_SIGMA_I = (8.93, 0.0, 0.0, 0.0, 0.893, 0.0, 0.0, 0.0, 0.893)
+EMG_SIGMA_E = (6.7, 0.0, 0.0, 0.0, 6.7, 0.0, 0.0, 0.0, 6.7)
+
+
+def emg_box(n_fibers_x: int = 13, n_fibers_y: int = 13, n_nodes: int = 1481, mesh_nodes=(25, 25, 149),
+            width: float = 3.0, end_time: float = 10.0, n_mus: int = 10, seed: int = 0, **kw):
+    """Fibers + EMG configuration in the shape of the fibers_emg example: a muscle box of width x width x
+    (n_nodes - 1) * 0.01 cm with a grid of n_fibers_x x n_fibers_y HH fibers along z (dx 0.01 cm, seeded
+    MU assignment and Poisson firing as batched_hh), a structured 3D mesh of mesh_nodes nodes over the box,
+    potential-flow Dirichlet values 0 on the bottom face and 1 on the top face, the example's sigma_i and
+    sigma_e.  Returns (system, fiber node positions [n, 3], StaticBidomainSolver keyword arguments)."""
+    nf = n_fibers_x * n_fibers_y
+    length = (n_nodes - 1) * 0.01
+    mus = inputs.exponential_mu_distribution(nf, n_mus, seed)
+    firing = inputs.poisson_firing_times(n_mus, end_time, 0.1, 10.0, 40.0, seed)
+    system = uniform_fibers(HH, [n_nodes] * nf, 0.01, SIGMA / (AM * CM), firing_events=firing, motor_unit_no=mus,
+                            call_frequency=0.1, repeat_after_first_call=0.1, call_enable_begin=0.0,
+                            end_time=end_time, dt_0d=1e-4, dt_1d=1e-3, dt_splitting=1e-3, dt_repeated_call=1e-3, **kw)
+    fx = (np.arange(n_fibers_x) + 0.5) * width / n_fibers_x
+    fy = (np.arange(n_fibers_y) + 0.5) * width / n_fibers_y
+    z = np.arange(n_nodes) * 0.01
+    pos = np.concatenate([np.stack([np.full(n_nodes, x), np.full(n_nodes, y), z], axis=1)
+                          for y in fy for x in fx])
+    nx, ny, nz = mesh_nodes
+    xs, ys, zs = np.linspace(0, width, nx), np.linspace(0, width, ny), np.linspace(0, length, nz)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    mesh = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    bottom = np.arange(nx * ny)
+    top = np.arange(nx * ny) + nx * ny * (nz - 1)
+    emg = dict(shape=(nx, ny, nz), node_positions=mesh, sigma_i=EMG_SIGMA_I, sigma_e=EMG_SIGMA_E,
+               dirichlet_nodes=np.concatenate([bottom, top]),
+               dirichlet_values=np.concatenate([np.zeros(nx * ny), np.ones(nx * ny)]))
+    return system, pos, emg

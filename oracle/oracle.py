@@ -179,6 +179,7 @@ class OracleRun:
         self.eq_status = np.full(max(sum(n_buf), 1), 2, np.uint8)
         self.eq_counter = np.zeros(R, np.int32)
         ns = model_info(spec["model"])[0]
+        self.n_states = ns
         init = model_info(spec["model"])[3]
         self.pad_states = np.tile(init, R * W).astype(np.float64)
         p.eq_status = _p(self.eq_status, C.c_uint8)
@@ -203,6 +204,8 @@ class OracleRun:
     def run(self, states: np.ndarray, t_start: Optional[float] = None, t_end: Optional[float] = None) -> int:
         """Advance the SoA states [s][node] in place; returns the number of split steps."""
         assert states.dtype == np.float64 and states.flags.c_contiguous
+        if states.shape != (self.n_states, self.n_nodes):
+            raise ValueError(f"oracle run: states must be [{self.n_states}, {self.n_nodes}], got {states.shape}")
         if t_start is not None:
             self.p.t_start = t_start
         if t_end is not None:

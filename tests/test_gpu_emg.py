@@ -1,0 +1,169 @@
+"""Fibers -> 3D static bidomain (EMG) on the GPU against the oracle (oracle/emg_oracle.py): the potential flow
+and fiber directions on a deformed mesh, the assembled stencils (one tensor for all elements and one per
+element), the fiber -> mesh transfer (host values and straight from the fiber solver's device Vm), phi_e,
+phi_e = -(Vm - mean Vm) without extracellular conduction at a larger size, and the Coupling driven from a
+reference-shaped settings dict against the oracles of both solvers."""
+import numpy as np
+import pytest
+
+import helpers as H
+from oracle import emg_oracle as EO
+from opendihu_b200 import emg as E
+from opendihu_b200 import solver as S
+from opendihu_b200 import workloads as WL
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = {"relativeTolerance": 1e-13, "absoluteTolerance": 1e-30, "maxIterations": 20000}
+
+
+def _deformed_mesh(shape=(6, 5, 9), ext=(1.0, 0.8, 2.0), seed=3):
+    rng = np.random.default_rng(seed)
+    pos = EO.box_mesh(shape, ext)
+    # a smooth bend (the fibers' direction varies) plus small random jitter
+    pos[:, 0] += 0.15 * np.sin(pos[:, 2] / ext[2] * np.pi)
+    pos += rng.uniform(-0.02, 0.02, size=pos.shape)
+    nx, ny, nz = shape
+    lo = np.arange(nx * ny)
+    hi = lo + nx * ny * (nz - 1)
+    return shape, pos, np.concatenate([lo, hi]), np.r_[np.zeros(nx * ny), np.ones(nx * ny)]
+
+
+def _solver(shape, pos, bn, bv, **kw):
+    kw.setdefault("sigma_i", WL.EMG_SIGMA_I)
+    kw.setdefault("sigma_e", WL.EMG_SIGMA_E)
+    return E.StaticBidomainSolver(shape, pos, dirichlet_nodes=bn, dirichlet_values=bv,
+                                  potential_flow_solver=TIGHT, emg_solver=TIGHT, **kw)
+
+
+@pytest.mark.parametrize("per_element", [False, True])
+def test_potential_flow_stencils_and_phi_match_oracle(per_element):
+    shape, pos, bn, bv = _deformed_mesh()
+    ne = (shape[0] - 1) * (shape[1] - 1) * (shape[2] - 1)
+    rng = np.random.default_rng(4)
+    si = np.asarray(WL.EMG_SIGMA_I, float).reshape(3, 3)
+    se = np.asarray(WL.EMG_SIGMA_E, float).reshape(3, 3)
+    if per_element:
+        si = si[None] * rng.uniform(0.5, 1.5, size=(ne, 1, 1))
+        se = se[None] * rng.uniform(0.5, 1.5, size=(ne, 1, 1))
+    u_ref, d_ref = EO.potential_flow(pos, shape, bn, bv, gauss=3)
+    Ki = EO.stiffness(pos, shape, si, 5, direction=d_ref)
+    Kie = EO.stiffness(pos, shape, si, 5, direction=d_ref, tensors2=se)
+    vm = rng.normal(-70.0, 20.0, size=len(pos))
+    phi_ref, rhs_ref = EO.bidomain(Ki, Kie, vm)
+    with _solver(shape, pos, bn, bv, sigma_i=si.reshape(-1, 9), sigma_e=se.reshape(-1, 9)) as slv:
+        np.testing.assert_allclose(slv.flow_potential(), u_ref, rtol=0, atol=1e-11)
+        np.testing.assert_allclose(slv.fiber_direction(), d_ref, rtol=0, atol=1e-10)
+        for which, K in ((0, Ki), (1, Kie)):
+            got = EO.stencil_to_sparse(slv.stencil(which), shape)
+            assert abs(got - K).max() <= 1e-9 * abs(K).max()
+        slv.set_vm(vm)
+        its = slv.advanceTimeSpan()
+        assert its > 0
+        np.testing.assert_allclose(slv.rhs(), rhs_ref, rtol=0, atol=1e-8 * np.abs(rhs_ref).max())
+        phi = slv.phi_e()
+    assert abs(phi.mean()) < 1e-10
+    np.testing.assert_allclose(phi, phi_ref, rtol=0, atol=1e-8 * np.abs(phi_ref).max())
+
+
+def test_mapping_matches_oracle_and_device_transfer():
+    s, fpos, kw = WL.emg_box(n_fibers_x=3, n_fibers_y=2, n_nodes=61, mesh_nodes=(4, 3, 7), width=1.0, end_time=0.3)
+    fpos = fpos.copy()
+    fpos[5] = [9.0, 9.0, 9.0]                       # one fiber node outside the mesh
+    el, fac = EO.fiber_mapping(kw["node_positions"], kw["shape"], fpos)
+    vals = np.random.default_rng(5).normal(size=len(fpos))
+    want = EO.map_values(kw["node_positions"], kw["shape"], el, fac, vals, default_value=-7.0)
+    with E.StaticBidomainSolver(**kw) as slv:
+        assert slv.set_fiber_mapping(fpos, default_value=-7.0) == len(fpos) - 1
+        slv.map_values(vals)
+        np.testing.assert_allclose(slv.vm(), want, rtol=0, atol=1e-12)
+        # straight from the fiber solver's device Vm, after an advance
+        with S.FastMonodomainSolver(H.complete(s.copy()), method="fused") as fib:
+            fib.advanceTimeSpan()
+            slv.map_fibers(fib)
+            got = slv.vm()
+            vm_f = fib.states()[0]
+        np.testing.assert_allclose(got, EO.map_values(kw["node_positions"], kw["shape"], el, fac, vm_f, -7.0),
+                                   rtol=0, atol=1e-12)
+
+
+def test_no_extracellular_conduction_at_size():
+    s, fpos, kw = WL.emg_box(n_fibers_x=2, n_fibers_y=2, n_nodes=101, mesh_nodes=(33, 33, 65), width=1.0)
+    kw["sigma_e"] = np.zeros(9)
+    rng = np.random.default_rng(6)
+    vm = rng.normal(size=33 * 33 * 65)
+    with E.StaticBidomainSolver(emg_solver=TIGHT, potential_flow_solver=TIGHT, **kw) as slv:
+        np.testing.assert_allclose(slv.fiber_direction(), np.tile([0, 0, 1.0], (33 * 33 * 65, 1)), atol=1e-9)
+        slv.set_vm(vm)
+        slv.advanceTimeSpan()
+        phi = slv.phi_e()
+        t = slv.timing()
+    np.testing.assert_allclose(phi, -(vm - vm.mean()), rtol=0, atol=1e-7)
+    assert t["iterations"] > 0 and t["solve_ms"] > 0
+
+
+def _settings(n_fx=2, n_fy=2, n_nodes=41, mesh=(4, 4, 6), width=1.0, dt3d=0.5, end=1.0):
+    s, fpos, kw = WL.emg_box(n_fibers_x=n_fx, n_fibers_y=n_fy, n_nodes=n_nodes, mesh_nodes=mesh, width=width,
+                             end_time=end)
+    nf = n_fx * n_fy
+    names = [f"MeshFiber_{i}" for i in range(nf)]
+    meshes = {n: {"nElements": [n_nodes - 1], "nodePositions": fpos[i * n_nodes:(i + 1) * n_nodes].tolist()}
+              for i, n in enumerate(names)}
+    nx, ny, nz = mesh
+    meshes["3Dmesh"] = {"nElements": [nx - 1, ny - 1, nz - 1], "physicalExtent": [width, width, (n_nodes - 1) * 0.01]}
+    heun = [{"Heun": {"timeStepWidth": 1e-4, "CellML": {
+        "modelFilename": "hodgkin_huxley_1952.c", "setSpecificStatesCallFrequency": 0.1,
+        "setSpecificStatesRepeatAfterFirstCall": 0.1, "setSpecificStatesCallEnableBegin": 0.0,
+        "parametersUsedAsAlgebraic": [], "parametersUsedAsConstant": [2, 3, 4],
+        "parametersInitialValues": [0.0, 120.0, 36.0], "meshName": n}}} for n in names]
+    diff = [{"ImplicitEuler": {"timeStepWidth": 1e-3, "FiniteElementMethod": {
+        "meshName": n, "prefactor": WL.SIGMA / (WL.AM * WL.CM)}}} for n in names]
+    strang = {"StrangSplitting": {"timeStepWidth": 1e-3, "Term1": {"MultipleInstances": {"instances": heun}},
+                                  "Term2": {"MultipleInstances": {"instances": diff}}}}
+    bc = {int(k): 0.0 for k in range(nx * ny)}
+    bc.update({int(k) - nx * ny: 1.0 for k in range(nx * ny)})      # negative: counted from the end
+    fem = {"meshName": "3Dmesh", "prefactor": 1.0, "solverName": "muscularEMGSolver",
+           "diffusionTensor": [list(WL.EMG_SIGMA_I)], "extracellularDiffusionTensor": [list(WL.EMG_SIGMA_E)]}
+    cfg = {
+        "Meshes": meshes,
+        "Solvers": {"potentialFlowSolver": TIGHT, "muscularEMGSolver": TIGHT},
+        "MappingsBetweenMeshes": {n: ["3Dmesh"] for n in names},
+        "Coupling": {
+            "timeStepWidth": dt3d, "endTime": end, "connectedSlotsTerm1To2": {0: 0}, "connectedSlotsTerm2To1": [None],
+            "Term1": {"MultipleInstances": {"instances": [strang]}, "onlyComputeIfHasBeenStimulated": False,
+                      "disableComputationWhenStatesAreCloseToEquilibrium": False},
+            "Term2": {"StaticBidomainSolver": {
+                "timeStepWidth": dt3d, "solverName": "muscularEMGSolver", "initialGuessNonzero": True,
+                "PotentialFlow": {"FiniteElementMethod": {"meshName": "3Dmesh", "solverName": "potentialFlowSolver",
+                                                          "prefactor": 1.0, "dirichletBoundaryConditions": bc}},
+                "Activation": {"FiniteElementMethod": fem}}},
+        },
+    }
+    return cfg, fpos, kw
+
+
+def test_coupling_from_settings_matches_oracles():
+    cfg, fpos, kw = _settings()
+    phis = []
+    cp = E.Coupling.from_settings(cfg)
+    cp.callback = lambda k, t, emg: phis.append((t, emg.phi_e()))
+    with cp:
+        assert cp.n_mapped == len(fpos)
+        cp.run()
+        system = cp.term1.system
+    assert [round(t, 9) for t, _ in phis] == [0.5, 1.0]
+    # oracle chain: fibers to 0.5 and 1.0 ms, mapped, bidomain
+    shape, pos = kw["shape"], kw["node_positions"]
+    u, d = EO.potential_flow(pos, shape, kw["dirichlet_nodes"], kw["dirichlet_values"], gauss=3)
+    si = np.asarray(WL.EMG_SIGMA_I).reshape(3, 3)
+    Ki = EO.stiffness(pos, shape, si, 5, direction=d)
+    Kie = EO.stiffness(pos, shape, si, 5, direction=d, tensors2=np.asarray(WL.EMG_SIGMA_E).reshape(3, 3))
+    el, fac = EO.fiber_mapping(pos, shape, fpos)
+    sysc = H.complete(system.copy())
+    run = H.O.OracleRun(H.oracle_spec(sysc.copy()))
+    st = np.ascontiguousarray(sysc.states, np.float64).copy()
+    for (t, phi), (a, b) in zip(phis, [(0.0, 0.5), (0.5, 1.0)]):
+        run.run(st, a, b)
+        want, _ = EO.bidomain(Ki, Kie, EO.map_values(pos, shape, el, fac, st[0]))
+        assert np.max(np.abs(phi - want)) <= 1e-6 * max(np.abs(want).max(), 1.0)
+    assert np.abs(phis[-1][1]).max() > 0
