@@ -208,8 +208,7 @@ struct AssembleArgs {
   int64_t n_tensor, n_tensor2;
   double prefactor;
   Quad q;
-  double* coef;            // [27][N]
-  double* diag;            // [N] (may be null)
+  double* coef;            // [EMG_NC][N]: the centre and forward coefficients of each row
 };
 
 // row of node n of the assembled stiffness matrix: the sum over its adjacent elements (in element order) of the
@@ -278,10 +277,9 @@ __global__ void __launch_bounds__(128) assemble_kernel(AssembleArgs a)
                 }
               }
         }
-    for (int q = 0; q < 27; q++)
-      a.coef[q * N + n] = row[q];
-    if (a.diag)
-      a.diag[n] = row[13];
+    // the centre and forward half (the backward half equals the neighbours' forward entries: K is symmetric)
+    for (int q = 13; q < 27; q++)
+      a.coef[(q - 13) * N + n] = row[q];
   }
 }
 
@@ -335,207 +333,256 @@ __global__ void gradient_direction_kernel(Grid g, const double* pos, const doubl
   }
 }
 
-// y = A x on the 27-point stencil; rows with mask[n] set give y = 0 (Dirichlet rows); partial[block] = sum p.y
-// when dot is set
-__global__ void __launch_bounds__(EMG_T) spmv_kernel(Grid g, const double* __restrict__ coef,
-                                                     const double* __restrict__ x, double* __restrict__ y,
-                                                     const unsigned char* __restrict__ mask, double* partial)
+// ---- symmetric stencil storage and the conjugate-gradient kernels ----------------------------------------
+// K is symmetric: only the centre and the 13 forward coefficients of each row are stored,
+// U[k * N + n] = K[n][n + off(13 + k)] for stencil index q = 13 + k = (dx+1) + 3(dy+1) + 9(dz+1) >= 13; the
+// backward entry K[n][n - off(q)] is the forward entry U[q - 13][n - off(q)] of the neighbour.
+constexpr int EMG_NC = 14;
+
+__host__ __device__ inline void stencil_offset(int q, int& dx, int& dy, int& dz)
 {
-  __shared__ double red[EMG_T / 32];
+  dx = q % 3 - 1;
+  dy = (q / 3) % 3 - 1;
+  dz = q / 9 - 1;
+}
+
+// Row n of K applied to the vector v(m).  The assembly leaves the coefficient of a neighbour outside the grid
+// at exactly 0, and every forward offset is positive in the linear numbering, so no bounds test is needed on
+// the coefficients: a forward coefficient towards a missing neighbour is 0, and the forward coefficient
+// U[q][n - off] of a node whose forward neighbour is not n (a wrap-around in the numbering) is 0 too; only
+// n - off < 0 is cut off.  The loads are then unconditional and issue together; v is read at clamped indices
+// (its values there meet a 0 coefficient and must only be finite).
+template<class V>
+__device__ __forceinline__ double stencil_row(const Grid& g, const double* __restrict__ U, int64_t n, V v)
+{
   const int64_t N = g.n_nodes();
-  const int64_t sx = 1, sy = g.nx, sz = (int64_t)g.nx * g.ny;
-  double acc = 0.0;
+  const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
+  double s = U[n] * v(n);
+#pragma unroll
+  for (int q = 14; q < 27; q++) {
+    int dx, dy, dz;
+    stencil_offset(q, dx, dy, dz);
+    const int64_t off = dx + dy * sy + dz * sz;
+    const int64_t f = min(n + off, N - 1), b = n - off;
+    const double cb = b >= 0 ? U[(q - 13) * N + b] : 0.0;
+    s += U[(q - 13) * N + n] * v(f) + cb * v(max(b, (int64_t)0));
+  }
+  return s;
+}
+
+// Grid-wide sums of K values per thread: each block writes its partials, the block that finishes last sums
+// all partials in block order (a fixed order: results do not depend on scheduling) and returns true in its
+// thread 0 with the totals in tot; the counter is reset for the next launch.
+template<int K>
+__device__ bool grid_sum(double (&v)[K], double* partial, unsigned* counter, double (&tot)[K])
+{
+  __shared__ double red[K][EMG_T / 32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < K; c++) {
+    double a = v[c];
+    for (int o = 16; o > 0; o >>= 1)
+      a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0)
+      red[c][warp] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < K; c++) {
+      double t = 0.0;
+      for (int w = 0; w < EMG_T / 32; w++)
+        t += red[c][w];
+      partial[c * EMG_MAX_BLOCKS + blockIdx.x] = t;
+    }
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last)
+    return false;
+  __threadfence();
+#pragma unroll
+  for (int c = 0; c < K; c++) {
+    double a = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += EMG_T)
+      a += __ldcg(&partial[c * EMG_MAX_BLOCKS + b]);
+    for (int o = 16; o > 0; o >>= 1)
+      a += __shfl_down_sync(0xffffffffu, a, o);
+    __syncthreads();
+    if (lane == 0)
+      red[c][warp] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0)
+    return false;
+#pragma unroll
+  for (int c = 0; c < K; c++) {
+    double t = 0.0;
+    for (int w = 0; w < EMG_T / 32; w++)
+      t += red[c][w];
+    tot[c] = t;
+  }
+  *counter = 0u;
+  return true;
+}
+
+// CG scalars in device memory: S[0] r.z, S[1] p.Ap, S[3] r.r, S[4] alpha, S[5] beta, S[6] sum, S[7] b.b
+enum { CG_RZ = 0, CG_PQ = 1, CG_RR = 3, CG_ALPHA = 4, CG_BETA = 5, CG_SUM = 6, CG_BB = 7 };
+
+// y = scale * K x
+__global__ void __launch_bounds__(EMG_T) apply_kernel(Grid g, const double* __restrict__ U,
+                                                      const double* __restrict__ x, double* __restrict__ y,
+                                                      double scale)
+{
+  const int64_t N = g.n_nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+    y[n] = scale * stencil_row(g, U, n, [&](int64_t m) { return x[m]; });
+}
+
+// r = b - K x (rows in mask: r = 0), z = dinv r; S[RZ], S[RR]; beta = 0 for the first direction
+__global__ void __launch_bounds__(EMG_T, 4) cg_init_kernel(Grid g, const double* __restrict__ U,
+                                                        const unsigned char* __restrict__ mask,
+                                                        const double* __restrict__ b, const double* __restrict__ x,
+                                                        double* r, double* z, const double* __restrict__ dinv,
+                                                        double* S, double* partial, unsigned* counter)
+{
+  const int64_t N = g.n_nodes();
+  double acc[2] = {0.0, 0.0}, tot[2];
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / sz);
-    double s = 0.0;
-    if (!(mask && mask[n])) {
-#pragma unroll
-      for (int dz = -1; dz <= 1; dz++) {
-        if (k + dz < 0 || k + dz >= g.nz)
-          continue;
-#pragma unroll
-        for (int dy = -1; dy <= 1; dy++) {
-          if (j + dy < 0 || j + dy >= g.ny)
-            continue;
-#pragma unroll
-          for (int dx = -1; dx <= 1; dx++) {
-            if (i + dx < 0 || i + dx >= g.nx)
-              continue;
-            const int q = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-            s += coef[q * N + n] * x[n + dx * sx + dy * sy + dz * sz];
-          }
-        }
-      }
-    }
-    y[n] = s;
-    acc += x[n] * s;
+    const bool fixed = mask && mask[n];
+    const double rn = fixed ? 0.0 : b[n] - stencil_row(g, U, n, [&](int64_t m) { return x[m]; });
+    const double zn = rn * dinv[n];
+    r[n] = rn;
+    z[n] = zn;
+    acc[0] += rn * zn;
+    acc[1] += rn * rn;
   }
-  if (partial) {
-    for (int o = 16; o > 0; o >>= 1)
-      acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0)
-      red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < EMG_T / 32; w++)
-        t += red[w];
-      partial[blockIdx.x] = t;
-    }
+  if (grid_sum<2>(acc, partial, counter, tot)) {
+    S[CG_RZ] = tot[0];
+    S[CG_RR] = tot[1];
+    S[CG_BETA] = 0.0;
   }
 }
 
-// sums nb partials of each of k rows (partial[r * EMG_MAX_BLOCKS + b]) in a fixed order into out[r]
-__global__ void reduce_kernel(const double* partial, int nb, int k, double* out)
+// The nine rows (dy, dz in {-1, 0, 1}) of z around the block's EMG_T consecutive nodes [n0, n0 + EMG_T), one
+// node of halo each side, staged in shared memory: neighbour (dx, dy, dz) of node n0 + t is
+// sv[(dy+1) + 3(dz+1)][t + 1 + dx].  Every global load is a coalesced row segment.
+__device__ __forceinline__ void stage_rows(const Grid& g, const double* __restrict__ z, int64_t n0,
+                                           double (*sv)[EMG_T + 2])
 {
-  __shared__ double red[EMG_T / 32];
-  for (int r = 0; r < k; r++) {
-    double acc = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x)
-      acc += partial[r * EMG_MAX_BLOCKS + b];
-    for (int o = 16; o > 0; o >>= 1)
-      acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0)
-      red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < EMG_T / 32; w++)
-        t += red[w];
-      out[r] = t;
-    }
-    __syncthreads();
+  const int64_t N = g.n_nodes();
+  for (int e = threadIdx.x; e < 9 * (EMG_T + 2); e += EMG_T) {
+    const int r = e / (EMG_T + 2), t = e % (EMG_T + 2);
+    const int dy = r % 3 - 1, dz = r / 3 - 1;
+    const int64_t m = n0 + dy * (int64_t)g.nx + dz * (int64_t)g.nx * g.ny + t - 1;
+    sv[r][t] = (m >= 0 && m < N) ? z[m] : 0.0;
   }
 }
 
-// CG scalars on the device: s[0] = r.z, s[1] = p.Ap, s[2] = r.z new, s[3] = r.r, s[4] = alpha, s[5] = beta
-__global__ void update_kernel(int64_t N, double* x, double* r, double* z, const double* p, const double* q,
-                              const double* dinv, const double* s, double* partial)
+// stencil_row with the neighbours' values from the staged rows (the same zero-coefficient argument)
+__device__ __forceinline__ double stencil_row_staged(const Grid& g, const double* __restrict__ U, int64_t n, int t,
+                                                     const double (*sv)[EMG_T + 2])
 {
-  __shared__ double red[2][EMG_T / 32];
-  const double alpha = s[1] != 0.0 ? s[0] / s[1] : 0.0;
-  double rz = 0.0, rr = 0.0;
+  const int64_t N = g.n_nodes();
+  const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
+  double s = U[n] * sv[4][t + 1];
+#pragma unroll
+  for (int q = 14; q < 27; q++) {
+    int dx, dy, dz;
+    stencil_offset(q, dx, dy, dz);
+    const int64_t b = n - (dx + dy * sy + dz * sz);
+    const double cb = b >= 0 ? U[(q - 13) * N + b] : 0.0;
+    s += U[(q - 13) * N + n] * sv[(dy + 1) + 3 * (dz + 1)][t + 1 + dx] + cb * sv[(1 - dy) + 3 * (1 - dz)][t + 1 - dx];
+  }
+  return s;
+}
+
+// Direction and product in one pass (the Chronopoulos-Gear arrangement of CG): w = K z, p = z + beta p,
+// q = w + beta q (= K p), so that only z is read around each node; alpha = r.z / p.q.  p and q start at 0.
+__global__ void __launch_bounds__(EMG_T, 4) cg_direction_kernel(Grid g, const double* __restrict__ U,
+                                                                const unsigned char* __restrict__ mask,
+                                                                const double* __restrict__ z, double* __restrict__ p,
+                                                                double* __restrict__ q, double* S, double* partial,
+                                                                unsigned* counter)
+{
+  __shared__ double sv[9][EMG_T + 2];
+  const int64_t N = g.n_nodes();
+  const double beta = S[CG_BETA];
+  double acc[1] = {0.0}, tot[1];
+  for (int64_t n0 = (int64_t)blockIdx.x * EMG_T; n0 < N; n0 += (int64_t)gridDim.x * EMG_T) {
+    stage_rows(g, z, n0, sv);
+    __syncthreads();
+    const int64_t n = n0 + threadIdx.x;
+    if (n < N) {
+      const double w = (mask && mask[n]) ? 0.0 : stencil_row_staged(g, U, n, threadIdx.x, sv);
+      const double pn = z[n] + beta * p[n];
+      const double qn = w + beta * q[n];
+      p[n] = pn;
+      q[n] = qn;
+      acc[0] += pn * qn;
+    }
+    __syncthreads();
+  }
+  if (grid_sum<1>(acc, partial, counter, tot)) {
+    S[CG_PQ] = tot[0];
+    S[CG_ALPHA] = tot[0] != 0.0 ? S[CG_RZ] / tot[0] : 0.0;
+  }
+}
+
+// x += alpha p, r -= alpha q, z = dinv r; beta = r.z new / r.z
+__global__ void __launch_bounds__(EMG_T) cg_update_kernel(int64_t N, double* __restrict__ x, double* __restrict__ r,
+                                                          double* __restrict__ z, const double* __restrict__ p,
+                                                          const double* __restrict__ q,
+                                                          const double* __restrict__ dinv, double* S, double* partial,
+                                                          unsigned* counter)
+{
+  const double alpha = S[CG_ALPHA];
+  double acc[2] = {0.0, 0.0}, tot[2];
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
     x[n] += alpha * p[n];
     const double rn = r[n] - alpha * q[n];
-    r[n] = rn;
     const double zn = rn * dinv[n];
-    z[n] = zn;
-    rz += rn * zn;
-    rr += rn * rn;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    rz += __shfl_down_sync(0xffffffffu, rz, o);
-    rr += __shfl_down_sync(0xffffffffu, rr, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = rz;
-    red[1][threadIdx.x >> 5] = rr;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int w = 0; w < EMG_T / 32; w++) {
-      a += red[0][w];
-      b += red[1][w];
-    }
-    partial[blockIdx.x] = a;
-    partial[EMG_MAX_BLOCKS + blockIdx.x] = b;
-  }
-}
-
-// p = z + (rz_new / rz) p; then rz = rz_new
-__global__ void direction_kernel(int64_t N, double* p, const double* z, const double* s)
-{
-  const double beta = s[0] != 0.0 ? s[2] / s[0] : 0.0;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
-    p[n] = z[n] + beta * p[n];
-}
-
-__global__ void shift_scalar_kernel(double* s)
-{
-  s[0] = s[2];
-}
-
-// r = b - y, z = dinv r, p = z; partials of r.z and r.r
-__global__ void init_residual_kernel(int64_t N, const double* b, const double* y, double* r, double* z, double* p,
-                                     const double* dinv, double* partial)
-{
-  __shared__ double red[2][EMG_T / 32];
-  double rz = 0.0, rr = 0.0;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
-    const double rn = b[n] - y[n];
     r[n] = rn;
-    const double zn = rn * dinv[n];
     z[n] = zn;
-    p[n] = zn;
-    rz += rn * zn;
-    rr += rn * rn;
+    acc[0] += rn * zn;
+    acc[1] += rn * rn;
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    rz += __shfl_down_sync(0xffffffffu, rz, o);
-    rr += __shfl_down_sync(0xffffffffu, rr, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = rz;
-    red[1][threadIdx.x >> 5] = rr;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0, c = 0.0;
-    for (int w = 0; w < EMG_T / 32; w++) {
-      a += red[0][w];
-      c += red[1][w];
-    }
-    partial[blockIdx.x] = a;
-    partial[EMG_MAX_BLOCKS + blockIdx.x] = c;
+  if (grid_sum<2>(acc, partial, counter, tot)) {
+    S[CG_BETA] = S[CG_RZ] != 0.0 ? tot[0] / S[CG_RZ] : 0.0;
+    S[CG_RZ] = tot[0];
+    S[CG_RR] = tot[1];
   }
 }
 
-// partial sums of x (for the mean) and of b.b
-__global__ void sum_kernel(int64_t N, const double* x, const double* b, double* partial)
+// S[SUM] = sum x, S[BB] = b.b (b may be null)
+__global__ void __launch_bounds__(EMG_T) sum_kernel(int64_t N, const double* __restrict__ x,
+                                                    const double* __restrict__ b, double* S, double* partial,
+                                                    unsigned* counter)
 {
-  __shared__ double red[2][EMG_T / 32];
-  double sx = 0.0, bb = 0.0;
+  double acc[2] = {0.0, 0.0}, tot[2];
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
-    sx += x[n];
+    acc[0] += x[n];
     if (b)
-      bb += b[n] * b[n];
+      acc[1] += b[n] * b[n];
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    sx += __shfl_down_sync(0xffffffffu, sx, o);
-    bb += __shfl_down_sync(0xffffffffu, bb, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = sx;
-    red[1][threadIdx.x >> 5] = bb;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0, c = 0.0;
-    for (int w = 0; w < EMG_T / 32; w++) {
-      a += red[0][w];
-      c += red[1][w];
-    }
-    partial[blockIdx.x] = a;
-    partial[EMG_MAX_BLOCKS + blockIdx.x] = c;
+  if (grid_sum<2>(acc, partial, counter, tot)) {
+    S[CG_SUM] = tot[0];
+    S[CG_BB] = tot[1];
   }
 }
 
-__global__ void subtract_mean_kernel(int64_t N, double* x, const double* sum)
+// y = x - mean(x) (x may equal y)
+__global__ void subtract_mean_kernel(int64_t N, const double* x, double* y, const double* S)
 {
-  const double m = sum[0] / (double)N;
+  const double m = S[CG_SUM] / (double)N;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
-    x[n] -= m;
+    y[n] = x[n] - m;
 }
 
-__global__ void negate_kernel(int64_t N, double* x)
-{
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
-    x[n] = -x[n];
-}
-
-__global__ void inverse_diag_kernel(int64_t N, const double* diag, const unsigned char* mask, double* dinv)
+__global__ void inverse_diag_kernel(int64_t N, const double* diag /* the centre coefficients */,
+                                    const unsigned char* mask, double* dinv)
 {
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
     dinv[n] = (mask && mask[n]) ? 0.0 : (diag[n] != 0.0 ? 1.0 / diag[n] : 1.0);
@@ -614,9 +661,12 @@ struct fdm_emg {
   cudaStream_t stream = nullptr;
   HostMesh hm;
   int64_t N = 0;
-  Buf<double> pos, dir, flow, coef_i, coef_ie, coef_lap, diag_ie, diag_lap, dinv, vm, rhs, phi, r, z, p, q, partial,
+  // stencils U (EMG_NC coefficients per node): K(sigma_i), K(sigma_i + sigma_e), the potential flow's Laplacian
+  Buf<double> pos, dir, flow, coef_i, coef_ie, coef_lap, dinv, vm, rhs, phi, r, z, p0, q, partial,
       scal, tensor_i, tensor_e, tmp;
   Buf<unsigned char> mask;
+  Buf<unsigned> counter;                       // last-block counter of the grid reductions
+  cudaGraphExec_t graphs[1] = {nullptr};       // CG chunk of the bidomain solve
   bool have_dir = false, have_ops = false, have_map = false;
   int64_t n_tensor_i = 0, n_tensor_e = 0;
   // fiber -> mesh transfer (CSR over 3D nodes)
@@ -650,66 +700,85 @@ int emg_fail(fdm_emg* m, int code, const std::string& msg)
 
 #define EMG_BIND(m) EMG_CUDA(m, cudaSetDevice((m)->device))
 
-// conjugate gradients on A x = b with A the stencil coef (Dirichlet rows in mask: x keeps its value there and
-// p, r vanish), Jacobi preconditioner dinv; nullspace: b's and x's mean removed (constant null space).
-// Convergence: ||r||_2 <= max(rtol ||b||_2, atol) (unpreconditioned residual), checked every 8 iterations.
-int cg_solve(fdm_emg* m, const double* coef, const unsigned char* mask, bool nullspace, const double* b, double* x,
-             double rtol, double atol, int max_it, int* iterations, double* residual)
+// conjugate gradients on A x = b with A the symmetric stencil U (Dirichlet rows in mask: x keeps its value
+// there and p, r vanish), Jacobi preconditioner dinv; nullspace: b's and x's means removed (constant null
+// space).  Two kernels per iteration (direction + product, update), their reductions finished by the last
+// block; chunks of 8 iterations run as one CUDA graph (captured on the first use for this right-hand side and
+// solution vector).  Convergence: ||r||_2 <= max(rtol ||b||_2, atol) (unpreconditioned residual, from the
+// recurrence), checked after every chunk.
+int cg_solve(fdm_emg* m, const double* U, const unsigned char* mask, bool nullspace, const double* b, double* x,
+             double rtol, double atol, int max_it, int* iterations, double* residual, int graph_slot)
 {
   const int64_t N = m->N;
   const Grid g = m->hm.g;
   const int nb = blocks_for(N);
   cudaStream_t s = m->stream;
-  double* S = m->scal.p; // [0] r.z [1] p.Ap [2] r.z new [3] r.r [4] sum x [5] b.b
+  double* S = m->scal.p;
   double* P = m->partial.p;
+  unsigned* C = m->counter.p;
   const double* bb = b;
   if (nullspace) {
     // b <- b - mean(b) (consistency of the singular system), into tmp
-    sum_kernel<<<nb, EMG_T, 0, s>>>(N, b, nullptr, P);
-    reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 4);
-    EMG_CUDA(m, cudaMemcpyAsync(m->tmp.p, b, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-    subtract_mean_kernel<<<nb, EMG_T, 0, s>>>(N, m->tmp.p, S + 4);
+    sum_kernel<<<nb, EMG_T, 0, s>>>(N, b, nullptr, S, P, C);
+    subtract_mean_kernel<<<nb, EMG_T, 0, s>>>(N, b, m->tmp.p, S);
     bb = m->tmp.p;
   }
-  sum_kernel<<<nb, EMG_T, 0, s>>>(N, bb, bb, P);
-  reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 2, S + 4);
-  // r = b - A x
-  spmv_kernel<<<nb, EMG_T, 0, s>>>(g, coef, x, m->q.p, mask, nullptr);
-  init_residual_kernel<<<nb, EMG_T, 0, s>>>(N, bb, m->q.p, m->r.p, m->z.p, m->p.p, m->dinv.p, P);
-  reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 0);
-  reduce_kernel<<<1, EMG_T, 0, s>>>(P + EMG_MAX_BLOCKS, nb, 1, S + 3);
-  double hs[6];
+  sum_kernel<<<nb, EMG_T, 0, s>>>(N, bb, bb, S, P, C);
+  EMG_CUDA(m, cudaMemsetAsync(m->p0.p, 0, sizeof(double) * N, s));
+  EMG_CUDA(m, cudaMemsetAsync(m->q.p, 0, sizeof(double) * N, s));
+  cg_init_kernel<<<nb, EMG_T, 0, s>>>(g, U, mask, bb, x, m->r.p, m->z.p, m->dinv.p, S, P, C);
+  double hs[8];
   EMG_CUDA(m, cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, s));
   EMG_CUDA(m, cudaStreamSynchronize(s));
   // relative to ||b|| (to the initial residual where b vanishes: the Dirichlet problem, whose right-hand side
   // -K_fd u_d sits in the initial residual)
-  const double bnorm = hs[5] > 0 ? std::sqrt(hs[5]) : std::sqrt(hs[3]);
+  const double bnorm = hs[CG_BB] > 0 ? std::sqrt(hs[CG_BB]) : std::sqrt(hs[CG_RR]);
   const double target = std::max(rtol * bnorm, atol);
-  double rn = std::sqrt(hs[3]);
+  double rn = std::sqrt(hs[CG_RR]);
+  // one iteration: direction and product, then the update
+  auto iteration = [&]() {
+    cg_direction_kernel<<<nb, EMG_T, 0, s>>>(g, U, mask, m->z.p, m->p0.p, m->q.p, S, P, C);
+    cg_update_kernel<<<nb, EMG_T, 0, s>>>(N, x, m->r.p, m->z.p, m->p0.p, m->q.p, m->dinv.p, S, P, C);
+  };
+  constexpr int CHUNK = 8;
+  cudaGraphExec_t no_graph = nullptr;
+  cudaGraphExec_t& ge = graph_slot >= 0 ? m->graphs[graph_slot] : no_graph;
+  if (!ge && graph_slot >= 0) {
+    cudaGraph_t gr = nullptr;
+    EMG_CUDA(m, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int c = 0; c < CHUNK; c++)
+      iteration();
+    cudaError_t e = cudaStreamEndCapture(s, &gr);
+    if (e == cudaSuccess)
+      e = cudaGraphInstantiate(&ge, gr, 0);
+    if (gr)
+      cudaGraphDestroy(gr);
+    if (e != cudaSuccess) {
+      ge = nullptr;
+      return emg_fail(m, FDM_ERR_CUDA, std::string("conjugate gradients: graph capture: ") + cudaGetErrorString(e));
+    }
+  }
   int it = 0;
   while (rn > target && it < max_it) {
-    const int chunk = std::min(8, max_it - it);
-    for (int c = 0; c < chunk; c++) {
-      spmv_kernel<<<nb, EMG_T, 0, s>>>(g, coef, m->p.p, m->q.p, mask, P);
-      reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 1);
-      update_kernel<<<nb, EMG_T, 0, s>>>(N, x, m->r.p, m->z.p, m->p.p, m->q.p, m->dinv.p, S, P);
-      reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 2);
-      reduce_kernel<<<1, EMG_T, 0, s>>>(P + EMG_MAX_BLOCKS, nb, 1, S + 3);
-      direction_kernel<<<nb, EMG_T, 0, s>>>(N, m->p.p, m->z.p, S);
-      shift_scalar_kernel<<<1, 1, 0, s>>>(S);
+    if (ge && max_it - it >= CHUNK) {
+      EMG_CUDA(m, cudaGraphLaunch(ge, s));
+      it += CHUNK;
+    } else {
+      const int chunk = std::min(CHUNK, max_it - it);
+      for (int c = 0; c < chunk; c++)
+        iteration();
+      it += chunk;
     }
-    it += chunk;
     EMG_CUDA(m, cudaGetLastError());
     EMG_CUDA(m, cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, s));
     EMG_CUDA(m, cudaStreamSynchronize(s));
-    rn = std::sqrt(hs[3]);
+    rn = std::sqrt(hs[CG_RR]);
     if (!std::isfinite(rn))
       return emg_fail(m, FDM_ERR_NAN, "conjugate gradients: non-finite residual");
   }
   if (nullspace) {
-    sum_kernel<<<nb, EMG_T, 0, s>>>(N, x, nullptr, P);
-    reduce_kernel<<<1, EMG_T, 0, s>>>(P, nb, 1, S + 4);
-    subtract_mean_kernel<<<nb, EMG_T, 0, s>>>(N, x, S + 4);
+    sum_kernel<<<nb, EMG_T, 0, s>>>(N, x, nullptr, S, P, C);
+    subtract_mean_kernel<<<nb, EMG_T, 0, s>>>(N, x, x, S);
   }
   EMG_CUDA(m, cudaGetLastError());
   EMG_CUDA(m, cudaStreamSynchronize(s));
@@ -721,7 +790,7 @@ int cg_solve(fdm_emg* m, const double* coef, const unsigned char* mask, bool nul
 }
 
 int assemble(fdm_emg* m, const double* tensor, int64_t nt, const double* tensor2, int64_t nt2, double prefactor,
-             int gauss, bool directional, double* coef, double* diag)
+             int gauss, bool directional, double* coef)
 {
   AssembleArgs a{};
   a.g = m->hm.g;
@@ -734,7 +803,6 @@ int assemble(fdm_emg* m, const double* tensor, int64_t nt, const double* tensor2
   a.prefactor = prefactor;
   a.q = gauss_legendre(gauss);
   a.coef = coef;
-  a.diag = diag;
   const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((m->N + 127) / 128, 148 * 16));
   assemble_kernel<<<nb, 128, 0, m->stream>>>(a);
   EMG_CUDA(m, cudaGetLastError());
@@ -792,14 +860,18 @@ extern "C" int fdm_emg_create(int nx, int ny, int nz, const double* node_positio
       e = b->alloc(3 * N);
   for (auto* b : {&m->coef_i, &m->coef_ie})
     if (e == cudaSuccess)
-      e = b->alloc(27 * N);
-  for (auto* b : {&m->flow, &m->diag_ie, &m->dinv, &m->vm, &m->rhs, &m->phi, &m->r, &m->z, &m->p, &m->q, &m->tmp})
+      e = b->alloc(EMG_NC * N);
+  for (auto* b : {&m->flow, &m->dinv, &m->vm, &m->rhs, &m->phi, &m->r, &m->z, &m->p0, &m->q, &m->tmp})
     if (e == cudaSuccess)
       e = b->alloc(N);
   if (e == cudaSuccess)
     e = m->partial.alloc(2 * EMG_MAX_BLOCKS);
   if (e == cudaSuccess)
     e = m->scal.alloc(8);
+  if (e == cudaSuccess)
+    e = m->counter.alloc(1);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(m->counter.p, 0, sizeof(unsigned), m->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(m->pos.p, node_positions, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, m->stream);
   if (e == cudaSuccess)
@@ -826,11 +898,15 @@ extern "C" int fdm_emg_destroy(fdm_emg* m)
   cudaSetDevice(m->device);
   if (m->stream)
     cudaStreamSynchronize(m->stream);
-  for (auto* b : {&m->pos, &m->dir, &m->flow, &m->coef_i, &m->coef_ie, &m->coef_lap, &m->diag_ie, &m->diag_lap,
-                  &m->dinv, &m->vm, &m->rhs, &m->phi, &m->r, &m->z, &m->p, &m->q, &m->partial, &m->scal,
-                  &m->tensor_i, &m->tensor_e, &m->tmp, &m->map_w, &m->map_fsum})
+  for (auto* b : {&m->pos, &m->dir, &m->flow, &m->coef_i, &m->coef_ie, &m->coef_lap, &m->dinv, &m->vm, &m->rhs,
+                  &m->phi, &m->r, &m->z, &m->p0, &m->q, &m->partial, &m->scal, &m->tensor_i, &m->tensor_e,
+                  &m->tmp, &m->map_w, &m->map_fsum})
     b->release();
+  for (auto& ge : m->graphs)
+    if (ge)
+      cudaGraphExecDestroy(ge);
   m->mask.release();
+  m->counter.release();
   m->map_ptr.release();
   m->map_src.release();
   if (m->ev0)
@@ -865,31 +941,29 @@ extern "C" int fdm_emg_potential_flow(fdm_emg* m, int64_t n_dirichlet, const int
     mk[nodes[d]] = 1;
     x0[nodes[d]] = values[d];
   }
-  EMG_CUDA(m, m->coef_lap.alloc(27 * N));
-  EMG_CUDA(m, m->diag_lap.alloc(N));
+  EMG_CUDA(m, m->coef_lap.alloc(EMG_NC * N));
   EMG_CUDA(m, m->mask.alloc(N));
   EMG_CUDA(m, m->tensor_i.alloc(9));
   const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   EMG_CUDA(m, cudaMemcpyAsync(m->tensor_i.p, eye, sizeof(eye), cudaMemcpyHostToDevice, m->stream));
   EMG_CUDA(m, cudaMemcpyAsync(m->mask.p, mk.data(), N, cudaMemcpyHostToDevice, m->stream));
   EMG_CUDA(m, cudaMemcpyAsync(m->flow.p, x0.data(), sizeof(double) * N, cudaMemcpyHostToDevice, m->stream));
-  int rc = assemble(m, m->tensor_i.p, 1, nullptr, 0, 1.0, gauss_points, false, m->coef_lap.p, m->diag_lap.p);
+  int rc = assemble(m, m->tensor_i.p, 1, nullptr, 0, 1.0, gauss_points, false, m->coef_lap.p);
   if (rc)
     return rc;
   const int nb = blocks_for(N);
-  inverse_diag_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->diag_lap.p, m->mask.p, m->dinv.p);
+  inverse_diag_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->coef_lap.p, m->mask.p, m->dinv.p);
   // free rows: K_ff u_f = -K_fd u_d (b = 0, x0 holding the Dirichlet values; Dirichlet rows masked)
   EMG_CUDA(m, cudaMemsetAsync(m->rhs.p, 0, sizeof(double) * N, m->stream));
   int its = 0;
   double res = 0.0;
-  rc = cg_solve(m, m->coef_lap.p, m->mask.p, false, m->rhs.p, m->flow.p, rtol, atol, max_iterations, &its, &res);
+  rc = cg_solve(m, m->coef_lap.p, m->mask.p, false, m->rhs.p, m->flow.p, rtol, atol, max_iterations, &its, &res, -1);
   if (rc)
     return rc;
   gradient_direction_kernel<<<nb, EMG_T, 0, m->stream>>>(m->hm.g, m->pos.p, m->flow.p, m->dir.p);
   EMG_CUDA(m, cudaGetLastError());
   EMG_CUDA(m, cudaStreamSynchronize(m->stream));
   m->coef_lap.release();
-  m->diag_lap.release();
   m->have_dir = true;
   m->have_ops = false;
   if (iterations)
@@ -927,10 +1001,9 @@ extern "C" int fdm_emg_set_conductivity(fdm_emg* m, int64_t n_sigma_i, const dou
                               m->stream));
   EMG_CUDA(m, cudaMemcpyAsync(m->tensor_e.p, sigma_e, sizeof(double) * 9 * n_sigma_e, cudaMemcpyHostToDevice,
                               m->stream));
-  int rc = assemble(m, m->tensor_i.p, n_sigma_i, nullptr, 0, 1.0, gauss_points, true, m->coef_i.p, nullptr);
+  int rc = assemble(m, m->tensor_i.p, n_sigma_i, nullptr, 0, 1.0, gauss_points, true, m->coef_i.p);
   if (!rc)
-    rc = assemble(m, m->tensor_i.p, n_sigma_i, m->tensor_e.p, n_sigma_e, 1.0, gauss_points, true, m->coef_ie.p,
-                  m->diag_ie.p);
+    rc = assemble(m, m->tensor_i.p, n_sigma_i, m->tensor_e.p, n_sigma_e, 1.0, gauss_points, true, m->coef_ie.p);
   if (rc)
     return rc;
   EMG_CUDA(m, cudaStreamSynchronize(m->stream));
@@ -1117,14 +1190,13 @@ extern "C" int fdm_emg_solve(fdm_emg* m, double rtol, double atol, int max_itera
   const int nb = blocks_for(N);
   EMG_CUDA(m, cudaEventRecord(m->ev0, m->stream));
   // rhs = -K(sigma_i) Vm
-  spmv_kernel<<<nb, EMG_T, 0, m->stream>>>(m->hm.g, m->coef_i.p, m->vm.p, m->rhs.p, nullptr, nullptr);
-  negate_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->rhs.p);
-  inverse_diag_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->diag_ie.p, nullptr, m->dinv.p);
+  apply_kernel<<<nb, EMG_T, 0, m->stream>>>(m->hm.g, m->coef_i.p, m->vm.p, m->rhs.p, -1.0);
+  inverse_diag_kernel<<<nb, EMG_T, 0, m->stream>>>(N, m->coef_ie.p, nullptr, m->dinv.p);
   if (!initial_guess_nonzero)
     EMG_CUDA(m, cudaMemsetAsync(m->phi.p, 0, sizeof(double) * N, m->stream));
   int its = 0;
   double res = 0.0;
-  int rc = cg_solve(m, m->coef_ie.p, nullptr, true, m->rhs.p, m->phi.p, rtol, atol, max_iterations, &its, &res);
+  int rc = cg_solve(m, m->coef_ie.p, nullptr, true, m->rhs.p, m->phi.p, rtol, atol, max_iterations, &its, &res, 0);
   if (rc)
     return rc;
   EMG_CUDA(m, cudaEventRecord(m->ev1, m->stream));
@@ -1164,9 +1236,28 @@ extern "C" int fdm_emg_get_stencil(fdm_emg* m, int which, double* out)
   if (!m || !out || !m->have_ops || (which != 0 && which != 1))
     return emg_fail(m, FDM_ERR_ARG, "fdm_emg_get_stencil: operators not assembled or bad argument");
   EMG_BIND(m);
-  EMG_CUDA(m, cudaMemcpyAsync(out, which == 0 ? m->coef_i.p : m->coef_ie.p, sizeof(double) * 27 * m->N,
+  const int64_t N = m->N;
+  std::vector<double> U(EMG_NC * N);
+  EMG_CUDA(m, cudaMemcpyAsync(U.data(), which == 0 ? m->coef_i.p : m->coef_ie.p, sizeof(double) * EMG_NC * N,
                               cudaMemcpyDeviceToHost, m->stream));
   EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  // the full 27-point rows: the forward half as stored, the backward half from the neighbours' forward entries
+  const Grid g = m->hm.g;
+  for (int64_t n = 0; n < N; n++) {
+    const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / ((int64_t)g.nx * g.ny));
+    for (int q = 0; q < 27; q++) {
+      int dx, dy, dz;
+      stencil_offset(q, dx, dy, dz);
+      double v = 0.0;
+      if (i + dx >= 0 && i + dx < g.nx && j + dy >= 0 && j + dy < g.ny && k + dz >= 0 && k + dz < g.nz) {
+        if (q >= 13)
+          v = U[(q - 13) * N + n];
+        else
+          v = U[(13 - q) * N + n + dx + (int64_t)g.nx * (dy + (int64_t)g.ny * dz)];
+      }
+      out[q * N + n] = v;
+    }
+  }
   return FDM_OK;
 }
 
