@@ -46,6 +46,7 @@ def parse_args():
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
+    p.add_argument("--skip-emg", action="store_true")
     return p.parse_args()
 
 
@@ -161,6 +162,66 @@ def cpu_baseline(system, sample_fibers: int, sample_ms: float, threads: int):
     st, _, tr, n = H.run_oracle(sub.copy(), n_threads=threads)
     dt = time.perf_counter() - t0
     return sub, st, n, sub.n_nodes * n / dt, dt
+
+
+def emg_measurement(device: int, peak_hbm: float):
+    """Coupled fibers + EMG (13 x 13 HH fibers x 1481 nodes, 25 x 25 x 149 3D nodes, one bidomain solve per
+    1 ms coupling step, FP32 fused fibers) and the CG iteration on a 97 x 97 x 297 mesh (2.8M nodes)."""
+    import torch
+    from opendihu_b200 import emg as E
+    from opendihu_b200 import solver as S
+    from opendihu_b200 import workloads as WL
+    out = {}
+    system, fpos, kw = WL.emg_box(n_fibers_x=13, n_fibers_y=13, n_nodes=1481, mesh_nodes=(25, 25, 149), end_time=5.0)
+    solver_cfg = {"relativeTolerance": 1e-8, "absoluteTolerance": 1e-30, "maxIterations": 20000}
+    fib = S.FastMonodomainSolver(system, method="fused", precision="fp32", device=device)
+    bid = E.StaticBidomainSolver(emg_solver=solver_cfg, potential_flow_solver=solver_cfg, device=device, **kw)
+    solves = []
+    cp = E.Coupling(fib, bid, 1.0, 5.0, fpos, callback=lambda k, t, b: solves.append(b.timing()))
+    with cp:
+        cp.term1.setTimeSpan(0.0, 1.0)       # warm-up: one coupling step outside the timed span
+        cp.term1.advanceTimeSpan()
+        cp.term2.map_fibers(cp.term1)
+        cp.term2.advanceTimeSpan()
+        cp.start_time = 1.0
+        solves.clear()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        cp.advanceTimeSpan()
+        torch.cuda.synchronize(device)
+        wall = time.perf_counter() - t0
+        phi = cp.term2.phi_e()
+    out["coupled"] = {
+        "workload": "fibers_emg-shaped box: 13 x 13 HH fibers x 1481 nodes (FP32 fused), 3D mesh 25 x 25 x 149 "
+                    "nodes, sigma_i/sigma_e of the example, coupling dt 1 ms, CG rtol 1e-8",
+        "coupling_steps": len(solves), "ms_per_coupling_step": wall / max(len(solves), 1) * 1e3,
+        "emg_solve_ms": float(np.mean([t["solve_ms"] for t in solves])) if solves else None,
+        "cg_iterations": [t["iterations"] for t in solves], "phi_e_max_abs": float(np.abs(phi).max()),
+        "timing": "host wall clock around the coupled steps (fiber advance + transfer + solve)"}
+    # CG iteration against the HBM roofline (mesh larger than L2)
+    _, _, kw2 = WL.emg_box(n_fibers_x=2, n_fibers_y=2, n_nodes=1481, mesh_nodes=(97, 97, 297), width=3.0)
+    z = kw2["node_positions"][:, 2]
+    with E.StaticBidomainSolver(emg_solver={"relativeTolerance": 1e-30, "absoluteTolerance": 0.0,
+                                            "maxIterations": 160},
+                                potential_flow_solver=solver_cfg, device=device, **kw2) as big:
+        big.set_vm(-75.0 + 100.0 * np.exp(-((z - z.mean()) / 0.3) ** 2))
+        big.advanceTimeSpan()
+        big.initial_guess_nonzero = False
+        big.advanceTimeSpan()
+        t = big.timing()
+        n = big.n_nodes
+    per_it_ms = t["solve_ms"] / max(t["iterations"], 1)
+    # algorithmic bytes per node and iteration: direction pass (14 stencil coefficients, z, p and q read, p and
+    # q written: 152 B) + update pass (x, r read and written, p, q, dinv read, z written: 64 B)
+    bytes_it = 216 * n
+    gbs = bytes_it / (per_it_ms / 1e3) / 1e9
+    out["cg_iteration"] = {"workload": "97 x 97 x 297 mesh (%d nodes), 160 iterations" % n, "iterations": t["iterations"],
+                           "solve_ms": t["solve_ms"], "ms_per_iteration": per_it_ms,
+                           "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak_hbm, "unit": "GB/s",
+                                        "frac": gbs / peak_hbm, "algorithmic_bytes_per_node_iteration": 216,
+                                        "timing": "CUDA events around the solve (includes the host checks every "
+                                                  "8 iterations)"}}
+    return out
 
 
 def run_reference(args):
@@ -322,6 +383,12 @@ def main():
                "grad_norm_sigma": float(np.linalg.norm(g["prefactor"] / (WL.AM * WL.CM))),
                "grad_norm_gna_scale": float(np.linalg.norm(g_na))}
 
+    # fibers -> 3D static bidomain (EMG): the coupled fibers_emg-shaped workload, and the conjugate-gradient
+    # iteration on a mesh larger than L2 against the HBM roofline
+    emg = None
+    if rank == 0 and not args.skip_emg:
+        emg = emg_measurement(local, peaks()[0])
+
     # accuracy against the FP64 oracle on a sample of the batch, and the oracle's CPU throughput
     acc = None
     cpu = None
@@ -379,6 +446,7 @@ def main():
             "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
             "plain_config_node_steps_per_s": plain_cfg,
             "adjoint": adj,
+            "emg": emg,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak_hbm, "unit": "GB/s",
                          "frac": (achieved_gbs / peak_hbm) if achieved_gbs else None, "traffic": traffic,
                          "peak_source": peak_kind,
