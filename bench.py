@@ -47,6 +47,9 @@ def parse_args():
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
     p.add_argument("--skip-emg", action="store_true")
+    p.add_argument("--only-emg", action="store_true", help="print the EMG measurement alone (profiling runs)")
+    p.add_argument("--emg-cg-mesh", default="97,97,297", help="3D nodes of the CG-iteration measurement")
+    p.add_argument("--emg-cg-iterations", type=int, default=160)
     return p.parse_args()
 
 
@@ -164,7 +167,7 @@ def cpu_baseline(system, sample_fibers: int, sample_ms: float, threads: int):
     return sub, st, n, sub.n_nodes * n / dt, dt
 
 
-def emg_measurement(device: int, peak_hbm: float):
+def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iterations: int = 160):
     """Coupled fibers + EMG (13 x 13 HH fibers x 1481 nodes, 25 x 25 x 149 3D nodes, one bidomain solve per
     1 ms coupling step, FP32 fused fibers) and the CG iteration on a 97 x 97 x 297 mesh (2.8M nodes)."""
     import torch
@@ -174,7 +177,7 @@ def emg_measurement(device: int, peak_hbm: float):
     out = {}
     system, fpos, kw = WL.emg_box(n_fibers_x=13, n_fibers_y=13, n_nodes=1481, mesh_nodes=(25, 25, 149), end_time=5.0)
     solver_cfg = {"relativeTolerance": 1e-8, "absoluteTolerance": 1e-30, "maxIterations": 20000}
-    fib = S.FastMonodomainSolver(system, method="fused", precision="fp32", device=device)
+    fib = S.FastMonodomainSolver(system, method="fused", precision="fp32", device=device, autotune=True)
     bid = E.StaticBidomainSolver(emg_solver=solver_cfg, potential_flow_solver=solver_cfg, device=device, **kw)
     solves = []
     cp = E.Coupling(fib, bid, 1.0, 5.0, fpos, callback=lambda k, t, b: solves.append(b.timing()))
@@ -191,18 +194,20 @@ def emg_measurement(device: int, peak_hbm: float):
         torch.cuda.synchronize(device)
         wall = time.perf_counter() - t0
         phi = cp.term2.phi_e()
+        layout = fib.fused_layout()
     out["coupled"] = {
         "workload": "fibers_emg-shaped box: 13 x 13 HH fibers x 1481 nodes (FP32 fused), 3D mesh 25 x 25 x 149 "
                     "nodes, sigma_i/sigma_e of the example, coupling dt 1 ms, CG rtol 1e-8",
         "coupling_steps": len(solves), "ms_per_coupling_step": wall / max(len(solves), 1) * 1e3,
         "emg_solve_ms": float(np.mean([t["solve_ms"] for t in solves])) if solves else None,
         "cg_iterations": [t["iterations"] for t in solves], "phi_e_max_abs": float(np.abs(phi).max()),
+        "fiber_layout": layout,
         "timing": "host wall clock around the coupled steps (fiber advance + transfer + solve)"}
     # CG iteration against the HBM roofline (mesh larger than L2)
-    _, _, kw2 = WL.emg_box(n_fibers_x=2, n_fibers_y=2, n_nodes=1481, mesh_nodes=(97, 97, 297), width=3.0)
+    _, _, kw2 = WL.emg_box(n_fibers_x=2, n_fibers_y=2, n_nodes=1481, mesh_nodes=tuple(cg_mesh), width=3.0)
     z = kw2["node_positions"][:, 2]
     with E.StaticBidomainSolver(emg_solver={"relativeTolerance": 1e-30, "absoluteTolerance": 0.0,
-                                            "maxIterations": 160},
+                                            "maxIterations": cg_iterations},
                                 potential_flow_solver=solver_cfg, device=device, **kw2) as big:
         big.set_vm(-75.0 + 100.0 * np.exp(-((z - z.mean()) / 0.3) ** 2))
         big.advanceTimeSpan()
@@ -215,7 +220,8 @@ def emg_measurement(device: int, peak_hbm: float):
     # q written: 152 B) + update pass (x, r read and written, p, q, dinv read, z written: 64 B)
     bytes_it = 216 * n
     gbs = bytes_it / (per_it_ms / 1e3) / 1e9
-    out["cg_iteration"] = {"workload": "97 x 97 x 297 mesh (%d nodes), 160 iterations" % n, "iterations": t["iterations"],
+    out["cg_iteration"] = {"workload": "%d x %d x %d mesh (%d nodes), %d iterations" % (*cg_mesh, n, cg_iterations),
+                           "iterations": t["iterations"],
                            "solve_ms": t["solve_ms"], "ms_per_iteration": per_it_ms,
                            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak_hbm, "unit": "GB/s",
                                         "frac": gbs / peak_hbm, "algorithmic_bytes_per_node_iteration": 216,
@@ -257,6 +263,13 @@ def main():
     world, rank, local, pg = dist_setup(args)
     from opendihu_b200 import solver as S
     from opendihu_b200 import workloads as WL
+    cg_mesh = tuple(int(x) for x in args.emg_cg_mesh.split(","))
+    if args.only_emg:
+        if rank == 0:
+            print(json.dumps({"emg": emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations)}), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
 
     system = WL.batched_hh(n_fibers=args.fibers, seed=rank)
     n_nodes = system.n_nodes
@@ -387,7 +400,7 @@ def main():
     # iteration on a mesh larger than L2 against the HBM roofline
     emg = None
     if rank == 0 and not args.skip_emg:
-        emg = emg_measurement(local, peaks()[0])
+        emg = emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations)
 
     # accuracy against the FP64 oracle on a sample of the batch, and the oracle's CPU throughput
     acc = None
@@ -435,6 +448,7 @@ def main():
                        "n_nodes_per_gpu": n_nodes, "step": f"{step} ms simulated = {split_steps // args.steps} Strang steps",
                        "method": "fused persistent kernel, FP32 reaction", "l2": "inputs larger than L2 (~0.5 GB/GPU)",
                        "fused_shape": {"threads": fused.threads_per_block, "nodes_per_thread": fused.nodes_per_thread,
+                                       "cluster_size": fused.cluster_size,
                                        "steps_per_launch": steps_per_launch, "autotuned": tuning is not None},
                        "parallelism": f"fibers sharded, {world} GPU(s), no collective"},
             "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": state_bytes,

@@ -1,11 +1,13 @@
 """Autotuner of the fused kernel's launch shape.
 
 The fused kernel packs whole fibers into bins of T*M nodes (T threads per CTA, M nodes per thread, so the
-number of fibers per CTA follows from the fiber lengths) and runs K Strang steps per launch.  The best
-(T, M) depends on the model's register footprint and on the length distribution (bin fill, waves on
-148 SMs); K trades launch overhead against stimulation-schedule memory.  The tuner times every built shape
-that holds the longest fiber on the actual workload for a few Strang steps (device time of the kernel
-launches, CUDA events) and then a few K values for the winner.  Results are cached per workload signature
+number of fibers per CTA follows from the fiber lengths) and runs K Strang steps per launch; in cluster mode
+it spreads each fiber over C CTAs of a thread-block cluster.  The best (T, M, C) depends on the model's
+register footprint and on the length distribution (bin fill, waves on 148 SMs: 169 fibers in 169 bins run
+in two waves, spread over clusters they fill the GPU evenly); K trades launch overhead against
+stimulation-schedule memory.  The tuner times every built shape that holds the longest fiber (cluster shapes
+with 2..8 CTAs per fiber where the model and options allow them) on the actual workload for a few Strang
+steps (device time of the kernel launches, CUDA events) and then a few K values for the winner.  Results are cached per workload signature
 in memory and, if FDM_AUTOTUNE_CACHE names a file, in that JSON file.
 """
 from __future__ import annotations
@@ -26,7 +28,8 @@ def signature(system, precision: str) -> str:
     lengths = np.diff(np.asarray(system.fiber_offsets))
     hist = np.histogram(lengths, bins=16, range=(0, int(lengths.max()) + 1))[0]
     desc = [system.model, precision, system.diffusion_scheme, bool(system.approximate_exponential_function),
-            int(lengths.max()), int(lengths.sum()), hist.tolist()]
+            bool(getattr(system, "only_compute_if_has_been_stimulated", False)), int(lengths.max()),
+            int(lengths.sum()), hist.tolist(), "cluster"]
     return hashlib.sha1(json.dumps(desc).encode()).hexdigest()[:16]
 
 
@@ -52,14 +55,14 @@ def _store_cache(key: str, value: dict):
     os.replace(tmp, path)
 
 
-def _time_shape(system, precision, threads, m, k, n_steps, device) -> float:
+def _time_shape(system, precision, threads, m, k, n_steps, device, cluster_size: int = 1) -> float:
     """Seconds of device time per Strang step (all GPU work of the advance: schedule + fused kernels)."""
     from .solver import FastMonodomainSolver
     s = system.copy()
     dt = s.dt_splitting
     with FastMonodomainSolver(s, method="fused", precision=precision, threads_per_block=threads,
                               nodes_per_thread=m, steps_per_launch=k, profile=True, device=device,
-                              check_nan=False) as slv:
+                              check_nan=False, cluster_size=cluster_size) as slv:
         slv.setTimeSpan(s.start_time, s.start_time + dt * min(k, n_steps))
         slv.advanceTimeSpan()  # warm-up (module load, factorization)
         slv.reset_timing()
@@ -72,7 +75,8 @@ def _time_shape(system, precision, threads, m, k, n_steps, device) -> float:
 
 def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0,
              steps_per_launch: Sequence[int] = (50, 100, 200), use_cache: bool = True) -> dict:
-    """Return {"threads", "nodes_per_thread", "steps_per_launch", "s_per_step", "trials"} for the workload."""
+    """Return {"threads", "nodes_per_thread", "cluster_size", "steps_per_launch", "s_per_step", "trials"} for the
+    workload (cluster_size 1: bins of whole fibers)."""
     key = signature(system, precision)
     if use_cache:
         if key in _MEMO:
@@ -82,23 +86,29 @@ def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0
             _MEMO[key] = cached
             return cached
     max_len = int(np.diff(np.asarray(system.fiber_offsets)).max())
-    shapes = [(t, m) for t, m in N.fused_shapes() if t * m >= max_len]
+    shapes = [(t, m, 1) for t, m in N.fused_shapes() if t * m >= max_len]
+    if (system.model == "hodgkin_huxley_1952" and not system.approximate_exponential_function
+            and not getattr(system, "only_compute_if_has_been_stimulated", False)):
+        for t, m in N.fused_shapes(cluster=True):
+            c = -(-max_len // (t * m))
+            if 2 <= c <= 8:
+                shapes.append((t, m, c))
     if not shapes:
         raise N.FdmError(N.FDM_ERR_UNSUPPORTED, f"no fused shape holds a fiber of {max_len} nodes")
     trials = []
     k0 = 100
-    for t, m in shapes:
-        trials.append({"threads": t, "nodes_per_thread": m, "steps_per_launch": min(k0, n_steps),
-                       "s_per_step": _time_shape(system, precision, t, m, min(k0, n_steps), n_steps, device)})
+    for t, m, c in shapes:
+        trials.append({"threads": t, "nodes_per_thread": m, "cluster_size": c, "steps_per_launch": min(k0, n_steps),
+                       "s_per_step": _time_shape(system, precision, t, m, min(k0, n_steps), n_steps, device, c)})
     best = min(trials, key=lambda r: r["s_per_step"])
     # window length for the winner, over a span of a few windows
     k_trials = []
     for k in steps_per_launch:
         span = max(n_steps, 2 * k)
         k_trials.append({"threads": best["threads"], "nodes_per_thread": best["nodes_per_thread"],
-                         "steps_per_launch": k,
+                         "cluster_size": best["cluster_size"], "steps_per_launch": k,
                          "s_per_step": _time_shape(system, precision, best["threads"], best["nodes_per_thread"], k,
-                                                   span, device)})
+                                                   span, device, best["cluster_size"])})
     best_k = min(k_trials, key=lambda r: r["s_per_step"])
     result = dict(best_k)
     result["trials"] = trials + k_trials

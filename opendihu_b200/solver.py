@@ -360,6 +360,7 @@ class FastMonodomainSolver:
             self.tuning = autotune(s, self.precision, device=self.device)
             self.threads_per_block = self.tuning["threads"]
             self.nodes_per_thread = self.tuning["nodes_per_thread"]
+            self.cluster_size = int(self.tuning.get("cluster_size", 1))
             if not self.steps_per_launch:
                 self.steps_per_launch = self.tuning["steps_per_launch"]
         cfg = N.default_config()

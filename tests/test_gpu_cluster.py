@@ -74,3 +74,18 @@ def test_fiber_longer_than_every_bin_runs_in_cluster_mode():
     lay = _layout(s)
     assert lay["cluster_size"] > 1
     GP.compare(s, "fused", "fp64", GP.VM_TOL_FP64, 1e-8)
+
+
+def test_autotuner_considers_cluster_shapes():
+    from opendihu_b200 import autotune as AT
+    s = H.complete(H.c1_system(n_fibers=4, n_nodes=1481, end_time=0.3))
+    res = AT.autotune(s, "fp64", n_steps=5, steps_per_launch=(50,), use_cache=False)
+    assert any(t.get("cluster_size", 1) > 1 for t in res["trials"])
+    assert any(t.get("cluster_size", 1) == 1 for t in res["trials"])
+    with S.FastMonodomainSolver(s.copy(), method="fused", precision="fp64", autotune=True) as slv:
+        slv.advanceTimeSpan()
+        lay = slv.fused_layout()
+        st = slv.states()
+    assert lay["cluster_size"] == slv.tuning["cluster_size"]
+    ref, _, _, _ = H.run_oracle(s.copy())
+    assert np.max(np.abs(st[0] - ref[0])) <= GP.VM_TOL_FP64
