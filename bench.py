@@ -47,7 +47,10 @@ def parse_args():
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
     p.add_argument("--skip-emg", action="store_true")
-    p.add_argument("--only-emg", action="store_true", help="print the EMG measurement alone (profiling runs)")
+    p.add_argument("--only", choices=["emg", "emg-cg", "shorten"],
+                   help="print one side measurement alone (profiling runs)")
+    p.add_argument("--skip-shorten", action="store_true")
+    p.add_argument("--shorten-ms", type=float, default=0.02, help="simulated span of the Shorten measurement")
     p.add_argument("--emg-cg-mesh", default="97,97,297", help="3D nodes of the CG-iteration measurement")
     p.add_argument("--emg-cg-iterations", type=int, default=160)
     return p.parse_args()
@@ -167,16 +170,54 @@ def cpu_baseline(system, sample_fibers: int, sample_ms: float, threads: int):
     return sub, st, n, sub.n_nodes * n / dt, dt
 
 
-def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iterations: int = 160):
+def shorten_measurement(device: int, span_ms: float):
+    """The Shorten 2007 configuration (56 states; 1369 fibers x 1481 nodes = 2.03M nodes, dt0D 1e-5, dt_split
+    5e-4, seeded per-MU firing): FP64 plain (split) against the FP32-reaction path on the same fibers over a
+    bounded span (the 50 ms of the configuration take minutes; node-steps/s does not depend on the span)."""
+    import torch
+    from opendihu_b200 import solver as S
+    from opendihu_b200 import workloads as WL
+    system = WL.shorten_grid(end_time=span_ms + 0.01)
+    out = {"workload": "Shorten 2007, 1369 fibers x 1481 nodes (%d nodes), dt0D 1e-5, dt_split 5e-4 (25 Heun "
+                       "substeps per half step), %.3f ms measured after 0.01 ms warm-up" % (system.n_nodes, span_ms)}
+    vm = {}
+    for name, prec in (("fp64_plain", "fp64"), ("fp32_reaction", "fp32")):
+        with S.FastMonodomainSolver(system.copy(), method="split", precision=prec, device=device) as sv:
+            sv.setTimeSpan(0.0, 0.01)
+            sv.advanceTimeSpan()
+            sv.reset_timing()
+            n0 = sv.split_steps()
+            sv.setTimeSpan(0.01, 0.01 + span_ms)
+            sv.advanceTimeSpan()
+            ms = sv.timing()["advance_ms"]
+            steps = sv.split_steps() - n0
+            vm[name] = sv.states()[0]
+        out[name] = {"node_steps_per_s": system.n_nodes * steps / (ms / 1e3), "ms": ms, "strang_steps": steps}
+    out["speedup_fp32_over_fp64"] = out["fp32_reaction"]["node_steps_per_s"] / out["fp64_plain"]["node_steps_per_s"]
+    out["vm_max_abs_diff_fp32_vs_fp64_mV"] = float(np.max(np.abs(vm["fp32_reaction"] - vm["fp64_plain"])))
+    out["method"] = "split path (the 56 states stay in the reaction kernel's registers over each half step); " \
+                    "the fused kernel is built for HH only"
+    return out
+
+
+def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iterations: int = 160,
+                    coupled: bool = True):
     """Coupled fibers + EMG (13 x 13 HH fibers x 1481 nodes, 25 x 25 x 149 3D nodes, one bidomain solve per
     1 ms coupling step, FP32 fused fibers) and the CG iteration on a 97 x 97 x 297 mesh (2.8M nodes)."""
+    out = {}
+    solver_cfg = {"relativeTolerance": 1e-8, "absoluteTolerance": 1e-30, "maxIterations": 20000}
+    if coupled:
+        out["coupled"] = emg_coupled(device, solver_cfg)
+    _cg_iteration(out, device, peak_hbm, cg_mesh, cg_iterations, solver_cfg)
+    return out
+
+
+def emg_coupled(device: int, solver_cfg: dict) -> dict:
     import torch
     from opendihu_b200 import emg as E
     from opendihu_b200 import solver as S
     from opendihu_b200 import workloads as WL
-    out = {}
     system, fpos, kw = WL.emg_box(n_fibers_x=13, n_fibers_y=13, n_nodes=1481, mesh_nodes=(25, 25, 149), end_time=5.0)
-    solver_cfg = {"relativeTolerance": 1e-8, "absoluteTolerance": 1e-30, "maxIterations": 20000}
     fib = S.FastMonodomainSolver(system, method="fused", precision="fp32", device=device, autotune=True)
     bid = E.StaticBidomainSolver(emg_solver=solver_cfg, potential_flow_solver=solver_cfg, device=device, **kw)
     solves = []
@@ -195,7 +236,7 @@ def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iter
         wall = time.perf_counter() - t0
         phi = cp.term2.phi_e()
         layout = fib.fused_layout()
-    out["coupled"] = {
+    return {
         "workload": "fibers_emg-shaped box: 13 x 13 HH fibers x 1481 nodes (FP32 fused), 3D mesh 25 x 25 x 149 "
                     "nodes, sigma_i/sigma_e of the example, coupling dt 1 ms, CG rtol 1e-8",
         "coupling_steps": len(solves), "ms_per_coupling_step": wall / max(len(solves), 1) * 1e3,
@@ -203,7 +244,12 @@ def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iter
         "cg_iterations": [t["iterations"] for t in solves], "phi_e_max_abs": float(np.abs(phi).max()),
         "fiber_layout": layout,
         "timing": "host wall clock around the coupled steps (fiber advance + transfer + solve)"}
-    # CG iteration against the HBM roofline (mesh larger than L2)
+
+
+def _cg_iteration(out: dict, device: int, peak_hbm: float, cg_mesh, cg_iterations: int, solver_cfg: dict):
+    """CG iteration of the bidomain solve against the HBM roofline (mesh larger than L2)."""
+    from opendihu_b200 import emg as E
+    from opendihu_b200 import workloads as WL
     _, _, kw2 = WL.emg_box(n_fibers_x=2, n_fibers_y=2, n_nodes=1481, mesh_nodes=tuple(cg_mesh), width=3.0)
     z = kw2["node_positions"][:, 2]
     with E.StaticBidomainSolver(emg_solver={"relativeTolerance": 1e-30, "absoluteTolerance": 0.0,
@@ -227,7 +273,6 @@ def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iter
                                         "frac": gbs / peak_hbm, "algorithmic_bytes_per_node_iteration": 216,
                                         "timing": "CUDA events around the solve (includes the host checks every "
                                                   "8 iterations)"}}
-    return out
 
 
 def run_reference(args):
@@ -264,9 +309,14 @@ def main():
     from opendihu_b200 import solver as S
     from opendihu_b200 import workloads as WL
     cg_mesh = tuple(int(x) for x in args.emg_cg_mesh.split(","))
-    if args.only_emg:
+    if args.only:
         if rank == 0:
-            print(json.dumps({"emg": emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations)}), flush=True)
+            if args.only in ("emg", "emg-cg"):
+                out = {"emg": emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations,
+                                              coupled=args.only == "emg")}
+            else:
+                out = {"shorten": shorten_measurement(local, args.shorten_ms)}
+            print(json.dumps(out), flush=True)
         if pg is not None:
             pg.destroy_process_group()
         return
@@ -401,6 +451,9 @@ def main():
     emg = None
     if rank == 0 and not args.skip_emg:
         emg = emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations)
+    shorten = None
+    if rank == 0 and not args.skip_shorten:
+        shorten = shorten_measurement(local, args.shorten_ms)
 
     # accuracy against the FP64 oracle on a sample of the batch, and the oracle's CPU throughput
     acc = None
@@ -461,6 +514,7 @@ def main():
             "plain_config_node_steps_per_s": plain_cfg,
             "adjoint": adj,
             "emg": emg,
+            "shorten": shorten,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak_hbm, "unit": "GB/s",
                          "frac": (achieved_gbs / peak_hbm) if achieved_gbs else None, "traffic": traffic,
                          "peak_source": peak_kind,
