@@ -91,3 +91,39 @@ def test_solver_continues_after_adjoint():
     np.testing.assert_array_equal(a, b)
     ref, _, _, _ = H.run_oracle(sysm.copy())
     assert np.max(np.abs(a[0] - ref[0])) <= 1e-6
+
+
+def test_shorten_adjoint_central_differences():
+    """The 56-state Shorten model through the same adjoint (generated vector-Jacobian product of its
+    right-hand side): prefactor and parameter gradients against central differences of the forward run."""
+    sysm = S.uniform_fibers(H.SHORTEN, [31, 25], 0.01, 3.828 / (500 * 0.58), call_frequency=0.1,
+                            repeat_after_first_call=0.1, end_time=0.02, dt_0d=1e-5, dt_1d=5e-4, dt_splitting=5e-4,
+                            dt_repeated_call=5e-4)
+    H.complete(sysm)
+    sensors = np.array([0, 7, 15, 31 + 4, 55])
+    rng = np.random.default_rng(8)
+    eng = ADJ.AdjointEngine(sysm, sensors, checkpoint_every=7)
+    try:
+        base = eng.forward(sysm.prefactor, sysm.parameters)
+        w = rng.standard_normal(base.shape)
+        g = eng.backward(w)
+
+        def L(pfv, Pv):
+            return float((w * eng.forward(pfv, Pv)).sum())
+        h = 1e-6
+        for f in range(2):
+            d = np.zeros(2)
+            d[f] = h * sysm.prefactor[f]
+            fd = (L(sysm.prefactor + d, sysm.parameters) - L(sysm.prefactor - d, sysm.parameters)) / (2 * d[f])
+            assert abs(fd - g["prefactor"][f]) <= 1e-4 * abs(fd) + 1e-8, (f, fd, g["prefactor"][f])
+        lengths = np.diff(sysm.fiber_offsets)
+        mask = np.repeat(np.arange(2) == 1, lengths)
+        p = sysm.parameters.shape[0] - 1
+        scale = max(abs(float(sysm.parameters[p, mask][0])), 1.0)
+        dP = np.zeros_like(sysm.parameters)
+        dP[p, mask] = h * scale
+        fd = (L(sysm.prefactor, sysm.parameters + dP) - L(sysm.prefactor, sysm.parameters - dP)) / (2 * h * scale)
+        ad = float(g["parameters"][p, mask].sum())
+        assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-8, (fd, ad)
+    finally:
+        eng.close()

@@ -167,3 +167,32 @@ def test_coupling_from_settings_matches_oracles():
         want, _ = EO.bidomain(Ki, Kie, EO.map_values(pos, shape, el, fac, st[0]))
         assert np.max(np.abs(phi - want)) <= 1e-6 * max(np.abs(want).max(), 1.0)
     assert np.abs(phis[-1][1]).max() > 0
+
+
+def test_surface_sample_and_bad_inputs():
+    shape, pos, bn, bv = _deformed_mesh()
+    rng = np.random.default_rng(9)
+    with _solver(shape, pos, bn, bv) as slv:
+        slv.set_vm(rng.normal(size=len(pos)))
+        slv.advanceTimeSpan()
+        phi = slv.phi_e()
+        nx, ny, nz = shape
+        top = slv.surface("2+")
+        assert top.shape == (ny, nx)
+        np.testing.assert_array_equal(top, phi[-nx * ny:].reshape(ny, nx))
+        np.testing.assert_array_equal(slv.surface("0-"), phi.reshape(nz, ny, nx)[:, :, 0])
+        # at nodes the interpolation returns the nodal values; outside the mesh NaN
+        pick = [0, 17, len(pos) // 2, len(pos) - 1]
+        np.testing.assert_allclose(slv.sample(pos[pick]), phi[pick], rtol=0, atol=1e-9)
+        assert np.isnan(slv.sample([[50.0, 50.0, 50.0]]))[0]
+        with pytest.raises(S.N.FdmError):
+            slv.set_fiber_mapping(np.zeros((3, 3)))
+            with S.FastMonodomainSolver(H.complete(H.c1_system(n_fibers=1, n_nodes=11, end_time=0.01))) as f:
+                f.initialize()
+                slv.map_fibers(f)                # 11 fiber nodes against a mapping of 3
+    inverted = pos.copy()
+    inverted[:, 0] *= -1.0                       # mirrored: every element inverted
+    with pytest.raises(S.N.FdmError) as e:
+        E.StaticBidomainSolver(shape, inverted, WL.EMG_SIGMA_I, WL.EMG_SIGMA_E, dirichlet_nodes=bn,
+                               dirichlet_values=bv).initialize()
+    assert e.value.code == S.N.FDM_ERR_ARG
