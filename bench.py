@@ -208,11 +208,13 @@ def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iter
     solver_cfg = {"relativeTolerance": 1e-8, "absoluteTolerance": 1e-30, "maxIterations": 20000}
     if coupled:
         out["coupled"] = emg_coupled(device, solver_cfg)
+        seq = emg_coupled(device, solver_cfg, overlap=False)
+        out["coupled"]["sequential_ms_per_coupling_step"] = seq["ms_per_coupling_step"]
     _cg_iteration(out, device, peak_hbm, cg_mesh, cg_iterations, solver_cfg)
     return out
 
 
-def emg_coupled(device: int, solver_cfg: dict) -> dict:
+def emg_coupled(device: int, solver_cfg: dict, overlap: bool = True) -> dict:
     import torch
     from opendihu_b200 import emg as E
     from opendihu_b200 import solver as S
@@ -221,7 +223,7 @@ def emg_coupled(device: int, solver_cfg: dict) -> dict:
     fib = S.FastMonodomainSolver(system, method="fused", precision="fp32", device=device, autotune=True)
     bid = E.StaticBidomainSolver(emg_solver=solver_cfg, potential_flow_solver=solver_cfg, device=device, **kw)
     solves = []
-    cp = E.Coupling(fib, bid, 1.0, 5.0, fpos, callback=lambda k, t, b: solves.append(b.timing()))
+    cp = E.Coupling(fib, bid, 1.0, 5.0, fpos, callback=lambda k, t, b: solves.append(b.timing()), overlap=overlap)
     with cp:
         cp.term1.setTimeSpan(0.0, 1.0)       # warm-up: one coupling step outside the timed span
         cp.term1.advanceTimeSpan()
@@ -243,7 +245,9 @@ def emg_coupled(device: int, solver_cfg: dict) -> dict:
         "emg_solve_ms": float(np.mean([t["solve_ms"] for t in solves])) if solves else None,
         "cg_iterations": [t["iterations"] for t in solves], "phi_e_max_abs": float(np.abs(phi).max()),
         "fiber_layout": layout,
-        "timing": "host wall clock around the coupled steps (fiber advance + transfer + solve)"}
+        "overlap": overlap,
+        "timing": "host wall clock around the coupled steps (fiber advance + transfer + solve; with overlap the "
+                  "solve of step k runs beside the fiber advance of step k + 1)"}
 
 
 def _cg_iteration(out: dict, device: int, peak_hbm: float, cg_mesh, cg_iterations: int, solver_cfg: dict):

@@ -354,11 +354,16 @@ def _find_element(pos, shape, x, tol: float = 1e-9):
 class Coupling:
     """Control::Coupling of the fiber solver (Term1) and the static bidomain solver (Term2): per step of
     ``time_step_width`` the fibers advance, their Vm is mapped onto the 3D mesh and phi_e is solved
-    (coupling_or_godunov.tpp:12-131); ``callback(step, t, bidomain)`` runs after each step."""
+    (coupling_or_godunov.tpp:12-131); ``callback(step, t, bidomain)`` runs after each step's solve.
+
+    Nothing flows back from the bidomain solver to the fibers (connectedSlotsTerm2To1 [None]), so with
+    ``overlap`` (default) the solve of step k runs on its own stream, driven by a worker thread, while the
+    fibers advance step k + 1; the transfer of step k + 1 waits for that solve.  The results are those of the
+    sequential order."""
 
     def __init__(self, term1: S.FastMonodomainSolver, term2: StaticBidomainSolver, time_step_width: float,
                  end_time: float, fiber_positions, start_time: float = 0.0, xi_tolerance: float = 0.1,
-                 default_value: float = 0.0, callback: Optional[Callable] = None):
+                 default_value: float = 0.0, callback: Optional[Callable] = None, overlap: bool = True):
         self.term1, self.term2 = term1, term2
         self.time_step_width = float(time_step_width)
         self.start_time, self.end_time = float(start_time), float(end_time)
@@ -367,8 +372,10 @@ class Coupling:
             raise ValueError("one position per fiber node needed")
         self.xi_tolerance, self.default_value = float(xi_tolerance), float(default_value)
         self.callback = callback
+        self.overlap = bool(overlap)
         self.n_mapped = 0
         self.initialized = False
+        self._pool = None
 
     @classmethod
     def from_settings(cls, config: dict, device: int = 0, **kw) -> "Coupling":
@@ -420,21 +427,44 @@ class Coupling:
         span = self.end_time - self.start_time
         dt = span / n
         t = self.start_time
-        for k in range(n):
-            self.term1.setTimeSpan(t, t + dt)
-            self.term1.advanceTimeSpan()
-            self.term2.map_fibers(self.term1)
-            self.term2.setTimeSpan(t, t + dt)
-            self.term2.advanceTimeSpan()
+        pending = None      # (future, step, time) of the solve still running
+
+        def finish(p):
+            p[0].result()
             if self.callback is not None:
-                self.callback(k, t + dt, self.term2)
-            t = self.start_time + (k + 1) / n * span
+                self.callback(p[1], p[2], self.term2)
+
+        if self.overlap and self._pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="bidomain")
+        try:
+            for k in range(n):
+                self.term1.setTimeSpan(t, t + dt)
+                self.term1.advanceTimeSpan()
+                if pending is not None:
+                    finish(pending)     # the previous solve reads the 3D Vm the transfer overwrites
+                    pending = None
+                self.term2.map_fibers(self.term1)
+                self.term2.setTimeSpan(t, t + dt)
+                if self.overlap:
+                    pending = (self._pool.submit(self.term2.advanceTimeSpan), k, t + dt)
+                else:
+                    self.term2.advanceTimeSpan()
+                    if self.callback is not None:
+                        self.callback(k, t + dt, self.term2)
+                t = self.start_time + (k + 1) / n * span
+        finally:
+            if pending is not None:
+                finish(pending)
 
     def run(self):
         self.initialize()
         self.advanceTimeSpan()
 
     def close(self):
+        if self._pool is not None:
+            self._pool.shutdown(wait=True)
+            self._pool = None
         self.term1.close()
         self.term2.close()
 

@@ -196,3 +196,23 @@ def test_surface_sample_and_bad_inputs():
         E.StaticBidomainSolver(shape, inverted, WL.EMG_SIGMA_I, WL.EMG_SIGMA_E, dirichlet_nodes=bn,
                                dirichlet_values=bv).initialize()
     assert e.value.code == S.N.FDM_ERR_ARG
+
+
+def test_overlapped_coupling_equals_sequential():
+    cfg, fpos, kw = _settings(end=1.5)
+    out = {}
+    for overlap in (False, True):
+        phis = []
+        cp = E.Coupling.from_settings(cfg)
+        cp.overlap = overlap
+        cp.callback = lambda k, t, emg: phis.append((k, round(t, 9), emg.phi_e(), emg.vm()))
+        with cp:
+            cp.run()
+            vm = cp.term1.states()[0]
+        out[overlap] = (phis, vm)
+    a, b = out[False], out[True]
+    np.testing.assert_array_equal(a[1], b[1])
+    assert [p[:2] for p in a[0]] == [p[:2] for p in b[0]] == [(0, 0.5), (1, 1.0), (2, 1.5)]
+    for pa, pb in zip(a[0], b[0]):
+        np.testing.assert_array_equal(pa[2], pb[2])
+        np.testing.assert_array_equal(pa[3], pb[3])
