@@ -1,0 +1,292 @@
+/* C++ host class over the C ABI of include/fdm_b200.h: the reference's operator API for the fast fiber path.
+ *
+ * fdm::FastMonodomainSolver has the method names and meaning of the reference's FastMonodomainSolverBase
+ * (core/src/specialized_solver/fast_monodomain_solver/fast_monodomain_solver_base.h:85-124): initialize, run,
+ * advanceTimeSpan, setTimeSpan, startTime, endTime, data, reset, callOutputWriter,
+ * saveFiberDataCheckpoint, restoreFiberDataCheckpoint.  advanceTimeSpan over [startTime, endTime] is the
+ * RepeatedCall loop that drives it in the reference (core/src/control/repeated_call.tpp:43-80).  It is built
+ * from fdm::FiberSettings -- the parsed settings (the fiber geometry, the CellML parameters and initial
+ * states, the stimulation tables and the time step widths) -- not from PETSc objects; FiberSettings::load
+ * reads the file opendihu_b200.solver.write_host_settings writes from a reference settings dict.
+ * Errors are fdm::Error exceptions carrying the library's status code and message.
+ * Header only; link with -lfdm_b200 (opendihu_b200/libfdm_b200.so). */
+#ifndef FDM_B200_HPP
+#define FDM_B200_HPP
+
+#include <cstdint>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "fdm_b200.h"
+
+namespace fdm {
+
+class Error : public std::runtime_error {
+ public:
+  Error(int code, const std::string& msg) : std::runtime_error(msg), code_(code) {}
+  int code() const { return code_; }
+
+ private:
+  int code_;
+};
+
+/* The parsed settings of one FastMonodomainSolver (all fibers of the rank). */
+struct FiberSettings {
+  fdm_config config{};                       // model, schemes, method, precision, time step widths, options
+  double start_time = 0.0, end_time = 0.0;   // RepeatedCall startTime / endTime
+  std::vector<int64_t> fiber_offsets;        // n_fibers + 1 node offsets
+  std::vector<double> element_lengths;       // per fiber n_f - 1 lengths, concatenated
+  std::vector<double> prefactor;             // per fiber sigma / (Am Cm)
+  std::vector<double> parameters;            // [parameter][node] (empty: the model's defaults)
+  std::vector<double> states;                // [state][node] (empty: the model's initial values)
+  std::vector<uint8_t> firing_events;        // [row][motor unit]
+  int firing_rows = 0, firing_cols = 0;
+  std::vector<int> motor_unit_no, stimulation_point_index;
+  std::vector<double> call_frequency, repeat_after_first_call, call_enable_begin;
+  std::vector<double> jitter;                // [fiber][k]
+  int n_jitter = 0;
+  std::vector<int> algebraics_for_transfer, states_for_transfer{0};
+
+  int n_fibers() const { return fiber_offsets.empty() ? 0 : (int)fiber_offsets.size() - 1; }
+  int64_t n_nodes() const { return fiber_offsets.empty() ? 0 : fiber_offsets.back(); }
+
+  /* Reads "key count value..." lines (the format write_host_settings writes; '#' starts a comment). */
+  static FiberSettings load(const std::string& path)
+  {
+    std::ifstream in(path);
+    if (!in)
+      throw Error(FDM_ERR_ARG, "fdm::FiberSettings::load: cannot open " + path);
+    std::map<std::string, std::vector<double>> kv;
+    std::string line;
+    while (std::getline(in, line)) {
+      if (line.empty() || line[0] == '#')
+        continue;
+      std::istringstream ls(line);
+      std::string key;
+      long long count = 0;
+      if (!(ls >> key >> count) || count < 0)
+        throw Error(FDM_ERR_ARG, "fdm::FiberSettings::load: bad line: " + line.substr(0, 80));
+      std::vector<double> v((size_t)count);
+      for (auto& x : v)
+        if (!(ls >> x))
+          throw Error(FDM_ERR_ARG, "fdm::FiberSettings::load: too few values for " + key);
+      kv[key] = std::move(v);
+    }
+    FiberSettings s;
+    fdm_config_default(&s.config);
+    auto has = [&](const char* k) { return kv.count(k) > 0; };
+    auto num = [&](const char* k) -> double {
+      auto it = kv.find(k);
+      if (it == kv.end() || it->second.size() != 1)
+        throw Error(FDM_ERR_ARG, std::string("fdm::FiberSettings::load: missing scalar ") + k);
+      return it->second[0];
+    };
+    auto vec = [&](const char* k) -> const std::vector<double>& {
+      static const std::vector<double> empty;
+      auto it = kv.find(k);
+      return it == kv.end() ? empty : it->second;
+    };
+    auto as_int = [&](const char* k) {
+      std::vector<int> o;
+      for (double x : vec(k))
+        o.push_back((int)x);
+      return o;
+    };
+    fdm_config& c = s.config;
+    c.model = (int)num("model");
+    c.diffusion_scheme = (int)num("diffusion_scheme");
+    c.method = (int)num("method");
+    c.reaction_precision = (int)num("reaction_precision");
+    c.approximate_exponential_function = (int)num("approximate_exponential_function");
+    c.clamp_rule = (int)num("clamp_rule");
+    c.vc_width = (int)num("vc_width");
+    c.n_ranks = (int)num("n_ranks");
+    c.stimulus_mode = (int)num("stimulus_mode");
+    c.stimulus_parameter = (int)num("stimulus_parameter");
+    c.stimulus_value = num("stimulus_value");
+    c.value_for_stimulated_point = num("value_for_stimulated_point");
+    c.dt_repeated_call = num("dt_repeated_call");
+    c.dt_splitting = num("dt_splitting");
+    c.dt_0d = num("dt_0d");
+    c.dt_1d = num("dt_1d");
+    c.only_compute_if_stimulated = (int)num("only_compute_if_stimulated");
+    c.skip_close_to_equilibrium = (int)num("skip_close_to_equilibrium");
+    if (has("device"))
+      c.device = (int)num("device");
+    s.start_time = num("start_time");
+    s.end_time = num("end_time");
+    for (double x : vec("fiber_offsets"))
+      s.fiber_offsets.push_back((int64_t)x);
+    s.element_lengths = vec("element_lengths");
+    s.prefactor = vec("prefactor");
+    s.parameters = vec("parameters");
+    s.states = vec("states");
+    for (double x : vec("firing_events"))
+      s.firing_events.push_back((uint8_t)x);
+    s.firing_rows = (int)num("firing_rows");
+    s.firing_cols = (int)num("firing_cols");
+    s.motor_unit_no = as_int("motor_unit_no");
+    s.stimulation_point_index = as_int("stimulation_point_index");
+    s.call_frequency = vec("call_frequency");
+    s.repeat_after_first_call = vec("repeat_after_first_call");
+    s.call_enable_begin = vec("call_enable_begin");
+    s.jitter = vec("jitter");
+    s.n_jitter = (int)num("n_jitter");
+    s.algebraics_for_transfer = as_int("algebraics_for_transfer");
+    if (has("states_for_transfer"))
+      s.states_for_transfer = as_int("states_for_transfer");
+    return s;
+  }
+};
+
+/* The transferred fiber data (updateFiberData: statesForTransfer, algebraicsForTransfer), [k][node]. */
+struct TransferData {
+  std::vector<double> vm;
+  std::vector<double> states;      // statesForTransfer[1..]
+  std::vector<double> algebraics;  // algebraicsForTransfer
+};
+
+class FastMonodomainSolver {
+ public:
+  explicit FastMonodomainSolver(FiberSettings settings) : s_(std::move(settings))
+  {
+    start_ = s_.start_time;
+    end_ = s_.end_time;
+  }
+  FastMonodomainSolver(const FastMonodomainSolver&) = delete;
+  FastMonodomainSolver& operator=(const FastMonodomainSolver&) = delete;
+  FastMonodomainSolver(FastMonodomainSolver&& o) noexcept : s_(std::move(o.s_)), h_(o.h_), start_(o.start_), end_(o.end_)
+  {
+    o.h_ = nullptr;
+  }
+  ~FastMonodomainSolver() { reset(); }
+
+  void initialize()
+  {
+    if (h_)
+      return;
+    fdm_solver* h = nullptr;
+    int rc = fdm_create(&s_.config, &h);
+    if (rc != FDM_OK)
+      throw Error(rc, std::string("fdm_create: ") + fdm_last_error(nullptr));
+    h_ = h;
+    try {
+      const int nf = s_.n_fibers();
+      check(fdm_set_fibers(h_, nf, s_.fiber_offsets.data(), s_.element_lengths.data(), s_.prefactor.data()));
+      if (!s_.parameters.empty())
+        check(fdm_set_parameters(h_, s_.parameters.data()));
+      if (!s_.states.empty())
+        check(fdm_set_states(h_, s_.states.data()));
+      const double zero = 0.0;
+      check(fdm_set_stimulation(h_, s_.firing_events.data(), s_.firing_rows, s_.firing_cols,
+                                s_.motor_unit_no.data(), s_.stimulation_point_index.data(), s_.call_frequency.data(),
+                                s_.repeat_after_first_call.data(), s_.call_enable_begin.data(),
+                                s_.jitter.empty() ? &zero : s_.jitter.data(), s_.n_jitter));
+      if (!s_.algebraics_for_transfer.empty())
+        check(fdm_set_algebraics_for_transfer(h_, (int)s_.algebraics_for_transfer.size(),
+                                              s_.algebraics_for_transfer.data()));
+    } catch (...) {
+      reset();
+      throw;
+    }
+  }
+
+  void run()
+  {
+    initialize();
+    advanceTimeSpan();
+  }
+
+  /* RepeatedCall over [startTime, endTime]; there are no output writers in this build, the flag is kept
+   * for the signature */
+  void advanceTimeSpan(bool withOutputWritersEnabled = true)
+  {
+    (void)withOutputWritersEnabled;
+    initialize();
+    check(fdm_advance(h_, start_, end_));
+  }
+
+  void setTimeSpan(double startTime, double endTime)
+  {
+    start_ = startTime;
+    end_ = endTime;
+  }
+  double startTime() const { return start_; }
+  double endTime() const { return end_; }
+
+  /* Vm, statesForTransfer[1..] and algebraicsForTransfer of every node */
+  TransferData data()
+  {
+    initialize();
+    TransferData d;
+    const int64_t n = s_.n_nodes();
+    int ns = 0, na = 0, np = 0;
+    check(fdm_model_info(s_.config.model, &ns, &na, &np, nullptr));
+    std::vector<double> st((size_t)ns * n);
+    if (n > 0)
+      check(fdm_get_states(h_, st.data()));
+    d.vm.assign(st.begin(), st.begin() + n);
+    for (size_t k = 1; k < s_.states_for_transfer.size(); k++) {
+      const int idx = s_.states_for_transfer[k];
+      d.states.insert(d.states.end(), st.begin() + (size_t)idx * n, st.begin() + (size_t)(idx + 1) * n);
+    }
+    if (!s_.algebraics_for_transfer.empty()) {
+      d.algebraics.resize(s_.algebraics_for_transfer.size() * (size_t)n);
+      check(fdm_get_algebraics(h_, d.algebraics.data()));
+    }
+    return d;
+  }
+
+  /* all states [state][node] */
+  std::vector<double> states()
+  {
+    initialize();
+    int ns = 0, na = 0, np = 0;
+    check(fdm_model_info(s_.config.model, &ns, &na, &np, nullptr));
+    std::vector<double> st((size_t)ns * s_.n_nodes());
+    if (!st.empty())
+      check(fdm_get_states(h_, st.data()));
+    return st;
+  }
+
+  void reset()
+  {
+    if (h_)
+      fdm_destroy(h_);
+    h_ = nullptr;
+  }
+
+  /* no output writers in this build (the fiber data comes back through data()) */
+  void callOutputWriter(int timeStepNo, double currentTime, int callCountIncrement = 1)
+  {
+    (void)timeStepNo;
+    (void)currentTime;
+    (void)callCountIncrement;
+  }
+
+  void saveFiberDataCheckpoint() { check(fdm_checkpoint_save(h_)); }
+  void restoreFiberDataCheckpoint() { check(fdm_checkpoint_restore(h_)); }
+
+  fdm_solver* handle() { return h_; }
+  const FiberSettings& settings() const { return s_; }
+
+ private:
+  void check(int rc)
+  {
+    if (rc != FDM_OK)
+      throw Error(rc, fdm_last_error(h_));
+  }
+
+  FiberSettings s_;
+  fdm_solver* h_ = nullptr;
+  double start_ = 0.0, end_ = 0.0;
+};
+
+}  // namespace fdm
+
+#endif /* FDM_B200_HPP */

@@ -308,6 +308,48 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     return sys_
 
 
+def write_host_settings(system: FiberSystem, path: str, method: Optional[str] = None,
+                        precision: Optional[str] = None, device: int = 0) -> None:
+    """The parsed settings as the "key count value..." lines fdm::FiberSettings::load reads
+    (include/fdm_b200.hpp): the input of the C++ host class fdm::FastMonodomainSolver."""
+    s = system
+    ns, _, npar, init, defaults = model_sizes(s.model)
+    n = s.n_nodes
+    states = s.states if s.states is not None else np.repeat(np.asarray(init)[:, None], n, axis=1)
+    params = s.parameters if s.parameters is not None else np.repeat(np.asarray(defaults)[:, None], n, axis=1)
+    fe = np.asarray(s.firing_events, np.uint8)
+    jit = np.asarray(s.jitter if s.jitter is not None else np.zeros((s.n_fibers, 0)), np.float64)
+    scalars = {
+        "model": N.MODEL_IDS[s.model], "diffusion_scheme": SCHEMES[s.diffusion_scheme],
+        "method": METHODS[method or getattr(s, "method", "split")],
+        "reaction_precision": PRECISIONS[precision or getattr(s, "precision", "fp64")],
+        "approximate_exponential_function": int(bool(s.approximate_exponential_function)),
+        "clamp_rule": CLAMP_RULES[s.clamp_rule], "vc_width": s.vc_width, "n_ranks": s.n_ranks,
+        "stimulus_mode": STIMULUS_MODES[s.stimulus_mode], "stimulus_parameter": s.stimulus_parameter,
+        "stimulus_value": s.stimulus_value, "value_for_stimulated_point": s.value_for_stimulated_point,
+        "dt_repeated_call": s.dt_repeated_call, "dt_splitting": s.dt_splitting, "dt_0d": s.dt_0d, "dt_1d": s.dt_1d,
+        "only_compute_if_stimulated": int(bool(s.only_compute_if_has_been_stimulated)),
+        "skip_close_to_equilibrium": int(bool(s.skip_close_to_equilibrium)), "device": device,
+        "start_time": s.start_time, "end_time": s.end_time, "firing_rows": fe.shape[0], "firing_cols": fe.shape[1],
+        "n_jitter": jit.shape[1] if jit.ndim == 2 else 0,
+    }
+    arrays = {
+        "fiber_offsets": s.fiber_offsets, "element_lengths": s.element_lengths, "prefactor": s.prefactor,
+        "parameters": params, "states": states, "firing_events": fe, "motor_unit_no": s.motor_unit_no,
+        "stimulation_point_index": s.stimulation_point_index, "call_frequency": s.call_frequency,
+        "repeat_after_first_call": s.repeat_after_first_call, "call_enable_begin": s.call_enable_begin,
+        "jitter": jit, "algebraics_for_transfer": s.algebraics_for_transfer,
+        "states_for_transfer": s.states_for_transfer,
+    }
+    with open(path, "w") as f:
+        f.write("# opendihu_b200 host settings: key count values\n")
+        for k, v in scalars.items():
+            f.write(f"{k} 1 {float(v)!r}\n")
+        for k, v in arrays.items():
+            a = np.asarray(v, np.float64).ravel()
+            f.write(f"{k} {a.size} " + " ".join(repr(float(x)) for x in a) + "\n")
+
+
 # ----------------------------------------------------------------------------------------------
 # the operator
 # ----------------------------------------------------------------------------------------------

@@ -1,0 +1,46 @@
+// Drives fdm::FastMonodomainSolver (include/fdm_b200.hpp) the way the reference's RepeatedCall and preCICE
+// drive its FastMonodomainSolver: settings in, setTimeSpan/advanceTimeSpan twice with a checkpoint between,
+// the checkpoint replayed, the states and the transferred algebraics written out.
+//   host_class_main <settings file> <output file> <intermediate time>
+// Exit status: 0 done, 2 fdm::Error (message on stderr), 3 the replay after the checkpoint differs.
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+
+#include "fdm_b200.hpp"
+
+int main(int argc, char** argv)
+{
+  if (argc != 4) {
+    std::fprintf(stderr, "usage: %s settings output t_mid\n", argv[0]);
+    return 1;
+  }
+  try {
+    fdm::FiberSettings s = fdm::FiberSettings::load(argv[1]);
+    const double t_mid = std::atof(argv[3]);
+    fdm::FastMonodomainSolver slv(s);
+    slv.initialize();
+    slv.setTimeSpan(s.start_time, t_mid);
+    slv.advanceTimeSpan();
+    slv.saveFiberDataCheckpoint();
+    slv.setTimeSpan(t_mid, s.end_time);
+    slv.advanceTimeSpan();
+    const std::vector<double> a = slv.states();
+    slv.restoreFiberDataCheckpoint();
+    slv.advanceTimeSpan();
+    const std::vector<double> b = slv.states();
+    if (a != b) {
+      std::fprintf(stderr, "the replay after restoreFiberDataCheckpoint differs\n");
+      return 3;
+    }
+    const fdm::TransferData d = slv.data();
+    std::ofstream out(argv[2], std::ios::binary);
+    out.write(reinterpret_cast<const char*>(a.data()), (std::streamsize)(a.size() * sizeof(double)));
+    out.write(reinterpret_cast<const char*>(d.algebraics.data()), (std::streamsize)(d.algebraics.size() * sizeof(double)));
+    std::printf("startTime %g endTime %g nodes %lld\n", slv.startTime(), slv.endTime(), (long long)s.n_nodes());
+    return 0;
+  } catch (const fdm::Error& e) {
+    std::fprintf(stderr, "fdm::Error %d: %s\n", e.code(), e.what());
+    return 2;
+  }
+}

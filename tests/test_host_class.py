@@ -1,0 +1,67 @@
+"""The C++ host class fdm::FastMonodomainSolver (include/fdm_b200.hpp): compiled with g++ against the
+library; on CPU it builds, reads the settings the Python harness writes and fails loudly without a device;
+on the GPU its run (two advances around a checkpoint, the checkpoint replayed) equals the Python operator's
+bit for bit and the oracle within the FP64 tolerance."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import helpers as H
+import test_gpu_parity as GP
+from opendihu_b200 import solver as S
+
+SRC = os.path.join(H.ROOT, "tests", "cpp", "host_class_main.cpp")
+LIBDIR = os.path.join(H.ROOT, "opendihu_b200")
+
+
+def _build(tmp_path):
+    exe = str(tmp_path / "host_class_main")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(H.ROOT, "include"), SRC,
+                    "-L", LIBDIR, "-lfdm_b200", "-Wl,-rpath," + LIBDIR, "-o", exe], check=True)
+    return exe
+
+
+def _system():
+    s = GP.small_system(end_time=0.6, algebraics_for_transfer=[0, 4])
+    return H.complete(s)
+
+
+def test_builds_reads_settings_and_fails_loudly_without_device(tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the GPU test runs the class")
+    exe = _build(tmp_path)
+    cfg = str(tmp_path / "settings.txt")
+    S.write_host_settings(_system(), cfg)
+    r = subprocess.run([exe, cfg, str(tmp_path / "out.bin"), "0.3"], capture_output=True, text=True)
+    assert r.returncode == 2 and "fdm::Error 5" in r.stderr, (r.returncode, r.stderr)
+    r = subprocess.run([exe, str(tmp_path / "missing.txt"), "x", "0.3"], capture_output=True, text=True)
+    assert r.returncode == 2 and "cannot open" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method,precision", [("split", "fp64"), ("fused", "fp32")])
+def test_cpp_host_class_equals_python_operator(tmp_path, method, precision):
+    exe = _build(tmp_path)
+    s = _system()
+    cfg = str(tmp_path / "settings.txt")
+    S.write_host_settings(s, cfg, method=method, precision=precision)
+    out = str(tmp_path / "out.bin")
+    r = subprocess.run([exe, cfg, out, "0.3"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = np.fromfile(out, np.float64)
+    ns = 4
+    st = raw[:ns * s.n_nodes].reshape(ns, s.n_nodes)
+    alg = raw[ns * s.n_nodes:].reshape(2, s.n_nodes)
+    with S.FastMonodomainSolver(s.copy(), method=method, precision=precision) as slv:
+        slv.setTimeSpan(0.0, 0.3)
+        slv.advanceTimeSpan()
+        slv.setTimeSpan(0.3, 0.6)
+        slv.advanceTimeSpan()
+        np.testing.assert_array_equal(st, slv.states())
+        np.testing.assert_array_equal(alg, slv.algebraics())
+    if precision == "fp64":
+        ref, _, _, _ = H.run_oracle(s.copy())
+        assert np.max(np.abs(st[0] - ref[0])) <= GP.VM_TOL_FP64
