@@ -256,22 +256,35 @@ def _cg_iteration(out: dict, device: int, peak_hbm: float, cg_mesh, cg_iteration
     from opendihu_b200 import workloads as WL
     _, _, kw2 = WL.emg_box(n_fibers_x=2, n_fibers_y=2, n_nodes=1481, mesh_nodes=tuple(cg_mesh), width=3.0)
     z = kw2["node_positions"][:, 2]
+    vm = -75.0 + 100.0 * np.exp(-((z - z.mean()) / 0.3) ** 2)
     with E.StaticBidomainSolver(emg_solver={"relativeTolerance": 1e-30, "absoluteTolerance": 0.0,
                                             "maxIterations": cg_iterations},
-                                potential_flow_solver=solver_cfg, device=device, **kw2) as big:
-        big.set_vm(-75.0 + 100.0 * np.exp(-((z - z.mean()) / 0.3) ** 2))
+                                potential_flow_solver=solver_cfg, device=device, preconditioner="jacobi",
+                                **kw2) as big:
+        big.set_vm(vm)
         big.advanceTimeSpan()
         big.initial_guess_nonzero = False
         big.advanceTimeSpan()
         t = big.timing()
         n = big.n_nodes
+    # the whole solve to rtol 1e-8 from a zero initial guess with either preconditioner
+    solves = {}
+    for pc in ("jacobi", "multigrid"):
+        with E.StaticBidomainSolver(emg_solver=solver_cfg, potential_flow_solver=solver_cfg, device=device,
+                                    preconditioner=pc, initial_guess_nonzero=False, **kw2) as sv:
+            sv.set_vm(vm)
+            sv.advanceTimeSpan()
+            sv.advanceTimeSpan()
+            tt = sv.timing()
+            solves[pc] = {"solve_ms": tt["solve_ms"], "iterations": tt["iterations"], "levels": sv.multigrid_levels}
     per_it_ms = t["solve_ms"] / max(t["iterations"], 1)
     # algorithmic bytes per node and iteration: direction pass (14 stencil coefficients, z, p and q read, p and
     # q written: 152 B) + update pass (x, r read and written, p, q, dinv read, z written: 64 B)
     bytes_it = 216 * n
     gbs = bytes_it / (per_it_ms / 1e3) / 1e9
     out["cg_iteration"] = {"workload": "%d x %d x %d mesh (%d nodes), %d iterations" % (*cg_mesh, n, cg_iterations),
-                           "iterations": t["iterations"],
+                           "iterations": t["iterations"], "preconditioner": "jacobi",
+                           "solve_to_rtol_1e-8": solves,
                            "solve_ms": t["solve_ms"], "ms_per_iteration": per_it_ms,
                            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak_hbm, "unit": "GB/s",
                                         "frac": gbs / peak_hbm, "algorithmic_bytes_per_node_iteration": 216,

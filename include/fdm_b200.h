@@ -272,6 +272,12 @@ int fdm_emg_map_values(fdm_emg *m, const double *fiber_values);
 int fdm_emg_set_vm(fdm_emg *m, const double *vm);
 int fdm_emg_solve(fdm_emg *m, double rtol, double atol, int max_iterations, int initial_guess_nonzero,
                   int *iterations, double *residual);
+/* preconditioner of the bidomain solve ("preconditionerType"): Jacobi, or (default) a geometric multigrid
+ * V-cycle (structured coarsening by 2, Galerkin coarse operators, two damped-Jacobi sweeps before and after);
+ * levels: the number of grid levels (1 for Jacobi; the hierarchy is built once the operators exist) */
+#define FDM_EMG_PRECOND_JACOBI 0
+#define FDM_EMG_PRECOND_MULTIGRID 1
+int fdm_emg_set_preconditioner(fdm_emg *m, int type, int *levels);
 int fdm_emg_get(fdm_emg *m, int field, double *out);
 /* the assembled stencils, coef[q * N + node] with q = (dx+1) + 3(dy+1) + 9(dz+1); which: 0 K(sigma_i),
  * 1 K(sigma_i + sigma_e) */

@@ -33,7 +33,7 @@ EXPORTED = [
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
     "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes", "fdm_get_equilibrium_state",
     "fdm_cellml_rhs_device", "fdm_cellml_rhs_configure", "fdm_fused_cluster_shapes", "fdm_fused_layout",
-    "fdm_get_compute_state_information", "fdm_emg_create", "fdm_emg_destroy", "fdm_emg_last_error",
+    "fdm_get_compute_state_information", "fdm_emg_set_preconditioner", "fdm_emg_create", "fdm_emg_destroy", "fdm_emg_last_error",
     "fdm_emg_potential_flow", "fdm_emg_set_direction", "fdm_emg_set_conductivity", "fdm_emg_set_fiber_mapping",
     "fdm_emg_map_fibers", "fdm_emg_map_values", "fdm_emg_set_vm", "fdm_emg_solve", "fdm_emg_get",
     "fdm_emg_get_stencil", "fdm_emg_timing",
@@ -41,6 +41,7 @@ EXPORTED = [
 
 #: fdm_emg_get fields of include/fdm_b200.h
 EMG_PHI_E, EMG_VM, EMG_RHS, EMG_FLOW_POTENTIAL, EMG_DIRECTION = 0, 1, 2, 3, 4
+EMG_PRECOND_JACOBI, EMG_PRECOND_MULTIGRID = 0, 1
 
 #: FDM_NOALLOC_MAX_NODES of include/fdm_b200.h
 NOALLOC_MAX_NODES = 262144
@@ -127,6 +128,7 @@ def lib() -> C.CDLL:
         "fdm_emg_get": (C.c_int, [P, C.c_int, d]),
         "fdm_emg_get_stencil": (C.c_int, [P, C.c_int, d]),
         "fdm_emg_timing": (C.c_int, [P, d, i32, d]),
+        "fdm_emg_set_preconditioner": (C.c_int, [P, C.c_int, i32]),
         "fdm_diffusion_solve": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_diffusion_solve_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, P, P]),
         "fdm_compat_configure": (C.c_int, [C.c_int] * 13),

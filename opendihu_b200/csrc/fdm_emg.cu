@@ -588,6 +588,226 @@ __global__ void inverse_diag_kernel(int64_t N, const double* diag /* the centre 
     dinv[n] = (mask && mask[n]) ? 0.0 : (diag[n] != 0.0 ? 1.0 / diag[n] : 1.0);
 }
 
+// ---- geometric multigrid preconditioner (bidomain solve) ----------------------------------------------
+// Coarsening per direction: coarse nodes at the fine indices 0, 2, 4, ... and the last one; interpolation
+// linear in the index between neighbouring coarse nodes (P); coarse operators P^T A P (Galerkin);
+// l1-Jacobi smoothing (x += (b - A x) / sum_m |a_nm|: convergent for symmetric positive semidefinite A
+// without a damping estimate -- Baker, Falgout, Kolev, Yang, "Multigrid smoothers for ultraparallel
+// computing", SIAM J. Sci. Comput. 33 (2011)), two sweeps before and after; on the coarsest grid the same
+// sweeps in one block.  Pre- and post-smoothing by the same symmetric smoother make the V-cycle a symmetric
+// positive semidefinite preconditioner.
+constexpr int MG_MAX_LEVELS = 12;
+constexpr int MG_COARSEST = 1024;   // nodes of the grid solved by sweeps in one block
+constexpr int MG_COARSEST_SWEEPS = 30;
+
+struct MgMap {
+  Grid fine, coarse;
+  const int* lo[3];      // per fine index: the coarse node at or below it
+  const double* w[3];    // per fine index: weight of coarse node lo + 1 (that of lo is 1 - w)
+  const int* rlo[3];     // per coarse index: the fine range of its interpolation support
+  const int* rhi[3];
+};
+
+__device__ __forceinline__ double mg_weight(const MgMap& M, int d, int i, int c)
+{
+  const int l = M.lo[d][i];
+  const double w = M.w[d][i];
+  return c == l ? 1.0 - w : (c == l + 1 ? w : 0.0);
+}
+
+// one row of P^T A P: coarse node I against its 27 coarse neighbours, the centre and forward half stored
+__global__ void mg_galerkin_kernel(MgMap M, const double* __restrict__ Uf, double* __restrict__ Uc)
+{
+  const int64_t Nc = M.coarse.n_nodes(), Nf = M.fine.n_nodes();
+  const int64_t sy = M.fine.nx, sz = (int64_t)M.fine.nx * M.fine.ny;
+  for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < Nc; I += (int64_t)gridDim.x * blockDim.x) {
+    const int ci = (int)(I % M.coarse.nx), cj = (int)((I / M.coarse.nx) % M.coarse.ny),
+              ck = (int)(I / ((int64_t)M.coarse.nx * M.coarse.ny));
+    double row[27];
+    for (int q = 0; q < 27; q++)
+      row[q] = 0.0;
+    for (int fk = M.rlo[2][ck]; fk <= M.rhi[2][ck]; fk++)
+      for (int fj = M.rlo[1][cj]; fj <= M.rhi[1][cj]; fj++)
+        for (int fi = M.rlo[0][ci]; fi <= M.rhi[0][ci]; fi++) {
+          const double wI = mg_weight(M, 0, fi, ci) * mg_weight(M, 1, fj, cj) * mg_weight(M, 2, fk, ck);
+          if (wI == 0.0)
+            continue;
+          const int64_t n = M.fine.node(fi, fj, fk);
+          for (int q = 0; q < 27; q++) {
+            int dx, dy, dz;
+            stencil_offset(q, dx, dy, dz);
+            const int mi = fi + dx, mj = fj + dy, mk = fk + dz;
+            if (mi < 0 || mj < 0 || mk < 0 || mi >= M.fine.nx || mj >= M.fine.ny || mk >= M.fine.nz)
+              continue;
+            const int64_t mn = n + dx + dy * sy + dz * sz;
+            const double a = q >= 13 ? Uf[(q - 13) * Nf + n] : Uf[(13 - q) * Nf + mn];
+            if (a == 0.0)
+              continue;
+            const int lx = M.lo[0][mi], ly = M.lo[1][mj], lz = M.lo[2][mk];
+            for (int c = 0; c < 8; c++) {
+              const int Jx = lx + (c & 1), Jy = ly + ((c >> 1) & 1), Jz = lz + (c >> 2);
+              if (Jx >= M.coarse.nx || Jy >= M.coarse.ny || Jz >= M.coarse.nz)
+                continue;
+              const double wJ = mg_weight(M, 0, mi, Jx) * mg_weight(M, 1, mj, Jy) * mg_weight(M, 2, mk, Jz);
+              // a nonzero weight puts J next to I (the fine neighbour lies between the coarse neighbours of I)
+              if (wJ == 0.0 || abs(Jx - ci) > 1 || abs(Jy - cj) > 1 || abs(Jz - ck) > 1)
+                continue;
+              row[(Jx - ci + 1) + 3 * (Jy - cj + 1) + 9 * (Jz - ck + 1)] += wI * a * wJ;
+            }
+          }
+        }
+    for (int q = 13; q < 27; q++)
+      Uc[(q - 13) * Nc + I] = row[q];
+  }
+}
+
+// b_c = P^T r
+__global__ void mg_restrict_kernel(MgMap M, const double* __restrict__ r, double* __restrict__ bc)
+{
+  const int64_t Nc = M.coarse.n_nodes();
+  for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < Nc; I += (int64_t)gridDim.x * blockDim.x) {
+    const int ci = (int)(I % M.coarse.nx), cj = (int)((I / M.coarse.nx) % M.coarse.ny),
+              ck = (int)(I / ((int64_t)M.coarse.nx * M.coarse.ny));
+    double s = 0.0;
+    for (int fk = M.rlo[2][ck]; fk <= M.rhi[2][ck]; fk++) {
+      const double wz = mg_weight(M, 2, fk, ck);
+      for (int fj = M.rlo[1][cj]; fj <= M.rhi[1][cj]; fj++) {
+        const double wyz = wz * mg_weight(M, 1, fj, cj);
+        for (int fi = M.rlo[0][ci]; fi <= M.rhi[0][ci]; fi++)
+          s += wyz * mg_weight(M, 0, fi, ci) * r[M.fine.node(fi, fj, fk)];
+      }
+    }
+    bc[I] = s;
+  }
+}
+
+// x += P e_c
+__global__ void mg_prolong_add_kernel(MgMap M, const double* __restrict__ ec, double* __restrict__ x)
+{
+  const int64_t Nf = M.fine.n_nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < Nf; n += (int64_t)gridDim.x * blockDim.x) {
+    const int fi = (int)(n % M.fine.nx), fj = (int)((n / M.fine.nx) % M.fine.ny),
+              fk = (int)(n / ((int64_t)M.fine.nx * M.fine.ny));
+    const int lx = M.lo[0][fi], ly = M.lo[1][fj], lz = M.lo[2][fk];
+    double s = 0.0;
+    for (int c = 0; c < 8; c++) {
+      const int Jx = lx + (c & 1), Jy = ly + ((c >> 1) & 1), Jz = lz + (c >> 2);
+      if (Jx >= M.coarse.nx || Jy >= M.coarse.ny || Jz >= M.coarse.nz)
+        continue;
+      const double w = mg_weight(M, 0, fi, Jx) * mg_weight(M, 1, fj, Jy) * mg_weight(M, 2, fk, Jz);
+      if (w != 0.0)
+        s += w * ec[M.coarse.node(Jx, Jy, Jz)];
+    }
+    x[n] += s;
+  }
+}
+
+// 1 / sum_m |a_nm| of each row (the l1-Jacobi scaling)
+__global__ void mg_l1_kernel(Grid g, const double* __restrict__ U, double* __restrict__ dl1)
+{
+  const int64_t N = g.n_nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    // the centre, the forward entries, and the backward entries (the neighbours' forward ones; zero where
+    // the neighbour does not exist, as in stencil_row)
+    const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
+    double sum = fabs(U[n]);
+    for (int q = 14; q < 27; q++) {
+      int dx, dy, dz;
+      stencil_offset(q, dx, dy, dz);
+      const int64_t bk = n - (dx + dy * sy + dz * sz);
+      sum += fabs(U[(q - 13) * N + n]) + (bk >= 0 ? fabs(U[(q - 13) * N + bk]) : 0.0);
+    }
+    dl1[n] = sum > 0.0 ? 1.0 / sum : 0.0;
+  }
+}
+
+// l1-Jacobi sweep: xo = x + dl1 (b - A x); from zero (x null): xo = dl1 b
+__global__ void __launch_bounds__(EMG_T, 4) mg_jacobi_kernel(Grid g, const double* __restrict__ U,
+                                                             const double* __restrict__ dl1,
+                                                             const double* __restrict__ b,
+                                                             const double* __restrict__ x, double* __restrict__ xo)
+{
+  const int64_t N = g.n_nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    if (!x) {
+      xo[n] = dl1[n] * b[n];
+    } else {
+      const double ax = stencil_row(g, U, n, [&](int64_t m) { return x[m]; });
+      xo[n] = x[n] + dl1[n] * (b[n] - ax);
+    }
+  }
+}
+
+// r = b - A x
+__global__ void __launch_bounds__(EMG_T, 4) mg_residual_kernel(Grid g, const double* __restrict__ U,
+                                                               const double* __restrict__ b,
+                                                               const double* __restrict__ x, double* __restrict__ r)
+{
+  const int64_t N = g.n_nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+    r[n] = b[n] - stencil_row(g, U, n, [&](int64_t m) { return x[m]; });
+}
+
+// coarsest grid: `sweeps` l1-Jacobi sweeps from zero in one block (x and t ping-pong; x holds the result)
+__global__ void __launch_bounds__(1024) mg_coarsest_kernel(Grid g, const double* __restrict__ U,
+                                                           const double* __restrict__ dl1,
+                                                           const double* __restrict__ b, double* x, double* t,
+                                                           int sweeps)
+{
+  const int64_t N = g.n_nodes();
+  for (int64_t n = threadIdx.x; n < N; n += blockDim.x)
+    x[n] = dl1[n] * b[n];
+  __syncthreads();
+  double* cur = x;
+  double* oth = t;
+  for (int s = 1; s < sweeps; s++) {
+    for (int64_t n = threadIdx.x; n < N; n += blockDim.x) {
+      const double ax = stencil_row(g, U, n, [&](int64_t m) { return cur[m]; });
+      oth[n] = cur[n] + dl1[n] * (b[n] - ax);
+    }
+    __syncthreads();
+    double* sw = cur;
+    cur = oth;
+    oth = sw;
+  }
+  if (cur != x) {
+    for (int64_t n = threadIdx.x; n < N; n += blockDim.x)
+      x[n] = cur[n];
+  }
+}
+
+// x = z after the update: partial r.z -> beta = r.z new / r.z, r.z (preconditioner applied outside)
+__global__ void __launch_bounds__(EMG_T) cg_rz_kernel(int64_t N, const double* __restrict__ r,
+                                                      const double* __restrict__ z, double* S, double* partial,
+                                                      unsigned* counter, int first)
+{
+  double acc[1] = {0.0}, tot[1];
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
+    acc[0] += r[n] * z[n];
+  if (grid_sum<1>(acc, partial, counter, tot)) {
+    S[CG_BETA] = (!first && S[CG_RZ] != 0.0) ? tot[0] / S[CG_RZ] : 0.0;
+    S[CG_RZ] = tot[0];
+  }
+}
+
+// the update without a preconditioner: x += alpha p, r -= alpha q; r.r
+__global__ void __launch_bounds__(EMG_T) cg_update_plain_kernel(int64_t N, double* __restrict__ x,
+                                                                double* __restrict__ r, const double* __restrict__ p,
+                                                                const double* __restrict__ q, double* S,
+                                                                double* partial, unsigned* counter)
+{
+  const double alpha = S[CG_ALPHA];
+  double acc[1] = {0.0}, tot[1];
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+    x[n] += alpha * p[n];
+    const double rn = r[n] - alpha * q[n];
+    r[n] = rn;
+    acc[0] += rn * rn;
+  }
+  if (grid_sum<1>(acc, partial, counter, tot))
+    S[CG_RR] = tot[0];
+}
+
 // 3D node n: sum over its contributions (fiber node, factor) in fiber-node order, divided by the factor sum
 __global__ void map_kernel(int64_t N, const int64_t* ptr, const int64_t* src, const double* w, const double* fsum,
                            const double* vm, double default_value, double* out)
@@ -655,6 +875,16 @@ struct HostMesh {
 
 // ---- the solver object -----------------------------------------------------------------------------------
 
+// one level of the multigrid hierarchy (level 0: the fine grid, whose operator and vectors belong to the CG)
+struct MgLevel {
+  Grid g{};
+  Buf<double> U, dinv, b, x, t, r;      // operator, l1 scaling and vectors (level 0: the operator and b, x are
+                                        // the CG's)
+  Buf<int> lo, rlo, rhi;                // map to the next coarser level, three directions concatenated
+  Buf<double> w;
+  MgMap map{};
+};
+
 struct fdm_emg {
   std::string err;
   int device = 0;
@@ -667,6 +897,8 @@ struct fdm_emg {
   Buf<unsigned char> mask;
   Buf<unsigned> counter;                       // last-block counter of the grid reductions
   cudaGraphExec_t graphs[1] = {nullptr};       // CG chunk of the bidomain solve
+  int precond = FDM_EMG_PRECOND_MULTIGRID;     // of the bidomain solve
+  std::vector<MgLevel*> mg;                    // multigrid hierarchy of K(sigma_i + sigma_e), built on first use
   bool have_dir = false, have_ops = false, have_map = false;
   int64_t n_tensor_i = 0, n_tensor_e = 0;
   // fiber -> mesh transfer (CSR over 3D nodes)
@@ -706,9 +938,145 @@ int emg_fail(fdm_emg* m, int code, const std::string& msg)
 // block; chunks of 8 iterations run as one CUDA graph (captured on the first use for this right-hand side and
 // solution vector).  Convergence: ||r||_2 <= max(rtol ||b||_2, atol) (unpreconditioned residual, from the
 // recurrence), checked after every chunk.
+// One V-cycle x = M^-1 b on level l (b, x, t, r: the level's right-hand side, result and two work vectors).
+void vcycle(fdm_emg* m, size_t l, const double* U, const double* dinv, const double* b, double* x, double* t,
+            double* r)
+{
+  cudaStream_t s = m->stream;
+  const Grid g = m->mg[l]->g;
+  const int64_t N = g.n_nodes();
+  const int nb = blocks_for(N);
+  if (l + 1 == m->mg.size()) {
+    mg_coarsest_kernel<<<1, 1024, 0, s>>>(g, U, dinv, b, x, t, MG_COARSEST_SWEEPS);
+    return;
+  }
+  MgLevel* c = m->mg[l + 1];
+  mg_jacobi_kernel<<<nb, EMG_T, 0, s>>>(g, U, dinv, b, nullptr, t);
+  mg_jacobi_kernel<<<nb, EMG_T, 0, s>>>(g, U, dinv, b, t, x);
+  mg_residual_kernel<<<nb, EMG_T, 0, s>>>(g, U, b, x, r);
+  mg_restrict_kernel<<<blocks_for(c->g.n_nodes()), EMG_T, 0, s>>>(m->mg[l]->map, r, c->b.p);
+  vcycle(m, l + 1, c->U.p, c->dinv.p, c->b.p, c->x.p, c->t.p, c->r.p);
+  mg_prolong_add_kernel<<<nb, EMG_T, 0, s>>>(m->mg[l]->map, c->x.p, x);
+  mg_jacobi_kernel<<<nb, EMG_T, 0, s>>>(g, U, dinv, b, x, t);
+  mg_jacobi_kernel<<<nb, EMG_T, 0, s>>>(g, U, dinv, b, t, x);
+}
+
+void mg_release(fdm_emg* m)
+{
+  for (MgLevel* L : m->mg)
+    delete L;
+  m->mg.clear();
+}
+
+// coarse nodes along one direction of n fine nodes: fine indices 0, 2, 4, ... and n - 1 (none coarsened
+// below 3 nodes)
+std::vector<int> coarse_indices(int n)
+{
+  std::vector<int> F;
+  if (n <= 2) {
+    for (int i = 0; i < n; i++)
+      F.push_back(i);
+    return F;
+  }
+  for (int i = 0; i < n; i += 2)
+    F.push_back(i);
+  if (F.back() != n - 1)
+    F.push_back(n - 1);
+  return F;
+}
+
+// the hierarchy of K(sigma_i + sigma_e): coarsen until at most MG_COARSEST nodes (or nothing coarsens)
+int mg_build(fdm_emg* m)
+{
+  mg_release(m);
+  MgLevel* L0 = new MgLevel();
+  L0->g = m->hm.g;
+  m->mg.push_back(L0);
+  EMG_CUDA(m, L0->t.alloc(m->N));
+  EMG_CUDA(m, L0->r.alloc(m->N));
+  EMG_CUDA(m, L0->dinv.alloc(m->N));     // level 0: the l1 scaling of the fine operator
+  mg_l1_kernel<<<blocks_for(m->N), EMG_T, 0, m->stream>>>(m->hm.g, m->coef_ie.p, L0->dinv.p);
+  const double* Uf = m->coef_ie.p;
+  while ((int)m->mg.size() < MG_MAX_LEVELS) {
+    MgLevel* F = m->mg.back();
+    if (F->g.n_nodes() <= MG_COARSEST)
+      break;
+    const int nf[3] = {F->g.nx, F->g.ny, F->g.nz};
+    std::vector<int> Fi[3];
+    bool coarsened = false;
+    for (int d = 0; d < 3; d++) {
+      Fi[d] = coarse_indices(nf[d]);
+      coarsened = coarsened || (int)Fi[d].size() < nf[d];
+    }
+    if (!coarsened)
+      break;
+    std::vector<int> lo, rlo, rhi;
+    std::vector<double> w;
+    int off_lo[3], off_r[3];
+    for (int d = 0; d < 3; d++) {
+      const std::vector<int>& C = Fi[d];
+      const int nc = (int)C.size();
+      off_lo[d] = (int)lo.size();
+      off_r[d] = (int)rlo.size();
+      for (int i = 0, c = 0; i < nf[d]; i++) {
+        while (c + 1 < nc && C[c + 1] <= i)
+          c++;
+        lo.push_back(c);
+        w.push_back(c + 1 < nc ? double(i - C[c]) / double(C[c + 1] - C[c]) : 0.0);
+      }
+      for (int c = 0; c < nc; c++) {
+        rlo.push_back(c == 0 ? 0 : C[c - 1] + 1);
+        rhi.push_back(c == nc - 1 ? nf[d] - 1 : C[c + 1] - 1);
+      }
+    }
+    MgLevel* Cl = new MgLevel();
+    m->mg.push_back(Cl);
+    Cl->g = Grid{(int)Fi[0].size(), (int)Fi[1].size(), (int)Fi[2].size()};
+    const int64_t Nc = Cl->g.n_nodes();
+    EMG_CUDA(m, F->lo.alloc(lo.size()));
+    EMG_CUDA(m, F->w.alloc(w.size()));
+    EMG_CUDA(m, F->rlo.alloc(rlo.size()));
+    EMG_CUDA(m, F->rhi.alloc(rhi.size()));
+    EMG_CUDA(m, cudaMemcpyAsync(F->lo.p, lo.data(), sizeof(int) * lo.size(), cudaMemcpyHostToDevice, m->stream));
+    EMG_CUDA(m, cudaMemcpyAsync(F->w.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, m->stream));
+    EMG_CUDA(m, cudaMemcpyAsync(F->rlo.p, rlo.data(), sizeof(int) * rlo.size(), cudaMemcpyHostToDevice, m->stream));
+    EMG_CUDA(m, cudaMemcpyAsync(F->rhi.p, rhi.data(), sizeof(int) * rhi.size(), cudaMemcpyHostToDevice, m->stream));
+    F->map.fine = F->g;
+    F->map.coarse = Cl->g;
+    for (int d = 0; d < 3; d++) {
+      F->map.lo[d] = F->lo.p + off_lo[d];
+      F->map.w[d] = F->w.p + off_lo[d];
+      F->map.rlo[d] = F->rlo.p + off_r[d];
+      F->map.rhi[d] = F->rhi.p + off_r[d];
+    }
+    for (auto* b : {&Cl->dinv, &Cl->b, &Cl->x, &Cl->t, &Cl->r})
+      EMG_CUDA(m, b->alloc(Nc));
+    EMG_CUDA(m, Cl->U.alloc(EMG_NC * Nc));
+    mg_galerkin_kernel<<<blocks_for(Nc), EMG_T, 0, m->stream>>>(F->map, Uf, Cl->U.p);
+    mg_l1_kernel<<<blocks_for(Nc), EMG_T, 0, m->stream>>>(Cl->g, Cl->U.p, Cl->dinv.p);
+    EMG_CUDA(m, cudaGetLastError());
+    Uf = Cl->U.p;
+  }
+  EMG_CUDA(m, cudaStreamSynchronize(m->stream));
+  return FDM_OK;
+}
+
+// after the operator or the preconditioner changes: the captured CG chunk and the hierarchy are rebuilt
+void emg_invalidate(fdm_emg* m)
+{
+  for (auto& ge : m->graphs)
+    if (ge) {
+      cudaGraphExecDestroy(ge);
+      ge = nullptr;
+    }
+  mg_release(m);
+}
+
 int cg_solve(fdm_emg* m, const double* U, const unsigned char* mask, bool nullspace, const double* b, double* x,
              double rtol, double atol, int max_it, int* iterations, double* residual, int graph_slot)
 {
+  // the multigrid preconditioner (bidomain operator only; the V-cycle replaces z = D^-1 r)
+  const bool use_mg = graph_slot == 0 && m->precond == FDM_EMG_PRECOND_MULTIGRID && m->mg.size() > 1;
   const int64_t N = m->N;
   const Grid g = m->hm.g;
   const int nb = blocks_for(N);
@@ -727,6 +1095,10 @@ int cg_solve(fdm_emg* m, const double* U, const unsigned char* mask, bool nullsp
   EMG_CUDA(m, cudaMemsetAsync(m->p0.p, 0, sizeof(double) * N, s));
   EMG_CUDA(m, cudaMemsetAsync(m->q.p, 0, sizeof(double) * N, s));
   cg_init_kernel<<<nb, EMG_T, 0, s>>>(g, U, mask, bb, x, m->r.p, m->z.p, m->dinv.p, S, P, C);
+  if (use_mg) {
+    vcycle(m, 0, U, m->mg[0]->dinv.p, m->r.p, m->z.p, m->mg[0]->t.p, m->mg[0]->r.p);
+    cg_rz_kernel<<<nb, EMG_T, 0, s>>>(N, m->r.p, m->z.p, S, P, C, 1);
+  }
   double hs[8];
   EMG_CUDA(m, cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, s));
   EMG_CUDA(m, cudaStreamSynchronize(s));
@@ -738,9 +1110,16 @@ int cg_solve(fdm_emg* m, const double* U, const unsigned char* mask, bool nullsp
   // one iteration: direction and product, then the update
   auto iteration = [&]() {
     cg_direction_kernel<<<nb, EMG_T, 0, s>>>(g, U, mask, m->z.p, m->p0.p, m->q.p, S, P, C);
-    cg_update_kernel<<<nb, EMG_T, 0, s>>>(N, x, m->r.p, m->z.p, m->p0.p, m->q.p, m->dinv.p, S, P, C);
+    if (use_mg) {
+      cg_update_plain_kernel<<<nb, EMG_T, 0, s>>>(N, x, m->r.p, m->p0.p, m->q.p, S, P, C);
+      vcycle(m, 0, U, m->mg[0]->dinv.p, m->r.p, m->z.p, m->mg[0]->t.p, m->mg[0]->r.p);
+      cg_rz_kernel<<<nb, EMG_T, 0, s>>>(N, m->r.p, m->z.p, S, P, C, 0);
+    } else {
+      cg_update_kernel<<<nb, EMG_T, 0, s>>>(N, x, m->r.p, m->z.p, m->p0.p, m->q.p, m->dinv.p, S, P, C);
+    }
   };
-  constexpr int CHUNK = 8;
+  // iterations per graph launch and convergence check: a multigrid iteration is long and few are needed
+  const int CHUNK = use_mg ? 2 : 8;
   cudaGraphExec_t no_graph = nullptr;
   cudaGraphExec_t& ge = graph_slot >= 0 ? m->graphs[graph_slot] : no_graph;
   if (!ge && graph_slot >= 0) {
@@ -905,6 +1284,7 @@ extern "C" int fdm_emg_destroy(fdm_emg* m)
   for (auto& ge : m->graphs)
     if (ge)
       cudaGraphExecDestroy(ge);
+  mg_release(m);
   m->mask.release();
   m->counter.release();
   m->map_ptr.release();
@@ -1010,6 +1390,7 @@ extern "C" int fdm_emg_set_conductivity(fdm_emg* m, int64_t n_sigma_i, const dou
   m->n_tensor_i = n_sigma_i;
   m->n_tensor_e = n_sigma_e;
   m->have_ops = true;
+  emg_invalidate(m);
   return FDM_OK;
 }
 
@@ -1188,6 +1569,11 @@ extern "C" int fdm_emg_solve(fdm_emg* m, double rtol, double atol, int max_itera
   EMG_BIND(m);
   const int64_t N = m->N;
   const int nb = blocks_for(N);
+  if (m->precond == FDM_EMG_PRECOND_MULTIGRID && m->mg.empty()) {
+    const int rb = mg_build(m);
+    if (rb)
+      return rb;
+  }
   EMG_CUDA(m, cudaEventRecord(m->ev0, m->stream));
   // rhs = -K(sigma_i) Vm
   apply_kernel<<<nb, EMG_T, 0, m->stream>>>(m->hm.g, m->coef_i.p, m->vm.p, m->rhs.p, -1.0);
@@ -1208,6 +1594,24 @@ extern "C" int fdm_emg_solve(fdm_emg* m, double rtol, double atol, int max_itera
     *iterations = its;
   if (residual)
     *residual = res;
+  return FDM_OK;
+}
+
+extern "C" int fdm_emg_set_preconditioner(fdm_emg* m, int type, int* levels)
+{
+  if (!m || (type != FDM_EMG_PRECOND_JACOBI && type != FDM_EMG_PRECOND_MULTIGRID))
+    return emg_fail(m, FDM_ERR_ARG, "fdm_emg_set_preconditioner: FDM_EMG_PRECOND_JACOBI or FDM_EMG_PRECOND_MULTIGRID");
+  EMG_BIND(m);
+  if (type != m->precond)
+    emg_invalidate(m);
+  m->precond = type;
+  if (type == FDM_EMG_PRECOND_MULTIGRID && m->have_ops && m->mg.empty()) {
+    const int rc = mg_build(m);
+    if (rc)
+      return rc;
+  }
+  if (levels)
+    *levels = type == FDM_EMG_PRECOND_MULTIGRID ? (int)m->mg.size() : 1;
   return FDM_OK;
 }
 

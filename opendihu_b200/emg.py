@@ -21,8 +21,10 @@ solver's device Vm, and the conjugate-gradient solve.  Settings keys read (refer
 ``maxIterations``; ``Meshes`` 3D entries with ``nElements`` and ``physicalExtent``/``physicalOffset`` or
 ``nodePositions``; ``MappingsBetweenMeshes`` ``xiTolerance``, ``defaultValue``; Coupling ``timeStepWidth``,
 ``endTime``, ``connectedSlotsTerm1To2``.  The linear solver is conjugate gradients with a Jacobi
-preconditioner whatever ``solverType``/``preconditionerType`` name (both systems are symmetric positive
-(semi)definite); quadrature: Gauss 3 points per direction for the potential flow and 5 for the activation
+or geometric-multigrid preconditioner whatever ``solverType`` names (both systems are symmetric positive
+(semi)definite): ``preconditionerType`` "gamg", "mg", "hypre"/"boomeramg" select the multigrid V-cycle, any
+other name the Jacobi preconditioner, none given the V-cycle from 300,000 nodes and Jacobi below (the
+potential flow always uses Jacobi); quadrature: Gauss 3 points per direction for the potential flow and 5 for the activation
 (the template arguments of fast_fibers_emg.cpp), changeable with a "B200" dict (``gaussPointsPotentialFlow``,
 ``gaussPointsActivation``).
 """
@@ -37,6 +39,8 @@ import numpy as np
 from . import _native as N
 from . import solver as S
 
+# mesh size from which the multigrid preconditioner is the default
+MULTIGRID_MIN_NODES = 300_000
 # PETSc's defaults where a solver entry leaves a key out
 _SOLVER_DEFAULTS = {"relativeTolerance": 1e-5, "absoluteTolerance": 1e-50, "maxIterations": 10000}
 FACES = {"0-": (0, 0), "0+": (0, 1), "1-": (1, 0), "1+": (1, 1), "2-": (2, 0), "2+": (2, 1)}
@@ -110,7 +114,8 @@ class StaticBidomainSolver:
     def __init__(self, shape, node_positions, sigma_i, sigma_e, *, dirichlet_nodes=None, dirichlet_values=None,
                  direction=None, potential_flow_solver: Optional[dict] = None,
                  emg_solver: Optional[dict] = None, initial_guess_nonzero: bool = True,
-                 gauss_points_potential_flow: int = 3, gauss_points_activation: int = 5, device: int = 0):
+                 gauss_points_potential_flow: int = 3, gauss_points_activation: int = 5, device: int = 0,
+                 preconditioner: Optional[str] = None):
         self.shape = tuple(int(x) for x in shape)
         self.node_positions = np.ascontiguousarray(node_positions, np.float64).reshape(-1, 3)
         self.n_nodes = self.shape[0] * self.shape[1] * self.shape[2]
@@ -130,6 +135,13 @@ class StaticBidomainSolver:
         self.gauss_pf = int(gauss_points_potential_flow)
         self.gauss_act = int(gauss_points_activation)
         self.device = int(device)
+        name = (preconditioner or self.emg_solver.get("preconditionerType") or "auto").lower()
+        if name == "auto":
+            # the V-cycle's launches cost more than its saved iterations below a few hundred thousand nodes
+            name = "multigrid" if self.n_nodes >= MULTIGRID_MIN_NODES else "jacobi"
+        self.preconditioner = "multigrid" if name in ("multigrid", "gamg", "mg", "hypre", "boomeramg", "ml") \
+            else "jacobi"
+        self.multigrid_levels = 0
         self.start_time = 0.0
         self.end_time = 0.0
         self.potential_flow_iterations = 0
@@ -188,6 +200,10 @@ class StaticBidomainSolver:
                 self.potential_flow_iterations = its.value
             self._call(L.fdm_emg_set_conductivity, len(self.sigma_i), N.ptr(self.sigma_i, C.c_double),
                        len(self.sigma_e), N.ptr(self.sigma_e, C.c_double), self.gauss_act)
+            lv = C.c_int()
+            self._call(L.fdm_emg_set_preconditioner, N.EMG_PRECOND_MULTIGRID if self.preconditioner == "multigrid"
+                       else N.EMG_PRECOND_JACOBI, C.byref(lv))
+            self.multigrid_levels = lv.value
         except Exception:
             self.close()
             raise

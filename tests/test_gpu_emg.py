@@ -216,3 +216,20 @@ def test_overlapped_coupling_equals_sequential():
     for pa, pb in zip(a[0], b[0]):
         np.testing.assert_array_equal(pa[2], pb[2])
         np.testing.assert_array_equal(pa[3], pb[3])
+
+
+@pytest.mark.parametrize("mesh", [(17, 13, 41), (33, 33, 65)])
+def test_multigrid_preconditioner_same_solution_fewer_iterations(mesh):
+    s, fpos, kw = WL.emg_box(n_fibers_x=2, n_fibers_y=2, n_nodes=101, mesh_nodes=mesh, width=1.0)
+    z = kw["node_positions"][:, 2]
+    vm = -75.0 + 100.0 * np.exp(-((z - z.mean()) / 0.1) ** 2) + np.random.default_rng(3).normal(size=len(z))
+    out = {}
+    for pc in ("jacobi", "multigrid"):
+        with E.StaticBidomainSolver(emg_solver=TIGHT, potential_flow_solver=TIGHT, preconditioner=pc, **kw) as slv:
+            slv.set_vm(vm)
+            its = slv.advanceTimeSpan()
+            out[pc] = (slv.phi_e(), its, slv.multigrid_levels)
+    assert out["multigrid"][2] > 1 and out["jacobi"][2] == 1
+    assert out["multigrid"][1] * 3 < out["jacobi"][1], (out["multigrid"][1], out["jacobi"][1])
+    ref = out["jacobi"][0]
+    np.testing.assert_allclose(out["multigrid"][0], ref, rtol=0, atol=1e-8 * np.abs(ref).max())
