@@ -18,7 +18,7 @@ from __future__ import annotations
 
 import heapq
 import threading
-from typing import Dict, List, Optional, Sequence
+from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -283,9 +283,34 @@ class ShardedSolver:
             out[:a.shape[0], self._sensor_split[k]] = a
         return out
 
-    def adjoint_backward(self, trace_grad: np.ndarray) -> Dict[str, np.ndarray]:
-        tg = np.asarray(trace_grad, np.float64)
-        r = self._each(lambda k, sv: sv.adjoint_backward(tg[:, self._sensor_split[k]]))
+    def adjoint(self, t_start: float, t_end: float, checkpoint_every: int, sensor_nodes,
+                loss_grad: Callable[[np.ndarray, np.ndarray], np.ndarray]):
+        """The adjoint one shard after the other, each shard's checkpoints and replay buffers freed before the
+        next starts (device memory for one shard's adjoint at a time, see plan_adjoint).  The loss must be a sum
+        over sensors: loss_grad(trace, sensors) gets a shard's trace [steps, k] and the positions of its k
+        sensors in sensor_nodes and returns dL/dtrace for them.  Returns (trace [steps, sensors], gradients)."""
+        sensor_nodes = np.asarray(sensor_nodes, np.int64)
+        owner = np.full(self.system.n_nodes, -1, np.int64)
+        local = np.zeros(self.system.n_nodes, np.int64)
+        for k, nodes in enumerate(self.nodes):
+            owner[nodes] = k
+            local[nodes] = np.arange(len(nodes))
+        traces, grads = {}, {}
+        for k, sv in enumerate(self.shards):
+            if sv is None:
+                continue
+            cols = np.nonzero(owner[sensor_nodes] == k)[0]
+            tr = sv.adjoint_forward(t_start, t_end, checkpoint_every, local[sensor_nodes[cols]])
+            grads[k] = sv.adjoint_backward(loss_grad(tr, cols))
+            sv.adjoint_release()
+            traces[k] = (cols, tr)
+        steps = max(tr.shape[0] for _, tr in traces.values())
+        out = np.zeros((steps, len(sensor_nodes)))
+        for cols, tr in traces.values():
+            out[:tr.shape[0], cols] = tr
+        return out, self._merge_gradients(grads)
+
+    def _merge_gradients(self, r: Dict[int, Dict[str, np.ndarray]]) -> Dict[str, np.ndarray]:
         nf, nn = self.system.n_fibers, self.system.n_nodes
         any_r = next(iter(r.values()))
         g = {"prefactor": np.zeros(nf), "parameters": np.zeros((any_r["parameters"].shape[0], nn)),
@@ -295,6 +320,55 @@ class ShardedSolver:
             g["parameters"][:, self.nodes[k]] = a["parameters"]
             g["states0"][:, self.nodes[k]] = a["states0"]
         return g
+
+    def adjoint_backward(self, trace_grad: np.ndarray) -> Dict[str, np.ndarray]:
+        tg = np.asarray(trace_grad, np.float64)
+        r = self._each(lambda k, sv: sv.adjoint_backward(tg[:, self._sensor_split[k]]))
+        return self._merge_gradients(r)
+
+
+def adjoint_bytes_per_node(model: str, n_substeps: int, n_steps: int, checkpoint_every: int) -> int:
+    """Device bytes per node the FP64 adjoint holds (fdm_adjoint_forward / fdm_adjoint_backward): one
+    checkpoint of the states per segment, two replay buffers of a segment's Heun substep states (the replay of
+    one segment overlaps the reverse sweep of the next) with Vm around each diffusion solve, and the adjoint
+    variables; n_substeps = Heun substeps per half step."""
+    from .solver import model_sizes
+    ns, _, npar = model_sizes(model)[:3]
+    kc = max(1, min(int(checkpoint_every), int(n_steps)))
+    segments = -(-int(n_steps) // kc)
+    checkpoints = segments * ns * 8
+    replay = 2 * kc * (2 * n_substeps * ns + 2) * 8
+    adjoint = (ns + max(npar, 1) + 3) * 8
+    return checkpoints + replay + adjoint
+
+
+def plan_adjoint(system: FiberSystem, t_start: float, t_end: float, budget_bytes: float) -> Dict[str, int]:
+    """Checkpoint interval and number of sequential fiber shards for an FP64 adjoint over [t_start, t_end] that
+    fits budget_bytes of device memory: the interval minimising the per-node memory (checkpoints ~ S/k against
+    replay ~ k, so k ~ sqrt(S / (4 n0))), then as many LPT shards as the largest shard needs to fit."""
+    import math
+    dt = system.dt_splitting
+    n_steps = max(1, int(math.ceil((t_end - t_start) / dt - 0.1)))
+    n0 = max(1, int(math.ceil(0.5 * dt / system.dt_0d - 0.1)))
+    best = None
+    k0 = max(1, int(round(math.sqrt(n_steps / (4.0 * n0)))))
+    for k in sorted({max(1, k0 // 2), k0, k0 + 1, 2 * k0, 1}):
+        b = adjoint_bytes_per_node(system.model, n0, n_steps, k)
+        if best is None or b < best[1]:
+            best = (k, b)
+    k, per_node = best
+    lengths = np.diff(np.asarray(system.fiber_offsets, np.int64))
+    n_shards = 1
+    while True:
+        parts = lpt_partition(lengths, n_shards)
+        largest = max(int(lengths[p].sum()) for p in parts if len(p)) if len(lengths) else 0
+        if largest * per_node <= budget_bytes or n_shards >= max(len(lengths), 1):
+            break
+        n_shards += 1
+    if largest * per_node > budget_bytes:
+        raise ValueError(f"one fiber alone needs {largest * per_node / 1e9:.1f} GB for the adjoint")
+    return {"checkpoint_every": k, "n_shards": n_shards, "bytes_per_node": per_node, "n_steps": n_steps,
+            "largest_shard_nodes": largest}
 
 
 def rank_shard(system: FiberSystem, rank: int, world: int):

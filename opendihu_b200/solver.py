@@ -614,6 +614,10 @@ class FastMonodomainSolver:
                    N.ptr(gp, C.c_double), N.ptr(g0, C.c_double))
         return {"prefactor": gpf, "parameters": gp[:npar], "states0": g0}
 
+    def adjoint_release(self):
+        """Free the adjoint's checkpoints and replay buffers (the solver keeps its state)."""
+        self._call(N.lib().fdm_adjoint_release)
+
     def adjoint_timing_ms(self) -> float:
         v = C.c_double()
         self._call(N.lib().fdm_adjoint_timing, C.byref(v))

@@ -66,3 +66,22 @@ def test_sharded_only_if_stimulated_equals_unsharded():
         sh.advanceTimeSpan()
         st = sh.states()
     np.testing.assert_array_equal(st, ref)
+
+
+def test_sequential_shard_adjoint_equals_unsharded():
+    s = _system(end_time=1.0)
+    sensors = np.asarray(s.fiber_offsets[:-1]) + 30
+    rng = np.random.default_rng(12)
+    with S.FastMonodomainSolver(s.copy()) as slv:
+        tr = slv.adjoint_forward(s.start_time, s.end_time, 50, sensors)
+        w = rng.standard_normal(tr.shape)
+        g = slv.adjoint_backward(w)
+    per_node = SH.plan_adjoint(s, s.start_time, s.end_time, 1e15)["bytes_per_node"]
+    plan = SH.plan_adjoint(s, s.start_time, s.end_time, s.n_nodes * per_node / 2.5)
+    assert plan["n_shards"] >= 3
+    with SH.ShardedSolver(s.copy(), devices=[0], n_shards=plan["n_shards"]) as sh:
+        tr2, g2 = sh.adjoint(s.start_time, s.end_time, plan["checkpoint_every"], sensors,
+                             lambda trace, cols: w[:trace.shape[0], cols])
+    np.testing.assert_array_equal(tr2, tr)
+    for k in ("prefactor", "parameters", "states0"):
+        np.testing.assert_allclose(g2[k], g[k], rtol=1e-12, atol=1e-300)

@@ -157,3 +157,18 @@ def test_shard_gate_codes_map_fibers():
         with pytest.raises(ValueError):
             for fib in SH.lpt_partition(np.diff(s.fiber_offsets), 3):
                 SH.shard_gate_codes(s, fib, codes)
+
+
+def test_adjoint_memory_plan():
+    s = WL.batched_hh(n_fibers=40, min_nodes=500, max_nodes=2500, seed=3, end_time=0.0)
+    one = SH.adjoint_bytes_per_node(s.model, 5, 1000, 16)
+    # checkpoints fall and replay grows with the interval
+    assert SH.adjoint_bytes_per_node(s.model, 5, 1000, 1) > one < SH.adjoint_bytes_per_node(s.model, 5, 1000, 500)
+    big = SH.plan_adjoint(s, 0.0, 1.0, 1e12)
+    assert big["n_shards"] == 1 and big["n_steps"] == 1000
+    assert 5 <= big["checkpoint_every"] <= 12           # ~ sqrt(1000 / (4 * 5))
+    budget = s.n_nodes * big["bytes_per_node"] / 3.5
+    plan = SH.plan_adjoint(s, 0.0, 1.0, budget)
+    assert plan["n_shards"] >= 4 and plan["largest_shard_nodes"] * plan["bytes_per_node"] <= budget
+    with pytest.raises(ValueError):
+        SH.plan_adjoint(s, 0.0, 1.0, 1000.0)
