@@ -1,5 +1,6 @@
 // Fused-kernel instantiations for one (precision, math policy); included by fdm_fused_*.cu.
 #pragma once
+#include <atomic>
 #include "fdm_internal.h"
 
 #include "generated/hodgkin_huxley_1952_anone_c2_3_4.cuh"
@@ -34,18 +35,32 @@ cudaError_t launch_fused_hh_f64_approx_gate(int shape, const FusedArgs& a, cudaS
 cudaError_t launch_fused_hh_f32_exact_gate(int shape, const FusedArgs& a, cudaStream_t s);
 cudaError_t launch_fused_hh_f32_approx_gate(int shape, const FusedArgs& a, cudaStream_t s);
 
+// The dynamic shared memory limit of a kernel is set per device: once on each device (bit d of done; the
+// solvers of several devices may launch from concurrent host threads).
+template<class K>
+static cudaError_t set_smem_once(K kernel, size_t smem, std::atomic<uint64_t>& done)
+{
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return e;
+  const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit))
+    return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && bit)
+    done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
+
 template<class Model, class RR, class Math, int T, int M, bool GATE>
 static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s)
 {
   constexpr size_t smem = fused_smem_bytes<Model, RR, Math, T, M>();
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(fused_kernel<Model, RR, Math, T, M, GATE, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return e;
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> attr_done{0};
+  cudaError_t e = set_smem_once(fused_kernel<Model, RR, Math, T, M, GATE, false>, smem, attr_done);
+  if (e != cudaSuccess)
+    return e;
   if (a.n_bins == 0)
     return cudaSuccess;
   fused_kernel<Model, RR, Math, T, M, GATE, false><<<a.n_bins, T, smem, s>>>(a);
@@ -71,13 +86,10 @@ static cudaError_t fused_cluster_one(const FusedArgs& a, int csize, cudaStream_t
 {
   constexpr size_t smem = fused_smem_bytes<Model, RR, Math, T, M>();
   auto kernel = fused_kernel<Model, RR, Math, T, M, false, true>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return e;
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> attr_done{0};
+  cudaError_t e = set_smem_once(kernel, smem, attr_done);
+  if (e != cudaSuccess)
+    return e;
   if (a.n_bins == 0)
     return cudaSuccess;
   cudaLaunchConfig_t cfg = {};
