@@ -721,31 +721,44 @@ __global__ void mg_l1_kernel(Grid g, const double* __restrict__ U, double* __res
   }
 }
 
-// l1-Jacobi sweep: xo = x + dl1 (b - A x); from zero (x null): xo = dl1 b
+// l1-Jacobi sweep: xo = x + dl1 (b - A x) (x's rows staged in shared memory); from zero (x null): xo = dl1 b
 __global__ void __launch_bounds__(EMG_T, 4) mg_jacobi_kernel(Grid g, const double* __restrict__ U,
                                                              const double* __restrict__ dl1,
                                                              const double* __restrict__ b,
                                                              const double* __restrict__ x, double* __restrict__ xo)
 {
+  __shared__ double sv[9][EMG_T + 2];
   const int64_t N = g.n_nodes();
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
-    if (!x) {
+  if (!x) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
       xo[n] = dl1[n] * b[n];
-    } else {
-      const double ax = stencil_row(g, U, n, [&](int64_t m) { return x[m]; });
-      xo[n] = x[n] + dl1[n] * (b[n] - ax);
-    }
+    return;
+  }
+  for (int64_t n0 = (int64_t)blockIdx.x * EMG_T; n0 < N; n0 += (int64_t)gridDim.x * EMG_T) {
+    stage_rows(g, x, n0, sv);
+    __syncthreads();
+    const int64_t n = n0 + threadIdx.x;
+    if (n < N)
+      xo[n] = sv[4][threadIdx.x + 1] + dl1[n] * (b[n] - stencil_row_staged(g, U, n, threadIdx.x, sv));
+    __syncthreads();
   }
 }
 
-// r = b - A x
+// r = b - A x (x's rows staged in shared memory)
 __global__ void __launch_bounds__(EMG_T, 4) mg_residual_kernel(Grid g, const double* __restrict__ U,
                                                                const double* __restrict__ b,
                                                                const double* __restrict__ x, double* __restrict__ r)
 {
+  __shared__ double sv[9][EMG_T + 2];
   const int64_t N = g.n_nodes();
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
-    r[n] = b[n] - stencil_row(g, U, n, [&](int64_t m) { return x[m]; });
+  for (int64_t n0 = (int64_t)blockIdx.x * EMG_T; n0 < N; n0 += (int64_t)gridDim.x * EMG_T) {
+    stage_rows(g, x, n0, sv);
+    __syncthreads();
+    const int64_t n = n0 + threadIdx.x;
+    if (n < N)
+      r[n] = b[n] - stencil_row_staged(g, U, n, threadIdx.x, sv);
+    __syncthreads();
+  }
 }
 
 // coarsest grid: `sweeps` l1-Jacobi sweeps from zero in one block (x and t ping-pong; x holds the result)
