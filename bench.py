@@ -481,6 +481,11 @@ def main():
         cpu = {"value": rate, "unit": "node-steps/s", "cores": threads, "kind": "port",
                "sample": f"first 10 fibers of the batch ({sub.n_nodes} nodes) x 20 ms ({n_ref} Strang steps), "
                          f"{cpu_s:.1f} s"}
+        # one thread: the reference's vc path runs one thread per MPI rank
+        sub1, _, n1, rate1, cpu1_s = cpu_baseline(system, 2, 10.0, 1)
+        cpu["single_thread"] = {"value": rate1, "unit": "node-steps/s", "cores": 1,
+                                "sample": f"first 2 fibers ({sub1.n_nodes} nodes) x 10 ms ({n1} Strang steps), "
+                                          f"{cpu1_s:.1f} s"}
         acc = {}
         for name, method, prec in (("fp32_fused", "fused", "fp32"), ("fp64_split", "split", "fp64")):
             with S.FastMonodomainSolver(sub.copy(), method=method, precision=prec, device=local) as slv:
