@@ -168,6 +168,12 @@ int fdm_get_trace(fdm_solver *s, double *out /* [step * n_nodes + k] */, int64_t
 
 /* RepeatedCall over [t_start, t_end]: blocking; returns after the device finished. */
 int fdm_advance(fdm_solver *s, double t_start, double t_end);
+/* the same, returning once the work is enqueued on the solver's stream (no counterpart in the reference,
+ * whose calls are synchronous): the host can prepare other work meanwhile.  fdm_wait completes it (timing,
+ * the NaN check of check_nan); every other call on the solver orders after the enqueued work, the next
+ * advance waits first. */
+int fdm_advance_async(fdm_solver *s, double t_start, double t_end);
+int fdm_wait(fdm_solver *s);
 /* number of split steps done by all advances so far */
 int64_t fdm_split_steps(const fdm_solver *s);
 /* summed device time and count of the main kernel launches (config.profile = 1), and of all GPU work

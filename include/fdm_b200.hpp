@@ -211,6 +211,14 @@ class FastMonodomainSolver {
     check(fdm_advance(h_, start_, end_));
   }
 
+  /* advanceTimeSpan that returns once the work is enqueued; wait() completes it */
+  void advanceTimeSpanAsync()
+  {
+    initialize();
+    check(fdm_advance_async(h_, start_, end_));
+  }
+  void wait() { check(fdm_wait(h_)); }
+
   void setTimeSpan(double startTime, double endTime)
   {
     start_ = startTime;

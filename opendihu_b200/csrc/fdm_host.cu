@@ -238,6 +238,7 @@ struct fdm_solver {
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   double main_ms = 0, adv_ms = 0, adj_ms = 0;
+  bool finish_pending = false;   // an fdm_advance_async whose timing and NaN check fdm_wait still owes
   int adjoint_tape = 1; // FDM_ADJOINT_TAPE=0 selects the re-evaluating reverse step (for measurements)
   int64_t main_launches = 0, launches = 0;
   cudaEvent_t adv_start = nullptr, adv_stop = nullptr;
@@ -1999,24 +2000,54 @@ static int finish_advance(fdm_solver* s)
   return FDM_OK;
 }
 
-extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
+extern "C" int fdm_wait(fdm_solver* s)
 {
   if (!s)
-    return fail(s, FDM_ERR_ARG, "fdm_advance: null solver");
+    return fail(s, FDM_ERR_ARG, "fdm_wait: null solver");
+  if (!s->finish_pending)
+    return FDM_OK;
+  FDM_BIND(s);
+  s->finish_pending = false;
+  return finish_advance(s);
+}
+
+// the work of an advance, enqueued on the solver's stream (the host waits only where the window buffers of
+// the step schedule are reused)
+static int enqueue_advance(fdm_solver* s, double t_start, double t_end, const char* who)
+{
+  if (!s)
+    return fail(s, FDM_ERR_ARG, std::string(who) + ": null solver");
   FDM_BIND(s);
   if (!(t_end >= t_start))
-    return fail(s, FDM_ERR_ARG, "fdm_advance: t_end must be >= t_start");
+    return fail(s, FDM_ERR_ARG, std::string(who) + ": t_end must be >= t_start");
   if (s->n_fibers > 0 && !s->stimulation_set)
-    return fail(s, FDM_ERR_ARG, "fdm_advance: call fdm_set_stimulation first");
+    return fail(s, FDM_ERR_ARG, std::string(who) + ": call fdm_set_stimulation first");
+  int r = fdm_wait(s);     // the timing and the NaN check of an earlier asynchronous advance
+  if (r)
+    return r;
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
   std::vector<SplitStep> steps;
   std::vector<double> dt1s;
   plan_advance(s, t_start, t_end, steps, dt1s);
-  int r = run_planned(s, steps, dt1s, 0, steps.size(), true);
+  return run_planned(s, steps, dt1s, 0, steps.size(), true);
+}
+
+extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
+{
+  const int r = enqueue_advance(s, t_start, t_end, "fdm_advance");
   if (r)
     return r;
   return finish_advance(s);
+}
+
+extern "C" int fdm_advance_async(fdm_solver* s, double t_start, double t_end)
+{
+  const int r = enqueue_advance(s, t_start, t_end, "fdm_advance_async");
+  if (r)
+    return r;
+  s->finish_pending = true;
+  return FDM_OK;
 }
 
 // Strang steps given explicitly, as the reference's generated computeMonodomain receives them
@@ -2024,6 +2055,11 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
 // currentTime + k*dt0D and midTime + k*dt0D, one diffusion solve with dt1D per step.
 static int advance_explicit(fdm_solver* s, double start, double dts, int ns, double dt0, int n0, double dt1)
 {
+  { // an asynchronous advance still owes its timing and NaN check
+    const int rw = fdm_wait(s);
+    if (rw)
+      return rw;
+  }
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
   std::vector<SplitStep> steps(ns);
@@ -2585,6 +2621,11 @@ extern "C" int fdm_adjoint_forward(fdm_solver* s, double t_start, double t_end, 
   FDM_CUDA(A.fin_jit.alloc(nf));
   FDM_CUDA(A.fin_jidx.alloc(nf));
   FDM_CUDA(A.fin_hbs.alloc(nf));
+  { // an asynchronous advance still owes its timing and NaN check
+    const int rw = fdm_wait(s);
+    if (rw)
+      return rw;
+  }
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
   for (int c = 0; c < A.n_seg; c++) {
@@ -2691,6 +2732,11 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
     }
   }
   auto coef_of = [&](size_t j) -> const double* { return pipelined ? A.coefs.p + (size_t)epoch[j] * 6 * N : s->coef.p; };
+  { // an asynchronous advance still owes its timing and NaN check
+    const int rw = fdm_wait(s);
+    if (rw)
+      return rw;
+  }
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
   std::vector<WindowInfo> win(A.n_seg);

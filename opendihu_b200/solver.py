@@ -521,6 +521,14 @@ class FastMonodomainSolver:
         self.initialize()
         self._call(N.lib().fdm_advance, self._start, self._end)
 
+    def advance_async(self):
+        """advanceTimeSpan without waiting for the device (``wait`` completes it: timing, the NaN check)."""
+        self.initialize()
+        self._call(N.lib().fdm_advance_async, self._start, self._end)
+
+    def wait(self):
+        self._call(N.lib().fdm_wait)
+
     def run(self):
         self.initialize()
         self.advanceTimeSpan()

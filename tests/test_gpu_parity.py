@@ -210,3 +210,28 @@ def test_plain_method_config_10ms(method, precision):
     assert np.array_equal(np.isnan(at), np.isnan(at_ref))
     ok = ~np.isnan(at)
     assert np.all(np.abs(at[ok] - at_ref[ok]) <= 1e-3 + 1e-12)
+
+
+def test_asynchronous_advance_equals_blocking():
+    sysm = small_system(end_time=0.6)
+    H.complete(sysm)
+    with S.FastMonodomainSolver(sysm.copy(), method="fused") as a, S.FastMonodomainSolver(sysm.copy(), method="fused") as b:
+        a.setTimeSpan(0.0, 0.3)
+        a.advanceTimeSpan()
+        a.setTimeSpan(0.3, 0.6)
+        a.advanceTimeSpan()
+        b.setTimeSpan(0.0, 0.3)
+        b.advance_async()
+        b.setTimeSpan(0.3, 0.6)
+        b.advance_async()            # waits for the first one itself
+        b.wait()
+        np.testing.assert_array_equal(a.states(), b.states())
+        assert b.timing()["advance_ms"] > 0
+    bad = small_system(end_time=0.01)
+    H.complete(bad)
+    bad.states[0, 5] = np.nan
+    with S.FastMonodomainSolver(bad, method="split") as c:
+        c.advance_async()
+        with pytest.raises(S.N.FdmError) as e:
+            c.wait()
+        assert e.value.code == S.N.FDM_ERR_NAN
