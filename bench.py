@@ -47,7 +47,7 @@ def parse_args():
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
     p.add_argument("--skip-emg", action="store_true")
-    p.add_argument("--only", choices=["emg", "emg-cg", "shorten"],
+    p.add_argument("--only", choices=["emg", "emg-cg", "shorten", "plain"],
                    help="print one side measurement alone (profiling runs)")
     p.add_argument("--skip-shorten", action="store_true")
     p.add_argument("--shorten-ms", type=float, default=0.02, help="simulated span of the Shorten measurement")
@@ -170,6 +170,29 @@ def cpu_baseline(system, sample_fibers: int, sample_ms: float, threads: int):
     return sub, st, n, sub.n_nodes * n / dt, dt
 
 
+def plain_measurement(device: int) -> dict:
+    """The plain-method configuration (16 HH fibers x 1481 nodes, implicit Euler, 10 ms): the FP64 split path
+    with CUDA graphs and the fused kernel (cluster mode: few fibers) in FP64 and FP32, 9 ms after 1 ms warm-up."""
+    from opendihu_b200 import solver as S
+    from opendihu_b200 import workloads as WL
+    c1 = WL.plain_hh(end_time=10.0)
+    out = {"workload": "16 HH fibers x 1481 nodes, implicit Euler, 10 ms"}
+    for name, method, prec in (("fp64_split", "split", "fp64"), ("fp64_fused", "fused", "fp64"),
+                               ("fp32_fused", "fused", "fp32")):
+        with S.FastMonodomainSolver(c1.copy(), method=method, precision=prec, device=device) as sv:
+            sv.setTimeSpan(0.0, 1.0)
+            sv.advanceTimeSpan()
+            sv.reset_timing()
+            sv.setTimeSpan(1.0, 10.0)
+            sv.advanceTimeSpan()
+            ms = sv.timing()["advance_ms"]
+            if method == "fused":
+                # few fibers: each fiber spread over the CTAs of a thread-block cluster
+                out["fused_layout"] = sv.fused_layout()
+        out[name] = c1.n_nodes * 9000 / (ms / 1e3)
+    return out
+
+
 def shorten_measurement(device: int, span_ms: float):
     """The Shorten 2007 configuration (56 states; 1369 fibers x 1481 nodes = 2.03M nodes, dt0D 1e-5, dt_split
     5e-4, seeded per-MU firing): FP64 plain (split) against the FP32-reaction path on the same fibers over a
@@ -238,7 +261,9 @@ def emg_coupled(device: int, solver_cfg: dict, overlap: bool = True) -> dict:
         wall = time.perf_counter() - t0
         phi = cp.term2.phi_e()
         layout = fib.fused_layout()
+        cpu = emg_cpu_baseline(cp.term2) if overlap else None
     return {
+        "cpu_baseline": cpu,
         "workload": "fibers_emg-shaped box: 13 x 13 HH fibers x 1481 nodes (FP32 fused), 3D mesh 25 x 25 x 149 "
                     "nodes, sigma_i/sigma_e of the example, coupling dt 1 ms, CG rtol 1e-8",
         "coupling_steps": len(solves), "ms_per_coupling_step": wall / max(len(solves), 1) * 1e3,
@@ -248,6 +273,38 @@ def emg_coupled(device: int, solver_cfg: dict, overlap: bool = True) -> dict:
         "overlap": overlap,
         "timing": "host wall clock around the coupled steps (fiber advance + transfer + solve; with overlap the "
                   "solve of step k runs beside the fiber advance of step k + 1)"}
+
+
+def emg_cpu_baseline(bid) -> dict:
+    """The last bidomain system solved on the host cores: scipy's conjugate gradients with the Jacobi
+    preconditioner on the same matrix (the device-assembled stencil as CSR) and right-hand side, from zero,
+    against the device solve from zero."""
+    import scipy.sparse.linalg as spla
+    sys.path.insert(0, ROOT)
+    from oracle import emg_oracle as EO
+    A = EO.stencil_to_sparse(bid.stencil(1), bid.shape).tocsr()
+    b = bid.rhs()
+    b = b - b.mean()
+    dinv = 1.0 / A.diagonal()
+    M = spla.LinearOperator(A.shape, matvec=lambda v: dinv * v)
+    its = [0]
+
+    def count(_):
+        its[0] += 1
+    t0 = time.perf_counter()
+    x, info = spla.cg(A, b, rtol=1e-8, atol=0.0, maxiter=20000, M=M, callback=count)
+    cpu_s = time.perf_counter() - t0
+    x -= x.mean()
+    keep = bid.initial_guess_nonzero
+    bid.initial_guess_nonzero = False
+    bid.advanceTimeSpan()
+    bid.initial_guess_nonzero = keep
+    t = bid.timing()
+    phi = bid.phi_e()
+    return {"kind": "port", "cores": 1, "solver": "scipy.sparse.linalg.cg, Jacobi preconditioner, rtol 1e-8, from 0",
+            "cpu_solve_ms": cpu_s * 1e3, "cpu_iterations": its[0], "gpu_solve_ms_from_zero": t["solve_ms"],
+            "gpu_iterations_from_zero": t["iterations"], "speedup": cpu_s * 1e3 / t["solve_ms"],
+            "max_abs_diff": float(np.max(np.abs(phi - x)))}
 
 
 def _cg_iteration(out: dict, device: int, peak_hbm: float, cg_mesh, cg_iterations: int, solver_cfg: dict):
@@ -331,6 +388,8 @@ def main():
             if args.only in ("emg", "emg-cg"):
                 out = {"emg": emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations,
                                               coupled=args.only == "emg")}
+            elif args.only == "plain":
+                out = {"plain_config_node_steps_per_s": plain_measurement(local)}
             else:
                 out = {"shorten": shorten_measurement(local, args.shorten_ms)}
             print(json.dumps(out), flush=True)
@@ -413,21 +472,7 @@ def main():
     # and the FP32 fused kernel on the same fibers)
     plain_cfg = None
     if rank == 0 and not args.skip_fp64:
-        c1 = WL.plain_hh(end_time=10.0)
-        plain_cfg = {"workload": "16 HH fibers x 1481 nodes, implicit Euler, 10 ms"}
-        for name, method, prec in (("fp64_split", "split", "fp64"), ("fp64_fused", "fused", "fp64"),
-                                   ("fp32_fused", "fused", "fp32")):
-            with S.FastMonodomainSolver(c1.copy(), method=method, precision=prec, device=local) as sv:
-                sv.setTimeSpan(0.0, 1.0)
-                sv.advanceTimeSpan()
-                sv.reset_timing()
-                sv.setTimeSpan(1.0, 10.0)
-                sv.advanceTimeSpan()
-                ms = sv.timing()["advance_ms"]
-                if method == "fused":
-                    # few fibers: each fiber spread over the CTAs of a thread-block cluster
-                    plain_cfg["fused_layout"] = sv.fused_layout()
-            plain_cfg[name] = c1.n_nodes * 9000 / (ms / 1e3)
+        plain_cfg = plain_measurement(local)
 
     # differentiation: adjoint gradient cost relative to one FP64 forward solve (256 HH fibers x 1481 nodes,
     # per-fiber sigma, g_Na, g_K; 32 sensors per fiber; checkpoint every 100 Strang steps)
