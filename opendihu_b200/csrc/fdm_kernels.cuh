@@ -1028,6 +1028,57 @@ __device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, do
   return block_scan_map<T, REVERSE>(acc, sF, sG, nullptr).G; // applied to the zero entering the first node
 }
 
+// Split path, few fibers: one diffusion solve per fiber with one CTA per fiber (a warp per fiber would leave
+// most of the GPU idle).  Thread tid owns a contiguous chunk of the fiber; the forward sweep and the back
+// substitution are block-wide scans of affine maps as in the fused kernel.  Same arguments and equilibrium
+// skip as diffusion_warp_kernel (forward results d' in scratch).
+template<int T>
+__global__ void __launch_bounds__(T) diffusion_block_kernel(const int64_t* __restrict__ fiber_offsets,
+                                                            const double* __restrict__ coef, int64_t stride,
+                                                            double* __restrict__ vm, double* __restrict__ scratch,
+                                                            const int* __restrict__ eq_counter,
+                                                            const int* __restrict__ eq_nbuf, int n_ranks)
+{
+  __shared__ double sF[2 * (T / 32) + 1], sG[2 * (T / 32) + 1];
+  const int f = blockIdx.x;
+  const int tid = threadIdx.x;
+  if (eq_counter && eq_counter[f % n_ranks] == eq_nbuf[f % n_ranks])
+    return; // the whole CTA: the rank's buffers are all inactive
+  const int64_t o = fiber_offsets[f];
+  const int64_t n = fiber_offsets[f + 1] - o;
+  const int64_t L = (n + T - 1) / T;
+  const int64_t lo = o + min((int64_t)tid * L, n);
+  const int64_t hi = o + min((int64_t)(tid + 1) * L, n);
+  const double* mulF = coef;
+  const double* inv = coef + stride;
+  const double* cp = coef + 2 * stride;
+  const double* cl = coef + 3 * stride;
+  const double* cm = coef + 4 * stride;
+  const double* cr = coef + 5 * stride;
+  auto rhs = [&](int64_t i) {
+    const double up = i > o ? vm[i - 1] : 0.0;
+    const double un = i < o + n - 1 ? vm[i + 1] : 0.0;
+    return cl[i] * up + cm[i] * vm[i] + cr[i] * un;
+  };
+  Affine acc{1.0, 0.0};
+  for (int64_t i = lo; i < hi; i++)
+    acc = compose(acc, Affine{mulF[i], inv[i] * rhs(i)});
+  double dp = block_scan_incoming<T, false>(acc, sF, sG);
+  for (int64_t i = lo; i < hi; i++) {
+    dp = mulF[i] * dp + inv[i] * rhs(i);
+    scratch[i] = dp;
+  }
+  __syncthreads(); // every read of the old Vm done, scratch complete, sF/sG free
+  Affine bacc{1.0, 0.0};
+  for (int64_t i = hi - 1; i >= lo; i--)
+    bacc = compose(bacc, Affine{-cp[i], scratch[i]});
+  double x = block_scan_incoming<T, true>(bacc, sF, sG);
+  for (int64_t i = hi - 1; i >= lo; i--) {
+    x = -cp[i] * x + scratch[i];
+    vm[i] = x;
+  }
+}
+
 // Adjoint of one diffusion solve (see adjoint_diffusion_warp_kernel for the algebra) with one CTA per
 // fiber of at most T*M nodes: thread tid owns nodes tid*M .. tid*M+M-1 in registers, the two sweeps of the
 // LU solve are block-wide scans of affine maps (as in the fused kernel), neighbours across threads go

@@ -101,12 +101,22 @@ cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, cons
   return cudaGetLastError();
 }
 
+// below this many fibers the diffusion solves take a CTA per fiber (4 warps' worth of CTAs per SM would be
+// needed before a warp per fiber fills the GPU)
+constexpr int DIFFUSION_BLOCK_MAX_FIBERS = 4 * 148;
+
 cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
                                   double* vm, double* scratch, cudaStream_t s, const int* eq_counter,
                                   const int* eq_nbuf, int n_ranks)
 {
   if (n_fibers == 0)
     return cudaSuccess;
+  if (n_fibers < DIFFUSION_BLOCK_MAX_FIBERS) {
+    // few fibers: a CTA per fiber fills more of the GPU than a warp per fiber
+    diffusion_block_kernel<256><<<(unsigned)n_fibers, 256, 0, s>>>(fiber_offsets, coef, stride, vm, scratch,
+                                                                   eq_counter, eq_nbuf, n_ranks > 0 ? n_ranks : 1);
+    return cudaGetLastError();
+  }
   const int T = 128;
   const int64_t threads = (int64_t)n_fibers * 32;
   diffusion_warp_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, s>>>(n_fibers, fiber_offsets, coef, stride, vm,
@@ -210,7 +220,7 @@ cudaError_t launch_adjoint_diffusion(int n_fibers, const int64_t* fiber_offsets,
   if (n_fibers == 0)
     return cudaSuccess;
   // few fibers: one CTA per fiber (block-wide scans); many fibers: one warp per fiber fills the GPU
-  if (n_fibers < 4 * 148) {
+  if (n_fibers < DIFFUSION_BLOCK_MAX_FIBERS) {
     if (max_fiber_len <= 512)
       return adjoint_diffusion_block<128, 4>(n_fibers, fiber_offsets, element_lengths, coef, stride, lam, u, x,
                                              implicit_euler, grad_prefactor, s);
