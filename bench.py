@@ -47,7 +47,7 @@ def parse_args():
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
     p.add_argument("--skip-emg", action="store_true")
-    p.add_argument("--only", choices=["emg", "emg-cg", "shorten", "plain"],
+    p.add_argument("--only", choices=["emg", "emg-cg", "shorten", "plain", "adjoint"],
                    help="print one side measurement alone (profiling runs)")
     p.add_argument("--skip-shorten", action="store_true")
     p.add_argument("--shorten-ms", type=float, default=0.02, help="simulated span of the Shorten measurement")
@@ -168,6 +168,42 @@ def cpu_baseline(system, sample_fibers: int, sample_ms: float, threads: int):
     st, _, tr, n = H.run_oracle(sub.copy(), n_threads=threads)
     dt = time.perf_counter() - t0
     return sub, st, n, sub.n_nodes * n / dt, dt
+
+
+def adjoint_measurement(device: int, span_ms: float) -> dict:
+    """Differentiation configuration: adjoint gradient cost relative to one FP64 forward solve (256 HH fibers x
+    1481 nodes, per-fiber sigma, g_Na, g_K; 32 sensors per fiber; checkpoint every 100 Strang steps)."""
+    from opendihu_b200 import adjoint as ADJ
+    from opendihu_b200 import solver as S
+    from opendihu_b200 import workloads as WL
+    dsys, sigma, s_na, s_k, sensors = WL.differentiation_hh(end_time=span_ms, seed=1)
+    _, sigma2, s_na2, s_k2, _ = WL.differentiation_hh(end_time=span_ms, seed=2)
+    eng = ADJ.AdjointEngine(dsys, sensors, checkpoint_every=100, device=device)
+    target = eng.forward(sigma2 / (WL.AM * WL.CM), WL.hh_parameters(dsys, s_na2, s_k2))
+    eng.solver.reset_timing()
+    trace = eng.forward(dsys.prefactor, dsys.parameters)
+    fwd_ck_ms = eng.solver.timing()["advance_ms"]
+    loss = float(((trace - target) ** 2).sum())
+    g = eng.backward(2.0 * (trace - target))
+    bwd_ms = eng.solver.adjoint_timing_ms()
+    eng.close()
+    with S.FastMonodomainSolver(dsys.copy(), method="split", precision="fp64", device=device) as fw:
+        fw.advanceTimeSpan()
+        fw.reset_timing()
+        fw.rewind()
+        fw.set_states(np.repeat(S.model_sizes(dsys.model)[3][:, None], dsys.n_nodes, axis=1))
+        fw.advanceTimeSpan()
+        plain_fwd_ms = fw.timing()["advance_ms"]
+    lengths = np.diff(dsys.fiber_offsets)
+    fiber_of = np.repeat(np.arange(dsys.n_fibers), lengths)
+    g_na = np.bincount(fiber_of, g["parameters"][1] * 120.0, minlength=dsys.n_fibers)
+    return {"workload": "256 HH fibers x 1481 nodes, %g ms, 32 sensors/fiber, checkpoint every 100 steps, "
+                        "768 parameters (sigma, g_Na scale, g_K scale per fiber)" % span_ms,
+            "forward_ms": plain_fwd_ms, "checkpointed_forward_ms": fwd_ck_ms, "backward_ms": bwd_ms,
+            "adjoint_over_forward": (fwd_ck_ms + bwd_ms) / plain_fwd_ms,
+            "backward_over_forward": bwd_ms / plain_fwd_ms, "loss": loss,
+            "grad_norm_sigma": float(np.linalg.norm(g["prefactor"] / (WL.AM * WL.CM))),
+            "grad_norm_gna_scale": float(np.linalg.norm(g_na))}
 
 
 def plain_measurement(device: int) -> dict:
@@ -390,6 +426,8 @@ def main():
                                               coupled=args.only == "emg")}
             elif args.only == "plain":
                 out = {"plain_config_node_steps_per_s": plain_measurement(local)}
+            elif args.only == "adjoint":
+                out = {"adjoint": adjoint_measurement(local, args.adjoint_ms)}
             else:
                 out = {"shorten": shorten_measurement(local, args.shorten_ms)}
             print(json.dumps(out), flush=True)
@@ -478,35 +516,7 @@ def main():
     # per-fiber sigma, g_Na, g_K; 32 sensors per fiber; checkpoint every 100 Strang steps)
     adj = None
     if rank == 0 and not args.skip_adjoint:
-        from opendihu_b200 import adjoint as ADJ
-        dsys, sigma, s_na, s_k, sensors = WL.differentiation_hh(end_time=args.adjoint_ms, seed=1)
-        _, sigma2, s_na2, s_k2, _ = WL.differentiation_hh(end_time=args.adjoint_ms, seed=2)
-        eng = ADJ.AdjointEngine(dsys, sensors, checkpoint_every=100, device=local)
-        target = eng.forward(sigma2 / (WL.AM * WL.CM), WL.hh_parameters(dsys, s_na2, s_k2))
-        eng.solver.reset_timing()
-        trace = eng.forward(dsys.prefactor, dsys.parameters)
-        fwd_ck_ms = eng.solver.timing()["advance_ms"]
-        loss = float(((trace - target) ** 2).sum())
-        g = eng.backward(2.0 * (trace - target))
-        bwd_ms = eng.solver.adjoint_timing_ms()
-        eng.close()
-        with S.FastMonodomainSolver(dsys.copy(), method="split", precision="fp64", device=local) as fw:
-            fw.advanceTimeSpan()
-            fw.reset_timing()
-            fw.rewind()
-            fw.set_states(np.repeat(S.model_sizes(dsys.model)[3][:, None], dsys.n_nodes, axis=1))
-            fw.advanceTimeSpan()
-            plain_fwd_ms = fw.timing()["advance_ms"]
-        lengths = np.diff(dsys.fiber_offsets)
-        fiber_of = np.repeat(np.arange(dsys.n_fibers), lengths)
-        g_na = np.bincount(fiber_of, g["parameters"][1] * 120.0, minlength=dsys.n_fibers)
-        adj = {"workload": "256 HH fibers x 1481 nodes, %g ms, 32 sensors/fiber, checkpoint every 100 steps, "
-                           "768 parameters (sigma, g_Na scale, g_K scale per fiber)" % args.adjoint_ms,
-               "forward_ms": plain_fwd_ms, "checkpointed_forward_ms": fwd_ck_ms, "backward_ms": bwd_ms,
-               "adjoint_over_forward": (fwd_ck_ms + bwd_ms) / plain_fwd_ms,
-               "backward_over_forward": bwd_ms / plain_fwd_ms, "loss": loss,
-               "grad_norm_sigma": float(np.linalg.norm(g["prefactor"] / (WL.AM * WL.CM))),
-               "grad_norm_gna_scale": float(np.linalg.norm(g_na))}
+        adj = adjoint_measurement(local, args.adjoint_ms)
 
     # fibers -> 3D static bidomain (EMG): the coupled fibers_emg-shaped workload, and the conjugate-gradient
     # iteration on a mesh larger than L2 against the HBM roofline
@@ -527,9 +537,9 @@ def main():
                "sample": f"first 10 fibers of the batch ({sub.n_nodes} nodes) x 20 ms ({n_ref} Strang steps), "
                          f"{cpu_s:.1f} s"}
         # one thread: the reference's vc path runs one thread per MPI rank
-        sub1, _, n1, rate1, cpu1_s = cpu_baseline(system, 2, 10.0, 1)
+        sub1, _, n1, rate1, cpu1_s = cpu_baseline(system, 1, 10.0, 1)
         cpu["single_thread"] = {"value": rate1, "unit": "node-steps/s", "cores": 1,
-                                "sample": f"first 2 fibers ({sub1.n_nodes} nodes) x 10 ms ({n1} Strang steps), "
+                                "sample": f"first fiber ({sub1.n_nodes} nodes) x 10 ms ({n1} Strang steps), "
                                           f"{cpu1_s:.1f} s"}
         acc = {}
         for name, method, prec in (("fp32_fused", "fused", "fp32"), ("fp64_split", "split", "fp64")):

@@ -191,9 +191,10 @@ struct fdm_solver {
     DevBuf<uint8_t> ck_hbs, fin_hbs;
     Tss fin_strang, fin_heun, fin_diff;
     int64_t fin_split = 0;
-    // two buffer sets (stored substep states H, Vm before/after each diffusion solve U/X, stimulation bits)
+    // two buffer sets (stored substep states H, Vm before each diffusion solve U -- Vm after it is the
+    // stored input of the next half step --, stimulation bits)
     // so that the replay of one segment overlaps the reverse sweep of the next one in reverse order
-    DevBuf<double> H[2], U[2], X[2], lam, gP, gpf, mu, ascratch, tgrad;
+    DevBuf<double> H[2], U[2], lam, gP, gpf, mu, ascratch, tgrad;
     DevBuf<double> coefs;                           // one factorization per distinct diffusion step width
     DevBuf<uint32_t> flags[2];
     DevBuf<uint8_t> gates[2];
@@ -203,7 +204,7 @@ struct fdm_solver {
     void release()
     {
       for (auto* b : {&ck_vm, &ck_states, &ck_last, &ck_jit, &fin_vm, &fin_states, &fin_last, &fin_jit, &H[0], &H[1],
-                      &U[0], &U[1], &X[0], &X[1], &lam, &gP, &gpf, &mu, &ascratch, &tgrad, &coefs})
+                      &U[0], &U[1], &lam, &gP, &gpf, &mu, &ascratch, &tgrad, &coefs})
         b->release();
       flags[0].release();
       flags[1].release();
@@ -2685,7 +2686,6 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       FDM_CUDA(A.gates[k].alloc((size_t)std::max(nf, 1) * 2 * s->step_capacity));
     FDM_CUDA(A.H[k].alloc((size_t)A.kc * 2 * hstride));
     FDM_CUDA(A.U[k].alloc((size_t)A.kc * N));
-    FDM_CUDA(A.X[k].alloc((size_t)A.kc * N));
     FDM_CUDA(A.flags[k].alloc((size_t)max_words * std::max(nf, 1)));
     if (!A.replayed[k])
       FDM_CUDA(cudaEventCreateWithFlags(&A.replayed[k], cudaEventDisableTiming));
@@ -2741,8 +2741,8 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
   std::vector<WindowInfo> win(A.n_seg);
 
-  // replay of segment c into buffer k (stream s->stream): every substep's input state and Vm before/after
-  // each diffusion solve
+  // replay of segment c into buffer k (stream s->stream): every substep's input state and Vm before each
+  // diffusion solve
   auto replay = [&](int c, int k) -> int {
     FDM_CUDA(cudaStreamWaitEvent(s->stream, A.reversed[k], 0));
     int rc = copy_state(s, A.ck_vm.p + (size_t)c * N, A.ck_states.p + (size_t)c * N * (NS - 1),
@@ -2783,15 +2783,14 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
       for (int half = 0; half < 2; half++) {
         ra.half = half;
         ra.store_states = A.H[k].p + ((size_t)jj * 2 + half) * hstride;
+        // Vm before the diffusion solve (U) comes out of the first half step; Vm after it is the stored input
+        // of the second half step's first substep
+        ra.store_vm_out = half == 0 ? A.U[k].p + (size_t)jj * N : nullptr;
         FDM_CUDA(launch_reaction(s->cfg.model, REAL_F64, mk, ra, s->stream));
         s->launches++;
         if (half == 0) {
-          FDM_CUDA(cudaMemcpyAsync(A.U[k].p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
-                                   s->stream));
           FDM_CUDA(launch_diffusion_warp(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream));
           s->launches++;
-          FDM_CUDA(cudaMemcpyAsync(A.X[k].p + (size_t)jj * N, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice,
-                                   s->stream));
         }
       }
     }
@@ -2838,7 +2837,7 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
           return rc;
       }
       FDM_CUDA(launch_adjoint_diffusion(nf, s->off_d.p, s->elem_d.p, coef_of(j), N, A.lam.p, A.U[k].p + (size_t)jj * N,
-                                        A.X[k].p + (size_t)jj * N, ie, A.gpf.p, A.ascratch.p, A.mu.p,
+                                        A.H[k].p + ((size_t)jj * 2 + 1) * hstride, ie, A.gpf.p, A.ascratch.p, A.mu.p,
                                         s->max_fiber_len, rs));
       aa.half = 0;
       aa.trace_row = -1;

@@ -391,6 +391,7 @@ struct ReactionArgs {
   int64_t trace_capacity;
   double* store_states;           // adjoint replay (FP64 only): input state of substep k at
                                   // store_states[(k*nStates + s)*stride + node], or null
+  double* store_vm_out;           // adjoint replay: Vm after the half step also written here, or null
   const int* gate;                // onlyComputeIfHasBeenStimulated: per node gate code, or null
   const uint8_t* gate_start;
   int gate_stride;
@@ -450,6 +451,8 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
     }
   }
   a.vm[i] = V;
+  if (a.store_vm_out)
+    a.store_vm_out[i] = V;
 #pragma unroll
   for (int s2 = 1; s2 < NS; s2++) {
     st[(s2 - 1) * a.stride + i] = S[s2 - 1];

@@ -330,14 +330,14 @@ class ShardedSolver:
 def adjoint_bytes_per_node(model: str, n_substeps: int, n_steps: int, checkpoint_every: int) -> int:
     """Device bytes per node the FP64 adjoint holds (fdm_adjoint_forward / fdm_adjoint_backward): one
     checkpoint of the states per segment, two replay buffers of a segment's Heun substep states (the replay of
-    one segment overlaps the reverse sweep of the next) with Vm around each diffusion solve, and the adjoint
+    one segment overlaps the reverse sweep of the next) with Vm before each diffusion solve, and the adjoint
     variables; n_substeps = Heun substeps per half step."""
     from .solver import model_sizes
     ns, _, npar = model_sizes(model)[:3]
     kc = max(1, min(int(checkpoint_every), int(n_steps)))
     segments = -(-int(n_steps) // kc)
     checkpoints = segments * ns * 8
-    replay = 2 * kc * (2 * n_substeps * ns + 2) * 8
+    replay = 2 * kc * (2 * n_substeps * ns + 1) * 8
     adjoint = (ns + max(npar, 1) + 3) * 8
     return checkpoints + replay + adjoint
 
