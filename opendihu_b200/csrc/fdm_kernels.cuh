@@ -801,7 +801,7 @@ struct AdjointForms<Model, Math, true> {
 // The stored input state of the next substep in reverse order is loaded while the current one is
 // differentiated (models with at most 8 states).
 template<class Model, class Math>
-__global__ void __launch_bounds__(128, 4) adjoint_half_kernel(AdjointArgs a)
+__global__ void __launch_bounds__(128, 3) adjoint_half_kernel(AdjointArgs a)
 {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n_nodes)
