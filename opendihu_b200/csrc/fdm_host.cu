@@ -1849,7 +1849,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
         s->launches += 6;
         cur ^= 1;
         if (half == 0) {
-          FDM_CUDA(launch_diffusion_warp(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
+          FDM_CUDA(launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
                                          s->stream, E.counter.p, E.nbuf.p, s->cfg.n_ranks));
           s->launches++;
         }
@@ -1873,7 +1873,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
           ra.store_alg = 0;
           ce = launch_reaction(s->cfg.model, rk, mk, ra, s->stream);
           if (ce == cudaSuccess && half == 0)
-            ce = launch_diffusion_warp(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
+            ce = launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
                                        s->stream);
         }
       }
@@ -1907,7 +1907,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
       if (prof)
         FDM_CUDA(cudaEventRecord(e1, s->stream));
       if (half == 0) {
-        FDM_CUDA(launch_diffusion_warp(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
+        FDM_CUDA(launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
                                        s->stream));
         s->launches++;
       }
@@ -2258,7 +2258,7 @@ extern "C" int fdm_diffusion_solve(int n_fibers, int64_t n_nodes, const int64_t*
   double* fwd = coef + 6 * (size_t)n_nodes;
   FDM_CUDA(launch_coefficients(n_fibers, d_fiber_offsets, d_element_lengths, d_prefactor, dt,
                                diffusion_scheme == FDM_IMPLICIT_EULER, coef, n_nodes, st));
-  FDM_CUDA(launch_diffusion_warp(n_fibers, d_fiber_offsets, coef, n_nodes, d_vm, fwd, st));
+  FDM_CUDA(launch_diffusion(n_fibers, d_fiber_offsets, coef, n_nodes, d_vm, fwd, st));
   FDM_CUDA(cudaStreamSynchronize(st));
   return FDM_OK;
 }
@@ -2789,7 +2789,7 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
         FDM_CUDA(launch_reaction(s->cfg.model, REAL_F64, mk, ra, s->stream));
         s->launches++;
         if (half == 0) {
-          FDM_CUDA(launch_diffusion_warp(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream));
+          FDM_CUDA(launch_diffusion(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream));
           s->launches++;
         }
       }

@@ -34,9 +34,11 @@ cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionA
 cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s);
 cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
                                 double* coef, int64_t stride, cudaStream_t s);
-cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
-                                  double* vm, double* scratch, cudaStream_t s, const int* eq_counter = nullptr,
-                                  const int* eq_nbuf = nullptr, int n_ranks = 1);
+// one diffusion solve of every fiber in place on vm (scratch: one double per node): a warp per fiber, or a
+// CTA per fiber when the fibers are few
+cudaError_t launch_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
+                             double* vm, double* scratch, cudaStream_t s, const int* eq_counter = nullptr,
+                             const int* eq_nbuf = nullptr, int n_ranks = 1);
 // one half step with the equilibrium skip (fdm_equilibrium.cuh): speculative reaction, equilibrium tests,
 // scan of the buffers, commit (and the trace after half 1)
 cudaError_t launch_equilibrium_half(int model, RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L,

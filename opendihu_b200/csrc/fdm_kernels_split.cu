@@ -105,7 +105,7 @@ cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, cons
 // needed before a warp per fiber fills the GPU)
 constexpr int DIFFUSION_BLOCK_MAX_FIBERS = 4 * 148;
 
-cudaError_t launch_diffusion_warp(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
+cudaError_t launch_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
                                   double* vm, double* scratch, cudaStream_t s, const int* eq_counter,
                                   const int* eq_nbuf, int n_ranks)
 {

@@ -82,7 +82,7 @@ extern "C" int fdm_diffusion_solve_noalloc(int n_fibers, int64_t n_nodes, const 
   e = fdm::launch_coefficients(n_fibers, d_fiber_offsets, d_element_lengths, d_prefactor, dt,
                                diffusion_scheme == FDM_IMPLICIT_EULER, coef, n_nodes, st);
   if (e == cudaSuccess)
-    e = fdm::launch_diffusion_warp(n_fibers, d_fiber_offsets, coef, n_nodes, d_vm, fwd, st);
+    e = fdm::launch_diffusion(n_fibers, d_fiber_offsets, coef, n_nodes, d_vm, fwd, st);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(st);
   if (e != cudaSuccess)

@@ -71,3 +71,15 @@ def test_fiber_longer_than_every_fused_launch_fails_loudly():
     with pytest.raises(S.N.FdmError) as e:
         S.FastMonodomainSolver(H.complete(s), method="fused").initialize()
     assert e.value.code == S.N.FDM_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("n_fibers", [591, 592])
+def test_split_diffusion_on_both_sides_of_the_block_threshold(n_fibers):
+    # below 592 fibers the split path solves each fiber with a CTA, from 592 on with a warp
+    rng = np.random.default_rng(n_fibers)
+    lengths = rng.integers(2, 40, size=n_fibers)
+    s = S.uniform_fibers(H.HH, lengths, 0.01, 3.828 / 500, call_frequency=0.2, repeat_after_first_call=0.1,
+                         firing_events=rng.integers(0, 2, size=(5, 4)).astype(np.uint8),
+                         motor_unit_no=rng.integers(0, 4, size=n_fibers).astype(np.int32), end_time=0.6,
+                         diffusion_scheme="CrankNicolson")
+    GP.compare(s, "split", "fp64", GP.VM_TOL_FP64, 1e-8)

@@ -139,3 +139,21 @@ def test_compute_state_information(skip, only, n_ranks, width):
         assert np.any(got == 0)       # buffers at rest were counted inactive
     if only:
         assert np.any(got == -1)      # fiber 3 starts at 1.2345 ms
+
+
+def test_many_fibers_warp_diffusion_with_the_skip():
+    # 600 fibers: the split path's diffusion takes a warp per fiber and skips the ranks counted at rest
+    s = WL.batched_hh(n_fibers=600, min_nodes=8, max_nodes=24, seed=7, end_time=0.6, n_ranks=2)
+    s.firing_events = np.zeros((1, 100), np.uint8)
+    s.firing_events[0, :3] = 1
+    H.complete(s)
+    s.states = np.repeat(_rest()[:, None], s.n_nodes, axis=1)
+    s.skip_close_to_equilibrium = True
+    ref, ref_status, ref_counter, _ = _oracle(s)
+    with S.FastMonodomainSolver(s.copy(), method="split", precision="fp64") as slv:
+        slv.advanceTimeSpan()
+        st = slv.states()
+        status, counter = slv.equilibrium_state()
+    assert np.max(np.abs(st[0] - ref[0])) <= GP.VM_TOL_FP64
+    np.testing.assert_array_equal(status, ref_status)
+    np.testing.assert_array_equal(counter, ref_counter)
