@@ -418,6 +418,10 @@ def main():
     world, rank, local, pg = dist_setup(args)
     from opendihu_b200 import solver as S
     from opendihu_b200 import workloads as WL
+    if world > 1:
+        # the side measurements (plain configuration, adjoint, EMG, Shorten, accuracy and CPU baseline) are
+        # single-GPU numbers reported by the 1-GPU run; on N GPUs rank 0 would hold the other GPUs meanwhile
+        args.skip_adjoint = args.skip_emg = args.skip_shorten = args.skip_accuracy = True
     cg_mesh = tuple(int(x) for x in args.emg_cg_mesh.split(","))
     if args.only:
         if rank == 0:
@@ -509,7 +513,7 @@ def main():
     # plain-method configuration (16 HH fibers x 1481 nodes, implicit Euler, FP64 split path with CUDA graphs,
     # and the FP32 fused kernel on the same fibers)
     plain_cfg = None
-    if rank == 0 and not args.skip_fp64:
+    if rank == 0 and not args.skip_fp64 and world == 1:
         plain_cfg = plain_measurement(local)
 
     # differentiation: adjoint gradient cost relative to one FP64 forward solve (256 HH fibers x 1481 nodes,
