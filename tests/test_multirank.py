@@ -40,7 +40,7 @@ def _worker(rank, world, port, out):
 
 def test_two_gloo_ranks_shard_independent_batches():
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     assert out[0][0] == out[1][0] == 2.0          # max over ranks

@@ -132,7 +132,7 @@ def _gather_worker(rank, world, port, out):
 
 def test_two_gloo_ranks_gather_shards():
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_gather_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     s = WL.batched_hh(n_fibers=6, min_nodes=12, max_nodes=30, seed=9, end_time=0.2, clamp_rule="center")
