@@ -174,6 +174,16 @@ int fdm_advance(fdm_solver *s, double t_start, double t_end);
  * advance waits first. */
 int fdm_advance_async(fdm_solver *s, double t_start, double t_end);
 int fdm_wait(fdm_solver *s);
+/* The RepeatedCall pieces of [t_start, t_end] (repeated_call.tpp:43-80: piece k is one call of
+ * FastMonodomainSolver::advanceTimeSpan, after which the reference calls the diffusion's output writers,
+ * fast_monodomain_solver_compute.tpp:35-44): their number, and, when steps_per_piece is not null, the number
+ * of split steps of each (the writers' callCountIncrement), planned from the solver's current time-stepping
+ * state without changing it. */
+int fdm_repeated_call_plan(fdm_solver *s, double t_start, double t_end, int64_t *n_pieces, int *steps_per_piece);
+/* advances the pieces k_begin <= k < k_end of that span (blocking): consecutive ranges covering all pieces
+ * give the same steps, bit for bit, as one fdm_advance over the span, with the host free between them
+ * (output at the reference's times) */
+int fdm_advance_pieces(fdm_solver *s, double t_start, double t_end, int64_t k_begin, int64_t k_end);
 /* number of split steps done by all advances so far */
 int64_t fdm_split_steps(const fdm_solver *s);
 /* summed device time and count of the main kernel launches (config.profile = 1), and of all GPU work

@@ -14,6 +14,8 @@
 #define FDM_B200_HPP
 
 #include <cstdint>
+#include <cstdio>
+#include <functional>
 #include <fstream>
 #include <map>
 #include <sstream>
@@ -151,16 +153,53 @@ struct TransferData {
   std::vector<double> algebraics;  // algebraicsForTransfer
 };
 
+/* One output writer of the diffusion solver.  When it writes restates OutputWriter::Generic::prepareWrite
+ * (core/src/output_writer/generic.tpp:14-115): every call adds callCountIncrement to a call counter, a call
+ * writes when the counter passes a multiple of outputInterval (or its increment is 0: the initial values),
+ * under <filename>_<no:07d>, no being the running file number or, with timeStepIndexNumbering, the counter.
+ * What is written is the callback's: it gets the numbered name and the current time, and reads the fiber
+ * data through FastMonodomainSolver::data(). */
+struct OutputWriter {
+  int outputInterval = 1;
+  std::string filename = "out";
+  bool timeStepIndexNumbering = false;
+  std::function<void(const std::string& name, double currentTime)> write;
+  int writeCallCount = 0;
+  int outputFileNo = 0;
+
+  /* counts one call; true (and the numbered name) when it writes */
+  bool prepare(int timeStepNo, int callCountIncrement, std::string& name)
+  {
+    const int interval = outputInterval > 0 ? outputInterval : 1;
+    const int old = writeCallCount;
+    writeCallCount += callCountIncrement;
+    const int last = writeCallCount - writeCallCount % interval;
+    if (!((old < last && last <= writeCallCount) || callCountIncrement == 0))
+      return false;
+    name = filename;
+    if (timeStepNo != -1) {
+      char no[16];
+      std::snprintf(no, sizeof(no), "_%07d", timeStepIndexNumbering ? writeCallCount : outputFileNo);
+      name += no;
+    }
+    outputFileNo++;
+    return true;
+  }
+};
+
 class FastMonodomainSolver {
  public:
   explicit FastMonodomainSolver(FiberSettings settings) : s_(std::move(settings))
   {
     start_ = s_.start_time;
     end_ = s_.end_time;
+    current_time_ = s_.start_time;
   }
   FastMonodomainSolver(const FastMonodomainSolver&) = delete;
   FastMonodomainSolver& operator=(const FastMonodomainSolver&) = delete;
-  FastMonodomainSolver(FastMonodomainSolver&& o) noexcept : s_(std::move(o.s_)), h_(o.h_), start_(o.start_), end_(o.end_)
+  FastMonodomainSolver(FastMonodomainSolver&& o) noexcept
+      : s_(std::move(o.s_)), h_(o.h_), start_(o.start_), end_(o.end_), writers_(std::move(o.writers_)),
+        current_time_(o.current_time_), piece_steps_(o.piece_steps_)
   {
     o.h_ = nullptr;
   }
@@ -202,13 +241,44 @@ class FastMonodomainSolver {
     advanceTimeSpan();
   }
 
-  /* RepeatedCall over [startTime, endTime]; there are no output writers in this build, the flag is kept
-   * for the signature */
+  /* RepeatedCall over [startTime, endTime].  The output writers run after every RepeatedCall piece, as the
+   * reference's advanceTimeSpan calls the diffusion's writers (fast_monodomain_solver_compute.tpp:35-44) with
+   * timeStepNo 0, the piece's end time and its number of split steps: the advance stops only after the
+   * pieces whose call writes, the steps stay those of one advance over the span (fdm_advance_pieces). */
   void advanceTimeSpan(bool withOutputWritersEnabled = true)
   {
-    (void)withOutputWritersEnabled;
     initialize();
-    check(fdm_advance(h_, start_, end_));
+    int64_t n = 0;
+    check(fdm_repeated_call_plan(h_, start_, end_, &n, nullptr));
+    std::vector<int> steps((size_t)(n > 0 ? n : 1), 0);
+    if (!writers_.empty())
+      check(fdm_repeated_call_plan(h_, start_, end_, &n, steps.data()));
+    if (!withOutputWritersEnabled || writers_.empty()) {
+      check(fdm_advance(h_, start_, end_));
+      current_time_ = piece_end(n - 1, n);
+      piece_steps_ = steps[(size_t)(n - 1)];
+      return;
+    }
+    int64_t done = 0;
+    for (int64_t k = 0; k < n; k++) {
+      current_time_ = piece_end(k, n);
+      piece_steps_ = steps[(size_t)k];
+      std::vector<std::pair<OutputWriter*, std::string>> due;
+      for (OutputWriter& w : writers_) {
+        std::string name;
+        if (w.prepare(0, piece_steps_, name))
+          due.emplace_back(&w, name);
+      }
+      if (!due.empty()) {
+        check(fdm_advance_pieces(h_, start_, end_, done, k + 1));
+        done = k + 1;
+        for (auto& d : due)
+          if (d.first->write)
+            d.first->write(d.second, current_time_);
+      }
+    }
+    if (done < n)
+      check(fdm_advance_pieces(h_, start_, end_, done, n));
   }
 
   /* advanceTimeSpan that returns once the work is enqueued; wait() completes it */
@@ -269,12 +339,24 @@ class FastMonodomainSolver {
     h_ = nullptr;
   }
 
-  /* no output writers in this build (the fiber data comes back through data()) */
+  /* the diffusion's output writers, called after each RepeatedCall piece of advanceTimeSpan(true) */
+  void addOutputWriter(OutputWriter w) { writers_.push_back(std::move(w)); }
+
+  /* The reference's callOutputWriter (fast_monodomain_solver_base.tpp:7-24): when timeStepNo is a multiple of
+   * callCountIncrement the writers are called as after a RepeatedCall piece, with the end time and split steps
+   * of the last piece (0 steps before the first advance: the initial-values call, which always writes);
+   * currentTime is not used, as in the reference. */
   void callOutputWriter(int timeStepNo, double currentTime, int callCountIncrement = 1)
   {
-    (void)timeStepNo;
     (void)currentTime;
-    (void)callCountIncrement;
+    initialize();
+    if (callCountIncrement == 0 || timeStepNo % callCountIncrement != 0)
+      return;
+    for (OutputWriter& w : writers_) {
+      std::string name;
+      if (w.prepare(0, piece_steps_, name) && w.write)
+        w.write(name, current_time_);
+    }
   }
 
   void saveFiberDataCheckpoint() { check(fdm_checkpoint_save(h_)); }
@@ -290,9 +372,20 @@ class FastMonodomainSolver {
       throw Error(rc, fdm_last_error(h_));
   }
 
+  /* end of RepeatedCall piece k of n (the Strang span's end time: start + k/n*span + span/n) */
+  double piece_end(int64_t k, int64_t n) const
+  {
+    const double span = end_ - start_;
+    const double t = k == 0 ? start_ : start_ + (double)k / (double)n * span;
+    return t + span / (double)n;
+  }
+
   FiberSettings s_;
   fdm_solver* h_ = nullptr;
   double start_ = 0.0, end_ = 0.0;
+  std::vector<OutputWriter> writers_;
+  double current_time_ = 0.0;  // the reference's currentTime_: end of the last RepeatedCall piece
+  int piece_steps_ = 0;        // its number of split steps (nTimeStepsSplitting_)
 };
 
 }  // namespace fdm

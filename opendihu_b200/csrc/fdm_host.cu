@@ -1919,8 +1919,13 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
 // The split steps of RepeatedCall<FastMonodomainSolver>::advanceTimeSpan over [t_start, t_end]
 // (repeated_call.tpp:43-75, fast_monodomain_solver_compute.tpp:64-129), with the time-step objects'
 // state carried from call to call as the reference's scheme objects carry it.
+// the RepeatedCall pieces k_begin <= k < k_end (k_end < 0: to the last) of the span [t_start, t_end] as split
+// steps (repeated_call.tpp:43-80: piece k starts at start + k/n*span); an advance split into consecutive piece
+// ranges gives the same step times as one over the whole span.  piece_steps, when given, receives the number of
+// split steps of each planned piece.
 static void plan_advance(fdm_solver* s, double t_start, double t_end, std::vector<SplitStep>& steps,
-                         std::vector<double>& dt1s)
+                         std::vector<double>& dt1s, int64_t k_begin = 0, int64_t k_end = -1,
+                         int* piece_steps = nullptr)
 {
   Tss rc;
   rc.init(t_start, t_end, s->cfg.dt_repeated_call);
@@ -1932,8 +1937,10 @@ static void plan_advance(fdm_solver* s, double t_start, double t_end, std::vecto
     s->diff.init(t_start, t_start + s->cfg.dt_1d, s->cfg.dt_1d);
     s->tss_init = true;
   }
-  double t = rc.start;
-  for (int k = 0; k < rc.n;) {
+  if (k_end < 0 || k_end > rc.n)
+    k_end = rc.n;
+  for (int64_t k = k_begin; k < k_end; k++) {
+    const double t = k == 0 ? rc.start : rc.start + (double)k / rc.n * span;
     s->strang.set_span(t, t + rc.dt);
     const double start = s->strang.start;
     const double dts = s->strang.dt;
@@ -1952,9 +1959,17 @@ static void plan_advance(fdm_solver* s, double t_start, double t_end, std::vecto
       steps.push_back(st);
       dt1s.push_back(s->diff.dt);
     }
-    k++;
-    t = rc.start + (double)k / rc.n * span;
+    if (piece_steps)
+      piece_steps[k - k_begin] = ns;
   }
+}
+
+static int64_t repeated_call_pieces(const fdm_solver* s, double t_start, double t_end)
+{
+  Tss rc;
+  rc.init(t_start, t_end, s->cfg.dt_repeated_call);
+  rc.set_dt(s->cfg.dt_repeated_call);
+  return rc.n;
 }
 
 // runs planned steps in windows of at most steps_per_launch steps that share the diffusion step width
@@ -2014,7 +2029,8 @@ extern "C" int fdm_wait(fdm_solver* s)
 
 // the work of an advance, enqueued on the solver's stream (the host waits only where the window buffers of
 // the step schedule are reused)
-static int enqueue_advance(fdm_solver* s, double t_start, double t_end, const char* who)
+static int enqueue_advance(fdm_solver* s, double t_start, double t_end, const char* who, int64_t k_begin = 0,
+                           int64_t k_end = -1)
 {
   if (!s)
     return fail(s, FDM_ERR_ARG, std::string(who) + ": null solver");
@@ -2030,7 +2046,7 @@ static int enqueue_advance(fdm_solver* s, double t_start, double t_end, const ch
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
   std::vector<SplitStep> steps;
   std::vector<double> dt1s;
-  plan_advance(s, t_start, t_end, steps, dt1s);
+  plan_advance(s, t_start, t_end, steps, dt1s, k_begin, k_end);
   return run_planned(s, steps, dt1s, 0, steps.size(), true);
 }
 
@@ -2075,6 +2091,40 @@ static int advance_explicit(fdm_solver* s, double start, double dts, int ns, dou
     s->split_no++;
   }
   int r = run_planned(s, steps, dt1s, 0, steps.size(), true);
+  if (r)
+    return r;
+  return finish_advance(s);
+}
+
+extern "C" int fdm_repeated_call_plan(fdm_solver* s, double t_start, double t_end, int64_t* n_pieces,
+                                      int* steps_per_piece)
+{
+  if (!s || !n_pieces || !(t_end >= t_start))
+    return fail(s, FDM_ERR_ARG, "fdm_repeated_call_plan: bad argument");
+  *n_pieces = repeated_call_pieces(s, t_start, t_end);
+  if (steps_per_piece) { // a dry run of the plan: the time-stepping state is put back
+    const Tss strang = s->strang, heun = s->heun, diff = s->diff;
+    const bool tss_init = s->tss_init;
+    const int64_t split_no = s->split_no;
+    std::vector<SplitStep> steps;
+    std::vector<double> dt1s;
+    plan_advance(s, t_start, t_end, steps, dt1s, 0, -1, steps_per_piece);
+    s->strang = strang;
+    s->heun = heun;
+    s->diff = diff;
+    s->tss_init = tss_init;
+    s->split_no = split_no;
+  }
+  return FDM_OK;
+}
+
+extern "C" int fdm_advance_pieces(fdm_solver* s, double t_start, double t_end, int64_t k_begin, int64_t k_end)
+{
+  if (!s)
+    return fail(s, FDM_ERR_ARG, "fdm_advance_pieces: null solver");
+  if (!(t_end >= t_start) || k_begin < 0 || k_end < k_begin || k_end > repeated_call_pieces(s, t_start, t_end))
+    return fail(s, FDM_ERR_ARG, "fdm_advance_pieces: need 0 <= k_begin <= k_end <= the number of pieces");
+  const int r = enqueue_advance(s, t_start, t_end, "fdm_advance_pieces", k_begin, k_end);
   if (r)
     return r;
   return finish_advance(s);

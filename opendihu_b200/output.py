@@ -12,7 +12,8 @@ from __future__ import annotations
 import json
 import os
 import pickle
-from typing import Dict, Optional, Sequence
+import warnings
+from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -81,3 +82,77 @@ def read(path: str) -> dict:
     except (UnicodeDecodeError, json.JSONDecodeError):
         with open(path, "rb") as fh:
             return pickle.load(fh)
+
+
+class OutputWriter:
+    """One entry of an ``"OutputWriter"`` settings list of the diffusion solver, for the fibers it covers.
+
+    When it writes restates ``OutputWriter::Generic::prepareWrite`` (core/src/output_writer/generic.tpp:14-115):
+    every call adds ``callCountIncrement`` to a call counter; a file is due when the counter passes a multiple
+    of ``outputInterval`` (``generic.cpp:20``, default 1), or when the increment is 0 (initial values).  Its
+    name is ``<filename>_<no:07d>`` with ``no`` the running file number (``"fileNumbering": "incremental"``,
+    the default) or the call counter (``"timeStepIndex"``).  Formats: ``PythonFile`` writes ``<name>.py``
+    (``<name>_<meshName>.py`` for a writer over several fibers, python_file.tpp:30-43) as JSON text, or as a
+    pickle with ``"binary": True`` (python_file.tpp:72); ``PythonCallback`` calls ``callback(list of the fiber
+    dicts)`` (python_callback_writer.tpp:68).  Other formats (Paraview, Exfile, MegaMol) are not built: they
+    warn once and write nothing.
+    """
+
+    FORMATS = ("PythonFile", "PythonCallback")
+
+    def __init__(self, settings: dict, fibers: Sequence[int], mesh_names: Optional[Sequence[str]] = None):
+        self.format = str(settings.get("format", "none"))
+        try:
+            interval = int(settings.get("outputInterval", 1))
+        except (TypeError, ValueError):
+            interval = 1
+        self.output_interval = interval if interval > 0 else 1
+        self.filename = str(settings.get("filename", "out"))
+        self.file_numbering = "timeStepIndex" if settings.get("fileNumbering") == "timeStepIndex" else "incremental"
+        self.binary = bool(settings.get("binary", False))
+        self.callback: Optional[Callable] = settings.get("callback")
+        self.fibers = [int(f) for f in fibers]
+        self.mesh_names = list(mesh_names) if mesh_names is not None else [f"MeshFiber_{f}" for f in self.fibers]
+        self.write_call_count = 0
+        self.output_file_no = 0
+        if self.format not in self.FORMATS:
+            warnings.warn(f"OutputWriter format {self.format!r} is not built (PythonFile and PythonCallback are); "
+                          f"nothing is written for it")
+        elif self.format == "PythonCallback" and not callable(self.callback):
+            raise ValueError("OutputWriter: format PythonCallback needs a callable 'callback'")
+
+    def prepare(self, time_step_no: int, current_time: float, call_count_increment: int = 1) -> Optional[str]:
+        """Counts one call; the numbered file name base when this call writes, else None."""
+        old = self.write_call_count
+        self.write_call_count += int(call_count_increment)
+        last = self.write_call_count - self.write_call_count % self.output_interval
+        if not ((old < last <= self.write_call_count) or call_count_increment == 0):
+            return None
+        name = self.filename
+        if time_step_no != -1:
+            no = self.output_file_no if self.file_numbering == "incremental" else self.write_call_count
+            name += f"_{no:07d}"
+        self.output_file_no += 1
+        return name
+
+    def write(self, name: str, dicts: Sequence[dict]) -> List[str]:
+        """Writes the fiber dicts (one per covered fiber, in order) under ``name``; the paths written."""
+        if self.format == "PythonCallback":
+            self.callback(list(dicts))
+            return []
+        if self.format != "PythonFile":
+            return []
+        d = os.path.dirname(name)
+        if d:
+            os.makedirs(d, exist_ok=True)
+        paths = []
+        for mesh, data in zip(self.mesh_names, dicts):
+            path = f"{name}.py" if len(dicts) == 1 else f"{name}_{mesh}.py"
+            if self.binary:
+                with open(path, "wb") as fh:
+                    pickle.dump(data, fh, 1)
+            else:
+                with open(path, "w") as fh:
+                    json.dump(data, fh)
+            paths.append(path)
+        return paths

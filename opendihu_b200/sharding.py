@@ -68,6 +68,10 @@ def subset(system: FiberSystem, fibers) -> FiberSystem:
         s.parameters = np.asarray(system.parameters)[:, nodes].copy()
     if system.states is not None:
         s.states = np.asarray(system.states)[:, nodes].copy()
+    if len(system.fiber_mesh_names) == system.n_fibers:
+        s.fiber_mesh_names = [system.fiber_mesh_names[int(f)] for f in fibers]
+    # output writers name fibers of the unsharded layout: a shard runs none
+    s.output_writers = ()
     return s
 
 

@@ -24,6 +24,7 @@ import numpy as np
 
 from . import _native as N
 from . import inputs
+from . import output
 
 SCHEMES = {"ImplicitEuler": 0, "CrankNicolson": 1}
 METHODS = {"split": 0, "fused": 1}
@@ -78,6 +79,11 @@ class FiberSystem:
     compute_state_information: bool = False
     # names of the fibers' meshes in the settings ("Meshes"), in fiber order (for their node positions)
     fiber_mesh_names: Sequence[str] = ()
+    # "OutputWriter" entries of the diffusion solvers: (settings dict, fibers it covers); run after each
+    # RepeatedCall piece of advanceTimeSpan (fast_monodomain_solver_compute.tpp:35-44)
+    output_writers: Sequence = ()
+    # "nAdditionalFieldVariables" of the diffusion solver: the output's additionalFieldVariable<k> fields
+    n_additional_field_variables: int = 0
 
     @property
     def n_fibers(self) -> int:
@@ -176,20 +182,27 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     meshes = config.get("Meshes", {})
     instances = fast["MultipleInstances"]["instances"]
     fibers: List[dict] = []
+    writers = []
     for inst in instances:
         _, strang = _first_key(inst, "StrangSplitting", "Strang")
         if strang is None:
             raise ValueError("settings: every instance needs a 'StrangSplitting' entry")
         t1 = strang["Term1"]["MultipleInstances"]["instances"]
         t2 = strang["Term2"]["MultipleInstances"]["instances"]
+        first = len(fibers)
         for a, b in zip(t1, t2):
             heun = a["Heun"]
             scheme, diff = _first_key(b, "ImplicitEuler", "CrankNicolson")
             if scheme is None:
                 raise ValueError("settings: Timestepping scheme of diffusion in FastMonodomainSolver must be either "
                                  "ImplicitEuler or CrankNicolson")
+            # a fiber's own diffusion writers
+            writers += [(w, [len(fibers)]) for w in (diff.get("OutputWriter") or [])]
             fibers.append({"strang": strang, "heun": heun, "cellml": heun["CellML"], "scheme": scheme,
                            "diff": diff, "fem": diff["FiniteElementMethod"]})
+        # the writers of the diffusion's MultipleInstances cover all its fibers
+        writers += [(w, list(range(first, len(fibers))))
+                    for w in (strang["Term2"]["MultipleInstances"].get("OutputWriter") or [])]
     if not fibers:
         raise ValueError("settings: no fibers")
     f0 = fibers[0]
@@ -303,6 +316,8 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     sys_.fiber_mesh_names = [fb["fem"].get("meshName", fb["cellml"].get("meshName")) for fb in fibers]
     sys_.compute_state_information = \
         int(f0["diff"].get("nAdditionalFieldVariables", 0)) > len(sys_.algebraics_for_transfer)
+    sys_.output_writers = writers
+    sys_.n_additional_field_variables = int(f0["diff"].get("nAdditionalFieldVariables", 0))
     sys_.method = b200.get("method", "split")
     sys_.precision = precision
     return sys_
@@ -385,6 +400,11 @@ class FastMonodomainSolver:
         self._start = system.start_time
         self._end = system.end_time
         self._ck = None
+        self._writers = None
+        # the reference's currentTime_ (end of the last RepeatedCall piece) and nTimeStepsSplitting_ (its
+        # split steps), which callOutputWriter hands to the writers
+        self._current_time = system.start_time
+        self._piece_steps = 0
         self.initialized = False
 
     @classmethod
@@ -517,9 +537,89 @@ class FastMonodomainSolver:
 
     def advanceTimeSpan(self, withOutputWritersEnabled: bool = True):
         """RepeatedCall over [startTime, endTime] (each repeated call is one setTimeSpan+advanceTimeSpan of
-        the reference solver)."""
+        the reference solver).  With output writers in the settings (and enabled) they run after every
+        RepeatedCall piece, as the reference's advanceTimeSpan calls them (fast_monodomain_solver_compute.tpp:
+        35-44): the advance stops only after the pieces whose call writes a file, the steps stay those of
+        one advance over the span."""
         self.initialize()
-        self._call(N.lib().fdm_advance, self._start, self._end)
+        writers = self._output_writers() if withOutputWritersEnabled else []
+        L = N.lib()
+        n = C.c_int64()
+        self._call(L.fdm_repeated_call_plan, self._start, self._end, C.byref(n), None)
+        steps = np.zeros(max(n.value, 1), np.int32)
+        if self.system.output_writers:   # the split steps per piece, for the writers' call counts
+            self._call(L.fdm_repeated_call_plan, self._start, self._end, C.byref(n), N.ptr(steps, C.c_int))
+        if not writers:
+            self._call(L.fdm_advance, self._start, self._end)
+            self._current_time = self._piece_end(n.value - 1, n.value)
+            self._piece_steps = int(steps[n.value - 1])
+            return
+        done = 0
+        for k in range(n.value):
+            t = self._piece_end(k, n.value)
+            due = [(w, name) for w in writers for name in [w.prepare(0, t, int(steps[k]))] if name]
+            self._piece_steps = int(steps[k])
+            self._current_time = t
+            if due:
+                self._call(L.fdm_advance_pieces, self._start, self._end, done, k + 1)
+                done = k + 1
+                self._write_output(due)
+        if done < n.value:
+            self._call(L.fdm_advance_pieces, self._start, self._end, done, n.value)
+
+    def callOutputWriter(self, timeStepNo: int, currentTime: float, callCountIncrement: int = 1):
+        """The reference's callOutputWriter (fast_monodomain_solver_base.tpp:7-24): when timeStepNo is a
+        multiple of callCountIncrement, the diffusion writers are called as after a RepeatedCall piece, with
+        the end time and split steps of the last piece (0 steps before the first advance: the call then
+        counts as the initial-values call, which always writes).  currentTime is not used, as in the
+        reference."""
+        self.initialize()
+        if int(timeStepNo) % int(callCountIncrement) != 0:
+            return
+        due = [(w, name) for w in self._output_writers()
+               for name in [w.prepare(0, self._current_time, self._piece_steps)] if name]
+        if due:
+            self._write_output(due)
+
+    def _piece_end(self, k: int, n: int) -> float:
+        """End of RepeatedCall piece k of n over [startTime, endTime] (the Strang span's endTime, the
+        reference's currentTime_): start + k/n*span + span/n, as repeated_call.tpp:59-70 forms it."""
+        span = self._end - self._start
+        t = self._start if k == 0 else self._start + k / n * span
+        return t + span / n
+
+    def _output_writers(self):
+        if self._writers is None:
+            names = list(self.system.fiber_mesh_names)
+            self._writers = [output.OutputWriter(w, fibers, [names[f] if f < len(names) and names[f] else
+                                                           f"MeshFiber_{f}" for f in fibers])
+                             for w, fibers in self.system.output_writers]
+        return self._writers
+
+    def _write_output(self, due):
+        """The diffusion data of the fibers each due writer covers: geometry (cumulative element lengths along
+        x), "solution" (Vm) and additionalFieldVariable<k> (algebraicsForTransfer, then the
+        computeStateInformation slot; fast_monodomain_solver_communication.tpp:437-488)."""
+        s = self.system
+        vm = self.vm()
+        extra = []
+        if len(s.algebraics_for_transfer):
+            extra += list(self.algebraics())
+        if s.compute_state_information:
+            extra.append(self.compute_state_information())
+        n_add = max(int(s.n_additional_field_variables), len(extra))
+        off = np.asarray(s.fiber_offsets, np.int64)
+        elem = np.asarray(s.element_lengths)
+        for w, name in due:
+            dicts = []
+            for f in w.fibers:
+                a, b = int(off[f]), int(off[f + 1])
+                x = np.concatenate([[0.0], np.cumsum(elem[a - f:b - f - 1])])
+                geom = np.stack([x, np.zeros_like(x), np.zeros_like(x)], axis=1)
+                add = {f"additionalFieldVariable{k}": (extra[k][a:b] if k < len(extra) else np.zeros(b - a))
+                       for k in range(n_add)}
+                dicts.append(output.fiber_dict({"0": vm[a:b]}, geom, 0, self._current_time, "solution", add))
+            w.write(name, dicts)
 
     def advance_async(self):
         """advanceTimeSpan without waiting for the device (``wait`` completes it: timing, the NaN check)."""

@@ -2,6 +2,9 @@
 // drive its FastMonodomainSolver: settings in, setTimeSpan/advanceTimeSpan twice with a checkpoint between,
 // the checkpoint replayed, the states and the transferred algebraics written out.
 //   host_class_main <settings file> <output file> <intermediate time>
+// With a fifth argument it instead advances [startTime, endTime] once with an output writer of that
+// outputInterval whose callback writes one line per call (numbered name, current time, Vm sum) to the
+// output file, then calls callOutputWriter(0, 0) once more.
 // Exit status: 0 done, 2 fdm::Error (message on stderr), 3 the replay after the checkpoint differs.
 #include <cstdio>
 #include <cstdlib>
@@ -11,12 +14,32 @@
 
 int main(int argc, char** argv)
 {
-  if (argc != 4) {
-    std::fprintf(stderr, "usage: %s settings output t_mid\n", argv[0]);
+  if (argc != 4 && argc != 5) {
+    std::fprintf(stderr, "usage: %s settings output t_mid [output_interval]\n", argv[0]);
     return 1;
   }
   try {
     fdm::FiberSettings s = fdm::FiberSettings::load(argv[1]);
+    if (argc == 5) {
+      fdm::FastMonodomainSolver slv(s);
+      std::FILE* f = std::fopen(argv[2], "w");
+      if (!f)
+        return 1;
+      fdm::OutputWriter w;
+      w.outputInterval = std::atoi(argv[4]);
+      w.filename = "out/fiber";
+      w.write = [&](const std::string& name, double t) {
+        double sum = 0.0;
+        for (double v : slv.data().vm)
+          sum += v;
+        std::fprintf(f, "%s %.17g %.17g\n", name.c_str(), t, sum);
+      };
+      slv.addOutputWriter(w);
+      slv.advanceTimeSpan();
+      slv.callOutputWriter(0, 0.0);
+      std::fclose(f);
+      return 0;
+    }
     const double t_mid = std::atof(argv[3]);
     fdm::FastMonodomainSolver slv(s);
     slv.initialize();

@@ -65,3 +65,30 @@ def test_cpp_host_class_equals_python_operator(tmp_path, method, precision):
     if precision == "fp64":
         ref, _, _, _ = H.run_oracle(s.copy())
         assert np.max(np.abs(st[0] - ref[0])) <= GP.VM_TOL_FP64
+
+
+@pytest.mark.gpu
+def test_cpp_output_writer_equals_python_writer(tmp_path):
+    # the C++ class's writer fires after the same RepeatedCall pieces, with the same names, times and Vm as
+    # the Python host class's PythonCallback writer of the same outputInterval
+    exe = _build(tmp_path)
+    s = _system()
+    cfg = str(tmp_path / "settings.txt")
+    S.write_host_settings(s, cfg, method="split", precision="fp64")
+    out = str(tmp_path / "writes.txt")
+    r = subprocess.run([exe, cfg, out, "0", "7"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = [ln.split() for ln in open(out).read().splitlines()]
+    got = []
+    s2 = s.copy()
+    s2.output_writers = [({"format": "PythonCallback", "outputInterval": 7, "filename": "out/fiber",
+                           "callback": got.append}, list(range(s.n_fibers)))]
+    with S.FastMonodomainSolver(s2, method="split", precision="fp64") as slv:
+        slv.advanceTimeSpan()
+        slv.callOutputWriter(0, 0.0)
+    assert len(lines) == len(got) >= 2
+    for (name, t, vm_sum), dicts in zip(lines, got):
+        assert float(t) == dicts[0]["currentTime"]
+        assert float(vm_sum) == pytest.approx(sum(float(np.sum(d["data"][1]["components"][0]["values"]))
+                                                  for d in dicts), rel=1e-13)
+    assert lines[0][0] == "out/fiber_0000000"
