@@ -184,6 +184,14 @@ int fdm_repeated_call_plan(fdm_solver *s, double t_start, double t_end, int64_t 
  * give the same steps, bit for bit, as one fdm_advance over the span, with the host free between them
  * (output at the reference's times) */
 int fdm_advance_pieces(fdm_solver *s, double t_start, double t_end, int64_t k_begin, int64_t k_end);
+/* Stimulation log (the reference's StimulationLogging, core/src/control/diagnostic_tool/stimulation_logging.cpp,
+ * fed at fast_monodomain_solver_compute.tpp:603-607): from now on every substep at which a fiber's stimulation
+ * begins (its decision stimulates, its previous decision did not) is recorded as (time, fiber), up to capacity
+ * entries.  A larger capacity keeps the entries recorded so far; 0 turns the log off and drops them. */
+int fdm_set_stimulation_log(fdm_solver *s, int64_t capacity);
+/* *n_total = entries recorded (including those past the capacity); times/fibers (may be null) receive the
+ * first min(n_total, capacity), in the order they were recorded (fibers of one window in no fixed order) */
+int fdm_get_stimulation_log(fdm_solver *s, int64_t *n_total, double *times, int *fibers);
 /* number of split steps done by all advances so far */
 int64_t fdm_split_steps(const fdm_solver *s);
 /* summed device time and count of the main kernel launches (config.profile = 1), and of all GPU work

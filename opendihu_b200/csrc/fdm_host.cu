@@ -145,6 +145,12 @@ struct fdm_solver {
     bool ck_valid = false;
   } eq;
   DevBuf<uint8_t> firing, evaluated_d, hbs;
+  DevBuf<uint8_t> cur_stim;        // per fiber: did its last stimulation decision stimulate
+  // stimulation log: (time, fiber) of the stimulation begins, log_cap entries, log_n counts all
+  DevBuf<double> log_t;
+  DevBuf<int> log_f;
+  DevBuf<unsigned long long> log_n;
+  int64_t log_cap = 0;
   DevBuf<int> mu;
   DevBuf<double> freq, repeat, begin, jitter, last_check, cur_jitter;
   DevBuf<int> jitter_idx;
@@ -162,7 +168,7 @@ struct fdm_solver {
   DevBuf<double> ck_vm, ck_last, ck_jit;
   DevBuf<unsigned char> ck_states, ck_states_lo;
   DevBuf<int> ck_jidx;
-  DevBuf<uint8_t> ck_hbs;
+  DevBuf<uint8_t> ck_hbs, ck_cur;
   bool ck_valid = false;
   Tss ck_strang, ck_heun, ck_diff;
   bool ck_tss_init = false;
@@ -495,6 +501,12 @@ extern "C" int fdm_destroy(fdm_solver* s)
   s->evaluated_d.release();
   s->hbs.release();
   s->ck_hbs.release();
+  s->cur_stim.release();
+  s->ck_cur.release();
+  s->log_t.release();
+  s->log_f.release();
+  s->log_n.release();
+  s->log_cap = 0;
   s->flags.release();
   s->steps_d.release();
   s->adj.release();
@@ -1356,6 +1368,7 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
   FDM_CUDA(s->cur_jitter.alloc(std::max(nf, 1)));
   FDM_CUDA(s->jitter_idx.alloc(std::max(nf, 1)));
   FDM_CUDA(s->hbs.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->cur_stim.alloc(std::max(nf, 1)));
   FDM_CUDA(s->evaluated_d.alloc(std::max(nf, 1)));
   FDM_CUDA(cudaMemcpyAsync(s->firing.p, firing_events, (size_t)rows * cols, cudaMemcpyHostToDevice, s->stream));
   if (nf > 0) {
@@ -1380,6 +1393,7 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
     FDM_CUDA(cudaMemcpyAsync(s->cur_jitter.p, cj.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, ji.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->hbs.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->cur_stim.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaStreamSynchronize(s->stream));
   }
   s->clamp_first.assign(nf, -1);
@@ -1682,6 +1696,15 @@ static int prepare_window(fdm_solver* s, const SplitStep* host_steps, int n_step
   sa.jitter_index = s->jitter_idx.p;
   sa.has_been_stimulated = s->hbs.p;
   sa.flags = flags_buf ? flags_buf : s->flags.p;
+  if (!flags_buf) { // an advance (the adjoint's replay windows bring their own flags and log nothing)
+    sa.currently = s->cur_stim.p;
+    if (s->log_cap > 0) {
+      sa.log_time = s->log_t.p;
+      sa.log_fiber = s->log_f.p;
+      sa.log_count = s->log_n.p;
+      sa.log_capacity = s->log_cap;
+    }
+  }
   sa.words_per_fiber = words;
   sa.nsub_stride = nsub;
   sa.n_fibers = s->n_fibers;
@@ -2132,6 +2155,74 @@ extern "C" int fdm_advance_pieces(fdm_solver* s, double t_start, double t_end, i
 
 extern "C" int64_t fdm_split_steps(const fdm_solver* s) { return s ? s->split_no : 0; }
 
+extern "C" int fdm_set_stimulation_log(fdm_solver* s, int64_t capacity)
+{
+  if (!s || capacity < 0)
+    return fail(s, FDM_ERR_ARG, "fdm_set_stimulation_log: bad argument");
+  FDM_BIND(s);
+  {
+    const int rw = fdm_wait(s);
+    if (rw)
+      return rw;
+  }
+  if (capacity == 0) {
+    s->log_t.release();
+    s->log_f.release();
+    s->log_n.release();
+    s->log_cap = 0;
+    return FDM_OK;
+  }
+  if (s->log_cap == 0) {
+    FDM_CUDA(s->log_n.alloc(1));
+    FDM_CUDA(cudaMemsetAsync(s->log_n.p, 0, sizeof(unsigned long long), s->stream));
+  }
+  if (capacity > s->log_cap) { // grow, keeping the entries recorded so far
+    DevBuf<double> t;
+    DevBuf<int> f;
+    FDM_CUDA(t.alloc((size_t)capacity));
+    FDM_CUDA(f.alloc((size_t)capacity));
+    if (s->log_cap > 0) {
+      FDM_CUDA(cudaMemcpyAsync(t.p, s->log_t.p, sizeof(double) * s->log_cap, cudaMemcpyDeviceToDevice, s->stream));
+      FDM_CUDA(cudaMemcpyAsync(f.p, s->log_f.p, sizeof(int) * s->log_cap, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+    s->log_t.release();
+    s->log_f.release();
+    s->log_t = t;
+    s->log_f = f;
+    t.p = nullptr;
+    f.p = nullptr;
+    s->log_cap = capacity;
+  }
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_stimulation_log(fdm_solver* s, int64_t* n_total, double* times, int* fibers)
+{
+  if (!s || !n_total)
+    return fail(s, FDM_ERR_ARG, "fdm_get_stimulation_log: bad argument");
+  FDM_BIND(s);
+  {
+    const int rw = fdm_wait(s);
+    if (rw)
+      return rw;
+  }
+  *n_total = 0;
+  if (s->log_cap == 0)
+    return FDM_OK;
+  unsigned long long n = 0;
+  FDM_CUDA(cudaMemcpyAsync(&n, s->log_n.p, sizeof(n), cudaMemcpyDeviceToHost, s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  *n_total = (int64_t)n;
+  const size_t k = (size_t)std::min<unsigned long long>(n, (unsigned long long)s->log_cap);
+  if (k > 0 && times)
+    FDM_CUDA(cudaMemcpyAsync(times, s->log_t.p, sizeof(double) * k, cudaMemcpyDeviceToHost, s->stream));
+  if (k > 0 && fibers)
+    FDM_CUDA(cudaMemcpyAsync(fibers, s->log_f.p, sizeof(int) * k, cudaMemcpyDeviceToHost, s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  return FDM_OK;
+}
+
 extern "C" int fdm_get_timing(const fdm_solver* s, double* main_ms, int64_t* main_launches, double* adv_ms,
                               int64_t* launches)
 {
@@ -2174,6 +2265,7 @@ extern "C" int fdm_checkpoint_save(fdm_solver* s)
   FDM_CUDA(s->ck_jit.alloc(std::max(nf, 1)));
   FDM_CUDA(s->ck_jidx.alloc(std::max(nf, 1)));
   FDM_CUDA(s->ck_hbs.alloc(std::max(nf, 1)));
+  FDM_CUDA(s->ck_cur.alloc(std::max(nf, 1)));
   if (N > 0) {
     FDM_CUDA(cudaMemcpyAsync(s->ck_vm.p, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->stream));
     if (NS > 1)
@@ -2190,6 +2282,7 @@ extern "C" int fdm_checkpoint_save(fdm_solver* s)
     FDM_CUDA(cudaMemcpyAsync(s->ck_jit.p, s->cur_jitter.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->ck_jidx.p, s->jitter_idx.p, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->ck_hbs.p, s->hbs.p, nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->ck_cur.p, s->cur_stim.p, nf, cudaMemcpyDeviceToDevice, s->stream));
   }
   if (s->eq.on) {
     auto& E = s->eq;
@@ -2241,6 +2334,7 @@ extern "C" int fdm_checkpoint_restore(fdm_solver* s)
     FDM_CUDA(cudaMemcpyAsync(s->cur_jitter.p, s->ck_jit.p, sizeof(double) * nf, cudaMemcpyDeviceToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, s->ck_jidx.p, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->hbs.p, s->ck_hbs.p, nf, cudaMemcpyDeviceToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->cur_stim.p, s->ck_cur.p, nf, cudaMemcpyDeviceToDevice, s->stream));
   }
   if (s->eq.on && s->eq.ck_valid) {
     auto& E = s->eq;
@@ -2981,6 +3075,7 @@ extern "C" int fdm_rewind(fdm_solver* s)
     FDM_CUDA(cudaMemcpyAsync(s->cur_jitter.p, cj.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->jitter_idx.p, ji.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaMemcpyAsync(s->hbs.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
+    FDM_CUDA(cudaMemcpyAsync(s->cur_stim.p, h0.data(), nf, cudaMemcpyHostToDevice, s->stream));
     FDM_CUDA(cudaStreamSynchronize(s->stream));
   }
   if (s->eq.on) {

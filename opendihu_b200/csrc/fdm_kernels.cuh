@@ -66,6 +66,11 @@ struct StimArgs {
   int gate_stride;                // window, 0 if the fiber's flag was set before the half step, 1 + the
                                   // substep that sets it, 255 if it stays unset:
                                   // [fiber * gate_stride + step*2 + half]
+  uint8_t* currently;             // stimulation log (or null): per fiber, did its last decision stimulate
+  double* log_time;               // (time, fiber) of every stimulation begin, log_capacity entries;
+  int* log_fiber;                 // log_count counts all of them (null: no entries are written)
+  unsigned long long* log_count;
+  long long log_capacity;
 };
 
 // onlyComputeIfHasBeenStimulated: the first substep of half step hs that a node with gate code `code`
@@ -130,6 +135,7 @@ __global__ void stimulation_schedule_kernel(StimArgs a, const SplitStep* __restr
   double last = a.last_check_time[f], jit = a.current_jitter[f];
   int jidx = a.jitter_index[f];
   uint8_t hbs = a.has_been_stimulated[f];
+  uint8_t cur = a.currently ? a.currently[f] : 0;
   for (int j = 0; j < n_steps; j++) {
     const SplitStep s = steps[j];
     for (int h = 0; h < 2; h++) {
@@ -140,6 +146,15 @@ __global__ void stimulation_schedule_kernel(StimArgs a, const SplitStep* __restr
       for (int k = 0; k < s.n0; k++) {
         const double t = xadd(t0, xmul((double)k, s.dt0));
         const bool st = stimulation_machine(a, f, t, last, jit, jidx);
+        // StimulationLogging::logStimulationBegin at the first stimulating decision (compute.tpp:603-607)
+        if (st && !cur && a.log_count) {
+          const unsigned long long idx = atomicAdd(a.log_count, 1ull);
+          if (idx < (unsigned long long)a.log_capacity) {
+            a.log_time[idx] = t;
+            a.log_fiber[idx] = f;
+          }
+        }
+        cur = st ? 1 : 0;
         if (st) {
           if (first == 255)
             first = k + 1;
@@ -164,6 +179,8 @@ __global__ void stimulation_schedule_kernel(StimArgs a, const SplitStep* __restr
   a.current_jitter[f] = jit;
   a.jitter_index[f] = jidx;
   a.has_been_stimulated[f] = hbs;
+  if (a.currently)
+    a.currently[f] = cur;
 }
 
 #endif // FDM_COMMON_KERNELS_TU

@@ -156,3 +156,30 @@ class OutputWriter:
                     json.dump(data, fh)
             paths.append(path)
         return paths
+
+
+def write_stimulation_log(filename: str, times, fibers, motor_units) -> None:
+    """The stimulation log file of the reference's StimulationLogging::writeLogFile
+    (core/src/control/diagnostic_tool/stimulation_logging.cpp:119-165): entries sorted by motor unit, then fiber,
+    then time; a header line, then one line ``<motor unit>;<fiber>;<t1>;<t2>;...;`` per (motor unit, fiber), the
+    times as a C++ stream writes a double (6 significant digits), no newline after the last line.  Nothing is
+    written for an empty log, as in the reference."""
+    t = np.asarray(times, np.float64)
+    f = np.asarray(fibers, np.int64)
+    m = np.asarray(motor_units, np.int64)
+    if len(t) == 0:
+        return
+    order = np.lexsort((t, f, m))
+    d = os.path.dirname(filename)
+    if d:
+        os.makedirs(d, exist_ok=True)
+    lines = []
+    cur = None
+    for i in order:
+        key = (int(m[i]), int(f[i]))
+        if key != cur:
+            cur = key
+            lines.append(f"{key[0]};{key[1]};")
+        lines[-1] += f"{float(t[i]):g};"
+    with open(filename, "w") as fh:
+        fh.write("# motor unit no; fiber no; stimulation times in ms\n" + "\n".join(lines))

@@ -84,6 +84,10 @@ class FiberSystem:
     output_writers: Sequence = ()
     # "nAdditionalFieldVariables" of the diffusion solver: the output's additionalFieldVariable<k> fields
     n_additional_field_variables: int = 0
+    # global fiber numbers ("additionalArgument" of the settings; default the fiber index), for the log
+    fiber_numbers: Sequence[int] = ()
+    # "stimulationLogFilename" of the CellML settings: the stimulation log written when the solver closes
+    stimulation_log_filename: str = ""
 
     @property
     def n_fibers(self) -> int:
@@ -270,10 +274,12 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     rep = np.zeros(nf)
     beg = np.zeros(nf)
     jit_lists = []
+    fiber_numbers = []
     for fi, fb in enumerate(fibers):
         c = fb["cellml"]
         fiber_no_global = int(c.get("additionalArgument", fi)) if isinstance(c.get("additionalArgument", fi), (int, np.integer)) else fi
         mu_no[fi] = mus[fiber_no_global % len(mus)]
+        fiber_numbers.append(fiber_no_global)
         freq[fi] = float(c.get("setSpecificStatesCallFrequency", 0.0) or 0.0)
         rep[fi] = float(c.get("setSpecificStatesRepeatAfterFirstCall", 0.0) or 0.0)
         beg[fi] = float(c.get("setSpecificStatesCallEnableBegin", 0.0) or 0.0)
@@ -317,6 +323,8 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     sys_.compute_state_information = \
         int(f0["diff"].get("nAdditionalFieldVariables", 0)) > len(sys_.algebraics_for_transfer)
     sys_.output_writers = writers
+    sys_.fiber_numbers = fiber_numbers
+    sys_.stimulation_log_filename = str(cellml.get("stimulationLogFilename") or "")
     sys_.n_additional_field_variables = int(f0["diff"].get("nAdditionalFieldVariables", 0))
     sys_.method = b200.get("method", "split")
     sys_.precision = precision
@@ -401,6 +409,7 @@ class FastMonodomainSolver:
         self._end = system.end_time
         self._ck = None
         self._writers = None
+        self._log_on = False
         # the reference's currentTime_ (end of the last RepeatedCall piece) and nTimeStepsSplitting_ (its
         # split steps), which callOutputWriter hands to the writers
         self._current_time = system.start_time
@@ -481,6 +490,9 @@ class FastMonodomainSolver:
             if len(self.trace_nodes):
                 self._call(L.fdm_set_trace, len(self.trace_nodes), N.ptr(self.trace_nodes, C.c_int64),
                            self.trace_capacity)
+            if s.stimulation_log_filename:
+                self._log_on = True
+                self._call(L.fdm_set_stimulation_log, self._log_bound(s.end_time - s.start_time))
         except Exception:
             self.close()
             raise
@@ -507,8 +519,13 @@ class FastMonodomainSolver:
 
     def close(self):
         if self._h is not None:
-            N.lib().fdm_destroy(self._h)
-            self._h = None
+            try:
+                if self.system.stimulation_log_filename and self._log_on:
+                    # the reference writes its log at the end of the run (dihu_context.cpp:85-86)
+                    self.writeStimulationLog()
+            finally:
+                N.lib().fdm_destroy(self._h)
+                self._h = None
         self.initialized = False
 
     def __del__(self):
@@ -544,6 +561,8 @@ class FastMonodomainSolver:
         self.initialize()
         writers = self._output_writers() if withOutputWritersEnabled else []
         L = N.lib()
+        if self._log_on:
+            self._grow_stimulation_log(self._end - self._start)
         n = C.c_int64()
         self._call(L.fdm_repeated_call_plan, self._start, self._end, C.byref(n), None)
         steps = np.zeros(max(n.value, 1), np.int32)
@@ -580,6 +599,55 @@ class FastMonodomainSolver:
                for name in [w.prepare(0, self._current_time, self._piece_steps)] if name]
         if due:
             self._write_output(due)
+
+    # -- stimulation log ----------------------------------------------------------------------------
+    def enable_stimulation_log(self, capacity: int = 0):
+        """Records every stimulation begin from now on (the reference's StimulationLogging; see
+        fdm_set_stimulation_log); the capacity grows before each advance to what its span can need."""
+        self.initialize()
+        self._log_on = True
+        self._call(N.lib().fdm_set_stimulation_log,
+                   max(int(capacity), self._log_bound(self.system.end_time - self.system.start_time)))
+
+    def _log_bound(self, span: float) -> int:
+        """Stimulation begins a span can hold: a fiber's machine checks at most once per 1/(f (1 + jitter))."""
+        s = self.system
+        f = np.asarray(s.call_frequency, np.float64)
+        jit = np.asarray(s.jitter, np.float64) if s.jitter is not None and np.size(s.jitter) else np.zeros((len(f), 1))
+        rate = f * (1.0 + np.max(np.abs(jit.reshape(len(f), -1)), axis=1, initial=0.0)) if len(f) else f
+        return int(np.sum(np.ceil(max(span, 0.0) * rate) + 2)) + 16
+
+    def _grow_stimulation_log(self, span: float):
+        n = C.c_int64()
+        self._call(N.lib().fdm_get_stimulation_log, C.byref(n), None, None)
+        self._call(N.lib().fdm_set_stimulation_log, n.value + self._log_bound(span))
+
+    def stimulation_log(self) -> Dict[str, np.ndarray]:
+        """The recorded stimulation begins, in time order: "time", "fiber" (global fiber numbers), "motorUnit"."""
+        self.initialize()
+        n = C.c_int64()
+        self._call(N.lib().fdm_get_stimulation_log, C.byref(n), None, None)
+        t = np.zeros(max(n.value, 1))
+        f = np.zeros(max(n.value, 1), np.int32)
+        self._call(N.lib().fdm_get_stimulation_log, C.byref(n), N.ptr(t, C.c_double), N.ptr(f, C.c_int))
+        k = min(n.value, len(t))
+        t, f = t[:k], f[:k]
+        order = np.lexsort((f, t))
+        t, f = t[order], f[order]
+        nums = np.asarray(self.system.fiber_numbers if len(self.system.fiber_numbers) == self.system.n_fibers
+                          else np.arange(self.system.n_fibers), np.int64)
+        return {"time": t, "fiber": nums[f] if k else f.astype(np.int64),
+                "motorUnit": np.asarray(self.system.motor_unit_no, np.int64)[f] if k else f.astype(np.int64)}
+
+    def writeStimulationLog(self, filename: Optional[str] = None) -> str:
+        """Writes the log in the reference's format (output.write_stimulation_log); the file name defaults to
+        the settings' stimulationLogFilename."""
+        name = filename or self.system.stimulation_log_filename
+        if not name:
+            raise ValueError("writeStimulationLog: no file name (settings have no stimulationLogFilename)")
+        d = self.stimulation_log()
+        output.write_stimulation_log(name, d["time"], d["fiber"], d["motorUnit"])
+        return name
 
     def _piece_end(self, k: int, n: int) -> float:
         """End of RepeatedCall piece k of n over [startTime, endTime] (the Strang span's endTime, the

@@ -187,6 +187,15 @@ typedef struct {
   uint8_t *eq_status;
   int *eq_counter;
   double *pad_states;
+  /* stimulation log (StimulationLogging::logStimulationBegin, called at compute.tpp:603-607): the time and
+   * fiber of every substep whose decision stimulates while the fiber's previous decision did not.
+   * currently_stimulating per fiber is in/out (NULL: all 0); log_times/log_fibers hold log_capacity entries,
+   * *log_count counts all (NULL: no log). */
+  int *currently_stimulating;
+  double *log_times;
+  int *log_fibers;
+  int64_t log_capacity;
+  int64_t *log_count;
 } oracle_problem;
 
 enum { EQ_INACTIVE = 0, EQ_NEIGHBOR_IS_ACTIVE = 1, EQ_ACTIVE = 2 };
@@ -236,6 +245,15 @@ static int stimulation_machine(const oracle_problem *p, int f, oracle_fiber_stat
   const int stimulate = check && p->firing_events[(int64_t)row * p->firing_cols + col];
   if (stimulate)
     st->has_been_stimulated = 1;
+  if (stimulate && !st->currently_stimulating && p->log_count) {
+    int64_t i;
+#pragma omp atomic capture
+    i = (*p->log_count)++;
+    if (i < p->log_capacity) {
+      p->log_times[i] = t;
+      p->log_fibers[i] = f;
+    }
+  }
   st->currently_stimulating = stimulate;
   return stimulate;
 }
@@ -678,6 +696,7 @@ int64_t oracle_run(const oracle_problem *p, double *states, double *last_check_t
     fs[f].current_jitter = current_jitter[f];
     fs[f].jitter_index = jitter_index[f];
     fs[f].has_been_stimulated = p->has_been_stimulated ? p->has_been_stimulated[f] : 0;
+    fs[f].currently_stimulating = p->currently_stimulating ? p->currently_stimulating[f] : 0;
   }
 
   /* RepeatedCall (repeated_call.tpp:43-75) */
@@ -765,6 +784,8 @@ int64_t oracle_run(const oracle_problem *p, double *states, double *last_check_t
     jitter_index[f] = fs[f].jitter_index;
     if (p->has_been_stimulated)
       p->has_been_stimulated[f] = fs[f].has_been_stimulated;
+    if (p->currently_stimulating)
+      p->currently_stimulating[f] = fs[f].currently_stimulating;
   }
   if (p->equilibrium) {
     for (int rk = 0; rk < p->n_ranks; rk++) {

@@ -56,6 +56,8 @@ class Problem(C.Structure):
         ("only_if_stimulated", C.c_int), ("has_been_stimulated", C.POINTER(C.c_int)),
         ("equilibrium", C.c_int), ("eq_status", C.POINTER(C.c_uint8)), ("eq_counter", C.POINTER(C.c_int)),
         ("pad_states", C.POINTER(C.c_double)),
+        ("currently_stimulating", C.POINTER(C.c_int)), ("log_times", C.POINTER(C.c_double)),
+        ("log_fibers", C.POINTER(C.c_int)), ("log_capacity", C.c_int64), ("log_count", C.POINTER(C.c_int64)),
     ]
 
 
@@ -187,6 +189,17 @@ class OracleRun:
         p.pad_states = _p(self.pad_states, C.c_double)
         self.has_been_stimulated = np.zeros(max(nf, 1), np.int32)
         p.has_been_stimulated = _p(self.has_been_stimulated, C.c_int)
+        # stimulation log (stimulation_log() returns it), kept across runs
+        self.currently_stimulating = np.zeros(max(nf, 1), np.int32)
+        p.currently_stimulating = _p(self.currently_stimulating, C.c_int)
+        cap = int(spec.get("log_capacity", 0))
+        self.log_times = np.zeros(max(cap, 1))
+        self.log_fibers = np.zeros(max(cap, 1), np.int32)
+        self.log_count = np.zeros(1, np.int64)
+        p.log_times = _p(self.log_times, C.c_double)
+        p.log_fibers = _p(self.log_fibers, C.c_int)
+        p.log_capacity = cap
+        p.log_count = _p(self.log_count, C.c_int64) if cap > 0 else None
         self.p = p
         self.last_check_time = np.zeros(nf)
         self.current_jitter = np.zeros(nf)
@@ -215,6 +228,13 @@ class OracleRun:
         if n < 0:
             raise RuntimeError("oracle_run failed")
         return int(n)
+
+    def stimulation_log(self):
+        """(times, fibers) of the logged stimulation begins, in the order they were recorded (with several
+        threads not in time order), and the number of entries that did not fit."""
+        n = int(self.log_count[0])
+        k = min(n, int(self.p.log_capacity))
+        return self.log_times[:k].copy(), self.log_fibers[:k].copy(), n - k
 
     def vc_clamp_nodes(self):
         nf = self.p.n_fibers

@@ -1,0 +1,154 @@
+"""Host logic of the Python host class without a device: the C ABI is replaced by a recording fake, so the
+order and arguments of the library calls that advanceTimeSpan, the output writers, callOutputWriter and the
+stimulation log make can be checked on CPU."""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import helpers as H
+from opendihu_b200 import _native as N
+from opendihu_b200 import output
+from opendihu_b200 import solver as S
+
+
+class FakeLib:
+    """Every fdm_* call succeeds and is recorded; the RepeatedCall plan follows the library's step-count rule
+    (one split step per piece here); Vm counts the pieces advanced so far."""
+
+    def __init__(self, n_nodes, dt_repeated_call):
+        self.calls = []
+        self.n_nodes = n_nodes
+        self.dt_rc = dt_repeated_call
+        self.pieces_done = 0
+        self.log_t = np.zeros(0)
+        self.log_f = np.zeros(0, np.int32)
+
+    def __getattr__(self, name):
+        def call(*args):
+            self.calls.append((name,) + args[1:])
+            return 0
+        return call
+
+    def fdm_create(self, cfg, h):
+        h._obj.value = 1234
+        return 0
+
+    def fdm_last_error(self, h):
+        return b"fake"
+
+    def _n(self, t0, t1):
+        return max(1, math.ceil((t1 - t0) / self.dt_rc - 0.1))
+
+    def fdm_repeated_call_plan(self, h, t0, t1, n, steps):
+        n._obj.value = self._n(t0, t1)
+        if steps:
+            np.ctypeslib.as_array(steps, (n._obj.value,))[:] = 1
+        return 0
+
+    def fdm_advance(self, h, t0, t1):
+        self.calls.append(("fdm_advance", t0, t1))
+        self.pieces_done += self._n(t0, t1)
+        return 0
+
+    def fdm_advance_pieces(self, h, t0, t1, k0, k1):
+        self.calls.append(("fdm_advance_pieces", k0, k1))
+        self.pieces_done += k1 - k0
+        return 0
+
+    def fdm_get_vm(self, h, out):
+        np.ctypeslib.as_array(out, (self.n_nodes,))[:] = self.pieces_done
+        return 0
+
+    def fdm_get_stimulation_log(self, h, n, t, f):
+        n._obj.value = len(self.log_t)
+        if t:
+            np.ctypeslib.as_array(t, (len(self.log_t),))[:] = self.log_t
+        if f:
+            np.ctypeslib.as_array(f, (len(self.log_f),))[:] = self.log_f
+        return 0
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    holder = {}
+
+    def install(system):
+        lib = FakeLib(system.n_nodes, system.dt_repeated_call)
+        monkeypatch.setattr(N, "lib", lambda: lib)
+        holder["lib"] = lib
+        return lib
+    return install
+
+
+def _system():
+    return H.complete(H.c1_system(n_fibers=2, n_nodes=11, end_time=0.01))
+
+
+def test_writers_split_the_advance_at_the_writing_pieces(fake):
+    s = _system()
+    a, b = [], []
+    s.output_writers = [({"format": "PythonCallback", "callback": a.append, "outputInterval": 3}, [1]),
+                        ({"format": "PythonCallback", "callback": b.append, "outputInterval": 4}, [0, 1])]
+    lib = fake(s)
+    slv = S.FastMonodomainSolver(s)
+    slv.advanceTimeSpan()
+    # 10 pieces of one split step: writer a after pieces 3, 6, 9, writer b after 4 and 8
+    adv = [c[1:] for c in lib.calls if c[0] == "fdm_advance_pieces"]
+    assert adv == [(0, 3), (3, 4), (4, 6), (6, 8), (8, 9), (9, 10)]
+    assert [len(x) for x in a] == [1, 1, 1] and [len(x) for x in b] == [2, 2]
+    np.testing.assert_allclose([x[0]["currentTime"] for x in a], [0.003, 0.006, 0.009], rtol=1e-12)
+    # each dict holds the Vm after its piece (the fake's Vm counts the pieces advanced)
+    assert [x[0]["data"][1]["components"][0]["values"][0] for x in a] == [3.0, 6.0, 9.0]
+    assert [x[1]["data"][1]["components"][0]["values"][0] for x in b] == [4.0, 8.0]
+    # writers off: one advance over the span
+    lib.calls.clear()
+    slv.setTimeSpan(0.01, 0.02)
+    slv.advanceTimeSpan(withOutputWritersEnabled=False)
+    assert [c for c in lib.calls if c[0].startswith("fdm_advance")] == [("fdm_advance", 0.01, 0.02)]
+    assert len(a) == 3
+    # callOutputWriter continues the counts with the last piece's single step
+    for k in range(3):
+        slv.callOutputWriter(k, 0.0)
+    assert len(a) == 4 and a[-1][0]["currentTime"] == pytest.approx(0.02)
+    slv.close()
+
+
+def test_call_output_writer_before_any_advance_writes_the_initial_values(fake):
+    s = _system()
+    got = []
+    s.output_writers = [({"format": "PythonCallback", "callback": got.append, "outputInterval": 5}, [0])]
+    fake(s)
+    slv = S.FastMonodomainSolver(s)
+    slv.callOutputWriter(0, 0.0)
+    assert len(got) == 1 and got[0][0]["currentTime"] == 0.0
+    slv.callOutputWriter(1, 0.0, 2)      # 1 % 2: not called
+    assert len(got) == 1
+    slv.close()
+
+
+def test_stimulation_log_enabled_from_settings_and_written_at_close(fake, tmp_path):
+    s = _system()
+    s.stimulation_log_filename = str(tmp_path / "out" / "stimulation.log")
+    s.fiber_numbers = [7, 9]
+    s.motor_unit_no = np.array([3, 1], np.int32)
+    lib = fake(s)
+    lib.log_t = np.array([10.0, 0.0, 0.0, 10.0])
+    lib.log_f = np.array([1, 1, 0, 0], np.int32)
+    slv = S.FastMonodomainSolver(s)
+    slv.initialize()
+    caps = [c[1] for c in lib.calls if c[0] == "fdm_set_stimulation_log"]
+    # at most one begin per check period 1/f = 10 ms: ceil(0.01 * 0.1) + 2 per fiber, plus a margin
+    assert caps == [2 * 3 + 16]
+    slv.advanceTimeSpan()
+    grow = [c for c in lib.calls if c[0] == "fdm_set_stimulation_log"]
+    assert grow[-1][1] == 4 + 2 * 3 + 16           # entries so far + what the span can add
+    log = slv.stimulation_log()
+    np.testing.assert_array_equal(log["time"], [0.0, 0.0, 10.0, 10.0])
+    np.testing.assert_array_equal(log["fiber"], [7, 9, 7, 9])
+    np.testing.assert_array_equal(log["motorUnit"], [3, 1, 3, 1])
+    slv.close()
+    assert (tmp_path / "out" / "stimulation.log").read_text() == \
+        "# motor unit no; fiber no; stimulation times in ms\n1;9;0;10;\n3;7;0;10;"
+    assert any(c[0] == "fdm_destroy" for c in lib.calls)

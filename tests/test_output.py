@@ -111,3 +111,14 @@ def test_output_writers_from_settings():
     for inst in term2["instances"]:
         inst["ImplicitEuler"].pop("OutputWriter")
     assert S.parse_settings(cfg).output_writers == []
+
+
+def test_stimulation_log_format(tmp_path):
+    # StimulationLogging::writeLogFile (stimulation_logging.cpp:119-165): sorted by motor unit, fiber, time;
+    # one line per (motor unit, fiber), times as a C++ stream writes doubles, no newline at the end
+    path = str(tmp_path / "log" / "stimulation.log")
+    output.write_stimulation_log(path, [10.0, 0.0, 5e-05, 20.0, 0.123456789], [3, 3, 1, 3, 1], [2, 2, 0, 2, 0])
+    assert open(path).read() == ("# motor unit no; fiber no; stimulation times in ms\n"
+                                 "0;1;5e-05;0.123457;\n2;3;0;10;20;")
+    output.write_stimulation_log(str(tmp_path / "empty.log"), [], [], [])
+    assert not os.path.exists(str(tmp_path / "empty.log"))
