@@ -31,7 +31,9 @@ the derived constants of ``initConsts`` keep using the file's raw values
 """
 from __future__ import annotations
 
+import json
 import math
+import numbers
 import os
 import re
 from dataclasses import dataclass, field
@@ -1370,4 +1372,102 @@ def emit_cuda_vjp(model: Model, params_alg: Sequence[int], params_const: Sequenc
     out.append("  }")
     for n in pows_vjp:
         out.append(f"#undef FDM_POW{n}")
+    return out
+
+
+# ----------------------------------------------------------------------------------------------
+# the "mappings" settings key
+# ----------------------------------------------------------------------------------------------
+
+def model_variable_names(model: str) -> Dict[str, List[str]]:
+    """Names ("component/variable") of the states, algebraics and constants of a built model, from the
+    generator's description next to its CUDA code."""
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "generated")
+    for f in sorted(os.listdir(here)):
+        if f.startswith(model + "_") and f.endswith(".json"):
+            with open(os.path.join(here, f)) as fh:
+                d = json.load(fh)
+            return {"state": d["state_names"], "algebraic": d["algebraic_names"], "constant": d["constant_names"]}
+    raise ValueError(f"no generated description for model {model!r}")
+
+
+def parse_mappings(mappings: dict, names: Dict[str, List[str]]) -> Dict[str, list]:
+    """The CellmlAdapter's ``"mappings"`` key (core/src/cellml/00_cellml_adapter_base.tpp:160-607).
+
+    Keys are ``("parameter", i)``, ``("connectorSlot", i)``, ``("connectorSlot", "slotName")`` (numbered on from
+    the last number) or ``(kind, i, "slotName")``; a key that is not a tuple is a parameter number.  Values are
+    ``(kind, name or number)`` with kind state / algebraic (or intermediate) / constant / parameter, or a bare
+    name, looked up among the algebraics, then the states, then the constants.  Entries are ordered by the
+    length of the key's first word and then by number (parameters before connector slots).  Parameters mapped to
+    algebraics and constants give parametersUsedAsAlgebraic / parametersUsedAsConstant in that order; connector
+    slots give statesForTransfer, algebraicsForTransfer and parametersForTransfer (a constant that is a parameter
+    counts as that parameter).  What the reference only logs as an error raises ValueError here."""
+    entries = []
+    slot_counter = 0
+    for key, value in mappings.items():
+        if isinstance(key, tuple):
+            word = str(key[0])
+            if len(key) == 2:
+                if isinstance(key[1], numbers.Integral):
+                    no, slot = int(key[1]), ""
+                    slot_counter = no + 1
+                else:
+                    no, slot = slot_counter, str(key[1])
+                    slot_counter += 1
+            elif len(key) == 3:
+                no, slot = int(key[1]), str(key[2])
+            else:
+                raise ValueError(f"mappings: key {key!r} is not a tuple with 2 or 3 entries")
+            if word not in ("parameter", "connectorSlot", "outputConnectorSlot"):
+                raise ValueError(f"mappings: key {key!r} is not ('parameter', i) or ('connectorSlot', i)")
+        else:
+            word, no, slot = "parameter", int(key), ""
+        if isinstance(value, tuple):
+            kind, what = str(value[0]), value[1]
+        else:
+            what = str(value)
+            kind = next((k for k in ("algebraic", "state", "constant") if what in names[k]), None)
+            if kind is None:
+                raise ValueError(f"mappings: {what!r} is neither a state, an algebraic nor a constant of the model")
+        if kind == "intermediate":
+            kind = "algebraic"
+        entries.append(((word, no, slot), (kind, what)))
+    entries.sort(key=lambda e: (len(e[0][0]), e[0][1]))
+
+    def field_no(kind, what):
+        if isinstance(what, numbers.Integral) or (isinstance(what, str) and what.isdigit()):
+            return int(what)
+        if kind not in names or what not in names[kind]:
+            raise ValueError(f"mappings: {kind} {what!r} is not a {kind} of the model")
+        return names[kind].index(what)
+
+    out = {"parametersUsedAsAlgebraic": [], "parametersUsedAsConstant": [], "statesForTransfer": [],
+           "algebraicsForTransfer": [], "parametersForTransfer": [], "slotNames": []}
+    slot_names = {"state": [], "algebraic": [], "parameter": []}
+    for (word, no, slot), (kind, what) in entries:
+        if kind not in ("state", "algebraic", "constant", "parameter"):
+            raise ValueError(f"mappings: invalid field {kind!r} (state, algebraic or constant)")
+        if kind == "parameter":
+            fno = int(what)
+        else:
+            fno = field_no(kind, what)
+        if word == "parameter":
+            if kind == "algebraic":
+                out["parametersUsedAsAlgebraic"].append(fno)
+            elif kind == "constant":
+                out["parametersUsedAsConstant"].append(fno)
+            else:
+                raise ValueError(f"mappings: parameter {no} maps to a {kind}; parameters map to algebraics and "
+                                 f"constants only")
+        elif kind in ("state", "algebraic", "parameter"):
+            out[{"state": "statesForTransfer", "algebraic": "algebraicsForTransfer",
+                 "parameter": "parametersForTransfer"}[kind]].append(fno)
+            slot_names[kind].append(slot)
+        elif fno in out["parametersUsedAsConstant"]:
+            out["parametersForTransfer"].append(len(out["parametersUsedAsAlgebraic"]) +
+                                                out["parametersUsedAsConstant"].index(fno))
+            slot_names["parameter"].append(slot)
+        else:
+            raise ValueError(f"mappings: connector slot {no} maps to constant {what!r}, which is no parameter")
+    out["slotNames"] = slot_names["state"] + slot_names["algebraic"] + slot_names["parameter"]
     return out

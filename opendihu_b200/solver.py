@@ -23,6 +23,7 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 from . import _native as N
+from . import cellml as CM
 from . import inputs
 from . import output
 
@@ -169,9 +170,13 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     Heun ``timeStepWidth``; CellML ``modelFilename``, ``approximateExponentialFunction``,
     ``setSpecificStates{CallFrequency,FrequencyJitter,RepeatAfterFirstCall,CallEnableBegin}``,
     ``additionalArgument``, ``parametersUsedAsAlgebraic``, ``parametersUsedAsConstant``,
-    ``parametersInitialValues``, ``statesInitialValues``, ``algebraicsForTransfer``, ``statesForTransfer``;
-    diffusion ``timeStepWidth``; FiniteElementMethod ``prefactor``, ``meshName``; ``Meshes`` entries with
-    ``nElements``/``physicalExtent`` or ``nodePositions``.  B200 options go in an optional ``"B200"`` dict
+    ``parametersInitialValues``, ``statesInitialValues``, ``algebraicsForTransfer``, ``statesForTransfer``,
+    ``mappings`` (instead of the four keys before it), ``stimulationLogFilename``; diffusion ``timeStepWidth``,
+    ``nAdditionalFieldVariables``, ``OutputWriter``; FiniteElementMethod ``prefactor``, ``meshName``; ``Meshes``
+    entries with ``nElements``/``physicalExtent`` or ``nodePositions``.  The code-generation keys
+    (``generateGPUSource``, ``libraryFilename``, ``compilerFlags``, ``preCompileCommand``,
+    ``postCompileCommand``, ``maximumNumberOfThreads``, ``useAoVSMemoryLayout``) are accepted and have no effect:
+    the kernels are compiled into the library.  B200 options go in an optional ``"B200"`` dict
     next to the FastMonodomainSolver keys (``method``, ``precision``, ``clampRule``, ``vcWidth``,
     ``nRanks``, ``stimulusMode``, ``stimulusParameter``, ``stimulusValue``, ``neuromuscularJunctionSeed``).
     """
@@ -232,8 +237,17 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
 
     # parameters: map the settings' parameter list onto the built variant's slots
     pa_var, pc_var = VARIANT_PARAMETERS[model]
-    pa = [int(x) for x in _as_list(cellml.get("parametersUsedAsAlgebraic", []))]
-    pc = [int(x) for x in _as_list(cellml.get("parametersUsedAsConstant", []))]
+    if cellml.get("mappings"):
+        # parameters and transfer slots by name (00_cellml_adapter_base.tpp:160-607); the key replaces
+        # parametersUsedAs*, statesForTransfer and algebraicsForTransfer
+        mp = CM.parse_mappings(cellml["mappings"], CM.model_variable_names(model))
+        pa, pc = mp["parametersUsedAsAlgebraic"], mp["parametersUsedAsConstant"]
+        st_transfer, alg_transfer = mp["statesForTransfer"], mp["algebraicsForTransfer"]
+    else:
+        pa = [int(x) for x in _as_list(cellml.get("parametersUsedAsAlgebraic", []))]
+        pc = [int(x) for x in _as_list(cellml.get("parametersUsedAsConstant", []))]
+        st_transfer = [int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))]
+        alg_transfer = [int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))]
     if tuple(pa) != tuple(pa_var) or any(c not in pc_var for c in pc):
         raise ValueError(f"settings: parametersUsedAsAlgebraic={pa}, parametersUsedAsConstant={pc} is not a prebuilt "
                          f"variant of {model} (algebraic {list(pa_var)}, constants within {list(pc_var)})")
@@ -316,8 +330,7 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         vc_width=int(b200.get("vcWidth", 4)), n_ranks=int(b200.get("nRanks", 1)),
         stimulus_mode=b200.get("stimulusMode", "clamp"), stimulus_parameter=int(b200.get("stimulusParameter", 0)),
         stimulus_value=float(b200.get("stimulusValue", 0.0)),
-        algebraics_for_transfer=[int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))],
-        states_for_transfer=[int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))] or [0],
+        algebraics_for_transfer=alg_transfer, states_for_transfer=st_transfer or [0],
         only_compute_if_has_been_stimulated=only_if_stimulated, skip_close_to_equilibrium=skip_equilibrium)
     sys_.fiber_mesh_names = [fb["fem"].get("meshName", fb["cellml"].get("meshName")) for fb in fibers]
     sys_.compute_state_information = \

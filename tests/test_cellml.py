@@ -115,3 +115,59 @@ def test_generated_rhs_matches_reference_model_file(model, params_alg, params_co
             assert dep.sum() <= 2, np.nonzero(dep)
         else:
             np.testing.assert_allclose(r, r_ref, rtol=1e-14, atol=1e-300)
+
+
+def test_mappings_of_the_example_settings():
+    # the "mappings" the fibers_emg example builds for its models (examples/electrophysiology/fibers/fibers_emg/
+    # helper.py:112-132) resolve to the parameter variants built into the library
+    from opendihu_b200 import cellml as CM
+    hh = CM.model_variable_names("hodgkin_huxley_1952")
+    m = CM.parse_mappings({("parameter", 0): ("constant", "membrane/i_Stim"),
+                           ("connectorSlot", 0): ("state", "membrane/V")}, hh)
+    assert m["parametersUsedAsConstant"] == [2] and m["parametersUsedAsAlgebraic"] == []
+    assert m["statesForTransfer"] == [0] and m["algebraicsForTransfer"] == []
+    sh = CM.model_variable_names("shorten_ocallaghan_davidson_soboleva_2007")
+    m = CM.parse_mappings({("parameter", 0): ("algebraic", "wal_environment/I_HH"),
+                           ("parameter", 1): ("constant", "razumova/L_x"),
+                           ("connectorSlot", 0): ("state", "wal_environment/vS")}, sh)
+    assert (m["parametersUsedAsAlgebraic"], m["parametersUsedAsConstant"], m["statesForTransfer"]) == ([32], [65], [0])
+
+
+def test_mappings_forms():
+    # 00_cellml_adapter_base.tpp:160-607: bare names are looked up among algebraics, states, constants; numbers
+    # may replace names; slots given by name are numbered on; parameters sort before connector slots; a
+    # constant that is a parameter can be a slot (as that parameter)
+    from opendihu_b200 import cellml as CM
+    names = {"state": ["c/V", "c/m"], "algebraic": ["c/i_Na", "c/i_K"], "constant": ["c/g", "c/E", "c/I"]}
+    m = CM.parse_mappings({("connectorSlot", "vm"): "c/V", ("connectorSlot", "ik"): "c/i_K",
+                           ("parameter", 1): ("constant", "c/I"), ("parameter", 0): ("algebraic", 0),
+                           ("connectorSlot", 5): ("constant", "2"), 2: ("constant", "c/g")}, names)
+    assert m["parametersUsedAsAlgebraic"] == [0] and m["parametersUsedAsConstant"] == [2, 0]
+    assert m["statesForTransfer"] == [0] and m["algebraicsForTransfer"] == [1]
+    assert m["parametersForTransfer"] == [1] and m["slotNames"] == ["vm", "ik", ""]
+    with pytest.raises(ValueError):
+        CM.parse_mappings({("parameter", 0): ("state", "c/V")}, names)
+    with pytest.raises(ValueError):
+        CM.parse_mappings({("parameter", 0): "c/unknown"}, names)
+    with pytest.raises(ValueError):
+        CM.parse_mappings({("connectorSlot", 0): ("constant", "c/E")}, names)
+
+
+def test_settings_with_mappings():
+    from test_only_if_stimulated import reference_settings
+    from opendihu_b200 import solver as S
+    cfg = reference_settings(n_fibers=2)
+    for inst in cfg["RepeatedCall"]["MultipleInstances"]["instances"][0]["StrangSplitting"]["Term1"][
+            "MultipleInstances"]["instances"]:
+        c = inst["Heun"]["CellML"]
+        del c["parametersUsedAsAlgebraic"], c["parametersUsedAsConstant"]
+        c["mappings"] = {("parameter", 0): ("constant", "membrane/i_Stim"),
+                         ("parameter", 1): ("constant", "sodium_channel/g_Na"),
+                         ("connectorSlot", 0): ("state", "membrane/V"),
+                         ("connectorSlot", 1): ("algebraic", "potassium_channel/i_K")}
+        c["parametersInitialValues"] = [0.0, 100.0]
+    s = S.parse_settings(cfg)
+    assert list(s.states_for_transfer) == [0]
+    assert list(s.algebraics_for_transfer) == [4]
+    # slots of the built variant: i_Stim, g_Na, g_K (g_K keeps its model value 36)
+    np.testing.assert_allclose(s.parameters[:, 0], [0.0, 100.0, 36.0])
