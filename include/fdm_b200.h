@@ -328,6 +328,13 @@ int fdm_compat_configure(int model, int n_fibers, int n_instances_per_fiber, int
 int fdm_cellml_rhs_device(int model, int approximate_exponential_function, int64_t n_instances, double t,
                           const double *states, const double *parameters, double *rates, double *algebraics,
                           void *stream);
+/* "initializeStatesToEquilibrium" of the CellmlAdapter (03_cellml_adapter.tpp:445-515): classical RK4 steps of one
+ * instance with the given parameters, from states (in/out, host) until no state increment exceeds 1e-5, dt halved
+ * and the search restarted from the initial values whenever one exceeds 1e4, at most 1e7 steps; computed on the
+ * device.  *iterations, *max_increment and *dt_final (each may be null) report the search; the result is FDM_OK
+ * also when it did not converge (the reference then logs an error and keeps the last values). */
+int fdm_model_equilibrium(int model, int device, int approximate_exponential_function, const double *parameters,
+                          double dt, double *states, int64_t *iterations, double *max_increment, double *dt_final);
 /* the reference's generated entry point with its signature (04_generator_gpu.cpp:25-26), host arrays, sized by a
  * preceding fdm_cellml_rhs_configure (the reference bakes n_instances into the source); process-wide */
 int fdm_cellml_rhs_configure(int model, int64_t n_instances, int approximate_exponential_function, int device);

@@ -2443,6 +2443,68 @@ extern "C" int fdm_cellml_rhs_device(int model, int approximate_exponential_func
   return FDM_OK;
 }
 
+extern "C" int fdm_model_equilibrium(int model, int device, int approximate_exponential_function,
+                                     const double* parameters, double dt, double* states, int64_t* iterations,
+                                     double* max_increment, double* dt_final)
+{
+  const ModelDesc* m = model_desc(model);
+  if (!m || !states || !(dt > 0) || (m->n_parameters > 0 && !parameters))
+    return fail(nullptr, FDM_ERR_ARG, "fdm_model_equilibrium: bad argument");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, FDM_ERR_NO_DEVICE, "fdm_model_equilibrium: no CUDA device");
+  if (device < 0 || device >= ndev)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_model_equilibrium: device ordinal out of range");
+  if (cudaSetDevice(device) != cudaSuccess)
+    return fail(nullptr, FDM_ERR_CUDA, "fdm_model_equilibrium: cudaSetDevice failed");
+  const int NS = m->n_states, NP = std::max(m->n_parameters, 1);
+  // 03_cellml_adapter.tpp:469: at most 1e7 RK4 steps, here in launches of bounded length
+  const int64_t limit = 10000000, chunk = NS <= 8 ? 100000 : 5000;
+  DevBuf<double> u, u0, P;
+  DevBuf<EquilibriumSearch> es;
+  cudaStream_t st = nullptr;
+  std::string err;
+  auto run = [&]() -> cudaError_t {
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess || (e = u.alloc(NS)) ||
+        (e = u0.alloc(NS)) || (e = P.alloc(NP)) || (e = es.alloc(1)))
+      return e;
+    EquilibriumSearch h{dt, 0.0, 0, 0, 0};
+    if ((e = cudaMemcpyAsync(u.p, states, sizeof(double) * NS, cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(u0.p, states, sizeof(double) * NS, cudaMemcpyHostToDevice, st)) ||
+        (m->n_parameters > 0 &&
+         (e = cudaMemcpyAsync(P.p, parameters, sizeof(double) * m->n_parameters, cudaMemcpyHostToDevice, st))) ||
+        (e = cudaMemcpyAsync(es.p, &h, sizeof(h), cudaMemcpyHostToDevice, st)))
+      return e;
+    for (int64_t done = 0; done < limit && !h.done; done += chunk) {
+      if ((e = launch_equilibrium_search(model, approximate_exponential_function ? MATH_APPROX : MATH_EXACT, u.p,
+                                         u0.p, P.p, es.p, std::min(chunk, limit - done), st)) ||
+          (e = cudaMemcpyAsync(&h, es.p, sizeof(h), cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
+        return e;
+    }
+    if ((e = cudaMemcpyAsync(states, u.p, sizeof(double) * NS, cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+      return e;
+    if (iterations)
+      *iterations = h.iterations;
+    if (max_increment)
+      *max_increment = h.max_increment;
+    if (dt_final)
+      *dt_final = h.dt;
+    return cudaSuccess;
+  };
+  const cudaError_t e = run();
+  u.release();
+  u0.release();
+  P.release();
+  es.release();
+  if (st)
+    cudaStreamDestroy(st);
+  if (e != cudaSuccess)
+    return fail(nullptr, FDM_ERR_CUDA, std::string("fdm_model_equilibrium: ") + cudaGetErrorString(e));
+  return FDM_OK;
+}
+
 namespace {
 struct CellmlRhs {
   int model = -1, approx = 0, device = 0;

@@ -31,6 +31,9 @@ const ModelDesc* model_desc(int model);
 
 // split path
 cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s);
+// at most max_iterations RK4 steps of the equilibrium search of one instance (u in/out, u0 the initial values)
+cudaError_t launch_equilibrium_search(int model, MathKind mk, double* u, const double* u0, const double* params,
+                               EquilibriumSearch* es, int64_t max_iterations, cudaStream_t s);
 cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s);
 cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
                                 double* coef, int64_t stride, cudaStream_t s);

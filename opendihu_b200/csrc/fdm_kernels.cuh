@@ -361,6 +361,76 @@ __global__ void __launch_bounds__(128) cellml_rhs_kernel(int64_t n, double t, co
   }
 }
 
+// "initializeStatesToEquilibrium" (CellmlAdapter::initializeToEquilibriumValues, 03_cellml_adapter.tpp:445-515):
+// classical RK4 steps of one instance (the time stays at 0: t, t + dt/2, t + dt) until the largest state
+// increment (k1 + 2 k2 + 2 k3 + k4)/6 falls below 1e-5; an increment above 1e4 restarts from the initial values
+// with dt/2.  One thread; a launch does at most max_iterations steps, the host repeats it up to the total limit.
+struct EquilibriumSearch {
+  double dt;
+  double max_increment;
+  int64_t iterations;
+  int max_rate_no;
+  int done;
+};
+
+template<class Model, class Math>
+__global__ void equilibrium_search_kernel(double* __restrict__ u, const double* __restrict__ u0,
+                                   const double* __restrict__ P, EquilibriumSearch* __restrict__ es,
+                                   int64_t max_iterations)
+{
+  if (blockIdx.x != 0 || threadIdx.x != 0 || es->done)
+    return;
+  constexpr int NS = Model::nStates;
+  double y[NS], k1[NS], k2[NS], k3[NS], k4[NS], w[NS], alg[Model::nAlgebraics];
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    y[s] = u[s];
+  double dt = es->dt, inc_max = es->max_increment;
+  int rate_no = es->max_rate_no;
+  for (int64_t it = 0; it < max_iterations; it++) {
+    Model::template rates<double, Math>(0.0, y, P, k1, alg);
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      w[s] = y[s] + dt / 2. * k1[s];
+    Model::template rates<double, Math>(dt / 2., w, P, k2, alg);
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      w[s] = y[s] + dt / 2. * k2[s];
+    Model::template rates<double, Math>(dt / 2., w, P, k3, alg);
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      w[s] = y[s] + dt * k3[s];
+    Model::template rates<double, Math>(dt, w, P, k4, alg);
+    inc_max = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      const double inc = (k1[s] + 2 * k2[s] + 2 * k3[s] + k4[s]) / 6.;
+      if (fabs(inc) > inc_max) {
+        inc_max = fabs(inc);
+        rate_no = s;
+      }
+      y[s] += dt * inc;
+    }
+    es->iterations++;
+    if (inc_max > 1e4) {
+      dt /= 2.0;
+#pragma unroll
+      for (int s = 0; s < NS; s++)
+        y[s] = u0[s];
+    }
+    if (inc_max < 1e-5) {
+      es->done = 1;
+      break;
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    u[s] = y[s];
+  es->dt = dt;
+  es->max_increment = inc_max;
+  es->max_rate_no = rate_no;
+}
+
 // algebraicsForTransfer: copy the requested entries (selected at run time) without dynamic
 // register indexing
 template<class Model, class RR>

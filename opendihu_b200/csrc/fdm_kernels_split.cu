@@ -80,6 +80,27 @@ cudaError_t launch_cellml_rhs(int model, MathKind mk, int64_t n, double t, const
   }
 }
 
+template<class Model>
+static cudaError_t equilibrium_search_model(MathKind mk, double* u, const double* u0, const double* P, EquilibriumSearch* es,
+                                     int64_t n, cudaStream_t s)
+{
+  if (mk == MATH_EXACT)
+    equilibrium_search_kernel<Model, fdm_math_exact><<<1, 1, 0, s>>>(u, u0, P, es, n);
+  else
+    equilibrium_search_kernel<Model, fdm_math_approx><<<1, 1, 0, s>>>(u, u0, P, es, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_equilibrium_search(int model, MathKind mk, double* u, const double* u0, const double* params,
+                               EquilibriumSearch* es, int64_t max_iterations, cudaStream_t s)
+{
+  switch (model) {
+  case 0: return equilibrium_search_model<HH>(mk, u, u0, params, es, max_iterations, s);
+  case 1: return equilibrium_search_model<SH>(mk, u, u0, params, es, max_iterations, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s)
 {
   if (a.n_fibers == 0)

@@ -89,6 +89,10 @@ class FiberSystem:
     fiber_numbers: Sequence[int] = ()
     # "stimulationLogFilename" of the CellML settings: the stimulation log written when the solver closes
     stimulation_log_filename: str = ""
+    # "initializeStatesToEquilibrium" / "initializeStatesToEquilibriumTimestepWidth" of the CellML settings: the
+    # initial states of every node are the equilibrium of the first node's initial states and parameters
+    initialize_states_to_equilibrium: bool = False
+    equilibrium_dt: float = 1e-4
 
     @property
     def n_fibers(self) -> int:
@@ -338,10 +342,32 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     sys_.output_writers = writers
     sys_.fiber_numbers = fiber_numbers
     sys_.stimulation_log_filename = str(cellml.get("stimulationLogFilename") or "")
+    sys_.initialize_states_to_equilibrium = bool(cellml.get("initializeStatesToEquilibrium", False))
+    sys_.equilibrium_dt = float(cellml.get("initializeStatesToEquilibriumTimestepWidth", 1e-4))
     sys_.n_additional_field_variables = int(f0["diff"].get("nAdditionalFieldVariables", 0))
     sys_.method = b200.get("method", "split")
     sys_.precision = precision
     return sys_
+
+
+def equilibrium_states(system: FiberSystem, device: int = 0) -> Dict[str, object]:
+    """The CellmlAdapter's equilibrium search (03_cellml_adapter.tpp:445-515) for the first node: its initial
+    states (the settings' statesInitialValues or the model's) and parameters, RK4 with the settings' time step
+    width (fdm_model_equilibrium).  A search that does not converge warns, as the reference logs an error, and
+    returns its last values."""
+    ns, _, npar, init, _ = model_sizes(system.model)
+    y = np.ascontiguousarray(system.states[:, 0] if system.states is not None else init, np.float64).copy()
+    p = np.ascontiguousarray(system.parameters[:, 0] if system.parameters is not None and npar else np.zeros(1),
+                             np.float64)
+    it, inc, dt = C.c_int64(), C.c_double(), C.c_double()
+    N.check(N.lib().fdm_model_equilibrium(N.MODEL_IDS[system.model], int(device),
+                                          int(bool(system.approximate_exponential_function)), N.ptr(p, C.c_double),
+                                          float(system.equilibrium_dt), N.ptr(y, C.c_double), C.byref(it),
+                                          C.byref(inc), C.byref(dt)))
+    if not inc.value < 1e-5:
+        warnings.warn(f"equilibrium values for the states were not found within {it.value} RK-4 steps: last "
+                      f"increment {inc.value}, time step width {dt.value}")
+    return {"states": y, "iterations": it.value, "max_increment": inc.value, "dt": dt.value}
 
 
 def write_host_settings(system: FiberSystem, path: str, method: Optional[str] = None,
@@ -423,6 +449,9 @@ class FastMonodomainSolver:
         self._ck = None
         self._writers = None
         self._log_on = False
+        self._equilibrium_done = False
+        #: result of the "initializeStatesToEquilibrium" search (states, iterations, max_increment, dt)
+        self.equilibrium = None
         # the reference's currentTime_ (end of the last RepeatedCall piece) and nTimeStepsSplitting_ (its
         # split steps), which callOutputWriter hands to the writers
         self._current_time = system.start_time
@@ -485,6 +514,10 @@ class FastMonodomainSolver:
             if s.parameters is not None and s.parameters.size:
                 p = np.ascontiguousarray(s.parameters, np.float64)
                 self._call(L.fdm_set_parameters, N.ptr(p, C.c_double))
+            if s.initialize_states_to_equilibrium and not self._equilibrium_done:
+                self.equilibrium = equilibrium_states(s, self.device)
+                s.states = np.repeat(self.equilibrium["states"][:, None], s.n_nodes, axis=1)
+                self._equilibrium_done = True
             if s.states is not None:
                 st = np.ascontiguousarray(s.states, np.float64)
                 self._call(L.fdm_set_states, N.ptr(st, C.c_double))

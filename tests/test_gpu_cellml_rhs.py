@@ -64,3 +64,42 @@ def test_reference_signature_export():
                                  N.ptr(pr, C.c_double))
     np.testing.assert_allclose(r, ref_r, rtol=1e-11, atol=1e-12 * np.abs(ref_r).max())
     np.testing.assert_allclose(a, ref_a[:na], rtol=1e-11, atol=1e-12 * np.abs(ref_a).max())
+
+
+def _rk4_increment(y, P, dt):
+    f = lambda u, t: O.rates(H.HH, u, P, t)[0]
+    k1 = f(y, 0.0)
+    k2 = f(y + dt / 2. * k1, dt / 2.)
+    k3 = f(y + dt / 2. * k2, dt / 2.)
+    k4 = f(y + dt * k3, dt)
+    return (k1 + 2 * k2 + 2 * k3 + k4) / 6.
+
+
+def test_equilibrium_search():
+    # initializeStatesToEquilibrium (03_cellml_adapter.tpp:445-515) for HH from its initial values: the same RK4
+    # search with the oracle's right-hand side on the CPU stops after 436,094 steps at the values below
+    from opendihu_b200 import solver as S
+    s = H.complete(H.c1_system(n_fibers=1, n_nodes=3, end_time=0.0))
+    eq = S.equilibrium_states(s)
+    assert eq["max_increment"] < 1e-5 and eq["dt"] == 1e-4
+    assert 436_000 <= eq["iterations"] <= 436_200
+    np.testing.assert_allclose(eq["states"], [-7.49951664e+01, 5.29626812e-02, 5.96036857e-01, 3.17728799e-01],
+                               rtol=1e-6)
+    assert np.max(np.abs(_rk4_increment(eq["states"], s.parameters[:, 0], 1e-4))) < 1.001e-5
+
+
+def test_settings_initialize_states_to_equilibrium():
+    from test_only_if_stimulated import reference_settings
+    from opendihu_b200 import solver as S
+    cfg = reference_settings(n_fibers=2)
+    for inst in cfg["RepeatedCall"]["MultipleInstances"]["instances"][0]["StrangSplitting"]["Term1"][
+            "MultipleInstances"]["instances"]:
+        inst["Heun"]["CellML"]["initializeStatesToEquilibrium"] = True
+        inst["Heun"]["CellML"]["initializeStatesToEquilibriumTimestepWidth"] = 2e-4
+    s = S.parse_settings(cfg)
+    assert s.initialize_states_to_equilibrium and s.equilibrium_dt == 2e-4
+    with S.FastMonodomainSolver(s, method="split", precision="fp64") as slv:
+        st = slv.states()
+        eq = slv.equilibrium["states"]
+    np.testing.assert_array_equal(st, np.repeat(eq[:, None], st.shape[1], axis=1))
+    assert np.max(np.abs(_rk4_increment(eq, s.parameters[:, 0], 2e-4))) < 1.001e-5

@@ -15,9 +15,11 @@ from opendihu_b200 import solver as S
 
 class FakeLib:
     """Every fdm_* call succeeds and is recorded; the RepeatedCall plan follows the library's step-count rule
-    (one split step per piece here); Vm counts the pieces advanced so far."""
+    (one split step per piece here); Vm counts the pieces advanced so far; the host-only model queries go to
+    the real library."""
 
-    def __init__(self, n_nodes, dt_repeated_call):
+    def __init__(self, n_nodes, dt_repeated_call, real=None):
+        self.real = real
         self.calls = []
         self.n_nodes = n_nodes
         self.dt_rc = dt_repeated_call
@@ -37,6 +39,23 @@ class FakeLib:
 
     def fdm_last_error(self, h):
         return b"fake"
+
+    def fdm_model_info(self, *args):
+        return self.real.fdm_model_info(*args)
+
+    def fdm_model_parameter_defaults(self, *args):
+        return self.real.fdm_model_parameter_defaults(*args)
+
+    def fdm_model_equilibrium(self, model, device, approx, params, dt, states, it, inc, dtf):
+        y = np.ctypeslib.as_array(states, (4,))
+        self.calls.append(("fdm_model_equilibrium", dt, y.copy(), np.ctypeslib.as_array(params, (3,)).copy()))
+        y[:] = [-74.99, 0.053, 0.596, 0.318]
+        it._obj.value, inc._obj.value, dtf._obj.value = 1000, 9e-6, dt
+        return 0
+
+    def fdm_set_states(self, h, st):
+        self.calls.append(("fdm_set_states", np.ctypeslib.as_array(st, (4, self.n_nodes)).copy()))
+        return 0
 
     def _n(self, t0, t1):
         return max(1, math.ceil((t1 - t0) / self.dt_rc - 0.1))
@@ -74,8 +93,10 @@ class FakeLib:
 def fake(monkeypatch):
     holder = {}
 
+    real = N.lib()
+
     def install(system):
-        lib = FakeLib(system.n_nodes, system.dt_repeated_call)
+        lib = FakeLib(system.n_nodes, system.dt_repeated_call, real)
         monkeypatch.setattr(N, "lib", lambda: lib)
         holder["lib"] = lib
         return lib
@@ -152,3 +173,27 @@ def test_stimulation_log_enabled_from_settings_and_written_at_close(fake, tmp_pa
     assert (tmp_path / "out" / "stimulation.log").read_text() == \
         "# motor unit no; fiber no; stimulation times in ms\n1;9;0;10;\n3;7;0;10;"
     assert any(c[0] == "fdm_destroy" for c in lib.calls)
+
+
+def test_states_initialized_to_equilibrium(fake):
+    # "initializeStatesToEquilibrium": the search starts from the first node's states and parameters with the
+    # settings' time step width, and every node starts from its result
+    s = _system()
+    s.states[:, 0] = [-70.0, 0.1, 0.5, 0.3]
+    s.parameters[1, 0] = 100.0
+    s.initialize_states_to_equilibrium = True
+    s.equilibrium_dt = 2e-4
+    lib = fake(s)
+    slv = S.FastMonodomainSolver(s)
+    slv.initialize()
+    (name, dt, y0, p0), = [c for c in lib.calls if c[0] == "fdm_model_equilibrium"]
+    assert dt == 2e-4
+    np.testing.assert_array_equal(y0, [-70.0, 0.1, 0.5, 0.3])
+    np.testing.assert_array_equal(p0, s.parameters[:, 0])
+    (_, st), = [c for c in lib.calls if c[0] == "fdm_set_states"]
+    np.testing.assert_array_equal(st, np.repeat(np.array([-74.99, 0.053, 0.596, 0.318])[:, None], s.n_nodes, 1))
+    assert slv.equilibrium["iterations"] == 1000
+    slv.close()
+    slv.initialize()                      # a second initialize keeps the equilibrium states, no new search
+    assert len([c for c in lib.calls if c[0] == "fdm_model_equilibrium"]) == 1
+    slv.close()
