@@ -13,6 +13,8 @@
 #ifndef FDM_B200_HPP
 #define FDM_B200_HPP
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <functional>
@@ -53,6 +55,9 @@ struct FiberSettings {
   std::vector<double> jitter;                // [fiber][k]
   int n_jitter = 0;
   std::vector<int> algebraics_for_transfer, states_for_transfer{0};
+  std::vector<int> fiber_numbers;            // global fiber numbers ("additionalArgument"; empty: the index)
+  bool initialize_states_to_equilibrium = false;  // "initializeStatesToEquilibrium" of the CellML settings
+  double equilibrium_dt = 1e-4;                   // "initializeStatesToEquilibriumTimestepWidth"
 
   int n_fibers() const { return fiber_offsets.empty() ? 0 : (int)fiber_offsets.size() - 1; }
   int64_t n_nodes() const { return fiber_offsets.empty() ? 0 : fiber_offsets.back(); }
@@ -142,8 +147,20 @@ struct FiberSettings {
     s.algebraics_for_transfer = as_int("algebraics_for_transfer");
     if (has("states_for_transfer"))
       s.states_for_transfer = as_int("states_for_transfer");
+    s.fiber_numbers = as_int("fiber_numbers");
+    if (has("initialize_states_to_equilibrium"))
+      s.initialize_states_to_equilibrium = num("initialize_states_to_equilibrium") != 0;
+    if (has("equilibrium_dt"))
+      s.equilibrium_dt = num("equilibrium_dt");
     return s;
   }
+};
+
+/* One entry of the stimulation log (StimulationLogging::StimulationLogEntry, stimulation_logging.h:28-33). */
+struct StimulationLogEntry {
+  double time;
+  int motorUnitNo;
+  int fiberNo;
 };
 
 /* The transferred fiber data (updateFiberData: statesForTransfer, algebraicsForTransfer), [k][node]. */
@@ -199,7 +216,8 @@ class FastMonodomainSolver {
   FastMonodomainSolver& operator=(const FastMonodomainSolver&) = delete;
   FastMonodomainSolver(FastMonodomainSolver&& o) noexcept
       : s_(std::move(o.s_)), h_(o.h_), start_(o.start_), end_(o.end_), writers_(std::move(o.writers_)),
-        current_time_(o.current_time_), piece_steps_(o.piece_steps_)
+        current_time_(o.current_time_), piece_steps_(o.piece_steps_), log_on_(o.log_on_),
+        equilibrium_done_(o.equilibrium_done_), equilibrium_iterations_(o.equilibrium_iterations_)
   {
     o.h_ = nullptr;
   }
@@ -216,6 +234,8 @@ class FastMonodomainSolver {
     h_ = h;
     try {
       const int nf = s_.n_fibers();
+      if (s_.initialize_states_to_equilibrium && !equilibrium_done_)
+        initialize_to_equilibrium();
       check(fdm_set_fibers(h_, nf, s_.fiber_offsets.data(), s_.element_lengths.data(), s_.prefactor.data()));
       if (!s_.parameters.empty())
         check(fdm_set_parameters(h_, s_.parameters.data()));
@@ -248,6 +268,8 @@ class FastMonodomainSolver {
   void advanceTimeSpan(bool withOutputWritersEnabled = true)
   {
     initialize();
+    if (log_on_)
+      grow_stimulation_log(end_ - start_);
     int64_t n = 0;
     check(fdm_repeated_call_plan(h_, start_, end_, &n, nullptr));
     std::vector<int> steps((size_t)(n > 0 ? n : 1), 0);
@@ -339,6 +361,65 @@ class FastMonodomainSolver {
     h_ = nullptr;
   }
 
+  /* StimulationLogging: from now on every stimulation begin is recorded (fdm_set_stimulation_log); the capacity
+   * grows before each advance to what its span can need */
+  void enableStimulationLog()
+  {
+    initialize();
+    log_on_ = true;
+    check(fdm_set_stimulation_log(h_, log_bound(s_.end_time - s_.start_time)));
+  }
+
+  /* the recorded stimulation begins in time order (fibers numbered by fiber_numbers) */
+  std::vector<StimulationLogEntry> stimulationLog()
+  {
+    initialize();
+    int64_t n = 0;
+    check(fdm_get_stimulation_log(h_, &n, nullptr, nullptr));
+    std::vector<double> t((size_t)(n > 0 ? n : 1));
+    std::vector<int> f(t.size());
+    check(fdm_get_stimulation_log(h_, &n, t.data(), f.data()));
+    std::vector<StimulationLogEntry> out;
+    for (int64_t i = 0; i < n && i < (int64_t)t.size(); i++) {
+      const int fi = f[(size_t)i];
+      out.push_back({t[(size_t)i], s_.motor_unit_no.empty() ? -1 : s_.motor_unit_no[(size_t)fi],
+                     s_.fiber_numbers.size() == (size_t)s_.n_fibers() ? s_.fiber_numbers[(size_t)fi] : fi});
+    }
+    std::sort(out.begin(), out.end(), [](const StimulationLogEntry& a, const StimulationLogEntry& b) {
+      return a.time < b.time || (a.time == b.time && a.fiberNo < b.fiberNo);
+    });
+    return out;
+  }
+
+  /* the log file of StimulationLogging::writeLogFile (stimulation_logging.cpp:119-165): sorted by motor unit,
+   * fiber and time, a header line and one "<motor unit>;<fiber>;<t1>;<t2>;...;" line per (motor unit, fiber),
+   * doubles as a stream writes them; nothing for an empty log */
+  void writeStimulationLog(const std::string& filename)
+  {
+    std::vector<StimulationLogEntry> e = stimulationLog();
+    if (e.empty())
+      return;
+    std::sort(e.begin(), e.end(), [](const StimulationLogEntry& a, const StimulationLogEntry& b) {
+      if (a.motorUnitNo != b.motorUnitNo)
+        return a.motorUnitNo < b.motorUnitNo;
+      if (a.fiberNo != b.fiberNo)
+        return a.fiberNo < b.fiberNo;
+      return a.time < b.time;
+    });
+    std::ofstream file(filename);
+    if (!file)
+      throw Error(FDM_ERR_ARG, "writeStimulationLog: cannot open " + filename);
+    file << "# motor unit no; fiber no; stimulation times in ms" << std::endl;
+    for (size_t i = 0; i < e.size(); i++) {
+      if (i == 0 || e[i].fiberNo != e[i - 1].fiberNo || e[i].motorUnitNo != e[i - 1].motorUnitNo) {
+        if (i != 0)
+          file << "\n";
+        file << e[i].motorUnitNo << ";" << e[i].fiberNo << ";";
+      }
+      file << e[i].time << ";";
+    }
+  }
+
   /* the diffusion's output writers, called after each RepeatedCall piece of advanceTimeSpan(true) */
   void addOutputWriter(OutputWriter w) { writers_.push_back(std::move(w)); }
 
@@ -372,6 +453,57 @@ class FastMonodomainSolver {
       throw Error(rc, fdm_last_error(h_));
   }
 
+  /* CellmlAdapter::initializeToEquilibriumValues (03_cellml_adapter.tpp:445-515) for the first node's states
+   * and parameters; every node starts from the result */
+  void initialize_to_equilibrium()
+  {
+    int ns = 0, na = 0, np = 0;
+    check(fdm_model_info(s_.config.model, &ns, &na, &np, nullptr));
+    const int64_t n = s_.n_nodes();
+    std::vector<double> y((size_t)ns), p((size_t)(np > 0 ? np : 1), 0.0);
+    if (s_.states.empty()) {
+      check(fdm_model_info(s_.config.model, &ns, &na, &np, y.data()));
+    } else {
+      for (int k = 0; k < ns; k++)
+        y[(size_t)k] = s_.states[(size_t)k * (size_t)n];
+    }
+    if (!s_.parameters.empty())
+      for (int q = 0; q < np; q++)
+        p[(size_t)q] = s_.parameters[(size_t)q * (size_t)n];
+    else if (np > 0)
+      check(fdm_model_parameter_defaults(s_.config.model, p.data()));
+    const int rc = fdm_model_equilibrium(s_.config.model, s_.config.device, s_.config.approximate_exponential_function,
+                                         p.data(), s_.equilibrium_dt, y.data(), &equilibrium_iterations_, nullptr,
+                                         nullptr);
+    if (rc != FDM_OK)
+      throw Error(rc, fdm_last_error(nullptr));
+    s_.states.assign((size_t)ns * (size_t)n, 0.0);
+    for (int k = 0; k < ns; k++)
+      for (int64_t i = 0; i < n; i++)
+        s_.states[(size_t)k * (size_t)n + (size_t)i] = y[(size_t)k];
+    equilibrium_done_ = true;
+  }
+
+  /* stimulation begins a span can hold: a fiber's machine checks at most once per 1/(f (1 + |jitter|)) */
+  int64_t log_bound(double span) const
+  {
+    int64_t b = 16;
+    for (int f = 0; f < s_.n_fibers(); f++) {
+      double jmax = 0.0;
+      for (int k = 0; k < s_.n_jitter; k++)
+        jmax = std::max(jmax, std::fabs(s_.jitter[(size_t)f * (size_t)s_.n_jitter + (size_t)k]));
+      b += (int64_t)std::ceil(std::max(span, 0.0) * s_.call_frequency[(size_t)f] * (1.0 + jmax)) + 2;
+    }
+    return b;
+  }
+
+  void grow_stimulation_log(double span)
+  {
+    int64_t n = 0;
+    check(fdm_get_stimulation_log(h_, &n, nullptr, nullptr));
+    check(fdm_set_stimulation_log(h_, n + log_bound(span)));
+  }
+
   /* end of RepeatedCall piece k of n (the Strang span's end time: start + k/n*span + span/n) */
   double piece_end(int64_t k, int64_t n) const
   {
@@ -386,6 +518,9 @@ class FastMonodomainSolver {
   std::vector<OutputWriter> writers_;
   double current_time_ = 0.0;  // the reference's currentTime_: end of the last RepeatedCall piece
   int piece_steps_ = 0;        // its number of split steps (nTimeStepsSplitting_)
+  bool log_on_ = false;
+  bool equilibrium_done_ = false;
+  int64_t equilibrium_iterations_ = 0;
 };
 
 }  // namespace fdm

@@ -394,6 +394,8 @@ def write_host_settings(system: FiberSystem, path: str, method: Optional[str] = 
         "skip_close_to_equilibrium": int(bool(s.skip_close_to_equilibrium)), "device": device,
         "start_time": s.start_time, "end_time": s.end_time, "firing_rows": fe.shape[0], "firing_cols": fe.shape[1],
         "n_jitter": jit.shape[1] if jit.ndim == 2 else 0,
+        "initialize_states_to_equilibrium": int(bool(s.initialize_states_to_equilibrium)),
+        "equilibrium_dt": s.equilibrium_dt,
     }
     arrays = {
         "fiber_offsets": s.fiber_offsets, "element_lengths": s.element_lengths, "prefactor": s.prefactor,
@@ -402,6 +404,7 @@ def write_host_settings(system: FiberSystem, path: str, method: Optional[str] = 
         "repeat_after_first_call": s.repeat_after_first_call, "call_enable_begin": s.call_enable_begin,
         "jitter": jit, "algebraics_for_transfer": s.algebraics_for_transfer,
         "states_for_transfer": s.states_for_transfer,
+        "fiber_numbers": s.fiber_numbers if len(s.fiber_numbers) == s.n_fibers else np.arange(s.n_fibers),
     }
     with open(path, "w") as f:
         f.write("# opendihu_b200 host settings: key count values\n")

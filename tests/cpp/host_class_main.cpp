@@ -2,13 +2,15 @@
 // drive its FastMonodomainSolver: settings in, setTimeSpan/advanceTimeSpan twice with a checkpoint between,
 // the checkpoint replayed, the states and the transferred algebraics written out.
 //   host_class_main <settings file> <output file> <intermediate time>
-// With a fifth argument it instead advances [startTime, endTime] once with an output writer of that
-// outputInterval whose callback writes one line per call (numbered name, current time, Vm sum) to the
-// output file, then calls callOutputWriter(0, 0) once more.
+// With a fifth argument it instead advances [startTime, endTime] once: "log" records the stimulation log and
+// writes it to the output file in the reference's format; a number is the outputInterval of an output writer
+// whose callback writes one line per call (numbered name, current time, Vm sum) to the output file, and
+// callOutputWriter(0, 0) is called once more.
 // Exit status: 0 done, 2 fdm::Error (message on stderr), 3 the replay after the checkpoint differs.
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <string>
 
 #include "fdm_b200.hpp"
 
@@ -20,6 +22,13 @@ int main(int argc, char** argv)
   }
   try {
     fdm::FiberSettings s = fdm::FiberSettings::load(argv[1]);
+    if (argc == 5 && std::string(argv[4]) == "log") {
+      fdm::FastMonodomainSolver slv(s);
+      slv.enableStimulationLog();
+      slv.advanceTimeSpan();
+      slv.writeStimulationLog(argv[2]);
+      return 0;
+    }
     if (argc == 5) {
       fdm::FastMonodomainSolver slv(s);
       std::FILE* f = std::fopen(argv[2], "w");

@@ -92,3 +92,40 @@ def test_cpp_output_writer_equals_python_writer(tmp_path):
         assert float(vm_sum) == pytest.approx(sum(float(np.sum(d["data"][1]["components"][0]["values"]))
                                                   for d in dicts), rel=1e-13)
     assert lines[0][0] == "out/fiber_0000000"
+
+
+@pytest.mark.gpu
+def test_cpp_stimulation_log_and_equilibrium_equal_python(tmp_path):
+    # the C++ class writes the same stimulation log file as the Python host class, and starts from the same
+    # equilibrium states when the settings ask for them
+    exe = _build(tmp_path)
+    s = _system()
+    s.end_time = 25.0
+    s.fiber_numbers = [4, 5, 6]
+    s.initialize_states_to_equilibrium = True
+    cfg = str(tmp_path / "settings.txt")
+    S.write_host_settings(s, cfg, method="split", precision="fp64")
+    out = str(tmp_path / "cpp.log")
+    r = subprocess.run([exe, cfg, out, "0", "log"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    s.stimulation_log_filename = str(tmp_path / "py.log")
+    slv = S.FastMonodomainSolver(s.copy(), method="split", precision="fp64")
+    slv.advanceTimeSpan()
+    n = len(slv.stimulation_log()["time"])
+    slv.close()
+    assert n == 9                          # three fibers stimulated every 10 ms from t = 0
+    assert open(out).read() == open(str(tmp_path / "py.log")).read()
+    # the default mode writes the states after its advances; with the equilibrium start they equal Python's
+    out = str(tmp_path / "out.bin")
+    s.end_time = 0.6
+    S.write_host_settings(s, cfg, method="split", precision="fp64")
+    r = subprocess.run([exe, cfg, out, "0.3"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    st = np.fromfile(out, np.float64)[:4 * s.n_nodes].reshape(4, s.n_nodes)
+    with S.FastMonodomainSolver(s.copy(), method="split", precision="fp64") as slv:
+        slv.setTimeSpan(0.0, 0.3)
+        slv.advanceTimeSpan()
+        slv.setTimeSpan(0.3, 0.6)
+        slv.advanceTimeSpan()
+        np.testing.assert_array_equal(st, slv.states())
+        assert slv.equilibrium["max_increment"] < 1e-5
