@@ -23,7 +23,8 @@ from typing import Callable, Dict, List, Optional, Sequence
 import numpy as np
 
 from . import _native as N
-from .solver import CLAMP_RULES, FastMonodomainSolver, FiberSystem
+from . import output
+from .solver import CLAMP_RULES, FastMonodomainSolver, FiberSystem, equilibrium_states
 
 
 def lpt_partition(weights: Sequence[int], n_shards: int) -> List[np.ndarray]:
@@ -70,8 +71,13 @@ def subset(system: FiberSystem, fibers) -> FiberSystem:
         s.states = np.asarray(system.states)[:, nodes].copy()
     if len(system.fiber_mesh_names) == system.n_fibers:
         s.fiber_mesh_names = [system.fiber_mesh_names[int(f)] for f in fibers]
-    # output writers name fibers of the unsharded layout: a shard runs none
+    nums = system.fiber_numbers if len(system.fiber_numbers) == system.n_fibers else range(system.n_fibers)
+    s.fiber_numbers = [int(nums[int(f)]) for f in fibers]
+    # output writers name fibers of the unsharded layout: a shard runs none; the stimulation log file and the
+    # equilibrium start belong to the whole system (ShardedSolver writes the one, computes the other once)
     s.output_writers = ()
+    s.stimulation_log_filename = ""
+    s.initialize_states_to_equilibrium = False
     return s
 
 
@@ -157,6 +163,9 @@ class ShardedSolver:
             self.shards.append(sv)
         self._start = system.start_time
         self._end = system.end_time
+        self._log_on = False
+        #: result of the "initializeStatesToEquilibrium" search, when the settings ask for it
+        self.equilibrium = None
 
     # -- parallel dispatch ------------------------------------------------------------------------
     def _each(self, fn):
@@ -186,12 +195,45 @@ class ShardedSolver:
 
     # -- lifecycle and the operator API ----------------------------------------------------------
     def initialize(self):
+        s = self.system
+        if s.initialize_states_to_equilibrium and self.equilibrium is None:
+            # one search for the whole system (the first node's states and parameters), as unsharded
+            self.equilibrium = equilibrium_states(s, self.devices[0])
+            s.states = np.repeat(self.equilibrium["states"][:, None], s.n_nodes, axis=1)
+            for k, sv in enumerate(self.shards):
+                if sv is not None:
+                    sv.system.states = np.ascontiguousarray(s.states[:, self.nodes[k]])
         self._each(lambda k, sv: sv.initialize())
+        if s.stimulation_log_filename and not self._log_on:
+            self._log_on = True
+            self._each(lambda k, sv: sv.enable_stimulation_log())
+
+    def stimulation_log(self) -> Dict[str, np.ndarray]:
+        """The shards' stimulation logs merged, fibers by their numbers in the whole system, in time order."""
+        r = self._each(lambda k, sv: sv.stimulation_log())
+        t = np.concatenate([d["time"] for d in r.values()]) if r else np.zeros(0)
+        f = np.concatenate([d["fiber"] for d in r.values()]) if r else np.zeros(0, np.int64)
+        m = np.concatenate([d["motorUnit"] for d in r.values()]) if r else np.zeros(0, np.int64)
+        order = np.lexsort((f, t))
+        return {"time": t[order], "fiber": f[order], "motorUnit": m[order]}
+
+    def writeStimulationLog(self, filename: Optional[str] = None) -> str:
+        name = filename or self.system.stimulation_log_filename
+        if not name:
+            raise ValueError("writeStimulationLog: no file name (settings have no stimulationLogFilename)")
+        d = self.stimulation_log()
+        output.write_stimulation_log(name, d["time"], d["fiber"], d["motorUnit"])
+        return name
 
     def close(self):
-        for sv in self.shards:
-            if sv is not None:
-                sv.close()
+        try:
+            if self.system.stimulation_log_filename and self._log_on and any(sv is not None and sv.initialized
+                                                                             for sv in self.shards):
+                self.writeStimulationLog()
+        finally:
+            for sv in self.shards:
+                if sv is not None:
+                    sv.close()
 
     def __enter__(self):
         self.initialize()

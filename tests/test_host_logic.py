@@ -26,6 +26,7 @@ class FakeLib:
         self.pieces_done = 0
         self.log_t = np.zeros(0)
         self.log_f = np.zeros(0, np.int32)
+        self.n_of = {}                     # nodes per solver handle (from fdm_set_fibers)
 
     def __getattr__(self, name):
         def call(*args):
@@ -34,7 +35,12 @@ class FakeLib:
         return call
 
     def fdm_create(self, cfg, h):
-        h._obj.value = 1234
+        h._obj.value = 1000 + len(self.n_of)
+        self.n_of[h._obj.value] = self.n_nodes
+        return 0
+
+    def fdm_set_fibers(self, h, nf, off, elem, pf):
+        self.n_of[h.value] = int(np.ctypeslib.as_array(off, (nf + 1,))[-1])
         return 0
 
     def fdm_last_error(self, h):
@@ -54,7 +60,7 @@ class FakeLib:
         return 0
 
     def fdm_set_states(self, h, st):
-        self.calls.append(("fdm_set_states", np.ctypeslib.as_array(st, (4, self.n_nodes)).copy()))
+        self.calls.append(("fdm_set_states", np.ctypeslib.as_array(st, (4, self.n_of[h.value])).copy()))
         return 0
 
     def _n(self, t0, t1):
@@ -77,7 +83,7 @@ class FakeLib:
         return 0
 
     def fdm_get_vm(self, h, out):
-        np.ctypeslib.as_array(out, (self.n_nodes,))[:] = self.pieces_done
+        np.ctypeslib.as_array(out, (self.n_of[h.value],))[:] = self.pieces_done
         return 0
 
     def fdm_get_stimulation_log(self, h, n, t, f):
@@ -197,3 +203,28 @@ def test_states_initialized_to_equilibrium(fake):
     slv.initialize()                      # a second initialize keeps the equilibrium states, no new search
     assert len([c for c in lib.calls if c[0] == "fdm_model_equilibrium"]) == 1
     slv.close()
+
+
+def test_sharded_solver_merges_the_logs_and_searches_the_equilibrium_once(fake, tmp_path):
+    from opendihu_b200 import sharding as SH
+    s = H.complete(H.c1_system(n_fibers=3, n_nodes=11, end_time=0.01))
+    s.stimulation_log_filename = str(tmp_path / "stimulation.log")
+    s.initialize_states_to_equilibrium = True
+    s.motor_unit_no = np.array([0, 1, 2], np.int32)
+    lib = fake(s)
+    lib.log_t = np.array([0.0])
+    lib.log_f = np.array([0], np.int32)       # every shard reports its first fiber stimulated at t = 0
+    sh = SH.ShardedSolver(s, devices=[0], n_shards=2)
+    assert all(not sv.system.stimulation_log_filename for sv in sh.shards)
+    sh.initialize()
+    assert len([c for c in lib.calls if c[0] == "fdm_model_equilibrium"]) == 1
+    sets = [c[1] for c in lib.calls if c[0] == "fdm_set_states"]
+    assert sorted(x.shape[1] for x in sets) == [11, 22]
+    assert all(np.array_equal(x[:, 0], [-74.99, 0.053, 0.596, 0.318]) for x in sets)
+    log = sh.stimulation_log()
+    first = sorted(int(f[0]) for f in sh.fibers)
+    np.testing.assert_array_equal(log["fiber"], first)
+    np.testing.assert_array_equal(log["motorUnit"], s.motor_unit_no[first])
+    sh.close()
+    lines = (tmp_path / "stimulation.log").read_text().split("\n")
+    assert lines[1:] == [f"{s.motor_unit_no[f]};{f};0;" for f in first]
