@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import heapq
 import threading
+import warnings
 from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
@@ -164,6 +165,7 @@ class ShardedSolver:
         self._start = system.start_time
         self._end = system.end_time
         self._log_on = False
+        self._warned_writers = False
         #: result of the "initializeStatesToEquilibrium" search, when the settings ask for it
         self.equilibrium = None
 
@@ -255,6 +257,11 @@ class ShardedSolver:
         return self._end
 
     def advanceTimeSpan(self, withOutputWritersEnabled: bool = True):
+        if withOutputWritersEnabled and self.system.output_writers and not self._warned_writers:
+            # the shards advance without the settings' output writers; states() gathers the whole system's
+            # fibers for output.write_fibers
+            warnings.warn("ShardedSolver runs no OutputWriter of the settings (use states() and output.write_fibers)")
+            self._warned_writers = True
         self._each(lambda k, sv: sv.advanceTimeSpan(withOutputWritersEnabled))
 
     def run(self):

@@ -228,3 +228,14 @@ def test_sharded_solver_merges_the_logs_and_searches_the_equilibrium_once(fake, 
     sh.close()
     lines = (tmp_path / "stimulation.log").read_text().split("\n")
     assert lines[1:] == [f"{s.motor_unit_no[f]};{f};0;" for f in first]
+
+
+def test_sharded_solver_warns_that_it_runs_no_output_writers(fake):
+    from opendihu_b200 import sharding as SH
+    s = H.complete(H.c1_system(n_fibers=2, n_nodes=11, end_time=0.01))
+    s.output_writers = [({"format": "PythonCallback", "callback": lambda d: None}, [0, 1])]
+    fake(s)
+    sh = SH.ShardedSolver(s, devices=[0], n_shards=2)
+    with pytest.warns(UserWarning, match="no OutputWriter"):
+        sh.advanceTimeSpan()
+    sh.close()
