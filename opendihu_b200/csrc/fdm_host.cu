@@ -2179,13 +2179,21 @@ extern "C" int fdm_set_stimulation_log(fdm_solver* s, int64_t capacity)
   if (capacity > s->log_cap) { // grow, keeping the entries recorded so far
     DevBuf<double> t;
     DevBuf<int> f;
-    FDM_CUDA(t.alloc((size_t)capacity));
-    FDM_CUDA(f.alloc((size_t)capacity));
-    if (s->log_cap > 0) {
-      FDM_CUDA(cudaMemcpyAsync(t.p, s->log_t.p, sizeof(double) * s->log_cap, cudaMemcpyDeviceToDevice, s->stream));
-      FDM_CUDA(cudaMemcpyAsync(f.p, s->log_f.p, sizeof(int) * s->log_cap, cudaMemcpyDeviceToDevice, s->stream));
+    cudaError_t e = t.alloc((size_t)capacity);
+    if (e == cudaSuccess)
+      e = f.alloc((size_t)capacity);
+    if (e == cudaSuccess && s->log_cap > 0) {
+      e = cudaMemcpyAsync(t.p, s->log_t.p, sizeof(double) * s->log_cap, cudaMemcpyDeviceToDevice, s->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(f.p, s->log_f.p, sizeof(int) * s->log_cap, cudaMemcpyDeviceToDevice, s->stream);
     }
-    FDM_CUDA(cudaStreamSynchronize(s->stream));
+    if (e == cudaSuccess)
+      e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) { // the log stays as it was
+      t.release();
+      f.release();
+      return cuda_fail(s, e, "fdm_set_stimulation_log");
+    }
     s->log_t.release();
     s->log_f.release();
     s->log_t = t;
