@@ -16,16 +16,17 @@ since the "vc" clamp rule depends on how all fibers of a rank are laid out toget
 """
 from __future__ import annotations
 
+import ctypes as C
 import heapq
 import threading
-import warnings
 from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
 
 from . import _native as N
 from . import output
-from .solver import CLAMP_RULES, FastMonodomainSolver, FiberSystem, equilibrium_states
+from .solver import (CLAMP_RULES, FastMonodomainSolver, FiberSystem, equilibrium_states, output_writers,
+                     piece_end, write_due_output)
 
 
 def lpt_partition(weights: Sequence[int], n_shards: int) -> List[np.ndarray]:
@@ -165,7 +166,9 @@ class ShardedSolver:
         self._start = system.start_time
         self._end = system.end_time
         self._log_on = False
-        self._warned_writers = False
+        self._writers = None
+        self._current_time = system.start_time
+        self._piece_steps = 0
         #: result of the "initializeStatesToEquilibrium" search, when the settings ask for it
         self.equilibrium = None
 
@@ -257,12 +260,63 @@ class ShardedSolver:
         return self._end
 
     def advanceTimeSpan(self, withOutputWritersEnabled: bool = True):
-        if withOutputWritersEnabled and self.system.output_writers and not self._warned_writers:
-            # the shards advance without the settings' output writers; states() gathers the whole system's
-            # fibers for output.write_fibers
-            warnings.warn("ShardedSolver runs no OutputWriter of the settings (use states() and output.write_fibers)")
-            self._warned_writers = True
-        self._each(lambda k, sv: sv.advanceTimeSpan(withOutputWritersEnabled))
+        """Every shard advances over [startTime, endTime].  With the settings' output writers (enabled) the shards
+        stop together after each RepeatedCall piece whose call writes, and the writers get the whole system's
+        fibers (as FastMonodomainSolver.advanceTimeSpan, fast_monodomain_solver_compute.tpp:35-44)."""
+        self.initialize()
+        live = [sv for sv in self.shards if sv is not None]
+        if not live:
+            return
+        writers = self._output_writers() if withOutputWritersEnabled else []
+        n, steps = self._plan(live[0])
+        if not writers:
+            self._each(lambda k, sv: sv.advanceTimeSpan(withOutputWritersEnabled))
+        else:
+            self._each(lambda k, sv: sv._prepare_advance())
+            done = 0
+            for k in range(n):
+                t = piece_end(self._start, self._end, k, n)
+                due = [(w, name) for w in writers for name in [w.prepare(0, t, int(steps[k]))] if name]
+                self._current_time, self._piece_steps = t, int(steps[k])
+                if due:
+                    k0, k1 = done, k + 1
+                    self._each(lambda j, sv: sv._advance_pieces(k0, k1))
+                    done = k1
+                    write_due_output(self, due, t)
+            if done < n:
+                k0 = done
+                self._each(lambda j, sv: sv._advance_pieces(k0, n))
+        self._current_time = piece_end(self._start, self._end, n - 1, n)
+        self._piece_steps = int(steps[n - 1])
+
+    def _plan(self, sv):
+        """The RepeatedCall pieces of the span and their split steps (every shard plans alike)."""
+        nn = C.c_int64()
+        N.check(N.lib().fdm_repeated_call_plan(sv._h, self._start, self._end, C.byref(nn), None), sv._h)
+        steps = np.zeros(max(nn.value, 1), np.int32)
+        if self.system.output_writers:
+            N.check(N.lib().fdm_repeated_call_plan(sv._h, self._start, self._end, C.byref(nn),
+                                                   N.ptr(steps, C.c_int)), sv._h)
+        return nn.value, steps
+
+    def _output_writers(self):
+        if self._writers is None:
+            self._writers = output_writers(self.system)
+        return self._writers
+
+    def callOutputWriter(self, timeStepNo: int, currentTime: float, callCountIncrement: int = 1):
+        """FastMonodomainSolver.callOutputWriter over the whole system."""
+        self.initialize()
+        if int(timeStepNo) % int(callCountIncrement) != 0:
+            return
+        due = [(w, name) for w in self._output_writers()
+               for name in [w.prepare(0, self._current_time, self._piece_steps)] if name]
+        if due:
+            write_due_output(self, due, self._current_time)
+
+    def compute_state_information(self) -> np.ndarray:
+        r = self._each(lambda k, sv: sv.compute_state_information()[None, :])
+        return self._gather_rows(r, 1)[0]
 
     def run(self):
         self.initialize()

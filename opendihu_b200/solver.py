@@ -350,6 +350,49 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     return sys_
 
 
+def piece_end(start: float, end: float, k: int, n: int) -> float:
+    """End of RepeatedCall piece k of n over [start, end] (the Strang span's endTime, the reference's
+    currentTime_): start + k/n*span + span/n, as repeated_call.tpp:59-70 forms it."""
+    span = end - start
+    t = start if k == 0 else start + k / n * span
+    return t + span / n
+
+
+def output_writers(system: FiberSystem) -> list:
+    """The settings' output writers of a system (output.OutputWriter, fibers named by their meshes)."""
+    names = list(system.fiber_mesh_names)
+    return [output.OutputWriter(w, fibers, [names[f] if f < len(names) and names[f] else f"MeshFiber_{f}"
+                                            for f in fibers])
+            for w, fibers in system.output_writers]
+
+
+def write_due_output(solver, due, current_time: float) -> None:
+    """The diffusion data of the fibers each due writer covers, read through the solver's vm(), algebraics()
+    and compute_state_information(): geometry (cumulative element lengths along x), "solution" (Vm) and
+    additionalFieldVariable<k> (algebraicsForTransfer, then the computeStateInformation slot;
+    fast_monodomain_solver_communication.tpp:437-488)."""
+    s = solver.system
+    vm = solver.vm()
+    extra = []
+    if len(s.algebraics_for_transfer):
+        extra += list(solver.algebraics())
+    if s.compute_state_information:
+        extra.append(solver.compute_state_information())
+    n_add = max(int(s.n_additional_field_variables), len(extra))
+    off = np.asarray(s.fiber_offsets, np.int64)
+    elem = np.asarray(s.element_lengths)
+    for w, name in due:
+        dicts = []
+        for f in w.fibers:
+            a, b = int(off[f]), int(off[f + 1])
+            x = np.concatenate([[0.0], np.cumsum(elem[a - f:b - f - 1])])
+            geom = np.stack([x, np.zeros_like(x), np.zeros_like(x)], axis=1)
+            add = {f"additionalFieldVariable{k}": (extra[k][a:b] if k < len(extra) else np.zeros(b - a))
+                   for k in range(n_add)}
+            dicts.append(output.fiber_dict({"0": vm[a:b]}, geom, 0, current_time, "solution", add))
+        w.write(name, dicts)
+
+
 def equilibrium_states(system: FiberSystem, device: int = 0) -> Dict[str, object]:
     """The CellmlAdapter's equilibrium search (03_cellml_adapter.tpp:445-515) for the first node: its initial
     states (the settings' statesInitialValues or the model's) and parameters, RK4 with the settings' time step
@@ -610,8 +653,7 @@ class FastMonodomainSolver:
         self.initialize()
         writers = self._output_writers() if withOutputWritersEnabled else []
         L = N.lib()
-        if self._log_on:
-            self._grow_stimulation_log(self._end - self._start)
+        self._prepare_advance()
         n = C.c_int64()
         self._call(L.fdm_repeated_call_plan, self._start, self._end, C.byref(n), None)
         steps = np.zeros(max(n.value, 1), np.int32)
@@ -699,44 +741,23 @@ class FastMonodomainSolver:
         return name
 
     def _piece_end(self, k: int, n: int) -> float:
-        """End of RepeatedCall piece k of n over [startTime, endTime] (the Strang span's endTime, the
-        reference's currentTime_): start + k/n*span + span/n, as repeated_call.tpp:59-70 forms it."""
-        span = self._end - self._start
-        t = self._start if k == 0 else self._start + k / n * span
-        return t + span / n
+        return piece_end(self._start, self._end, k, n)
 
     def _output_writers(self):
         if self._writers is None:
-            names = list(self.system.fiber_mesh_names)
-            self._writers = [output.OutputWriter(w, fibers, [names[f] if f < len(names) and names[f] else
-                                                           f"MeshFiber_{f}" for f in fibers])
-                             for w, fibers in self.system.output_writers]
+            self._writers = output_writers(self.system)
         return self._writers
 
     def _write_output(self, due):
-        """The diffusion data of the fibers each due writer covers: geometry (cumulative element lengths along
-        x), "solution" (Vm) and additionalFieldVariable<k> (algebraicsForTransfer, then the
-        computeStateInformation slot; fast_monodomain_solver_communication.tpp:437-488)."""
-        s = self.system
-        vm = self.vm()
-        extra = []
-        if len(s.algebraics_for_transfer):
-            extra += list(self.algebraics())
-        if s.compute_state_information:
-            extra.append(self.compute_state_information())
-        n_add = max(int(s.n_additional_field_variables), len(extra))
-        off = np.asarray(s.fiber_offsets, np.int64)
-        elem = np.asarray(s.element_lengths)
-        for w, name in due:
-            dicts = []
-            for f in w.fibers:
-                a, b = int(off[f]), int(off[f + 1])
-                x = np.concatenate([[0.0], np.cumsum(elem[a - f:b - f - 1])])
-                geom = np.stack([x, np.zeros_like(x), np.zeros_like(x)], axis=1)
-                add = {f"additionalFieldVariable{k}": (extra[k][a:b] if k < len(extra) else np.zeros(b - a))
-                       for k in range(n_add)}
-                dicts.append(output.fiber_dict({"0": vm[a:b]}, geom, 0, self._current_time, "solution", add))
-            w.write(name, dicts)
+        write_due_output(self, due, self._current_time)
+
+    def _prepare_advance(self):
+        """What an advance over [startTime, endTime] needs first: room in the stimulation log."""
+        if self._log_on:
+            self._grow_stimulation_log(self._end - self._start)
+
+    def _advance_pieces(self, k_begin: int, k_end: int):
+        self._call(N.lib().fdm_advance_pieces, self._start, self._end, k_begin, k_end)
 
     def advance_async(self):
         """advanceTimeSpan without waiting for the device (``wait`` completes it: timing, the NaN check)."""

@@ -27,6 +27,7 @@ class FakeLib:
         self.log_t = np.zeros(0)
         self.log_f = np.zeros(0, np.int32)
         self.n_of = {}                     # nodes per solver handle (from fdm_set_fibers)
+        self.done_of = {}                  # RepeatedCall pieces advanced per solver handle
 
     def __getattr__(self, name):
         def call(*args):
@@ -74,16 +75,16 @@ class FakeLib:
 
     def fdm_advance(self, h, t0, t1):
         self.calls.append(("fdm_advance", t0, t1))
-        self.pieces_done += self._n(t0, t1)
+        self.done_of[h.value] = self.done_of.get(h.value, 0) + self._n(t0, t1)
         return 0
 
     def fdm_advance_pieces(self, h, t0, t1, k0, k1):
         self.calls.append(("fdm_advance_pieces", k0, k1))
-        self.pieces_done += k1 - k0
+        self.done_of[h.value] = self.done_of.get(h.value, 0) + k1 - k0
         return 0
 
     def fdm_get_vm(self, h, out):
-        np.ctypeslib.as_array(out, (self.n_of[h.value],))[:] = self.pieces_done
+        np.ctypeslib.as_array(out, (self.n_of[h.value],))[:] = self.done_of.get(h.value, 0)
         return 0
 
     def fdm_get_stimulation_log(self, h, n, t, f):
@@ -230,12 +231,27 @@ def test_sharded_solver_merges_the_logs_and_searches_the_equilibrium_once(fake, 
     assert lines[1:] == [f"{s.motor_unit_no[f]};{f};0;" for f in first]
 
 
-def test_sharded_solver_warns_that_it_runs_no_output_writers(fake):
+def test_sharded_solver_runs_the_writers_over_the_whole_system(fake):
     from opendihu_b200 import sharding as SH
-    s = H.complete(H.c1_system(n_fibers=2, n_nodes=11, end_time=0.01))
-    s.output_writers = [({"format": "PythonCallback", "callback": lambda d: None}, [0, 1])]
-    fake(s)
+    s = H.complete(H.c1_system(n_fibers=3, n_nodes=11, end_time=0.01))
+    got = []
+    s.output_writers = [({"format": "PythonCallback", "callback": got.append, "outputInterval": 4}, [0, 1, 2])]
+    lib = fake(s)
     sh = SH.ShardedSolver(s, devices=[0], n_shards=2)
-    with pytest.warns(UserWarning, match="no OutputWriter"):
-        sh.advanceTimeSpan()
+    sh.advanceTimeSpan()
+    # both shards stop after pieces 4 and 8 and finish the span; the writer sees all three fibers each time
+    adv = [c[1:] for c in lib.calls if c[0] == "fdm_advance_pieces"]
+    assert sorted(adv) == sorted([(0, 4), (4, 8), (8, 10)] * 2)
+    assert [len(x) for x in got] == [3, 3]
+    assert [[d["data"][1]["components"][0]["values"][0] for d in x] for x in got] == [[4.0] * 3, [8.0] * 3]
+    np.testing.assert_allclose([x[0]["currentTime"] for x in got], [0.004, 0.008], rtol=1e-12)
+    # callOutputWriter continues the count with the last piece's step: calls 11 and 12 write at 12
+    sh.callOutputWriter(0, 0.0)
+    sh.callOutputWriter(0, 0.0)
+    assert len(got) == 3 and got[-1][0]["currentTime"] == pytest.approx(0.01)
+    # writers off: one advance per shard
+    lib.calls.clear()
+    sh.setTimeSpan(0.01, 0.02)
+    sh.advanceTimeSpan(withOutputWritersEnabled=False)
+    assert [c for c in lib.calls if c[0].startswith("fdm_advance")] == [("fdm_advance", 0.01, 0.02)] * 2
     sh.close()
