@@ -2,7 +2,8 @@
 // drive its FastMonodomainSolver: settings in, setTimeSpan/advanceTimeSpan twice with a checkpoint between,
 // the checkpoint replayed, the states and the transferred algebraics written out.
 //   host_class_main <settings file> <output file> <intermediate time>
-// With a fifth argument it instead advances [startTime, endTime] once: "log" records the stimulation log and
+// With a fifth argument "settings" it only writes what FiberSettings::load read (no device needed).
+// With a fifth argument it otherwise advances [startTime, endTime] once: "log" records the stimulation log and
 // writes it to the output file in the reference's format; a number is the outputInterval of an output writer
 // whose callback writes one line per call (numbered name, current time, Vm sum) to the output file, and
 // callOutputWriter(0, 0) is called once more.
@@ -22,6 +23,24 @@ int main(int argc, char** argv)
   }
   try {
     fdm::FiberSettings s = fdm::FiberSettings::load(argv[1]);
+    if (argc == 5 && std::string(argv[4]) == "settings") { // host only: what FiberSettings::load read
+      std::FILE* f = std::fopen(argv[2], "w");
+      if (!f)
+        return 1;
+      std::fprintf(f, "n_fibers %d\nn_nodes %lld\nequilibrium %d %.17g\nfiber_numbers", s.n_fibers(),
+                   (long long)s.n_nodes(), (int)s.initialize_states_to_equilibrium, s.equilibrium_dt);
+      for (int x : s.fiber_numbers)
+        std::fprintf(f, " %d", x);
+      std::fprintf(f, "\nstates_for_transfer");
+      for (int x : s.states_for_transfer)
+        std::fprintf(f, " %d", x);
+      std::fprintf(f, "\nalgebraics_for_transfer");
+      for (int x : s.algebraics_for_transfer)
+        std::fprintf(f, " %d", x);
+      std::fprintf(f, "\n");
+      std::fclose(f);
+      return 0;
+    }
     if (argc == 5 && std::string(argv[4]) == "log") {
       fdm::FastMonodomainSolver slv(s);
       slv.enableStimulationLog();

@@ -41,6 +41,26 @@ def test_builds_reads_settings_and_fails_loudly_without_device(tmp_path):
     assert r.returncode == 2 and "cannot open" in r.stderr
 
 
+def test_settings_file_round_trip(tmp_path):
+    # what write_host_settings writes from a parsed system is what FiberSettings::load reads (host only)
+    exe = _build(tmp_path)
+    s = _system()
+    s.fiber_numbers = [7, 8, 9]
+    s.initialize_states_to_equilibrium = True
+    s.equilibrium_dt = 2.5e-4
+    cfg = str(tmp_path / "settings.txt")
+    S.write_host_settings(s, cfg)
+    out = str(tmp_path / "read.txt")
+    r = subprocess.run([exe, cfg, out, "0", "settings"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = dict(line.split(" ", 1) for line in open(out).read().splitlines())
+    assert got["n_fibers"] == "3" and got["n_nodes"] == str(s.n_nodes)
+    assert got["equilibrium"] == "1 0.00025000000000000001"
+    assert got["fiber_numbers"] == "7 8 9"
+    assert got["states_for_transfer"] == " ".join(str(x) for x in s.states_for_transfer)
+    assert got["algebraics_for_transfer"] == "0 4"
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("method,precision", [("split", "fp64"), ("fused", "fp32")])
 def test_cpp_host_class_equals_python_operator(tmp_path, method, precision):
