@@ -37,7 +37,7 @@ extern "C" {
 #define FDM_ERR_NAN 3          /* NaN or Inf in the transmembrane potential after an advance */
 #define FDM_ERR_UNSUPPORTED 4  /* combination not built into this library */
 #define FDM_ERR_NO_DEVICE 5    /* no CUDA device */
-#define FDM_ERR_TIMEOUT 6      /* a device-side wait gave up */
+#define FDM_ERR_TIMEOUT 6      /* a wait gave up before the device finished (fdm_wait_for) */
 
 #define FDM_MODEL_HODGKIN_HUXLEY_1952 0
 #define FDM_MODEL_SHORTEN_2007 1
@@ -174,6 +174,11 @@ int fdm_advance(fdm_solver *s, double t_start, double t_end);
  * advance waits first. */
 int fdm_advance_async(fdm_solver *s, double t_start, double t_end);
 int fdm_wait(fdm_solver *s);
+/* fdm_wait with a limit (no counterpart in the reference, whose calls block without one): polls the solver's
+ * stream for at most timeout_seconds; FDM_ERR_TIMEOUT if the advance is still running then (it stays enqueued
+ * and the solver usable: a later fdm_wait or fdm_wait_for completes it), otherwise as fdm_wait.  For callers
+ * that must notice a device that stopped making progress without blocking on it forever. */
+int fdm_wait_for(fdm_solver *s, double timeout_seconds);
 /* The RepeatedCall pieces of [t_start, t_end] (repeated_call.tpp:43-80: piece k is one call of
  * FastMonodomainSolver::advanceTimeSpan, after which the reference calls the diffusion's output writers,
  * fast_monodomain_solver_compute.tpp:35-44): their number, and, when steps_per_piece is not null, the number
@@ -189,11 +194,21 @@ int fdm_advance_pieces(fdm_solver *s, double t_start, double t_end, int64_t k_be
  * begins (its decision stimulates, its previous decision did not) is recorded as (time, fiber), up to capacity
  * entries.  A larger capacity keeps the entries recorded so far; 0 turns the log off and drops them. */
 int fdm_set_stimulation_log(fdm_solver *s, int64_t capacity);
-/* *n_total = entries recorded (including those past the capacity); times/fibers (may be null) receive the
- * first min(n_total, capacity), in the order they were recorded (fibers of one window in no fixed order) */
+/* *n_total = stimulation begins recorded; times/fibers (may be null) receive all n_total of them, in the order
+ * they were recorded (fibers of one window in no fixed order).  If more begins happened than the capacity
+ * held, *n_total still counts them all, nothing is copied and the call fails with FDM_ERR_ARG (the log is
+ * incomplete): grow the capacity before each advance to what its span can need.  With times and fibers both
+ * null the call only counts (it does not fail on an incomplete log). */
 int fdm_get_stimulation_log(fdm_solver *s, int64_t *n_total, double *times, int *fibers);
 /* number of split steps done by all advances so far */
 int64_t fdm_split_steps(const fdm_solver *s);
+/* Fault injection for tests (no counterpart in the reference): the k-th allocation of solver memory (device
+ * buffers and pinned host staging, any solver of this process) from now on fails as if the device were out of
+ * memory; k = 0 turns it off.  The call that meets the failure returns FDM_ERR_CUDA and leaves the solver safe:
+ * a failed fdm_set_fibers leaves it without fibers, a failed fdm_set_stimulation, fdm_set_trace,
+ * fdm_set_algebraics_for_transfer or fdm_checkpoint_save leaves that setting unset, a failed advance can be
+ * repeated; fdm_destroy always releases what was allocated. */
+int fdm_debug_fail_allocation(int64_t k);
 /* summed device time and count of the main kernel launches (config.profile = 1), and of all GPU work
  * of the advances */
 int fdm_get_timing(const fdm_solver *s, double *main_kernel_ms, int64_t *main_kernel_launches,
@@ -221,9 +236,11 @@ int fdm_diffusion_solve(int n_fibers, int64_t n_nodes, const int64_t *d_fiber_of
  * coupled code that has reserved HBM for its own mesh, a stepping loop that must not synchronize on
  * cudaMalloc/cudaFree).  The scratch is one array compiled into the library, sized for at most
  * FDM_NOALLOC_MAX_NODES nodes (14.7 MB held on every GPU that loads the library until the process exits);
- * larger n_nodes fail with FDM_ERR_ARG.  The first call on a device looks the array's address up; make it
- * before any stream capture.  All calls share the array: calls that overlap on the GPU race, so order them
- * on one stream.  Arguments and result as fdm_diffusion_solve. */
+ * larger n_nodes fail with FDM_ERR_ARG.  The fiber offsets index that array: they must not decrease and must
+ * lie in [0, n_nodes] (d_fiber_offsets[n_fibers] <= n_nodes); the call reads their first and last entry back
+ * and fails with FDM_ERR_ARG when either end is outside.  The first call on a device looks the array's
+ * address up; make it before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * race, so order them on one stream.  Arguments and result as fdm_diffusion_solve. */
 #define FDM_NOALLOC_MAX_NODES 262144
 int fdm_diffusion_solve_noalloc(int n_fibers, int64_t n_nodes, const int64_t *d_fiber_offsets,
                                 const double *d_element_lengths, const double *d_prefactor, double dt,

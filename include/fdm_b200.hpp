@@ -307,9 +307,20 @@ class FastMonodomainSolver {
   void advanceTimeSpanAsync()
   {
     initialize();
+    if (log_on_)
+      grow_stimulation_log(end_ - start_);
     check(fdm_advance_async(h_, start_, end_));
   }
   void wait() { check(fdm_wait(h_)); }
+  /* wait() for at most timeoutSeconds: true once the advance is complete, false while it still runs */
+  bool waitFor(double timeoutSeconds)
+  {
+    const int rc = fdm_wait_for(h_, timeoutSeconds);
+    if (rc == FDM_ERR_TIMEOUT)
+      return false;
+    check(rc);
+    return true;
+  }
 
   void setTimeSpan(double startTime, double endTime)
   {

@@ -33,12 +33,12 @@ EXPORTED = [
     "fdm_adjoint_backward", "fdm_adjoint_release", "fdm_adjoint_timing", "fdm_rewind", "fdm_set_clamp_nodes",
     "fdm_select_clamp_nodes", "fdm_select_gate_codes", "fdm_set_gate_codes", "fdm_get_equilibrium_state",
     "fdm_cellml_rhs_device", "fdm_cellml_rhs_configure", "fdm_fused_cluster_shapes", "fdm_fused_layout",
-    "fdm_get_compute_state_information", "fdm_advance_async", "fdm_wait", "fdm_repeated_call_plan",
+    "fdm_get_compute_state_information", "fdm_advance_async", "fdm_wait", "fdm_wait_for", "fdm_repeated_call_plan",
     "fdm_advance_pieces", "fdm_set_stimulation_log", "fdm_get_stimulation_log",
     "fdm_model_equilibrium", "fdm_emg_set_preconditioner", "fdm_emg_create", "fdm_emg_destroy", "fdm_emg_last_error",
     "fdm_emg_potential_flow", "fdm_emg_set_direction", "fdm_emg_set_conductivity", "fdm_emg_set_fiber_mapping",
     "fdm_emg_map_fibers", "fdm_emg_map_values", "fdm_emg_set_vm", "fdm_emg_solve", "fdm_emg_get",
-    "fdm_emg_get_stencil", "fdm_emg_timing",
+    "fdm_emg_get_stencil", "fdm_emg_timing", "fdm_debug_fail_allocation",
 ]
 
 #: fdm_emg_get fields of include/fdm_b200.h
@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
         "fdm_advance": (C.c_int, [P, C.c_double, C.c_double]),
         "fdm_advance_async": (C.c_int, [P, C.c_double, C.c_double]),
         "fdm_wait": (C.c_int, [P]),
+        "fdm_wait_for": (C.c_int, [P, C.c_double]),
+        "fdm_debug_fail_allocation": (C.c_int, [C.c_int64]),
         "fdm_repeated_call_plan": (C.c_int, [P, C.c_double, C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
         "fdm_advance_pieces": (C.c_int, [P, C.c_double, C.c_double, C.c_int64, C.c_int64]),
         "fdm_set_stimulation_log": (C.c_int, [P, C.c_int64]),

@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -60,6 +62,35 @@ struct Tss {
   }
 };
 
+// Allocation-failure hook (fdm_debug_fail_allocation): the countdown-th allocation of a solver buffer from
+// the moment it is set fails as if the device were out of memory; 0 = off.
+std::atomic<int64_t> g_fail_countdown{0};
+
+bool injected_allocation_failure()
+{
+  int64_t c = g_fail_countdown.load();
+  while (c > 0) {
+    if (g_fail_countdown.compare_exchange_weak(c, c - 1))
+      return c == 1;
+  }
+  return false;
+}
+
+// device memory of the solver handles (pinned host staging: pinned_alloc); both honour the hook
+cudaError_t device_alloc(void** p, size_t bytes)
+{
+  if (injected_allocation_failure())
+    return cudaErrorMemoryAllocation;
+  return cudaMalloc(p, bytes);
+}
+
+cudaError_t pinned_alloc(void** p, size_t bytes)
+{
+  if (injected_allocation_failure())
+    return cudaErrorMemoryAllocation;
+  return cudaMallocHost(p, bytes);
+}
+
 template<class T>
 struct DevBuf {
   T* p = nullptr;
@@ -74,7 +105,7 @@ struct DevBuf {
     n = 0;
     if (count == 0)
       count = 1;
-    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    cudaError_t e = device_alloc((void**)&p, count * sizeof(T));
     if (e == cudaSuccess)
       n = count;
     return e;
@@ -151,6 +182,7 @@ struct fdm_solver {
   DevBuf<int> log_f;
   DevBuf<unsigned long long> log_n;
   int64_t log_cap = 0;
+  int64_t log_dropped = 0;  // begins counted past the capacity before the log last grew (not stored)
   DevBuf<int> mu;
   DevBuf<double> freq, repeat, begin, jitter, last_check, cur_jitter;
   DevBuf<int> jitter_idx;
@@ -454,7 +486,7 @@ extern "C" int fdm_create(const fdm_config* cfg, fdm_solver** out)
     s->adjoint_tape = std::atoi(env) != 0;
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess)
-    e = cudaMallocHost((void**)&s->steps_h, sizeof(SplitStep) * 2 * s->cfg.steps_per_launch);
+    e = pinned_alloc((void**)&s->steps_h, sizeof(SplitStep) * 2 * s->cfg.steps_per_launch);
   if (e == cudaSuccess)
     e = cudaEventCreateWithFlags(&s->slot_ev[0], cudaEventDisableTiming);
   if (e == cudaSuccess)
@@ -507,6 +539,7 @@ extern "C" int fdm_destroy(fdm_solver* s)
   s->log_f.release();
   s->log_n.release();
   s->log_cap = 0;
+  s->log_dropped = 0;
   s->flags.release();
   s->steps_d.release();
   s->adj.release();
@@ -658,8 +691,8 @@ static int upload_gate(fdm_solver* s);
 static int eq_copy_pad_params(fdm_solver* s);
 static int eq_reset(fdm_solver* s);
 
-extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_offsets,
-                              const double* element_lengths, const double* prefactor)
+static int set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_offsets, const double* element_lengths,
+                      const double* prefactor)
 {
   if (!s || n_fibers < 0 || (n_fibers > 0 && (!fiber_offsets || !element_lengths || !prefactor)))
     return fail(s, FDM_ERR_ARG, "fdm_set_fibers: bad argument");
@@ -782,6 +815,34 @@ extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_
   return FDM_OK;
 }
 
+// A failed fdm_set_fibers (a bad argument, a failed allocation) leaves the solver without fibers: its buffers
+// may be partly released, so nothing may run on them until fdm_set_fibers succeeds.
+extern "C" int fdm_set_fibers(fdm_solver* s, int n_fibers, const int64_t* fiber_offsets,
+                              const double* element_lengths, const double* prefactor)
+{
+  const int rc = set_fibers(s, n_fibers, fiber_offsets, element_lengths, prefactor);
+  if (rc != FDM_OK && s) {
+    s->n_fibers = 0;
+    s->n_nodes = 0;
+    s->max_fiber_len = 0;
+    s->off.assign(1, 0);
+    s->elem_off.assign(1, 0);
+    s->prefactor.clear();
+    s->n_bins = 0;
+    s->bin_start.assign(1, 0);
+    s->bin_fibers.clear();
+    s->stimulation_set = false;
+    s->gate_set = false;
+    s->ck_valid = false;
+    s->eq.on = false;
+    s->n_alg_out = 0;
+    s->n_trace = 0;
+    s->trace_capacity = 0;
+    s->coef_valid = false;
+  }
+  return rc;
+}
+
 extern "C" int fdm_set_prefactor(fdm_solver* s, const double* prefactor)
 {
   if (!s || !prefactor)
@@ -827,7 +888,7 @@ static cudaError_t ensure_stage(fdm_solver* s, size_t bytes)
     cudaFreeHost(s->stage);
   s->stage = nullptr;
   s->stage_bytes = 0;
-  cudaError_t e = cudaMallocHost(&s->stage, bytes);
+  cudaError_t e = pinned_alloc(&s->stage, bytes);
   if (e == cudaSuccess)
     s->stage_bytes = bytes;
   return e;
@@ -1149,6 +1210,7 @@ extern "C" int fdm_select_clamp_nodes(int clamp_rule, int vc_width, int n_ranks,
 
 static int upload_gate(fdm_solver* s)
 {
+  s->gate_set = false;
   FDM_CUDA(s->gate.alloc((size_t)std::max<int64_t>(s->n_nodes, 1)));
   FDM_CUDA(cudaMemcpyAsync(s->gate.p, s->gate_h.data(), sizeof(int) * s->n_nodes, cudaMemcpyHostToDevice, s->stream));
   FDM_CUDA(cudaStreamSynchronize(s->stream));
@@ -1207,6 +1269,7 @@ static int eq_reset(fdm_solver* s)
 static int eq_build(fdm_solver* s, const std::vector<int>& center)
 {
   auto& E = s->eq;
+  E.on = false;   // until every buffer below is in place
   const int W = s->cfg.vc_width, R = s->cfg.n_ranks, nf = s->n_fibers;
   const int64_t N = s->n_nodes;
   const int NS = s->model->n_states, NP = s->model->n_parameters;
@@ -1355,6 +1418,9 @@ extern "C" int fdm_set_stimulation(fdm_solver* s, const uint8_t* firing_events, 
                   "fdm_set_stimulation: setSpecificStatesCallFrequency is set but setSpecificStatesRepeatAfterFirstCall "
                   "is not (03_cellml_adapter.tpp:177-181)");
   }
+  s->stimulation_set = false;   // until every buffer below is in place
+  s->eq.on = false;
+  s->gate_set = false;
   s->firing_rows = rows;
   s->firing_cols = cols;
   s->n_jitter = n_jitter;
@@ -1542,7 +1608,7 @@ extern "C" int fdm_set_algebraics_for_transfer(fdm_solver* s, int n, const int* 
   for (int k = 0; k < n; k++)
     if (idx[k] < 0 || idx[k] >= s->model->n_algebraics)
       return fail(s, FDM_ERR_ARG, "fdm_set_algebraics_for_transfer: algebraic index out of range");
-  s->n_alg_out = n;
+  s->n_alg_out = 0;   // set once the buffers are in place
   FDM_CUDA(s->alg_idx.alloc(std::max(n, 1)));
   FDM_CUDA(s->alg_out.alloc(std::max<size_t>((size_t)n * s->n_nodes, 1)));
   if (n > 0) {
@@ -1550,6 +1616,7 @@ extern "C" int fdm_set_algebraics_for_transfer(fdm_solver* s, int n, const int* 
     FDM_CUDA(cudaMemsetAsync(s->alg_out.p, 0, sizeof(double) * n * s->n_nodes, s->stream));
   }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
+  s->n_alg_out = n;
   return FDM_OK;
 }
 
@@ -1580,8 +1647,8 @@ extern "C" int fdm_set_trace(fdm_solver* s, int n, const int64_t* nodes, int64_t
       return fail(s, FDM_ERR_ARG, "fdm_set_trace: duplicate node");
     slot[nodes[k]] = k;
   }
-  s->n_trace = n;
-  s->trace_capacity = n > 0 ? capacity : 0;
+  s->n_trace = 0;   // set once the buffers are in place
+  s->trace_capacity = 0;
   if (n > 0) {
     FDM_CUDA(s->trace_slot.alloc(s->n_nodes));
     FDM_CUDA(s->trace.alloc(std::max<size_t>((size_t)n * capacity, 1)));
@@ -1590,6 +1657,8 @@ extern "C" int fdm_set_trace(fdm_solver* s, int n, const int64_t* nodes, int64_t
     FDM_CUDA(cudaMemsetAsync(s->trace.p, 0, sizeof(double) * std::max<size_t>((size_t)n * capacity, 1), s->stream));
   }
   FDM_CUDA(cudaStreamSynchronize(s->stream));
+  s->n_trace = n;
+  s->trace_capacity = n > 0 ? capacity : 0;
   return FDM_OK;
 }
 
@@ -1651,7 +1720,8 @@ static int ensure_step_capacity(fdm_solver* s, int n)
   if (s->steps_h)
     FDM_CUDA(cudaFreeHost(s->steps_h));
   s->steps_h = nullptr;
-  FDM_CUDA(cudaMallocHost((void**)&s->steps_h, sizeof(SplitStep) * 2 * (size_t)n));
+  s->step_capacity = 0;   // until both buffers are in place
+  FDM_CUDA(pinned_alloc((void**)&s->steps_h, sizeof(SplitStep) * 2 * (size_t)n));
   FDM_CUDA(s->steps_d.alloc(n));
   s->step_capacity = n;
   return FDM_OK;
@@ -2013,13 +2083,20 @@ static int run_planned(fdm_solver* s, const std::vector<SplitStep>& steps, const
   return FDM_OK;
 }
 
-static int finish_advance(fdm_solver* s)
+// the end of an advance's device work: its stop event and the count of non-finite Vm values, enqueued behind it
+static int enqueue_finish(fdm_solver* s)
 {
   FDM_CUDA(cudaEventRecord(s->adv_stop, s->stream));
   if (s->cfg.check_nan && s->n_nodes > 0) {
     FDM_CUDA(cudaMemsetAsync(s->nonfinite.p, 0, sizeof(int), s->stream));
     FDM_CUDA(launch_count_nonfinite(s->vm.p, s->n_nodes, s->nonfinite.p, s->stream));
   }
+  return FDM_OK;
+}
+
+// waits for the advance's device work, then adds up its timing and reads the non-finite count
+static int complete_finish(fdm_solver* s)
+{
   FDM_CUDA(cudaStreamSynchronize(s->stream));
   float ms = 0;
   FDM_CUDA(cudaEventElapsedTime(&ms, s->adv_start, s->adv_stop));
@@ -2039,6 +2116,12 @@ static int finish_advance(fdm_solver* s)
   return FDM_OK;
 }
 
+static int finish_advance(fdm_solver* s)
+{
+  const int r = enqueue_finish(s);
+  return r ? r : complete_finish(s);
+}
+
 extern "C" int fdm_wait(fdm_solver* s)
 {
   if (!s)
@@ -2047,7 +2130,32 @@ extern "C" int fdm_wait(fdm_solver* s)
     return FDM_OK;
   FDM_BIND(s);
   s->finish_pending = false;
-  return finish_advance(s);
+  return complete_finish(s);
+}
+
+extern "C" int fdm_wait_for(fdm_solver* s, double timeout_seconds)
+{
+  if (!s || !(timeout_seconds >= 0))
+    return fail(s, FDM_ERR_ARG, "fdm_wait_for: bad argument");
+  if (!s->finish_pending)
+    return FDM_OK;
+  FDM_BIND(s);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t q = cudaStreamQuery(s->stream);
+    if (q == cudaSuccess)
+      break;
+    if (q != cudaErrorNotReady) {
+      s->finish_pending = false;
+      return cuda_fail(s, q, "fdm_wait_for");
+    }
+    const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (waited >= timeout_seconds)
+      return fail(s, FDM_ERR_TIMEOUT, "fdm_wait_for: the advance is still running after " +
+                                          std::to_string(waited) + " s; it stays enqueued (fdm_wait completes it)");
+    std::this_thread::sleep_for(std::chrono::microseconds(waited < 1e-3 ? 20 : 200));
+  }
+  return fdm_wait(s);
 }
 
 // the work of an advance, enqueued on the solver's stream (the host waits only where the window buffers of
@@ -2083,7 +2191,10 @@ extern "C" int fdm_advance(fdm_solver* s, double t_start, double t_end)
 
 extern "C" int fdm_advance_async(fdm_solver* s, double t_start, double t_end)
 {
-  const int r = enqueue_advance(s, t_start, t_end, "fdm_advance_async");
+  int r = enqueue_advance(s, t_start, t_end, "fdm_advance_async");
+  if (r)
+    return r;
+  r = enqueue_finish(s);
   if (r)
     return r;
   s->finish_pending = true;
@@ -2155,6 +2266,15 @@ extern "C" int fdm_advance_pieces(fdm_solver* s, double t_start, double t_end, i
 
 extern "C" int64_t fdm_split_steps(const fdm_solver* s) { return s ? s->split_no : 0; }
 
+extern "C" int fdm_debug_fail_allocation(int64_t k)
+{
+  if (k < 0)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_debug_fail_allocation: k must be >= 0");
+  g_fail_countdown.store(k);
+  return FDM_OK;
+}
+
+
 extern "C" int fdm_set_stimulation_log(fdm_solver* s, int64_t capacity)
 {
   if (!s || capacity < 0)
@@ -2170,6 +2290,7 @@ extern "C" int fdm_set_stimulation_log(fdm_solver* s, int64_t capacity)
     s->log_f.release();
     s->log_n.release();
     s->log_cap = 0;
+    s->log_dropped = 0;
     return FDM_OK;
   }
   if (s->log_cap == 0) {
@@ -2187,8 +2308,22 @@ extern "C" int fdm_set_stimulation_log(fdm_solver* s, int64_t capacity)
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(f.p, s->log_f.p, sizeof(int) * s->log_cap, cudaMemcpyDeviceToDevice, s->stream);
     }
+    // the counter may have run past the old capacity (those begins were counted, not stored): the new
+    // entries must follow the stored ones, so the counter restarts at the stored count and the excess is
+    // kept aside, where fdm_get_stimulation_log reports it
+    unsigned long long n = 0;
+    if (e == cudaSuccess && s->log_cap > 0)
+      e = cudaMemcpyAsync(&n, s->log_n.p, sizeof(n), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess)
       e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess && n > (unsigned long long)s->log_cap) {
+      const unsigned long long stored = (unsigned long long)s->log_cap;
+      e = cudaMemcpyAsync(s->log_n.p, &stored, sizeof(stored), cudaMemcpyHostToDevice, s->stream);
+      if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s->stream);
+      if (e == cudaSuccess)
+        s->log_dropped += (int64_t)(n - stored);
+    }
     if (e != cudaSuccess) { // the log stays as it was
       t.release();
       f.release();
@@ -2221,8 +2356,15 @@ extern "C" int fdm_get_stimulation_log(fdm_solver* s, int64_t* n_total, double* 
   unsigned long long n = 0;
   FDM_CUDA(cudaMemcpyAsync(&n, s->log_n.p, sizeof(n), cudaMemcpyDeviceToHost, s->stream));
   FDM_CUDA(cudaStreamSynchronize(s->stream));
-  *n_total = (int64_t)n;
-  const size_t k = (size_t)std::min<unsigned long long>(n, (unsigned long long)s->log_cap);
+  *n_total = (int64_t)n + s->log_dropped;
+  if (!times && !fibers)
+    return FDM_OK;
+  if (*n_total > s->log_cap)
+    return fail(s, FDM_ERR_ARG, "fdm_get_stimulation_log: " + std::to_string(*n_total) +
+                                    " stimulation begins were recorded but the log holds only " +
+                                    std::to_string(s->log_cap) + "; the log is incomplete (grow its capacity "
+                                    "before each advance)");
+  const size_t k = (size_t)n;
   if (k > 0 && times)
     FDM_CUDA(cudaMemcpyAsync(times, s->log_t.p, sizeof(double) * k, cudaMemcpyDeviceToHost, s->stream));
   if (k > 0 && fibers)
@@ -2267,6 +2409,8 @@ extern "C" int fdm_checkpoint_save(fdm_solver* s)
   const int64_t N = s->n_nodes;
   const int NS = s->model->n_states;
   const int nf = s->n_fibers;
+  s->ck_valid = false;   // until the snapshot below is complete
+  s->eq.ck_valid = false;
   FDM_CUDA(s->ck_vm.alloc(std::max<int64_t>(N, 1)));
   FDM_CUDA(s->ck_states.alloc((size_t)std::max<int64_t>(N, 1) * std::max(NS - 1, 1) * s->real_bytes));
   FDM_CUDA(s->ck_last.alloc(std::max(nf, 1)));

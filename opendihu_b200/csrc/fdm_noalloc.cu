@@ -77,6 +77,22 @@ extern "C" int fdm_diffusion_solve_noalloc(int n_fibers, int64_t n_nodes, const 
     scratch = g_addr[dev];
   }
   cudaStream_t st = (cudaStream_t)stream;
+  // The kernels find each fiber's nodes through the device offsets and write the scratch at those nodes, so
+  // the offsets must stay inside [0, n_nodes]: their two ends are read back and checked (two 8-byte copies
+  // into host stack variables, no allocation); that they do not decrease in between is the caller's part.
+  int64_t ends[2] = {0, 0};
+  e = cudaMemcpyAsync(&ends[0], d_fiber_offsets, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&ends[1], d_fiber_offsets + n_fibers, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess)
+    return fdm_report_error(FDM_ERR_CUDA, std::string("fdm_diffusion_solve_noalloc: reading the fiber offsets: ") +
+                                              cudaGetErrorString(e));
+  if (ends[0] < 0 || ends[1] < ends[0] || ends[1] > n_nodes)
+    return fdm_report_error(FDM_ERR_ARG, "fdm_diffusion_solve_noalloc: fiber offsets [" + std::to_string(ends[0]) +
+                                             ", " + std::to_string(ends[1]) + "] outside [0, n_nodes = " +
+                                             std::to_string(n_nodes) + "]");
   double* coef = scratch;
   double* fwd = scratch + 6 * (size_t)n_nodes;
   e = fdm::launch_coefficients(n_fibers, d_fiber_offsets, d_element_lengths, d_prefactor, dt,

@@ -721,7 +721,7 @@ class FastMonodomainSolver:
         t = np.zeros(max(n.value, 1))
         f = np.zeros(max(n.value, 1), np.int32)
         self._call(N.lib().fdm_get_stimulation_log, C.byref(n), N.ptr(t, C.c_double), N.ptr(f, C.c_int))
-        k = min(n.value, len(t))
+        k = n.value  # the library fails (FDM_ERR_ARG) rather than return an incomplete log
         t, f = t[:k], f[:k]
         order = np.lexsort((f, t))
         t, f = t[order], f[order]
@@ -762,10 +762,20 @@ class FastMonodomainSolver:
     def advance_async(self):
         """advanceTimeSpan without waiting for the device (``wait`` completes it: timing, the NaN check)."""
         self.initialize()
+        self._prepare_advance()
         self._call(N.lib().fdm_advance_async, self._start, self._end)
 
     def wait(self):
         self._call(N.lib().fdm_wait)
+
+    def wait_for(self, timeout_s: float) -> bool:
+        """``wait`` for at most ``timeout_s`` seconds: True once the advance is complete, False if it is still
+        running (it stays enqueued; a later ``wait``/``wait_for`` completes it)."""
+        rc = N.lib().fdm_wait_for(self._h, float(timeout_s))
+        if rc == N.FDM_ERR_TIMEOUT:
+            return False
+        N.check(rc, self._h)
+        return True
 
     def run(self):
         self.initialize()

@@ -91,3 +91,47 @@ def test_stimulation_log_file_from_settings(tmp_path):
     expect = [f"{m};{f};" + "".join(f"{t:g};" for t in log["time"][log["fiber"] == f])
               for m, f in sorted({(int(m), int(f)) for m, f in zip(log["motorUnit"], log["fiber"])})]
     assert lines[1:] == expect
+
+
+@pytest.mark.parametrize("method,precision", [("split", "fp64"), ("fused", "fp32")])
+def test_stimulation_log_over_async_advances_equals_oracle(method, precision):
+    """advance_async grows the log before it enqueues, as the blocking advance does: two asynchronous advances
+    from a capacity of one entry record every begin of the oracle."""
+    s = _system()
+    t_ref, f_ref = _oracle_log(s)
+    with S.FastMonodomainSolver(s.copy(), method=method, precision=precision, steps_per_launch=100) as slv:
+        slv.enable_stimulation_log(capacity=1)
+        slv._call(S.N.lib().fdm_set_stimulation_log, 1)   # shrink back to one entry: the growth must come
+        slv.setTimeSpan(0.0, 5.0)                           # from the asynchronous advances themselves
+        slv.advance_async()
+        slv.wait()
+        slv.setTimeSpan(5.0, 12.0)
+        slv.advance_async()
+        slv.wait()
+        log = slv.stimulation_log()
+    np.testing.assert_array_equal(log["fiber"], f_ref)
+    np.testing.assert_allclose(log["time"], t_ref, rtol=0, atol=1e-12)
+
+
+def test_stimulation_log_never_returns_an_incomplete_log():
+    """A capacity too small for the span (the growth before the advance bypassed): the count still counts every
+    begin, but reading the entries fails loudly instead of returning unwritten records."""
+    import ctypes as C
+    s = _system()
+    t_ref, _ = _oracle_log(s)
+    L = S.N.lib()
+    with S.FastMonodomainSolver(s.copy(), method="split", precision="fp64", steps_per_launch=100) as slv:
+        slv.initialize()
+        slv._call(L.fdm_set_stimulation_log, 3)
+        slv._call(L.fdm_advance, 0.0, 12.0)            # the C ABI directly: no growth before the advance
+        n = C.c_int64()
+        slv._call(L.fdm_get_stimulation_log, C.byref(n), None, None)
+        assert n.value == len(t_ref)
+        with pytest.raises(RuntimeError, match="incomplete"):
+            slv.stimulation_log()
+        # growing the log afterwards keeps the three stored entries and the dropped count
+        slv._call(L.fdm_set_stimulation_log, 1000)
+        slv._call(L.fdm_get_stimulation_log, C.byref(n), None, None)
+        assert n.value == len(t_ref)
+        with pytest.raises(RuntimeError, match="incomplete"):
+            slv.stimulation_log()

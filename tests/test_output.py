@@ -9,7 +9,9 @@ import pytest
 import helpers as H
 from opendihu_b200 import output
 
-REF_READER = os.path.join(os.environ.get("OPENDIHU_REFERENCE", "/root/reference"), "testing/unit_testing/src/py_reader.py")
+#: the reference's reader, where a run names the checkout ($OPENDIHU_REFERENCE); skipped otherwise
+REF = os.environ.get("OPENDIHU_REFERENCE", "")
+REF_READER = os.path.join(REF, "testing/unit_testing/src/py_reader.py") if REF else ""
 
 
 @pytest.mark.parametrize("binary", [False, True])
