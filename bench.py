@@ -47,10 +47,13 @@ def parse_args():
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
     p.add_argument("--skip-emg", action="store_true")
-    p.add_argument("--only", choices=["emg", "emg-cg", "shorten", "plain", "adjoint"],
+    p.add_argument("--only", choices=["emg", "emg-cg", "shorten", "plain", "adjoint", "c2-accuracy"],
                    help="print one side measurement alone (profiling runs)")
+    p.add_argument("--accuracy-ms", type=float, default=100.0, help="span of the batch accuracy comparison")
     p.add_argument("--skip-shorten", action="store_true")
-    p.add_argument("--shorten-ms", type=float, default=0.02, help="simulated span of the Shorten measurement")
+    p.add_argument("--shorten-ms", type=float, default=0.02, help="simulated span of the Shorten timing (full grid)")
+    p.add_argument("--shorten-accuracy-ms", type=float, default=5.0,
+                   help="simulated span of the Shorten FP32-vs-FP64 comparison (16-fiber sample)")
     p.add_argument("--emg-cg-mesh", default="97,97,297", help="3D nodes of the CG-iteration measurement")
     p.add_argument("--emg-cg-iterations", type=int, default=160)
     return p.parse_args()
@@ -229,17 +232,18 @@ def plain_measurement(device: int) -> dict:
     return out
 
 
-def shorten_measurement(device: int, span_ms: float):
+def shorten_measurement(device: int, span_ms: float, accuracy_ms: float = 5.0):
     """The Shorten 2007 configuration (56 states; 1369 fibers x 1481 nodes = 2.03M nodes, dt0D 1e-5, dt_split
-    5e-4, seeded per-MU firing): FP64 plain (split) against the FP32-reaction path on the same fibers over a
-    bounded span (the 50 ms of the configuration take minutes; node-steps/s does not depend on the span)."""
-    import torch
+    5e-4, seeded per-MU firing): FP64 plain (split) against the FP32-reaction path, timed on the full grid over
+    a bounded span (the 50 ms of the configuration take minutes; node-steps/s does not depend on the span), and
+    compared on a 16-fiber sample of the grid (fibers whose motor unit fires at t = 0, so the span holds action
+    potentials) over accuracy_ms: Vm of all nodes and activation steps at 32 nodes per fiber."""
+    from opendihu_b200 import accuracy as ACC
     from opendihu_b200 import solver as S
     from opendihu_b200 import workloads as WL
     system = WL.shorten_grid(end_time=span_ms + 0.01)
     out = {"workload": "Shorten 2007, 1369 fibers x 1481 nodes (%d nodes), dt0D 1e-5, dt_split 5e-4 (25 Heun "
-                       "substeps per half step), %.3f ms measured after 0.01 ms warm-up" % (system.n_nodes, span_ms)}
-    vm = {}
+                       "substeps per half step), %.3f ms timed after 0.01 ms warm-up" % (system.n_nodes, span_ms)}
     for name, prec in (("fp64_plain", "fp64"), ("fp32_reaction", "fp32")):
         with S.FastMonodomainSolver(system.copy(), method="split", precision=prec, device=device) as sv:
             sv.setTimeSpan(0.0, 0.01)
@@ -250,12 +254,27 @@ def shorten_measurement(device: int, span_ms: float):
             sv.advanceTimeSpan()
             ms = sv.timing()["advance_ms"]
             steps = sv.split_steps() - n0
-            vm[name] = sv.states()[0]
         out[name] = {"node_steps_per_s": system.n_nodes * steps / (ms / 1e3), "ms": ms, "strang_steps": steps}
     out["speedup_fp32_over_fp64"] = out["fp32_reaction"]["node_steps_per_s"] / out["fp64_plain"]["node_steps_per_s"]
-    out["vm_max_abs_diff_fp32_vs_fp64_mV"] = float(np.max(np.abs(vm["fp32_reaction"] - vm["fp64_plain"])))
-    out["method"] = "split path (the 56 states stay in the reaction kernel's registers over each half step); " \
-                    "the fused kernel is built for HH only"
+    # accuracy on a sample over a span with action potentials
+    grid = WL.shorten_grid(end_time=accuracy_ms)
+    fires0 = np.nonzero(np.asarray(grid.firing_events)[0, np.asarray(grid.motor_unit_no) % grid.firing_events.shape[1]])[0]
+    sample = WL.subset(grid, fires0[:16])
+    nodes = ACC.traced_nodes(sample, 32)
+    res = {}
+    for name, prec in (("fp64", "fp64"), ("fp32", "fp32")):
+        with S.FastMonodomainSolver(sample.copy(), method="split", precision=prec, device=device, trace_nodes=nodes,
+                                    trace_capacity=0) as sv:
+            sv.record_activation(0.0, 16)
+            sv.advanceTimeSpan()
+            res[name] = (sv.states()[0], *sv.activation_steps())
+    out["accuracy"] = {"sample": "%d fibers x 1481 nodes (motor units firing at t = 0), %g ms (%d Strang steps)" % (
+                           sample.n_fibers, accuracy_ms, int(round(accuracy_ms / sample.dt_splitting))),
+                       "vm_max_abs_diff_fp32_vs_fp64_mV": float(np.max(np.abs(res["fp32"][0] - res["fp64"][0]))),
+                       "vm_range_fp64_mV": [float(res["fp64"][0].min()), float(res["fp64"][0].max())],
+                       "activation": ACC.compare_activation(res["fp32"][1], res["fp32"][2], res["fp64"][1],
+                                                            res["fp64"][2])}
+    out["method"] = "split path (the 56 states stay in the reaction kernel's registers over each half step)"
     return out
 
 
@@ -410,12 +429,18 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def side_line(name: str, value) -> None:
+    """A side measurement as its own JSON line (printed before the headline line)."""
+    print(json.dumps({"side": name, name: value}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
         return
     world, rank, local, pg = dist_setup(args)
+    from opendihu_b200 import accuracy as ACC
     from opendihu_b200 import solver as S
     from opendihu_b200 import workloads as WL
     if world > 1:
@@ -432,8 +457,11 @@ def main():
                 out = {"plain_config_node_steps_per_s": plain_measurement(local)}
             elif args.only == "adjoint":
                 out = {"adjoint": adjoint_measurement(local, args.adjoint_ms)}
+            elif args.only == "c2-accuracy":
+                out = {"c2_accuracy": ACC.batch_accuracy(WL.batched_hh(n_fibers=args.fibers, seed=0), local,
+                                                         args.accuracy_ms)}
             else:
-                out = {"shorten": shorten_measurement(local, args.shorten_ms)}
+                out = {"shorten": shorten_measurement(local, args.shorten_ms, args.shorten_accuracy_ms)}
             print(json.dumps(out), flush=True)
         if pg is not None:
             pg.destroy_process_group()
@@ -472,97 +500,85 @@ def main():
     launches_per_kernel = tm["main_kernel_launches"]
     steps_per_launch = split_steps / max(launches_per_kernel, 1)
 
-    # end to end through the C ABI with host buffers: H2D of the states, advance, D2H of the states
+    # end to end through the public API with host buffers, over the same K steps: H2D of the states from
+    # pinned staging, the advance, D2H of the states, every step
     host_states = fused.states()
-    e2e_steps = max(1, min(args.steps, 3))
     barrier(pg)
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         fused.set_states(host_states)
         fused.setTimeSpan(t, t + step)
         fused.advanceTimeSpan()
         host_states = fused.states(out=host_states)
         t += step
     e2e_s = allmax(pg, time.perf_counter() - t0)
-    e2e_value = n_nodes * (split_steps / args.steps) * e2e_steps * world / e2e_s
+    e2e_value = n_nodes * split_steps * world / e2e_s
     state_bytes = n_nodes * 8 * 4
+    fused_shape = {"threads": fused.threads_per_block, "nodes_per_thread": fused.nodes_per_thread,
+                   "cluster_size": fused.cluster_size, "steps_per_launch": steps_per_launch,
+                   "autotuned": tuning is not None}
     fused.close()
 
-    # FP64 split ("plain") solver on the same batch
-    fp64_value = None
+    # FP64 split ("plain") and FP64 fused solvers on the same batch: the first is the reference's method, the
+    # second separates the gain of fusion from the gain of the FP32 reaction
+    fp64 = {}
     if not args.skip_fp64:
-        plain = S.FastMonodomainSolver(system.copy(), method="split", precision="fp64", device=local)
-        plain.initialize()
-        tp = 0.0
-        plain.setTimeSpan(tp, tp + step)
-        plain.advanceTimeSpan()
-        tp += step
-        barrier(pg)
-        plain.reset_timing()
-        p0 = plain.split_steps()
-        n_plain = 2
-        for _ in range(n_plain):
-            plain.setTimeSpan(tp, tp + step)
-            plain.advanceTimeSpan()
+        for name, method in (("split", "split"), ("fused", "fused")):
+            slv = S.FastMonodomainSolver(system.copy(), method=method, precision="fp64", device=local,
+                                         autotune=method == "fused")
+            slv.initialize()
+            tp = 0.0
+            slv.setTimeSpan(tp, tp + step)
+            slv.advanceTimeSpan()
             tp += step
-        tmp = plain.timing()
-        p_s = allmax(pg, tmp["advance_ms"] / 1e3)
-        fp64_value = n_nodes * (plain.split_steps() - p0) * world / p_s
-        plain.close()
+            barrier(pg)
+            slv.reset_timing()
+            p0 = slv.split_steps()
+            for _ in range(2):
+                slv.setTimeSpan(tp, tp + step)
+                slv.advanceTimeSpan()
+                tp += step
+            p_s = allmax(pg, slv.timing()["advance_ms"] / 1e3)
+            fp64[name] = n_nodes * (slv.split_steps() - p0) * world / p_s
+            slv.close()
 
-    # plain-method configuration (16 HH fibers x 1481 nodes, implicit Euler, FP64 split path with CUDA graphs,
-    # and the FP32 fused kernel on the same fibers)
-    plain_cfg = None
+    # side measurements, each printed as its own line before the headline line
+    plain_cfg = adj = acc = cpu = None
     if rank == 0 and not args.skip_fp64 and world == 1:
         plain_cfg = plain_measurement(local)
-
-    # differentiation: adjoint gradient cost relative to one FP64 forward solve (256 HH fibers x 1481 nodes,
-    # per-fiber sigma, g_Na, g_K; 32 sensors per fiber; checkpoint every 100 Strang steps)
-    adj = None
+        side_line("plain_config_node_steps_per_s", plain_cfg)
     if rank == 0 and not args.skip_adjoint:
         adj = adjoint_measurement(local, args.adjoint_ms)
-
-    # fibers -> 3D static bidomain (EMG): the coupled fibers_emg-shaped workload, and the conjugate-gradient
-    # iteration on a mesh larger than L2 against the HBM roofline
-    emg = None
+        side_line("adjoint", adj)
     if rank == 0 and not args.skip_emg:
-        emg = emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations)
-    shorten = None
+        side_line("emg", emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations))
     if rank == 0 and not args.skip_shorten:
-        shorten = shorten_measurement(local, args.shorten_ms)
-
-    # accuracy against the FP64 oracle on a sample of the batch, and the oracle's CPU throughput
-    acc = None
-    cpu = None
+        side_line("shorten", shorten_measurement(local, args.shorten_ms, args.shorten_accuracy_ms))
     if rank == 0 and not args.skip_accuracy:
+        acc = ACC.batch_accuracy(system, local, args.accuracy_ms)
+        side_line("c2_accuracy", acc)
+        # the oracle's CPU throughput on a bounded sample of the batch, all host threads, and one thread (the
+        # reference's vc path runs one thread per MPI rank)
         threads = os.cpu_count() or 1
         sub, ref, n_ref, rate, cpu_s = cpu_baseline(system, 10, 20.0, threads)
         cpu = {"value": rate, "unit": "node-steps/s", "cores": threads, "kind": "port",
                "sample": f"first 10 fibers of the batch ({sub.n_nodes} nodes) x 20 ms ({n_ref} Strang steps), "
                          f"{cpu_s:.1f} s"}
-        # one thread: the reference's vc path runs one thread per MPI rank
         sub1, _, n1, rate1, cpu1_s = cpu_baseline(system, 1, 10.0, 1)
-        cpu["single_thread"] = {"value": rate1, "unit": "node-steps/s", "cores": 1,
-                                "sample": f"first fiber ({sub1.n_nodes} nodes) x 10 ms ({n1} Strang steps), "
-                                          f"{cpu1_s:.1f} s"}
-        acc = {}
-        for name, method, prec in (("fp32_fused", "fused", "fp32"), ("fp64_split", "split", "fp64")):
-            with S.FastMonodomainSolver(sub.copy(), method=method, precision=prec, device=local) as slv:
-                slv.advanceTimeSpan()
-                st = slv.states()
-            acc[name] = {"vm_max_abs_err_mV": float(np.max(np.abs(st[0] - ref[0])))}
+        cpu["single_thread"] = {"value": rate1, "cores": 1,
+                                "sample": f"first fiber ({sub1.n_nodes} nodes) x 10 ms ({n1} Strang steps)"}
 
     peak_hbm, sm_max, peak_kind = peaks()
     ops = hh_ops()
     n0d = 5
     fp32_flops_node_step = 2 * n0d * (2 * ops["flops"] + 6 + 9)
-    fp64_flops_node_step = 2 * n0d * 5 + 15
     # algorithmic HBM bytes of one fused launch, per node: states read and written once (Vm f64, 3 gates and
     # their 3 compensation residuals f32), 3 parameters (f32), 6 diffusion coefficients (f64), clamp map (i32)
     bytes_launch = n_nodes * (2 * (8 + 12 + 12) + 12 + 48 + 4)
     achieved_gbs = bytes_launch / (kernel_avg_ms / 1e3) / 1e9 if kernel_avg_ms > 0 else None
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
-    achieved_tf = n_nodes * steps_per_launch * fp32_flops_node_step / (kernel_avg_ms / 1e3) / 1e12 if kernel_avg_ms > 0 else None
+    achieved_tf = (n_nodes * steps_per_launch * fp32_flops_node_step / (kernel_avg_ms / 1e3) / 1e12
+                   if kernel_avg_ms > 0 else None)
     traffic = None
     prof = os.path.join(ROOT, "profiles", "fused_kernel_batched_hh.md")
     if os.path.exists(prof):
@@ -571,41 +587,42 @@ def main():
                 traffic = float(ln.split(":", 1)[1]) * n_nodes
 
     if rank == 0:
+        acc_line = None
+        if acc:
+            a32 = acc["fp32_fused_vs_fp64_fused"]
+            acc_line = {"span_ms": args.accuracy_ms, "fibers": system.n_fibers,
+                        "vm_max_abs_mV": a32["vm_max_abs_diff_mV"],
+                        "activation_max_step_diff": a32["activation"]["max_step_diff"],
+                        "activation_nodes_count_mismatch": a32["activation"]["nodes_count_mismatch"],
+                        "crossings": a32["activation"]["crossings"],
+                        "traced_nodes": a32["activation"]["traced_nodes"],
+                        "fp64_split_vs_fused_vm_max_abs_mV": acc["fp64_split_vs_fp64_fused"]["vm_max_abs_diff_mV"],
+                        "reference": "FP64 fused, all fibers; FP64 split on %d fibers" % (
+                            acc["fp64_split_vs_fp64_fused"]["fibers"])}
         line = {
             "metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 reaction + f64 Vm/diffusion",
             "data": "synthetic (seeded)",
-            "config": {"workload": "batched_hh: 4096 HH fibers/GPU, lengths U[500,2500] (seed=rank), dx 0.01 cm, "
-                                   "100 MUs (exponential sizes), Poisson 10-40 Hz firing, Crank-Nicolson, "
-                                   "dt0D 1e-4 ms, dt_split 1e-3 ms",
-                       "n_nodes_per_gpu": n_nodes, "step": f"{step} ms simulated = {split_steps // args.steps} Strang steps",
-                       "method": "fused persistent kernel, FP32 reaction", "l2": "inputs larger than L2 (~0.5 GB/GPU)",
-                       "fused_shape": {"threads": fused.threads_per_block, "nodes_per_thread": fused.nodes_per_thread,
-                                       "cluster_size": fused.cluster_size,
-                                       "steps_per_launch": steps_per_launch, "autotuned": tuning is not None},
-                       "parallelism": f"fibers sharded, {world} GPU(s), no collective"},
+            "config": {"workload": "batched_hh: 4096 HH fibers/GPU, lengths U[500,2500] (seed=rank), 100 MUs, "
+                                   "Poisson 10-40 Hz, Crank-Nicolson, dt0D 1e-4 ms, dt_split 1e-3 ms",
+                       "n_nodes_per_gpu": n_nodes, "step": f"{step} ms = {split_steps // args.steps} Strang steps",
+                       "method": "fused persistent kernel, FP32 reaction", "l2": "inputs larger than L2",
+                       "fused_shape": fused_shape, "parallelism": f"fibers sharded, {world} GPU(s), no collective"},
             "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": state_bytes,
-                    "d2h_bytes_per_step": state_bytes},
+                    "d2h_bytes_per_step": state_bytes, "steps": args.steps},
             "gpu_launches": int(tm["kernel_launches"]),
-            "fp64_plain": {"value": fp64_value, "unit": "node-steps/s",
-                           "speedup_fp32_fused_over_fp64_plain": (value / fp64_value) if fp64_value else None},
-            "accuracy_vs_fp64_oracle": acc,
+            "fp64_plain": {"value": fp64.get("split"), "speedup": (value / fp64["split"]) if fp64.get("split") else None},
+            "fp64_fused": {"value": fp64.get("fused"), "speedup": (value / fp64["fused"]) if fp64.get("fused") else None},
+            "accuracy_vs_fp64": acc_line,
             "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
-            "plain_config_node_steps_per_s": plain_cfg,
-            "adjoint": adj,
-            "emg": emg,
-            "shorten": shorten,
-            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak_hbm, "unit": "GB/s",
-                         "frac": (achieved_gbs / peak_hbm) if achieved_gbs else None, "traffic": traffic,
-                         "peak_source": peak_kind,
-                         "kernel": "fused_kernel (avg launch %.3f ms, %.0f Strang steps per launch)" % (
+            "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": (achieved_tf / fp32_peak) if achieved_tf else None, "traffic": traffic,
+                         "peak_source": "derived: 148 SMs x 128 FP32 lanes x 2 flop x sm_max_mhz (no measured FP32 peak)",
+                         "kernel": "fused_kernel, avg launch %.3f ms, %.0f Strang steps/launch" % (
                              kernel_avg_ms, steps_per_launch)},
-            "roofline_compute": {"bound": "fp32-alu", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
-                                 "frac": (achieved_tf / fp32_peak) if achieved_tf else None,
-                                 "peak_source": "derived: 148 SMs x 128 FP32 lanes x 2 x sm_max_mhz",
-                                 "flops_per_node_step": {"fp32": fp32_flops_node_step, "fp64": fp64_flops_node_step,
-                                                         "sfu_exp": 2 * n0d * 2 * ops["special"]}},
+            "roofline_hbm": {"achieved": achieved_gbs, "peak": peak_hbm, "unit": "GB/s",
+                             "frac": (achieved_gbs / peak_hbm) if achieved_gbs else None, "peak_source": peak_kind},
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -162,9 +162,18 @@ int fdm_select_clamp_nodes(int clamp_rule, int vc_width, int n_ranks, int n_fibe
 int fdm_set_algebraics_for_transfer(fdm_solver *s, int n, const int *algebraic_indices);
 int fdm_get_algebraics(fdm_solver *s, double *out /* [k * n_nodes + node] */);
 
-/* record Vm at the given nodes after every split step (for activation times); capacity in split steps */
+/* record Vm at the given nodes after every split step (for activation times); capacity in split steps; the
+ * rows count the split steps from this call on (row 0 = the first step after it) */
 int fdm_set_trace(fdm_solver *s, int n_nodes, const int64_t *nodes, int64_t capacity);
 int fdm_get_trace(fdm_solver *s, double *out /* [step * n_nodes + k] */, int64_t *n_steps_recorded);
+/* Activation recording on the traced nodes (no counterpart in the reference; its scripts find activation
+ * times in the written Vm): after each Strang step, a traced node whose Vm rose above threshold (Vm after the
+ * previous step <= threshold < Vm now) records the step's trace row (Strang steps since fdm_set_trace, 0 =
+ * the first).  The first capacity_per_node rows per node are kept, every crossing is counted; the step right
+ * after the recording starts never records.  0 turns it off; fdm_set_trace turns it off (call this after). */
+int fdm_set_activation_recording(fdm_solver *s, double threshold, int capacity_per_node);
+/* counts[k] = crossings of traced node k; steps[k * capacity_per_node + j] = its j-th row (-1: none) */
+int fdm_get_activation_steps(fdm_solver *s, int *counts, int *steps);
 
 /* RepeatedCall over [t_start, t_end]: blocking; returns after the device finished. */
 int fdm_advance(fdm_solver *s, double t_start, double t_end);

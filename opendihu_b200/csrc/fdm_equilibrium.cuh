@@ -380,8 +380,8 @@ __global__ void eq_trace_kernel(ReactionArgs a)
     return;
   const SplitStep s = a.steps[a.step];
   const int slot = a.trace_slot[i];
-  if (slot >= 0 && s.global_no < a.trace_capacity)
-    a.trace[(int64_t)s.global_no * a.n_trace + slot] = a.vm[i];
+  if (slot >= 0)
+    record_trace(a.trace, a.n_trace, a.trace_capacity, a.act, slot, s.global_no, a.vm[i]);
 }
 #endif // FDM_COMMON_KERNELS_TU
 

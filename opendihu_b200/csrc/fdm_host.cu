@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <numeric>
 #include <string>
@@ -217,6 +218,12 @@ struct fdm_solver {
   int n_alg_out = 0;
   int n_trace = 0;
   int64_t trace_capacity = 0;
+  int64_t trace_base = 0;        // split step number at fdm_set_trace: trace rows count from it
+  // activation recording on the traced nodes (fdm_set_activation_recording)
+  DevBuf<double> act_prev;
+  DevBuf<int> act_count, act_steps;
+  double act_threshold = 0.0;
+  int act_cap = 0;
 
   // adjoint (checkpointed forward, replay + reverse)
   struct Adjoint {
@@ -540,6 +547,9 @@ extern "C" int fdm_destroy(fdm_solver* s)
   s->log_n.release();
   s->log_cap = 0;
   s->log_dropped = 0;
+  s->act_prev.release();
+  s->act_count.release();
+  s->act_steps.release();
   s->flags.release();
   s->steps_d.release();
   s->adj.release();
@@ -1649,6 +1659,8 @@ extern "C" int fdm_set_trace(fdm_solver* s, int n, const int64_t* nodes, int64_t
   }
   s->n_trace = 0;   // set once the buffers are in place
   s->trace_capacity = 0;
+  s->act_cap = 0;   // the slots change: activation recording stops (fdm_set_activation_recording restarts it)
+  s->trace_base = s->split_no;
   if (n > 0) {
     FDM_CUDA(s->trace_slot.alloc(s->n_nodes));
     FDM_CUDA(s->trace.alloc(std::max<size_t>((size_t)n * capacity, 1)));
@@ -1667,13 +1679,65 @@ extern "C" int fdm_get_trace(fdm_solver* s, double* out, int64_t* n_steps)
   if (!s)
     return fail(s, FDM_ERR_ARG, "fdm_get_trace: bad argument");
   FDM_BIND(s);
-  const int64_t rec = std::min(s->split_no, s->trace_capacity);
+  const int64_t rec = std::min(std::max<int64_t>(s->split_no - s->trace_base, 0), s->trace_capacity);
   if (n_steps)
     *n_steps = rec;
   if (out && rec > 0 && s->n_trace > 0) {
     FDM_CUDA(cudaMemcpyAsync(out, s->trace.p, sizeof(double) * rec * s->n_trace, cudaMemcpyDeviceToHost, s->stream));
     FDM_CUDA(cudaStreamSynchronize(s->stream));
   }
+  return FDM_OK;
+}
+
+extern "C" int fdm_set_activation_recording(fdm_solver* s, double threshold, int capacity_per_node)
+{
+  if (!s || capacity_per_node < 0 || !std::isfinite(threshold))
+    return fail(s, FDM_ERR_ARG, "fdm_set_activation_recording: bad argument");
+  if (capacity_per_node > 0 && s->n_trace == 0)
+    return fail(s, FDM_ERR_ARG, "fdm_set_activation_recording: set the traced nodes first (fdm_set_trace)");
+  FDM_BIND(s);
+  {
+    const int rw = fdm_wait(s);
+    if (rw)
+      return rw;
+  }
+  invalidate_graphs(s);
+  s->act_cap = 0;   // set once the buffers are in place
+  if (capacity_per_node == 0)
+    return FDM_OK;
+  const size_t n = (size_t)s->n_trace;
+  FDM_CUDA(s->act_prev.alloc(n));
+  FDM_CUDA(s->act_count.alloc(n));
+  FDM_CUDA(s->act_steps.alloc(n * (size_t)capacity_per_node));
+  std::vector<double> nan(n, std::numeric_limits<double>::quiet_NaN());
+  FDM_CUDA(cudaMemcpyAsync(s->act_prev.p, nan.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+  FDM_CUDA(cudaMemsetAsync(s->act_count.p, 0, sizeof(int) * n, s->stream));
+  FDM_CUDA(cudaMemsetAsync(s->act_steps.p, 0xff, sizeof(int) * n * (size_t)capacity_per_node, s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
+  s->act_threshold = threshold;
+  s->act_cap = capacity_per_node;
+  return FDM_OK;
+}
+
+extern "C" int fdm_get_activation_steps(fdm_solver* s, int* counts, int* steps)
+{
+  if (!s)
+    return fail(s, FDM_ERR_ARG, "fdm_get_activation_steps: bad argument");
+  if (s->act_cap == 0)
+    return fail(s, FDM_ERR_ARG, "fdm_get_activation_steps: activation recording is off");
+  FDM_BIND(s);
+  {
+    const int rw = fdm_wait(s);
+    if (rw)
+      return rw;
+  }
+  const size_t n = (size_t)s->n_trace;
+  if (counts)
+    FDM_CUDA(cudaMemcpyAsync(counts, s->act_count.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (steps)
+    FDM_CUDA(cudaMemcpyAsync(steps, s->act_steps.p, sizeof(int) * n * (size_t)s->act_cap, cudaMemcpyDeviceToHost,
+                             s->stream));
+  FDM_CUDA(cudaStreamSynchronize(s->stream));
   return FDM_OK;
 }
 
@@ -1711,6 +1775,19 @@ struct WindowInfo {
   const uint8_t* gate_start = nullptr; // onlyComputeIfHasBeenStimulated: first substeps of the window
   int gate_stride = 0;
 };
+
+static ActivationRec activation_rec(const fdm_solver* s)
+{
+  ActivationRec r{};
+  if (s->act_cap > 0 && s->n_trace > 0) {
+    r.threshold = s->act_threshold;
+    r.prev = s->act_prev.p;
+    r.count = s->act_count.p;
+    r.steps = s->act_steps.p;
+    r.capacity = s->act_cap;
+  }
+  return r;
+}
 
 static int ensure_step_capacity(fdm_solver* s, int n)
 {
@@ -1851,6 +1928,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
     fa.trace = s->trace.p;
     fa.n_trace = s->n_trace;
     fa.trace_capacity = s->trace_capacity;
+    fa.act = activation_rec(s);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (prof) {
       e0 = next_event(s);
@@ -1893,6 +1971,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
   ra.trace = s->trace.p;
   ra.n_trace = s->n_trace;
   ra.trace_capacity = s->trace_capacity;
+  ra.act = activation_rec(s);
   if (s->eq.on) {
     // equilibrium skip: every half step is a speculative reaction, the buffer scan and a commit; the statuses
     // alternate between the two status arrays, and a window has an even number of half steps
@@ -2047,7 +2126,7 @@ static void plan_advance(fdm_solver* s, double t_start, double t_end, std::vecto
       st.mid = tc + 0.5 * dts;
       st.dt0 = s->heun.dt;
       st.n0 = s->heun.n;
-      st.global_no = (int)std::min<int64_t>(s->split_no, 2147483647);
+      st.global_no = (int)std::min<int64_t>(std::max<int64_t>(s->split_no - s->trace_base, 0), 2147483647);
       s->split_no++;
       steps.push_back(st);
       dt1s.push_back(s->diff.dt);
@@ -2221,7 +2300,7 @@ static int advance_explicit(fdm_solver* s, double start, double dts, int ns, dou
     steps[j].mid = tc + 0.5 * dts;
     steps[j].dt0 = dt0;
     steps[j].n0 = n0;
-    steps[j].global_no = (int)std::min<int64_t>(s->split_no, 2147483647);
+    steps[j].global_no = (int)std::min<int64_t>(std::max<int64_t>(s->split_no - s->trace_base, 0), 2147483647);
     s->split_no++;
   }
   int r = run_planned(s, steps, dt1s, 0, steps.size(), true);
@@ -2958,6 +3037,7 @@ extern "C" int fdm_adjoint_forward(fdm_solver* s, double t_start, double t_end, 
   int rc = fdm_set_trace(s, n_sensors, sensor_nodes, NT);
   if (rc)
     return rc;
+  s->trace_base = s->split_no - NT;   // the rows are this run's steps (planned above)
   const int64_t N = s->n_nodes;
   const int NS = s->model->n_states;
   const int nf = s->n_fibers;
@@ -3277,6 +3357,7 @@ extern "C" int fdm_rewind(fdm_solver* s)
   FDM_BIND(s);
   s->tss_init = false;
   s->split_no = 0;
+  s->trace_base = 0;
   s->ck_valid = false;
   const int nf = s->n_fibers;
   if (s->stimulation_set && nf > 0) {

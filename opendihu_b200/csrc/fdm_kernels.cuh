@@ -41,8 +41,38 @@ struct SplitStep {
   double mid;    // midTime = currentTime + 0.5*dtSplit
   double dt0;    // Heun substep width
   int n0;        // number of Heun substeps per half step
-  int global_no; // split step number since the start of the run (trace row)
+  int global_no; // split step number since the trace was set (trace row)
 };
+
+// Activation recording on the traced nodes: after every Strang step, a node whose Vm rose above the threshold
+// (Vm after the previous step <= threshold < Vm now) records the step's trace row; the first `capacity` rows
+// per node are kept, `count` counts them all.  `prev` starts as NaN, so the first step after the recording
+// starts never records.  Each traced node is written by one thread per step: no atomics.
+struct ActivationRec {
+  double threshold;
+  double* prev;                   // [slot] Vm after the previous step (null: recording off)
+  int* count;                     // [slot]
+  int* steps;                     // [slot * capacity + k]
+  int capacity;
+};
+
+// the trace value of a traced node after a Strang step, and its activation record
+__device__ __forceinline__ void record_trace(double* trace, int n_trace, int64_t capacity, const ActivationRec& act,
+                                             int slot, int row, double V)
+{
+  if (row < capacity)
+    trace[(int64_t)row * n_trace + slot] = V;
+  if (act.prev) {
+    const double p = act.prev[slot];
+    if (p <= act.threshold && V > act.threshold) {
+      const int c = act.count[slot];
+      if (c < act.capacity)
+        act.steps[(int64_t)slot * act.capacity + c] = row;
+      act.count[slot] = c + 1;
+    }
+    act.prev[slot] = V;
+  }
+}
 
 struct StimArgs {
   const uint8_t* firing_events;   // [row][col]
@@ -476,6 +506,7 @@ struct ReactionArgs {
   double* trace;                  // [global split no][slot]
   int n_trace;
   int64_t trace_capacity;
+  ActivationRec act;
   double* store_states;           // adjoint replay (FP64 only): input state of substep k at
                                   // store_states[(k*nStates + s)*stride + node], or null
   double* store_vm_out;           // adjoint replay: Vm after the half step also written here, or null
@@ -548,8 +579,8 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
   }
   if (a.half == 1 && a.trace_slot) {
     const int slot = a.trace_slot[i];
-    if (slot >= 0 && s.global_no < a.trace_capacity)
-      a.trace[(int64_t)s.global_no * a.n_trace + slot] = V;
+    if (slot >= 0)
+      record_trace(a.trace, a.n_trace, a.trace_capacity, a.act, slot, s.global_no, V);
   }
 }
 
@@ -1033,6 +1064,7 @@ struct FusedArgs {
   double* trace;
   int n_trace;
   int64_t trace_capacity;
+  ActivationRec act;
   const int* gate;                // onlyComputeIfHasBeenStimulated: per node gate code, or null
   const uint8_t* gate_start;
   int gate_stride;
@@ -1684,8 +1716,8 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     if (a.trace_slot) {
 #pragma unroll
       for (int j = 0; j < M; j++)
-        if (s_ts[tid * M + j] >= 0 && s.global_no < a.trace_capacity)
-          a.trace[(int64_t)s.global_no * a.n_trace + s_ts[tid * M + j]] = V[j];
+        if (s_ts[tid * M + j] >= 0)
+          record_trace(a.trace, a.n_trace, a.trace_capacity, a.act, s_ts[tid * M + j], s.global_no, V[j]);
     }
   }
 

@@ -479,6 +479,7 @@ class FastMonodomainSolver:
         self.profile = profile
         self.trace_nodes = np.asarray(trace_nodes, np.int64)
         self.trace_capacity = int(trace_capacity)
+        self._act_cap = 0
         self.device = int(device)
         self.autotune = bool(autotune)
         #: fused method: CTAs of one thread-block cluster per fiber (0: chosen by the library, 1: off)
@@ -838,6 +839,29 @@ class FastMonodomainSolver:
         if n.value and len(self.trace_nodes):
             self._call(N.lib().fdm_get_trace, N.ptr(out, C.c_double), C.byref(n))
         return out[:n.value, :len(self.trace_nodes)]
+
+    def set_trace(self, nodes, capacity: int):
+        """Traces Vm at ``nodes`` after each Strang step from now on (``capacity`` steps; rows count from here)."""
+        self.initialize()
+        self.trace_nodes = np.ascontiguousarray(nodes, np.int64)
+        self.trace_capacity = int(capacity)
+        self._call(N.lib().fdm_set_trace, len(self.trace_nodes), N.ptr(self.trace_nodes, C.c_int64),
+                   self.trace_capacity)
+
+    def record_activation(self, threshold: float = 0.0, capacity: int = 16):
+        """Records, on the traced nodes, the Strang steps (trace rows) after which Vm rose above ``threshold``
+        (fdm_set_activation_recording); ``capacity`` rows per node are kept, all crossings are counted."""
+        self.initialize()
+        self._act_cap = int(capacity)
+        self._call(N.lib().fdm_set_activation_recording, float(threshold), self._act_cap)
+
+    def activation_steps(self):
+        """(counts [traced node], steps [traced node, capacity]; -1 where none) of record_activation."""
+        n = len(self.trace_nodes)
+        counts = np.zeros(max(n, 1), np.int32)
+        steps = np.zeros((max(n, 1), max(self._act_cap, 1)), np.int32)
+        self._call(N.lib().fdm_get_activation_steps, N.ptr(counts, C.c_int), N.ptr(steps, C.c_int))
+        return counts[:n], steps[:n, :self._act_cap]
 
     def rewind(self):
         """Back to the start time: time-stepping state and stimulation machine reset, states kept."""
