@@ -298,6 +298,38 @@ static void heun_step(const oracle_model *m, double *y, const double *prm, doubl
       alg_store[k * stride] = alg2[p->algebraic_indices[k]];
 }
 
+/* n_steps Heun steps of one W-lane point buffer as compute0D calls the generated compute0DInstance
+ * (03_generator_vc.cpp:913-1163): y[s * W + lane], params[q * W + lane]; step k at t0 + k * dt; when stimulate
+ * is set the lanes 0..min(3, W)-1 are clamped to v_stim (the vc rule's lanes of the junction buffer); after
+ * the last step the algebraics alg_indices[0..n_alg) of the second evaluation go to alg_out[k * W + lane].
+ * Exported for the cross-check against the reference's own generated code. */
+int oracle_heun_buffer(int model, int W, int approx, double *y, const double *params, double t0, double dt,
+                       int n_steps, int stimulate, double v_stim, int n_alg, const int *alg_indices, double *alg_out)
+{
+  if (model < 0 || model >= ORACLE_N_MODELS || W < 1 || W > ORACLE_MAX_VC_WIDTH || n_alg < 0)
+    return -1;
+  const oracle_model *m = &oracle_models[model];
+  oracle_problem p;
+  memset(&p, 0, sizeof(p));
+  p.approx_exp = approx;
+  p.n_algebraics_out = n_alg;
+  p.algebraic_indices = alg_indices;
+  for (int lane = 0; lane < W; lane++) {
+    double ys[ORACLE_MAX_STATES], prm[ORACLE_MAX_PARAMETERS];
+    for (int s = 0; s < m->n_states; s++)
+      ys[s] = y[s * W + lane];
+    for (int q = 0; q < m->n_parameters; q++)
+      prm[q] = params[q * W + lane];
+    const int clamp = lane < (W < 3 ? W : 3);
+    for (int k = 0; k < n_steps; k++)
+      heun_step(m, ys, prm, t0 + k * dt, dt, stimulate, clamp, v_stim, k == n_steps - 1 && n_alg > 0, &p,
+                alg_out ? alg_out + lane : NULL, W);
+    for (int s = 0; s < m->n_states; s++)
+      y[s * W + lane] = ys[s];
+  }
+  return 0;
+}
+
 /* equilibriumAccelerationUpdate (compute.tpp:630-762) for buffer b after its substeps: the buffer is at
  * equilibrium if no state of any lane changed by more than 1e-6 (relative, or absolute when the smallest
  * lane value of the state is below 1e-11 in magnitude); statuses and the rank's count follow the
