@@ -217,7 +217,8 @@ def plain_measurement(device: int) -> dict:
     c1 = WL.plain_hh(end_time=10.0)
     out = {"workload": "16 HH fibers x 1481 nodes, implicit Euler, 10 ms"}
     for name, method, prec in (("fp64_split", "split", "fp64"), ("fp64_fused", "fused", "fp64"),
-                               ("fp32_fused", "fused", "fp32")):
+                               ("fp32_fused", "fused", "fp32"), ("fp64_auto", "auto", "fp64"),
+                               ("fp32_auto", "auto", "fp32")):
         with S.FastMonodomainSolver(c1.copy(), method=method, precision=prec, device=device) as sv:
             sv.setTimeSpan(0.0, 1.0)
             sv.advanceTimeSpan()
@@ -225,9 +226,12 @@ def plain_measurement(device: int) -> dict:
             sv.setTimeSpan(1.0, 10.0)
             sv.advanceTimeSpan()
             ms = sv.timing()["advance_ms"]
-            if method == "fused":
+            if method == "fused" and prec == "fp64":
                 # few fibers: each fiber spread over the CTAs of a thread-block cluster
                 out["fused_layout"] = sv.fused_layout()
+            if method == "auto":
+                out[name + "_choice"] = {k: sv.tuning.get(k) for k in ("method", "threads", "nodes_per_thread",
+                                                                       "cluster_size", "steps_per_launch")}
         out[name] = c1.n_nodes * 9000 / (ms / 1e3)
     return out
 

@@ -73,11 +73,34 @@ def _time_shape(system, precision, threads, m, k, n_steps, device, cluster_size:
     return tm["advance_ms"] / 1e3 / n_steps
 
 
+def _time_split(system, precision, k, n_steps, device) -> float:
+    """Seconds of device time per Strang step of the split method (window launches replayed as CUDA graphs)."""
+    from .solver import FastMonodomainSolver
+    s = system.copy()
+    dt = s.dt_splitting
+    with FastMonodomainSolver(s, method="split", precision=precision, steps_per_launch=k, device=device,
+                              check_nan=False) as slv:
+        slv.setTimeSpan(s.start_time, s.start_time + dt * min(k, n_steps))
+        slv.advanceTimeSpan()
+        slv.reset_timing()
+        t0 = s.start_time + dt * min(k, n_steps)
+        slv.setTimeSpan(t0, t0 + dt * n_steps)
+        slv.advanceTimeSpan()
+        tm = slv.timing()
+    return tm["advance_ms"] / 1e3 / n_steps
+
+
 def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0,
-             steps_per_launch: Sequence[int] = (50, 100, 200), use_cache: bool = True) -> dict:
-    """Return {"threads", "nodes_per_thread", "cluster_size", "steps_per_launch", "s_per_step", "trials"} for the
-    workload (cluster_size 1: bins of whole fibers)."""
-    key = signature(system, precision)
+             steps_per_launch: Sequence[int] = (50, 100, 200), use_cache: bool = True,
+             include_split: bool = False) -> dict:
+    """Return {"method", "threads", "nodes_per_thread", "cluster_size", "steps_per_launch", "s_per_step",
+    "trials"} for the workload (cluster_size 1: bins of whole fibers).  With include_split the split method (a
+    reaction launch per half step and a diffusion launch per step, as CUDA graphs) competes too: with few
+    nodes its one thread per node can outrun the fused kernel's shapes."""
+    if include_split and getattr(system, "skip_close_to_equilibrium", False):
+        return {"method": "split", "threads": 0, "nodes_per_thread": 0, "cluster_size": 1, "steps_per_launch": 0,
+                "s_per_step": None, "trials": [], "reason": "the equilibrium skip runs on the split method"}
+    key = signature(system, precision) + ("+split" if include_split else "")
     if use_cache:
         if key in _MEMO:
             return _MEMO[key]
@@ -93,19 +116,38 @@ def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0
             c = -(-max_len // (t * m))
             if 2 <= c <= 8:
                 shapes.append((t, m, c))
-    if not shapes:
+    if not shapes and not include_split:
         raise N.FdmError(N.FDM_ERR_UNSUPPORTED, f"no fused shape holds a fiber of {max_len} nodes")
     trials = []
+    if include_split:
+        trials.append({"method": "split", "threads": 0, "nodes_per_thread": 0, "cluster_size": 1,
+                       "steps_per_launch": 100, "s_per_step": _time_split(system, precision, 100, max(n_steps, 100),
+                                                                         device)})
+        if not shapes:
+            result = dict(trials[0])
+            result["trials"] = trials
+            _MEMO[key] = result
+            if use_cache:
+                _store_cache(key, result)
+            return result
     k0 = 100
     for t, m, c in shapes:
-        trials.append({"threads": t, "nodes_per_thread": m, "cluster_size": c, "steps_per_launch": min(k0, n_steps),
+        trials.append({"method": "fused", "threads": t, "nodes_per_thread": m, "cluster_size": c,
+                       "steps_per_launch": min(k0, n_steps),
                        "s_per_step": _time_shape(system, precision, t, m, min(k0, n_steps), n_steps, device, c)})
     best = min(trials, key=lambda r: r["s_per_step"])
+    if best["method"] == "split":
+        result = dict(best)
+        result["trials"] = trials
+        _MEMO[key] = result
+        if use_cache:
+            _store_cache(key, result)
+        return result
     # window length for the winner, over a span of a few windows
     k_trials = []
     for k in steps_per_launch:
         span = max(n_steps, 2 * k)
-        k_trials.append({"threads": best["threads"], "nodes_per_thread": best["nodes_per_thread"],
+        k_trials.append({"method": "fused", "threads": best["threads"], "nodes_per_thread": best["nodes_per_thread"],
                          "cluster_size": best["cluster_size"], "steps_per_launch": k,
                          "s_per_step": _time_shape(system, precision, best["threads"], best["nodes_per_thread"], k,
                                                    span, device, best["cluster_size"])})

@@ -515,7 +515,20 @@ class FastMonodomainSolver:
             return
         s = self.system
         L = N.lib()
-        if self.autotune and self.method == "fused" and not self.threads_per_block:
+        if self.method == "auto":
+            # the autotuner times the split method against every fused shape and keeps the fastest
+            from .autotune import autotune
+            self.tuning = autotune(s, self.precision, device=self.device, include_split=True)
+            self.method = self.tuning["method"]
+            if self.method == "split":
+                self.steps_per_launch = self.steps_per_launch or int(self.tuning["steps_per_launch"] or 0)
+            else:
+                self.threads_per_block = self.tuning["threads"]
+                self.nodes_per_thread = self.tuning["nodes_per_thread"]
+                self.cluster_size = int(self.tuning.get("cluster_size", 1))
+                if not self.steps_per_launch:
+                    self.steps_per_launch = self.tuning["steps_per_launch"]
+        elif self.autotune and self.method == "fused" and not self.threads_per_block:
             from .autotune import autotune
             self.tuning = autotune(s, self.precision, device=self.device)
             self.threads_per_block = self.tuning["threads"]

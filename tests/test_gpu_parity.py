@@ -47,7 +47,7 @@ def small_system(**kw):
     return H.c1_system(n_fibers=3, n_nodes=301, end_time=kw.pop("end_time", 2.0), **kw)
 
 
-@pytest.mark.parametrize("method", ["split", "fused", "fused_bins"])
+@pytest.mark.parametrize("method", ["split", "fused", "fused_bins", "auto"])
 def test_fp64_matches_oracle(method):
     st, ref, dv = compare(small_system(), method, "fp64", VM_TOL_FP64, 1e-8)
     assert ref[0].max() > 0  # an action potential happened
