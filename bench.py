@@ -47,10 +47,13 @@ def parse_args():
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--adjoint-ms", type=float, default=20.0, help="simulated span of the adjoint measurement")
     p.add_argument("--skip-emg", action="store_true")
-    p.add_argument("--only", choices=["emg", "emg-cg", "shorten", "plain", "adjoint", "c2-accuracy"],
+    p.add_argument("--only", choices=["emg", "emg-cg", "shorten", "plain", "adjoint", "c2-accuracy", "c5"],
                    help="print one side measurement alone (profiling runs)")
     p.add_argument("--accuracy-ms", type=float, default=100.0, help="span of the batch accuracy comparison")
     p.add_argument("--skip-shorten", action="store_true")
+    p.add_argument("--skip-c5", action="store_true")
+    p.add_argument("--c5-ms", type=float, default=0.5, help="simulated span of the Shorten-at-scale run")
+    p.add_argument("--c5-adjoint-steps", type=int, default=4, help="Strang steps of the Shorten-at-scale adjoint")
     p.add_argument("--shorten-ms", type=float, default=0.02, help="simulated span of the Shorten timing (full grid)")
     p.add_argument("--shorten-accuracy-ms", type=float, default=5.0,
                    help="simulated span of the Shorten FP32-vs-FP64 comparison (16-fiber sample)")
@@ -282,6 +285,85 @@ def shorten_measurement(device: int, span_ms: float, accuracy_ms: float = 5.0):
     return out
 
 
+def c5_measurement(device: int, span_ms: float = 0.5, adjoint_steps: int = 4, subset_fibers: int = 16) -> dict:
+    """Shorten 2007 at scale with the three extensions, over a bounded span: 10,000 fibers of U[1000,2500]
+    nodes (17.5M nodes), 200 motor units, FP32 reaction with the autotuned method and launch shape, span_ms of
+    simulated time (the configuration's 100 ms take hours at this size); Vm after the span against the FP64
+    split solver on subset_fibers fibers of the system (same clamp nodes); and the FP64 adjoint of the sigma
+    field (loss 1/2 sum of Vm^2 at 32 sensors per fiber over the last adjoint_steps Strang steps) with the
+    memory plan of plan_adjoint for this device: checkpoint interval and sequential fiber shards."""
+    import torch
+    from opendihu_b200 import sharding as SH
+    from opendihu_b200 import solver as S
+    from opendihu_b200 import workloads as WL
+    from opendihu_b200 import accuracy as ACC
+    system = WL.shorten_scale(end_time=span_ms)
+    dt = system.dt_splitting
+    t_adj = span_ms - adjoint_steps * dt
+    out = {"workload": "Shorten 2007, %d fibers x U[1000,2500] (%d nodes), 200 MUs, dt0D 1e-5, dt_split 5e-4, "
+                       "%g ms" % (system.n_fibers, system.n_nodes, span_ms)}
+    with S.FastMonodomainSolver(system.copy(), method="auto", precision="fp32", device=device) as sv:
+        sv.setTimeSpan(0.0, 0.01)
+        sv.advanceTimeSpan()
+        sv.reset_timing()
+        n0 = sv.split_steps()
+        sv.setTimeSpan(0.01, t_adj)
+        sv.advanceTimeSpan()
+        states_adj = sv.states()
+        sv.setTimeSpan(t_adj, span_ms)
+        sv.advanceTimeSpan()
+        ms = sv.timing()["advance_ms"]
+        steps = sv.split_steps() - n0
+        vm32 = sv.vm()
+        out["fp32_forward"] = {"node_steps_per_s": system.n_nodes * steps / (ms / 1e3), "ms": ms,
+                               "strang_steps": steps, "method": sv.method,
+                               "tuning": {k: (sv.tuning or {}).get(k) for k in ("method", "steps_per_launch")}}
+    sub = np.unique(np.linspace(0, system.n_fibers - 1, subset_fibers).round().astype(np.int64))
+    ssys = WL.subset(system, sub)
+    with S.FastMonodomainSolver(ssys, method="split", precision="fp64", device=device) as sv:
+        sv.clamp_override = SH.shard_clamp_nodes(system, sub, SH.global_clamp_nodes(system))
+        sv.advanceTimeSpan()
+        vm64 = sv.vm()
+    vm32_sub = vm32[SH.node_index(system.fiber_offsets, sub)]
+    out["accuracy"] = {"sample": "%d fibers (%d nodes), FP64 split, same clamp nodes" % (len(sub), ssys.n_nodes),
+                       "vm_max_abs_diff_fp32_vs_fp64_mV": float(np.max(np.abs(vm32_sub - vm64))),
+                       "vm_range_mV": [float(vm64.min()), float(vm64.max())]}
+    del vm32, vm32_sub
+    # adjoint of sigma over the last Strang steps, from the FP32 run's state
+    win = system.copy()
+    win.states = states_adj
+    win.start_time, win.end_time = t_adj, span_ms
+    free, _ = torch.cuda.mem_get_info(device)
+    budget = 0.6 * free
+    plan = SH.plan_adjoint(win, t_adj, span_ms, budget)
+    sensors = ACC.traced_nodes(win, 32)
+    with S.FastMonodomainSolver(win, method="split", precision="fp64", device=device) as fw:
+        fw.advanceTimeSpan()        # warm-up (module load, factorization)
+        fw.reset_timing()
+        fw.rewind()
+        fw.set_states(states_adj)
+        fw.advanceTimeSpan()
+        fwd_ms = fw.timing()["advance_ms"]
+    sh = SH.ShardedSolver(win, devices=(device,), n_shards=plan["n_shards"], method="split", precision="fp64")
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    trace, grads = sh.adjoint(t_adj, span_ms, plan["checkpoint_every"], sensors, lambda tr, cols: tr)
+    torch.cuda.synchronize(device)
+    adj_s = time.perf_counter() - t0
+    sh.close()
+    out["adjoint"] = {"window": "%d Strang steps [%g, %g] ms, %d sensors, loss 1/2 sum Vm^2" % (
+                          plan["n_steps"], t_adj, span_ms, len(sensors)),
+                      "plan": {k: plan[k] for k in ("checkpoint_every", "n_shards", "bytes_per_node",
+                                                    "largest_shard_nodes")},
+                      "budget_bytes": budget, "peak_bytes_estimate": plan["largest_shard_nodes"] * plan["bytes_per_node"],
+                      "fp64_forward_ms": fwd_ms, "adjoint_wall_ms": adj_s * 1e3,
+                      "adjoint_over_forward": adj_s * 1e3 / fwd_ms,
+                      "timing": "adjoint: host wall clock around the sequential shards (checkpointed forward, "
+                                "backward, set-up of each shard); forward: CUDA events of one FP64 advance",
+                      "grad_sigma_norm": float(np.linalg.norm(grads["prefactor"] / (WL.AM * 0.58)))}
+    return out
+
+
 def emg_measurement(device: int, peak_hbm: float, cg_mesh=(97, 97, 297), cg_iterations: int = 160,
                     coupled: bool = True):
     """Coupled fibers + EMG (13 x 13 HH fibers x 1481 nodes, 25 x 25 x 149 3D nodes, one bidomain solve per
@@ -450,7 +532,7 @@ def main():
     if world > 1:
         # the side measurements (plain configuration, adjoint, EMG, Shorten, accuracy and CPU baseline) are
         # single-GPU numbers reported by the 1-GPU run; on N GPUs rank 0 would hold the other GPUs meanwhile
-        args.skip_adjoint = args.skip_emg = args.skip_shorten = args.skip_accuracy = True
+        args.skip_adjoint = args.skip_emg = args.skip_shorten = args.skip_accuracy = args.skip_c5 = True
     cg_mesh = tuple(int(x) for x in args.emg_cg_mesh.split(","))
     if args.only:
         if rank == 0:
@@ -461,6 +543,8 @@ def main():
                 out = {"plain_config_node_steps_per_s": plain_measurement(local)}
             elif args.only == "adjoint":
                 out = {"adjoint": adjoint_measurement(local, args.adjoint_ms)}
+            elif args.only == "c5":
+                out = {"c5": c5_measurement(local, args.c5_ms, args.c5_adjoint_steps)}
             elif args.only == "c2-accuracy":
                 out = {"c2_accuracy": ACC.batch_accuracy(WL.batched_hh(n_fibers=args.fibers, seed=0), local,
                                                          args.accuracy_ms)}
@@ -558,6 +642,8 @@ def main():
         side_line("emg", emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations))
     if rank == 0 and not args.skip_shorten:
         side_line("shorten", shorten_measurement(local, args.shorten_ms, args.shorten_accuracy_ms))
+    if rank == 0 and not args.skip_c5:
+        side_line("c5", c5_measurement(local, args.c5_ms, args.c5_adjoint_steps))
     if rank == 0 and not args.skip_accuracy:
         acc = ACC.batch_accuracy(system, local, args.accuracy_ms)
         side_line("c2_accuracy", acc)

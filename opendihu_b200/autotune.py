@@ -132,9 +132,16 @@ def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0
             return result
     k0 = 100
     for t, m, c in shapes:
+        try:
+            sec = _time_shape(system, precision, t, m, min(k0, n_steps), n_steps, device, c)
+        except N.FdmError as e:
+            if e.code != N.FDM_ERR_UNSUPPORTED:
+                raise
+            continue    # a combination the library does not build (a model without a fused kernel)
         trials.append({"method": "fused", "threads": t, "nodes_per_thread": m, "cluster_size": c,
-                       "steps_per_launch": min(k0, n_steps),
-                       "s_per_step": _time_shape(system, precision, t, m, min(k0, n_steps), n_steps, device, c)})
+                       "steps_per_launch": min(k0, n_steps), "s_per_step": sec})
+    if not trials:
+        raise N.FdmError(N.FDM_ERR_UNSUPPORTED, "no fused kernel is built for this workload")
     best = min(trials, key=lambda r: r["s_per_step"])
     if best["method"] == "split":
         result = dict(best)

@@ -57,6 +57,19 @@ def shorten_grid(n_fibers: int = 1369, n_nodes: int = 1481, end_time: float = 50
                           end_time=end_time, dt_0d=1e-5, dt_1d=5e-4, dt_splitting=5e-4, dt_repeated_call=5e-4, **kw)
 
 
+def shorten_scale(n_fibers: int = 10000, min_nodes: int = 1000, max_nodes: int = 2500, n_mus: int = 200,
+                  end_time: float = 100.0, seed: int = 0, **kw) -> FiberSystem:
+    """Shorten 2007 at scale: fiber lengths uniform in [1000, 2500] nodes (seeded), 200 motor units with
+    exponential sizes, Poisson firing 10-40 Hz sampled at 0.1/ms, Heun dt 1e-5 ms, Strang dt 5e-4 ms."""
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(min_nodes, max_nodes + 1, size=n_fibers)
+    mus = inputs.exponential_mu_distribution(n_fibers, n_mus, seed)
+    firing = inputs.poisson_firing_times(n_mus, max(end_time, 0.1), 0.1, 10.0, 40.0, seed)
+    return uniform_fibers(SHORTEN, lengths, 0.01, SIGMA / (AM * 0.58), firing_events=firing, motor_unit_no=mus,
+                          call_frequency=0.1, repeat_after_first_call=0.1, call_enable_begin=0.0,
+                          end_time=end_time, dt_0d=1e-5, dt_1d=5e-4, dt_splitting=5e-4, dt_repeated_call=5e-4, **kw)
+
+
 def differentiation_hh(n_fibers: int = 256, n_nodes: int = 1481, end_time: float = 20.0, n_sensors: int = 32,
                        seed: int = 1, **kw):
     """Differentiation configuration: HH, 256 fibers x 1481 nodes, per-fiber sigma ~ U[2.5, 5.0] mS/cm and
