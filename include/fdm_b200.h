@@ -103,6 +103,15 @@ int fdm_destroy(fdm_solver *s);
 /* message of the last failed call on s (or of the last failed fdm_create if s is NULL) */
 const char *fdm_last_error(const fdm_solver *s);
 
+/* Loads a run-time model module: a shared library compiled from a generated translation unit for one CellML
+ * model or parameter variant that is not built into this library (opendihu_b200/csrc/fdm_model_module.cuh;
+ * the Python settings layer generates and compiles it on demand, as the reference generates, compiles and
+ * dlopens a library from the model file: fast_monodomain_solver_gpu.tpp:106-205, the CellmlAdapter's
+ * libraryFilename option).  *model_id receives the number to pass as fdm_config.model (a module loaded again
+ * keeps its number).  Module models run the split method, the equilibrium skip and the adjoint; the fused
+ * method is built for the library's own models only. */
+int fdm_register_model_library(const char *path, int *model_id);
+
 /* model description: sizes and initial state values of the model's OpenCOR file */
 int fdm_model_info(int model, int *n_states, int *n_algebraics, int *n_parameters, double *states_initial);
 /* default value of every parameter slot: the raw CONSTANTS value for a constant parameter, 0 for an

@@ -39,7 +39,7 @@ EXPORTED = [
     "fdm_emg_potential_flow", "fdm_emg_set_direction", "fdm_emg_set_conductivity", "fdm_emg_set_fiber_mapping",
     "fdm_emg_map_fibers", "fdm_emg_map_values", "fdm_emg_set_vm", "fdm_emg_solve", "fdm_emg_get",
     "fdm_emg_get_stencil", "fdm_emg_timing", "fdm_debug_fail_allocation", "fdm_set_activation_recording",
-    "fdm_get_activation_steps",
+    "fdm_get_activation_steps", "fdm_register_model_library",
 ]
 
 #: fdm_emg_get fields of include/fdm_b200.h
@@ -108,6 +108,7 @@ def lib() -> C.CDLL:
         "fdm_set_trace": (C.c_int, [P, C.c_int, i64, C.c_int64]),
         "fdm_get_trace": (C.c_int, [P, d, i64]),
         "fdm_set_activation_recording": (C.c_int, [P, C.c_double, C.c_int]),
+        "fdm_register_model_library": (C.c_int, [C.c_char_p, i32]),
         "fdm_get_activation_steps": (C.c_int, [P, i32, i32]),
         "fdm_advance": (C.c_int, [P, C.c_double, C.c_double]),
         "fdm_advance_async": (C.c_int, [P, C.c_double, C.c_double]),

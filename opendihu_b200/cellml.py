@@ -1028,6 +1028,42 @@ def tree_from_json(j):
     raise ValueError(j)
 
 
+def model_to_json(model: Model) -> dict:
+    """The parsed model (its equations as expression trees, initial values, names) as plain JSON data."""
+    return {"name": model.name, "source": os.path.basename(model.source), "n_states": model.n_states,
+            "n_algebraics": model.n_algebraics, "n_constants": model.n_constants,
+            "states_initial": model.states_initial, "state_names": model.state_names,
+            "algebraic_names": model.algebraic_names, "constant_names": model.constant_names,
+            "uses_voi": model.uses_voi,
+            "constant_lines": [[i, _tree_to_json(e)] for i, e in model.constant_lines],
+            "lines": [[k, i, _tree_to_json(e)] for k, i, e in model.lines]}
+
+
+def model_from_json(j: dict) -> Model:
+    """Inverse of model_to_json: the constants are folded again from their assignments, in IEEE double."""
+    constant_lines = [(int(i), tree_from_json(e)) for i, e in j["constant_lines"]]
+    consts = [0.0] * int(j["n_constants"])
+    env = {"S": list(j["states_initial"]), "C": consts, "A": [], "R": [], "T": 0.0}
+    for idx, expr in constant_lines:
+        consts[idx] = eval_expr(expr, env)
+    return Model(name=j["name"], source=j["source"], n_states=int(j["n_states"]),
+                 n_algebraics=int(j["n_algebraics"]), n_constants=int(j["n_constants"]),
+                 states_initial=[float(x) for x in j["states_initial"]], constants=consts,
+                 constant_lines=constant_lines, lines=[(k, int(i), tree_from_json(e)) for k, i, e in j["lines"]],
+                 state_names=list(j["state_names"]), algebraic_names=list(j["algebraic_names"]),
+                 constant_names=list(j["constant_names"]), uses_voi=bool(j["uses_voi"]))
+
+
+def builtin_model(name: str) -> Model:
+    """A built-in model (one the library carries generated code for), from its generated description."""
+    gen = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "generated")
+    for fname, pa, pc in VARIANTS:
+        if os.path.splitext(fname)[0] == name:
+            with open(os.path.join(gen, f"{name}_{variant_tag(pa, pc)}.json")) as f:
+                return model_from_json(__import__("json").load(f)["model"])
+    raise KeyError(name)
+
+
 def generate_all(input_dir: str, cuda_dir: str, c_dir: str) -> List[str]:
     """(Re)generate the device and oracle model sources for every prebuilt variant."""
     written = []
@@ -1052,7 +1088,10 @@ def generate_all(input_dir: str, cuda_dir: str, c_dir: str) -> List[str]:
                        "state_names": model.state_names, "algebraic_names": model.algebraic_names,
                        "constant_names": model.constant_names, "uses_time": model.uses_voi,
                        "operations_per_rhs": count_operations(model, pa, pc),
-                       "rhs_lines": [[k, i, _tree_to_json(e)] for k, i, e in substitute_parameters(model, pa, pc)]},
+                       "rhs_lines": [[k, i, _tree_to_json(e)] for k, i, e in substitute_parameters(model, pa, pc)],
+                       # the model as parsed, before any parameter substitution: other parameter variants are
+                       # generated from it at run time (opendihu_b200/models.py)
+                       "model": model_to_json(model)},
                       f, indent=1)
         written.append(meta)
     return written

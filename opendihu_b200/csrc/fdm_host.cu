@@ -11,6 +11,7 @@
 // Time values are computed here with the exact C expressions of the reference; this file is
 // compiled with -ffp-contract=off so that no multiply-add is fused.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <atomic>
@@ -21,6 +22,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -373,6 +375,46 @@ extern "C" int fdm_model_parameter_defaults(int model, double* defaults)
     return fail(nullptr, FDM_ERR_ARG, "fdm_model_parameter_defaults: bad argument");
   std::memcpy(defaults, m->parameter_defaults, sizeof(double) * m->n_parameters);
   return FDM_OK;
+}
+
+extern "C" int fdm_register_model_library(const char* path, int* model_id)
+{
+  if (!path || !model_id)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_register_model_library: bad argument");
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+  if (!h) {
+    const char* why = dlerror();
+    return fail(nullptr, FDM_ERR_ARG, std::string("fdm_register_model_library: cannot load ") + path + ": " +
+                                          (why ? why : "unknown error"));
+  }
+  auto entry = (ModelModuleEntry)dlsym(h, "fdm_model_module_v1");
+  ModelModule m{};
+  if (!entry || entry(&m) != 0) {
+    dlclose(h);
+    return fail(nullptr, FDM_ERR_ARG, std::string("fdm_register_model_library: ") + path +
+                                          " is not a model module (no fdm_model_module_v1)");
+  }
+  if (m.abi != FDM_MODEL_MODULE_ABI) {
+    dlclose(h);
+    return fail(nullptr, FDM_ERR_ARG, std::string("fdm_register_model_library: ") + path +
+                                          " was built against another version of this library; rebuild it");
+  }
+  for (int k = 0; k < n_models(); k++) { // the same model loaded again: its existing number
+    const ModelDesc* d = model_desc(k);
+    if (d && d->name && m.desc.name && std::strcmp(d->name, m.desc.name) == 0) {
+      *model_id = k;
+      return FDM_OK;   // the library stays loaded (its handle is kept by the first registration)
+    }
+  }
+  const int id = register_model_module(m);
+  if (id < 0) {
+    dlclose(h);
+    return fail(nullptr, FDM_ERR_ARG, "fdm_register_model_library: too many model modules");
+  }
+  *model_id = id;
+  return FDM_OK;   // the library stays loaded for the life of the process
 }
 
 extern "C" int fdm_model_info(int model, int* n_states, int* n_algebraics, int* n_parameters, double* states_initial)

@@ -25,9 +25,33 @@ struct ModelDesc {
   bool fused_supported;
 };
 
-// model table (fdm_kernels_split.cu)
+// model table (fdm_kernels_split.cu): the built-in models, then the registered run-time model modules
 int n_models();
 const ModelDesc* model_desc(int model);
+
+// A run-time model module: a shared library built from a generated translation unit (fdm_model_module.cuh)
+// that holds the kernels of one further CellML model or parameter variant.  Its entry point
+// fdm_model_module_v1 fills this table; abi must equal FDM_MODEL_MODULE_ABI of the library that loads it (the
+// argument structures the two pass between them must have the same layout).
+struct ModelModule {
+  int abi;
+  ModelDesc desc;
+  cudaError_t (*reaction)(RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s);
+  cudaError_t (*cellml_rhs)(MathKind mk, int64_t n, double t, const double* states, const double* params,
+                            double* rates, double* algebraics, cudaStream_t s);
+  cudaError_t (*equilibrium_search)(MathKind mk, double* u, const double* u0, const double* params,
+                                    EquilibriumSearch* es, int64_t max_iterations, cudaStream_t s);
+  cudaError_t (*reaction_eq)(RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L, const EqSpec& e,
+                             cudaStream_t s);
+  cudaError_t (*adjoint_half)(MathKind mk, const AdjointArgs& a, cudaStream_t s);
+};
+#define FDM_MODEL_MODULE_ABI                                                                                     \
+  (int)(1000000 + 97 * sizeof(fdm::ReactionArgs) + 89 * sizeof(fdm::AdjointArgs) + 83 * sizeof(fdm::EqLayout) +   \
+        79 * sizeof(fdm::EqSpec) + 73 * sizeof(fdm::ModelDesc) + 71 * sizeof(fdm::EquilibriumSearch) +            \
+        67 * sizeof(fdm::SplitStep))
+typedef int (*ModelModuleEntry)(ModelModule* out);
+// registers a module's table; returns its model number (after the built-in ones) or -1
+int register_model_module(const ModelModule& m);
 
 // split path
 cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s);

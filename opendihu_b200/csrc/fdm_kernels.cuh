@@ -351,6 +351,50 @@ __device__ __forceinline__ void heun_step2(double& V0, double& V1, const fdm_f2*
     V1 = vstim;
 }
 
+// heun_step2 with Vm carried the way the gates are within a half step: Vf is the node pair's Vm rounded to
+// FP32 at the start of the half step and LV the sum of its Vm increments since then (FP32); the right-hand side
+// sees Vf + LV, and the caller adds LV to the FP64 Vm once, at the end of the half step (vm_fold).  A clamped
+// lane restarts from the stimulation value: its FP64 Vm is set, Vf holds the value, LV restarts at 0.  This
+// keeps FP64 <-> FP32 conversions and FP64 additions out of the substep loop.
+template<class Model>
+__device__ __forceinline__ void heun_step2_res(fdm_f2& Vf, fdm_f2& LV, double& V0, double& V1,
+                                               const fdm_f2* __restrict__ S, fdm_f2* __restrict__ L,
+                                               const fdm_f2* __restrict__ P, const fdm_f2 tr, fdm_f2 dtr, fdm_f2 hdt,
+                                               bool clamp0, bool clamp1, double vstim)
+{
+  constexpr int NS = Model::nStates;
+  const float vs = (float)vstim;
+  fdm_f2 y[NS], r[NS], ys[NS], r2[NS];
+  fdm_f2 alg[Model::nAlgebraics];
+  y[0] = Vf + LV;
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    y[s] = S[s - 1] + L[s - 1];
+  Model::template rates_fast2<fdm_math_exact>(tr, y, P, r, alg);
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    ys[s] = dtr * r[s] + y[s];
+  if (clamp0)
+    ys[0].v.x = vs;
+  if (clamp1)
+    ys[0].v.y = vs;
+  Model::template rates_fast2<fdm_math_exact>(tr, ys, P, r2, alg);
+#pragma unroll
+  for (int s = 1; s < NS; s++)
+    L[s - 1] = hdt * (r[s] + r2[s]) + L[s - 1];
+  LV = hdt * (r[0] + r2[0]) + LV;
+  if (clamp0) {
+    V0 = vstim;
+    Vf.v.x = vs;
+    LV.v.x = 0.f;
+  }
+  if (clamp1) {
+    V1 = vstim;
+    Vf.v.y = vs;
+    LV.v.y = 0.f;
+  }
+}
+
 // (S, L) -> (S + L rounded, the rounding error): the Fast2Sum normalization of a compensated pair
 __device__ __forceinline__ void normalize_pair(fdm_f2& S, fdm_f2& L)
 {
@@ -1563,6 +1607,15 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
                             << (8 * (j & 3));
       }
       auto node_on = [&](int j, int k) -> bool { return k >= (int)((gfirst[j >> 2] >> (8 * (j & 3))) & 0xffu); };
+      // paired nodes: Vm in FP32 over the half step (value at its start + the sum of the increments since)
+      fdm_f2 Vf[MP > 0 ? MP : 1], LV[MP > 0 ? MP : 1];
+      if constexpr (PAIR) {
+#pragma unroll
+        for (int p = 0; p < MP; p++) {
+          Vf[p] = fdm_f2((float)V[2 * p], (float)V[2 * p + 1]);
+          LV[p] = fdm_f2(0.f, 0.f);
+        }
+      }
 #pragma unroll 1
       for (int k = 0; k < k_end; k++) {
         const double t = xadd(t0, xmul((double)k, s.dt0));
@@ -1611,9 +1664,11 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
                     Pk[q].v.y = sv;
                 }
               }
-              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pk, t, dtr, hdt, false, false, a.vstim);
+              heun_step2_res<Model>(Vf[p], LV[p], V[j0], V[j0 + 1], S2[p], L2[p], Pk, fdm_f2((float)t), dtr, hdt,
+                                    false, false, a.vstim);
             } else {
-              heun_step2<Model>(V[j0], V[j0 + 1], S2[p], L2[p], Pp, t, dtr, hdt, stim0, stim1, a.vstim);
+              heun_step2_res<Model>(Vf[p], LV[p], V[j0], V[j0 + 1], S2[p], L2[p], Pp, fdm_f2((float)t), dtr, hdt,
+                                    stim0, stim1, a.vstim);
             }
           }
           if constexpr (M % 2 == 1) {
@@ -1631,10 +1686,13 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       }
       if constexpr (PAIR) {
 #pragma unroll
-        for (int p = 0; p < MP; p++)
+        for (int p = 0; p < MP; p++) {
+          V[2 * p] += (double)LV[p].v.x;
+          V[2 * p + 1] += (double)LV[p].v.y;
 #pragma unroll
           for (int q = 0; q < NSM; q++)
             normalize_pair(S2[p][q], L2[p][q]);
+        }
       }
       if (store_here) {
         const int k = s.n0 - 1;

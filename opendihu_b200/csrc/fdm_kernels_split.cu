@@ -1,7 +1,11 @@
 // Split-path kernels (reaction, diffusion, stimulation schedule) and the model table.
 #define FDM_COMMON_KERNELS_TU
+#include <atomic>
+#include <mutex>
+
 #include "fdm_internal.h"
 #include "fdm_equilibrium.cuh"
+#include "fdm_model_launch.cuh"
 
 #include "generated/hodgkin_huxley_1952_anone_c2_3_4.cuh"
 #include "generated/shorten_ocallaghan_davidson_soboleva_2007_a32_c65.cuh"
@@ -16,34 +20,40 @@ static const ModelDesc g_models[] = {
   {SH::name, SH::nStates, SH::nAlgebraics, SH::nParameters, SH::statesInitialValues, SH::parameterDefaults, false},
 };
 
-int n_models() { return (int)(sizeof(g_models) / sizeof(g_models[0])); }
+constexpr int kBuiltinModels = (int)(sizeof(g_models) / sizeof(g_models[0]));
+constexpr int kMaxModules = 64;
+
+// run-time model modules, appended by register_model_module and never removed (their libraries stay loaded)
+static ModelModule g_modules[kMaxModules];
+static std::atomic<int> g_n_modules{0};
+static std::mutex g_modules_mu;
+
+int n_models() { return kBuiltinModels + g_n_modules.load(std::memory_order_acquire); }
+
+static const ModelModule* module_of(int model)
+{
+  const int k = model - kBuiltinModels;
+  return (k >= 0 && k < g_n_modules.load(std::memory_order_acquire)) ? &g_modules[k] : nullptr;
+}
 
 const ModelDesc* model_desc(int model)
 {
-  if (model < 0 || model >= n_models())
-    return nullptr;
-  return &g_models[model];
+  if (model >= 0 && model < kBuiltinModels)
+    return &g_models[model];
+  const ModelModule* m = module_of(model);
+  return m ? &m->desc : nullptr;
 }
 
-template<class Model, class RR, class Math>
-static cudaError_t reaction_one(const ReactionArgs& a, cudaStream_t s)
+int register_model_module(const ModelModule& m)
 {
-  const int T = 128;
-  const int64_t blocks = (a.n_nodes + T - 1) / T;
-  if (blocks == 0)
-    return cudaSuccess;
-  reaction_kernel<Model, RR, Math><<<(unsigned)blocks, T, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
-template<class Model>
-static cudaError_t reaction_model(RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s)
-{
-  if (rk == REAL_F64)
-    return mk == MATH_EXACT ? reaction_one<Model, double, fdm_math_exact>(a, s)
-                            : reaction_one<Model, double, fdm_math_approx>(a, s);
-  return mk == MATH_EXACT ? reaction_one<Model, float, fdm_math_exact>(a, s)
-                          : reaction_one<Model, float, fdm_math_approx>(a, s);
+  std::lock_guard<std::mutex> lock(g_modules_mu);
+  const int k = g_n_modules.load(std::memory_order_relaxed);
+  if (k >= kMaxModules || m.abi != FDM_MODEL_MODULE_ABI)
+    return -1;
+  g_modules[k] = m;
+  g_modules[k].desc.fused_supported = false;   // modules carry the split-path, equilibrium and adjoint kernels
+  g_n_modules.store(k + 1, std::memory_order_release);
+  return kBuiltinModels + k;
 }
 
 cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s)
@@ -51,21 +61,11 @@ cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionA
   switch (model) {
   case 0: return reaction_model<HH>(rk, mk, a, s);
   case 1: return reaction_model<SH>(rk, mk, a, s);
-  default: return cudaErrorInvalidValue;
+  default: {
+    const ModelModule* m = module_of(model);
+    return m ? m->reaction(rk, mk, a, s) : cudaErrorInvalidValue;
   }
-}
-
-template<class Model>
-static cudaError_t cellml_rhs_model(MathKind mk, int64_t n, double t, const double* st, const double* p, double* r,
-                                    double* alg, cudaStream_t s)
-{
-  const int T = 128;
-  const unsigned blocks = (unsigned)((n + T - 1) / T);
-  if (mk == MATH_EXACT)
-    cellml_rhs_kernel<Model, fdm_math_exact><<<blocks, T, 0, s>>>(n, t, st, p, r, alg);
-  else
-    cellml_rhs_kernel<Model, fdm_math_approx><<<blocks, T, 0, s>>>(n, t, st, p, r, alg);
-  return cudaGetLastError();
+  }
 }
 
 cudaError_t launch_cellml_rhs(int model, MathKind mk, int64_t n, double t, const double* states, const double* params,
@@ -76,19 +76,11 @@ cudaError_t launch_cellml_rhs(int model, MathKind mk, int64_t n, double t, const
   switch (model) {
   case 0: return cellml_rhs_model<HH>(mk, n, t, states, params, rates, algebraics, s);
   case 1: return cellml_rhs_model<SH>(mk, n, t, states, params, rates, algebraics, s);
-  default: return cudaErrorInvalidValue;
+  default: {
+    const ModelModule* m = module_of(model);
+    return m ? m->cellml_rhs(mk, n, t, states, params, rates, algebraics, s) : cudaErrorInvalidValue;
   }
-}
-
-template<class Model>
-static cudaError_t equilibrium_search_model(MathKind mk, double* u, const double* u0, const double* P, EquilibriumSearch* es,
-                                     int64_t n, cudaStream_t s)
-{
-  if (mk == MATH_EXACT)
-    equilibrium_search_kernel<Model, fdm_math_exact><<<1, 1, 0, s>>>(u, u0, P, es, n);
-  else
-    equilibrium_search_kernel<Model, fdm_math_approx><<<1, 1, 0, s>>>(u, u0, P, es, n);
-  return cudaGetLastError();
+  }
 }
 
 cudaError_t launch_equilibrium_search(int model, MathKind mk, double* u, const double* u0, const double* params,
@@ -97,7 +89,10 @@ cudaError_t launch_equilibrium_search(int model, MathKind mk, double* u, const d
   switch (model) {
   case 0: return equilibrium_search_model<HH>(mk, u, u0, params, es, max_iterations, s);
   case 1: return equilibrium_search_model<SH>(mk, u, u0, params, es, max_iterations, s);
-  default: return cudaErrorInvalidValue;
+  default: {
+    const ModelModule* m = module_of(model);
+    return m ? m->equilibrium_search(mk, u, u0, params, es, max_iterations, s) : cudaErrorInvalidValue;
+  }
   }
 }
 
@@ -147,28 +142,6 @@ cudaError_t launch_diffusion(int n_fibers, const int64_t* fiber_offsets, const d
 }
 
 // ---- equilibrium skip ----
-template<class Model, class RR, class Math>
-static cudaError_t reaction_eq_one(const ReactionArgs& a, const EqLayout& L, const EqSpec& e, cudaStream_t s)
-{
-  const int T = 128;
-  const int64_t blocks = (e.nt + T - 1) / T;
-  if (blocks == 0)
-    return cudaSuccess;
-  reaction_eq_kernel<Model, RR, Math><<<(unsigned)blocks, T, 0, s>>>(a, L, e);
-  return cudaGetLastError();
-}
-
-template<class Model>
-static cudaError_t reaction_eq_model(RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L,
-                                     const EqSpec& e, cudaStream_t s)
-{
-  if (rk == REAL_F64)
-    return mk == MATH_EXACT ? reaction_eq_one<Model, double, fdm_math_exact>(a, L, e, s)
-                            : reaction_eq_one<Model, double, fdm_math_approx>(a, L, e, s);
-  return mk == MATH_EXACT ? reaction_eq_one<Model, float, fdm_math_exact>(a, L, e, s)
-                          : reaction_eq_one<Model, float, fdm_math_approx>(a, L, e, s);
-}
-
 cudaError_t launch_equilibrium_half(int model, RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L,
                                     const EqSpec& e, uint8_t* info, uint8_t* prefix, uint8_t* block_agg, int n_states,
                                     bool trace, cudaStream_t s)
@@ -177,7 +150,12 @@ cudaError_t launch_equilibrium_half(int model, RealKind rk, MathKind mk, const R
   switch (model) {
   case 0: ce = reaction_eq_model<HH>(rk, mk, a, L, e, s); break;
   case 1: ce = reaction_eq_model<SH>(rk, mk, a, L, e, s); break;
-  default: return cudaErrorInvalidValue;
+  default: {
+    const ModelModule* m = module_of(model);
+    if (!m)
+      return cudaErrorInvalidValue;
+    ce = m->reaction_eq(rk, mk, a, L, e, s);
+  }
   }
   if (ce != cudaSuccess || L.n_buffers == 0)
     return ce;
@@ -199,26 +177,15 @@ cudaError_t launch_equilibrium_half(int model, RealKind rk, MathKind mk, const R
   return cudaGetLastError();
 }
 
-template<class Model>
-static cudaError_t adjoint_model(MathKind mk, const AdjointArgs& a, cudaStream_t s)
-{
-  const int T = 128;
-  const int64_t blocks = (a.n_nodes + T - 1) / T;
-  if (blocks == 0)
-    return cudaSuccess;
-  if (mk == MATH_EXACT)
-    adjoint_half_kernel<Model, fdm_math_exact><<<(unsigned)blocks, T, 0, s>>>(a);
-  else
-    adjoint_half_kernel<Model, fdm_math_approx><<<(unsigned)blocks, T, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_adjoint_half(int model, MathKind mk, const AdjointArgs& a, cudaStream_t s)
 {
   switch (model) {
   case 0: return adjoint_model<HH>(mk, a, s);
   case 1: return adjoint_model<SH>(mk, a, s);
-  default: return cudaErrorInvalidValue;
+  default: {
+    const ModelModule* m = module_of(model);
+    return m ? m->adjoint_half(mk, a, s) : cudaErrorInvalidValue;
+  }
   }
 }
 

@@ -25,6 +25,7 @@ import numpy as np
 from . import _native as N
 from . import cellml as CM
 from . import inputs
+from . import models as MD
 from . import output
 
 SCHEMES = {"ImplicitEuler": 0, "CrankNicolson": 1}
@@ -220,10 +221,10 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         raise ValueError("settings: no fibers")
     f0 = fibers[0]
     cellml = f0["cellml"]
-    model = os.path.splitext(os.path.basename(cellml["modelFilename"]))[0]
-    if model not in N.MODEL_IDS:
-        raise ValueError(f"settings: model {model!r} is not built into the library (have {sorted(N.MODEL_IDS)})")
-    ns, na, npar, init, defaults = model_sizes(model)
+    model_file = cellml["modelFilename"]
+    if not os.path.isabs(model_file):
+        model_file = os.path.join(base_dir, model_file)
+    model = os.path.splitext(os.path.basename(model_file))[0]
 
     # geometry
     lengths = []
@@ -240,11 +241,17 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
     prefactor = np.array([float(fb["fem"].get("prefactor", 1.0)) for fb in fibers])
 
     # parameters: map the settings' parameter list onto the built variant's slots
-    pa_var, pc_var = VARIANT_PARAMETERS[model]
     if cellml.get("mappings"):
         # parameters and transfer slots by name (00_cellml_adapter_base.tpp:160-607); the key replaces
         # parametersUsedAs*, statesForTransfer and algebraicsForTransfer
-        mp = CM.parse_mappings(cellml["mappings"], CM.model_variable_names(model))
+        if model in VARIANT_PARAMETERS:
+            names = CM.model_variable_names(model)
+        elif os.path.exists(model_file):
+            m = CM.parse_model_file(model_file)
+            names = {"state": m.state_names, "algebraic": m.algebraic_names, "constant": m.constant_names}
+        else:
+            raise ValueError(f"settings: model file {model_file!r} not found")
+        mp = CM.parse_mappings(cellml["mappings"], names)
         pa, pc = mp["parametersUsedAsAlgebraic"], mp["parametersUsedAsConstant"]
         st_transfer, alg_transfer = mp["statesForTransfer"], mp["algebraicsForTransfer"]
     else:
@@ -252,9 +259,14 @@ def parse_settings(config: dict, base_dir: str = ".") -> FiberSystem:
         pc = [int(x) for x in _as_list(cellml.get("parametersUsedAsConstant", []))]
         st_transfer = [int(x) for x in _as_list(cellml.get("statesForTransfer", [0]))]
         alg_transfer = [int(x) for x in _as_list(cellml.get("algebraicsForTransfer", []))]
-    if tuple(pa) != tuple(pa_var) or any(c not in pc_var for c in pc):
-        raise ValueError(f"settings: parametersUsedAsAlgebraic={pa}, parametersUsedAsConstant={pc} is not a prebuilt "
-                         f"variant of {model} (algebraic {list(pa_var)}, constants within {list(pc_var)})")
+    if model in VARIANT_PARAMETERS and MD.builtin_variant(model, pa, pc):
+        pa_var, pc_var = VARIANT_PARAMETERS[model]
+    else:
+        # a variant (or model) the library does not carry: generated, compiled and loaded as a model module, as
+        # the reference generates and compiles its model library at run time (gpu.tpp:106-205)
+        model = MD.load_model(model, pa, pc, model_file=model_file if os.path.exists(model_file) else None)
+        pa_var, pc_var = tuple(pa), tuple(pc)
+    ns, na, npar, init, defaults = model_sizes(model)
     n_user = len(pa) + len(pc)
     slot_of = list(range(len(pa))) + [len(pa_var) + pc_var.index(c) for c in pc]
     n_nodes = int(off[-1])

@@ -127,3 +127,43 @@ def test_shorten_adjoint_central_differences():
         assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-8, (fd, ad)
     finally:
         eng.close()
+
+
+@pytest.mark.slow
+def test_adjoint_at_configuration_size_against_central_differences():
+    """The differentiation configuration as specified: 256 HH fibers x 1481 nodes, per-fiber sigma ~ U[2.5, 5]
+    and g_Na, g_K scales ~ U[0.8, 1.2] (seed 1), loss = sum of squared Vm differences at 32 sensors per fiber over
+    20 ms against the trace of a second parameter set (seed 2), checkpoint every 100 Strang steps.  The adjoint
+    gradient of sigma, g_Na scale and g_K scale of two fibers against central differences with relative step
+    h = 1e-6 of the CUDA FP64 forward."""
+    dsys, sigma, s_na, s_k, sensors = WL.differentiation_hh(end_time=20.0, seed=1)
+    _, sigma2, s_na2, s_k2, _ = WL.differentiation_hh(end_time=20.0, seed=2)
+    eng = ADJ.AdjointEngine(dsys, sensors, checkpoint_every=100)
+    lengths = np.diff(dsys.fiber_offsets)
+    fiber_of = np.repeat(np.arange(dsys.n_fibers), lengths)
+    try:
+        target = eng.forward(sigma2 / (WL.AM * WL.CM), WL.hh_parameters(dsys, s_na2, s_k2))
+
+        def loss(sig, sna, sk):
+            tr = eng.forward(sig / (WL.AM * WL.CM), WL.hh_parameters(dsys, sna, sk))
+            return float(((tr - target) ** 2).sum()), tr
+
+        L0, tr = loss(sigma, s_na, s_k)
+        assert tr.shape == (20000, 256 * 32)
+        g = eng.backward(2.0 * (tr - target))
+        g_sigma = g["prefactor"] / (WL.AM * WL.CM)
+        g_na = np.bincount(fiber_of, g["parameters"][1] * 120.0, minlength=dsys.n_fibers)
+        g_k = np.bincount(fiber_of, g["parameters"][2] * 36.0, minlength=dsys.n_fibers)
+        for f in (0, 255):
+            for name, vec, grad in (("sigma", sigma, g_sigma), ("g_Na", s_na, g_na), ("g_K", s_k, g_k)):
+                h = 1e-6 * vec[f]
+                plus, minus = vec.copy(), vec.copy()
+                plus[f] += h
+                minus[f] -= h
+                args_p = {"sigma": (plus, s_na, s_k), "g_Na": (sigma, plus, s_k), "g_K": (sigma, s_na, plus)}[name]
+                args_m = {"sigma": (minus, s_na, s_k), "g_Na": (sigma, minus, s_k), "g_K": (sigma, s_na, minus)}[name]
+                fd = (loss(*args_p)[0] - loss(*args_m)[0]) / (2 * h)
+                print(name, f, grad[f], fd)
+                assert abs(grad[f] - fd) <= 1e-4 * max(abs(fd), 1e-6 * abs(L0)), (name, f, grad[f], fd)
+    finally:
+        eng.close()
