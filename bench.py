@@ -52,6 +52,7 @@ def parse_args():
     p.add_argument("--accuracy-ms", type=float, default=100.0, help="span of the batch accuracy comparison")
     p.add_argument("--skip-shorten", action="store_true")
     p.add_argument("--skip-c5", action="store_true")
+    p.add_argument("--plain-legs", default="", help="comma-separated legs of --only plain (default: all)")
     p.add_argument("--c5-ms", type=float, default=0.5, help="simulated span of the Shorten-at-scale run")
     p.add_argument("--c5-adjoint-steps", type=int, default=4, help="Strang steps of the Shorten-at-scale adjoint")
     p.add_argument("--shorten-ms", type=float, default=0.02, help="simulated span of the Shorten timing (full grid)")
@@ -212,7 +213,7 @@ def adjoint_measurement(device: int, span_ms: float) -> dict:
             "grad_norm_gna_scale": float(np.linalg.norm(g_na))}
 
 
-def plain_measurement(device: int) -> dict:
+def plain_measurement(device: int, legs=None) -> dict:
     """The plain-method configuration (16 HH fibers x 1481 nodes, implicit Euler, 10 ms): the FP64 split path
     with CUDA graphs and the fused kernel (cluster mode: few fibers) in FP64 and FP32, 9 ms after 1 ms warm-up."""
     from opendihu_b200 import solver as S
@@ -222,6 +223,8 @@ def plain_measurement(device: int) -> dict:
     for name, method, prec in (("fp64_split", "split", "fp64"), ("fp64_fused", "fused", "fp64"),
                                ("fp32_fused", "fused", "fp32"), ("fp64_auto", "auto", "fp64"),
                                ("fp32_auto", "auto", "fp32")):
+        if legs and name not in legs:
+            continue
         with S.FastMonodomainSolver(c1.copy(), method=method, precision=prec, device=device) as sv:
             sv.setTimeSpan(0.0, 1.0)
             sv.advanceTimeSpan()
@@ -540,7 +543,8 @@ def main():
                 out = {"emg": emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations,
                                               coupled=args.only == "emg")}
             elif args.only == "plain":
-                out = {"plain_config_node_steps_per_s": plain_measurement(local)}
+                out = {"plain_config_node_steps_per_s": plain_measurement(
+                    local, args.plain_legs.split(",") if args.plain_legs else None)}
             elif args.only == "adjoint":
                 out = {"adjoint": adjoint_measurement(local, args.adjoint_ms)}
             elif args.only == "c5":

@@ -1462,16 +1462,19 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   };
 
   // coefficients into shared memory (zero beyond the bin: those nodes carry x = 0); the forward sweep's
-  // inv * d is formed as (inv l) u_{i-1} + (inv m) u_i + (inv r) u_{i+1}
-  for (int q = tid; q < CAP; q += T) {
+  // inv * d is formed as (inv l) u_{i-1} + (inv m) u_i + (inv r) u_{i+1}.  The per-node shared arrays hold
+  // node j of thread t (bin node t * M + j) at slot j * T + t: a warp's accesses to one j are consecutive
+  // words, free of bank conflicts
+  for (int sl = tid; sl < CAP; sl += T) {
+    const int q = (sl % T) * M + sl / T;
     const bool ok = q < nb;
     const int64_t g = ok ? global_node(q) : 0;
     const double inv = ok ? a.coef[1 * a.stride + g] : 0.0;
-    sc[0 * CAP + q] = ok ? a.coef[0 * a.stride + g] : 0.0;
-    sc[1 * CAP + q] = ok ? a.coef[2 * a.stride + g] : 0.0;
+    sc[0 * CAP + sl] = ok ? a.coef[0 * a.stride + g] : 0.0;
+    sc[1 * CAP + sl] = ok ? a.coef[2 * a.stride + g] : 0.0;
 #pragma unroll
     for (int k = 3; k < 6; k++)
-      sc[(k - 1) * CAP + q] = ok ? inv * a.coef[k * a.stride + g] : 0.0;
+      sc[(k - 1) * CAP + sl] = ok ? inv * a.coef[k * a.stride + g] : 0.0;
   }
 
   const RR* pr = (const RR*)a.params;
@@ -1497,14 +1500,14 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     for (int p = 0; p < Model::nParameters; p++)
       P[j][p] = ok ? pr[p * a.stride + i] : (RR)0;
     const int cfj = ok ? a.clamp_fiber[i] : -1;
-    s_cf[q] = cfj;
+    s_cf[j * T + tid] = cfj;
     cmask |= (cfj >= 0 ? 1u : 0u) << j;
-    s_ts[q] = (ok && a.trace_slot) ? a.trace_slot[i] : -1;
-    s_gate[q] = (ok && a.gate) ? a.gate[i] : 0;
+    s_ts[j * T + tid] = (ok && a.trace_slot) ? a.trace_slot[i] : -1;
+    s_gate[j * T + tid] = (ok && a.gate) ? a.gate[i] : 0;
   }
   // stimulation bit of node j at substep bit `bit` (junction nodes only read their fiber's bit)
   auto node_stim = [&](int j, int bit) -> bool {
-    return ((cmask >> j) & 1u) && stim_bit(a.flags, a.words_per_fiber, s_cf[tid * M + j], bit);
+    return ((cmask >> j) & 1u) && stim_bit(a.flags, a.words_per_fiber, s_cf[j * T + tid], bit);
   };
   // FP32 exact-exponential reaction: nodes (2p, 2p+1) advance together in packed FP32 (heun_step2);
   // an odd last node runs alone
@@ -1603,7 +1606,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       if constexpr (gate_on) {
 #pragma unroll
         for (int j = 0; j < M; j++)
-          gfirst[j >> 2] |= (unsigned)gate_first(a.gate_start, a.gate_stride, s_gate[tid * M + j], step * 2 + half)
+          gfirst[j >> 2] |= (unsigned)gate_first(a.gate_start, a.gate_stride, s_gate[j * T + tid], step * 2 + half)
                             << (8 * (j & 3));
       }
       auto node_on = [&](int j, int k) -> bool { return k >= (int)((gfirst[j >> 2] >> (8 * (j & 3))) & 0xffu); };
@@ -1733,7 +1736,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       double d[M];
 #pragma unroll
       for (int j = 0; j < M; j++) {
-        const int q = tid * M + j;
+        const int q = j * T + tid;
         const double um = j > 0 ? V[j - 1] : vprev;
         const double up = j < M - 1 ? V[j + 1] : vnext;
         d[j] = sc[2 * CAP + q] * um + sc[3 * CAP + q] * V[j] + sc[4 * CAP + q] * up;
@@ -1741,7 +1744,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       Affine acc{1.0, 0.0};
 #pragma unroll
       for (int j = 0; j < M; j++) {
-        const int q = tid * M + j;
+        const int q = j * T + tid;
         acc = compose(acc, Affine{sc[0 * CAP + q], d[j]});
       }
       Affine tot_f;
@@ -1749,14 +1752,14 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       double dp = cluster_incoming(ex_f, tot_f, false);
 #pragma unroll
       for (int j = 0; j < M; j++) {
-        const int q = tid * M + j;
+        const int q = j * T + tid;
         dp = sc[0 * CAP + q] * dp + d[j];
         d[j] = dp;
       }
       Affine bacc{1.0, 0.0};
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
-        const int q = tid * M + j;
+        const int q = j * T + tid;
         bacc = compose(bacc, Affine{-sc[1 * CAP + q], d[j]});
       }
       __syncthreads(); // sF/sG reuse
@@ -1765,7 +1768,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       double x = cluster_incoming(ex_b, tot_b, true);
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
-        const int q = tid * M + j;
+        const int q = j * T + tid;
         x = -sc[1 * CAP + q] * x + d[j];
         V[j] = x;
       }
@@ -1774,8 +1777,8 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     if (a.trace_slot) {
 #pragma unroll
       for (int j = 0; j < M; j++)
-        if (s_ts[tid * M + j] >= 0)
-          record_trace(a.trace, a.n_trace, a.trace_capacity, a.act, s_ts[tid * M + j], s.global_no, V[j]);
+        if (s_ts[j * T + tid] >= 0)
+          record_trace(a.trace, a.n_trace, a.trace_capacity, a.act, s_ts[j * T + tid], s.global_no, V[j]);
     }
   }
 
