@@ -307,57 +307,20 @@ __device__ __forceinline__ void heun_step(double& V, RR* __restrict__ S, RR* __r
   }
 }
 
-// The FP32 Heun step of two nodes at once, over fdm_f2 pairs (packed FP32 instructions): Vm of each
-// node in FP64; every other state is a pair (S, L) whose sum is its value.  dtr / hdt are the step width
-// and its half per node (a node that skips the substep has 0: y* = y, and S, L, Vm stay as they are).
-// Within a half step the
-// increments dt/2 (f + f*) are summed into L and the right-hand side sees S + L; normalize_pair
-// folds L back into S (Fast2Sum) at the end of the half step.  L stays of the size of a few
-// increments, so no increment is lost against S (the stagnation the compensation exists for) at
-// four packed operations per state and substep instead of the seven of a Fast2Sum per substep.
-// Used with the FP32 exact-exponential policy only.
+// The FP32 Heun step of two nodes at once, over fdm_f2 pairs (packed FP32 instructions).  Every state
+// other than Vm is a pair (S, L) whose sum is its value: within a half step the increments dt/2 (f + f*) are
+// summed into L and the right-hand side sees S + L; normalize_pair folds L back into S (Fast2Sum) at the end
+// of the half step.  L stays of the size of a few increments, so no increment is lost against S (the
+// stagnation the compensation exists for) at four packed operations per state and substep instead of the
+// seven of a Fast2Sum per substep.  Vm is carried the same way: Vf is the node pair's Vm rounded to FP32 at
+// the start of the half step and LV the sum of its increments since then; the right-hand side sees Vf + LV,
+// and the caller adds LV to the FP64 Vm once, at the end of the half step, so no FP64 <-> FP32 conversion
+// and no FP64 addition is left in the substep loop.  A clamped lane restarts from the stimulation value: its
+// FP64 Vm is set, Vf holds the value, LV restarts at 0.  dtr / hdt are the step width and its half per node
+// (a node that skips the substep has 0: y* = y, and the states stay as they are).  Used with the FP32
+// exact-exponential policy only.
 template<class Model>
-__device__ __forceinline__ void heun_step2(double& V0, double& V1, const fdm_f2* __restrict__ S,
-                                           fdm_f2* __restrict__ L, const fdm_f2* __restrict__ P, double t,
-                                           fdm_f2 dtr, fdm_f2 hdt, bool clamp0, bool clamp1, double vstim)
-{
-  constexpr int NS = Model::nStates;
-  fdm_f2 y[NS], r[NS], ys[NS], r2[NS];
-  fdm_f2 alg[Model::nAlgebraics];
-  y[0] = fdm_f2((float)V0, (float)V1);
-#pragma unroll
-  for (int s = 1; s < NS; s++)
-    y[s] = S[s - 1] + L[s - 1];
-  const fdm_f2 tr((float)t);
-  Model::template rates_fast2<fdm_math_exact>(tr, y, P, r, alg);
-#pragma unroll
-  for (int s = 0; s < NS; s++)
-    ys[s] = dtr * r[s] + y[s];
-  const float vs = (float)vstim;
-  if (clamp0)
-    ys[0].v.x = vs;
-  if (clamp1)
-    ys[0].v.y = vs;
-  Model::template rates_fast2<fdm_math_exact>(tr, ys, P, r2, alg);
-  const fdm_f2 dv = hdt * (r[0] + r2[0]);
-  V0 += (double)dv.v.x;
-  V1 += (double)dv.v.y;
-#pragma unroll
-  for (int s = 1; s < NS; s++)
-    L[s - 1] = hdt * (r[s] + r2[s]) + L[s - 1];
-  if (clamp0)
-    V0 = vstim;
-  if (clamp1)
-    V1 = vstim;
-}
-
-// heun_step2 with Vm carried the way the gates are within a half step: Vf is the node pair's Vm rounded to
-// FP32 at the start of the half step and LV the sum of its Vm increments since then (FP32); the right-hand side
-// sees Vf + LV, and the caller adds LV to the FP64 Vm once, at the end of the half step (vm_fold).  A clamped
-// lane restarts from the stimulation value: its FP64 Vm is set, Vf holds the value, LV restarts at 0.  This
-// keeps FP64 <-> FP32 conversions and FP64 additions out of the substep loop.
-template<class Model>
-__device__ __forceinline__ void heun_step2_res(fdm_f2& Vf, fdm_f2& LV, double& V0, double& V1,
+__device__ __forceinline__ void heun_step2(fdm_f2& Vf, fdm_f2& LV, double& V0, double& V1,
                                                const fdm_f2* __restrict__ S, fdm_f2* __restrict__ L,
                                                const fdm_f2* __restrict__ P, const fdm_f2 tr, fdm_f2 dtr, fdm_f2 hdt,
                                                bool clamp0, bool clamp1, double vstim)
@@ -1667,10 +1630,10 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
                     Pk[q].v.y = sv;
                 }
               }
-              heun_step2_res<Model>(Vf[p], LV[p], V[j0], V[j0 + 1], S2[p], L2[p], Pk, fdm_f2((float)t), dtr, hdt,
+              heun_step2<Model>(Vf[p], LV[p], V[j0], V[j0 + 1], S2[p], L2[p], Pk, fdm_f2((float)t), dtr, hdt,
                                     false, false, a.vstim);
             } else {
-              heun_step2_res<Model>(Vf[p], LV[p], V[j0], V[j0 + 1], S2[p], L2[p], Pp, fdm_f2((float)t), dtr, hdt,
+              heun_step2<Model>(Vf[p], LV[p], V[j0], V[j0 + 1], S2[p], L2[p], Pp, fdm_f2((float)t), dtr, hdt,
                                     stim0, stim1, a.vstim);
             }
           }
