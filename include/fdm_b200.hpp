@@ -372,6 +372,41 @@ class FastMonodomainSolver {
     h_ = nullptr;
   }
 
+  /* Vm at the given nodes after every Strang step from now on (fdm_set_trace; rows count from this call) and,
+   * with capacityPerNode > 0, the Strang steps after which their Vm rose above threshold
+   * (fdm_set_activation_recording) */
+  void traceNodes(const std::vector<int64_t>& nodes, int64_t capacity, double threshold = 0.0,
+                  int capacityPerNode = 0)
+  {
+    initialize();
+    trace_nodes_ = nodes;
+    act_cap_ = capacityPerNode;
+    check(fdm_set_trace(h_, (int)nodes.size(), nodes.data(), capacity));
+    if (capacityPerNode > 0)
+      check(fdm_set_activation_recording(h_, threshold, capacityPerNode));
+  }
+  /* the traced Vm, [step * nodes + k] */
+  std::vector<double> trace()
+  {
+    int64_t n = 0;
+    check(fdm_get_trace(h_, nullptr, &n));
+    std::vector<double> out((size_t)(n * (int64_t)trace_nodes_.size()));
+    if (!out.empty())
+      check(fdm_get_trace(h_, out.data(), &n));
+    return out;
+  }
+  /* per traced node the Strang steps of its threshold crossings (at most capacityPerNode each) */
+  std::vector<std::vector<int>> activationSteps()
+  {
+    std::vector<int> counts(trace_nodes_.size()), steps(trace_nodes_.size() * (size_t)act_cap_);
+    check(fdm_get_activation_steps(h_, counts.data(), steps.data()));
+    std::vector<std::vector<int>> out(trace_nodes_.size());
+    for (size_t k = 0; k < out.size(); k++)
+      for (int j = 0; j < counts[k] && j < act_cap_; j++)
+        out[k].push_back(steps[k * (size_t)act_cap_ + (size_t)j]);
+    return out;
+  }
+
   /* StimulationLogging: from now on every stimulation begin is recorded (fdm_set_stimulation_log); the capacity
    * grows before each advance to what its span can need */
   void enableStimulationLog()
@@ -530,6 +565,8 @@ class FastMonodomainSolver {
   double current_time_ = 0.0;  // the reference's currentTime_: end of the last RepeatedCall piece
   int piece_steps_ = 0;        // its number of split steps (nTimeStepsSplitting_)
   bool log_on_ = false;
+  std::vector<int64_t> trace_nodes_;
+  int act_cap_ = 0;
   bool equilibrium_done_ = false;
   int64_t equilibrium_iterations_ = 0;
 };
