@@ -523,6 +523,20 @@ def side_line(name: str, value) -> None:
     print(json.dumps({"side": name, name: value}), flush=True)
 
 
+def side(name: str, fn):
+    """Runs one side measurement and prints its line; a failure is printed as the measurement's error and does
+    not stop the benchmark (the headline line is printed regardless)."""
+    try:
+        value = fn()
+    except Exception as e:  # noqa: BLE001 - reported, the headline still follows
+        import traceback
+        print(json.dumps({"side": name, "error": f"{type(e).__name__}: {e}",
+                          "where": traceback.format_exc().strip().splitlines()[-3:]}), flush=True)
+        return None
+    side_line(name, value)
+    return value
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -637,20 +651,17 @@ def main():
     # side measurements, each printed as its own line before the headline line
     plain_cfg = adj = acc = cpu = None
     if rank == 0 and not args.skip_fp64 and world == 1:
-        plain_cfg = plain_measurement(local)
-        side_line("plain_config_node_steps_per_s", plain_cfg)
+        plain_cfg = side("plain_config_node_steps_per_s", lambda: plain_measurement(local))
     if rank == 0 and not args.skip_adjoint:
-        adj = adjoint_measurement(local, args.adjoint_ms)
-        side_line("adjoint", adj)
+        adj = side("adjoint", lambda: adjoint_measurement(local, args.adjoint_ms))
     if rank == 0 and not args.skip_emg:
-        side_line("emg", emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations))
+        side("emg", lambda: emg_measurement(local, peaks()[0], cg_mesh, args.emg_cg_iterations))
     if rank == 0 and not args.skip_shorten:
-        side_line("shorten", shorten_measurement(local, args.shorten_ms, args.shorten_accuracy_ms))
+        side("shorten", lambda: shorten_measurement(local, args.shorten_ms, args.shorten_accuracy_ms))
     if rank == 0 and not args.skip_c5:
-        side_line("c5", c5_measurement(local, args.c5_ms, args.c5_adjoint_steps))
+        side("c5", lambda: c5_measurement(local, args.c5_ms, args.c5_adjoint_steps))
     if rank == 0 and not args.skip_accuracy:
-        acc = ACC.batch_accuracy(system, local, args.accuracy_ms)
-        side_line("c2_accuracy", acc)
+        acc = side("c2_accuracy", lambda: ACC.batch_accuracy(system, local, args.accuracy_ms, chunk_ms=2.0))
         # the oracle's CPU throughput on a bounded sample of the batch, all host threads, and one thread (the
         # reference's vc path runs one thread per MPI rank)
         threads = os.cpu_count() or 1

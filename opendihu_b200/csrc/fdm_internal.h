@@ -88,12 +88,15 @@ struct FusedShape {
   int threads, nodes_per_thread;
 };
 int fused_shapes(FusedShape* out, int capacity);
-// cluster mode shapes (threads per CTA, nodes per thread); a fiber spans up to 8 CTAs of one cluster
+// cluster mode shapes (threads per CTA, nodes per thread); a fiber spans up to 8 CTAs of one cluster.  One node
+// per thread gives the few-fiber case the most independent Heun chains per SM
 #define FDM_CLUSTER_SHAPES(X) \
   X(128, 2)                   \
   X(256, 2)                   \
   X(512, 2)                   \
-  X(256, 4)
+  X(256, 4)                   \
+  X(192, 1)                   \
+  X(256, 1)
 constexpr int FDM_MAX_CLUSTER = 8;
 int cluster_shapes(FusedShape* out, int capacity);
 // one fiber per cluster of csize CTAs (FP32/FP64 reaction with exact exponentials, no onlyComputeIfHasBeenStimulated)

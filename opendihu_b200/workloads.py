@@ -35,12 +35,16 @@ def batched_hh(n_fibers: int = 4096, min_nodes: int = 500, max_nodes: int = 2500
     """Batching + precision configuration: HH, fiber lengths uniform in [500, 2500] nodes (seeded),
     dx 0.01 cm, fibers assigned to 100 motor units by a seeded exponential size distribution, per-MU
     Poisson firing at 10-40 Hz sampled at the 0.1/ms call frequency, Crank-Nicolson, dt as the plain
-    configuration."""
+    configuration, junction = NMJ node and its two neighbours of each fiber."""
     rng = np.random.default_rng(seed)
     lengths = rng.integers(min_nodes, max_nodes + 1, size=n_fibers)
     mus = inputs.exponential_mu_distribution(n_fibers, n_mus, seed)
     firing = inputs.poisson_firing_times(n_mus, end_time, 0.1, 10.0, 40.0, seed)
     kw.setdefault("diffusion_scheme", "CrankNicolson")
+    # fibers of uneven length: each fiber's junction is its own NMJ node and its two neighbours (the rule of the
+    # reference's GPU path); the vc path's rule attributes point buffers to fibers as if all had the length of
+    # the first (fast_monodomain_solver_compute.tpp:158-161) and would leave most junctions unstimulated
+    kw.setdefault("clamp_rule", "center")
     return uniform_fibers(HH, lengths, 0.01, SIGMA / (AM * CM), firing_events=firing, motor_unit_no=mus,
                           call_frequency=0.1, repeat_after_first_call=0.1, call_enable_begin=0.0,
                           end_time=end_time, dt_0d=1e-4, dt_1d=1e-3, dt_splitting=1e-3, dt_repeated_call=1e-3, **kw)
@@ -65,6 +69,7 @@ def shorten_scale(n_fibers: int = 10000, min_nodes: int = 1000, max_nodes: int =
     lengths = rng.integers(min_nodes, max_nodes + 1, size=n_fibers)
     mus = inputs.exponential_mu_distribution(n_fibers, n_mus, seed)
     firing = inputs.poisson_firing_times(n_mus, max(end_time, 0.1), 0.1, 10.0, 40.0, seed)
+    kw.setdefault("clamp_rule", "center")   # uneven lengths: each fiber's own junction (see batched_hh)
     return uniform_fibers(SHORTEN, lengths, 0.01, SIGMA / (AM * 0.58), firing_events=firing, motor_unit_no=mus,
                           call_frequency=0.1, repeat_after_first_call=0.1, call_enable_begin=0.0,
                           end_time=end_time, dt_0d=1e-5, dt_1d=5e-4, dt_splitting=5e-4, dt_repeated_call=5e-4, **kw)

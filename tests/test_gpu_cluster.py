@@ -50,7 +50,7 @@ def test_forced_cluster_sizes_ragged_fibers(csize):
     GP.compare(s, "fused", "fp64", GP.VM_TOL_FP64, 1e-8, **kw)
 
 
-@pytest.mark.parametrize("shape", [(128, 2), (256, 2), (512, 2), (256, 4)])
+@pytest.mark.parametrize("shape", [(128, 2), (256, 2), (512, 2), (256, 4), (192, 1), (256, 1)])
 def test_cluster_shapes_fp32_within_01mV(shape):
     s = H.c1_system(n_fibers=5, n_nodes=1481, end_time=1.0)
     kw = dict(threads_per_block=shape[0], nodes_per_thread=shape[1], cluster_size=-(-1481 // (shape[0] * shape[1])))
