@@ -32,7 +32,7 @@ def test_few_fibers_choose_cluster_mode_and_match_oracle():
 
 
 def test_many_fibers_keep_bins():
-    s = WL.batched_hh(n_fibers=600, min_nodes=500, max_nodes=900, seed=1, end_time=0.0)
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=600, min_nodes=500, max_nodes=900, seed=1, end_time=0.0)
     assert _layout(s)["cluster_size"] == 1
 
 

@@ -33,7 +33,7 @@ def test_junction_at_the_fiber_ends(method, rule):
 @pytest.mark.parametrize("method", ["split", "fused"])
 def test_lane_width_one_and_wrapping_tables(method):
     rng = np.random.default_rng(13)
-    s = WL.batched_hh(n_fibers=5, min_nodes=30, max_nodes=50, seed=13, end_time=2.0, vc_width=1, n_ranks=2)
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=5, min_nodes=30, max_nodes=50, seed=13, end_time=2.0, vc_width=1, n_ranks=2)
     s.firing_events = rng.integers(0, 2, size=(3, 2)).astype(np.uint8)      # rows and motor units wrap
     s.motor_unit_no = np.array([0, 1, 5, 8, 13], np.int32)
     s.call_frequency = np.full(5, 2.0)

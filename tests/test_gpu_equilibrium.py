@@ -25,7 +25,7 @@ def _rest():
 
 
 def _system(at_rest=True, only=False, n_ranks=1, width=4, scheme="ImplicitEuler", end_time=2.0, seed=5):
-    s = WL.batched_hh(n_fibers=5, min_nodes=30, max_nodes=61, seed=seed, end_time=end_time,
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=5, min_nodes=30, max_nodes=61, seed=seed, end_time=end_time,
                       diffusion_scheme=scheme, n_ranks=n_ranks, vc_width=width)
     s.firing_events = np.array([[1, 0, 1, 1, 0]], np.uint8)
     s.motor_unit_no = np.arange(5, dtype=np.int32)
@@ -143,7 +143,7 @@ def test_compute_state_information(skip, only, n_ranks, width):
 
 def test_many_fibers_warp_diffusion_with_the_skip():
     # 600 fibers: the split path's diffusion takes a warp per fiber and skips the ranks counted at rest
-    s = WL.batched_hh(n_fibers=600, min_nodes=8, max_nodes=24, seed=7, end_time=0.6, n_ranks=2)
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=600, min_nodes=8, max_nodes=24, seed=7, end_time=0.6, n_ranks=2)
     s.firing_events = np.zeros((1, 100), np.uint8)
     s.firing_events[0, :3] = 1
     H.complete(s)

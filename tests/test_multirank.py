@@ -27,7 +27,7 @@ def _worker(rank, world, port, out):
         impl = "reference"   # gloo backend
     w, r, local, pg = bench.dist_setup(A)
     assert (w, r) == (world, rank)
-    batch = WL.batched_hh(n_fibers=8, min_nodes=20, max_nodes=40, seed=rank, end_time=0.2)
+    batch = WL.batched_hh(clamp_rule="vc", n_fibers=8, min_nodes=20, max_nodes=40, seed=rank, end_time=0.2)
     sub = WL.subset(batch, np.arange(2))
     H.complete(sub)
     st, _, _, n = H.run_oracle(sub, n_threads=1)

@@ -36,7 +36,7 @@ def test_lpt_partition_covers_and_balances():
 
 
 def test_subset_keeps_per_fiber_inputs():
-    s = WL.batched_hh(n_fibers=9, min_nodes=10, max_nodes=30, seed=2, end_time=0.1)
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=9, min_nodes=10, max_nodes=30, seed=2, end_time=0.1)
     H.complete(s)
     s.jitter = np.arange(9 * 2, dtype=float).reshape(9, 2)
     fib = np.array([7, 1, 4])
@@ -55,7 +55,7 @@ def test_subset_keeps_per_fiber_inputs():
 
 @pytest.mark.parametrize("n_ranks,width", [(1, 4), (2, 4), (3, 8), (1, 2), (4, 1)])
 def test_library_clamp_selection_matches_oracle(n_ranks, width):
-    s = WL.batched_hh(n_fibers=23, min_nodes=7, max_nodes=90, seed=n_ranks * 10 + width, end_time=0.0)
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=23, min_nodes=7, max_nodes=90, seed=n_ranks * 10 + width, end_time=0.0)
     s.n_ranks, s.vc_width = n_ranks, width
     rng = np.random.default_rng(width)
     lengths = np.diff(s.fiber_offsets)
@@ -81,7 +81,7 @@ def test_center_rule_selection_and_bad_arguments():
 
 
 def test_shard_clamp_mapping():
-    s = WL.batched_hh(n_fibers=11, min_nodes=20, max_nodes=60, seed=5, end_time=0.0)
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=11, min_nodes=20, max_nodes=60, seed=5, end_time=0.0)
     clamp = SH.global_clamp_nodes(s)
     for fib in SH.lpt_partition(np.diff(s.fiber_offsets), 3):
         lf, lc, le = SH.shard_clamp_nodes(s, fib, clamp)
@@ -160,7 +160,7 @@ def test_shard_gate_codes_map_fibers():
 
 
 def test_adjoint_memory_plan():
-    s = WL.batched_hh(n_fibers=40, min_nodes=500, max_nodes=2500, seed=3, end_time=0.0)
+    s = WL.batched_hh(clamp_rule="vc", n_fibers=40, min_nodes=500, max_nodes=2500, seed=3, end_time=0.0)
     one = SH.adjoint_bytes_per_node(s.model, 5, 1000, 16)
     # checkpoints fall and replay grows with the interval
     assert SH.adjoint_bytes_per_node(s.model, 5, 1000, 1) > one < SH.adjoint_bytes_per_node(s.model, 5, 1000, 500)
