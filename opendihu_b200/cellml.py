@@ -914,6 +914,9 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
         out.append(f"#undef FDM_POW{n}")
     out.append("#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
     out.append("  }")
+    # the right-hand side split by state (few-node reaction kernel)
+    out.append("  // the right-hand side of one state at a time: rates_group<R, M, G> = RATES[G]")
+    out.extend(emit_group_rates(model, params_alg, params_const))
     # reverse mode (adjoint)
     out.append("  // vector-Jacobian product: LAM_STATES += J^T LAM_RATES, LAM_PARAMS += (dRATES/dPARAMS)^T LAM_RATES")
     out.extend(emit_cuda_vjp(model, params_alg, params_const))
@@ -922,6 +925,89 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     out.append("};")
     out.append("")
     return "\n".join(out)
+
+
+def _algebraic_reads(e, out: set):
+    t = e[0]
+    if t == "var":
+        if e[1] == "A":
+            out.add(e[2])
+    elif t in ("neg", "pos", "not"):
+        _algebraic_reads(e[1], out)
+    elif t == "bin":
+        _algebraic_reads(e[2], out)
+        _algebraic_reads(e[3], out)
+    elif t == "tern":
+        for k in (1, 2, 3):
+            _algebraic_reads(e[k], out)
+    elif t == "call":
+        for a in e[2]:
+            _algebraic_reads(a, out)
+
+
+def rate_cone(lines, states: Sequence[int]) -> List[int]:
+    """Indices (into lines, in their order) of the lines the rates of the given states need: their RATES lines
+    and, transitively, the ALGEBRAIC lines those read."""
+    where = {(k, i): n for n, (k, i, _) in enumerate(lines)}
+    need, stack = set(), [where[("R", s)] for s in states if ("R", s) in where]
+    while stack:
+        n = stack.pop()
+        if n in need:
+            continue
+        need.add(n)
+        reads = set()
+        _algebraic_reads(lines[n][2], reads)
+        stack.extend(where[("A", a)] for a in reads if ("A", a) in where)
+    return sorted(need)
+
+
+#: models with at most this many states get the state-group form (one warp per state of the node group)
+MAX_GROUP_STATES = 8
+
+
+def emit_group_rates(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> List[str]:
+    """The right-hand side split by state: ``rates_group<R, M, G>`` computes RATES[G] only, from the lines its
+    cone needs, so that the warps of a node group can each evaluate one state's rate (the reaction kernel for
+    few nodes, where one thread per node leaves the SMs short of independent work).  Same expressions as
+    ``rates``, so the same values."""
+    lines = substitute_parameters(model, params_alg, params_const)
+    em = _Emitter("R", model.constants, "cuda")
+    pows = _collect_int_pows(lines)
+    out = [f"  static constexpr int nGroups = {model.n_states if model.n_states <= MAX_GROUP_STATES else 0};"]
+    if model.n_states > MAX_GROUP_STATES:
+        return out
+    out.append("  template<class R, class M, int G>")
+    out.append("  __device__ __forceinline__ static R rates_group(const R VOI, const R* __restrict__ STATES,"
+               " const R* __restrict__ PARAMS)")
+    out.append("  {")
+    out.append("    (void)VOI; (void)PARAMS;")
+    out.append(f"    R ALGEBRAIC[{max(model.n_algebraics, 1)}];")
+    out.append("    (void)ALGEBRAIC;")
+    out.append("#define FDM_EXP(x) M::exp(x)")
+    out.append("#define FDM_LOG(x) M::log(x)")
+    out.append("#define FDM_POWF(x, y) M::pow(x, y)")
+    out.append("#define FDM_ABS(x) fabs(x)")
+    out.append("#define FDM_SQRT(x) sqrt(x)")
+    out.extend("#define " + s2.split("#define ", 1)[1] for s2 in _pow_macro_defs(pows))
+    for g in range(model.n_states):
+        out.append(f"    {'if' if g == 0 else 'else if'} constexpr (G == {g}) {{")
+        rate = None
+        for n in rate_cone(lines, [g]):
+            kind, idx, expr = lines[n]
+            if kind == "A":
+                out.append(f"      ALGEBRAIC[{idx}] = {em.expr(expr)};")
+            else:
+                rate = em.expr(expr)
+        out.append(f"      return {rate if rate is not None else '(R)0'};")
+        out.append("    }")
+    out.append("    else {")
+    out.append("      return (R)0;")
+    out.append("    }")
+    for n in pows:
+        out.append(f"#undef FDM_POW{n}")
+    out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
+    out.append("  }")
+    return out
 
 
 def emit_c_model(model: Model, params_alg: Sequence[int], params_const: Sequence[int]) -> str:

@@ -287,6 +287,7 @@ struct fdm_solver {
   size_t ev_used = 0;
   double main_ms = 0, adv_ms = 0, adj_ms = 0;
   bool finish_pending = false;   // an fdm_advance_async whose timing and NaN check fdm_wait still owes
+  bool adj_forward = false;      // inside fdm_adjoint_forward: the reaction runs one thread per node
   int adjoint_tape = 1; // FDM_ADJOINT_TAPE=0 selects the re-evaluating reverse step (for measurements)
   int64_t main_launches = 0, launches = 0;
   cudaEvent_t adv_start = nullptr, adv_stop = nullptr;
@@ -2014,6 +2015,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
   ra.n_trace = s->n_trace;
   ra.trace_capacity = s->trace_capacity;
   ra.act = activation_rec(s);
+  ra.per_node = s->adj_forward ? 1 : 0;
   if (s->eq.on) {
     // equilibrium skip: every half step is a speculative reaction, the buffer scan and a commit; the statuses
     // alternate between the two status arrays, and a window has an even number of half steps
@@ -3109,16 +3111,22 @@ extern "C" int fdm_adjoint_forward(fdm_solver* s, double t_start, double t_end, 
   }
   s->ev_used = 0;
   FDM_CUDA(cudaEventRecord(s->adv_start, s->stream));
-  for (int c = 0; c < A.n_seg; c++) {
+  // the replay in fdm_adjoint_backward runs the one-thread-per-node reaction kernel; the forward runs it too,
+  // so that the replay reproduces it bit for bit (window graphs captured with the other kernel are dropped)
+  invalidate_graphs(s);
+  s->adj_forward = true;
+  for (int c = 0; c < A.n_seg && !rc; c++) {
     rc = copy_state(s, A.ck_vm.p + (size_t)c * N, A.ck_states.p + (size_t)c * N * (NS - 1), A.ck_last.p + (size_t)c * nf,
                     A.ck_jit.p + (size_t)c * nf, A.ck_jidx.p + (size_t)c * nf, A.ck_hbs.p + (size_t)c * nf, true);
     if (rc)
-      return rc;
+      break;
     const size_t b = (size_t)c * A.kc, e = std::min<size_t>(b + A.kc, NT);
     rc = run_planned(s, A.steps, A.dt1s, b, e, c == A.n_seg - 1);
-    if (rc)
-      return rc;
   }
+  s->adj_forward = false;
+  invalidate_graphs(s);
+  if (rc)
+    return rc;
   rc = copy_state(s, A.fin_vm.p, A.fin_states.p, A.fin_last.p, A.fin_jit.p, A.fin_jidx.p, A.fin_hbs.p, true);
   if (rc)
     return rc;

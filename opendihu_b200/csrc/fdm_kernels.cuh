@@ -517,6 +517,8 @@ struct ReactionArgs {
   double* store_states;           // adjoint replay (FP64 only): input state of substep k at
                                   // store_states[(k*nStates + s)*stride + node], or null
   double* store_vm_out;           // adjoint replay: Vm after the half step also written here, or null
+  int per_node;                   // 1: one thread per node whatever the size (the adjoint's checkpointed
+                                  // forward, which its replay reproduces bit for bit)
   const int* gate;                // onlyComputeIfHasBeenStimulated: per node gate code, or null
   const uint8_t* gate_start;
   int gate_stride;
@@ -588,6 +590,92 @@ __global__ void __launch_bounds__(128) reaction_kernel(ReactionArgs a)
     const int slot = a.trace_slot[i];
     if (slot >= 0)
       record_trace(a.trace, a.n_trace, a.trace_capacity, a.act, slot, s.global_no, V);
+  }
+}
+
+// Split-path reaction for few nodes, FP64: the warps of a CTA share 32 nodes, warp g advancing state g of
+// each (Model::rates_group evaluates one state's rate from the lines it needs).  With one thread per node a
+// problem of a few ten thousand nodes leaves each SM a handful of warps whose Heun chains stall on FP64
+// latency; here every node gives nStates independent chains.  The states of the 32 nodes live in shared
+// memory; per substep each warp forms its y*, the CTA synchronizes, each warp forms its new state from both
+// rates, the CTA synchronizes.  Same expressions and operation order as heun_step (FP64), so the same values.
+template<class Model, class Math, int G>
+__device__ __forceinline__ double group_rate(int g, double t, const double* y, const double* P)
+{
+  if constexpr (G < Model::nGroups) {
+    if (g == G)
+      return Model::template rates_group<double, Math, G>(t, y, P);
+    return group_rate<Model, Math, G + 1>(g, t, y, P);
+  } else {
+    return 0.0;
+  }
+}
+
+template<class Model, class Math>
+__global__ void __launch_bounds__(32 * (Model::nGroups > 0 ? Model::nGroups : 1)) reaction_group_kernel(ReactionArgs a)
+{
+  constexpr int NS = Model::nStates;
+  constexpr int NP = Model::nParameters > 0 ? Model::nParameters : 1;
+  __shared__ double sy[NS][32], sys[NS][32];
+  const int lane = threadIdx.x, g = threadIdx.y;
+  const int64_t i = (int64_t)blockIdx.x * 32 + lane;
+  const bool ok = i < a.n_nodes;
+  const double* st = (const double*)a.states;
+  const double* pr = (const double*)a.params;
+  double own = 0.0;
+  if (ok)
+    own = g == 0 ? a.vm[i] : st[(g - 1) * a.stride + i];
+  sy[g][lane] = own;
+  double P[NP], Pstim[NP];
+#pragma unroll
+  for (int q = 0; q < Model::nParameters; q++) {
+    P[q] = ok ? pr[q * a.stride + i] : 0.0;
+    Pstim[q] = (a.stimulus_mode == 1 && q == a.stimulus_parameter) ? a.stimulus_value : P[q];
+  }
+  const int cf = ok ? a.clamp_fiber[i] : -1;
+  const SplitStep s = a.steps[a.step];
+  const double t0 = a.half ? s.mid : s.t;
+  const int base = (a.step * 2 + a.half) * a.nsub_stride;
+  __syncthreads();
+  for (int k = 0; k < s.n0; k++) {
+    const double t = xadd(t0, xmul((double)k, s.dt0));
+    const bool stim = cf >= 0 && stim_bit(a.flags, a.words_per_fiber, cf, base + k);
+    const bool vclamp = stim && a.stimulus_mode == 0;
+    double Pk[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+      Pk[q] = (stim && a.stimulus_mode == 1) ? Pstim[q] : P[q];
+    double y[NS];
+#pragma unroll
+    for (int q = 0; q < NS; q++)
+      y[q] = sy[q][lane];
+    const double r = group_rate<Model, Math, 0>(g, t, y, Pk);
+    double ys = own + s.dt0 * r;
+    if (g == 0 && vclamp)
+      ys = a.vstim;
+    sys[g][lane] = ys;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NS; q++)
+      y[q] = sys[q][lane];
+    const double r2 = group_rate<Model, Math, 0>(g, t, y, Pk);
+    own += 0.5 * s.dt0 * (r + r2);
+    if (g == 0 && vclamp)
+      own = a.vstim;
+    sy[g][lane] = own;
+    __syncthreads();
+  }
+  if (!ok)
+    return;
+  if (g == 0) {
+    a.vm[i] = own;
+    if (a.half == 1 && a.trace_slot) {
+      const int slot = a.trace_slot[i];
+      if (slot >= 0)
+        record_trace(a.trace, a.n_trace, a.trace_capacity, a.act, slot, s.global_no, own);
+    }
+  } else {
+    ((double*)a.states)[(g - 1) * a.stride + i] = own;
   }
 }
 

@@ -18,9 +18,28 @@ inline cudaError_t reaction_one(const ReactionArgs& a, cudaStream_t s)
   return cudaGetLastError();
 }
 
+// up to this many nodes the FP64 split path advances a node's states on separate warps (reaction_group_kernel):
+// one thread per node would leave fewer than about 16 warps per SM
+constexpr int64_t kGroupKernelMaxNodes = 65536;
+
+template<class Model, class Math>
+inline cudaError_t reaction_group_one(const ReactionArgs& a, cudaStream_t s)
+{
+  const dim3 block(32, Model::nGroups);
+  reaction_group_kernel<Model, Math><<<(unsigned)((a.n_nodes + 31) / 32), block, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 template<class Model>
 inline cudaError_t reaction_model(RealKind rk, MathKind mk, const ReactionArgs& a, cudaStream_t s)
 {
+  if constexpr (Model::nGroups > 0) {
+    // few nodes, nothing but the Heun substeps asked of the launch: a warp per state of 32 nodes
+    if (rk == REAL_F64 && a.n_nodes > 0 && a.n_nodes <= kGroupKernelMaxNodes && !a.gate && !a.store_states &&
+        !a.store_vm_out && !a.store_alg && !a.per_node)
+      return mk == MATH_EXACT ? reaction_group_one<Model, fdm_math_exact>(a, s)
+                              : reaction_group_one<Model, fdm_math_approx>(a, s);
+  }
   if (rk == REAL_F64)
     return mk == MATH_EXACT ? reaction_one<Model, double, fdm_math_exact>(a, s)
                             : reaction_one<Model, double, fdm_math_approx>(a, s);
