@@ -657,7 +657,30 @@ def _uses_algebraic(e) -> bool:
     return False
 
 
-def _batched_denominators(lines, consts, max_group: int = 3):
+def _one_minus_exp(e, consts):
+    """(sign, exp node) if e is 1 - exp(u) (sign +1) or exp(u) - 1 (sign -1), else None.  Such a difference is
+    exactly 0 in FP32 wherever the SFU exponential rounds to 1 (|u| below about 2^-23): a removable singularity
+    of the model (e.g. the Goldman-Hodgkin-Katz flux x / (1 - exp(-a x))) would become 0/0."""
+    if e[0] != "bin" or e[1] != "-":
+        return None
+    for sign, one, ex in ((1, e[2], e[3]), (-1, e[3], e[2])):
+        c = _affine(one, consts)
+        if c is not None and not c[0] and c[1] == 1.0 and ex[0] == "call" and ex[1] == "exp":
+            return sign, ex
+    return None
+
+
+def _unsafe_one_minus_exp(e, consts, repl) -> bool:
+    """1 - exp(u) / exp(u) - 1 as the FP32 form would write it with a bare SFU exponential (not a shared
+    exponential times a factor other than 1, which is one FMA and never exactly 0): see fdm_1mexp2."""
+    om = _one_minus_exp(e, consts)
+    if om is None:
+        return False
+    shared = repl.get(repr(om[1]))
+    return shared is None or shared[1] == 0.0
+
+
+def _batched_denominators(lines, consts, max_group: int = 3, repl=None):
     """Denominators of divisions that depend on states, parameters, time and constants only (no algebraic
     variables) and are not constants, in order of first appearance; grouped by max_group for a batched
     reciprocal (one SFU reciprocal per group, see fdm_rcp_batch)."""
@@ -669,7 +692,10 @@ def _batched_denominators(lines, consts, max_group: int = 3):
             if e[1] == "/":
                 den = e[3]
                 af = _affine(den, consts)
-                if not (af is not None and not af[0]) and not _uses_algebraic(den) and repr(den) not in seen:
+                # an unsafe 1 - exp(u) stays out: near u = 0 it is tiny, and a tiny factor would underflow the
+                # group's product
+                if (not (af is not None and not af[0]) and not _uses_algebraic(den) and repr(den) not in seen
+                        and not _unsafe_one_minus_exp(den, consts, repl or {})):
                     seen.append(repr(den))
                     found.append(den)
             walk(e[2])
@@ -755,6 +781,15 @@ class _FastEmitter(_Emitter):
                 return f"({self.affine_text(sorted(af[0].items()), af[1], 1.0)})"
         if t == "neg":
             return self.neg_text(e[1])
+        if t == "bin" and e[1] == "-":
+            # 1 - exp(u), exp(u) - 1: formed without cancellation and never exactly 0 (fdm_1mexp2), unless the
+            # exponential is a shared one with a factor other than 1 (then e * c - 1 is one FMA, not exactly 0)
+            if _unsafe_one_minus_exp(e, self.consts, self.repl):
+                sign, ex = _one_minus_exp(e, self.consts)
+                af = _affine(ex[2][0], self.consts)
+                arg = (self.affine_text(sorted(af[0].items()), af[1], _LOG2E) if af is not None
+                       else f"(({self.real}){_hexf(_LOG2E)}) * {self.expr(ex[2][0])}")
+                return f"fdm_1mexp2({arg})" if sign > 0 else f"(-fdm_1mexp2({arg}))"
         if t == "bin" and e[1] == "-":
             # x - c for a constant c: x + (-c), so that a product x = a b fuses with it
             c = _affine(e[3], self.consts)
@@ -865,7 +900,7 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     out.append("  }")
     # FP32 variant with shared exponentials
     repl, groups = _exp_groups(lines, model.constants)
-    rgroups = _batched_denominators(lines, model.constants)
+    rgroups = _batched_denominators(lines, model.constants, repl=repl)
     fem = _FastEmitter("R", model.constants, repl)
     out.append("  // FP32 form: exponentials exp(a.x + b_k) that share a.x are evaluated once as exp(a.x) * e^{b_k};")
     out.append("  // exponentials, logarithms and reciprocals as single SFU instructions (fdm_ex2/fdm_lg2/fdm_rcp)")

@@ -2482,11 +2482,11 @@ extern "C" int fdm_get_stimulation_log(fdm_solver* s, int64_t* n_total, double* 
   *n_total = (int64_t)n + s->log_dropped;
   if (!times && !fibers)
     return FDM_OK;
-  if (*n_total > s->log_cap)
+  if (s->log_dropped > 0 || *n_total > s->log_cap)
     return fail(s, FDM_ERR_ARG, "fdm_get_stimulation_log: " + std::to_string(*n_total) +
-                                    " stimulation begins were recorded but the log holds only " +
-                                    std::to_string(s->log_cap) + "; the log is incomplete (grow its capacity "
-                                    "before each advance)");
+                                    " stimulation begins were recorded but the log kept only " +
+                                    std::to_string(std::min<int64_t>(*n_total - s->log_dropped, s->log_cap)) +
+                                    "; the log is incomplete (grow its capacity before each advance)");
   const size_t k = (size_t)n;
   if (k > 0 && times)
     FDM_CUDA(cudaMemcpyAsync(times, s->log_t.p, sizeof(double) * k, cudaMemcpyDeviceToHost, s->stream));

@@ -127,6 +127,24 @@ __device__ __forceinline__ fdm_f2 fdm_sel(fdm_b2 c, fdm_f2 a, fdm_f2 b)
 // FP32-reaction mode is specified for physiological potentials.  No range test is made: a
 // branch inside the right-hand side costs more than the reciprocals it saves.
 // --------------------------------------------------------------------------------------------
+// 1 - 2^t without cancellation and never exactly 0, for the FP32 form of 1 - exp(u) (t = u log2 e): for
+// |t| < 2^-6 the series -x (1 + x/2 + x^2/6), x = t ln 2 (relative error below 2^-26 there), else 1 - ex2(t);
+// t = 0 gives the smallest normal float instead of 0, so a removable singularity x / (1 - e^-ax) at x = 0
+// evaluates to 0 rather than 0/0
+__device__ __forceinline__ float fdm_1mexp2(float t)
+{
+  const float x = t * 0.69314718055994531f;
+  const float series = -x * (1.f + x * (0.5f + x * (1.f / 6.f)));
+  float d = fabsf(t) < 0.015625f ? series : 1.f - fdm_ex2(t);
+  return d == 0.f ? 1.17549435e-38f : d;
+}
+__device__ __forceinline__ fdm_f2 fdm_1mexp2(fdm_f2 t) { return fdm_f2(fdm_1mexp2(t.v.x), fdm_1mexp2(t.v.y)); }
+__device__ __forceinline__ double fdm_1mexp2(double t)
+{
+  const double d = -expm1(t * 0.69314718055994531);
+  return d == 0.0 ? 2.2250738585072014e-308 : d;
+}
+
 template<class R>
 __device__ __forceinline__ void fdm_rcp_batch(R d0, R d1, R& r0, R& r1)
 {

@@ -13,7 +13,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _system(**kw):
-    s = WL.batched_hh(clamp_rule="vc", n_fibers=37, min_nodes=60, max_nodes=400, seed=11, end_time=kw.pop("end_time", 3.0), **kw)
+    kw.setdefault("clamp_rule", "vc")
+    s = WL.batched_hh(n_fibers=37, min_nodes=60, max_nodes=400, seed=11, end_time=kw.pop("end_time", 3.0), **kw)
     s.call_enable_begin[:] = 0.0
     return H.complete(s)
 
