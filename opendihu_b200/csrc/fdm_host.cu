@@ -2066,7 +2066,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
         cur ^= 1;
         if (half == 0) {
           FDM_CUDA(launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
-                                         s->stream, E.counter.p, E.nbuf.p, s->cfg.n_ranks));
+                                         s->stream, E.counter.p, E.nbuf.p, s->cfg.n_ranks, s->max_fiber_len));
           s->launches++;
         }
       }
@@ -2090,7 +2090,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
           ce = launch_reaction(s->cfg.model, rk, mk, ra, s->stream);
           if (ce == cudaSuccess && half == 0)
             ce = launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
-                                       s->stream);
+                                       s->stream, nullptr, nullptr, 1, s->max_fiber_len);
         }
       }
       cudaError_t ee = cudaStreamEndCapture(s->stream, &g);
@@ -2124,7 +2124,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
         FDM_CUDA(cudaEventRecord(e1, s->stream));
       if (half == 0) {
         FDM_CUDA(launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
-                                       s->stream));
+                                       s->stream, nullptr, nullptr, 1, s->max_fiber_len));
         s->launches++;
       }
     }
@@ -3277,7 +3277,8 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
         FDM_CUDA(launch_reaction(s->cfg.model, REAL_F64, mk, ra, s->stream));
         s->launches++;
         if (half == 0) {
-          FDM_CUDA(launch_diffusion(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream));
+          FDM_CUDA(launch_diffusion(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream, nullptr, nullptr, 1,
+                                    s->max_fiber_len));
           s->launches++;
         }
       }
