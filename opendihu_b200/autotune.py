@@ -90,6 +90,26 @@ def _time_split(system, precision, k, n_steps, device) -> float:
     return tm["advance_ms"] / 1e3 / n_steps
 
 
+def _fused_built(system, precision, device) -> bool:
+    """Whether the library builds the fused kernel for the model (fdm_create refuses it otherwise; nothing is
+    allocated before that check)."""
+    import ctypes as C
+    cfg = N.default_config()
+    cfg.model = N.MODEL_IDS[system.model]
+    cfg.method = 1
+    cfg.reaction_precision = 0 if precision == "fp64" else 1
+    cfg.device = int(device)
+    h = C.c_void_p()
+    rc = N.lib().fdm_create(C.byref(cfg), C.byref(h))
+    if rc == N.FDM_OK:
+        N.lib().fdm_destroy(h)
+        return True
+    if rc == N.FDM_ERR_UNSUPPORTED:
+        return False
+    N.check(rc)
+    return True
+
+
 def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0,
              steps_per_launch: Sequence[int] = (50, 100, 200), use_cache: bool = True,
              include_split: bool = False) -> dict:
@@ -100,6 +120,9 @@ def autotune(system, precision: str = "fp32", n_steps: int = 20, device: int = 0
     if include_split and getattr(system, "skip_close_to_equilibrium", False):
         return {"method": "split", "threads": 0, "nodes_per_thread": 0, "cluster_size": 1, "steps_per_launch": 0,
                 "s_per_step": None, "trials": [], "reason": "the equilibrium skip runs on the split method"}
+    if include_split and not _fused_built(system, precision, device):
+        return {"method": "split", "threads": 0, "nodes_per_thread": 0, "cluster_size": 1, "steps_per_launch": 0,
+                "s_per_step": None, "trials": [], "reason": "no fused kernel is built for this model"}
     key = signature(system, precision) + ("+split" if include_split else "")
     if use_cache:
         if key in _MEMO:
