@@ -358,6 +358,47 @@ __device__ __forceinline__ void heun_step2(fdm_f2& Vf, fdm_f2& LV, double& V0, d
   }
 }
 
+// heun_step2 over the MP node pairs of one thread, without branches: every pair computes (the caller zeroes
+// the Vm of nodes beyond its bin), clamps are selects (bit 2p / 2p + 1 of `clamp`: node 2p / 2p + 1 clamped;
+// a constant 0 removes them).  Arithmetic per pair identical to heun_step2.  (Issuing the pairs' first
+// right-hand sides before their second ones measured 0.7 % slower than pair after pair.)
+template<class Model, int MP, int NSM, int NP>
+__device__ __forceinline__ void heun_step2_pairs(fdm_f2 (&Vf)[MP], fdm_f2 (&LV)[MP], double* V,
+                                                 fdm_f2 (&S)[MP][NSM], fdm_f2 (&L)[MP][NSM],
+                                                 const fdm_f2 (&P)[MP][NP], const fdm_f2 tr, const fdm_f2 dtr,
+                                                 const fdm_f2 hdt, const unsigned clamp, double vstim)
+{
+  constexpr int NS = Model::nStates;
+  const float vs = (float)vstim;
+  fdm_f2 alg[Model::nAlgebraics];
+#pragma unroll
+  for (int p = 0; p < MP; p++) {
+    fdm_f2 r[NS], ys[NS], y[NS], r2[NS];
+    y[0] = Vf[p] + LV[p];
+#pragma unroll
+    for (int s = 1; s < NS; s++)
+      y[s] = S[p][s - 1] + L[p][s - 1];
+    Model::template rates_fast2<fdm_math_exact>(tr, y, P[p], r, alg);
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      ys[s] = dtr * r[s] + y[s];
+    ys[0].v.x = ((clamp >> (2 * p)) & 1u) ? vs : ys[0].v.x;
+    ys[0].v.y = ((clamp >> (2 * p + 1)) & 1u) ? vs : ys[0].v.y;
+    Model::template rates_fast2<fdm_math_exact>(tr, ys, P[p], r2, alg);
+#pragma unroll
+    for (int s = 1; s < NS; s++)
+      L[p][s - 1] = hdt * (r[s] + r2[s]) + L[p][s - 1];
+    LV[p] = hdt * (r[0] + r2[0]) + LV[p];
+    const bool c0 = (clamp >> (2 * p)) & 1u, c1 = (clamp >> (2 * p + 1)) & 1u;
+    V[2 * p] = c0 ? vstim : V[2 * p];
+    V[2 * p + 1] = c1 ? vstim : V[2 * p + 1];
+    Vf[p].v.x = c0 ? vs : Vf[p].v.x;
+    Vf[p].v.y = c1 ? vs : Vf[p].v.y;
+    LV[p].v.x = c0 ? 0.f : LV[p].v.x;
+    LV[p].v.y = c1 ? 0.f : LV[p].v.y;
+  }
+}
+
 // (S, L) -> (S + L rounded, the rounding error): the Fast2Sum normalization of a compensated pair
 __device__ __forceinline__ void normalize_pair(fdm_f2& S, fdm_f2& L)
 {
@@ -1625,6 +1666,18 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
     s_ts[j * T + tid] = (ok && a.trace_slot) ? a.trace_slot[i] : -1;
     s_gate[j * T + tid] = (ok && a.gate) ? a.gate[i] : 0;
   }
+  // the clamp fiber of the thread's junction nodes when they all belong to one fiber (the usual case: a
+  // junction is a few consecutive nodes of one fiber): one flag read per substep instead of one per node
+  int cf_first = -1;
+  bool cf_one = true;
+#pragma unroll
+  for (int j = 0; j < M; j++) {
+    if ((cmask >> j) & 1u) {
+      const int c = s_cf[j * T + tid];
+      cf_one = cf_one && (cf_first < 0 || c == cf_first);
+      cf_first = cf_first < 0 ? c : cf_first;
+    }
+  }
   // stimulation bit of node j at substep bit `bit` (junction nodes only read their fiber's bit)
   auto node_stim = [&](int j, int bit) -> bool {
     return ((cmask >> j) & 1u) && stim_bit(a.flags, a.words_per_fiber, s_cf[j * T + tid], bit);
@@ -1633,6 +1686,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
   // an odd last node runs alone
   constexpr bool PAIR = std::is_same<RR, float>::value && std::is_same<Math, fdm_math_exact>::value;
   constexpr int MP = PAIR ? M / 2 : 0;
+  constexpr unsigned pair_mask = (1u << (2 * MP)) - 1u; // the paired nodes' bits
   constexpr int NSM = NS > 1 ? NS - 1 : 1;
   fdm_f2 S2[MP > 0 ? MP : 1][NSM], L2[MP > 0 ? MP : 1][NSM];
   if constexpr (PAIR) {
@@ -1751,7 +1805,50 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
           if (!__any_sync(0xffffffffu, any))
             continue;
         }
-        if constexpr (PAIR) {
+        if constexpr (PAIR && !gate_on && MP > 0) {
+          // all pairs in one block (nodes beyond the bin compute too; their Vm is zeroed after the half step).
+          // Stimulated junction nodes are rare (a few substeps per firing): the clamp and the stimulus
+          // parameter are applied in a second copy of the step that a warp takes only when one of its nodes
+          // is stimulated, so the common step carries no selects and no per-node flag reads
+          const float dtf = (float)s.dt0;
+          unsigned clamp = 0u; // bit j: node j stimulated in this substep
+          if (cmask) {
+            if (cf_one) {
+              clamp = stim_bit(a.flags, a.words_per_fiber, cf_first, base + k) ? cmask : 0u;
+            } else {
+#pragma unroll
+              for (int j = 0; j < 2 * MP; j++)
+                clamp |= (node_stim(j, base + k) ? 1u : 0u) << j;
+            }
+          }
+          fdm_f2 Pk[MP > 0 ? MP : 1][NP];
+#pragma unroll
+          for (int p = 0; p < MP; p++)
+#pragma unroll
+            for (int q = 0; q < NP; q++)
+              Pk[p][q] = sP2[(p * NP + q) * T + tid];
+          if (__any_sync(0xffffffffu, (clamp & pair_mask) != 0u)) {
+            const bool m1 = a.stimulus_mode == 1;
+            const float sv = (float)a.stimulus_value;
+#pragma unroll
+            for (int p = 0; p < MP; p++)
+#pragma unroll
+              for (int q = 0; q < NP; q++) {
+                const bool hit = m1 && q == a.stimulus_parameter;
+                Pk[p][q] = fdm_f2((hit && ((clamp >> (2 * p)) & 1u)) ? sv : Pk[p][q].v.x,
+                                  (hit && ((clamp >> (2 * p + 1)) & 1u)) ? sv : Pk[p][q].v.y);
+              }
+            heun_step2_pairs<Model, MP, NSM, NP>(Vf, LV, V, S2, L2, Pk, fdm_f2((float)t), fdm_f2(dtf),
+                                                 fdm_f2(0.5f * dtf), m1 ? 0u : (clamp & pair_mask), a.vstim);
+          } else {
+            heun_step2_pairs<Model, MP, NSM, NP>(Vf, LV, V, S2, L2, Pk, fdm_f2((float)t), fdm_f2(dtf),
+                                                 fdm_f2(0.5f * dtf), 0u, a.vstim);
+          }
+          if constexpr (M % 2 == 1) {
+            if (tid * M + M - 1 < nb)
+              scalar_node(M - 1, t, s.dt0, base + k);
+          }
+        } else if constexpr (PAIR) {
           const float dtf = (float)s.dt0;
           const fdm_f2 dt_all(dtf), hdt_all(0.5f * dtf);
 #pragma unroll
@@ -1815,6 +1912,12 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
 #pragma unroll
           for (int q = 0; q < NSM; q++)
             normalize_pair(S2[p][q], L2[p][q]);
+        }
+        if constexpr (!gate_on) {
+          // nodes beyond the bin carry Vm = 0 into the diffusion (zero coefficients, finite values)
+#pragma unroll
+          for (int j = 0; j < 2 * MP; j++)
+            V[j] = tid * M + j < nb ? V[j] : 0.0;
         }
       }
       if (store_here) {

@@ -403,12 +403,18 @@ class ShardedSolver:
             owner[nodes] = k
             local[nodes] = np.arange(len(nodes))
         traces, grads = {}, {}
+        #: device time (CUDA events) of the last adjoint: checkpointed forwards and backward sweeps of all shards
+        self.adjoint_device_ms = {"checkpointed_forward_ms": 0.0, "backward_ms": 0.0}
         for k, sv in enumerate(self.shards):
             if sv is None:
                 continue
             cols = np.nonzero(owner[sensor_nodes] == k)[0]
+            sv.initialize()
+            sv.reset_timing()
             tr = sv.adjoint_forward(t_start, t_end, checkpoint_every, local[sensor_nodes[cols]])
+            self.adjoint_device_ms["checkpointed_forward_ms"] += sv.timing()["advance_ms"]
             grads[k] = sv.adjoint_backward(loss_grad(tr, cols))
+            self.adjoint_device_ms["backward_ms"] += sv.adjoint_timing_ms()
             sv.adjoint_release()
             traces[k] = (cols, tr)
         steps = max(tr.shape[0] for _, tr in traces.values())

@@ -95,3 +95,27 @@ def test_shorten_over_2ms_against_oracle():
         ok = ~np.isnan(at)
         assert ok.any()
         assert np.all(np.abs(at[ok] - at_ref[ok]) <= 5e-4 + 1e-12)
+
+
+def test_shorten_at_scale_sample_against_oracle():
+    """Shorten at scale (10,000 fibers of U[1000,2500] nodes, 200 motor units): the 4 shortest fibers among
+    those whose motor unit fires at t = 0, over 0.5 ms (1000 Strang steps, an action potential under way):
+    FP64 split against the oracle to 1e-6 mV, the FP32 reaction within 0.1 mV."""
+    system = WL.shorten_scale(end_time=0.5)
+    mu = np.asarray(system.motor_unit_no)
+    fires0 = np.nonzero(np.asarray(system.firing_events)[0, mu % system.firing_events.shape[1]])[0]
+    lengths = np.diff(np.asarray(system.fiber_offsets))[fires0]
+    pick = np.sort(fires0[np.argsort(lengths, kind="stable")[:4]])
+    sub = WL.subset(system, pick)
+    H.complete(sub)
+    ref, _, _, n = H.run_oracle(sub.copy())
+    assert n == 1000
+    assert ref[0].max() > 0.0                                  # depolarised nodes at the end of the span
+    for precision, tol in (("fp64", VM_TOL_FP64), ("fp32", VM_TOL_FP32)):
+        with S.FastMonodomainSolver(sub.copy(), method="split", precision=precision) as slv:
+            slv.advanceTimeSpan()
+            st = slv.states()
+            assert slv.split_steps() == n
+        dv = float(np.max(np.abs(st[0] - ref[0])))
+        print({"fibers": pick.tolist(), "nodes": sub.n_nodes, "precision": precision, "vm_max_abs_diff_mV": dv})
+        assert dv <= tol, (precision, dv)
