@@ -1985,7 +1985,12 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         const int q = j * T + tid;
         bacc = compose(bacc, Affine{-sc[1 * CAP + q], d[j]});
       }
-      __syncthreads(); // sF/sG reuse
+      // No barrier is needed before the backward scan reuses sF/sG: its first writes (warp totals, slots
+      // < T/32) do not overlap the slots the forward scan's results are still read from (T/32 and up), and
+      // warp 0 writes those only after the backward scan's first barrier, which every forward read precedes.
+      // Cluster mode keeps the barrier (its scan totals travel through the cluster).
+      if constexpr (CLUSTER)
+        __syncthreads();
       Affine tot_b;
       const Affine ex_b = block_scan_map<T, true>(bacc, sF, sG, &tot_b);
       double x = cluster_incoming(ex_b, tot_b, true);
@@ -1995,7 +2000,10 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         x = -sc[1 * CAP + q] * x + d[j];
         V[j] = x;
       }
-      __syncthreads(); // vfirst/vlast and sF/sG reuse
+      // the next writes of vfirst/vlast and sF/sG come after the next diffusion's first barrier, which every
+      // read of this one precedes
+      if constexpr (CLUSTER)
+        __syncthreads();
     }
     if (a.trace_slot) {
 #pragma unroll

@@ -82,6 +82,19 @@ def test_uneven_lengths_center_rule_and_jitter(method):
     compare(sysm, method, "fp64", VM_TOL_FP64, 1e-8)
 
 
+@pytest.mark.parametrize("scheme", ["ImplicitEuler", "CrankNicolson"])
+def test_split_many_ragged_fibers(scheme):
+    # 200 ragged fibers: the split path's diffusion solves take a CTA per fiber with the fiber staged in shared
+    # memory (more fibers than SMs, fewer than the warp-per-fiber threshold)
+    rng = np.random.default_rng(11)
+    lengths = rng.integers(20, 700, size=200)
+    sysm = S.uniform_fibers(H.HH, lengths, 0.01, 3.828 / 500, call_frequency=0.5, repeat_after_first_call=0.1,
+                            firing_events=rng.integers(0, 2, size=(4, 6)).astype(np.uint8),
+                            motor_unit_no=rng.integers(0, 6, size=200).astype(np.int32), end_time=1.0,
+                            clamp_rule="center", diffusion_scheme=scheme)
+    compare(sysm, "split", "fp64", VM_TOL_FP64, 1e-8)
+
+
 @pytest.mark.parametrize("method", ["split", "fused"])
 def test_vc_rule_multiple_ranks_and_width8(method):
     compare(small_system(n_ranks=2, vc_width=8), method, "fp64", VM_TOL_FP64, 1e-8)
