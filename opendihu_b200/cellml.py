@@ -726,11 +726,38 @@ class _FastEmitter(_Emitter):
         denominators free of algebraic variables share one SFU reciprocal per group of up to three
         (fdm_rcp_batch: 1/d_k from 1/(d_0 d_1 d_2) and the other factors)."""
 
-    def __init__(self, real, consts, repl, paired: bool = False, recip=None):
+    def __init__(self, real, consts, repl, paired: bool = False, recip=None, alg_defs=None):
         super().__init__(real, consts, "cuda")
         self.repl = repl
         self.paired = paired        # fdm_f2 operands: conditional expressions become per-component selects
         self.recip = recip or {}    # repr(denominator) -> name of its batched reciprocal
+        # paired form: definitions of the algebraic variables (index -> expression), for _folded_subtrahend
+        self.alg_defs = alg_defs or {}
+
+    def _folded_subtrahend(self, acc_text, b):
+        """acc - b for an algebraic variable b defined as F (x + k) with one state or parameter x (a current
+        F (V - E)): written F (-k - x) + acc, a packed subtraction and a packed FMA, the negation folded into
+        the constant (packed instructions take no negated operand); None if b has no such form.  For HH this
+        left the FP32 results bit for bit as they were and took one instruction per current off each
+        right-hand side"""
+        if not self.paired or b[0] != "var" or b[1] != "A" or b[2] not in self.alg_defs:
+            return None
+        d = self.alg_defs[b[2]]
+        if d[0] != "bin" or d[1] != "*":
+            return None
+        for f_side, g_side in ((d[2], d[3]), (d[3], d[2])):
+            g = _affine(g_side, self.consts)
+            if g is None or len(g[0]) != 1 or _affine(f_side, self.consts) is not None:
+                continue
+            (x_key, coef), = g[0].items()
+            if coef not in (1.0, -1.0):
+                continue
+            x = self.var(x_key[0], x_key[1])
+            k = g[1]
+            neg_g = (f"((({self.real}){_hexf(-k)}) - {x})" if coef == 1.0
+                     else f"({x} + (({self.real}){_hexf(-k)}))")
+            return f"(({self.expr(f_side)}) * {neg_g} + {acc_text})"
+        return None
 
     def coef_text(self, v, x):
         if v == 1.0:
@@ -805,6 +832,9 @@ class _FastEmitter(_Emitter):
                         and a[0] == "var" and b[0] == "var" and s2[0] == "var" and repr(one_minus[3]) == repr(s2)):
                     A, B, S = self.expr(a), self.expr(b), self.expr(s2)
                     return f"({A} - ({A} + {B}) * {S})"
+            folded = self._folded_subtrahend(self.expr(l), r)
+            if folded is not None:
+                return folded
         if t == "bin" and e[1] == "/":
             den = _affine(e[3], self.consts)
             if den is not None and not den[0] and den[1] != 0.0:
@@ -826,6 +856,9 @@ class _FastEmitter(_Emitter):
         if t == "neg":
             return self.expr(e[1])
         if t == "bin" and e[1] == "+":
+            folded = self._folded_subtrahend(self.neg_text(e[2]), e[3])
+            if folded is not None:
+                return folded
             return f"({self.neg_text(e[2])} - {self.expr(e[3])})"
         if t == "bin" and e[1] == "-":
             return f"({self.neg_text(e[2])} + {self.expr(e[3])})"
@@ -927,7 +960,8 @@ def emit_cuda_model(model: Model, params_alg: Sequence[int], params_const: Seque
     out.append("#undef FDM_EXP\n#undef FDM_LOG\n#undef FDM_POWF\n#undef FDM_ABS\n#undef FDM_SQRT")
     out.append("  }")
     # the same FP32 form over node pairs (packed FP32 instructions)
-    fem2 = _FastEmitter("R", model.constants, repl, paired=True)
+    fem2 = _FastEmitter("R", model.constants, repl, paired=True,
+                        alg_defs={idx: expr for kind, idx, expr in lines if kind == "A"})
     out.append("  // paired FP32 form: the FP32 form over two nodes at once (fdm_f2, packed FP32 instructions)")
     out.append("  template<class M>")
     out.append("  __device__ __forceinline__ static void rates_fast2(const fdm_f2 VOI, const fdm_f2* __restrict__ STATES,"
