@@ -71,3 +71,28 @@ def test_mapping_normalises_by_the_factor_sum():
         hit[EO.element_nodes(shape)[e]] = True
     np.testing.assert_allclose(out[hit], 3.5, atol=1e-12)
     assert np.all(out[~hit] == -1.0)
+
+
+def test_laplace_3d_matches_the_reference_test():
+    # LaplaceTest.StructuredDeformableMatrixIsCorrect3DStencils of the reference (fixture made from its source by
+    # tests/golden/make_golden.py): 4 x 4 x 4 trilinear elements of unit size, Gauss quadrature of order 2; the
+    # expected matrix is the element stencil summed over the elements, in the reference's sign (-K)
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "laplace3d_golden.json")))
+    nx, ny, nz = g["n_elements"]
+    shape = (nx + 1, ny + 1, nz + 1)
+    st = np.asarray(g["stencil_dy_dx_dz"])
+    n = shape[0] * shape[1] * shape[2]
+    node = lambda x, y, z: z * shape[0] * shape[1] + y * shape[0] + x
+    want = np.zeros((n, n))
+    for x in range(nx):
+        for y in range(ny):
+            for z in range(nz):
+                corners = [(x + i, y + j, z + k) for k in (0, 1) for j in (0, 1) for i in (0, 1)]
+                for a in corners:
+                    for b in corners:
+                        want[node(*a), node(*b)] += st[abs(a[1] - b[1]), abs(a[0] - b[0]), abs(a[2] - b[2])]
+    pos = EO.box_mesh(shape, g["physical_extent"])
+    K = EO.stiffness(pos, shape, np.eye(3), gauss=2).toarray()
+    np.testing.assert_allclose(-K, want, rtol=0, atol=g["tolerance"])
