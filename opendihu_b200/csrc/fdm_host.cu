@@ -275,9 +275,11 @@ struct fdm_solver {
     }
   } adj;
 
-  // pinned host staging for the state transfers
+  // pinned host staging for the state transfers, and the events that mark the chunks of a device-to-host
+  // transfer as landed
   void* stage = nullptr;
   size_t stage_bytes = 0;
+  std::vector<cudaEvent_t> xfer_ev;
 
   // split-path window graphs: (steps, words, nsub, flags pointer) -> executable graph
   std::map<std::tuple<int, int, int, const void*>, cudaGraphExec_t> graphs;
@@ -331,6 +333,9 @@ static int cuda_fail(fdm_solver* s, cudaError_t e, const char* what)
 // captured window graphs hold kernel arguments by value: drop them whenever those can change
 static void invalidate_graphs(fdm_solver* s)
 {
+  for (cudaEvent_t e : s->xfer_ev)
+    cudaEventDestroy(e);
+  s->xfer_ev.clear();
   for (auto& kv : s->graphs)
     cudaGraphExecDestroy(kv.second);
   s->graphs.clear();
@@ -947,6 +952,57 @@ static cudaError_t ensure_stage(fdm_solver* s, size_t bytes)
   return e;
 }
 
+// State transfers between the caller's FP64 arrays and the device, through pinned staging: the work is cut
+// into chunks of nodes; host threads take the chunks in order, and a chunk's DMA is queued as soon as its
+// staging part is written (set) or its staging part is converted as soon as its DMA has landed (get), so the
+// host copies and conversions overlap the transfers.  A chunk of the other states carries FP64 values, or
+// FP32 (value, residual) pairs in FP32 mode.
+namespace {
+struct XferChunk {
+  bool vm;        // Vm (FP64) or the other states
+  size_t a, b;    // element range of Vm [0, N) or of the other states [0, M)
+};
+constexpr size_t kXferChunk = (size_t)1 << 20;
+
+std::vector<XferChunk> xfer_chunks(size_t N, size_t M)
+{
+  std::vector<XferChunk> c;
+  for (size_t a = 0; a < N; a += kXferChunk)
+    c.push_back({true, a, std::min(N, a + kXferChunk)});
+  for (size_t a = 0; a < M; a += kXferChunk)
+    c.push_back({false, a, std::min(M, a + kXferChunk)});
+  return c;
+}
+
+// runs fn(chunk index) on up to 16 host threads, chunks claimed in order; the first error wins
+template<class F>
+cudaError_t for_chunks(int device, size_t n, F fn)
+{
+  std::atomic<size_t> next{0};
+  std::atomic<int> err{(int)cudaSuccess};
+  auto work = [&]() {
+    cudaError_t e = cudaSetDevice(device);
+    for (size_t j; e == cudaSuccess && (j = next.fetch_add(1)) < n;)
+      e = fn(j);
+    if (e != cudaSuccess) {
+      int expected = (int)cudaSuccess;
+      err.compare_exchange_strong(expected, (int)e);
+    }
+  };
+  const unsigned nt = (unsigned)std::min<size_t>(n, std::min(16u, std::max(1u, std::thread::hardware_concurrency())));
+  if (nt <= 1) {
+    work();
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; t++)
+      th.emplace_back(work);
+    for (auto& t : th)
+      t.join();
+  }
+  return (cudaError_t)err.load();
+}
+} // namespace
+
 // SoA host doubles -> device (Vm in FP64, other states in the reaction precision)
 extern "C" int fdm_set_states(fdm_solver* s, const double* states)
 {
@@ -957,34 +1013,39 @@ extern "C" int fdm_set_states(fdm_solver* s, const double* states)
   FDM_BIND(s);
   const int NS = s->model->n_states;
   const size_t N = (size_t)s->n_nodes;
-  if (N == 0)
-    return FDM_OK;
   const size_t M = N * (size_t)std::max(NS - 1, 0);
-  // staging layout: Vm (N doubles), then the other states as FP64 or as FP32 (value, residual) pairs
-  const size_t bytes = N * 8 + (s->real_bytes == 8 ? M * 8 : M * 8);
+  // staging layout: Vm (N doubles), then the other states as FP64 or as FP32 (value, residual) arrays
   FDM_CUDA(cudaStreamSynchronize(s->stream));
-  FDM_CUDA(ensure_stage(s, bytes));
+  FDM_CUDA(ensure_stage(s, N * 8 + M * 8));
   double* vm = (double*)s->stage;
-  parallel_for(N, [&](size_t a, size_t b) { std::memcpy(vm + a, states + a, (b - a) * sizeof(double)); });
-  FDM_CUDA(cudaMemcpyAsync(s->vm.p, vm, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream));
-  if (M > 0) {
-    if (s->real_bytes == 8) {
-      double* st = vm + N;
-      parallel_for(M, [&](size_t a, size_t b) { std::memcpy(st + a, states + N + a, (b - a) * sizeof(double)); });
-      FDM_CUDA(cudaMemcpyAsync(s->states.p, st, sizeof(double) * M, cudaMemcpyHostToDevice, s->stream));
-    } else {
-      float* hi = (float*)(vm + N);
-      float* lo = hi + M;
-      parallel_for(M, [&](size_t a, size_t b) {
-        for (size_t i = a; i < b; i++) {
-          hi[i] = (float)states[N + i];
-          lo[i] = (float)(states[N + i] - (double)hi[i]);
-        }
-      });
-      FDM_CUDA(cudaMemcpyAsync(s->states.p, hi, sizeof(float) * M, cudaMemcpyHostToDevice, s->stream));
-      FDM_CUDA(cudaMemcpyAsync(s->states_lo.p, lo, sizeof(float) * M, cudaMemcpyHostToDevice, s->stream));
+  double* st = vm + N;
+  float* hi = (float*)(vm + N);
+  float* lo = hi + M;
+  const bool f64 = s->real_bytes == 8;
+  const std::vector<XferChunk> chunks = xfer_chunks(N, M);
+  FDM_CUDA(for_chunks(s->cfg.device, chunks.size(), [&](size_t j) -> cudaError_t {
+    const XferChunk& c = chunks[j];
+    const size_t n = c.b - c.a;
+    if (c.vm) {
+      std::memcpy(vm + c.a, states + c.a, n * sizeof(double));
+      return cudaMemcpyAsync(s->vm.p + c.a, vm + c.a, n * sizeof(double), cudaMemcpyHostToDevice, s->stream);
     }
-  }
+    if (f64) {
+      std::memcpy(st + c.a, states + N + c.a, n * sizeof(double));
+      return cudaMemcpyAsync((double*)s->states.p + c.a, st + c.a, n * sizeof(double), cudaMemcpyHostToDevice,
+                             s->stream);
+    }
+    for (size_t i = c.a; i < c.b; i++) {
+      hi[i] = (float)states[N + i];
+      lo[i] = (float)(states[N + i] - (double)hi[i]);
+    }
+    cudaError_t e = cudaMemcpyAsync((float*)s->states.p + c.a, hi + c.a, n * sizeof(float), cudaMemcpyHostToDevice,
+                                    s->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync((float*)s->states_lo.p + c.a, lo + c.a, n * sizeof(float), cudaMemcpyHostToDevice,
+                          s->stream);
+    return e;
+  }));
   FDM_CUDA(cudaStreamSynchronize(s->stream));
   return FDM_OK;
 }
@@ -998,36 +1059,51 @@ extern "C" int fdm_get_states(fdm_solver* s, double* states)
   FDM_BIND(s);
   const int NS = s->model->n_states;
   const size_t N = (size_t)s->n_nodes;
-  if (N == 0)
-    return FDM_OK;
   const size_t M = N * (size_t)std::max(NS - 1, 0);
   FDM_CUDA(ensure_stage(s, N * 8 + M * 8));
   double* vm = (double*)s->stage;
-  FDM_CUDA(cudaMemcpyAsync(vm, s->vm.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream));
-  if (M > 0) {
-    if (s->real_bytes == 8) {
-      FDM_CUDA(cudaMemcpyAsync(vm + N, s->states.p, sizeof(double) * M, cudaMemcpyDeviceToHost, s->stream));
-    } else {
-      float* hi = (float*)(vm + N);
-      FDM_CUDA(cudaMemcpyAsync(hi, s->states.p, sizeof(float) * M, cudaMemcpyDeviceToHost, s->stream));
-      FDM_CUDA(cudaMemcpyAsync(hi + M, s->states_lo.p, sizeof(float) * M, cudaMemcpyDeviceToHost, s->stream));
-    }
+  double* st = vm + N;
+  float* hi = (float*)(vm + N);
+  float* lo = hi + M;
+  const bool f64 = s->real_bytes == 8;
+  const std::vector<XferChunk> chunks = xfer_chunks(N, M);
+  while (s->xfer_ev.size() < chunks.size()) {
+    cudaEvent_t e = nullptr;
+    FDM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    s->xfer_ev.push_back(e);
   }
+  // every chunk's DMA queued in order, each followed by its event
+  for (size_t j = 0; j < chunks.size(); j++) {
+    const XferChunk& c = chunks[j];
+    const size_t n = c.b - c.a;
+    if (c.vm) {
+      FDM_CUDA(cudaMemcpyAsync(vm + c.a, s->vm.p + c.a, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    } else if (f64) {
+      FDM_CUDA(cudaMemcpyAsync(st + c.a, (const double*)s->states.p + c.a, n * sizeof(double), cudaMemcpyDeviceToHost,
+                               s->stream));
+    } else {
+      FDM_CUDA(cudaMemcpyAsync(hi + c.a, (const float*)s->states.p + c.a, n * sizeof(float), cudaMemcpyDeviceToHost,
+                               s->stream));
+      FDM_CUDA(cudaMemcpyAsync(lo + c.a, (const float*)s->states_lo.p + c.a, n * sizeof(float),
+                               cudaMemcpyDeviceToHost, s->stream));
+    }
+    FDM_CUDA(cudaEventRecord(s->xfer_ev[j], s->stream));
+  }
+  FDM_CUDA(for_chunks(s->cfg.device, chunks.size(), [&](size_t j) -> cudaError_t {
+    const cudaError_t e = cudaEventSynchronize(s->xfer_ev[j]);
+    if (e != cudaSuccess)
+      return e;
+    const XferChunk& c = chunks[j];
+    if (c.vm)
+      std::memcpy(states + c.a, vm + c.a, (c.b - c.a) * sizeof(double));
+    else if (f64)
+      std::memcpy(states + N + c.a, st + c.a, (c.b - c.a) * sizeof(double));
+    else
+      for (size_t i = c.a; i < c.b; i++)
+        states[N + i] = (double)hi[i] + (double)lo[i];
+    return cudaSuccess;
+  }));
   FDM_CUDA(cudaStreamSynchronize(s->stream));
-  parallel_for(N, [&](size_t a, size_t b) { std::memcpy(states + a, vm + a, (b - a) * sizeof(double)); });
-  if (M > 0) {
-    if (s->real_bytes == 8) {
-      const double* st = vm + N;
-      parallel_for(M, [&](size_t a, size_t b) { std::memcpy(states + N + a, st + a, (b - a) * sizeof(double)); });
-    } else {
-      const float* hi = (const float*)(vm + N);
-      const float* lo = hi + M;
-      parallel_for(M, [&](size_t a, size_t b) {
-        for (size_t i = a; i < b; i++)
-          states[N + i] = (double)hi[i] + (double)lo[i];
-      });
-    }
-  }
   return FDM_OK;
 }
 
@@ -2066,7 +2142,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
         cur ^= 1;
         if (half == 0) {
           FDM_CUDA(launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
-                                         s->stream, E.counter.p, E.nbuf.p, s->cfg.n_ranks, s->max_fiber_len));
+                                         s->stream, E.counter.p, E.nbuf.p, s->cfg.n_ranks));
           s->launches++;
         }
       }
@@ -2090,7 +2166,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
           ce = launch_reaction(s->cfg.model, rk, mk, ra, s->stream);
           if (ce == cudaSuccess && half == 0)
             ce = launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
-                                       s->stream, nullptr, nullptr, 1, s->max_fiber_len);
+                                       s->stream);
         }
       }
       cudaError_t ee = cudaStreamEndCapture(s->stream, &g);
@@ -2124,7 +2200,7 @@ static int run_window(fdm_solver* s, const SplitStep* host_steps, int n_steps, d
         FDM_CUDA(cudaEventRecord(e1, s->stream));
       if (half == 0) {
         FDM_CUDA(launch_diffusion(s->n_fibers, s->off_d.p, s->coef.p, s->n_nodes, s->vm.p, s->scratch.p,
-                                       s->stream, nullptr, nullptr, 1, s->max_fiber_len));
+                                       s->stream));
         s->launches++;
       }
     }
@@ -3277,8 +3353,7 @@ extern "C" int fdm_adjoint_backward(fdm_solver* s, const double* trace_grad, dou
         FDM_CUDA(launch_reaction(s->cfg.model, REAL_F64, mk, ra, s->stream));
         s->launches++;
         if (half == 0) {
-          FDM_CUDA(launch_diffusion(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream, nullptr, nullptr, 1,
-                                    s->max_fiber_len));
+          FDM_CUDA(launch_diffusion(nf, s->off_d.p, coef_of(b + jj), N, s->vm.p, s->scratch.p, s->stream));
           s->launches++;
         }
       }

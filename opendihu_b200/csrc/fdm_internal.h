@@ -63,11 +63,9 @@ cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, cons
                                 double* coef, int64_t stride, cudaStream_t s);
 // one diffusion solve of every fiber in place on vm (scratch: one double per node): a warp per fiber, or a
 // CTA per fiber when the fibers are few
-// CTA per fiber when the fibers are few; given the longest fiber (max_fiber_len > 0) such a CTA stages its fiber
-// in shared memory when it fits
 cudaError_t launch_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
                              double* vm, double* scratch, cudaStream_t s, const int* eq_counter = nullptr,
-                             const int* eq_nbuf = nullptr, int n_ranks = 1, int64_t max_fiber_len = 0);
+                             const int* eq_nbuf = nullptr, int n_ranks = 1);
 // one half step with the equilibrium skip (fdm_equilibrium.cuh): speculative reaction, equilibrium tests,
 // scan of the buffers, commit (and the trace after half 1)
 cudaError_t launch_equilibrium_half(int model, RealKind rk, MathKind mk, const ReactionArgs& a, const EqLayout& L,

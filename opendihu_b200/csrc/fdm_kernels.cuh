@@ -1337,75 +1337,6 @@ __global__ void __launch_bounds__(T) diffusion_block_kernel(const int64_t* __res
   }
 }
 
-// diffusion_block_kernel with the fiber staged in shared memory: its six coefficient arrays and Vm are
-// loaded once with coalesced loads (consecutive threads, consecutive nodes), the two scans run on shared memory,
-// and the new Vm is stored back coalesced.  The per-thread node ranges of the scans are contiguous, so without
-// staging every thread's loads fall in other cache lines than its neighbours' and each sweep waits on L2.
-// Dynamic shared memory: 8 doubles per node of the longest fiber (the host falls back to the unstaged kernel
-// for fibers that do not fit).
-template<int T>
-__global__ void __launch_bounds__(T) diffusion_block_staged_kernel(const int64_t* __restrict__ fiber_offsets,
-                                                                   const double* __restrict__ coef, int64_t stride,
-                                                                   double* __restrict__ vm,
-                                                                   const int* __restrict__ eq_counter,
-                                                                   const int* __restrict__ eq_nbuf, int n_ranks)
-{
-  extern __shared__ double sm[];
-  __shared__ double sF[2 * (T / 32) + 1], sG[2 * (T / 32) + 1];
-  const int f = blockIdx.x;
-  const int tid = threadIdx.x;
-  if (eq_counter && eq_counter[f % n_ranks] == eq_nbuf[f % n_ranks])
-    return; // the whole CTA: the rank's buffers are all inactive
-  const int64_t o = fiber_offsets[f];
-  const int n = (int)(fiber_offsets[f + 1] - o);
-  const int L = (n + T - 1) / T;
-  const int cap = L * T;
-  double* mulF = sm;
-  double* inv = mulF + cap;
-  double* cp = inv + cap;
-  double* cl = cp + cap;
-  double* cm = cl + cap;
-  double* cr = cm + cap;
-  double* v = cr + cap;
-  double* dps = v + cap;
-  for (int j = tid; j < n; j += T) {
-    mulF[j] = coef[o + j];
-    inv[j] = coef[stride + o + j];
-    cp[j] = coef[2 * stride + o + j];
-    cl[j] = coef[3 * stride + o + j];
-    cm[j] = coef[4 * stride + o + j];
-    cr[j] = coef[5 * stride + o + j];
-    v[j] = vm[o + j];
-  }
-  __syncthreads();
-  const int lo = min(tid * L, n), hi = min((tid + 1) * L, n);
-  auto rhs = [&](int j) {
-    const double up = j > 0 ? v[j - 1] : 0.0;
-    const double un = j < n - 1 ? v[j + 1] : 0.0;
-    return cl[j] * up + cm[j] * v[j] + cr[j] * un;
-  };
-  Affine acc{1.0, 0.0};
-  for (int j = lo; j < hi; j++)
-    acc = compose(acc, Affine{mulF[j], inv[j] * rhs(j)});
-  double dp = block_scan_incoming<T, false>(acc, sF, sG);
-  for (int j = lo; j < hi; j++) {
-    dp = mulF[j] * dp + inv[j] * rhs(j);
-    dps[j] = dp;
-  }
-  __syncthreads(); // every read of the old Vm done, sF/sG free
-  Affine bacc{1.0, 0.0};
-  for (int j = hi - 1; j >= lo; j--)
-    bacc = compose(bacc, Affine{-cp[j], dps[j]});
-  double x = block_scan_incoming<T, true>(bacc, sF, sG);
-  for (int j = hi - 1; j >= lo; j--) {
-    x = -cp[j] * x + dps[j];
-    v[j] = x;
-  }
-  __syncthreads();
-  for (int j = tid; j < n; j += T)
-    vm[o + j] = v[j];
-}
-
 // Adjoint of one diffusion solve (see adjoint_diffusion_warp_kernel for the algebra) with one CTA per
 // fiber of at most T*M nodes: thread tid owns nodes tid*M .. tid*M+M-1 in registers, the two sweeps of the
 // LU solve are block-wide scans of affine maps (as in the fused kernel), neighbours across threads go

@@ -121,43 +121,12 @@ cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, cons
 // needed before a warp per fiber fills the GPU)
 constexpr int DIFFUSION_BLOCK_MAX_FIBERS = 4 * 148;
 
-// the staged block kernel's dynamic shared memory limit, set once per device (bit d of the mask)
-static std::atomic<uint64_t> g_staged_attr{0};
-constexpr int kStagedT = 256;
-constexpr size_t kStagedMaxBytes = 200 * 1024;
-// the staged form pays for its coalesced copies only when the solves load the memory system: with fewer
-// fibers than SMs each CTA's solve is pure latency, and the copy phase adds to it (16 fibers x 1481 nodes:
-// 12.1 us staged against 9.2 us direct per solve)
-constexpr int kStagedMinFibers = 148;
-
 cudaError_t launch_diffusion(int n_fibers, const int64_t* fiber_offsets, const double* coef, int64_t stride,
                                   double* vm, double* scratch, cudaStream_t s, const int* eq_counter,
-                                  const int* eq_nbuf, int n_ranks, int64_t max_fiber_len)
+                                  const int* eq_nbuf, int n_ranks)
 {
   if (n_fibers == 0)
     return cudaSuccess;
-  const size_t staged_bytes =
-      max_fiber_len > 0 ? (size_t)8 * sizeof(double) * (size_t)((max_fiber_len + kStagedT - 1) / kStagedT) * kStagedT
-                        : 0;
-  if (n_fibers < DIFFUSION_BLOCK_MAX_FIBERS && n_fibers >= kStagedMinFibers && staged_bytes > 0 &&
-      staged_bytes <= kStagedMaxBytes) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-      return e;
-    const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
-    if (!bit || !(g_staged_attr.load(std::memory_order_acquire) & bit)) {
-      e = cudaFuncSetAttribute(diffusion_block_staged_kernel<kStagedT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kStagedMaxBytes);
-      if (e != cudaSuccess)
-        return e;
-      if (bit)
-        g_staged_attr.fetch_or(bit, std::memory_order_acq_rel);
-    }
-    diffusion_block_staged_kernel<kStagedT><<<(unsigned)n_fibers, kStagedT, staged_bytes, s>>>(
-        fiber_offsets, coef, stride, vm, eq_counter, eq_nbuf, n_ranks > 0 ? n_ranks : 1);
-    return cudaGetLastError();
-  }
   if (n_fibers < DIFFUSION_BLOCK_MAX_FIBERS) {
     // few fibers: a CTA per fiber fills more of the GPU than a warp per fiber
     diffusion_block_kernel<256><<<(unsigned)n_fibers, 256, 0, s>>>(fiber_offsets, coef, stride, vm, scratch,
