@@ -612,8 +612,8 @@ def main():
     steps_per_launch = split_steps / max(launches_per_kernel, 1)
 
     # end to end through the public API with host buffers, over the same K steps: H2D of the states from
-    # pinned staging, the advance, D2H of the states, every step
-    host_states = fused.states()
+    # page-locked host memory, the advance, D2H of the states, every step
+    host_states = fused.states(out=fused.pinned_states())
     barrier(pg)
     t0 = time.perf_counter()
     for _ in range(args.steps):

@@ -25,6 +25,7 @@
 #ifndef FDM_B200_H
 #define FDM_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -130,9 +131,18 @@ int fdm_set_prefactor(fdm_solver *s, const double *prefactor);
 int fdm_set_parameters(fdm_solver *s, const double *parameters);
 int fdm_get_parameters(fdm_solver *s, double *parameters);
 
-/* states[state * n_nodes + node] (SoA); state 0 is Vm */
+/* states[state * n_nodes + node] (SoA); state 0 is Vm.  Host arrays from fdm_host_alloc are transferred
+ * directly (the other states converted on the device); other host memory goes through pinned staging, with
+ * the host copies overlapping the transfers.  Both forms give bit-identical results. */
 int fdm_set_states(fdm_solver *s, const double *states);
 int fdm_get_states(fdm_solver *s, double *states);
+
+/* Page-locked host memory for state arrays (the reference keeps its fiber data in host vectors,
+ * fast_monodomain_solver_initialization.tpp:145-347, and copies them in and out every call,
+ * gpu.tpp:478-481): *ptr receives `bytes` of pinned memory the transfers use without staging.
+ * fdm_host_free releases it (FDM_ERR_ARG for a pointer fdm_host_alloc did not return). */
+int fdm_host_alloc(size_t bytes, void **ptr);
+int fdm_host_free(void *ptr);
 int fdm_get_vm(fdm_solver *s, double *vm);
 
 /* Stimulation inputs (fast_monodomain_solver_initialization.tpp:145-347):

@@ -39,7 +39,7 @@ EXPORTED = [
     "fdm_emg_potential_flow", "fdm_emg_set_direction", "fdm_emg_set_conductivity", "fdm_emg_set_fiber_mapping",
     "fdm_emg_map_fibers", "fdm_emg_map_values", "fdm_emg_set_vm", "fdm_emg_solve", "fdm_emg_get",
     "fdm_emg_get_stencil", "fdm_emg_timing", "fdm_debug_fail_allocation", "fdm_set_activation_recording",
-    "fdm_get_activation_steps", "fdm_register_model_library",
+    "fdm_get_activation_steps", "fdm_register_model_library", "fdm_host_alloc", "fdm_host_free",
 ]
 
 #: fdm_emg_get fields of include/fdm_b200.h
@@ -100,6 +100,8 @@ def lib() -> C.CDLL:
         "fdm_get_parameters": (C.c_int, [P, d]),
         "fdm_set_states": (C.c_int, [P, d]),
         "fdm_get_states": (C.c_int, [P, d]),
+        "fdm_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
+        "fdm_host_free": (C.c_int, [C.c_void_p]),
         "fdm_get_vm": (C.c_int, [P, d]),
         "fdm_set_stimulation": (C.c_int, [P, u8, C.c_int, C.c_int, i32, i32, d, d, d, d, C.c_int]),
         "fdm_get_clamp_nodes": (C.c_int, [P, i64, i32, u8]),
@@ -183,6 +185,30 @@ def check(rc: int, handle=None):
     if rc != FDM_OK:
         msg = lib().fdm_last_error(handle)
         raise FdmError(rc, msg.decode() if msg else "")
+
+
+class _PinnedBuffer:
+    """Page-locked host memory from fdm_host_alloc, exposed to numpy and released with the last array over it."""
+
+    def __init__(self, shape, dtype):
+        self.ptr = None
+        dt = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dt.itemsize
+        p = C.c_void_p()
+        check(lib().fdm_host_alloc(max(nbytes, 1), C.byref(p)))
+        self.ptr = p.value
+        self.__array_interface__ = {"shape": tuple(int(n) for n in shape), "typestr": dt.str,
+                                    "data": (self.ptr, False), "version": 3}
+
+    def __del__(self):
+        if self.ptr:
+            lib().fdm_host_free(C.c_void_p(self.ptr))
+            self.ptr = None
+
+
+def pinned_array(shape, dtype=np.float64) -> np.ndarray:
+    """A C-contiguous array in page-locked host memory (fdm_host_alloc): the state transfers DMA it directly."""
+    return np.asarray(_PinnedBuffer(shape, dtype))
 
 
 def default_config() -> Config:

@@ -280,6 +280,7 @@ struct fdm_solver {
   void* stage = nullptr;
   size_t stage_bytes = 0;
   std::vector<cudaEvent_t> xfer_ev;
+  DevBuf<double> xfer64; // direct transfers from fdm_host_alloc memory: the other states in FP64 (FP32 mode)
 
   // split-path window graphs: (steps, words, nsub, flags pointer) -> executable graph
   std::map<std::tuple<int, int, int, const void*>, cudaGraphExec_t> graphs;
@@ -336,6 +337,7 @@ static void invalidate_graphs(fdm_solver* s)
   for (cudaEvent_t e : s->xfer_ev)
     cudaEventDestroy(e);
   s->xfer_ev.clear();
+  s->xfer64.release();
   for (auto& kv : s->graphs)
     cudaGraphExecDestroy(kv.second);
   s->graphs.clear();
@@ -952,6 +954,61 @@ static cudaError_t ensure_stage(fdm_solver* s, size_t bytes)
   return e;
 }
 
+// Page-locked host buffers handed out by fdm_host_alloc: start -> size.  A state array that lies inside one
+// is transferred by DMA directly, without the staging copy.
+static std::mutex g_host_mu;
+static std::map<uintptr_t, size_t> g_host_bufs;
+
+static bool host_buffer_holds(const void* p, size_t bytes)
+{
+  const uintptr_t a = (uintptr_t)p;
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  auto it = g_host_bufs.upper_bound(a);
+  if (it == g_host_bufs.begin())
+    return false;
+  --it;
+  return a >= it->first && a + bytes <= it->first + it->second;
+}
+
+extern "C" int fdm_host_alloc(size_t bytes, void** ptr)
+{
+  if (!ptr || bytes == 0)
+    return fail(nullptr, FDM_ERR_ARG, "fdm_host_alloc: bad argument");
+  *ptr = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(nullptr, FDM_ERR_NO_DEVICE, "fdm_host_alloc: no CUDA device");
+  }
+  void* p = nullptr;
+  const cudaError_t e = pinned_alloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(nullptr, FDM_ERR_CUDA, std::string("fdm_host_alloc: ") + cudaGetErrorString(e));
+  }
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  g_host_bufs[(uintptr_t)p] = bytes;
+  *ptr = p;
+  return FDM_OK;
+}
+
+extern "C" int fdm_host_free(void* ptr)
+{
+  if (!ptr)
+    return FDM_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_host_mu);
+    auto it = g_host_bufs.find((uintptr_t)ptr);
+    if (it == g_host_bufs.end())
+      return fail(nullptr, FDM_ERR_ARG, "fdm_host_free: not a pointer from fdm_host_alloc");
+    g_host_bufs.erase(it);
+  }
+  const cudaError_t e = cudaFreeHost(ptr);
+  if (e != cudaSuccess)
+    return fail(nullptr, FDM_ERR_CUDA, std::string("fdm_host_free: ") + cudaGetErrorString(e));
+  return FDM_OK;
+}
+
 // State transfers between the caller's FP64 arrays and the device, through pinned staging: the work is cut
 // into chunks of nodes; host threads take the chunks in order, and a chunk's DMA is queued as soon as its
 // staging part is written (set) or its staging part is converted as soon as its DMA has landed (get), so the
@@ -1014,6 +1071,24 @@ extern "C" int fdm_set_states(fdm_solver* s, const double* states)
   const int NS = s->model->n_states;
   const size_t N = (size_t)s->n_nodes;
   const size_t M = N * (size_t)std::max(NS - 1, 0);
+  if (host_buffer_holds(states, (N + M) * sizeof(double))) {
+    // page-locked caller memory: DMA straight from it (FP32 mode: the other states through a device FP64
+    // buffer and the conversion kernel)
+    FDM_CUDA(cudaMemcpyAsync(s->vm.p, states, N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    if (M > 0) {
+      if (s->real_bytes == 8) {
+        FDM_CUDA(cudaMemcpyAsync(s->states.p, states + N, M * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+      } else {
+        if (s->xfer64.n < M)
+          FDM_CUDA(s->xfer64.alloc(M));
+        FDM_CUDA(cudaMemcpyAsync(s->xfer64.p, states + N, M * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+        FDM_CUDA(launch_states_to_pairs(s->xfer64.p, (float*)s->states.p, (float*)s->states_lo.p, (int64_t)M,
+                                        s->stream));
+      }
+    }
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+    return FDM_OK;
+  }
   // staging layout: Vm (N doubles), then the other states as FP64 or as FP32 (value, residual) arrays
   FDM_CUDA(cudaStreamSynchronize(s->stream));
   FDM_CUDA(ensure_stage(s, N * 8 + M * 8));
@@ -1060,6 +1135,22 @@ extern "C" int fdm_get_states(fdm_solver* s, double* states)
   const int NS = s->model->n_states;
   const size_t N = (size_t)s->n_nodes;
   const size_t M = N * (size_t)std::max(NS - 1, 0);
+  if (host_buffer_holds(states, (N + M) * sizeof(double))) {
+    if (M > 0) {
+      if (s->real_bytes == 8) {
+        FDM_CUDA(cudaMemcpyAsync(states + N, s->states.p, M * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+      } else {
+        if (s->xfer64.n < M)
+          FDM_CUDA(s->xfer64.alloc(M));
+        FDM_CUDA(launch_pairs_to_states((const float*)s->states.p, (const float*)s->states_lo.p, s->xfer64.p,
+                                        (int64_t)M, s->stream));
+        FDM_CUDA(cudaMemcpyAsync(states + N, s->xfer64.p, M * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+      }
+    }
+    FDM_CUDA(cudaMemcpyAsync(states, s->vm.p, N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    FDM_CUDA(cudaStreamSynchronize(s->stream));
+    return FDM_OK;
+  }
   FDM_CUDA(ensure_stage(s, N * 8 + M * 8));
   double* vm = (double*)s->stage;
   double* st = vm + N;

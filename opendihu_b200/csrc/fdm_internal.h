@@ -59,6 +59,10 @@ cudaError_t launch_reaction(int model, RealKind rk, MathKind mk, const ReactionA
 cudaError_t launch_equilibrium_search(int model, MathKind mk, double* u, const double* u0, const double* params,
                                EquilibriumSearch* es, int64_t max_iterations, cudaStream_t s);
 cudaError_t launch_schedule(const StimArgs& a, const SplitStep* steps, int n_steps, cudaStream_t s);
+// FP64 states <-> FP32 (value, residual) pairs on the device: hi = (float)x, lo = (float)(x - hi); x = hi + lo
+// (the same expressions as the host conversions of the staged transfers, so both give the same bits)
+cudaError_t launch_states_to_pairs(const double* x, float* hi, float* lo, int64_t n, cudaStream_t s);
+cudaError_t launch_pairs_to_states(const float* hi, const float* lo, double* x, int64_t n, cudaStream_t s);
 cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, const double* element_lengths, const double* prefactor, double dt, int implicit_euler,
                                 double* coef, int64_t stride, cudaStream_t s);
 // one diffusion solve of every fiber in place on vm (scratch: one double per node): a warp per fiber, or a

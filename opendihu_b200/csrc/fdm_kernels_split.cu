@@ -1,5 +1,6 @@
 // Split-path kernels (reaction, diffusion, stimulation schedule) and the model table.
 #define FDM_COMMON_KERNELS_TU
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -114,6 +115,46 @@ cudaError_t launch_coefficients(int n_fibers, const int64_t* fiber_offsets, cons
   const int T = 64;
   diffusion_coefficients_kernel<<<(n_fibers + T - 1) / T, T, 0, s>>>(n_fibers, fiber_offsets, element_lengths,
                                                                      prefactor, dt, implicit_euler, coef, stride);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) states_to_pairs_kernel(const double* __restrict__ x, float* __restrict__ hi,
+                                                              float* __restrict__ lo, int64_t n)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    const float h = __double2float_rn(v);
+    hi[i] = h;
+    lo[i] = __double2float_rn(__dsub_rn(v, (double)h));
+  }
+}
+
+__global__ void __launch_bounds__(256) pairs_to_states_kernel(const float* __restrict__ hi,
+                                                              const float* __restrict__ lo, double* __restrict__ x,
+                                                              int64_t n)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = __dadd_rn((double)hi[i], (double)lo[i]);
+}
+
+static unsigned elementwise_blocks(int64_t n)
+{
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+}
+
+cudaError_t launch_states_to_pairs(const double* x, float* hi, float* lo, int64_t n, cudaStream_t s)
+{
+  if (n <= 0)
+    return cudaSuccess;
+  states_to_pairs_kernel<<<elementwise_blocks(n), 256, 0, s>>>(x, hi, lo, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_to_states(const float* hi, const float* lo, double* x, int64_t n, cudaStream_t s)
+{
+  if (n <= 0)
+    return cudaSuccess;
+  pairs_to_states_kernel<<<elementwise_blocks(n), 256, 0, s>>>(hi, lo, x, n);
   return cudaGetLastError();
 }
 

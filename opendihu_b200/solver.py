@@ -826,6 +826,11 @@ class FastMonodomainSolver:
         self._call(N.lib().fdm_get_states, N.ptr(out, C.c_double))
         return out
 
+    def pinned_states(self) -> np.ndarray:
+        """An array for all states [state, node] in page-locked host memory: ``set_states`` and
+        ``states(out=...)`` move it by DMA without the staging copy (the values are the same either way)."""
+        return N.pinned_array((model_sizes(self.system.model)[0], self.system.n_nodes))
+
     def set_states(self, states: np.ndarray):
         st = np.ascontiguousarray(states, np.float64)
         self._call(N.lib().fdm_set_states, N.ptr(st, C.c_double))

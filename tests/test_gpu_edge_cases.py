@@ -83,3 +83,34 @@ def test_split_diffusion_on_both_sides_of_the_block_threshold(n_fibers):
                          motor_unit_no=rng.integers(0, 4, size=n_fibers).astype(np.int32), end_time=0.6,
                          diffusion_scheme="CrankNicolson")
     GP.compare(s, "split", "fp64", GP.VM_TOL_FP64, 1e-8)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_page_locked_state_arrays_transfer_like_pageable_ones(precision):
+    # fdm_host_alloc memory is moved by DMA directly (FP32 mode: converted on the device); pageable arrays go
+    # through the staging copy: the same bits either way, in both directions
+    from opendihu_b200 import _native as N
+    s = WL.batched_hh(n_fibers=40, seed=5, end_time=0.5)
+    H.complete(s)
+    with S.FastMonodomainSolver(s.copy(), method="fused", precision=precision) as slv:
+        slv.advanceTimeSpan()
+        pageable = slv.states()
+        pinned = slv.states(out=slv.pinned_states())
+        assert np.array_equal(pageable.view(np.int64), pinned.view(np.int64))
+        rng = np.random.default_rng(1)
+        new = pageable + rng.normal(scale=1e-3, size=pageable.shape)
+        src = slv.pinned_states()
+        src[...] = new
+        slv.set_states(src)
+        a = slv.states()
+        slv.set_states(new)
+        b = slv.states(out=slv.pinned_states())
+        assert np.array_equal(a.view(np.int64), b.view(np.int64))
+        if precision == "fp64":
+            assert np.array_equal(a.view(np.int64), new.view(np.int64))
+        else:
+            # FP32 mode keeps (value, residual) pairs: FP64 values survive the round trip to ~1e-14 relative
+            np.testing.assert_allclose(a, new, rtol=1e-13, atol=1e-300)
+    buf = np.zeros(4)
+    import ctypes as C
+    assert N.lib().fdm_host_free(buf.ctypes.data_as(C.c_void_p)) == N.FDM_ERR_ARG

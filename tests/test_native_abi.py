@@ -70,3 +70,19 @@ def test_cluster_mode_config_checked_before_the_device(field, value, code):
     h = C.c_void_p()
     assert N.lib().fdm_create(C.byref(cfg), C.byref(h)) == code
     assert b"cluster" in N.lib().fdm_last_error(None)
+
+
+def test_host_alloc_fails_loudly_without_device_and_free_checks_its_pointer():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("the device form is tested in test_gpu_edge_cases.py")
+    p = C.c_void_p()
+    assert N.lib().fdm_host_alloc(1024, C.byref(p)) == N.FDM_ERR_NO_DEVICE
+    assert p.value is None
+    assert b"no CUDA device" in N.lib().fdm_last_error(None)
+    assert N.lib().fdm_host_alloc(0, C.byref(p)) == N.FDM_ERR_ARG
+    buf = np.zeros(4)
+    assert N.lib().fdm_host_free(buf.ctypes.data_as(C.c_void_p)) == N.FDM_ERR_ARG
+    assert N.lib().fdm_host_free(None) == N.FDM_OK
+    with pytest.raises(N.FdmError):
+        N.pinned_array((2, 3))
