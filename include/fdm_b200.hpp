@@ -39,6 +39,31 @@ class Error : public std::runtime_error {
   int code_;
 };
 
+/* Page-locked host memory (fdm_host_alloc) for std::vector: state arrays in it are transferred by DMA without
+ * staging, e.g. std::vector<double, fdm::PinnedAllocator<double>> states(nStates * nNodes). */
+template<class T>
+struct PinnedAllocator {
+  using value_type = T;
+  PinnedAllocator() = default;
+  template<class U>
+  PinnedAllocator(const PinnedAllocator<U>&) {}
+  T* allocate(size_t n)
+  {
+    void* p = nullptr;
+    const int rc = fdm_host_alloc(n * sizeof(T), &p);
+    if (rc != FDM_OK) {
+      const char* m = fdm_last_error(nullptr);
+      throw Error(rc, m ? m : "fdm_host_alloc failed");
+    }
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t) { fdm_host_free(p); }
+  template<class U>
+  bool operator==(const PinnedAllocator<U>&) const { return true; }
+  template<class U>
+  bool operator!=(const PinnedAllocator<U>&) const { return false; }
+};
+
 /* The parsed settings of one FastMonodomainSolver (all fibers of the rank). */
 struct FiberSettings {
   fdm_config config{};                       // model, schemes, method, precision, time step widths, options

@@ -1039,8 +1039,12 @@ cudaError_t for_chunks(int device, size_t n, F fn)
   std::atomic<int> err{(int)cudaSuccess};
   auto work = [&]() {
     cudaError_t e = cudaSetDevice(device);
-    for (size_t j; e == cudaSuccess && (j = next.fetch_add(1)) < n;)
+    while (e == cudaSuccess) {
+      const size_t j = next.fetch_add(1);
+      if (j >= n)
+        break;
       e = fn(j);
+    }
     if (e != cudaSuccess) {
       int expected = (int)cudaSuccess;
       err.compare_exchange_strong(expected, (int)e);

@@ -8,6 +8,7 @@
 // whose callback writes one line per call (numbered name, current time, Vm sum) to the output file, and
 // callOutputWriter(0, 0) is called once more.
 // Exit status: 0 done, 2 fdm::Error (message on stderr), 3 the replay after the checkpoint differs.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -82,6 +83,12 @@ int main(int argc, char** argv)
     const std::vector<double> b = slv.states();
     if (a != b) {
       std::fprintf(stderr, "the replay after restoreFiberDataCheckpoint differs\n");
+      return 3;
+    }
+    // page-locked host memory (fdm::PinnedAllocator over fdm_host_alloc) holds the states like any vector
+    const std::vector<double, fdm::PinnedAllocator<double>> pinned(a.begin(), a.end());
+    if (!std::equal(a.begin(), a.end(), pinned.begin())) {
+      std::fprintf(stderr, "the page-locked copy of the states differs\n");
       return 3;
     }
     const fdm::TransferData d = slv.data();
