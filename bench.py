@@ -266,6 +266,17 @@ def shorten_measurement(device: int, span_ms: float, accuracy_ms: float = 5.0):
             steps = sv.split_steps() - n0
         out[name] = {"node_steps_per_s": system.n_nodes * steps / (ms / 1e3), "ms": ms, "strang_steps": steps}
     out["speedup_fp32_over_fp64"] = out["fp32_reaction"]["node_steps_per_s"] / out["fp64_plain"]["node_steps_per_s"]
+    # compute roofline of the FP32 split step, counting the model's own operations: per Heun substep two
+    # right-hand sides and the Heun update (y + dt r, then y + dt/2 (r + r2): 5 per state)
+    meta = json.load(open(os.path.join(ROOT, "opendihu_b200/csrc/generated/"
+                                             "shorten_ocallaghan_davidson_soboleva_2007_a32_c65.json")))
+    n_sub = 2 * int(round(0.5 * system.dt_splitting / system.dt_0d))
+    flops_node_step = n_sub * (2 * meta["operations_per_rhs"]["flops"] + 5 * meta["n_states"])
+    achieved = out["fp32_reaction"]["node_steps_per_s"] * flops_node_step / 1e12
+    fp32_peak = 148 * 128 * 2 * peaks()[1] * 1e6 / 1e12
+    out["fp32_roofline"] = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                            "frac": achieved / fp32_peak, "flops_per_node_step": flops_node_step,
+                            "peak_source": "derived: 148 SMs x 128 FP32 lanes x 2 flop x sm_max_mhz"}
     # accuracy on a sample over a span with action potentials
     grid = WL.shorten_grid(end_time=accuracy_ms)
     fires0 = np.nonzero(np.asarray(grid.firing_events)[0, np.asarray(grid.motor_unit_no) % grid.firing_events.shape[1]])[0]
