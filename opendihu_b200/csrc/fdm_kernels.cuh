@@ -1280,6 +1280,67 @@ __device__ __forceinline__ Affine block_scan_map(Affine acc, double* sF, double*
   return compose(wp, Affine{exF, exG});
 }
 
+// block_scan_map with one barrier: after the warp totals are in sF/sG[0, T/32), every warp scans them itself
+// (the same Hillis-Steele scan block_scan_map runs in warp 0, so the same values) instead of warp 0 scanning
+// and broadcasting through a second barrier.  sF/sG hold T/32 doubles each; a caller that scans again must
+// give the next scan other buffers (warps may still read these totals when a fast warp writes the next ones).
+template<int T, bool REVERSE>
+__device__ __forceinline__ Affine block_scan_map1(Affine acc, double* sF, double* sG, Affine* total)
+{
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  constexpr int NW = T / 32;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    double F, G;
+    if (!REVERSE) {
+      F = __shfl_up_sync(0xffffffffu, acc.F, off);
+      G = __shfl_up_sync(0xffffffffu, acc.G, off);
+      if (lane >= off)
+        acc = compose(Affine{F, G}, acc);
+    } else {
+      F = __shfl_down_sync(0xffffffffu, acc.F, off);
+      G = __shfl_down_sync(0xffffffffu, acc.G, off);
+      if (lane + off < 32)
+        acc = compose(Affine{F, G}, acc);
+    }
+  }
+  const int last_lane = REVERSE ? 0 : 31;
+  if (lane == last_lane) {
+    sF[warp] = acc.F;
+    sG[warp] = acc.G;
+  }
+  double exF = REVERSE ? __shfl_down_sync(0xffffffffu, acc.F, 1) : __shfl_up_sync(0xffffffffu, acc.F, 1);
+  double exG = REVERSE ? __shfl_down_sync(0xffffffffu, acc.G, 1) : __shfl_up_sync(0xffffffffu, acc.G, 1);
+  const bool first_in_warp = REVERSE ? (lane == 31) : (lane == 0);
+  if (first_in_warp) {
+    exF = 1.0;
+    exG = 0.0;
+  }
+  __syncthreads();
+  // lane k holds the total of the k-th warp in scan order; inclusive scan over the lanes
+  const int w = REVERSE ? (NW - 1 - lane) : lane;
+  Affine v = lane < NW ? Affine{sF[w], sG[w]} : Affine{1.0, 0.0};
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double F = __shfl_up_sync(0xffffffffu, v.F, off);
+    const double G = __shfl_up_sync(0xffffffffu, v.G, off);
+    if (lane >= off)
+      v = compose(Affine{F, G}, v);
+  }
+  // this warp's position in scan order; its exclusive prefix is the inclusive scan of the position before
+  const int pos = REVERSE ? (NW - 1 - warp) : warp;
+  const double pF = __shfl_sync(0xffffffffu, v.F, pos > 0 ? pos - 1 : 0);
+  const double pG = __shfl_sync(0xffffffffu, v.G, pos > 0 ? pos - 1 : 0);
+  const Affine wp = pos > 0 ? Affine{pF, pG} : Affine{1.0, 0.0};
+  if (total) {
+    total->F = __shfl_sync(0xffffffffu, v.F, NW - 1);
+    total->G = __shfl_sync(0xffffffffu, v.G, NW - 1);
+  }
+  return compose(wp, Affine{exF, exG});
+}
+
 template<int T, bool REVERSE>
 __device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, double* sG)
 {
@@ -1845,10 +1906,13 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
             normalize_pair(S2[p][q], L2[p][q]);
         }
         if constexpr (!gate_on) {
-          // nodes beyond the bin carry Vm = 0 into the diffusion (zero coefficients, finite values)
+          // nodes beyond the bin carry Vm = 0 into the diffusion (zero coefficients, finite values); only the
+          // threads at the bin's end hold such nodes
+          if (tid * M + 2 * MP > nb) {
 #pragma unroll
-          for (int j = 0; j < 2 * MP; j++)
-            V[j] = tid * M + j < nb ? V[j] : 0.0;
+            for (int j = 0; j < 2 * MP; j++)
+              V[j] = tid * M + j < nb ? V[j] : 0.0;
+          }
         }
       }
       if (store_here) {
@@ -1902,7 +1966,10 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         acc = compose(acc, Affine{sc[0 * CAP + q], d[j]});
       }
       Affine tot_f;
-      const Affine ex_f = block_scan_map<T, false>(acc, sF, sG, &tot_f);
+      // bins mode: one barrier per scan (block_scan_map1), forward and backward totals in separate halves of
+      // sF/sG; cluster mode keeps block_scan_map
+      const Affine ex_f = CLUSTER ? block_scan_map<T, false>(acc, sF, sG, &tot_f)
+                                  : block_scan_map1<T, false>(acc, sF, sG, &tot_f);
       double dp = cluster_incoming(ex_f, tot_f, false);
 #pragma unroll
       for (int j = 0; j < M; j++) {
@@ -1916,14 +1983,14 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         const int q = j * T + tid;
         bacc = compose(bacc, Affine{-sc[1 * CAP + q], d[j]});
       }
-      // No barrier is needed before the backward scan reuses sF/sG: its first writes (warp totals, slots
-      // < T/32) do not overlap the slots the forward scan's results are still read from (T/32 and up), and
-      // warp 0 writes those only after the backward scan's first barrier, which every forward read precedes.
-      // Cluster mode keeps the barrier (its scan totals travel through the cluster).
+      // No barrier is needed before the backward scan: in bins mode its warp totals go to the other half of
+      // sF/sG (the forward totals may still be read).  Cluster mode keeps the barrier (block_scan_map reuses the
+      // same slots, and its scan totals travel through the cluster).
       if constexpr (CLUSTER)
         __syncthreads();
       Affine tot_b;
-      const Affine ex_b = block_scan_map<T, true>(bacc, sF, sG, &tot_b);
+      const Affine ex_b = CLUSTER ? block_scan_map<T, true>(bacc, sF, sG, &tot_b)
+                                  : block_scan_map1<T, true>(bacc, sF + T / 32, sG + T / 32, &tot_b);
       double x = cluster_incoming(ex_b, tot_b, true);
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
