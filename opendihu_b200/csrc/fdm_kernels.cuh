@@ -1346,6 +1346,12 @@ __device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, do
 {
   return block_scan_map<T, REVERSE>(acc, sF, sG, nullptr).G; // applied to the zero entering the first node
 }
+// the same with one barrier (block_scan_map1: the next scan takes other sF/sG slots or follows a barrier)
+template<int T, bool REVERSE>
+__device__ __forceinline__ double block_scan_incoming1(Affine acc, double* sF, double* sG)
+{
+  return block_scan_map1<T, REVERSE>(acc, sF, sG, nullptr).G;
+}
 
 // Split path, few fibers: one diffusion solve per fiber with one CTA per fiber (a warp per fiber would leave
 // most of the GPU idle).  Thread tid owns a contiguous chunk of the fiber; the forward sweep and the back
@@ -1382,7 +1388,7 @@ __global__ void __launch_bounds__(T) diffusion_block_kernel(const int64_t* __res
   Affine acc{1.0, 0.0};
   for (int64_t i = lo; i < hi; i++)
     acc = compose(acc, Affine{mulF[i], inv[i] * rhs(i)});
-  double dp = block_scan_incoming<T, false>(acc, sF, sG);
+  double dp = block_scan_incoming1<T, false>(acc, sF, sG);
   for (int64_t i = lo; i < hi; i++) {
     dp = mulF[i] * dp + inv[i] * rhs(i);
     scratch[i] = dp;
@@ -1391,7 +1397,7 @@ __global__ void __launch_bounds__(T) diffusion_block_kernel(const int64_t* __res
   Affine bacc{1.0, 0.0};
   for (int64_t i = hi - 1; i >= lo; i--)
     bacc = compose(bacc, Affine{-cp[i], scratch[i]});
-  double x = block_scan_incoming<T, true>(bacc, sF, sG);
+  double x = block_scan_incoming1<T, true>(bacc, sF, sG);
   for (int64_t i = hi - 1; i >= lo; i--) {
     x = -cp[i] * x + scratch[i];
     vm[i] = x;
@@ -1410,7 +1416,7 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
     const double* __restrict__ x, int implicit_euler, double* __restrict__ grad_prefactor)
 {
   __shared__ double sF[2 * (T / 32) + 1], sG[2 * (T / 32) + 1];
-  __shared__ double sfirst[T], slast[T], sred[T / 32];
+  __shared__ double sfirst[T], slast[T], swfirst[T], swlast[T], sred[T / 32];
   const int f = blockIdx.x;
   const int tid = threadIdx.x;
   const int64_t o = fiber_offsets[f];
@@ -1435,7 +1441,8 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
       d[j] = 0.0;
     }
   }
-  double dp = block_scan_incoming<T, false>(acc, sF, sG);
+  // forward and backward scans with one barrier each, their warp totals in the two halves of sF/sG
+  double dp = block_scan_incoming1<T, false>(acc, sF, sG);
 #pragma unroll
   for (int j = 0; j < M; j++) {
     const int q = tid * M + j;
@@ -1451,8 +1458,7 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
     const int q = tid * M + j;
     bacc = compose(bacc, q < n ? Affine{-cp[o + q], d[j]} : Affine{0.0, 0.0});
   }
-  __syncthreads(); // sF/sG reuse
-  double xx = block_scan_incoming<T, true>(bacc, sF, sG);
+  double xx = block_scan_incoming1<T, true>(bacc, sF + T / 32, sG + T / 32);
 #pragma unroll
   for (int j = M - 1; j >= 0; j--) {
     const int q = tid * M + j;
@@ -1460,18 +1466,16 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
     mu[j] = xx;
     w[j] = q < n ? (implicit_euler ? x[o + q] : 0.5 * (x[o + q] + u[o + q])) : 0.0;
   }
-  // neighbours of the thread's first and last node: mu and w
+  // neighbours of the thread's first and last node: mu and w, exchanged together
   sfirst[tid] = mu[0];
   slast[tid] = mu[M - 1];
+  swfirst[tid] = w[0];
+  swlast[tid] = w[M - 1];
   __syncthreads();
   const double mu_prev = tid > 0 ? slast[tid - 1] : 0.0;
   const double mu_next = tid < T - 1 ? sfirst[tid + 1] : 0.0;
-  __syncthreads();
-  sfirst[tid] = w[0];
-  slast[tid] = w[M - 1];
-  __syncthreads();
-  const double w_prev = tid > 0 ? slast[tid - 1] : 0.0;
-  const double w_next = tid < T - 1 ? sfirst[tid + 1] : 0.0;
+  const double w_prev = tid > 0 ? swlast[tid - 1] : 0.0;
+  const double w_next = tid < T - 1 ? swfirst[tid + 1] : 0.0;
   // lam_u = B mu and the prefactor gradient -mu^T K1 w
   double g = 0.0;
 #pragma unroll
