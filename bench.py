@@ -508,6 +508,14 @@ def _cg_iteration(out: dict, device: int, peak_hbm: float, cg_mesh, cg_iteration
                                                   "8 iterations)"}}
 
 
+def workload_config(args, world: int) -> dict:
+    """The benchmark workload, the same dict in both arms (the implementation is described beside it)."""
+    return {"workload": "batched_hh: %d HH fibers/GPU, lengths U[500,2500] (seed=rank), 100 MUs, Poisson 10-40 Hz, "
+                        "Crank-Nicolson, dt0D 1e-4 ms, dt_split 1e-3 ms" % args.fibers,
+            "step": "%g ms = %d Strang steps" % (args.step_ms, int(round(args.step_ms / 1e-3))),
+            "l2": "inputs larger than L2", "parallelism": "fibers sharded, %d GPU(s), no collective" % world}
+
+
 def run_reference(args):
     world, rank, local, pg = dist_setup(args)
     if rank != 0:
@@ -524,12 +532,11 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": f"batched_hh sample: first {threads} fibers of the 4096-fiber HH batch (one per host "
-                                   "thread), 0.2 ms per step",
-                       "implementation": "CPU oracle port of the reference's vc FastMonodomainSolver (the reference "
-                                         "needs PETSc/MPI/Vc and cannot be built here)"},
+            "config": workload_config(args, world),
+            "implementation": "CPU oracle port of the reference's vc FastMonodomainSolver (the reference needs "
+                              "PETSc/MPI/Vc and cannot be built here), one fiber per host thread",
             "cpu_baseline": {"value": value, "unit": "node-steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{threads} fibers x 0.2 ms per step"},
+                             "sample": f"each step the first {threads} fibers of the batch over 0.2 ms"},
             "e2e": {"value": value, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -726,11 +733,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 reaction + f64 Vm/diffusion",
             "data": "synthetic (seeded)",
-            "config": {"workload": "batched_hh: 4096 HH fibers/GPU, lengths U[500,2500] (seed=rank), 100 MUs, "
-                                   "Poisson 10-40 Hz, Crank-Nicolson, dt0D 1e-4 ms, dt_split 1e-3 ms",
-                       "n_nodes_per_gpu": n_nodes, "step": f"{step} ms = {split_steps // args.steps} Strang steps",
-                       "method": "fused persistent kernel, FP32 reaction", "l2": "inputs larger than L2",
-                       "fused_shape": fused_shape, "parallelism": f"fibers sharded, {world} GPU(s), no collective"},
+            "config": workload_config(args, world),
+            "implementation": {"method": "fused persistent kernel, FP32 reaction", "n_nodes_per_gpu": n_nodes,
+                               "fused_shape": fused_shape},
             "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": args.steps},
             "gpu_launches": int(tm["kernel_launches"]),
