@@ -1970,10 +1970,8 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         acc = compose(acc, Affine{sc[0 * CAP + q], d[j]});
       }
       Affine tot_f;
-      // bins mode: one barrier per scan (block_scan_map1), forward and backward totals in separate halves of
-      // sF/sG; cluster mode keeps block_scan_map
-      const Affine ex_f = CLUSTER ? block_scan_map<T, false>(acc, sF, sG, &tot_f)
-                                  : block_scan_map1<T, false>(acc, sF, sG, &tot_f);
+      // one barrier per scan (block_scan_map1), the forward and backward warp totals in separate halves of sF/sG
+      const Affine ex_f = block_scan_map1<T, false>(acc, sF, sG, &tot_f);
       double dp = cluster_incoming(ex_f, tot_f, false);
 #pragma unroll
       for (int j = 0; j < M; j++) {
@@ -1987,14 +1985,11 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         const int q = j * T + tid;
         bacc = compose(bacc, Affine{-sc[1 * CAP + q], d[j]});
       }
-      // No barrier is needed before the backward scan: in bins mode its warp totals go to the other half of
-      // sF/sG (the forward totals may still be read).  Cluster mode keeps the barrier (block_scan_map reuses the
-      // same slots, and its scan totals travel through the cluster).
-      if constexpr (CLUSTER)
-        __syncthreads();
+      // No barrier is needed before the backward scan: its warp totals go to the other half of sF/sG (the
+      // forward totals may still be read).  In cluster mode the backward scan's CTA totals take other slots of
+      // ctot, and cpre is rewritten only after the backward cluster barrier, which every forward read precedes.
       Affine tot_b;
-      const Affine ex_b = CLUSTER ? block_scan_map<T, true>(bacc, sF, sG, &tot_b)
-                                  : block_scan_map1<T, true>(bacc, sF + T / 32, sG + T / 32, &tot_b);
+      const Affine ex_b = block_scan_map1<T, true>(bacc, sF + T / 32, sG + T / 32, &tot_b);
       double x = cluster_incoming(ex_b, tot_b, true);
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
@@ -2002,10 +1997,8 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         x = -sc[1 * CAP + q] * x + d[j];
         V[j] = x;
       }
-      // the next writes of vfirst/vlast and sF/sG come after the next diffusion's first barrier, which every
-      // read of this one precedes
-      if constexpr (CLUSTER)
-        __syncthreads();
+      // the next writes of vfirst/vlast, sF/sG and ctot come after the next diffusion's first (cluster)
+      // barrier, or after this one's backward cluster barrier, which every read of this one precedes
     }
     if (a.trace_slot) {
 #pragma unroll
