@@ -1206,86 +1206,15 @@ struct FusedArgs {
   int gate_stride;
 };
 
-// block-wide exclusive scan of affine maps in thread order (REVERSE: from the last thread down): returns the
+// Block-wide exclusive scan of affine maps in thread order (REVERSE: from the last thread down): returns the
 // composition of the maps of the threads before this one in scan order, and in *total (if given) the
-// composition of all threads' maps; sF/sG hold 2 * (T/32) + 1 doubles each
+// composition of all threads' maps.  A Hillis-Steele scan within each warp; the warp totals go to sF/sG[0, T/32)
+// and, after the one barrier, every warp scans the totals itself (rather than one warp scanning them and
+// broadcasting the prefixes through a second barrier).  sF/sG hold T/32 doubles each; a caller that scans again
+// without a barrier in between must give the next scan other slots (warps may still read these totals when a
+// fast warp writes the next ones).
 template<int T, bool REVERSE>
 __device__ __forceinline__ Affine block_scan_map(Affine acc, double* sF, double* sG, Affine* total)
-{
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int warp = tid >> 5;
-  constexpr int NW = T / 32;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    double F, G;
-    if (!REVERSE) {
-      F = __shfl_up_sync(0xffffffffu, acc.F, off);
-      G = __shfl_up_sync(0xffffffffu, acc.G, off);
-      if (lane >= off)
-        acc = compose(Affine{F, G}, acc);
-    } else {
-      F = __shfl_down_sync(0xffffffffu, acc.F, off);
-      G = __shfl_down_sync(0xffffffffu, acc.G, off);
-      if (lane + off < 32)
-        acc = compose(Affine{F, G}, acc);
-    }
-  }
-  // warp totals
-  const int last_lane = REVERSE ? 0 : 31;
-  if (lane == last_lane) {
-    sF[warp] = acc.F;
-    sG[warp] = acc.G;
-  }
-  // intra-warp exclusive prefix
-  double exF = REVERSE ? __shfl_down_sync(0xffffffffu, acc.F, 1) : __shfl_up_sync(0xffffffffu, acc.F, 1);
-  double exG = REVERSE ? __shfl_down_sync(0xffffffffu, acc.G, 1) : __shfl_up_sync(0xffffffffu, acc.G, 1);
-  const bool first_in_warp = REVERSE ? (lane == 31) : (lane == 0);
-  if (first_in_warp) {
-    exF = 1.0;
-    exG = 0.0;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    // exclusive scan over the NW warp totals, in scan order
-    const int w = REVERSE ? (NW - 1 - lane) : lane;
-    Affine v = lane < NW ? Affine{sF[w], sG[w]} : Affine{1.0, 0.0};
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const double F = __shfl_up_sync(0xffffffffu, v.F, off);
-      const double G = __shfl_up_sync(0xffffffffu, v.G, off);
-      if (lane >= off)
-        v = compose(Affine{F, G}, v);
-    }
-    double pF = __shfl_up_sync(0xffffffffu, v.F, 1);
-    double pG = __shfl_up_sync(0xffffffffu, v.G, 1);
-    if (lane == 0) {
-      pF = 1.0;
-      pG = 0.0;
-    }
-    __syncwarp();
-    if (lane < NW) {
-      sF[NW + w] = pF;
-      sG[NW + w] = pG;
-    }
-    if (lane == NW - 1) {
-      sF[2 * NW] = v.F;
-      sG[2 * NW] = v.G;
-    }
-  }
-  __syncthreads();
-  const Affine wp{sF[NW + warp], sG[NW + warp]};
-  if (total)
-    *total = Affine{sF[2 * NW], sG[2 * NW]};
-  return compose(wp, Affine{exF, exG});
-}
-
-// block_scan_map with one barrier: after the warp totals are in sF/sG[0, T/32), every warp scans them itself
-// (the same Hillis-Steele scan block_scan_map runs in warp 0, so the same values) instead of warp 0 scanning
-// and broadcasting through a second barrier.  sF/sG hold T/32 doubles each; a caller that scans again must
-// give the next scan other buffers (warps may still read these totals when a fast warp writes the next ones).
-template<int T, bool REVERSE>
-__device__ __forceinline__ Affine block_scan_map1(Affine acc, double* sF, double* sG, Affine* total)
 {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -1341,16 +1270,12 @@ __device__ __forceinline__ Affine block_scan_map1(Affine acc, double* sF, double
   return compose(wp, Affine{exF, exG});
 }
 
+// the value entering this thread's first node: the exclusive prefix map applied to the zero entering the
+// first node of the scan
 template<int T, bool REVERSE>
 __device__ __forceinline__ double block_scan_incoming(Affine acc, double* sF, double* sG)
 {
-  return block_scan_map<T, REVERSE>(acc, sF, sG, nullptr).G; // applied to the zero entering the first node
-}
-// the same with one barrier (block_scan_map1: the next scan takes other sF/sG slots or follows a barrier)
-template<int T, bool REVERSE>
-__device__ __forceinline__ double block_scan_incoming1(Affine acc, double* sF, double* sG)
-{
-  return block_scan_map1<T, REVERSE>(acc, sF, sG, nullptr).G;
+  return block_scan_map<T, REVERSE>(acc, sF, sG, nullptr).G;
 }
 
 // Split path, few fibers: one diffusion solve per fiber with one CTA per fiber (a warp per fiber would leave
@@ -1364,7 +1289,7 @@ __global__ void __launch_bounds__(T) diffusion_block_kernel(const int64_t* __res
                                                             const int* __restrict__ eq_counter,
                                                             const int* __restrict__ eq_nbuf, int n_ranks)
 {
-  __shared__ double sF[2 * (T / 32) + 1], sG[2 * (T / 32) + 1];
+  __shared__ double sF[T / 32], sG[T / 32]; // warp totals (both scans: the barrier between them orders the reuse)
   const int f = blockIdx.x;
   const int tid = threadIdx.x;
   if (eq_counter && eq_counter[f % n_ranks] == eq_nbuf[f % n_ranks])
@@ -1388,7 +1313,7 @@ __global__ void __launch_bounds__(T) diffusion_block_kernel(const int64_t* __res
   Affine acc{1.0, 0.0};
   for (int64_t i = lo; i < hi; i++)
     acc = compose(acc, Affine{mulF[i], inv[i] * rhs(i)});
-  double dp = block_scan_incoming1<T, false>(acc, sF, sG);
+  double dp = block_scan_incoming<T, false>(acc, sF, sG);
   for (int64_t i = lo; i < hi; i++) {
     dp = mulF[i] * dp + inv[i] * rhs(i);
     scratch[i] = dp;
@@ -1397,7 +1322,7 @@ __global__ void __launch_bounds__(T) diffusion_block_kernel(const int64_t* __res
   Affine bacc{1.0, 0.0};
   for (int64_t i = hi - 1; i >= lo; i--)
     bacc = compose(bacc, Affine{-cp[i], scratch[i]});
-  double x = block_scan_incoming1<T, true>(bacc, sF, sG);
+  double x = block_scan_incoming<T, true>(bacc, sF, sG);
   for (int64_t i = hi - 1; i >= lo; i--) {
     x = -cp[i] * x + scratch[i];
     vm[i] = x;
@@ -1415,7 +1340,7 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
     const double* __restrict__ coef, int64_t stride, double* __restrict__ lam, const double* __restrict__ u,
     const double* __restrict__ x, int implicit_euler, double* __restrict__ grad_prefactor)
 {
-  __shared__ double sF[2 * (T / 32) + 1], sG[2 * (T / 32) + 1];
+  __shared__ double sF[2 * (T / 32)], sG[2 * (T / 32)]; // warp totals: forward, backward
   __shared__ double sfirst[T], slast[T], swfirst[T], swlast[T], sred[T / 32];
   const int f = blockIdx.x;
   const int tid = threadIdx.x;
@@ -1442,7 +1367,7 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
     }
   }
   // forward and backward scans with one barrier each, their warp totals in the two halves of sF/sG
-  double dp = block_scan_incoming1<T, false>(acc, sF, sG);
+  double dp = block_scan_incoming<T, false>(acc, sF, sG);
 #pragma unroll
   for (int j = 0; j < M; j++) {
     const int q = tid * M + j;
@@ -1458,7 +1383,7 @@ __global__ void __launch_bounds__(T) adjoint_diffusion_block_kernel(
     const int q = tid * M + j;
     bacc = compose(bacc, q < n ? Affine{-cp[o + q], d[j]} : Affine{0.0, 0.0});
   }
-  double xx = block_scan_incoming1<T, true>(bacc, sF + T / 32, sG + T / 32);
+  double xx = block_scan_incoming<T, true>(bacc, sF + T / 32, sG + T / 32);
 #pragma unroll
   for (int j = M - 1; j >= 0; j--) {
     const int q = tid * M + j;
@@ -1970,8 +1895,8 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
         acc = compose(acc, Affine{sc[0 * CAP + q], d[j]});
       }
       Affine tot_f;
-      // one barrier per scan (block_scan_map1), the forward and backward warp totals in separate halves of sF/sG
-      const Affine ex_f = block_scan_map1<T, false>(acc, sF, sG, &tot_f);
+      // one barrier per scan (block_scan_map), the forward and backward warp totals in separate halves of sF/sG
+      const Affine ex_f = block_scan_map<T, false>(acc, sF, sG, &tot_f);
       double dp = cluster_incoming(ex_f, tot_f, false);
 #pragma unroll
       for (int j = 0; j < M; j++) {
@@ -1989,7 +1914,7 @@ __global__ void __launch_bounds__(T, 1) fused_kernel(FusedArgs a)
       // forward totals may still be read).  In cluster mode the backward scan's CTA totals take other slots of
       // ctot, and cpre is rewritten only after the backward cluster barrier, which every forward read precedes.
       Affine tot_b;
-      const Affine ex_b = block_scan_map1<T, true>(bacc, sF + T / 32, sG + T / 32, &tot_b);
+      const Affine ex_b = block_scan_map<T, true>(bacc, sF + T / 32, sG + T / 32, &tot_b);
       double x = cluster_incoming(ex_b, tot_b, true);
 #pragma unroll
       for (int j = M - 1; j >= 0; j--) {
