@@ -202,7 +202,10 @@ class _PinnedBuffer:
 
     def __del__(self):
         if self.ptr:
-            lib().fdm_host_free(C.c_void_p(self.ptr))
+            try:
+                lib().fdm_host_free(C.c_void_p(self.ptr))
+            except Exception:  # noqa: BLE001 - interpreter shutdown: the library may be gone already
+                pass
             self.ptr = None
 
 
