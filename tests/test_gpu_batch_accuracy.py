@@ -5,8 +5,8 @@
   every 1 ms, and its activation steps at 32 nodes per fiber within one split step; the FP64 fused solver equal
   to the FP64 split ("plain") solver on 64 fibers of the batch to 1e-6 mV with identical activation steps.
 * The FP64 split solver against the CPU oracle on the shortest fibers of that batch over the same 100 ms:
-  Vm to 1e-6 mV and identical activation steps at 32 nodes per fiber (OPENDIHU_ORACLE_FIBERS fibers, 16 by
-  default; the oracle runs on all host cores).
+  Vm to 1e-6 mV and identical activation steps at 32 nodes per fiber (OPENDIHU_ORACLE_FIBERS fibers, 64 by
+  default; the oracle runs on all host cores, about 3 minutes on 16).
 * Shorten 2007 (56 states) over 2 ms with an action potential: split FP64 against the oracle to 1e-6 mV, the
   FP32 reaction within 0.1 mV.
 """
@@ -41,7 +41,7 @@ def test_batch_fp32_fused_within_01mV_and_one_step_over_100ms():
 
 
 def test_fp64_split_equals_oracle_over_the_batch_span():
-    n_fibers = int(os.environ.get("OPENDIHU_ORACLE_FIBERS", "16"))
+    n_fibers = int(os.environ.get("OPENDIHU_ORACLE_FIBERS", "64"))
     system = WL.batched_hh(n_fibers=4096, seed=0)
     lengths = np.diff(np.asarray(system.fiber_offsets))
     pick = np.sort(np.argsort(lengths, kind="stable")[:n_fibers])   # the shortest fibers: bounded CPU time
